@@ -1,0 +1,315 @@
+"""Benchmark: grid-point RK steps/s of the LEE time advance on B200.
+
+Workload (one GPU): 3-D curvilinear block of 256^3 points, x = xi + 0.1 sin(2 pi eta/L)
+sin(2 pi zeta/L) and cyclic permutations, uniform mean flow Mach 0.5 along x, eight
+Gaussian pulses (amplitude 1e-3, half-width 4, centres from numpy seed 2), RK4 at
+CFL 0.5, 4th-order central differences and the 8th-order filter. Synthetic data.
+
+The headline form is FP32 with compensated accumulation; the plain FP64 form is timed
+in the same run for the mixed-vs-FP64 ratio, and the p' error of the compensated form
+against FP64 after 500 steps is measured in the same run.
+
+`python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]`
+For N > 1 (torchrun) every rank advances its own replica: the path does not shard
+(one GPU holds all blocks; no inter-GPU exchange), so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from camille_b200 import api, cases  # noqa: E402
+
+METRIC = "grid-point RK steps/s, mixed vs FP64 @<=1e-5 rel L2 p'; adjoint/forward time"
+UNIT = "grid-point RK steps/s"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def measured_hbm_gbs() -> tuple[float, str]:
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.TemporaryFile(mode="w+")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu)], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def stage_bytes_per_point(info, comp: bool) -> float:
+    """Algorithmic HBM bytes per grid point of one fused stage launch, averaged over the
+    four RK4 stages: every stage reads its input, y_n and the accumulator once and writes
+    the next input and the accumulator once (words per stage: FP64 3,5,5,3 x V;
+    compensated 4,5,5,5 x V), plus the non-uniform coefficient fields."""
+    V, e = info.state_vars, info.bytes_per_value
+    words = (4 + 5 + 5 + 5) / 4.0 if comp else (3 + 5 + 5 + 3) / 4.0
+    return words * V * e + info.num_coef_fields * e
+
+
+def step_bytes_per_point(info, comp: bool, dim: int) -> float:
+    """Algorithmic bytes per grid point per RK4 step: four stages and the filter passes
+    (FP64: read+write per pass plus the blend input; compensated: the increment sums)."""
+    V, e = info.state_vars, info.bytes_per_value
+    if comp:
+        filt = {2: 3 + 6, 3: 3 + 4 + 6}[dim]
+    else:
+        filt = {2: 2 + 3, 3: 2 + 2 + 3}[dim]
+    return 4 * stage_bytes_per_point(info, comp) + filt * V * e
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.n
+    case = cases.curvi3d(n=n, nsteps=args.error_steps)
+    lib = api.product_library()
+    K, W = args.steps, args.warmup
+    results = {}
+    solvers = {}
+    clocks = None
+    for form, prec in (("fp32c", api.FP32_COMPENSATED), ("fp64", api.FP64)):
+        s = api.Solver(lib, case, precision=prec, device=local)
+        solvers[form] = s
+        dt = s.compute_dt(case.cfl)
+        s.advance(W, dt)
+        barrier()
+        sampler = ClockSampler(local) if form == "fp32c" else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        s.set_timing(True)
+        s.advance(K, dt)
+        st = s.stats()
+        s.set_timing(False)
+        barrier()
+        if sampler:
+            clocks = sampler.stop()
+        ms = max_over_ranks(st.advance_ms)
+        info = s.info()
+        results[form] = {"ms": ms, "stats": st, "info": info, "dt": dt}
+    npts = case.npoints
+
+    # accuracy of the compensated form against FP64 at the step count of the workload
+    done = W + K
+    for s in solvers.values():
+        if args.error_steps > done:
+            s.advance(args.error_steps - done, results["fp64"]["dt"])
+    p32 = solvers["fp32c"].download(0)[0][4]
+    p64 = solvers["fp64"].download(0)[0][4]
+    err = api.rel_l2(p32, p64)
+    solvers["fp64"].close()
+
+    # end to end through the C ABI with host buffers: upload from pinned host memory,
+    # K steps, download of the state to pinned host memory
+    s = solvers["fp32c"]
+    host_in = [torch.from_numpy(np.ascontiguousarray(case.blocks[0].state[v])).pin_memory() for v in range(5)]
+    host_out = [torch.empty_like(host_in[v]).pin_memory() for v in range(5)]
+    pin_in = (C.POINTER(C.c_double) * 5)(*[C.cast(t.data_ptr(), C.POINTER(C.c_double)) for t in host_in])
+    pin_out = (C.POINTER(C.c_double) * 5)(*[C.cast(t.data_ptr(), C.POINTER(C.c_double)) for t in host_out])
+    dt = results["fp32c"]["dt"]
+    barrier()
+    t0 = time.perf_counter()
+    s._chk(lib.upload_state(s.ctx, 0, pin_in, 0, 0.0))
+    s._chk(lib.advance(s.ctx, K, dt))
+    stp, tm = C.c_int(), C.c_double()
+    s._chk(lib.download_state(s.ctx, 0, pin_out, C.byref(stp), C.byref(tm)))
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    state_bytes = 5 * npts * 8
+
+    r32, r64 = results["fp32c"], results["fp64"]
+    value = world * npts * K / (r32["ms"] / 1e3)
+    value64 = world * npts * K / (r64["ms"] / 1e3)
+    st = r32["stats"]
+    info = r32["info"]
+    peak, peak_kind = measured_hbm_gbs()
+    stage_avg_ms = st.stage_ms / max(st.stage_launches, 1)
+    filt_avg_ms = st.filter_ms / max(st.filter_launches, 1)
+    stage_b = stage_bytes_per_point(info, True) * npts
+    achieved = stage_b / (stage_avg_ms / 1e3) / 1e9
+    step_b = step_bytes_per_point(info, True, 3) * npts
+    step_gbs = step_b * K / (r32["ms"] / 1e3) / 1e9
+    dominant = "stage" if st.stage_ms >= st.filter_ms else "filter"
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": r32["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32-compensated (fp64 setup)", "data": "synthetic",
+            "config": {"workload": f"curvi3d {n}^3 Mach 0.5, 8 Gaussian pulses (seed 2), RK4 CFL 0.5, "
+                                   "OA4 central FD + OA8 filter, closures only",
+                       "points_per_gpu": npts, "parallelism": f"replicas x{world} (no sharding)",
+                       "l2": "inputs larger than L2 (state 335 MB fp32 / 671 MB fp64 vs 126 MB L2)",
+                       "dt": dt},
+            "fp64": {"value": value64, "ms_per_step": r64["ms"] / K},
+            "mixed_over_fp64": value / value64,
+            "p_rel_l2_vs_fp64": {"value": err, "steps": max(args.error_steps, W + K)},
+            "roofline": {"bound": "hbm", "kernel": "fused RK stage (fp32-compensated)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} copy bandwidth", "traffic": None,
+                         "bytes_per_point": stage_bytes_per_point(info, True),
+                         "avg_launch_ms": stage_avg_ms, "dominant": dominant,
+                         "filter_avg_launch_ms": filt_avg_ms,
+                         "step_gbs": step_gbs, "step_frac": step_gbs / peak,
+                         "step_bytes_per_point": step_bytes_per_point(info, True, 3)},
+            "e2e": {"value": world * npts * K / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K,
+                    "note": "lee_upload_state from pinned host memory, lee_advance(K), lee_download_state"},
+            "gpu_launches": int(st.kernel_launches),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    solvers["fp32c"].close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(args) -> dict:
+    """The compiled reference (oracle/_ref) on a bounded sample of the workload."""
+    try:
+        from oracle import run_ref
+        if not run_ref.available():
+            return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                    "sample": "oracle/_ref/camille_ref not built"}
+        n, k = args.cpu_n, args.cpu_steps
+        case = cases.curvi3d(n=n, nsteps=k)
+        r = run_ref.run(case, mode="run", nsteps=k, dt=0.28, timeout=600)
+        sec = r["result"]["seconds"]
+        return {"value": n ** 3 * k / sec, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"curvi3d {n}^3, {k} RK4 steps, solver::solve wall time, 1 rank, g++ -O3"}
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+
+def run_reference(args) -> None:
+    """Reference arm: the camille reference's own FP64 CPU solver on this box's cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import run_ref
+    if not run_ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/camille_ref is not built"}))
+        return
+    cores = os.cpu_count() or 1
+    nprocs = max(1, min(args.ref_ranks or cores, 8))
+    n = args.ref_n
+    steps = args.steps + args.warmup
+    case = cases.curvi3d(n=n, nsteps=steps)
+    r = run_ref.run(case, mode="run", nsteps=steps, dt=0.28, nprocs=nprocs, timeout=1800)
+    sec = r["result"]["seconds"]
+    value = n ** 3 * steps / sec
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": steps, "warmup": 0, "ms_per_step": sec * 1e3 / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"curvi3d {n}^3 (bounded sample of the 256^3 workload), Mach 0.5, "
+                                   "RK4, OA4 FD + OA8 filter", "ranks": nprocs},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nprocs, "kind": "reference",
+                             "sample": f"curvi3d {n}^3 x {steps} steps, {nprocs} MPI ranks (DECOMP_1D)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--error-steps", type=int, default=500)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-n", type=int, default=64)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--ref-n", type=int, default=48)
+    ap.add_argument("--ref-ranks", type=int, default=1)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,243 @@
+"""ctypes binding of the C ABI in include/lee_b200.h.
+
+``Library`` binds one shared object exporting that ABI under a symbol prefix:
+``lee_`` for this package's CUDA library (camille_b200/liblee_b200.so) and
+``orc_`` for the test-only CPU oracle. ``Solver`` drives a :class:`cases.Case`
+through the calls in the order a replacement ``solver::solve`` makes them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import cases as _cases
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+PRODUCT_LIB = os.path.join(PKG, "liblee_b200.so")
+
+LEE_OK = 0
+ERRORS = {1: "LEE_ERR_ARG", 2: "LEE_ERR_STATE", 3: "LEE_ERR_CUDA", 4: "LEE_ERR_NOMEM",
+          5: "LEE_ERR_UNSUPPORTED", 6: "LEE_ERR_NONFINITE", 7: "LEE_ERR_NODEVICE", 8: "LEE_ERR_TIMEOUT"}
+FD = {"STANDARD_CENTRAL": 1, "FDO11P": 11}
+FILTER = {"NONE": 0, "STANDARD_CENTRAL": 1, "SFO11P": 11}
+RK = {"RUNGE_KUTTA2": 2, "RUNGE_KUTTA4": 4}
+FP64, FP32_COMPENSATED = 0, 1
+SETUP_METRICS, SETUP_JACOBIAN, SETUP_MEAN_GRADIENT, SETUP_SPONGE = 0, 1, 2, 3
+SOURCE_MONOPOLE = 1
+
+
+class LeeConfig(C.Structure):
+    _fields_ = [
+        ("num_dim", C.c_int), ("num_blocks", C.c_int), ("gamma", C.c_double),
+        ("fd_scheme", C.c_int), ("fd_order", C.c_int),
+        ("filter_scheme", C.c_int), ("filter_order", C.c_int),
+        ("filter_strength", C.c_double), ("filter_blend", C.c_double),
+        ("rk_scheme", C.c_int), ("precision", C.c_int),
+        ("sponge_order", C.c_int), ("sponge_constant", C.c_double),
+        ("device", C.c_int),
+    ]
+
+
+class LeeInfo(C.Structure):
+    _fields_ = [("points", C.c_longlong), ("state_vars", C.c_int), ("bytes_per_value", C.c_int),
+                ("num_coef_fields", C.c_int), ("device_bytes", C.c_longlong)]
+
+
+class LeeStats(C.Structure):
+    _fields_ = [("advance_ms", C.c_double), ("stage_ms", C.c_double), ("filter_ms", C.c_double),
+                ("stage_launches", C.c_longlong), ("filter_launches", C.c_longlong),
+                ("kernel_launches", C.c_longlong)]
+
+
+class LeeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+_PP = C.POINTER(_DP)
+
+# name -> (restype, argtypes); the first argument of most is the context pointer.
+SIGNATURES = {
+    "create": (C.c_int, [C.POINTER(LeeConfig), C.POINTER(C.c_void_p)]),
+    "destroy": (None, [C.c_void_p]),
+    "last_error": (C.c_char_p, [C.c_void_p]),
+    "set_block": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _IP]),
+    "set_mean": (C.c_int, [C.c_void_p, C.c_int, _PP]),
+    "add_boundary": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP]),
+    "set_source": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
+    "prepare": (C.c_int, [C.c_void_p]),
+    "upload_state": (C.c_int, [C.c_void_p, C.c_int, _PP, C.c_int, C.c_double]),
+    "download_state": (C.c_int, [C.c_void_p, C.c_int, _PP, _IP, _DP]),
+    "compute_dt": (C.c_int, [C.c_void_p, C.c_double, _DP]),
+    "advance": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "eval_rhs": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _PP]),
+    "apply_filter": (C.c_int, [C.c_void_p]),
+    "get_setup": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _DP]),
+    "get_info": (C.c_int, [C.c_void_p, C.POINTER(LeeInfo)]),
+    "set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "get_stats": (C.c_int, [C.c_void_p, C.POINTER(LeeStats)]),
+}
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+def _fields_ptrs(arrs) -> C.Array:
+    return (_DP * len(arrs))(*[_dptr(a) for a in arrs])
+
+
+class Library:
+    def __init__(self, path: str, prefix: str):
+        if not os.path.isfile(path):
+            raise FileNotFoundError(f"{path} is not built")
+        self.path = path
+        self.prefix = prefix
+        self.dll = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(self.dll, prefix + name)
+            fn.restype = res
+            fn.argtypes = args
+            setattr(self, name, fn)
+
+
+def product_library() -> Library:
+    """The CUDA library. Raises if it is not built: there is no CPU fallback."""
+    return Library(PRODUCT_LIB, "lee_")
+
+
+def config_for(case: "_cases.Case", precision: int = FP64, device: int = 0) -> LeeConfig:
+    return LeeConfig(
+        num_dim=case.num_dim, num_blocks=len(case.blocks), gamma=case.gamma,
+        fd_scheme=FD[case.fd_scheme], fd_order=case.fd_order,
+        filter_scheme=FILTER[case.filter_scheme], filter_order=case.filter_order,
+        filter_strength=case.filter_strength, filter_blend=case.filter_blend,
+        rk_scheme=RK[case.rk], precision=precision,
+        sponge_order=case.sponge_order, sponge_constant=case.sponge_constant, device=device)
+
+
+class Solver:
+    """A context loaded with one Case: grids, means, boundaries, source and state."""
+
+    def __init__(self, lib: Library, case: "_cases.Case", precision: int = FP64, device: int = 0,
+                 upload: bool = True):
+        self.lib = lib
+        self.case = case
+        self.ctx = C.c_void_p()
+        cfg = config_for(case, precision, device)
+        rc = lib.create(C.byref(cfg), C.byref(self.ctx))
+        if rc != LEE_OK:
+            raise LeeError(rc, lib.last_error(None).decode())
+        try:
+            for b, blk in enumerate(case.blocks):
+                nx, ny, nz = blk.dims
+                xs = [np.ascontiguousarray(a, np.float64) for a in (blk.x, blk.y, blk.z)]
+                ib = None
+                if blk.iblank is not None:
+                    ibarr = np.ascontiguousarray(blk.iblank, np.int32)
+                    ib = ibarr.ctypes.data_as(_IP)
+                self._chk(lib.set_block(self.ctx, b, nx, ny, nz, *[_dptr(a) for a in xs], ib))
+                mean = [np.ascontiguousarray(blk.mean[v], np.float64) for v in range(5)]
+                self._chk(lib.set_mean(self.ctx, b, _fields_ptrs(mean)))
+            for bd in case.boundaries:
+                lo = (C.c_int * 3)(*bd.lo)
+                hi = (C.c_int * 3)(*bd.hi)
+                self._chk(lib.add_boundary(self.ctx, bd.block, _cases.BC_TYPES[bd.kind], bd.dir, bd.end,
+                                           lo, hi, None))
+            if case.monopole is not None:
+                p = np.array(case.monopole, np.float64)
+                self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))
+            self._chk(lib.prepare(self.ctx))
+            if upload:
+                for b, blk in enumerate(case.blocks):
+                    self.upload(b, blk.state)
+        except Exception:
+            self.close()
+            raise
+
+    def _chk(self, rc: int) -> None:
+        if rc != LEE_OK:
+            raise LeeError(rc, self.lib.last_error(self.ctx).decode())
+
+    def close(self) -> None:
+        if self.ctx:
+            self.lib.destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, b: int, state: np.ndarray, step: int = 0, time: float = 0.0) -> None:
+        f = [np.ascontiguousarray(state[v], np.float64) for v in range(5)]
+        self._chk(self.lib.upload_state(self.ctx, b, _fields_ptrs(f), step, time))
+
+    def download(self, b: int = 0) -> tuple[np.ndarray, int, float]:
+        nx, ny, nz = self.case.blocks[b].dims
+        out = np.zeros((5, nz, ny, nx))
+        ptrs = _fields_ptrs([out[v] for v in range(5)])
+        step = C.c_int()
+        time = C.c_double()
+        self._chk(self.lib.download_state(self.ctx, b, ptrs, C.byref(step), C.byref(time)))
+        return out, step.value, time.value
+
+    def compute_dt(self, cfl: Optional[float] = None) -> float:
+        dt = C.c_double()
+        self._chk(self.lib.compute_dt(self.ctx, self.case.cfl if cfl is None else cfl, C.byref(dt)))
+        return dt.value
+
+    def advance(self, nsteps: int, dt: float) -> None:
+        self._chk(self.lib.advance(self.ctx, nsteps, dt))
+
+    def eval_rhs(self, b: int = 0, time: float = 0.0) -> np.ndarray:
+        nx, ny, nz = self.case.blocks[b].dims
+        out = np.zeros((5, nz, ny, nx))
+        self._chk(self.lib.eval_rhs(self.ctx, b, time, _fields_ptrs([out[v] for v in range(5)])))
+        return out
+
+    def apply_filter(self) -> None:
+        self._chk(self.lib.apply_filter(self.ctx))
+
+    def get_setup(self, b: int, what: int) -> np.ndarray:
+        nx, ny, nz = self.case.blocks[b].dims
+        nf = {SETUP_METRICS: 9, SETUP_JACOBIAN: 1, SETUP_MEAN_GRADIENT: 5 * self.case.num_dim,
+              SETUP_SPONGE: 1}[what]
+        out = np.zeros((nf, nz, ny, nx))
+        self._chk(self.lib.get_setup(self.ctx, b, what, _dptr(out)))
+        return out
+
+
+def _solver_info(self) -> LeeInfo:
+    info = LeeInfo()
+    self._chk(self.lib.get_info(self.ctx, C.byref(info)))
+    return info
+
+
+def _solver_stats(self) -> LeeStats:
+    st = LeeStats()
+    self._chk(self.lib.get_stats(self.ctx, C.byref(st)))
+    return st
+
+
+def _solver_timing(self, on: bool) -> None:
+    self._chk(self.lib.set_timing(self.ctx, 1 if on else 0))
+
+
+Solver.info = _solver_info
+Solver.stats = _solver_stats
+Solver.set_timing = _solver_timing
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    """Relative L2 norm of a - b with respect to b."""
+    nb = float(np.linalg.norm(b.ravel()))
+    d = float(np.linalg.norm((a - b).ravel()))
+    return d / nb if nb > 0 else d

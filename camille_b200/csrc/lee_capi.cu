@@ -1,0 +1,1190 @@
+// Host side of the C ABI (include/lee_b200.h): context, device memory, one-time
+// setup on the GPU, and the time-advance schedule.
+//
+// Schedule of one step (temporal::time_advance, camille src/solver/temporal_discretization.cpp:334-374):
+//   time += dt (solver::solve increments before advancing, src/solver/solver.cpp:72)
+//   for each RK stage s: one fused stage kernel per block (RHS + RK update, reading the
+//     stage input with its stencil neighbours and writing the next stage input and the
+//     accumulator), then the boundary conditions of the stage output
+//   filter passes (dimension split, src/solver/spatial_discretization.cpp:2191-2246)
+//   hole mask (temporal::iblank_correction, :380-393)
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "lee_internal.h"
+
+using namespace lee;
+
+namespace {
+
+char g_create_error[512] = "";
+
+struct Boundary {
+  int kind, dir, end, lo[3], hi[3];
+  std::vector<double> sigma;  // host copy when given by the caller
+  double* d_sigma = nullptr;  // FP64 strengths
+  void* d_sigma_t = nullptr;  // strengths in the working precision
+};
+
+struct BlockData {
+  int nx = 0, ny = 0, nz = 0;
+  long long N = 0;
+  bool set = false, has_mean = false;
+  std::vector<double> hx, hy, hz;
+  std::vector<int> hib;
+  std::vector<double> hmean[5];
+  std::vector<Boundary> bnd;
+  // FP64 setup products
+  double* d_xyz[3] = {};
+  double* d_mean[5] = {};
+  double* d_met[9] = {};
+  double* d_minv[9] = {};
+  double* d_jac = nullptr;
+  double* d_invjac = nullptr;
+  double* d_grad[15] = {};
+  double* d_jm[9] = {};
+  double* d_rbi = nullptr;
+  int* d_iblank = nullptr;
+  int8_t* d_code_fd[3] = {};
+  int8_t* d_code_flt[3] = {};
+  bool has_holes = false;
+  // monopole factor on a box
+  int src_lo[3] = {0, 0, 0}, src_hi[3] = {-1, -1, -1};
+  double* d_src_g = nullptr;
+  void* d_src_g_t = nullptr;
+  // coefficients in the working precision
+  Coef<double> cd_jm[9], cd_ub[3], cd_pb, cd_rbi, cd_gs[3], cd_gu[9], cd_gp[3];
+  Coef<float> cf_jm[9], cf_ub[3], cf_pb, cf_rbi, cf_gs[3], cf_gu[9], cf_gp[3];
+  int need_rho = 0;
+  int n_coef_fields = 0;
+  // state buffers (element size 8 or 4), V fields each
+  void* y[kMaxVars] = {};
+  void* acc[kMaxVars] = {};
+  void* zb[2][kMaxVars] = {};
+  void* comp[kMaxVars] = {};
+  void* dsum[kMaxVars] = {};
+  void* rho_prev = nullptr;
+  void* rho_next = nullptr;
+};
+
+}  // namespace
+
+struct lee_ctx {
+  lee_config cfg;
+  int V = 0;
+  size_t esz = 8;
+  bool comp = false;
+  OpTable fd{}, flt{}, fltd{};
+  std::vector<BlockData> blk;
+  cudaStream_t stream = nullptr;
+  int src_kind = LEE_SOURCE_NONE;
+  double src[7] = {0, 0, 0, 0, 0, 0, 0};
+  bool prepared = false, uploaded = false;
+  int step = 0;
+  double time = 0.0;
+  std::vector<void*> allocs;
+  long long device_bytes = 0;
+  std::string err;
+  // timing
+  bool timing = false;
+  lee_stats stats{};
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_marks;  // (kind, event index pair start); kind 0 stage, 1 filter
+  size_t ev_used = 0;
+};
+
+namespace {
+
+int fail(lee_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c)
+    c->err = buf;
+  else
+    snprintf(g_create_error, sizeof g_create_error, "%s", buf);
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(c, LEE_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
+  } while (0)
+
+int dev_alloc(lee_ctx* c, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 8);
+  if (e != cudaSuccess) return fail(c, LEE_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+  c->allocs.push_back(*p);
+  c->device_bytes += (long long)bytes;
+  return LEE_OK;
+}
+
+template <typename P>
+int dalloc(lee_ctx* c, P** p, size_t count) {
+  return dev_alloc(c, reinterpret_cast<void**>(p), count * sizeof(P));
+}
+
+// Coefficient tables (src/solver/spatial_discretization.cpp:28-492); the numbers are the
+// published tables (Lele 1992; Bogey & Bailly 2004; Berland et al. 2007).
+bool make_fd(OpTable* o, int scheme, int order) {
+  memset(o, 0, sizeof *o);
+  o->mfac = -1.0;
+  if (scheme == LEE_FD_STANDARD_CENTRAL && order == 4) {
+    o->h = 2; o->nb = 2; o->S = 3;
+    o->c[3] = 8.0 / 12.0; o->c[4] = -1.0 / 12.0;
+    o->B[0][0] = -3.0 / 2.0; o->B[0][1] = 4.0 / 2.0; o->B[0][2] = -1.0 / 2.0;
+    o->B[1][0] = -1.0 / 2.0; o->B[1][1] = 0.0; o->B[1][2] = 1.0 / 2.0;
+  } else if (scheme == LEE_FD_FDO11P) {
+    o->h = 5; o->nb = 5; o->S = 9;
+    const double in[6] = {0.0, 0.872756993962, -0.286511173973, 0.090320001280, -0.020779405824, 0.002484594688};
+    for (int k = 0; k <= 5; ++k) o->c[5 + k] = in[k];
+    const double r0[7] = {-2.225833963270, 4.827779580575, -5.001388453836, 3.911103941646,
+                          -2.115267458633, 0.718882784412, -0.115276430894};
+    const double r1[7] = {-0.212932721951, -1.060320390770, 2.078926116439, -1.287179452384,
+                          0.685176395471, -0.245320613994, 0.041650667189};
+    const double r2[5] = {1.0 / 12.0, -8.0 / 12.0, 0.0, 8.0 / 12.0, -1.0 / 12.0};
+    const double r3[7] = {-0.02625099337517627, 0.18833730683403838, -0.797921633542548, 0.0,
+                          0.797921633542548, -0.18833730683403838, 0.02625099337517627};
+    const double r4[9] = {0.007650904064, -0.059463584768, 0.244678631765, -0.841570125482, 0.0,
+                          0.841570125482, -0.244678631765, 0.059463584768, -0.007650904064};
+    for (int s = 0; s < 7; ++s) { o->B[0][s] = r0[s]; o->B[1][s] = r1[s]; o->B[3][s] = r3[s]; }
+    for (int s = 0; s < 5; ++s) o->B[2][s] = r2[s];
+    for (int s = 0; s < 9; ++s) o->B[4][s] = r4[s];
+  } else {
+    return false;
+  }
+  for (int k = 1; k <= o->h; ++k) o->c[o->h - k] = -o->c[o->h + k];
+  return true;
+}
+
+bool make_filter(OpTable* o, int scheme, int order, double strength) {
+  memset(o, 0, sizeof *o);
+  o->mfac = 1.0;
+  const double r2[5] = {(-1.0 / 8.0) / 2.0, (1.0 / 2.0) / 2.0, 5.0 / 8.0, (1.0 / 2.0) / 2.0, (-1.0 / 8.0) / 2.0};
+  const double r3[7] = {(1.0 / 32.0) / 2.0, (-3.0 / 16.0) / 2.0, (15.0 / 32.0) / 2.0, 11.0 / 16.0,
+                        (15.0 / 32.0) / 2.0, (-3.0 / 16.0) / 2.0, (1.0 / 32.0) / 2.0};
+  if (scheme == LEE_FILTER_STANDARD_CENTRAL && order == 4) {
+    o->h = 2; o->nb = 2; o->S = 3;
+    o->c[2] = 5.0 / 8.0; o->c[3] = (1.0 / 2.0) / 2.0; o->c[4] = (-1.0 / 8.0) / 2.0;
+    o->B[0][0] = 1.0; o->B[1][1] = 1.0;
+  } else if (scheme == LEE_FILTER_STANDARD_CENTRAL && order == 8) {
+    o->h = 4; o->nb = 4; o->S = 7;
+    o->c[4] = 1.0 - strength * (35.0 / 128.0);
+    const double d[4] = {-7.0 / 32.0, 7.0 / 64.0, -1.0 / 32.0, 1.0 / 256.0};
+    for (int k = 1; k <= 4; ++k) o->c[4 + k] = d[k - 1] * -strength;
+    o->B[0][0] = 1.0; o->B[1][1] = 1.0;
+    for (int s = 0; s < 5; ++s) o->B[2][s] = r2[s];
+    for (int s = 0; s < 7; ++s) o->B[3][s] = r3[s];
+  } else if (scheme == LEE_FILTER_SFO11P) {
+    o->h = 5; o->nb = 5; o->S = 9;
+    const double d[6] = {0.215044884112, -0.187772883589, 0.123755948787, -0.059227575576, 0.018721609157,
+                         -0.002999540835};
+    o->c[5] = 1.0 - strength * d[0];
+    for (int k = 1; k <= 5; ++k) o->c[5 + k] = d[k] * -strength;
+    o->B[0][0] = 1.0; o->B[1][1] = 1.0;
+    for (int s = 0; s < 5; ++s) o->B[2][s] = r2[s];
+    for (int s = 0; s < 7; ++s) o->B[3][s] = r3[s];
+    const double r4[9] = {0.008228661760, -0.045211119360, 0.120007591680, -0.204788880640, 0.243527493120,
+                          -0.204788880640, 0.120007591680, -0.045211119360, 0.008228661760};
+    for (int s = 0; s < 9; ++s) o->B[4][s] = (s == 4) ? 1.0 - strength * r4[s] : r4[s] * -strength;
+  } else {
+    return false;
+  }
+  for (int k = 1; k <= o->h; ++k) o->c[o->h - k] = o->c[o->h + k];
+  return true;
+}
+
+// F - I of a filter table: the increment form used by the compensated time advance.
+OpTable minus_identity(const OpTable& f) {
+  OpTable d = f;
+  d.c[d.h] -= 1.0;
+  for (int r = 0; r < d.nb; ++r) d.B[r][r] -= 1.0;
+  return d;
+}
+
+// Closure codes of one direction: the reference's per-line scan (see lee_internal.h).
+// Returns false when a hole closure would lack fluid support (the reference asserts,
+// src/solver/spatial_discretization.cpp:1749-1798).
+bool closure_codes(const OpTable& op, const BlockData& b, int d, std::vector<int8_t>& code) {
+  int n[3] = {b.nx, b.ny, b.nz};
+  long long st[3] = {1, b.nx, (long long)b.nx * b.ny};
+  int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+  int nd = n[d];
+  code.assign((size_t)b.N, 0);
+  for (int b2 = 0; b2 < n[o2]; ++b2)
+    for (int b1 = 0; b1 < n[o1]; ++b1) {
+      long long base = b1 * st[o1] + b2 * st[o2];
+      auto at = [&](int p) { return base + p * st[d]; };
+      for (int p = 0; p < nd; ++p) {
+        int c = 0;
+        if (p < op.h) c = 1 + p;
+        else if (p > nd - 1 - op.h) c = -(1 + (nd - 1 - p));
+        code[(size_t)at(p)] = (int8_t)c;
+      }
+      int last = b.hib[(size_t)at(0)];
+      for (int p = 0; p < nd; ++p) {
+        int my = b.hib[(size_t)at(p)];
+        if (my == 1) {
+          if (last == 1) {
+            code[(size_t)at(p)] = kCodeZero;
+          } else if (last == -1 && p > 0) {  // `last_iblank /= BLANKED` (:1391) is true only after -1
+            for (int ib = 0; ib < op.nb; ++ib) {
+              int q = p - 1 - ib;
+              if (q < 0 || b.hib[(size_t)at(q)] > 0) return false;
+            }
+            if (p - 1 - (op.S - 1) < 0) return false;  // the mirrored rows read S points to the left
+            for (int ib = 0; ib < op.nb; ++ib) code[(size_t)at(p - 1 - ib)] = (int8_t)(-(1 + ib));
+          }
+        } else if (last == 1) {
+          for (int ib = 0; ib < op.nb; ++ib) {
+            int q = p + ib;
+            if (q > nd - 1 || b.hib[(size_t)at(q)] > 0) return false;
+          }
+          if (p + op.S - 1 > nd - 1) return false;  // the rows read S points to the right
+          for (int ib = 0; ib < op.nb; ++ib) code[(size_t)at(p + ib)] = (int8_t)(1 + ib);
+        }
+        last = my;
+      }
+    }
+  return true;
+}
+
+// Record an event on the context stream (timing on); returns its index or -1.
+int mark(lee_ctx* c) {
+  if (!c->timing) return -1;
+  if (c->ev_used == c->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    c->ev_pool.push_back(e);
+  }
+  cudaEventRecord(c->ev_pool[c->ev_used], c->stream);
+  return (int)c->ev_used++;
+}
+
+void span(lee_ctx* c, int kind, int a, int b) {
+  if (a >= 0 && b >= 0) c->ev_marks.push_back({kind, a});
+  (void)b;
+}
+
+template <typename T>
+__global__ void k_convert(long long n, T* out, const double* in) {
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
+    out[l] = (T)in[l];
+}
+
+template <typename T>
+__global__ void k_to_double(long long n, double* out, const T* y, const T* comp) {
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
+    out[l] = comp ? (double)y[l] + (double)comp[l] : (double)y[l];
+}
+
+__global__ void k_zero_bytes(long long n, unsigned char* p) {
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
+    p[l] = 0;
+}
+
+int grid1d(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
+}
+
+// Decide whether an FP64 field is uniform over the block (then the kernels use a constant).
+int classify(lee_ctx* c, const double* d_field, long long N, double scale, double* lo, double* hi, bool* uniform,
+             bool* zero) {
+  double* d_mm = nullptr;
+  CK(cudaMallocAsync((void**)&d_mm, 2 * sizeof(double), c->stream));
+  double init[2] = {-1e308, -1e308};
+  CK(cudaMemcpyAsync(d_mm, init, sizeof init, cudaMemcpyHostToDevice, c->stream));
+  CK(setup_minmax((int)N, d_field, d_mm, c->stream));
+  double h[2];
+  CK(cudaMemcpyAsync(h, d_mm, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaFreeAsync(d_mm, c->stream));
+  *lo = -h[0];
+  *hi = h[1];
+  double mag = fmax(fabs(*lo), fabs(*hi));
+  *zero = mag <= 1e-12 * scale;
+  *uniform = *zero || (*hi - *lo) <= 1e-12 * mag;
+  return LEE_OK;
+}
+
+template <typename T>
+int make_coef(lee_ctx* c, BlockData& b, const double* d_field, double scale, Coef<T>* out) {
+  double lo, hi;
+  bool uni, zero;
+  int rc = classify(c, d_field, b.N, scale, &lo, &hi, &uni, &zero);
+  if (rc) return rc;
+  out->zero = zero ? 1 : 0;
+  if (uni) {
+    out->p = nullptr;
+    out->c = zero ? T(0) : (T)(0.5 * (lo + hi));
+    return LEE_OK;
+  }
+  b.n_coef_fields += 1;
+  if (std::is_same<T, double>::value) {
+    out->p = reinterpret_cast<const T*>(d_field);
+  } else {
+    T* d = nullptr;
+    rc = dalloc(c, &d, (size_t)b.N);
+    if (rc) return rc;
+    k_convert<T><<<grid1d(b.N), 256, 0, c->stream>>>(b.N, d, d_field);
+    CK(cudaGetLastError());
+    out->p = d;
+  }
+  out->c = T(0);
+  return LEE_OK;
+}
+
+int upload(lee_ctx* c, double** d, const std::vector<double>& h) {
+  int rc = dalloc(c, d, h.size());
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return LEE_OK;
+}
+
+// metrics::compute with Thomas-Lombard products (src/metrics/metrics.cpp:9-251), the
+// Jacobian (:255-328; 3-D determinant of oracle patch P1) and inverse metrics (:355-426).
+int compute_metrics(lee_ctx* c, BlockData& b) {
+  int dim = c->cfg.num_dim;
+  int N = (int)b.N;
+  cudaStream_t s = c->stream;
+  double* xx[9] = {};
+  int rc;
+  for (int q = 0; q < 9; ++q) {
+    if ((rc = dalloc(c, &b.d_met[q], (size_t)N))) return rc;
+    if ((rc = dalloc(c, &b.d_minv[q], (size_t)N))) return rc;
+    if ((rc = dalloc(c, &xx[q], (size_t)N))) return rc;
+    CK(cudaMemsetAsync(b.d_met[q], 0, (size_t)N * 8, s));
+    CK(cudaMemsetAsync(b.d_minv[q], 0, (size_t)N * 8, s));
+  }
+  if ((rc = dalloc(c, &b.d_jac, (size_t)N))) return rc;
+  if ((rc = dalloc(c, &b.d_invjac, (size_t)N))) return rc;
+  for (int ip = 0; ip < dim; ++ip)
+    for (int ic = 0; ic < dim; ++ic)
+      CK(setup_apply_dir(c->fd, b.nx, b.ny, b.nz, ic, b.d_xyz[ip], xx[ip * 3 + ic], nullptr, 1, s));
+  double** m = b.d_met;
+#define XX(p, q) xx[(p) * 3 + (q)]
+#define MT(l, i) m[(l) * 3 + (i)]
+  if (dim == 2) {
+    CK(setup_axpby(N, MT(0, 0), 1.0, XX(1, 1), 0.0, nullptr, s));
+    CK(setup_axpby(N, MT(0, 1), -1.0, XX(0, 1), 0.0, nullptr, s));
+    CK(setup_axpby(N, MT(1, 0), -1.0, XX(1, 0), 0.0, nullptr, s));
+    CK(setup_axpby(N, MT(1, 1), 1.0, XX(0, 0), 0.0, nullptr, s));
+  } else {
+    double *func = nullptr, *tmp = nullptr;
+    if ((rc = dalloc(c, &func, (size_t)N))) return rc;
+    if ((rc = dalloc(c, &tmp, (size_t)N))) return rc;
+    double* const* z = b.d_xyz;
+    // (product of a grid derivative and a coordinate, derivative direction,
+    //  target metric, sign, assign (1) or accumulate (0)), in the order of
+    //  compute_ThomasLombard_3D (src/metrics/metrics.cpp:133-251).
+    struct Term { int pa, pb, cz, dir, tl, ti; double sign; int assign; };
+    const Term terms[] = {
+        {1, 1, 2, 2, 0, 0, 1.0, 1}, {1, 1, 2, 0, 2, 0, -1.0, 1},
+        {0, 1, 2, 2, 0, 1, -1.0, 1}, {0, 1, 2, 0, 2, 1, 1.0, 1},
+        {0, 1, 1, 2, 0, 2, 1.0, 1}, {0, 1, 1, 0, 2, 2, -1.0, 1},
+        {1, 0, 2, 2, 1, 0, -1.0, 1}, {1, 0, 2, 1, 2, 0, 1.0, 0},
+        {0, 0, 2, 2, 1, 1, 1.0, 1}, {0, 0, 2, 1, 2, 1, -1.0, 0},
+        {0, 0, 1, 2, 1, 2, -1.0, 1}, {0, 0, 1, 1, 2, 2, 1.0, 0},
+        {1, 2, 2, 1, 0, 0, -1.0, 0}, {1, 2, 2, 0, 1, 0, 1.0, 0},
+        {0, 2, 2, 1, 0, 1, 1.0, 0}, {0, 2, 2, 0, 1, 1, -1.0, 0},
+        {0, 2, 1, 1, 0, 2, -1.0, 0}, {0, 2, 1, 0, 1, 2, 1.0, 0},
+    };
+    for (size_t t = 0; t < sizeof terms / sizeof terms[0]; ++t) {
+      const Term& T = terms[t];
+      if (t % 2 == 0) CK(setup_mul(N, func, XX(T.pa, T.pb), z[T.cz], s));
+      CK(setup_apply_dir(c->fd, b.nx, b.ny, b.nz, T.dir, func, tmp, nullptr, 1, s));
+      if (T.assign)
+        CK(setup_axpby(N, MT(T.tl, T.ti), T.sign, tmp, 0.0, nullptr, s));
+      else
+        CK(setup_axpby(N, MT(T.tl, T.ti), 1.0, MT(T.tl, T.ti), T.sign, tmp, s));
+    }
+  }
+#undef XX
+#undef MT
+  double** d_xx = nullptr;
+  double** d_mm = nullptr;
+  double** d_mi = nullptr;
+  if ((rc = dalloc(c, &d_xx, 9))) return rc;
+  if ((rc = dalloc(c, &d_mm, 9))) return rc;
+  if ((rc = dalloc(c, &d_mi, 9))) return rc;
+  CK(cudaMemcpyAsync(d_xx, xx, sizeof xx, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_mm, b.d_met, sizeof b.d_met, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_mi, b.d_minv, sizeof b.d_minv, cudaMemcpyHostToDevice, s));
+  CK(setup_jacobian(N, dim, d_xx, b.d_invjac, b.d_jac, s));
+  CK(setup_inverse_metrics(N, dim, d_mm, d_mi, s));
+  CK(cudaStreamSynchronize(s));
+  return LEE_OK;
+}
+
+template <typename T>
+void** as_void(T** p) {
+  return reinterpret_cast<void**>(p);
+}
+
+int alloc_fields(lee_ctx* c, void** f, long long N) {
+  for (int v = 0; v < c->V; ++v) {
+    int rc = dev_alloc(c, &f[v], (size_t)N * c->esz);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(f[v], 0, (size_t)N * c->esz, c->stream));
+  }
+  return LEE_OK;
+}
+
+// Map the reference's five slots (s', u', v', w', p') to the V device fields.
+int slot_of(int V, int v) { return v == V - 1 ? 4 : v; }
+
+template <typename T>
+void fill_stage_common(lee_ctx* c, BlockData& b, StageParams<T>& p) {
+  memset(&p, 0, sizeof p);
+  p.nx = b.nx; p.ny = b.ny; p.nz = b.nz;
+  p.dim = c->cfg.num_dim;
+  p.V = c->V;
+  const bool dbl = std::is_same<T, double>::value;
+  const Coef<T>* jm = dbl ? (const Coef<T>*)b.cd_jm : (const Coef<T>*)b.cf_jm;
+  const Coef<T>* ub = dbl ? (const Coef<T>*)b.cd_ub : (const Coef<T>*)b.cf_ub;
+  const Coef<T>* gs = dbl ? (const Coef<T>*)b.cd_gs : (const Coef<T>*)b.cf_gs;
+  const Coef<T>* gu = dbl ? (const Coef<T>*)b.cd_gu : (const Coef<T>*)b.cf_gu;
+  const Coef<T>* gp = dbl ? (const Coef<T>*)b.cd_gp : (const Coef<T>*)b.cf_gp;
+  for (int q = 0; q < 9; ++q) { p.jm[q] = jm[q]; p.gu[q] = gu[q]; }
+  for (int q = 0; q < 3; ++q) { p.ubar[q] = ub[q]; p.gs[q] = gs[q]; p.gp[q] = gp[q]; }
+  p.pbar = dbl ? *(const Coef<T>*)&b.cd_pb : *(const Coef<T>*)&b.cf_pb;
+  p.rhobar_inv = dbl ? *(const Coef<T>*)&b.cd_rbi : *(const Coef<T>*)&b.cf_rbi;
+  p.need_rho = b.need_rho;
+  p.gamma = (T)c->cfg.gamma;
+  p.inv_gamma = (T)(1.0 / c->cfg.gamma);
+  p.nzones = 0;
+  for (auto& z : b.bnd) {
+    if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+    Zone<T>& zn = p.zones[p.nzones++];
+    for (int d = 0; d < 3; ++d) { zn.lo[d] = z.lo[d]; zn.hi[d] = z.hi[d]; }
+    zn.sig = dbl ? (const T*)z.d_sigma : (const T*)z.d_sigma_t;
+  }
+  p.has_src = b.d_src_g != nullptr;
+  for (int d = 0; d < 3; ++d) { p.src_lo[d] = b.src_lo[d]; p.src_hi[d] = b.src_hi[d]; }
+  p.src_g = dbl ? (const T*)b.d_src_g : (const T*)b.d_src_g_t;
+  for (int d = 0; d < 3; ++d) p.code[d] = b.has_holes ? b.d_code_fd[d] : nullptr;
+  p.iblank = b.has_holes ? b.d_iblank : nullptr;
+  p.fd = c->fd;
+}
+
+// Amplitude of the monopole at time t (oracle patch P2, modelled on src/solver/source.cpp:60-92).
+double source_amp(const lee_ctx* c, double t) {
+  double T = c->src[6];
+  double ramp = 1.0;
+  if (T > 0.0 && t < T) {
+    double sn = sin(0.5 * M_PI * t / T);
+    ramp = sn * sn;
+  }
+  return c->src[3] * (c->cfg.gamma - 1.0) * ramp * sin(c->src[4] * t);
+}
+
+// Dimension-split filter of `in` (spatial::apply_filter, src/solver/spatial_discretization.cpp:2191-2246).
+// The passes alternate between the two free buffers f0/f1; *result names the buffer that holds the
+// filtered state. FP64: the last pass blends (1-beta) in + beta F(in). Compensated: `in` is y_pre, `err`
+// its rounding error; the increments D = F - I are summed over the passes and the last pass writes
+// y = y_pre + beta D + err as a two-float sum, its new rounding error going to comp_out.
+template <typename T>
+int run_filter(lee_ctx* c, BlockData& b, void** in, void** err, void** comp_out, void** f0, void** f1,
+               void*** result) {
+  int dims[3] = {b.nx, b.ny, b.nz};
+  int passes[3], np = 0;
+  for (int d = 0; d < c->cfg.num_dim; ++d)
+    if (dims[d] > 1) passes[np++] = d;
+  void** fr[2] = {f0, f1};
+  void** src = in;
+  for (int q = 0; q < np; ++q) {
+    FilterParams<T> fp;
+    memset(&fp, 0, sizeof fp);
+    fp.nx = b.nx; fp.ny = b.ny; fp.nz = b.nz;
+    fp.V = c->V;
+    fp.dir = passes[q];
+    fp.first = q == 0;
+    fp.last = q == np - 1;
+    fp.blend = (T)c->cfg.filter_blend;
+    fp.code = b.has_holes ? b.d_code_flt[passes[q]] : nullptr;
+    fp.iblank = b.has_holes ? b.d_iblank : nullptr;
+    fp.op = c->comp ? c->fltd : c->flt;
+    void** dst = fr[q % 2];
+    for (int v = 0; v < c->V; ++v) {
+      fp.in[v] = (const T*)src[v];
+      fp.out[v] = (T*)dst[v];
+      fp.y0[v] = (const T*)in[v];
+      fp.dsum[v] = (T*)b.dsum[v];
+      fp.dsum_in[v] = (const T*)b.dsum[v];
+      fp.comp[v] = comp_out ? (T*)comp_out[v] : nullptr;
+      fp.err[v] = err ? (const T*)err[v] : nullptr;
+    }
+    int e0 = mark(c);
+    CK(launch_filter_pass<T>(fp, c->comp ? 1 : 0, c->stream));
+    int e1 = mark(c);
+    span(c, 1, e0, e1);
+    c->stats.filter_launches += 1;
+    c->stats.kernel_launches += 1;
+    src = dst;
+  }
+  *result = np > 0 ? fr[(np - 1) % 2] : in;
+  return LEE_OK;
+}
+
+void swap_fields(int V, void** a, void** b) {
+  if (a == b) return;
+  for (int v = 0; v < V; ++v) std::swap(a[v], b[v]);
+}
+
+template <typename T>
+int advance_impl(lee_ctx* c, int nsteps, double dt) {
+  const int rk = c->cfg.rk_scheme;
+  double bi[4], ci[4], aij[4];
+  int ns;
+  if (rk == LEE_RK4) {
+    ns = 4;
+    bi[0] = 1.0 / 6.0; bi[1] = 1.0 / 3.0; bi[2] = 1.0 / 3.0; bi[3] = 1.0 / 6.0;
+    ci[0] = 0.0; ci[1] = 1.0 / 2.0; ci[2] = 1.0 / 2.0; ci[3] = 1.0;
+    aij[0] = 1.0 / 2.0; aij[1] = 1.0 / 2.0; aij[2] = 1.0; aij[3] = 0.0;
+  } else {
+    ns = 2;
+    bi[0] = 1.0 / 2.0; bi[1] = 1.0 / 2.0;
+    ci[0] = 0.0; ci[1] = 1.0;
+    aij[0] = 1.0; aij[1] = 0.0;
+  }
+  for (int it = 0; it < nsteps; ++it) {
+    c->time += dt;
+    c->step += 1;
+    const double tn = c->time;
+    for (int s = 0; s < ns; ++s) {
+      for (auto& b : c->blk) {
+        StageParams<T> p;
+        fill_stage_common<T>(c, b, p);
+        p.stage = s;
+        p.last = s == ns - 1;
+        p.h = (T)dt;
+        p.b = (T)bi[s];
+        p.a = (T)aij[s];
+        p.src_amp = (T)(c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, tn + ci[s] * dt) : 0.0);
+        void** zin = s == 0 ? b.y : b.zb[(s + 1) % 2];
+        void** zout = b.zb[s % 2];
+        for (int v = 0; v < c->V; ++v) {
+          p.zin[v] = (const T*)zin[v];
+          p.yn[v] = (const T*)b.y[v];
+          p.acc[v] = (T*)b.acc[v];
+          p.zout[v] = (T*)zout[v];
+          p.comp[v] = (T*)b.comp[v];
+        }
+        p.rho_prev = (const T*)b.rho_prev;
+        int e0 = mark(c);
+        CK(launch_stage<T>(p, c->comp ? 1 : 0, c->stream));
+        int e1 = mark(c);
+        span(c, 0, e0, e1);
+        c->stats.stage_launches += 1;
+        c->stats.kernel_launches += 1;
+      }
+      // boundary conditions and overset updates of the stage output come here
+    }
+    for (auto& b : c->blk) {
+      if (b.need_rho) {
+        // rho'/rho_bar of the pre-filter state for the next step's first stage (F9 ordering)
+        return fail(c, LEE_ERR_UNSUPPORTED, "non-uniform mean velocity is not supported yet");
+      }
+      void** last_out = b.zb[(ns - 1) % 2];
+      void** other = b.zb[ns % 2];
+      if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
+        void** res = nullptr;
+        int rc = c->comp ? run_filter<T>(c, b, last_out, b.acc, b.comp, other, b.y, &res)
+                         : run_filter<T>(c, b, b.acc, nullptr, nullptr, last_out, other, &res);
+        if (rc) return rc;
+        swap_fields(c->V, b.y, res);
+      } else if (!c->comp) {
+        swap_fields(c->V, b.y, b.acc);
+      } else {
+        swap_fields(c->V, b.y, last_out);
+        swap_fields(c->V, b.comp, b.acc);
+      }
+    }
+  }
+  return LEE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lee_create(const lee_config* cfg, lee_ctx** out) {
+  lee_ctx* c = nullptr;
+  if (!cfg || !out) return fail(nullptr, LEE_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->num_dim != 2 && cfg->num_dim != 3) return fail(nullptr, LEE_ERR_ARG, "num_dim must be 2 or 3");
+  if (cfg->num_blocks < 1 || cfg->num_blocks > 64) return fail(nullptr, LEE_ERR_ARG, "num_blocks out of range");
+  if (cfg->rk_scheme != LEE_RK4 && cfg->rk_scheme != LEE_RK2) return fail(nullptr, LEE_ERR_ARG, "rk_scheme");
+  if (cfg->precision != LEE_FP64 && cfg->precision != LEE_FP32_COMPENSATED)
+    return fail(nullptr, LEE_ERR_ARG, "precision");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, LEE_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  if (cfg->device < 0 || cfg->device >= ndev) return fail(nullptr, LEE_ERR_ARG, "device ordinal");
+  c = new lee_ctx();
+  c->cfg = *cfg;
+  c->V = cfg->num_dim + 2;
+  c->comp = cfg->precision == LEE_FP32_COMPENSATED;
+  c->esz = c->comp ? 4 : 8;
+  if (!make_fd(&c->fd, cfg->fd_scheme, cfg->fd_order)) {
+    delete c;
+    return fail(nullptr, LEE_ERR_UNSUPPORTED, "spatial scheme %d order %d", cfg->fd_scheme, cfg->fd_order);
+  }
+  if (cfg->filter_scheme != LEE_FILTER_NONE) {
+    double strength = cfg->filter_scheme == LEE_FILTER_STANDARD_CENTRAL ? 1.0 : cfg->filter_strength;
+    if (strength < 0.0 || strength > 1.0 || cfg->filter_blend < 0.0 || cfg->filter_blend > 1.0 ||
+        !make_filter(&c->flt, cfg->filter_scheme, cfg->filter_order, strength)) {
+      delete c;
+      return fail(nullptr, LEE_ERR_UNSUPPORTED, "filter scheme %d order %d", cfg->filter_scheme, cfg->filter_order);
+    }
+    c->fltd = minus_identity(c->flt);
+  }
+  c->blk.resize((size_t)cfg->num_blocks);
+  e = cudaSetDevice(cfg->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(nullptr, LEE_ERR_CUDA, "stream creation failed: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return LEE_OK;
+}
+
+void lee_destroy(lee_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->cfg.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* lee_last_error(const lee_ctx* c) { return c ? c->err.c_str() : g_create_error; }
+
+int lee_set_block(lee_ctx* c, int b, int nx, int ny, int nz, const double* x, const double* y, const double* z,
+                  const int* iblank) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_block after lee_prepare");
+  if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "block index %d", b);
+  if (!x || !y || !z) return fail(c, LEE_ERR_ARG, "null coordinates");
+  int need = std::max(2 * c->fd.h + 1, c->fd.S);
+  if (c->cfg.filter_scheme != LEE_FILTER_NONE) need = std::max(need, std::max(2 * c->flt.h + 1, c->flt.S));
+  int dims[3] = {nx, ny, nz};
+  for (int d = 0; d < 3; ++d) {
+    if (dims[d] < 1) return fail(c, LEE_ERR_ARG, "dimension %d is %d", d, dims[d]);
+    if (d < c->cfg.num_dim && dims[d] < need)
+      return fail(c, LEE_ERR_ARG, "direction %d has %d points; the stencils need at least %d", d, dims[d], need);
+  }
+  if (c->cfg.num_dim == 2 && nz != 1) return fail(c, LEE_ERR_ARG, "2-D blocks have nzeta = 1");
+  BlockData& bk = c->blk[(size_t)b];
+  bk.nx = nx; bk.ny = ny; bk.nz = nz;
+  bk.N = (long long)nx * ny * nz;
+  bk.hx.assign(x, x + bk.N);
+  bk.hy.assign(y, y + bk.N);
+  bk.hz.assign(z, z + bk.N);
+  bk.hib.clear();
+  bk.has_holes = false;
+  if (iblank) {
+    bk.hib.assign(iblank, iblank + bk.N);
+    for (int v : bk.hib) {
+      if (v != 0 && v != 1 && v != -1) return fail(c, LEE_ERR_ARG, "iblank values are 0, 1 or -1");
+      if (v != 0) bk.has_holes = true;
+    }
+  }
+  bk.set = true;
+  return LEE_OK;
+}
+
+int lee_set_mean(lee_ctx* c, int b, const double* const mean[5]) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_mean after lee_prepare");
+  if (b < 0 || b >= (int)c->blk.size() || !c->blk[(size_t)b].set) return fail(c, LEE_ERR_STATE, "lee_set_block first");
+  BlockData& bk = c->blk[(size_t)b];
+  for (int v = 0; v < 5; ++v) {
+    if (!mean[v]) return fail(c, LEE_ERR_ARG, "null mean field");
+    bk.hmean[v].assign(mean[v], mean[v] + bk.N);
+  }
+  for (long long l = 0; l < bk.N; ++l)
+    if (!(bk.hmean[4][(size_t)l] > 0.0)) return fail(c, LEE_ERR_ARG, "mean pressure must be positive");
+  bk.has_mean = true;
+  return LEE_OK;
+}
+
+int lee_add_boundary(lee_ctx* c, int b, int kind, int dir, int end, const int lo[3], const int hi[3],
+                     const double* sigma) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_add_boundary after lee_prepare");
+  if (b < 0 || b >= (int)c->blk.size() || !c->blk[(size_t)b].set) return fail(c, LEE_ERR_STATE, "lee_set_block first");
+  BlockData& bk = c->blk[(size_t)b];
+  if (kind != LEE_SPONGE_FREUND_AMBIENT)
+    return fail(c, LEE_ERR_UNSUPPORTED, "boundary kind %d is not supported yet", kind);
+  if (dir < 0 || dir >= c->cfg.num_dim || (end != 0 && end != 1)) return fail(c, LEE_ERR_ARG, "dir/end");
+  int dims[3] = {bk.nx, bk.ny, bk.nz};
+  Boundary z;
+  z.kind = kind; z.dir = dir; z.end = end;
+  for (int d = 0; d < 3; ++d) {
+    if (lo[d] < 0 || hi[d] >= dims[d] || lo[d] > hi[d]) return fail(c, LEE_ERR_ARG, "boundary box outside block");
+    z.lo[d] = lo[d];
+    z.hi[d] = hi[d];
+  }
+  int nzones = 0;
+  for (auto& q : bk.bnd) nzones += q.kind == LEE_SPONGE_FREUND_AMBIENT;
+  if (nzones >= kMaxZones) return fail(c, LEE_ERR_UNSUPPORTED, "more than %d sponge zones in a block", kMaxZones);
+  if (sigma) {
+    size_t nb = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    z.sigma.assign(sigma, sigma + nb);
+  }
+  bk.bnd.push_back(std::move(z));
+  return LEE_OK;
+}
+
+int lee_set_source(lee_ctx* c, int kind, const double* params, int nparams) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_source after lee_prepare");
+  if (kind == LEE_SOURCE_NONE) {
+    c->src_kind = kind;
+    return LEE_OK;
+  }
+  if (kind != LEE_SOURCE_MONOPOLE || !params || nparams != 7) return fail(c, LEE_ERR_ARG, "monopole takes 7 params");
+  if (!(params[5] > 0.0)) return fail(c, LEE_ERR_ARG, "monopole half-width must be positive");
+  c->src_kind = kind;
+  for (int q = 0; q < 7; ++q) c->src[q] = params[q];
+  return LEE_OK;
+}
+
+int lee_prepare(lee_ctx* c) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare called twice");
+  CK(cudaSetDevice(c->cfg.device));
+  const int dim = c->cfg.num_dim;
+  cudaStream_t s = c->stream;
+  int rc;
+  for (auto& b : c->blk) {
+    if (!b.set || !b.has_mean) return fail(c, LEE_ERR_STATE, "every block needs lee_set_block and lee_set_mean");
+    const int N = (int)b.N;
+    if ((rc = upload(c, &b.d_xyz[0], b.hx))) return rc;
+    if ((rc = upload(c, &b.d_xyz[1], b.hy))) return rc;
+    if ((rc = upload(c, &b.d_xyz[2], b.hz))) return rc;
+    for (int v = 0; v < 5; ++v)
+      if ((rc = upload(c, &b.d_mean[v], b.hmean[v]))) return rc;
+    if ((rc = compute_metrics(c, b))) return rc;
+    // hole closures
+    if (b.has_holes) {
+      if ((rc = dalloc(c, &b.d_iblank, (size_t)N))) return rc;
+      CK(cudaMemcpyAsync(b.d_iblank, b.hib.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, s));
+      std::vector<int8_t> code;
+      int dims[3] = {b.nx, b.ny, b.nz};
+      for (int d = 0; d < dim; ++d) {
+        if (dims[d] == 1) continue;
+        if (!closure_codes(c->fd, b, d, code)) return fail(c, LEE_ERR_ARG, "hole closure lacks fluid support");
+        if ((rc = dalloc(c, &b.d_code_fd[d], (size_t)N))) return rc;
+        CK(cudaMemcpyAsync(b.d_code_fd[d], code.data(), (size_t)N, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
+          if (!closure_codes(c->flt, b, d, code))
+            return fail(c, LEE_ERR_ARG, "filter hole closure lacks fluid support");
+          if ((rc = dalloc(c, &b.d_code_flt[d], (size_t)N))) return rc;
+          CK(cudaMemcpyAsync(b.d_code_flt[d], code.data(), (size_t)N, cudaMemcpyHostToDevice, s));
+          CK(cudaStreamSynchronize(s));
+        }
+      }
+    }
+    // mean gradients (spatial::precompute_something, src/solver/spatial_discretization.cpp:2250-2271)
+    double *sum = nullptr, *tmp = nullptr;
+    if ((rc = dalloc(c, &sum, (size_t)N))) return rc;
+    if ((rc = dalloc(c, &tmp, (size_t)N))) return rc;
+    for (int v = 0; v < 5; ++v)
+      for (int j = 0; j < dim; ++j) {
+        if ((rc = dalloc(c, &b.d_grad[v * dim + j], (size_t)N))) return rc;
+        CK(cudaMemsetAsync(sum, 0, (size_t)N * 8, s));
+        for (int l = 0; l < dim; ++l) {
+          CK(setup_apply_dir(c->fd, b.nx, b.ny, b.nz, l, b.d_mean[v], tmp, b.has_holes ? b.d_code_fd[l] : nullptr,
+                             1, s));
+          CK(setup_grad_accum(N, sum, b.d_met[l * 3 + j], tmp, s));
+        }
+        CK(setup_scale(N, b.d_grad[v * dim + j], sum, b.d_jac, s));
+      }
+    // J * metrics products read by the stage kernels
+    for (int l = 0; l < dim; ++l)
+      for (int x = 0; x < dim; ++x) {
+        if ((rc = dalloc(c, &b.d_jm[l * 3 + x], (size_t)N))) return rc;
+        CK(setup_mul(N, b.d_jm[l * 3 + x], b.d_jac, b.d_met[l * 3 + x], s));
+      }
+    // 1 / rho_bar with rho_bar = (gamma p_bar)^(1/gamma) exp(-s_bar) (src/core/state.cpp:712-714),
+    // evaluated on the host with the reference's libm calls
+    {
+      if ((rc = dalloc(c, &b.d_rbi, (size_t)N))) return rc;
+      std::vector<double> rbi((size_t)N);
+      double g = c->cfg.gamma, gi = 1.0 / g;
+      for (int l = 0; l < N; ++l) rbi[(size_t)l] = 1.0 / (pow(g * b.hmean[4][(size_t)l], gi) * exp(-b.hmean[0][(size_t)l]));
+      CK(cudaMemcpyAsync(b.d_rbi, rbi.data(), (size_t)N * 8, cudaMemcpyHostToDevice, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    // sponge strengths
+    double** d_xyzp = nullptr;
+    if ((rc = dalloc(c, &d_xyzp, 3))) return rc;
+    CK(cudaMemcpyAsync(d_xyzp, b.d_xyz, sizeof b.d_xyz, cudaMemcpyHostToDevice, s));
+    for (auto& z : b.bnd) {
+      if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+      size_t nb = (size_t)(z.hi[0] - z.lo[0] + 1) * (z.hi[1] - z.lo[1] + 1) * (z.hi[2] - z.lo[2] + 1);
+      if ((rc = dalloc(c, &z.d_sigma, nb))) return rc;
+      if (!z.sigma.empty()) {
+        CK(cudaMemcpyAsync(z.d_sigma, z.sigma.data(), nb * 8, cudaMemcpyHostToDevice, s));
+      } else {
+        CK(setup_sigma(b.nx, b.ny, b.nz, d_xyzp, z.lo, z.hi, z.dir, z.end, c->cfg.sponge_order,
+                       c->cfg.sponge_constant, z.d_sigma, s));
+      }
+      if (c->comp) {
+        float* f = nullptr;
+        if ((rc = dalloc(c, &f, nb))) return rc;
+        k_convert<float><<<grid1d((long long)nb), 256, 0, s>>>((long long)nb, f, z.d_sigma);
+        CK(cudaGetLastError());
+        z.d_sigma_t = f;
+      }
+    }
+    // monopole spatial factor on the box where exp() is nonzero in FP64
+    if (c->src_kind == LEE_SOURCE_MONOPOLE) {
+      double ef = -log(2.0) / (c->src[5] * c->src[5]);
+      double rmax = sqrt(746.0 / -ef);
+      int lo[3] = {b.nx, b.ny, b.nz}, hi[3] = {-1, -1, -1};
+      for (long long l = 0; l < b.N; ++l) {
+        double dx = b.hx[(size_t)l] - c->src[0], dy = b.hy[(size_t)l] - c->src[1], dz = b.hz[(size_t)l] - c->src[2];
+        if (dx * dx + dy * dy + dz * dz <= rmax * rmax) {
+          int ijk[3] = {(int)(l % b.nx), (int)((l / b.nx) % b.ny), (int)(l / ((long long)b.nx * b.ny))};
+          for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], ijk[d]);
+            hi[d] = std::max(hi[d], ijk[d]);
+          }
+        }
+      }
+      if (hi[0] >= 0) {
+        size_t nb = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+        if ((rc = dalloc(c, &b.d_src_g, nb))) return rc;
+        CK(setup_monopole_g(b.nx, b.ny, d_xyzp, lo, hi, c->src[0], c->src[1], c->src[2], ef, b.d_src_g, s));
+        for (int d = 0; d < 3; ++d) { b.src_lo[d] = lo[d]; b.src_hi[d] = hi[d]; }
+        if (c->comp) {
+          float* f = nullptr;
+          if ((rc = dalloc(c, &f, nb))) return rc;
+          k_convert<float><<<grid1d((long long)nb), 256, 0, s>>>((long long)nb, f, b.d_src_g);
+          CK(cudaGetLastError());
+          b.d_src_g_t = f;
+        }
+      }
+    }
+    CK(cudaStreamSynchronize(s));
+    // coefficient fields: constant ones become kernel constants
+    b.n_coef_fields = 0;
+    double jscale = 0.0;
+    for (int l = 0; l < dim; ++l)
+      for (int x = 0; x < dim; ++x) {
+        double lo, hi;
+        bool u, z;
+        if ((rc = classify(c, b.d_jm[l * 3 + x], b.N, 1e300, &lo, &hi, &u, &z))) return rc;
+        jscale = fmax(jscale, fmax(fabs(lo), fabs(hi)));
+      }
+    double mscale[5];
+    for (int v = 0; v < 5; ++v) {
+      double lo, hi;
+      bool u, z;
+      if ((rc = classify(c, b.d_mean[v], b.N, 1e300, &lo, &hi, &u, &z))) return rc;
+      mscale[v] = fmax(fmax(fabs(lo), fabs(hi)), 1e-300) * jscale;
+    }
+    auto coef = [&](const double* f, double scale, Coef<double>* cd, Coef<float>* cf) -> int {
+      if (c->comp) return make_coef<float>(c, b, f, scale, cf);
+      return make_coef<double>(c, b, f, scale, cd);
+    };
+    for (int q = 0; q < 9; ++q) {
+      b.cd_jm[q] = Coef<double>{nullptr, 0.0, 1};
+      b.cf_jm[q] = Coef<float>{nullptr, 0.0f, 1};
+      b.cd_gu[q] = Coef<double>{nullptr, 0.0, 1};
+      b.cf_gu[q] = Coef<float>{nullptr, 0.0f, 1};
+    }
+    for (int q = 0; q < 3; ++q) {
+      b.cd_ub[q] = b.cd_gs[q] = b.cd_gp[q] = Coef<double>{nullptr, 0.0, 1};
+      b.cf_ub[q] = b.cf_gs[q] = b.cf_gp[q] = Coef<float>{nullptr, 0.0f, 1};
+    }
+    for (int l = 0; l < dim; ++l)
+      for (int x = 0; x < dim; ++x)
+        if ((rc = coef(b.d_jm[l * 3 + x], 1e-300, &b.cd_jm[l * 3 + x], &b.cf_jm[l * 3 + x]))) return rc;
+    for (int x = 0; x < dim; ++x)
+      if ((rc = coef(b.d_mean[1 + x], 1e-300, &b.cd_ub[x], &b.cf_ub[x]))) return rc;
+    if ((rc = coef(b.d_mean[4], 1e-300, &b.cd_pb, &b.cf_pb))) return rc;
+    if ((rc = coef(b.d_rbi, 1e-300, &b.cd_rbi, &b.cf_rbi))) return rc;
+    for (int x = 0; x < dim; ++x) {
+      if ((rc = coef(b.d_grad[0 * dim + x], mscale[0], &b.cd_gs[x], &b.cf_gs[x]))) return rc;
+      if ((rc = coef(b.d_grad[4 * dim + x], mscale[4], &b.cd_gp[x], &b.cf_gp[x]))) return rc;
+      for (int a = 0; a < dim; ++a)
+        if ((rc = coef(b.d_grad[(1 + a) * dim + x], mscale[1 + a], &b.cd_gu[a * 3 + x], &b.cf_gu[a * 3 + x])))
+          return rc;
+    }
+    b.need_rho = 0;
+    for (int q = 0; q < 9; ++q) b.need_rho |= c->comp ? !b.cf_gu[q].zero : !b.cd_gu[q].zero;
+    if (b.need_rho) return fail(c, LEE_ERR_UNSUPPORTED, "non-uniform mean velocity is not supported yet");
+    // state buffers
+    if ((rc = alloc_fields(c, b.y, b.N))) return rc;
+    if ((rc = alloc_fields(c, b.acc, b.N))) return rc;
+    if ((rc = alloc_fields(c, b.zb[0], b.N))) return rc;
+    if ((rc = alloc_fields(c, b.zb[1], b.N))) return rc;
+    if (c->comp) {
+      if ((rc = alloc_fields(c, b.comp, b.N))) return rc;
+      if ((rc = alloc_fields(c, b.dsum, b.N))) return rc;
+    }
+  }
+  CK(cudaStreamSynchronize(s));
+  c->prepared = true;
+  return LEE_OK;
+}
+
+int lee_upload_state(lee_ctx* c, int b, const double* const sol[5], int step, double time) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "block index");
+  BlockData& bk = c->blk[(size_t)b];
+  CK(cudaSetDevice(c->cfg.device));
+  if (c->cfg.num_dim == 2)
+    for (long long l = 0; l < bk.N; ++l)
+      if (sol[3][l] != 0.0) return fail(c, LEE_ERR_ARG, "2-D state must have w' = 0");
+  int rc;
+  double* tmp = nullptr;
+  CK(cudaMallocAsync((void**)&tmp, (size_t)bk.N * 8, c->stream));
+  for (int v = 0; v < c->V; ++v) {
+    CK(cudaMemcpyAsync(tmp, sol[slot_of(c->V, v)], (size_t)bk.N * 8, cudaMemcpyHostToDevice, c->stream));
+    if (!c->comp) {
+      CK(cudaMemcpyAsync(bk.y[v], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+      k_convert<float><<<grid1d(bk.N), 256, 0, c->stream>>>(bk.N, (float*)bk.y[v], tmp);
+      CK(cudaGetLastError());
+      CK(cudaMemsetAsync(bk.comp[v], 0, (size_t)bk.N * 4, c->stream));
+    }
+  }
+  CK(cudaFreeAsync(tmp, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  (void)rc;
+  c->step = step;
+  c->time = time;
+  c->uploaded = true;
+  return LEE_OK;
+}
+
+int lee_download_state(lee_ctx* c, int b, double* const sol[5], int* step, double* time) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "block index");
+  BlockData& bk = c->blk[(size_t)b];
+  CK(cudaSetDevice(c->cfg.device));
+  double* tmp = nullptr;
+  CK(cudaMallocAsync((void**)&tmp, (size_t)bk.N * 8, c->stream));
+  for (int v = 0; v < c->V; ++v) {
+    if (!c->comp) {
+      CK(cudaMemcpyAsync(sol[slot_of(c->V, v)], bk.y[v], (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+      k_to_double<float><<<grid1d(bk.N), 256, 0, c->stream>>>(bk.N, tmp, (const float*)bk.y[v],
+                                                             (const float*)bk.comp[v]);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(sol[slot_of(c->V, v)], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
+  CK(cudaFreeAsync(tmp, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->cfg.num_dim == 2) memset(sol[3], 0, (size_t)bk.N * 8);
+  if (step) *step = c->step;
+  if (time) *time = c->time;
+  return LEE_OK;
+}
+
+int lee_compute_dt(lee_ctx* c, double cfl, double* dt) {
+  if (!c || !dt) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (!(cfl > 0.0)) return fail(c, LEE_ERR_ARG, "cfl must be positive");
+  CK(cudaSetDevice(c->cfg.device));
+  double* d_max = nullptr;
+  CK(cudaMallocAsync((void**)&d_max, sizeof(double), c->stream));
+  double init = -1e308;
+  CK(cudaMemcpyAsync(d_max, &init, sizeof init, cudaMemcpyHostToDevice, c->stream));
+  const double dt0 = 1e-6;  // the reference's dummy initial dt (src/core/input.cpp:131)
+  for (auto& b : c->blk) {
+    double** d_m = nullptr;
+    double** d_u = nullptr;
+    CK(cudaMallocAsync((void**)&d_m, 9 * sizeof(double*), c->stream));
+    CK(cudaMallocAsync((void**)&d_u, 3 * sizeof(double*), c->stream));
+    CK(cudaMemcpyAsync(d_m, b.d_met, 9 * sizeof(double*), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_u, b.d_mean + 1, 3 * sizeof(double*), cudaMemcpyHostToDevice, c->stream));
+    CK(setup_cfl((int)b.N, c->cfg.num_dim, d_m, b.d_jac, d_u, b.d_mean[4], b.d_mean[0],
+                 b.has_holes ? b.d_iblank : nullptr, c->cfg.gamma, dt0, d_max, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaFreeAsync(d_m, c->stream));
+    CK(cudaFreeAsync(d_u, c->stream));
+  }
+  double cmax = 0.0;
+  CK(cudaMemcpyAsync(&cmax, d_max, sizeof cmax, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaFreeAsync(d_max, c->stream));
+  double ratio = cfl / cmax;
+  double d = dt0;
+  d *= ratio;
+  *dt = d;
+  return LEE_OK;
+}
+
+int lee_advance(lee_ctx* c, int nsteps, double dt) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (nsteps < 0 || !(dt > 0.0)) return fail(c, LEE_ERR_ARG, "nsteps >= 0 and dt > 0");
+  CK(cudaSetDevice(c->cfg.device));
+  memset(&c->stats, 0, sizeof c->stats);
+  c->ev_used = 0;
+  c->ev_marks.clear();
+  cudaEvent_t t0, t1;
+  CK(cudaEventCreate(&t0));
+  CK(cudaEventCreate(&t1));
+  CK(cudaEventRecord(t0, c->stream));
+  int rc = c->comp ? advance_impl<float>(c, nsteps, dt) : advance_impl<double>(c, nsteps, dt);
+  CK(cudaEventRecord(t1, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, t0, t1));
+  c->stats.advance_ms = ms;
+  for (auto& m : c->ev_marks) {
+    float d = 0.f;
+    if (cudaEventElapsedTime(&d, c->ev_pool[(size_t)m.second], c->ev_pool[(size_t)m.second + 1]) == cudaSuccess) {
+      if (m.first == 0) c->stats.stage_ms += d;
+      else c->stats.filter_ms += d;
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (rc) return rc;
+  return LEE_OK;
+}
+
+int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "block index");
+  CK(cudaSetDevice(c->cfg.device));
+  BlockData& bk = c->blk[(size_t)b];
+  double* tmp = nullptr;
+  CK(cudaMallocAsync((void**)&tmp, (size_t)bk.N * 8, c->stream));
+  if (!c->comp) {
+    StageParams<double> p;
+    fill_stage_common<double>(c, bk, p);
+    p.stage = -1;
+    p.src_amp = c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, time) : 0.0;
+    for (int v = 0; v < c->V; ++v) {
+      p.zin[v] = (const double*)bk.y[v];
+      p.zout[v] = (double*)bk.zb[0][v];
+    }
+    CK(launch_stage<double>(p, 0, c->stream));
+    for (int v = 0; v < c->V; ++v)
+      CK(cudaMemcpyAsync(rhs[slot_of(c->V, v)], bk.zb[0][v], (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    StageParams<float> p;
+    fill_stage_common<float>(c, bk, p);
+    p.stage = -1;
+    p.src_amp = (float)(c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, time) : 0.0);
+    for (int v = 0; v < c->V; ++v) {
+      p.zin[v] = (const float*)bk.y[v];
+      p.zout[v] = (float*)bk.zb[0][v];
+    }
+    CK(launch_stage<float>(p, 1, c->stream));
+    for (int v = 0; v < c->V; ++v) {
+      k_to_double<float><<<grid1d(bk.N), 256, 0, c->stream>>>(bk.N, tmp, (const float*)bk.zb[0][v], nullptr);
+      CK(cudaMemcpyAsync(rhs[slot_of(c->V, v)], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
+  CK(cudaFreeAsync(tmp, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->cfg.num_dim == 2) memset(rhs[3], 0, (size_t)bk.N * 8);
+  return LEE_OK;
+}
+
+int lee_apply_filter(lee_ctx* c) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (c->cfg.filter_scheme == LEE_FILTER_NONE) return LEE_OK;
+  CK(cudaSetDevice(c->cfg.device));
+  for (auto& b : c->blk) {
+    void** res = nullptr;
+    int rc = c->comp ? run_filter<float>(c, b, b.y, b.comp, b.comp, b.zb[0], b.zb[1], &res)
+                     : run_filter<double>(c, b, b.y, nullptr, nullptr, b.zb[0], b.zb[1], &res);
+    if (rc) return rc;
+    swap_fields(c->V, b.y, res);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return LEE_OK;
+}
+
+int lee_get_info(lee_ctx* c, lee_info* info) {
+  if (!c || !info) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  memset(info, 0, sizeof *info);
+  for (auto& b : c->blk) {
+    info->points += b.N;
+    info->num_coef_fields = std::max(info->num_coef_fields, b.n_coef_fields);
+  }
+  info->state_vars = c->V;
+  info->bytes_per_value = (int)c->esz;
+  info->device_bytes = c->device_bytes;
+  return LEE_OK;
+}
+
+int lee_set_timing(lee_ctx* c, int on) {
+  if (!c) return LEE_ERR_ARG;
+  c->timing = on != 0;
+  return LEE_OK;
+}
+
+int lee_get_stats(lee_ctx* c, lee_stats* st) {
+  if (!c || !st) return LEE_ERR_ARG;
+  *st = c->stats;
+  return LEE_OK;
+}
+
+int lee_get_setup(lee_ctx* c, int b, int what, double* out) {
+  if (!c || !out) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "block index");
+  BlockData& bk = c->blk[(size_t)b];
+  const size_t N = (size_t)bk.N;
+  CK(cudaSetDevice(c->cfg.device));
+  if (what == LEE_SETUP_METRICS) {
+    for (int q = 0; q < 9; ++q) CK(cudaMemcpyAsync(out + q * N, bk.d_met[q], N * 8, cudaMemcpyDeviceToHost, c->stream));
+  } else if (what == LEE_SETUP_JACOBIAN) {
+    CK(cudaMemcpyAsync(out, bk.d_jac, N * 8, cudaMemcpyDeviceToHost, c->stream));
+  } else if (what == LEE_SETUP_MEAN_GRADIENT) {
+    for (int q = 0; q < 5 * c->cfg.num_dim; ++q)
+      CK(cudaMemcpyAsync(out + q * N, bk.d_grad[q], N * 8, cudaMemcpyDeviceToHost, c->stream));
+  } else if (what == LEE_SETUP_SPONGE) {
+    CK(cudaStreamSynchronize(c->stream));
+    memset(out, 0, N * 8);
+    for (auto& z : bk.bnd) {
+      if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+      int b0 = z.hi[0] - z.lo[0] + 1, b1 = z.hi[1] - z.lo[1] + 1, b2 = z.hi[2] - z.lo[2] + 1;
+      std::vector<double> h((size_t)b0 * b1 * b2);
+      CK(cudaMemcpy(h.data(), z.d_sigma, h.size() * 8, cudaMemcpyDeviceToHost));
+      for (int k = 0; k < b2; ++k)
+        for (int j = 0; j < b1; ++j)
+          for (int i = 0; i < b0; ++i)
+            out[(size_t)(z.lo[0] + i) + (size_t)bk.nx * ((size_t)(z.lo[1] + j) + (size_t)bk.ny * (size_t)(z.lo[2] + k))] +=
+                h[(size_t)i + (size_t)b0 * ((size_t)j + (size_t)b1 * (size_t)k)];
+    }
+  } else {
+    return fail(c, LEE_ERR_ARG, "unknown setup selector %d", what);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return LEE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+// Internal declarations shared by the host orchestration (lee_capi.cu), the FP64
+// setup kernels (lee_setup.cu) and the time-advance kernels (lee_step.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/lee_b200.h"
+
+namespace lee {
+
+constexpr int kMaxZones = 8;  // sponge zones per block read by the stage kernel
+constexpr int kMaxVars = 5;   // s', u'(1..num_dim), p'
+
+// One directional operator: interior stencil c[l+h] (l = -h..h), closure rows
+// B[row][s] (row < nb, s < S) and the right-boundary sign (-1 difference, +1 filter).
+// Values are those of the reference's StandardCentral / StandardCentralFilter /
+// OptimizedCentral* classes (camille src/solver/spatial_discretization.cpp:28-492).
+struct OpTable {
+  int h, nb, S;
+  double c[11];
+  double B[5][9];
+  double mfac;
+};
+
+// Closure code of a point along one direction, precomputed on the host by running
+// the reference's per-line scan (StandardCentral::apply_spatial_discretization and
+// iblank_correction, src/solver/spatial_discretization.cpp:1078-1652):
+//   0        interior stencil
+//   1 + r    left closure row r, anchored r points to the left
+//  -(1 + r)  right closure row r (mirrored), anchored r points to the right
+//   kZero    the value is zero (a hole following a hole)
+constexpr int8_t kCodeZero = 100;
+
+// A per-point coefficient: a device field, or a constant when the field is uniform
+// over the block (checked in FP64 at setup). `zero` marks an identically-zero term.
+template <typename T>
+struct Coef {
+  const T* p;
+  T c;
+  int zero;
+};
+
+// A sponge zone: inclusive index box and its strengths (box-shaped, i fastest).
+template <typename T>
+struct Zone {
+  int lo[3], hi[3];
+  const T* sig;
+};
+
+// Everything one stage kernel launch needs for one block.
+template <typename T>
+struct StageParams {
+  int nx, ny, nz, dim, V;
+  // RK stage
+  int stage, last;        // stage index, 1 on the last stage
+  T h, b, a;              // step size, b_i and a_{i+1,i} of the Butcher tableau
+  const T* zin[kMaxVars];   // stage input (read with neighbours)
+  const T* yn[kMaxVars];    // y_n
+  T* acc[kMaxVars];         // FP64: running y_next; compensated: running increment
+  T* zout[kMaxVars];        // next stage input, or (last stage, compensated) y_pre
+  T* comp[kMaxVars];        // compensated form: carried rounding error of y
+  // coefficients (physical gradient d/dx_i f = sum_l JM[l][i] D_l f)
+  Coef<T> jm[9];            // J * metrics[l][i] at l*3+i
+  Coef<T> ubar[3], pbar, rhobar_inv;
+  Coef<T> gs[3], gu[9], gp[3];  // mean gradients: d s_bar/dx_j, d u_bar_i/dx_j at i*3+j, d p_bar/dx_j
+  int need_rho;                 // 1 when some d u_bar_i/dx_j is nonzero
+  const T* rho_prev;            // rho'/rho_bar from the previous step's last stage (stage 0 input)
+  T* rho_next;                  // written on the last stage
+  T gamma, inv_gamma;
+  // sponges
+  int nzones;
+  Zone<T> zones[kMaxZones];
+  // monopole source: rhs[p] += src_amp * g, g on a box (src_lo..src_hi), i fastest
+  int has_src;
+  T src_amp;
+  int src_lo[3], src_hi[3];
+  const T* src_g;
+  // holes and closure codes (nullptr when the block has no holes)
+  const int8_t* code[3];
+  const int* iblank;
+  OpTable fd;
+};
+
+template <typename T>
+struct FilterParams {
+  int nx, ny, nz, V, dir, first, last;
+  const T* in[kMaxVars];
+  T* out[kMaxVars];
+  // FP64: y0 for the blend on the last pass; compensated: see lee_step.cu
+  const T* y0[kMaxVars];
+  T* dsum[kMaxVars];
+  const T* dsum_in[kMaxVars];
+  T* comp[kMaxVars];
+  const T* err[kMaxVars];
+  T blend;
+  const int8_t* code;
+  const int* iblank;
+  OpTable op;
+};
+
+// lee_step.cu
+template <typename T>
+cudaError_t launch_stage(const StageParams<T>& p, int comp, cudaStream_t s);
+template <typename T>
+cudaError_t launch_filter_pass(const FilterParams<T>& p, int comp, cudaStream_t s);
+cudaError_t launch_hole_zero(int n, int V, double** f, const int* iblank, cudaStream_t s);
+cudaError_t launch_hole_zero_f(int n, int V, float** f, const int* iblank, cudaStream_t s);
+
+// lee_setup.cu (FP64, no FMA contraction)
+cudaError_t setup_apply_dir(const OpTable& op, int nx, int ny, int nz, int dir, const double* f, double* out,
+                            const int8_t* code, int zero_if_one_cell, cudaStream_t s);
+cudaError_t setup_axpby(int n, double* out, double a, const double* x, double b, const double* y,
+                        cudaStream_t s);  // out = a*x + b*y (y may be null)
+cudaError_t setup_mul(int n, double* out, const double* x, const double* y, cudaStream_t s);
+cudaError_t setup_jacobian(int n, int dim, double* const* xx, double* invjac, double* jac, cudaStream_t s);
+cudaError_t setup_inverse_metrics(int n, int dim, double* const* met, double* const* minv, cudaStream_t s);
+cudaError_t setup_grad_accum(int n, double* sum, const double* m, const double* d, cudaStream_t s);
+cudaError_t setup_scale(int n, double* out, const double* sum, const double* jac, cudaStream_t s);
+cudaError_t setup_sigma(int nx, int ny, int nz, const double* const* xyz, const int lo[3], const int hi[3], int dir,
+                        int end, int order, double constant, double* sig, cudaStream_t s);
+cudaError_t setup_minmax(int n, const double* f, double* d_out2, cudaStream_t s);
+cudaError_t setup_cfl(int n, int dim, const double* const* met, const double* jac, const double* const* ubar,
+                      const double* pbar, const double* sbar, const int* iblank, double gamma, double dt,
+                      double* d_max, cudaStream_t s);
+cudaError_t setup_rho_ratio(int n, int V, double gamma, const double* sv, const double* p, const double* pbar,
+                            double* out, cudaStream_t s);
+cudaError_t setup_monopole_g(int nx, int ny, const double* const* xyz, const int lo[3], const int hi[3],
+                             double x0, double y0, double z0, double ef, double* g, cudaStream_t s);
+
+}  // namespace lee

@@ -1,0 +1,180 @@
+/*
+ * lee_b200.h -- C ABI of the B200 linearized-Euler (LEE) time-advance path.
+ *
+ * This library replaces the RK loop of the camille solver: the seam is
+ * solver::solve(UserInput*, StructuredGrid*, StructuredBlock*, State*)
+ * (camille src/solver/solver.h:21, src/solver/solver.cpp:41-89), called once by
+ * simulation::run (src/core/simulation.cpp:256) after the deck, grids, mean
+ * flow, BC file and restart file have been read. A replacement solve() marshals
+ * the reference's host arrays through the calls below; every array crosses the
+ * boundary as plain float64/int32 pointers in the reference's own layout:
+ * one array per variable, index l = i + nxi*(j + neta*k), i fastest
+ * (src/geometry/geometry.h:131-136). The library copies host buffers on every
+ * set/upload/download call; the caller keeps ownership of them.
+ *
+ * Conventions
+ *  - Every entry point returns LEE_OK (0) or an LEE_ERR_* code; the message of
+ *    the last failure on a context is lee_last_error(ctx). The reference has no
+ *    status codes (it calls mpi::graceful_exit, src/parallel/parallel.cpp:90-96).
+ *  - A context is single-threaded and owns one CUDA stream on its device. All
+ *    blocks of a context are resident in that GPU's memory; block-halo and
+ *    overset exchanges happen on the device.
+ *  - State variables follow the reference's LEE slots (src/core/param.h:67-80):
+ *    0 = s' (entropy), 1..3 = u', v', w', 4 = p'. The mean flow has the same
+ *    slots (s_bar, u_bar, v_bar, w_bar, p_bar). In 2-D the w' slot must be zero
+ *    on upload and is zero on download (in the reference it only ever carries
+ *    the sponge term acting on a zero field).
+ *  - There is no CPU fallback: lee_create fails with LEE_ERR_NODEVICE when no
+ *    CUDA device is usable.
+ */
+#ifndef LEE_B200_H
+#define LEE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LEE_ABI_VERSION 1
+
+/* status codes */
+#define LEE_OK 0
+#define LEE_ERR_ARG 1          /* invalid argument */
+#define LEE_ERR_STATE 2        /* call made in the wrong order */
+#define LEE_ERR_CUDA 3         /* CUDA runtime error */
+#define LEE_ERR_NOMEM 4        /* device or host allocation failed */
+#define LEE_ERR_UNSUPPORTED 5  /* combination not implemented */
+#define LEE_ERR_NONFINITE 6    /* NaN/Inf detected in the state */
+#define LEE_ERR_NODEVICE 7     /* no usable CUDA device */
+#define LEE_ERR_TIMEOUT 8      /* a bounded device-side wait gave up */
+
+/* SPATIAL_SCHEME (src/core/input.cpp:147-150) */
+#define LEE_FD_STANDARD_CENTRAL 1  /* with fd_order 2 or 4 (src/solver/spatial_discretization.cpp:28-109) */
+#define LEE_FD_FDO11P 11           /* Bogey & Bailly 11-point (:228-344) */
+/* SPATIAL_FILTER (src/core/input.cpp:152-165) */
+#define LEE_FILTER_NONE 0
+#define LEE_FILTER_STANDARD_CENTRAL 1  /* with filter_order 4 or 8 (:113-224) */
+#define LEE_FILTER_SFO11P 11           /* with filter_strength (:348-492) */
+/* TEMPORAL_SCHEME (src/solver/temporal_discretization.cpp:33-85) */
+#define LEE_RK2 2
+#define LEE_RK4 4
+/* arithmetic form of the time advance */
+#define LEE_FP64 0                /* the reference's own FP64 arithmetic */
+#define LEE_FP32_COMPENSATED 1    /* FP32 state/stencils, compensated RK sum */
+
+/* boundary kinds: the reference's codes (src/core/param.h:101-121) */
+#define LEE_BC_NEUMANN 100
+#define LEE_BC_WALL_SLIP_KINEMATIC 201
+#define LEE_SPONGE_FREUND_AMBIENT 1000
+
+/* physical sources */
+#define LEE_SOURCE_NONE 0
+#define LEE_SOURCE_MONOPOLE 1  /* params: x0, y0, z0, amplitude, omega, halfwidth, ramp_time */
+
+/* lee_get_setup selectors: products of the one-time setup, per block */
+#define LEE_SETUP_METRICS 0     /* 9 fields, metrics[l][i] = (1/J) dxi_l/dx_i, row-major (l*3+i) */
+#define LEE_SETUP_JACOBIAN 1    /* 1 field, J */
+#define LEE_SETUP_MEAN_GRADIENT 2 /* 5*num_dim fields, d(mean_v)/dx_j at v*num_dim + j */
+#define LEE_SETUP_SPONGE 3      /* 1 field, sum of the Freund sponge strengths at each point */
+
+typedef struct lee_ctx lee_ctx;
+
+typedef struct {
+  int num_dim;            /* DIMENSION: 2 or 3 */
+  int num_blocks;         /* number of structured blocks */
+  double gamma;           /* GAMMA_SPECIFICHEAT */
+  int fd_scheme;          /* LEE_FD_* */
+  int fd_order;           /* ORDER_ACCURACY of STANDARD_CENTRAL: 2 or 4 */
+  int filter_scheme;      /* LEE_FILTER_* */
+  int filter_order;       /* ORDER_ACCURACY of the standard filter: 4 or 8 */
+  double filter_strength; /* SFO11P STRENGTH (the standard filter forces 1.0) */
+  double filter_blend;    /* BLEND */
+  int rk_scheme;          /* LEE_RK2 or LEE_RK4 */
+  int precision;          /* LEE_FP64 or LEE_FP32_COMPENSATED */
+  int sponge_order;       /* BUFFER_ZONE POLYNOMIAL_ORDER */
+  double sponge_constant; /* BUFFER_ZONE CONSTANT */
+  int device;             /* CUDA device ordinal */
+} lee_config;
+
+/* Create a context (replaces solver::initialize, src/solver/solver.cpp:8-15). */
+int lee_create(const lee_config *cfg, lee_ctx **out);
+/* Release every device and host resource of the context. */
+void lee_destroy(lee_ctx *ctx);
+/* Message of the last failure on ctx (or of the last failed lee_create when ctx is NULL). */
+const char *lee_last_error(const lee_ctx *ctx);
+
+/* Grid of block b: coordinates (io::read_grid, src/io/plot3d.cpp:443-671) and the
+ * overset iblank (src/geometry/geometry.h:24-26; NULL = all NOTBLANKED). The
+ * metrics and Jacobian are generated from these on the GPU in FP64 by
+ * lee_prepare (metrics::compute, src/metrics/metrics.cpp:9-44). */
+int lee_set_block(lee_ctx *ctx, int b, int nxi, int neta, int nzeta, const double *x, const double *y,
+                  const double *z, const int *iblank);
+/* Mean flow of block b, five fields (io::read_function, src/io/plot3d.cpp:881-989). */
+int lee_set_mean(lee_ctx *ctx, int b, const double *const mean[5]);
+/* One BC-file line (io::read_bc, src/io/io.cpp:957-1105): kind LEE_BC_* or
+ * LEE_SPONGE_*, dir 0/1/2 (XI/ETA/ZETA), end 0 (left, "+dir") or 1 (right,
+ * "-dir"), inclusive index box lo..hi. For sponges, sigma may hold the zone's
+ * strengths (box-shaped, i fastest, as StructuredBufferZone::buffer_strength,
+ * src/geometry/geometry.cpp:1126-1127); NULL computes them on the GPU. */
+int lee_add_boundary(lee_ctx *ctx, int b, int kind, int dir, int end, const int lo[3], const int hi[3],
+                     const double *sigma);
+/* Physical source (source::apply_physicalSource, src/solver/source.cpp:22-107). */
+int lee_set_source(lee_ctx *ctx, int kind, const double *params, int nparams);
+/* Finish setup on the GPU: metrics, Jacobian, mean gradients (spatial::precompute_something,
+ * src/solver/spatial_discretization.cpp:2250-2271), sponge strengths, hole closures,
+ * and the per-point coefficient fields the kernels read. */
+int lee_prepare(lee_ctx *ctx);
+
+/* Restart state of block b with its step and time (io::read_solution, src/io/plot3d.cpp:715-835). */
+int lee_upload_state(lee_ctx *ctx, int b, const double *const sol[5], int step, double time);
+/* Current state of block b (State::sol, src/core/state.h:39). */
+int lee_download_state(lee_ctx *ctx, int b, double *const sol[5], int *step, double *time);
+
+/* Time step for a target CFL (temporal::compute_CFL, src/solver/temporal_discretization.cpp:397-450),
+ * including the reference's truncation of the convective term to an int (abs(double) resolving to
+ * int abs(int) at :425): dt = cfl / max over non-hole points of the per-unit-dt CFL. */
+int lee_compute_dt(lee_ctx *ctx, double cfl, double *dt);
+/* Advance every block by nsteps RK steps of size dt (FIX_DT): per step the RK stages with
+ * boundary conditions and overset updates, the filter and the hole mask
+ * (temporal::time_advance, src/solver/temporal_discretization.cpp:334-374). */
+int lee_advance(lee_ctx *ctx, int nsteps, double dt);
+
+/* Inner seams, for operator-level parity checks. */
+/* Right-hand side of the current state of block b at the given time (spatial::compute_RHS,
+ * src/solver/spatial_discretization.cpp:1963-1990). */
+int lee_eval_rhs(lee_ctx *ctx, int b, double time, double *const rhs[5]);
+/* Apply the filter once to the current state of every block (spatial::apply_filter, :2191-2246). */
+int lee_apply_filter(lee_ctx *ctx);
+/* Copy a setup product of block b (LEE_SETUP_*) to host memory; out holds the selector's fields
+ * back to back, each nxi*neta*nzeta long. */
+int lee_get_setup(lee_ctx *ctx, int b, int what, double *out);
+
+/* Sizes and coefficient layout chosen by lee_prepare (no reference counterpart: the
+ * reference has no timers or counters, finding F13). */
+typedef struct {
+  long long points;          /* grid points over all blocks */
+  int state_vars;            /* active state variables per point (num_dim + 2) */
+  int bytes_per_value;       /* 8 for LEE_FP64, 4 for LEE_FP32_COMPENSATED */
+  int num_coef_fields;       /* per-point coefficient fields read by every stage; uniform
+                                fields are folded into kernel constants at setup */
+  long long device_bytes;    /* device memory held by the context */
+} lee_info;
+int lee_get_info(lee_ctx *ctx, lee_info *info);
+
+/* Device-side timing of the last lee_advance, from CUDA events recorded on the
+ * context's stream. Per-kernel times are collected only while timing is on. */
+typedef struct {
+  double advance_ms;         /* whole lee_advance */
+  double stage_ms;           /* fused RK stage kernels */
+  double filter_ms;          /* filter kernels */
+  long long stage_launches;
+  long long filter_launches;
+  long long kernel_launches; /* every kernel this library launched in the last lee_advance */
+} lee_stats;
+int lee_set_timing(lee_ctx *ctx, int on);
+int lee_get_stats(lee_ctx *ctx, lee_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LEE_B200_H */

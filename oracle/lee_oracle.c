@@ -1,0 +1,914 @@
+/*
+ * lee_oracle.c -- CPU restatement of the camille reference's LEE time-advance
+ * path, in plain C. TEST INFRASTRUCTURE ONLY: the parity tests, smoke() and
+ * bench.py's CPU-baseline leg load it as the checker; the product never links,
+ * loads or calls it.
+ *
+ * It exports the ABI of include/lee_b200.h with the prefix orc_ instead of lee_,
+ * so a test drives the oracle and the CUDA library with identical calls. Every
+ * function follows the reference's arithmetic step by step, in the reference's
+ * order of summation, so that on one rank it reproduces the reference to the
+ * last bits or close to them. It is pinned against the compiled reference
+ * (oracle/_ref/camille_ref) by tests/test_oracle_pin.py.
+ *
+ * Citations are files of the camille reference, relative to its root.
+ */
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../include/lee_b200.h"
+
+#define NOTBLANKED 0
+#define BLANKED 1
+#define INTERPOLATED (-1)
+#define MAXB 8
+#define MAXBND 64
+
+/* One directional operator: interior stencil c[l+h] for l = -h..h, boundary rows
+ * B[row][s] for row < nb, s < S, and the right-boundary sign (-1 for the
+ * antisymmetric difference, +1 for the symmetric filter), as the classes of
+ * src/solver/spatial_discretization.h:49-132 hold them. */
+typedef struct {
+  int h, nb, S;
+  double c[11];
+  double B[5][9];
+  double mfac;
+} op_t;
+
+typedef struct {
+  int kind, dir, end, lo[3], hi[3];
+  double *sigma; /* sponge strengths over the box, i fastest */
+} bnd_t;
+
+typedef struct {
+  int set, nx, ny, nz, N;
+  double *xyz[3];
+  int *iblank;
+  double *met[9];  /* metrics[l][i] at l*3+i */
+  double *minv[9]; /* metricsInverse[i][l] at i*3+l */
+  double *jac, *invjac;
+  double *mean[5];
+  double *grad[15]; /* d mean_v / dx_j at v*ndim + j */
+  double *aux[4];   /* rho', rho_bar, T', T_bar (IAUX_*, src/core/param.h:77-80) */
+  double *sol[5];
+  int nbnd;
+  bnd_t bnd[MAXBND];
+} blk_t;
+
+struct orc_ctx {
+  lee_config cfg;
+  op_t fd, flt;
+  int nblk;
+  blk_t blk[MAXB];
+  int src_kind;
+  double src[7];
+  int prepared, step;
+  double time;
+  char err[512];
+};
+typedef struct orc_ctx orc_ctx;
+
+static char g_err[512];
+
+static int fail(orc_ctx *c, int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(c ? c->err : g_err, 512, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+
+/* ---------------------------------------------------------------------------
+ * Coefficient tables: StandardCentral::initialize (:28-109), StandardCentralFilter
+ * ::initialize (:113-224), OptimizedCentralExplicit::initialize (:228-344),
+ * OptimizedCentralFilterExplicit::initialize (:348-492) of
+ * src/solver/spatial_discretization.cpp. The numbers are the published tables
+ * (Lele 1992; Bogey & Bailly 2004; Berland et al. 2007) and must be identical. */
+static int make_fd(op_t *o, int scheme, int order) {
+  memset(o, 0, sizeof *o);
+  o->mfac = -1.0;
+  if (scheme == LEE_FD_STANDARD_CENTRAL && order == 4) {
+    o->h = 2; o->nb = 2; o->S = 3;
+    o->c[2 + 0] = 0.0; o->c[2 + 1] = 8.0 / 12.0; o->c[2 + 2] = -1.0 / 12.0;
+    o->B[0][0] = -3.0 / 2.0; o->B[0][1] = 4.0 / 2.0; o->B[0][2] = -1.0 / 2.0;
+    o->B[1][0] = -1.0 / 2.0; o->B[1][1] = 0.0; o->B[1][2] = 1.0 / 2.0;
+  } else if (scheme == LEE_FD_FDO11P) {
+    o->h = 5; o->nb = 5; o->S = 9;
+    o->c[5 + 0] = 0.0; o->c[5 + 1] = 0.872756993962; o->c[5 + 2] = -0.286511173973;
+    o->c[5 + 3] = 0.090320001280; o->c[5 + 4] = -0.020779405824; o->c[5 + 5] = 0.002484594688;
+    double r0[7] = {-2.225833963270, 4.827779580575, -5.001388453836, 3.911103941646,
+                    -2.115267458633, 0.718882784412, -0.115276430894};
+    double r1[7] = {-0.212932721951, -1.060320390770, 2.078926116439, -1.287179452384,
+                    0.685176395471, -0.245320613994, 0.041650667189};
+    double r2[5] = {1.0 / 12.0, -8.0 / 12.0, 0.0, 8.0 / 12.0, -1.0 / 12.0};
+    double r3[7] = {-0.02625099337517627, 0.18833730683403838, -0.797921633542548, 0.0,
+                    0.797921633542548, -0.18833730683403838, 0.02625099337517627};
+    double r4[9] = {0.007650904064, -0.059463584768, 0.244678631765, -0.841570125482, 0.0,
+                    0.841570125482, -0.244678631765, 0.059463584768, -0.007650904064};
+    for (int s = 0; s < 7; ++s) { o->B[0][s] = r0[s]; o->B[1][s] = r1[s]; o->B[3][s] = r3[s]; }
+    for (int s = 0; s < 5; ++s) o->B[2][s] = r2[s];
+    for (int s = 0; s < 9; ++s) o->B[4][s] = r4[s];
+  } else {
+    return 0;
+  }
+  for (int k = 1; k <= o->h; ++k) o->c[o->h - k] = -o->c[o->h + k];
+  return 1;
+}
+
+static int make_filter(op_t *o, int scheme, int order, double strength) {
+  memset(o, 0, sizeof *o);
+  o->mfac = 1.0;
+  double r2[5] = {(-1.0 / 8.0) / 2.0, (1.0 / 2.0) / 2.0, 5.0 / 8.0, (1.0 / 2.0) / 2.0, (-1.0 / 8.0) / 2.0};
+  double r3[7] = {(1.0 / 32.0) / 2.0, (-3.0 / 16.0) / 2.0, (15.0 / 32.0) / 2.0, 11.0 / 16.0,
+                  (15.0 / 32.0) / 2.0, (-3.0 / 16.0) / 2.0, (1.0 / 32.0) / 2.0};
+  if (scheme == LEE_FILTER_STANDARD_CENTRAL && order == 4) {
+    o->h = 2; o->nb = 2; o->S = 3;
+    o->c[2] = 5.0 / 8.0; o->c[3] = (1.0 / 2.0) / 2.0; o->c[4] = (-1.0 / 8.0) / 2.0;
+    o->B[0][0] = 1.0; o->B[1][1] = 1.0;
+  } else if (scheme == LEE_FILTER_STANDARD_CENTRAL && order == 8) {
+    o->h = 4; o->nb = 4; o->S = 7;
+    o->c[4] = 35.0 / 128.0; o->c[5] = -7.0 / 32.0; o->c[6] = 7.0 / 64.0; o->c[7] = -1.0 / 32.0;
+    o->c[8] = 1.0 / 256.0;
+    o->c[4] = 1.0 - strength * o->c[4];
+    for (int k = 1; k <= 4; ++k) o->c[4 + k] *= -strength;
+    o->B[0][0] = 1.0; o->B[1][1] = 1.0;
+    for (int s = 0; s < 5; ++s) o->B[2][s] = r2[s];
+    for (int s = 0; s < 7; ++s) o->B[3][s] = r3[s];
+  } else if (scheme == LEE_FILTER_SFO11P) {
+    o->h = 5; o->nb = 5; o->S = 9;
+    double d[6] = {0.215044884112, -0.187772883589, 0.123755948787, -0.059227575576, 0.018721609157,
+                   -0.002999540835};
+    for (int k = 0; k <= 5; ++k) o->c[5 + k] = d[k];
+    o->c[5] = 1.0 - strength * o->c[5];
+    for (int k = 1; k <= 5; ++k) o->c[5 + k] *= -strength;
+    o->B[0][0] = 1.0; o->B[1][1] = 1.0;
+    for (int s = 0; s < 5; ++s) o->B[2][s] = r2[s];
+    for (int s = 0; s < 7; ++s) o->B[3][s] = r3[s];
+    double r4[9] = {0.008228661760, -0.045211119360, 0.120007591680, -0.204788880640, 0.243527493120,
+                    -0.204788880640, 0.120007591680, -0.045211119360, 0.008228661760};
+    for (int s = 0; s < 9; ++s) o->B[4][s] = (s == 4) ? 1.0 - strength * r4[s] : r4[s] * -strength;
+  } else {
+    return 0;
+  }
+  for (int k = 1; k <= o->h; ++k) o->c[o->h - k] = o->c[o->h + k];
+  return 1;
+}
+
+/* ---------------------------------------------------------------------------
+ * One directional application of an operator to f, written to out:
+ * StandardCentral::apply_spatial_discretization (src/solver/spatial_discretization.cpp:1078-1290)
+ * on a single rank (no ghost cells: is = iso = 0, ie = ieo = n-1, and the stencil
+ * ranges of src/geometry/geometry.cpp:931-1001), followed by
+ * StandardCentral::iblank_correction (:1356-1652) with the right/left hole
+ * closures of :1656-1745. iblank may be NULL (all fluid). Returns 0, or -1 when
+ * the reference's fluid-support assert (:1749-1798) would fire. */
+static int apply_dir(const op_t *o, const blk_t *bk, const int *iblank, const double *f, double *out, int d) {
+  int n[3] = {bk->nx, bk->ny, bk->nz};
+  int st[3] = {1, bk->nx, bk->nx * bk->ny};
+  int nd = n[d], sd = st[d];
+  int o1 = (d == 0) ? 1 : 0, o2 = (d == 2) ? 1 : 2;
+  int h = o->h, nb = o->nb, S = o->S;
+  for (int b2 = 0; b2 < n[o2]; ++b2)
+    for (int b1 = 0; b1 < n[o1]; ++b1) {
+      int base = b1 * st[o1] + b2 * st[o2];
+      for (int i = 0; i < nd; ++i) out[base + i * sd] = 0.0;
+      for (int i = h; i <= nd - 1 - h; ++i) {
+        int l0 = base + i * sd;
+        double acc = out[l0];
+        for (int l = -h; l <= h; ++l) acc += o->c[l + h] * f[l0 + l * sd];
+        out[l0] = acc;
+      }
+      for (int i = 0; i < h; ++i) { /* left boundary rows anchored at the first point */
+        int l0 = base + i * sd;
+        double acc = out[l0];
+        for (int s = 0; s < S; ++s) acc += o->B[i][s] * f[base + s * sd];
+        out[l0] = acc;
+      }
+      for (int i = nd - 1; i > nd - 1 - h; --i) { /* right rows mirrored from the last point */
+        int r = nd - 1 - i;
+        int l0 = base + i * sd, le = base + (nd - 1) * sd;
+        double acc = out[l0];
+        for (int s = 0; s < S; ++s) acc += o->mfac * o->B[r][s] * f[le - s * sd];
+        out[l0] = acc;
+      }
+      if (!iblank) continue;
+      int last = iblank[base];
+      for (int i = 0; i < nd; ++i) {
+        int l0 = base + i * sd;
+        int my = iblank[l0];
+        if (my == BLANKED) {
+          if (last == BLANKED) {
+            out[l0] = 0.0;
+          } else if (last / BLANKED) { /* `last_iblank /= BLANKED` (:1391): true only after an INTERPOLATED point */
+            if (i > 0) {
+              for (int ib = 0; ib < nb; ++ib) {
+                int p = i - 1 - ib;
+                if (p < 0) return -1;
+                if (iblank[base + p * sd] > 0) return -1;
+              }
+              if (i - 1 - (S - 1) < 0) return -1; /* the rows would read outside the line */
+              int lref = base + (i - 1) * sd;
+              for (int ib = 0; ib < nb; ++ib) {
+                int p = i - 1 - ib;
+                if (p >= 0 && p <= nd - 1) {
+                  int l1 = base + p * sd;
+                  out[l1] = 0.0;
+                  for (int s = 0; s < S; ++s) out[l1] += o->mfac * o->B[ib][s] * f[lref - s * sd];
+                }
+              }
+            }
+          }
+        } else {
+          if (last == BLANKED && i <= nd - 1) {
+            for (int ib = 0; ib < nb; ++ib) {
+              int p = i + ib;
+              if (p > nd - 1) return -1;
+              if (iblank[base + p * sd] > 0) return -1;
+            }
+            if (i + S - 1 > nd - 1) return -1; /* the rows would read outside the line */
+            for (int ib = 0; ib < nb; ++ib) {
+              int p = i + ib;
+              if (p >= 0 && p <= nd - 1) {
+                int l1 = base + p * sd;
+                out[l1] = 0.0;
+                for (int s = 0; s < S; ++s) out[l1] += o->B[ib][s] * f[l0 + s * sd];
+              }
+            }
+          }
+        }
+        last = my;
+      }
+    }
+  return 0;
+}
+
+/* take_derivative_xi_eta_zeta (:1322-1336): dflux <- 0, then the operator; a
+ * one-cell direction leaves zero (:1080-1081). */
+static int d_xi(orc_ctx *c, const blk_t *bk, const int *ib, const double *f, double *out, int d) {
+  int n[3] = {bk->nx, bk->ny, bk->nz};
+  if (n[d] == 1) {
+    memset(out, 0, sizeof(double) * (size_t)bk->N);
+    return 0;
+  }
+  if (apply_dir(&c->fd, bk, ib, f, out, d)) return fail(c, LEE_ERR_ARG, "hole closure lacks fluid support");
+  return 0;
+}
+
+/* take_derivative_xyz (:1802-1826): dflux = J * sum_l metrics[l][i] * d/dxi_l f. */
+static int d_x(orc_ctx *c, const blk_t *bk, const double *f, double *out, int i, double *work) {
+  int nd = c->cfg.num_dim, N = bk->N;
+  double *sum = dalloc((size_t)N);
+  for (int l = 0; l < nd; ++l) {
+    int rc = d_xi(c, bk, bk->iblank, f, work, l);
+    if (rc) { free(sum); return rc; }
+    const double *m = bk->met[l * 3 + i];
+    for (int p = 0; p < N; ++p) sum[p] += m[p] * work[p];
+  }
+  for (int p = 0; p < N; ++p) out[p] = sum[p] * bk->jac[p];
+  free(sum);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Metrics: metrics::compute (src/metrics/metrics.cpp:9-44) with Thomas-Lombard
+ * products (:107-251), the Jacobian (:255-328, with oracle patch P1 in 3-D: the
+ * determinant formula kept as comments at :297-307) and the inverse (:355-426).
+ * The reference computes metrics before the overset iblank exists
+ * (src/core/simulation.cpp:207 vs :214), so no hole closures apply here. */
+static int compute_metrics(orc_ctx *c, blk_t *bk) {
+  int nd = c->cfg.num_dim, N = bk->N;
+  double *xx[3][3] = {{0}};
+  double *func = dalloc((size_t)N), *tmp = dalloc((size_t)N);
+  for (int k = 0; k < 9; ++k) {
+    bk->met[k] = dalloc((size_t)N);
+    bk->minv[k] = dalloc((size_t)N);
+  }
+  bk->jac = dalloc((size_t)N);
+  bk->invjac = dalloc((size_t)N);
+  for (int ip = 0; ip < nd; ++ip)
+    for (int ic = 0; ic < nd; ++ic) {
+      xx[ip][ic] = dalloc((size_t)N);
+      if (d_xi(c, bk, NULL, bk->xyz[ip], xx[ip][ic], ic)) return LEE_ERR_ARG;
+    }
+  double **m = bk->met;
+#define M(l, i) m[(l) * 3 + (i)]
+  if (nd == 2) {
+    for (int p = 0; p < N; ++p) {
+      M(0, 0)[p] = xx[1][1][p];
+      M(0, 1)[p] = -xx[0][1][p];
+      M(1, 0)[p] = -xx[1][0][p];
+      M(1, 1)[p] = xx[0][0][p];
+    }
+  } else {
+    double **z = bk->xyz;
+    /* xi_x and zeta_x from (y_eta z) */
+    for (int p = 0; p < N; ++p) func[p] = xx[1][1][p] * z[2][p];
+    d_xi(c, bk, NULL, func, tmp, 2); for (int p = 0; p < N; ++p) M(0, 0)[p] = tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 0); for (int p = 0; p < N; ++p) M(2, 0)[p] = -tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[0][1][p] * z[2][p];
+    d_xi(c, bk, NULL, func, tmp, 2); for (int p = 0; p < N; ++p) M(0, 1)[p] = -tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 0); for (int p = 0; p < N; ++p) M(2, 1)[p] = tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[0][1][p] * z[1][p];
+    d_xi(c, bk, NULL, func, tmp, 2); for (int p = 0; p < N; ++p) M(0, 2)[p] = tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 0); for (int p = 0; p < N; ++p) M(2, 2)[p] = -tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[1][0][p] * z[2][p];
+    d_xi(c, bk, NULL, func, tmp, 2); for (int p = 0; p < N; ++p) M(1, 0)[p] = -tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 1); for (int p = 0; p < N; ++p) M(2, 0)[p] += tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[0][0][p] * z[2][p];
+    d_xi(c, bk, NULL, func, tmp, 2); for (int p = 0; p < N; ++p) M(1, 1)[p] = tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 1); for (int p = 0; p < N; ++p) M(2, 1)[p] -= tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[0][0][p] * z[1][p];
+    d_xi(c, bk, NULL, func, tmp, 2); for (int p = 0; p < N; ++p) M(1, 2)[p] = -tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 1); for (int p = 0; p < N; ++p) M(2, 2)[p] += tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[1][2][p] * z[2][p];
+    d_xi(c, bk, NULL, func, tmp, 1); for (int p = 0; p < N; ++p) M(0, 0)[p] -= tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 0); for (int p = 0; p < N; ++p) M(1, 0)[p] += tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[0][2][p] * z[2][p];
+    d_xi(c, bk, NULL, func, tmp, 1); for (int p = 0; p < N; ++p) M(0, 1)[p] += tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 0); for (int p = 0; p < N; ++p) M(1, 1)[p] -= tmp[p];
+    for (int p = 0; p < N; ++p) func[p] = xx[0][2][p] * z[1][p];
+    d_xi(c, bk, NULL, func, tmp, 1); for (int p = 0; p < N; ++p) M(0, 2)[p] -= tmp[p];
+    d_xi(c, bk, NULL, func, tmp, 0); for (int p = 0; p < N; ++p) M(1, 2)[p] += tmp[p];
+  }
+  for (int p = 0; p < N; ++p) {
+    if (nd == 2) {
+      bk->invjac[p] = xx[0][0][p] * xx[1][1][p] - xx[0][1][p] * xx[1][0][p];
+    } else {
+      bk->invjac[p] = xx[0][0][p] * (xx[1][1][p] * xx[2][2][p] - xx[1][2][p] * xx[2][1][p])
+                    - xx[0][1][p] * (xx[1][0][p] * xx[2][2][p] - xx[1][2][p] * xx[2][0][p])
+                    + xx[0][2][p] * (xx[1][0][p] * xx[2][1][p] - xx[1][1][p] * xx[2][0][p]);
+    }
+    bk->jac[p] = 1.0 / bk->invjac[p];
+  }
+  double **mi = bk->minv;
+#define MI(i, l) mi[(i) * 3 + (l)]
+  for (int p = 0; p < N; ++p) {
+    if (nd == 2) {
+      MI(0, 0)[p] = M(1, 1)[p];
+      MI(0, 1)[p] = -M(0, 1)[p];
+      MI(1, 0)[p] = -M(1, 0)[p];
+      MI(1, 1)[p] = M(0, 0)[p];
+    } else {
+      MI(0, 0)[p] = M(1, 1)[p] * M(2, 2)[p] - M(1, 2)[p] * M(2, 1)[p];
+      MI(0, 1)[p] = M(0, 2)[p] * M(2, 1)[p] - M(0, 1)[p] * M(2, 2)[p];
+      MI(0, 2)[p] = M(0, 1)[p] * M(1, 2)[p] - M(0, 2)[p] * M(1, 1)[p];
+      MI(1, 0)[p] = M(1, 2)[p] * M(2, 0)[p] - M(1, 0)[p] * M(2, 2)[p];
+      MI(1, 1)[p] = M(0, 0)[p] * M(2, 2)[p] - M(0, 2)[p] * M(2, 0)[p];
+      MI(1, 2)[p] = M(0, 2)[p] * M(1, 0)[p] - M(0, 0)[p] * M(1, 2)[p];
+      MI(2, 0)[p] = M(1, 0)[p] * M(2, 1)[p] - M(1, 1)[p] * M(2, 0)[p];
+      MI(2, 1)[p] = M(0, 1)[p] * M(2, 0)[p] - M(0, 0)[p] * M(2, 1)[p];
+      MI(2, 2)[p] = M(0, 0)[p] * M(1, 1)[p] - M(0, 1)[p] * M(1, 0)[p];
+    }
+  }
+#undef M
+#undef MI
+  for (int ip = 0; ip < 3; ++ip)
+    for (int ic = 0; ic < 3; ++ic) free(xx[ip][ic]);
+  free(func);
+  free(tmp);
+  return 0;
+}
+
+/* State::compute_auxiliary_variables_linear_Euler (src/core/state.cpp:701-736). */
+static void compute_aux(orc_ctx *c, blk_t *bk, double *const *y) {
+  double g = c->cfg.gamma, gi = 1.0 / g, gg = g / (g - 1.0);
+  for (int p = 0; p < bk->N; ++p) {
+    double sbar = bk->mean[0][p], pbar = bk->mean[4][p];
+    double pbi = 1.0 / pbar;
+    double rhobar = pow(g * pbar, gi) * exp(-sbar);
+    double rbi = 1.0 / rhobar;
+    double Tbar = pbar * gg * rbi;
+    bk->aux[1][p] = rhobar;
+    bk->aux[0][p] = y[4][p] * gi * pbi - y[0][p];
+    bk->aux[0][p] *= rhobar;
+    bk->aux[3][p] = Tbar;
+    bk->aux[2][p] = y[4][p] * pbi - bk->aux[0][p] * rbi;
+    bk->aux[2][p] *= Tbar;
+  }
+}
+
+/* Sponge strength: Geometry::additionalInit_bufferZones (src/geometry/geometry.cpp:1028-1142)
+ * with the zone's IN/OUT faces of StructuredBufferZone::set_parameters_4bufferZone (:715-743). */
+static void compute_sigma(orc_ctx *c, blk_t *bk, bnd_t *z) {
+  int bn[3], face[2][2];
+  for (int d = 0; d < 3; ++d) bn[d] = z->hi[d] - z->lo[d] + 1;
+  int nb = bn[0] * bn[1] * bn[2];
+  z->sigma = dalloc((size_t)nb);
+  int d = z->dir;
+  /* [side][0] = index of the face in direction d; side 0 = IN, 1 = OUT */
+  if (z->end == 0) { face[0][0] = z->hi[d]; face[1][0] = z->lo[d]; }
+  else { face[0][0] = z->lo[d]; face[1][0] = z->hi[d]; }
+  for (int k = z->lo[2]; k <= z->hi[2]; ++k)
+    for (int j = z->lo[1]; j <= z->hi[1]; ++j)
+      for (int i = z->lo[0]; i <= z->hi[0]; ++i) {
+        int l0 = i + bk->nx * (j + bk->ny * k);
+        double xb[3] = {bk->xyz[0][l0], bk->xyz[1][l0], bk->xyz[2][l0]};
+        double dist[2];
+        for (int side = 0; side < 2; ++side) {
+          double dmin = 1000000000.0; /* abs(DUMMY_DOUBLE) through int abs (:1110) */
+          int flo[3] = {z->lo[0], z->lo[1], z->lo[2]}, fhi[3] = {z->hi[0], z->hi[1], z->hi[2]};
+          flo[d] = fhi[d] = face[side][0];
+          for (int kk = flo[2]; kk <= fhi[2]; ++kk)
+            for (int jj = flo[1]; jj <= fhi[1]; ++jj)
+              for (int ii = flo[0]; ii <= fhi[0]; ++ii) {
+                int lf = ii + bk->nx * (jj + bk->ny * kk);
+                double s = 0.0;
+                for (int q = 0; q < 3; ++q) s += pow(xb[q] - bk->xyz[q][lf], 2);
+                if (s < dmin) dmin = s;
+              }
+          dist[side] = sqrt(dmin);
+        }
+        double rel = dist[0] / (dist[0] + dist[1]);
+        int lb = (i - z->lo[0]) + bn[0] * ((j - z->lo[1]) + bn[1] * (k - z->lo[2]));
+        z->sigma[lb] = c->cfg.sponge_constant * pow(rel, c->cfg.sponge_order);
+      }
+}
+
+/* ---------------------------------------------------------------------------
+ * Right-hand side: spatial::compute_RHS (src/solver/spatial_discretization.cpp:1963-1990),
+ * compute_RHS_linearized_Euler (:2053-2130) and source::add_RHSSourceTerms
+ * (src/solver/source.cpp:10-18): physical source, then Freund sponges (:174-201). */
+static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, double time) {
+  int nd = c->cfg.num_dim, N = bk->N;
+  double g = c->cfg.gamma;
+  double *df = dalloc((size_t)N), *work = dalloc((size_t)N);
+  int rc = 0;
+  for (int v = 0; v < 5; ++v) memset(rhs[v], 0, sizeof(double) * (size_t)N);
+  for (int j = 0; j < nd && !rc; ++j) { /* entropy */
+    rc = d_x(c, bk, y[0], df, j, work);
+    for (int p = 0; p < N; ++p) rhs[0][p] -= bk->mean[1 + j][p] * df[p];
+    for (int p = 0; p < N; ++p) rhs[0][p] -= y[1 + j][p] * bk->grad[0 * nd + j][p];
+  }
+  for (int i = 0; i < nd && !rc; ++i) { /* velocity */
+    for (int j = 0; j < nd && !rc; ++j) {
+      rc = d_x(c, bk, y[1 + i], df, j, work);
+      for (int p = 0; p < N; ++p) rhs[1 + i][p] -= bk->mean[1 + j][p] * df[p];
+      for (int p = 0; p < N; ++p)
+        rhs[1 + i][p] -= (y[1 + j][p] + bk->aux[0][p] / bk->aux[1][p] * bk->mean[1 + j][p]) *
+                         bk->grad[(1 + i) * nd + j][p];
+    }
+    if (!rc) rc = d_x(c, bk, y[4], df, i, work);
+    for (int p = 0; p < N; ++p) rhs[1 + i][p] -= df[p] / bk->aux[1][p];
+  }
+  for (int j = 0; j < nd && !rc; ++j) { /* pressure */
+    rc = d_x(c, bk, y[4], df, j, work);
+    for (int p = 0; p < N; ++p) rhs[4][p] -= bk->mean[1 + j][p] * df[p];
+    for (int p = 0; p < N; ++p) rhs[4][p] -= y[1 + j][p] * bk->grad[4 * nd + j][p];
+    if (!rc) rc = d_x(c, bk, y[1 + j], df, j, work);
+    for (int p = 0; p < N; ++p) rhs[4][p] -= g * bk->mean[4][p] * df[p];
+    for (int p = 0; p < N; ++p) rhs[4][p] -= g * y[4][p] * bk->grad[(1 + j) * nd + j][p];
+  }
+  free(df);
+  free(work);
+  if (rc) return rc;
+  if (c->src_kind == LEE_SOURCE_MONOPOLE) { /* oracle patch P2 (oracle/ref_patch_source.cpp) */
+    double x0 = c->src[0], y0 = c->src[1], z0 = c->src[2], amp = c->src[3], om = c->src[4];
+    double b = c->src[5], T = c->src[6];
+    double ramp = 1.0;
+    if (T > 0.0 && time < T) {
+      double s = sin(0.5 * M_PI * time / T);
+      ramp = s * s;
+    }
+    double fac = amp * (g - 1.0) * ramp * sin(om * time);
+    double ef = -log(2.0) / (b * b);
+    for (int p = 0; p < N; ++p) {
+      double dx = bk->xyz[0][p] - x0, dy = bk->xyz[1][p] - y0, dz = bk->xyz[2][p] - z0;
+      rhs[4][p] += fac * exp(ef * (dx * dx + dy * dy + dz * dz));
+    }
+  }
+  for (int zi = 0; zi < bk->nbnd; ++zi) {
+    bnd_t *z = &bk->bnd[zi];
+    if (z->kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+    int bn0 = z->hi[0] - z->lo[0] + 1, bn1 = z->hi[1] - z->lo[1] + 1;
+    for (int k = z->lo[2]; k <= z->hi[2]; ++k)
+      for (int j = z->lo[1]; j <= z->hi[1]; ++j)
+        for (int i = z->lo[0]; i <= z->hi[0]; ++i) {
+          int lb = (i - z->lo[0]) + bn0 * ((j - z->lo[1]) + bn1 * (k - z->lo[2]));
+          int l0 = i + bk->nx * (j + bk->ny * k);
+          double sg = z->sigma[lb];
+          for (int v = 0; v < 5; ++v) {
+            double relax = -sg * (y[v][l0] - 0.0);
+            rhs[v][l0] += relax;
+          }
+        }
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Boundary conditions: bc::apply_BC (src/solver/boundary_condition.cpp:46-209) with
+ * bc_neumann (:348-444) and bc_wall_slip_kinematic (:448-494). The boundary is the
+ * box's end face in its direction (src/geometry/geometry.cpp:583-645). */
+static void apply_bc(orc_ctx *c, blk_t *bk, double **y) {
+  int nd = c->cfg.num_dim;
+  int st[3] = {1, bk->nx, bk->nx * bk->ny};
+  const op_t *o = &c->fd;
+  for (int zi = 0; zi < bk->nbnd; ++zi) {
+    bnd_t *z = &bk->bnd[zi];
+    if (z->kind != LEE_BC_NEUMANN && z->kind != LEE_BC_WALL_SLIP_KINEMATIC) continue;
+    int lo[3] = {z->lo[0], z->lo[1], z->lo[2]}, hi[3] = {z->hi[0], z->hi[1], z->hi[2]};
+    lo[z->dir] = hi[z->dir] = (z->end == 0) ? z->lo[z->dir] : z->hi[z->dir];
+    int sd = st[z->dir];
+    int nbx = hi[0] - lo[0] + 1, nby = hi[1] - lo[1] + 1, nbz = hi[2] - lo[2] + 1;
+    int nbp = nbx * nby * nbz;
+    double *data[5];
+    for (int v = 0; v < 5; ++v) data[v] = dalloc((size_t)nbp);
+    int vars_neu[5], nneu = 0;
+    if (z->kind == LEE_BC_NEUMANN) {
+      for (int v = 0; v < 5; ++v) vars_neu[nneu++] = v;
+    } else {
+      vars_neu[nneu++] = 0;
+      vars_neu[nneu++] = 4;
+    }
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          int lb = (i - lo[0]) + nbx * ((j - lo[1]) + nby * (k - lo[2]));
+          int l0 = i + bk->nx * (j + bk->ny * k);
+          int hole = bk->iblank && bk->iblank[l0] == BLANKED;
+          if (!hole) {
+            for (int q = 0; q < nneu; ++q) {
+              int v = vars_neu[q];
+              data[v][lb] = 0.0;
+              if (z->end == 0) {
+                for (int s = 1; s < o->S; ++s) data[v][lb] -= o->B[0][s] * y[v][l0 + sd * s];
+                data[v][lb] /= o->B[0][0];
+              } else {
+                for (int s = 1; s < o->S; ++s) data[v][lb] += o->B[0][s] * y[v][l0 - sd * s];
+                data[v][lb] /= -o->B[0][0];
+              }
+            }
+          }
+          if (z->kind == LEE_BC_WALL_SLIP_KINEMATIC) {
+            double vc[3] = {0, 0, 0}, vel[3] = {0, 0, 0};
+            if (!hole) {
+              for (int q = 0; q < 3; ++q) vel[q] = y[1 + q][l0];
+              for (int l = 0; l < nd; ++l) {
+                vc[l] = 0.0;
+                for (int q = 0; q < nd; ++q) vc[l] += bk->met[l * 3 + q][l0] * vel[q];
+              }
+              vc[z->dir] = 0.0;
+              for (int q = 0; q < nd; ++q) {
+                vel[q] = 0.0;
+                for (int l = 0; l < nd; ++l) vel[q] += bk->minv[q * 3 + l][l0] * vc[l];
+                vel[q] *= bk->jac[l0];
+              }
+            }
+            for (int q = 0; q < 3; ++q) data[1 + q][lb] = vel[q];
+          }
+        }
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          int lb = (i - lo[0]) + nbx * ((j - lo[1]) + nby * (k - lo[2]));
+          int l0 = i + bk->nx * (j + bk->ny * k);
+          if (bk->iblank && bk->iblank[l0] == BLANKED) continue;
+          for (int v = 0; v < 5; ++v) y[v][l0] = data[v][lb];
+        }
+    for (int v = 0; v < 5; ++v) free(data[v]);
+  }
+}
+
+/* spatial::apply_filter (src/solver/spatial_discretization.cpp:2191-2246) for one block. */
+static int filter_block(orc_ctx *c, blk_t *bk, double **y) {
+  int N = bk->N, n[3] = {bk->nx, bk->ny, bk->nz};
+  double *func0 = dalloc((size_t)N), *func = dalloc((size_t)N), *out = dalloc((size_t)N);
+  double blend = c->cfg.filter_blend, rem = 1.0 - blend;
+  for (int v = 0; v < 5; ++v) {
+    memcpy(func0, y[v], sizeof(double) * (size_t)N);
+    memcpy(func, func0, sizeof(double) * (size_t)N);
+    for (int d = 0; d < c->cfg.num_dim; ++d) {
+      if (n[d] == 1) continue; /* dflux = func: a one-cell direction is left alone */
+      if (apply_dir(&c->flt, bk, bk->iblank, func, out, d)) {
+        free(func0); free(func); free(out);
+        return fail(c, LEE_ERR_ARG, "filter hole closure lacks fluid support");
+      }
+      memcpy(func, out, sizeof(double) * (size_t)N);
+    }
+    for (int p = 0; p < N; ++p) y[v][p] = rem * func0[p] + blend * func[p];
+  }
+  free(func0); free(func); free(out);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Exported ABI (orc_ prefix). */
+int orc_create(const lee_config *cfg, orc_ctx **out) {
+  if (!cfg || !out) return fail(NULL, LEE_ERR_ARG, "null argument");
+  if (cfg->num_dim != 2 && cfg->num_dim != 3) return fail(NULL, LEE_ERR_ARG, "num_dim must be 2 or 3");
+  if (cfg->num_blocks < 1 || cfg->num_blocks > MAXB) return fail(NULL, LEE_ERR_ARG, "bad num_blocks");
+  orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
+  c->cfg = *cfg;
+  if (!make_fd(&c->fd, cfg->fd_scheme, cfg->fd_order)) {
+    free(c);
+    return fail(NULL, LEE_ERR_UNSUPPORTED, "unsupported spatial scheme");
+  }
+  if (cfg->filter_scheme != LEE_FILTER_NONE) {
+    double s = cfg->filter_scheme == LEE_FILTER_STANDARD_CENTRAL ? 1.0 : cfg->filter_strength;
+    if (!make_filter(&c->flt, cfg->filter_scheme, cfg->filter_order, s)) {
+      free(c);
+      return fail(NULL, LEE_ERR_UNSUPPORTED, "unsupported filter");
+    }
+  }
+  c->nblk = cfg->num_blocks;
+  *out = c;
+  return LEE_OK;
+}
+
+void orc_destroy(orc_ctx *c) {
+  if (!c) return;
+  for (int b = 0; b < c->nblk; ++b) {
+    blk_t *bk = &c->blk[b];
+    for (int q = 0; q < 3; ++q) free(bk->xyz[q]);
+    free(bk->iblank);
+    for (int q = 0; q < 9; ++q) { free(bk->met[q]); free(bk->minv[q]); }
+    free(bk->jac); free(bk->invjac);
+    for (int q = 0; q < 5; ++q) { free(bk->mean[q]); free(bk->sol[q]); }
+    for (int q = 0; q < 15; ++q) free(bk->grad[q]);
+    for (int q = 0; q < 4; ++q) free(bk->aux[q]);
+    for (int q = 0; q < bk->nbnd; ++q) free(bk->bnd[q].sigma);
+  }
+  free(c);
+}
+
+const char *orc_last_error(const orc_ctx *c) { return c ? c->err : g_err; }
+
+int orc_set_block(orc_ctx *c, int b, int nx, int ny, int nz, const double *x, const double *y,
+                  const double *z, const int *iblank) {
+  if (b < 0 || b >= c->nblk) return fail(c, LEE_ERR_ARG, "block index");
+  blk_t *bk = &c->blk[b];
+  bk->nx = nx; bk->ny = ny; bk->nz = nz;
+  bk->N = nx * ny * nz;
+  const double *src[3] = {x, y, z};
+  for (int q = 0; q < 3; ++q) {
+    bk->xyz[q] = dalloc((size_t)bk->N);
+    memcpy(bk->xyz[q], src[q], sizeof(double) * (size_t)bk->N);
+  }
+  if (iblank) {
+    bk->iblank = (int *)malloc(sizeof(int) * (size_t)bk->N);
+    memcpy(bk->iblank, iblank, sizeof(int) * (size_t)bk->N);
+  }
+  for (int q = 0; q < 5; ++q) { bk->mean[q] = dalloc((size_t)bk->N); bk->sol[q] = dalloc((size_t)bk->N); }
+  for (int q = 0; q < 4; ++q) bk->aux[q] = dalloc((size_t)bk->N);
+  bk->set = 1;
+  return LEE_OK;
+}
+
+int orc_set_mean(orc_ctx *c, int b, const double *const mean[5]) {
+  if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_STATE, "set_block first");
+  for (int q = 0; q < 5; ++q) memcpy(c->blk[b].mean[q], mean[q], sizeof(double) * (size_t)c->blk[b].N);
+  return LEE_OK;
+}
+
+int orc_add_boundary(orc_ctx *c, int b, int kind, int dir, int end, const int lo[3], const int hi[3],
+                     const double *sigma) {
+  if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_STATE, "set_block first");
+  blk_t *bk = &c->blk[b];
+  if (bk->nbnd >= MAXBND) return fail(c, LEE_ERR_ARG, "too many boundaries");
+  bnd_t *z = &bk->bnd[bk->nbnd++];
+  z->kind = kind; z->dir = dir; z->end = end;
+  for (int d = 0; d < 3; ++d) { z->lo[d] = lo[d]; z->hi[d] = hi[d]; }
+  z->sigma = NULL;
+  if (kind == LEE_SPONGE_FREUND_AMBIENT && sigma) {
+    int nb = (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    z->sigma = dalloc((size_t)nb);
+    memcpy(z->sigma, sigma, sizeof(double) * (size_t)nb);
+  }
+  return LEE_OK;
+}
+
+int orc_set_source(orc_ctx *c, int kind, const double *params, int np) {
+  c->src_kind = kind;
+  for (int i = 0; i < 7 && i < np; ++i) c->src[i] = params[i];
+  return LEE_OK;
+}
+
+int orc_prepare(orc_ctx *c) {
+  for (int b = 0; b < c->nblk; ++b) {
+    blk_t *bk = &c->blk[b];
+    if (!bk->set) return fail(c, LEE_ERR_STATE, "block %d not set", b);
+    int rc = compute_metrics(c, bk);
+    if (rc) return rc;
+    for (int zi = 0; zi < bk->nbnd; ++zi)
+      if (bk->bnd[zi].kind == LEE_SPONGE_FREUND_AMBIENT && !bk->bnd[zi].sigma) compute_sigma(c, bk, &bk->bnd[zi]);
+    /* mean gradients: spatial::precompute_something (:2250-2271), with hole closures */
+    int nd = c->cfg.num_dim;
+    double *work = dalloc((size_t)bk->N);
+    for (int v = 0; v < 5; ++v)
+      for (int j = 0; j < nd; ++j) {
+        bk->grad[v * nd + j] = dalloc((size_t)bk->N);
+        rc = d_x(c, bk, bk->mean[v], bk->grad[v * nd + j], j, work);
+        if (rc) { free(work); return rc; }
+      }
+    free(work);
+    compute_aux(c, bk, bk->sol);
+  }
+  c->prepared = 1;
+  return LEE_OK;
+}
+
+int orc_upload_state(orc_ctx *c, int b, const double *const sol[5], int step, double time) {
+  if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_STATE, "set_block first");
+  blk_t *bk = &c->blk[b];
+  for (int q = 0; q < 5; ++q) memcpy(bk->sol[q], sol[q], sizeof(double) * (size_t)bk->N);
+  c->step = step;
+  c->time = time;
+  if (c->prepared) compute_aux(c, bk, bk->sol);
+  return LEE_OK;
+}
+
+int orc_download_state(orc_ctx *c, int b, double *const sol[5], int *step, double *time) {
+  if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_STATE, "set_block first");
+  blk_t *bk = &c->blk[b];
+  for (int q = 0; q < 5; ++q) memcpy(sol[q], bk->sol[q], sizeof(double) * (size_t)bk->N);
+  if (step) *step = c->step;
+  if (time) *time = c->time;
+  return LEE_OK;
+}
+
+/* temporal::compute_CFL (src/solver/temporal_discretization.cpp:397-450) with the
+ * reference's dummy initial dt of 1e-6 (src/core/input.cpp:131) and the FIX_CFL
+ * rescale of solver::solve (src/solver/solver.cpp:58-64). */
+int orc_compute_dt(orc_ctx *c, double cfl_target, double *dt_out) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  int nd = c->cfg.num_dim;
+  double dt = 1e-6, cmax = -1e99, gm1 = c->cfg.gamma - 1.0;
+  for (int b = 0; b < c->nblk; ++b) {
+    blk_t *bk = &c->blk[b];
+    for (int p = 0; p < bk->N; ++p) {
+      if (bk->iblank && bk->iblank[p] != NOTBLANKED) continue;
+      double vcart[3] = {bk->mean[1][p], bk->mean[2][p], bk->mean[3][p]}, vc[3];
+      for (int q = nd; q < 3; ++q) vcart[q] = 0.0;
+      for (int l = 0; l < nd; ++l) {
+        vc[l] = 0.0;
+        for (int q = 0; q < nd; ++q) vc[l] += bk->met[l * 3 + q][p] * vcart[q];
+      }
+      double cfl = 0.0;
+      for (int l = 0; l < nd; ++l)
+        for (int q = 0; q < nd; ++q) cfl += abs((int)(vc[l] * bk->met[l * 3 + q][p]));
+      double fac = 0.0;
+      for (int l = 0; l < nd; ++l)
+        for (int q = 0; q < nd; ++q) fac += bk->met[l * 3 + q][p] * bk->met[l * 3 + q][p];
+      double sos = sqrt(gm1 * bk->aux[3][p]);
+      cfl += sos * sqrt(fac);
+      cfl *= dt * bk->jac[p];
+      if (cfl > cmax) cmax = cfl;
+    }
+  }
+  double ratio = cfl_target / cmax;
+  dt *= ratio;
+  *dt_out = dt;
+  return LEE_OK;
+}
+
+/* RungeKutta::integrate (src/solver/temporal_discretization.cpp:177-252) and
+ * temporal::time_advance (:334-374) for every block. Blocks advance in lockstep
+ * stage by stage, as the reference's ranks do between barriers. */
+int orc_advance(orc_ctx *c, int nsteps, double dt) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  double bi[4], ci[4], aij[4];
+  int ns;
+  if (c->cfg.rk_scheme == LEE_RK4) {
+    ns = 4;
+    bi[0] = 1.0 / 6.0; bi[1] = 1.0 / 3.0; bi[2] = 1.0 / 3.0; bi[3] = 1.0 / 6.0;
+    ci[0] = 0.0; ci[1] = 1.0 / 2.0; ci[2] = 1.0 / 2.0; ci[3] = 1.0;
+    aij[0] = 1.0 / 2.0; aij[1] = 1.0 / 2.0; aij[2] = 1.0; aij[3] = 0.0;
+  } else if (c->cfg.rk_scheme == LEE_RK2) {
+    ns = 2;
+    bi[0] = 1.0 / 2.0; bi[1] = 1.0 / 2.0;
+    ci[0] = 0.0; ci[1] = 1.0;
+    aij[0] = 1.0; aij[1] = 0.0;
+  } else {
+    return fail(c, LEE_ERR_UNSUPPORTED, "rk scheme");
+  }
+  int nb = c->nblk;
+  double *yn[MAXB][5], *ynext[MAXB][5], *zi[MAXB][5], *rhs[MAXB][5];
+  for (int b = 0; b < nb; ++b)
+    for (int v = 0; v < 5; ++v) {
+      size_t N = (size_t)c->blk[b].N;
+      yn[b][v] = dalloc(N); ynext[b][v] = dalloc(N); zi[b][v] = dalloc(N); rhs[b][v] = dalloc(N);
+    }
+  int rc = 0;
+  for (int it = 0; it < nsteps && !rc; ++it) {
+    c->time += dt; /* solver::solve increments the time before time_advance (src/solver/solver.cpp:72) */
+    c->step += 1;
+    double tn = c->time, h = dt;
+    for (int b = 0; b < nb; ++b)
+      for (int v = 0; v < 5; ++v) {
+        size_t N = (size_t)c->blk[b].N;
+        memcpy(yn[b][v], c->blk[b].sol[v], N * sizeof(double));
+        memcpy(ynext[b][v], yn[b][v], N * sizeof(double));
+        memcpy(zi[b][v], yn[b][v], N * sizeof(double));
+      }
+    for (int s = 0; s < ns && !rc; ++s) {
+      for (int b = 0; b < nb && !rc; ++b) {
+        blk_t *bk = &c->blk[b];
+        rc = rhs_block(c, bk, zi[b], rhs[b], tn + ci[s] * h);
+        for (int p = 0; p < bk->N; ++p) {
+          if (!(bk->iblank && bk->iblank[p] == BLANKED)) {
+            for (int v = 0; v < 5; ++v) {
+              rhs[b][v][p] *= h;
+              ynext[b][v][p] += bi[s] * rhs[b][v][p];
+              if (s < ns - 1) zi[b][v][p] = yn[b][v][p] + aij[s] * rhs[b][v][p];
+            }
+          } else {
+            for (int v = 0; v < 5; ++v) {
+              rhs[b][v][p] = 0.0;
+              ynext[b][v][p] = 0.0;
+              zi[b][v][p] = 0.0;
+            }
+          }
+        }
+      }
+      for (int b = 0; b < nb; ++b) { /* spatial::update_boundary (:2162-2187), then aux */
+        double **tgt = (s < ns - 1) ? zi[b] : ynext[b];
+        apply_bc(c, &c->blk[b], tgt);
+      }
+      for (int b = 0; b < nb; ++b) compute_aux(c, &c->blk[b], (s < ns - 1) ? zi[b] : ynext[b]);
+    }
+    for (int b = 0; b < nb && !rc; ++b) {
+      blk_t *bk = &c->blk[b];
+      if (c->cfg.filter_scheme != LEE_FILTER_NONE) rc = filter_block(c, bk, ynext[b]);
+      for (int p = 0; p < bk->N; ++p) /* temporal::iblank_correction (:380-393) */
+        if (bk->iblank && bk->iblank[p] == BLANKED)
+          for (int v = 0; v < 5; ++v) ynext[b][v][p] = 0.0;
+      for (int v = 0; v < 5; ++v) memcpy(bk->sol[v], ynext[b][v], sizeof(double) * (size_t)bk->N);
+    }
+  }
+  for (int b = 0; b < nb; ++b)
+    for (int v = 0; v < 5; ++v) { free(yn[b][v]); free(ynext[b][v]); free(zi[b][v]); free(rhs[b][v]); }
+  return rc;
+}
+
+int orc_eval_rhs(orc_ctx *c, int b, double time, double *const rhs[5]) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  blk_t *bk = &c->blk[b];
+  double *r[5];
+  for (int v = 0; v < 5; ++v) r[v] = rhs[v];
+  return rhs_block(c, bk, bk->sol, r, time);
+}
+
+int orc_apply_filter(orc_ctx *c) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  if (c->cfg.filter_scheme == LEE_FILTER_NONE) return LEE_OK;
+  for (int b = 0; b < c->nblk; ++b) {
+    int rc = filter_block(c, &c->blk[b], c->blk[b].sol);
+    if (rc) return rc;
+  }
+  return LEE_OK;
+}
+
+int orc_get_setup(orc_ctx *c, int b, int what, double *out) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  blk_t *bk = &c->blk[b];
+  size_t N = (size_t)bk->N;
+  int nd = c->cfg.num_dim;
+  if (what == LEE_SETUP_METRICS) {
+    for (int q = 0; q < 9; ++q) memcpy(out + q * N, bk->met[q], N * sizeof(double));
+  } else if (what == LEE_SETUP_JACOBIAN) {
+    memcpy(out, bk->jac, N * sizeof(double));
+  } else if (what == LEE_SETUP_MEAN_GRADIENT) {
+    for (int q = 0; q < 5 * nd; ++q) memcpy(out + q * N, bk->grad[q], N * sizeof(double));
+  } else if (what == LEE_SETUP_SPONGE) {
+    memset(out, 0, N * sizeof(double));
+    for (int zi = 0; zi < bk->nbnd; ++zi) {
+      bnd_t *z = &bk->bnd[zi];
+      if (z->kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+      int bn0 = z->hi[0] - z->lo[0] + 1, bn1 = z->hi[1] - z->lo[1] + 1;
+      for (int k = z->lo[2]; k <= z->hi[2]; ++k)
+        for (int j = z->lo[1]; j <= z->hi[1]; ++j)
+          for (int i = z->lo[0]; i <= z->hi[0]; ++i)
+            out[i + bk->nx * (j + bk->ny * k)] +=
+                z->sigma[(i - z->lo[0]) + bn0 * ((j - z->lo[1]) + bn1 * (k - z->lo[2]))];
+    }
+  } else {
+    return fail(c, LEE_ERR_ARG, "unknown setup selector");
+  }
+  return LEE_OK;
+}
+
+/* Sizes of the oracle context (the oracle has no device and no timers). */
+int orc_get_info(orc_ctx *c, lee_info *info) {
+  memset(info, 0, sizeof *info);
+  for (int b = 0; b < c->nblk; ++b) info->points += c->blk[b].N;
+  info->state_vars = c->cfg.num_dim + 2;
+  info->bytes_per_value = 8;
+  return LEE_OK;
+}
+
+int orc_set_timing(orc_ctx *c, int on) {
+  (void)c;
+  (void)on;
+  return LEE_OK;
+}
+
+int orc_get_stats(orc_ctx *c, lee_stats *st) {
+  (void)c;
+  memset(st, 0, sizeof *st);
+  return LEE_OK;
+}

@@ -1,0 +1,61 @@
+"""Generate the golden fixtures in tests/golden/ by running the compiled camille
+reference (oracle/_ref/camille_ref, built by oracle/build_ref.py from the
+reference's own sources with oracle patches P1-P3).
+
+The reference ships no tests, golden vectors or known-answer fixtures, so these
+outputs of the reference itself pin the oracle and the CUDA path. Each fixture
+holds, for one small workload: setup products (metrics, Jacobian, mean
+gradients, sponge strength), one right-hand side, one filter application, the
+FIX_CFL time step of the first step, and the state after 1 and after `steps`
+FIX_DT steps.
+
+Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from camille_b200 import cases  # noqa: E402
+from oracle import run_ref  # noqa: E402
+
+WORKLOADS = {
+    # 2-D quiescent pulse with four sponges: the 256^2 workload's spacing (100/255) and
+    # sponge constants on a 48^2 block (a coarser spacing makes the sponge's sigma*dt
+    # leave RK4's stability region, in the reference as well)
+    "pulse2d_48": lambda: cases.pulse2d(n=48, length=47 * 100.0 / 255.0, sponge=8, nsteps=20),
+    # 3-D curvilinear, Mach 0.5, closures only (the 256^3 workload at 16^3)
+    "curvi3d_16": lambda: cases.curvi3d(n=16, seed=2, npulses=8, nsteps=5, halfwidth=2.0),
+}
+
+
+def make(name: str) -> str:
+    case = WORKLOADS[name]()
+    nd = case.num_dim
+    setup = run_ref.assemble(case, run_ref.run(case, mode="setup")["ranks"])[0]
+    rhs = run_ref.assemble(case, run_ref.run(case, mode="rhs")["ranks"])[0]
+    filt = run_ref.assemble(case, run_ref.run(case, mode="filter")["ranks"])[0]
+    first = run_ref.run(case, mode="run", nsteps=1, dt=None)
+    dt = float(first["result"]["dt"])
+    step1 = run_ref.assemble(case, run_ref.run(case, mode="run", nsteps=1, dt=dt)["ranks"])[0]
+    stepn = run_ref.assemble(case, run_ref.run(case, mode="run", nsteps=case.nsteps, dt=dt)["ranks"])[0]
+    out = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(
+        out,
+        metrics=setup[0:9], jacobian=setup[9], mean_gradient=setup[12:12 + 5 * nd],
+        sponge=setup[12 + 5 * nd + 4], rhs=rhs, filter=filt, dt=np.float64(dt),
+        step1=step1, stepn=stepn, nsteps=np.int64(case.nsteps))
+    return out
+
+
+if __name__ == "__main__":
+    if not run_ref.available():
+        sys.exit("build the reference first: python oracle/build_ref.py")
+    for n in WORKLOADS:
+        print(make(n))

@@ -1,0 +1,83 @@
+"""Pin the CPU oracle (oracle/lee_oracle.c) to the camille reference.
+
+1. Against the committed golden fixtures (outputs of the compiled reference, made by
+   tests/golden/make_golden.py): setup products, one RHS, one filter, the FIX_CFL dt,
+   and the state after 1 and N steps must match to the last bit.
+2. Against the compiled reference run live (skipped where oracle/_ref is not built):
+   the other scheme combinations the reference offers (FDO11P, SFO11P, RK2, the
+   4th-order filter) and the sponge-free 2-D case.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from camille_b200 import api, cases
+from tests.conftest import golden_case, load_golden
+
+NAMES = ["pulse2d_48", "curvi3d_16"]
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_setup_matches_golden(oracle_lib, name):
+    g = load_golden(name)
+    case = golden_case(name)
+    s = api.Solver(oracle_lib, case)
+    np.testing.assert_array_equal(s.get_setup(0, api.SETUP_METRICS), g["metrics"])
+    np.testing.assert_array_equal(s.get_setup(0, api.SETUP_JACOBIAN)[0], g["jacobian"])
+    np.testing.assert_array_equal(s.get_setup(0, api.SETUP_MEAN_GRADIENT), g["mean_gradient"])
+    np.testing.assert_array_equal(s.get_setup(0, api.SETUP_SPONGE)[0], g["sponge"])
+    assert s.compute_dt() == float(g["dt"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_operators_match_golden(oracle_lib, name):
+    g = load_golden(name)
+    case = golden_case(name)
+    s = api.Solver(oracle_lib, case)
+    np.testing.assert_array_equal(s.eval_rhs(0, 0.0), g["rhs"])
+    s.apply_filter()
+    np.testing.assert_array_equal(s.download(0)[0], g["filter"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_steps_match_golden(oracle_lib, name):
+    g = load_golden(name)
+    case = golden_case(name)
+    dt = float(g["dt"])
+    s = api.Solver(oracle_lib, case)
+    s.advance(1, dt)
+    y, step, t = s.download(0)
+    np.testing.assert_array_equal(y, g["step1"])
+    assert step == 1 and t == dt
+    s.advance(int(g["nsteps"]) - 1, dt)
+    np.testing.assert_array_equal(s.download(0)[0], g["stepn"])
+
+
+def _live_cases():
+    c1 = cases.curvi3d(n=14, nsteps=3, halfwidth=2.0)
+    c1.fd_scheme, c1.filter_scheme, c1.filter_strength = "FDO11P", "SFO11P", 0.2
+    c2 = cases.pulse2d(n=40, length=39 * 100.0 / 255.0, sponge=6, nsteps=4)
+    c2.rk, c2.filter_order = "RUNGE_KUTTA2", 4
+    c3 = cases.pulse2d(n=36, length=35 * 100.0 / 255.0, sponge=0, nsteps=3)
+    c3.filter_blend = 0.75
+    c4 = cases.curvi3d(n=12, nsteps=2, mach=0.3, halfwidth=2.0)
+    c4.filter_scheme = "NONE"
+    return {"fdo11p_sfo11p_3d": c1, "rk2_filter4_2d": c2, "blend_2d": c3, "nofilter_3d": c4}
+
+
+@pytest.mark.parametrize("label", list(_live_cases().keys()))
+def test_oracle_matches_reference_live(oracle_lib, label):
+    from oracle import run_ref
+    if not run_ref.available():
+        pytest.skip("oracle/_ref/camille_ref not built here")
+    case = _live_cases()[label]
+    s = api.Solver(oracle_lib, case)
+    r1 = run_ref.run(case, mode="run", nsteps=1, dt=None)
+    dt = s.compute_dt()
+    assert dt == r1["result"]["dt"]
+    ref_rhs = run_ref.assemble(case, run_ref.run(case, mode="rhs")["ranks"])[0]
+    np.testing.assert_array_equal(s.eval_rhs(0, 0.0), ref_rhs)
+    ref = run_ref.assemble(case, run_ref.run(case, mode="run", nsteps=case.nsteps, dt=dt)["ranks"])[0]
+    s.advance(case.nsteps, dt)
+    np.testing.assert_array_equal(s.download(0)[0], ref)

@@ -1,0 +1,110 @@
+"""Parity of the CUDA path with the camille reference (golden fixtures made by running
+the compiled reference) and with the CPU oracle at larger sizes.
+
+Tolerances (relative L2 over all state variables): FP64 within 1e-12 after one step
+and within 1e-10 after N steps; operator-level FP64 results within 1e-12; setup
+products within 1e-13. The FP32-compensated form is held to 1e-5 relative L2 in p'
+against the FP64 reference.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from camille_b200 import api, cases
+from tests.conftest import golden_case, load_golden
+
+pytestmark = pytest.mark.gpu
+NAMES = ["pulse2d_48", "curvi3d_16"]
+
+
+def rl2(a, b):
+    return api.rel_l2(np.asarray(a), np.asarray(b))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_setup_products(product_lib, name):
+    g = load_golden(name)
+    s = api.Solver(product_lib, golden_case(name))
+    assert rl2(s.get_setup(0, api.SETUP_METRICS), g["metrics"]) <= 1e-14
+    assert rl2(s.get_setup(0, api.SETUP_JACOBIAN)[0], g["jacobian"]) <= 1e-14
+    mg = s.get_setup(0, api.SETUP_MEAN_GRADIENT)
+    scale = max(1.0, float(np.abs(g["mean_gradient"]).max()))
+    assert float(np.abs(mg - g["mean_gradient"]).max()) <= 1e-13 * scale
+    sp = s.get_setup(0, api.SETUP_SPONGE)[0]
+    assert float(np.abs(sp - g["sponge"]).max()) <= 1e-13 * max(1.0, float(g["sponge"].max()))
+    dt = s.compute_dt()
+    assert abs(dt - float(g["dt"])) <= 1e-14 * float(g["dt"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_rhs_and_filter(product_lib, name):
+    g = load_golden(name)
+    s = api.Solver(product_lib, golden_case(name))
+    assert rl2(s.eval_rhs(0, 0.0), g["rhs"]) <= 1e-12
+    s.apply_filter()
+    assert rl2(s.download(0)[0], g["filter"]) <= 1e-13
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fp64_steps(product_lib, name):
+    g = load_golden(name)
+    dt = float(g["dt"])
+    s = api.Solver(product_lib, golden_case(name))
+    s.advance(1, dt)
+    y, step, t = s.download(0)
+    assert step == 1 and t == dt
+    assert rl2(y, g["step1"]) <= 1e-12
+    s.advance(int(g["nsteps"]) - 1, dt)
+    assert rl2(s.download(0)[0], g["stepn"]) <= 1e-10
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fp32_compensated_steps(product_lib, name):
+    g = load_golden(name)
+    dt = float(g["dt"])
+    s = api.Solver(product_lib, golden_case(name), precision=api.FP32_COMPENSATED)
+    s.advance(int(g["nsteps"]), dt)
+    y = s.download(0)[0]
+    assert rl2(y[4], g["stepn"][4]) <= 1e-5
+
+
+def _larger():
+    a = cases.pulse2d(n=128, length=127 * 100.0 / 255.0, sponge=20, nsteps=60)
+    b = cases.curvi3d(n=40, nsteps=12, halfwidth=3.0)
+    c = cases.curvi3d(n=24, nsteps=6, halfwidth=2.0)
+    c.fd_scheme, c.filter_scheme, c.filter_strength = "FDO11P", "SFO11P", 0.2
+    d = cases.pulse2d(n=64, length=63 * 100.0 / 255.0, sponge=10, nsteps=10)
+    d.rk, d.filter_order, d.filter_blend = "RUNGE_KUTTA2", 4, 0.6
+    return {"pulse2d_128": a, "curvi3d_40": b, "fdo11p_3d_24": c, "rk2_2d_64": d}
+
+
+@pytest.mark.parametrize("label", list(_larger().keys()))
+def test_fp64_matches_oracle(product_lib, oracle_lib, label):
+    case = _larger()[label]
+    o = api.Solver(oracle_lib, case)
+    dt = o.compute_dt()
+    p = api.Solver(product_lib, case)
+    assert abs(p.compute_dt() - dt) <= 1e-14 * dt
+    assert rl2(p.eval_rhs(0, 0.3), o.eval_rhs(0, 0.3)) <= 1e-12
+    o.advance(1, dt)
+    p.advance(1, dt)
+    assert rl2(p.download(0)[0], o.download(0)[0]) <= 1e-12
+    o.advance(case.nsteps - 1, dt)
+    p.advance(case.nsteps - 1, dt)
+    yo, so, to = o.download(0)
+    yp, sp, tp = p.download(0)
+    assert (so, to) == (sp, tp)
+    assert rl2(yp, yo) <= 1e-10
+
+
+@pytest.mark.parametrize("label", ["pulse2d_128", "curvi3d_40"])
+def test_fp32_compensated_error_vs_oracle(product_lib, oracle_lib, label):
+    case = _larger()[label]
+    o = api.Solver(oracle_lib, case)
+    dt = o.compute_dt()
+    o.advance(case.nsteps, dt)
+    p = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
+    p.advance(case.nsteps, dt)
+    err = rl2(p.download(0)[0][4], o.download(0)[0][4])
+    assert err <= 1e-5, err
