@@ -21,6 +21,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
 UNITS = {
     "lee_setup.cu": ["--fmad=false"],
     "lee_step.cu": [],
+    "lee_tma.cu": [],
     "lee_capi.cu": [],
 }
 

@@ -16,7 +16,10 @@
 #include <utility>
 #include <vector>
 
+#include <map>
+
 #include "lee_internal.h"
+#include "lee_tma.h"
 
 using namespace lee;
 
@@ -70,7 +73,29 @@ struct BlockData {
   void* dsum[kMaxVars] = {};
   void* rho_prev = nullptr;
   void* rho_next = nullptr;
+  // TMA-staged kernels (blocks without holes, 4th-order difference)
+  bool tma = false, tma_filter = false;
+  int tiles_x = 0, tiles_y = 0;
+  int stage_chunk = 0, filter_chunk = 0;
 };
+
+struct MapKey {
+  const void* p;
+  int bx, by;
+  bool operator<(const MapKey& o) const {
+    if (p != o.p) return p < o.p;
+    if (bx != o.bx) return bx < o.bx;
+    return by < o.by;
+  }
+};
+
+struct MapBytes {
+  unsigned char b[sizeof(CUtensorMap)];
+};
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 }  // namespace
 
@@ -96,6 +121,14 @@ struct lee_ctx {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, int>> ev_marks;  // (kind, event index pair start); kind 0 stage, 1 filter
   size_t ev_used = 0;
+  // TMA: tensor maps per field buffer, weight tables by closure class, device error flag
+  EncodeTiledFn encode = nullptr;
+  std::map<MapKey, MapBytes> tmaps;
+  double wst[5][5] = {};
+  double wfl[11][11] = {};
+  int hf = 0;
+  bool wst_ok = false, wfl_ok = false;
+  int* d_err = nullptr;
 };
 
 namespace {
@@ -541,6 +574,203 @@ void swap_fields(int V, void** a, void** b) {
   for (int v = 0; v < V; ++v) std::swap(a[v], b[v]);
 }
 
+// Weights of an operator by closure class for offsets -H..H (see lee_tma.h); false when a
+// nonzero coefficient falls outside the window.
+bool class_weights(const OpTable& op, int H, double* w /* [(1+2nb)][(2H+1)] */) {
+  const int W = 2 * H + 1, nb = op.nb;
+  for (int q = 0; q < (1 + 2 * nb) * W; ++q) w[q] = 0.0;
+  if (op.h > H) return false;
+  for (int o = -op.h; o <= op.h; ++o) w[0 * W + H + o] = op.c[o + op.h];
+  for (int r = 0; r < nb; ++r)
+    for (int s = 0; s < op.S; ++s) {
+      if (op.B[r][s] == 0.0) continue;
+      int ol = s - r, orr = r - s;
+      if (ol < -H || ol > H || orr < -H || orr > H) return false;
+      w[(1 + r) * W + H + ol] += op.B[r][s];
+      w[(1 + nb + r) * W + H + orr] += op.mfac * op.B[r][s];
+    }
+  return true;
+}
+
+int ensure_encoder(lee_ctx* c) {
+  if (c->encode) return LEE_OK;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+    return fail(c, LEE_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  c->encode = reinterpret_cast<EncodeTiledFn>(fn);
+  return LEE_OK;
+}
+
+// Tensor maps (box bx x by x 1) of the V fields of a buffer, cached per device pointer.
+int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int by, FieldMaps* out) {
+  int rc = ensure_encoder(c);
+  if (rc) return rc;
+  for (int v = 0; v < c->V; ++v) {
+    MapKey key{fields[v], bx, by};
+    auto it = c->tmaps.find(key);
+    if (it == c->tmaps.end()) {
+      CUtensorMap m;
+      cuuint64_t dims[3] = {(cuuint64_t)b.nx, (cuuint64_t)b.ny, (cuuint64_t)b.nz};
+      cuuint64_t strides[2] = {(cuuint64_t)b.nx * c->esz, (cuuint64_t)b.nx * b.ny * c->esz};
+      cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+      cuuint32_t es[3] = {1, 1, 1};
+      CUresult r = c->encode(&m, c->esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                             fields[v], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return fail(c, LEE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+      MapBytes mb;
+      memcpy(mb.b, &m, sizeof m);
+      it = c->tmaps.emplace(key, mb).first;
+    }
+    memcpy(&out->m[v], it->second.b, sizeof(CUtensorMap));
+  }
+  return LEE_OK;
+}
+
+int filter_box(const lee_ctx* c, int* bx, int* by) {
+  const int A = (int)(16 / c->esz);
+  const int hx = ((c->hf + A - 1) / A) * A;
+  *bx = kTileX + 2 * hx;
+  *by = kTileY + 2 * c->hf;
+  return LEE_OK;
+}
+
+template <typename T>
+int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* const* zin, int chunk_override = 0) {
+  if (!b.tma) {
+    CK(launch_stage<T>(p, c->comp ? 1 : 0, c->stream));
+    return LEE_OK;
+  }
+  TmaStageParams<T> tp;
+  memset(&tp, 0, sizeof tp);
+  tp.s = p;
+  tp.tiles_x = b.tiles_x;
+  tp.k_chunk = chunk_override ? chunk_override : b.stage_chunk;
+  for (int a = 0; a < 5; ++a)
+    for (int o = 0; o < 5; ++o) tp.w[a][o] = (T)c->wst[a][o];
+  tp.err = c->d_err;
+  FieldMaps fm;
+  int rc = field_maps(c, b, zin, Box<T, kFdHalf>::BX, Box<T, kFdHalf>::BY, &fm);
+  if (rc) return rc;
+  const int chunks = c->cfg.num_dim == 3 ? (b.nz + tp.k_chunk - 1) / tp.k_chunk : 1;
+  CK(launch_stage_tma<T>(fm, tp, c->comp ? 1 : 0, b.tiles_x * b.tiles_y, chunks, c->stream));
+  return LEE_OK;
+}
+
+// Fused filter (all directions, one read and one write of the state): in -> out.
+template <typename T>
+int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* err, void* const* out,
+                        void* const* comp_out, int chunk_override = 0) {
+  TmaFilterParams<T> fp;
+  memset(&fp, 0, sizeof fp);
+  fp.nx = b.nx; fp.ny = b.ny; fp.nz = b.nz;
+  fp.V = c->V;
+  fp.tiles_x = b.tiles_x;
+  fp.k_chunk = chunk_override ? chunk_override : b.filter_chunk;
+  for (int a = 0; a < 11; ++a)
+    for (int o = 0; o < 11; ++o) fp.w[a][o] = (T)c->wfl[a][o];
+  fp.blend = (T)c->cfg.filter_blend;
+  for (int v = 0; v < c->V; ++v) {
+    fp.err[v] = err ? (const T*)err[v] : nullptr;
+    fp.out[v] = (T*)out[v];
+    fp.comp[v] = comp_out ? (T*)comp_out[v] : nullptr;
+  }
+  fp.errflag = c->d_err;
+  int bx, by;
+  filter_box(c, &bx, &by);
+  FieldMaps fm;
+  int rc = field_maps(c, b, in, bx, by, &fm);
+  if (rc) return rc;
+  const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
+  int e0 = mark(c);
+  CK(launch_filter_tma<T>(fm, fp, c->hf, c->cfg.num_dim, c->comp ? 1 : 0, b.tiles_x * b.tiles_y, chunks, c->stream));
+  int e1 = mark(c);
+  span(c, 1, e0, e1);
+  c->stats.filter_launches += 1;
+  c->stats.kernel_launches += 1;
+  return LEE_OK;
+}
+
+int check_device_error(lee_ctx* c);
+
+// Pick the k-chunk (planes marched by one CTA) of the stage and filter kernels by timing
+// the candidates on this block: short chunks give more CTAs, long chunks re-load fewer
+// halo planes. Runs at setup on the (not yet uploaded) state buffers.
+template <typename T>
+int autotune(lee_ctx* c, BlockData& b) {
+  if (c->cfg.num_dim != 3 || (!b.tma && !b.tma_filter)) return LEE_OK;
+  const int cands[] = {8, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const bool saved = c->timing;
+  c->timing = false;
+  for (int which = 0; which < 2; ++which) {
+    if ((which == 0 && !b.tma) || (which == 1 && !b.tma_filter)) continue;
+    float best = 1e30f;
+    int best_chunk = b.nz;
+    for (int ch : cands) {
+      if (ch > b.nz) continue;
+      float tsum = 0.f;
+      for (int rep = 0; rep < 3; ++rep) {
+        CK(cudaEventRecord(e0, c->stream));
+        int rc;
+        if (which == 0) {
+          StageParams<T> p;
+          fill_stage_common<T>(c, b, p);
+          p.stage = 1;
+          p.last = 0;
+          p.h = (T)1e-3;
+          p.b = (T)(1.0 / 3.0);
+          p.a = (T)0.5;
+          for (int v = 0; v < c->V; ++v) {
+            p.zin[v] = (const T*)b.zb[0][v];
+            p.yn[v] = (const T*)b.y[v];
+            p.acc[v] = (T*)b.acc[v];
+            p.zout[v] = (T*)b.zb[1][v];
+            p.comp[v] = (T*)b.comp[v];
+          }
+          rc = launch_stage_any<T>(c, b, p, b.zb[0], ch);
+        } else {
+          rc = c->comp ? launch_filter_fused<T>(c, b, b.zb[1], b.acc, b.zb[0], b.comp, ch)
+                       : launch_filter_fused<T>(c, b, b.acc, nullptr, b.zb[0], nullptr, ch);
+        }
+        if (rc) return rc;
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0) tsum += ms;
+      }
+      if (tsum < best) {
+        best = tsum;
+        best_chunk = ch;
+      }
+    }
+    if (which == 0) b.stage_chunk = best_chunk;
+    else b.filter_chunk = best_chunk;
+  }
+  c->timing = saved;
+  c->stats = lee_stats{};
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return check_device_error(c);
+}
+
+int check_device_error(lee_ctx* c) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->d_err, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (h) {
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    return fail(c, LEE_ERR_TIMEOUT, "a bounded wait on a TMA transfer gave up (device flag %d)", h);
+  }
+  return LEE_OK;
+}
+
 template <typename T>
 int advance_impl(lee_ctx* c, int nsteps, double dt) {
   const int rk = c->cfg.rk_scheme;
@@ -582,7 +812,8 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
         }
         p.rho_prev = (const T*)b.rho_prev;
         int e0 = mark(c);
-        CK(launch_stage<T>(p, c->comp ? 1 : 0, c->stream));
+        int rc = launch_stage_any<T>(c, b, p, zin);
+        if (rc) return rc;
         int e1 = mark(c);
         span(c, 0, e0, e1);
         c->stats.stage_launches += 1;
@@ -597,7 +828,12 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
       }
       void** last_out = b.zb[(ns - 1) % 2];
       void** other = b.zb[ns % 2];
-      if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
+      if (c->cfg.filter_scheme != LEE_FILTER_NONE && b.tma_filter) {
+        // pre-filter state (FP64: acc; compensated: y_pre with its error in acc) -> y
+        int rc = c->comp ? launch_filter_fused<T>(c, b, last_out, b.acc, b.y, b.comp)
+                         : launch_filter_fused<T>(c, b, b.acc, nullptr, b.y, nullptr);
+        if (rc) return rc;
+      } else if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
         void** res = nullptr;
         int rc = c->comp ? run_filter<T>(c, b, last_out, b.acc, b.comp, other, b.y, &res)
                          : run_filter<T>(c, b, b.acc, nullptr, nullptr, last_out, other, &res);
@@ -649,14 +885,22 @@ int lee_create(const lee_config* cfg, lee_ctx** out) {
       return fail(nullptr, LEE_ERR_UNSUPPORTED, "filter scheme %d order %d", cfg->filter_scheme, cfg->filter_order);
     }
     c->fltd = minus_identity(c->flt);
+    c->hf = c->flt.h;
+    c->wfl_ok = c->hf <= 5 && class_weights(c->comp ? c->fltd : c->flt, c->hf, &c->wfl[0][0]);
   }
+  c->wst_ok = c->fd.h == kFdHalf && class_weights(c->fd, kFdHalf, &c->wst[0][0]);
   c->blk.resize((size_t)cfg->num_blocks);
   e = cudaSetDevice(cfg->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
   if (e != cudaSuccess) {
+    if (c->d_err) cudaFree(c->d_err);
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return fail(nullptr, LEE_ERR_CUDA, "stream creation failed: %s", cudaGetErrorString(e));
   }
+  c->allocs.push_back(c->d_err);
   *out = c;
   return LEE_OK;
 }
@@ -941,6 +1185,15 @@ int lee_prepare(lee_ctx* c) {
       if ((rc = alloc_fields(c, b.comp, b.N))) return rc;
       if ((rc = alloc_fields(c, b.dsum, b.N))) return rc;
     }
+    // TMA-staged kernels: no holes, the 4th-order difference, rows of 16-byte multiples
+    const bool rows16 = ((size_t)b.nx * c->esz) % 16 == 0;
+    b.tiles_x = (b.nx + kTileX - 1) / kTileX;
+    b.tiles_y = (b.ny + kTileY - 1) / kTileY;
+    b.tma = c->wst_ok && !b.has_holes && rows16 && !b.need_rho;
+    b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE;
+    b.stage_chunk = b.filter_chunk = b.nz;
+    if ((b.tma || b.tma_filter) && (rc = ensure_encoder(c))) return rc;
+    if ((rc = c->comp ? autotune<float>(c, b) : autotune<double>(c, b))) return rc;
   }
   CK(cudaStreamSynchronize(s));
   c->prepared = true;
@@ -1066,7 +1319,7 @@ int lee_advance(lee_ctx* c, int nsteps, double dt) {
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   if (rc) return rc;
-  return LEE_OK;
+  return check_device_error(c);
 }
 
 int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
@@ -1086,7 +1339,8 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
       p.zin[v] = (const double*)bk.y[v];
       p.zout[v] = (double*)bk.zb[0][v];
     }
-    CK(launch_stage<double>(p, 0, c->stream));
+    int rc = launch_stage_any<double>(c, bk, p, bk.y);
+    if (rc) return rc;
     for (int v = 0; v < c->V; ++v)
       CK(cudaMemcpyAsync(rhs[slot_of(c->V, v)], bk.zb[0][v], (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
   } else {
@@ -1098,7 +1352,8 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
       p.zin[v] = (const float*)bk.y[v];
       p.zout[v] = (float*)bk.zb[0][v];
     }
-    CK(launch_stage<float>(p, 1, c->stream));
+    int rc = launch_stage_any<float>(c, bk, p, bk.y);
+    if (rc) return rc;
     for (int v = 0; v < c->V; ++v) {
       k_to_double<float><<<grid1d(bk.N), 256, 0, c->stream>>>(bk.N, tmp, (const float*)bk.zb[0][v], nullptr);
       CK(cudaMemcpyAsync(rhs[slot_of(c->V, v)], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -1116,6 +1371,14 @@ int lee_apply_filter(lee_ctx* c) {
   if (c->cfg.filter_scheme == LEE_FILTER_NONE) return LEE_OK;
   CK(cudaSetDevice(c->cfg.device));
   for (auto& b : c->blk) {
+    if (b.tma_filter) {
+      // y (and its carried error) -> zb[0], then the buffers swap roles
+      int rc = c->comp ? launch_filter_fused<float>(c, b, b.y, b.comp, b.zb[0], b.comp)
+                       : launch_filter_fused<double>(c, b, b.y, nullptr, b.zb[0], nullptr);
+      if (rc) return rc;
+      swap_fields(c->V, b.y, b.zb[0]);
+      continue;
+    }
     void** res = nullptr;
     int rc = c->comp ? run_filter<float>(c, b, b.y, b.comp, b.comp, b.zb[0], b.zb[1], &res)
                      : run_filter<double>(c, b, b.y, nullptr, nullptr, b.zb[0], b.zb[1], &res);

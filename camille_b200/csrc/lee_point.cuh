@@ -1,0 +1,144 @@
+// Pointwise part of the fused RK stage, shared by every stage kernel: the LEE
+// right-hand side from the physical gradients (compute_RHS_linearized_Euler,
+// camille src/solver/spatial_discretization.cpp:2053-2130), the monopole source and
+// the Freund sponges (src/solver/source.cpp:10-18, :174-201), then the Runge-Kutta
+// stage update with the hole bypass (RungeKutta::integrate,
+// src/solver/temporal_discretization.cpp:205-229).
+#pragma once
+
+#include "lee_internal.h"
+
+namespace lee {
+
+template <typename T>
+__device__ __forceinline__ T cval(const Coef<T>& c, long long l) {
+  return c.p ? __ldg(c.p + l) : c.c;
+}
+
+// D[v][d]: computational-space derivative of field v along direction d; q[v]: the
+// stage input at the point. Writes the next stage input and the accumulator.
+template <typename T, int DIM, bool COMP>
+__device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l, int i, int j, int k,
+                                           const T (&D)[DIM + 2][DIM], const T (&q)[DIM + 2]) {
+  constexpr int V = DIM + 2;
+  constexpr int P = DIM + 1;
+  // physical gradients g[v][x] = sum_d JM[d][x] D_d f_v (take_derivative_xyz, :1802-1826)
+  T g[V][DIM];
+#pragma unroll
+  for (int x = 0; x < DIM; ++x) {
+    T m[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) m[d] = cval(p.jm[d * 3 + x], l);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      T s = T(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) s += m[d] * D[v][d];
+      g[v][x] = s;
+    }
+  }
+  T ub[DIM];
+#pragma unroll
+  for (int x = 0; x < DIM; ++x) ub[x] = cval(p.ubar[x], l);
+  T r[V];
+  {
+    T rs = T(0);
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) {
+      rs -= ub[x] * g[0][x];
+      if (!p.gs[x].zero) rs -= q[1 + x] * cval(p.gs[x], l);
+    }
+    r[0] = rs;
+  }
+  T rr = T(0);
+  if (p.need_rho) {
+    if (p.stage == 0 && p.rho_prev) {
+      rr = p.rho_prev[l];
+    } else {
+      rr = q[P] * p.inv_gamma * (T(1) / cval(p.pbar, l)) - q[0];
+    }
+  }
+  const T rbi = cval(p.rhobar_inv, l);
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    T ru = T(0);
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) {
+      ru -= ub[x] * g[1 + a][x];
+      const Coef<T>& gu = p.gu[a * 3 + x];
+      if (!gu.zero) ru -= (q[1 + x] + rr * ub[x]) * cval(gu, l);
+    }
+    ru -= g[P][a] * rbi;
+    r[1 + a] = ru;
+  }
+  {
+    T rp = T(0);
+    const T pb = cval(p.pbar, l);
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) {
+      rp -= ub[x] * g[P][x];
+      if (!p.gp[x].zero) rp -= q[1 + x] * cval(p.gp[x], l);
+      rp -= p.gamma * pb * g[1 + x][x];
+      const Coef<T>& gu = p.gu[x * 3 + x];
+      if (!gu.zero) rp -= p.gamma * q[P] * cval(gu, l);
+    }
+    r[P] = rp;
+  }
+  if (p.has_src && i >= p.src_lo[0] && i <= p.src_hi[0] && j >= p.src_lo[1] && j <= p.src_hi[1] &&
+      k >= p.src_lo[2] && k <= p.src_hi[2]) {
+    int b0 = p.src_hi[0] - p.src_lo[0] + 1, b1 = p.src_hi[1] - p.src_lo[1] + 1;
+    long long lb = (i - p.src_lo[0]) + (long long)b0 * ((j - p.src_lo[1]) + (long long)b1 * (k - p.src_lo[2]));
+    r[P] += p.src_amp * p.src_g[lb];
+  }
+  for (int z = 0; z < p.nzones; ++z) {
+    const Zone<T>& zn = p.zones[z];
+    if (i < zn.lo[0] || i > zn.hi[0] || j < zn.lo[1] || j > zn.hi[1] || k < zn.lo[2] || k > zn.hi[2]) continue;
+    int b0 = zn.hi[0] - zn.lo[0] + 1, b1 = zn.hi[1] - zn.lo[1] + 1;
+    long long lb = (i - zn.lo[0]) + (long long)b0 * ((j - zn.lo[1]) + (long long)b1 * (k - zn.lo[2]));
+    T sg = zn.sig[lb];
+#pragma unroll
+    for (int v = 0; v < V; ++v) r[v] += -sg * (q[v] - T(0));
+  }
+
+  if (p.stage < 0) {  // right-hand side only (spatial::compute_RHS)
+#pragma unroll
+    for (int v = 0; v < V; ++v) p.zout[v][l] = r[v];
+    return;
+  }
+  const bool hole = p.iblank && p.iblank[l] == 1;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    if (hole) {
+      p.acc[v][l] = T(0);
+      if (!p.last || COMP) p.zout[v][l] = T(0);
+      continue;
+    }
+    const T hk = r[v] * p.h;
+    if (!COMP) {
+      // y_next = y_n + sum b_i h k_i; the next stage input y_n + a h k_i
+      const T yv = p.stage == 0 ? q[v] : (p.last ? T(0) : p.yn[v][l]);
+      const T prev = p.stage == 0 ? q[v] : p.acc[v][l];
+      p.acc[v][l] = prev + p.b * hk;
+      if (!p.last) p.zout[v][l] = yv + p.a * hk;
+    } else {
+      // compensated form: acc carries the increment of y since y_n plus the carried
+      // rounding error of y; the last stage forms y_pre = y_n + increment as an exact
+      // two-float sum (y_pre in zout, its rounding error in acc)
+      const T yv = p.stage == 0 ? q[v] : p.yn[v][l];
+      const T prev = p.stage == 0 ? p.comp[v][l] : p.acc[v][l];
+      const T inc = prev + p.b * hk;
+      if (!p.last) {
+        p.acc[v][l] = inc;
+        p.zout[v][l] = yv + p.a * hk;
+      } else {
+        const T s = yv + inc;
+        const T bb = s - yv;
+        const T e = (yv - (s - bb)) + (inc - bb);
+        p.zout[v][l] = s;
+        p.acc[v][l] = e;
+      }
+    }
+  }
+}
+
+}  // namespace lee

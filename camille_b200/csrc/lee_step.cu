@@ -9,14 +9,10 @@
 #include <type_traits>
 
 #include "lee_internal.h"
+#include "lee_point.cuh"
 
 namespace lee {
 namespace {
-
-template <typename T>
-__device__ __forceinline__ T cval(const Coef<T>& c, long long l) {
-  return c.p ? __ldg(c.p + l) : c.c;
-}
 
 // Operator value at one point: the interior stencil, or a closure row selected by
 // position along the line or by the precomputed code (src/solver/spatial_discretization.cpp:1094-1149
@@ -60,137 +56,19 @@ __global__ void __launch_bounds__(256) k_stage(StageParams<T> p) {
   const int k = blockIdx.z;
   if (i >= p.nx || j >= p.ny) return;
   constexpr int V = DIM + 2;
-  constexpr int P = DIM + 1;
   const long long nxy = (long long)p.nx * p.ny;
   const long long l = i + (long long)p.nx * j + nxy * k;
   const int pos[3] = {i, j, k};
   const int nn[3] = {p.nx, p.ny, p.nz};
   const long long sd[3] = {1, p.nx, nxy};
-
-  // physical gradients g[v][x] = sum_l JM[l][x] D_l f_v  (take_derivative_xyz, :1802-1826)
-  T g[V][DIM];
+  T D[V][DIM], q[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
-    T D[DIM];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) D[d] = dop<T>(p.fd, p.zin[v], l, pos[d], nn[d], sd[d], p.code[d]);
-#pragma unroll
-    for (int x = 0; x < DIM; ++x) {
-      T s = T(0);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) s += cval(p.jm[d * 3 + x], l) * D[d];
-      g[v][x] = s;
-    }
+    for (int d = 0; d < DIM; ++d) D[v][d] = dop<T>(p.fd, p.zin[v], l, pos[d], nn[d], sd[d], p.code[d]);
+    q[v] = p.zin[v][l];
   }
-  T q[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) q[v] = p.zin[v][l];
-  T ub[DIM];
-#pragma unroll
-  for (int x = 0; x < DIM; ++x) ub[x] = cval(p.ubar[x], l);
-
-  // compute_RHS_linearized_Euler (src/solver/spatial_discretization.cpp:2053-2130)
-  T r[V];
-  {
-    T rs = T(0);
-#pragma unroll
-    for (int x = 0; x < DIM; ++x) {
-      rs -= ub[x] * g[0][x];
-      if (!p.gs[x].zero) rs -= q[1 + x] * cval(p.gs[x], l);
-    }
-    r[0] = rs;
-  }
-  T rr = T(0);
-  if (p.need_rho) {
-    if (p.stage == 0 && p.rho_prev) {
-      rr = p.rho_prev[l];
-    } else {
-      T pb = cval(p.pbar, l);
-      rr = q[P] * p.inv_gamma * (T(1) / pb) - q[0];
-    }
-  }
-  const T rbi = cval(p.rhobar_inv, l);
-#pragma unroll
-  for (int a = 0; a < DIM; ++a) {
-    T ru = T(0);
-#pragma unroll
-    for (int x = 0; x < DIM; ++x) {
-      ru -= ub[x] * g[1 + a][x];
-      const Coef<T>& gu = p.gu[a * 3 + x];
-      if (!gu.zero) ru -= (q[1 + x] + rr * ub[x]) * cval(gu, l);
-    }
-    ru -= g[P][a] * rbi;
-    r[1 + a] = ru;
-  }
-  {
-    T rp = T(0);
-    const T pb = cval(p.pbar, l);
-#pragma unroll
-    for (int x = 0; x < DIM; ++x) {
-      rp -= ub[x] * g[P][x];
-      if (!p.gp[x].zero) rp -= q[1 + x] * cval(p.gp[x], l);
-      rp -= p.gamma * pb * g[1 + x][x];
-      const Coef<T>& gu = p.gu[x * 3 + x];
-      if (!gu.zero) rp -= p.gamma * q[P] * cval(gu, l);
-    }
-    r[P] = rp;
-  }
-  // source::apply_physicalSource, then the Freund sponges (src/solver/source.cpp:10-18, :174-201)
-  if (p.has_src && i >= p.src_lo[0] && i <= p.src_hi[0] && j >= p.src_lo[1] && j <= p.src_hi[1] &&
-      k >= p.src_lo[2] && k <= p.src_hi[2]) {
-    int b0 = p.src_hi[0] - p.src_lo[0] + 1, b1 = p.src_hi[1] - p.src_lo[1] + 1;
-    long long lb = (i - p.src_lo[0]) + (long long)b0 * ((j - p.src_lo[1]) + (long long)b1 * (k - p.src_lo[2]));
-    r[P] += p.src_amp * p.src_g[lb];
-  }
-  for (int z = 0; z < p.nzones; ++z) {
-    const Zone<T>& zn = p.zones[z];
-    if (i < zn.lo[0] || i > zn.hi[0] || j < zn.lo[1] || j > zn.hi[1] || k < zn.lo[2] || k > zn.hi[2]) continue;
-    int b0 = zn.hi[0] - zn.lo[0] + 1, b1 = zn.hi[1] - zn.lo[1] + 1;
-    long long lb = (i - zn.lo[0]) + (long long)b0 * ((j - zn.lo[1]) + (long long)b1 * (k - zn.lo[2]));
-    T sg = zn.sig[lb];
-#pragma unroll
-    for (int v = 0; v < V; ++v) r[v] += -sg * (q[v] - T(0));
-  }
-
-  if (p.stage < 0) {  // right-hand side only (spatial::compute_RHS)
-#pragma unroll
-    for (int v = 0; v < V; ++v) p.zout[v][l] = r[v];
-    return;
-  }
-
-  const bool hole = p.iblank && p.iblank[l] == 1;
-  // RungeKutta::integrate stage update (src/solver/temporal_discretization.cpp:205-229)
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    if (hole) {
-      p.acc[v][l] = T(0);
-      if (!p.last || COMP) p.zout[v][l] = T(0);
-      continue;
-    }
-    const T hk = r[v] * p.h;
-    if (!COMP) {
-      const T prev = p.stage == 0 ? p.yn[v][l] : p.acc[v][l];
-      p.acc[v][l] = prev + p.b * hk;
-      if (!p.last) p.zout[v][l] = p.yn[v][l] + p.a * hk;
-    } else {
-      const T yv = p.yn[v][l];
-      // compensated form: acc carries the increment of y since y_n (plus the carried
-      // rounding error of y); the last stage forms y_pre = y_n + increment exactly
-      // as a sum of two floats (y_pre in zout, its rounding error in acc).
-      const T prev = p.stage == 0 ? p.comp[v][l] : p.acc[v][l];
-      const T inc = prev + p.b * hk;
-      if (!p.last) {
-        p.acc[v][l] = inc;
-        p.zout[v][l] = yv + p.a * hk;
-      } else {
-        const T s = yv + inc;
-        const T bb = s - yv;
-        const T e = (yv - (s - bb)) + (inc - bb);
-        p.zout[v][l] = s;
-        p.acc[v][l] = e;
-      }
-    }
-  }
+  rhs_update<T, DIM, COMP>(p, l, i, j, k, D, q);
 }
 
 // One direction of spatial::apply_filter (src/solver/spatial_discretization.cpp:2191-2246).

@@ -1,0 +1,361 @@
+// TMA-staged, k-marching kernels for blocks without holes (sm_100a).
+//
+// Stage kernel: a CTA owns a 32 x 8 tile in (i, j) and marches along k through a
+// chunk of planes. Each plane of every state field arrives in shared memory as one
+// box (tile plus stencil halo) through cp.async.bulk.tensor, completing on an
+// mbarrier; a ring of 2h+2 planes holds the zeta stencil and one plane of prefetch,
+// so HBM loads for plane k+h+1 overlap the arithmetic of plane k. Every point then
+// takes its xi/eta/zeta derivatives from shared memory and runs the pointwise RHS and
+// RK update (lee_point.cuh) with coalesced loads/stores of y_n, the accumulator and
+// the coefficient fields.
+//
+// Filter kernel: the dimension-split filter of spatial::apply_filter
+// (src/solver/spatial_discretization.cpp:2191-2246) fused into one pass per field:
+// for each incoming plane, F_xi on the tile plus its eta halo (into shared memory),
+// F_eta at the tile points, and a register queue of 2h+1 planes for F_zeta, so the
+// pre-filter state is read once and the filtered state written once.
+//
+// Every mbarrier wait is bounded (about one second of %globaltimer); on expiry the
+// CTA records the failure in a device flag, waits (bounded) for its own copies in
+// flight and returns, and the host reports LEE_ERR_TIMEOUT.
+#include "lee_point.cuh"
+#include "lee_tma.h"
+
+namespace lee {
+namespace {
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned n) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ unsigned mbar_try(uint64_t* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok;
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for the phase of the given parity; false after about one second.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+  if (mbar_try(b, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try(b, parity)) return true;
+    if ((it & 63u) == 0u && gtimer() - t0 > 1000000000ull) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Closure class of a position along a line with nb closure rows at each end:
+// 0 interior, 1 + p for the left rows, 1 + nb + (n - 1 - p) for the right rows.
+__device__ __forceinline__ int cls_of(int pos, int n, int nb) {
+  return pos < nb ? 1 + pos : (pos > n - 1 - nb ? 1 + nb + (n - 1 - pos) : 0);
+}
+
+template <typename T, int DIM, bool COMP>
+__global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ FieldMaps zm,
+                                                   const __grid_constant__ TmaStageParams<T> P) {
+  constexpr int H = kFdHalf, TX = kTileX, TY = kTileY, V = DIM + 2;
+  constexpr int HX = Box<T, H>::HX, BX = Box<T, H>::BX, BY = Box<T, H>::BY;
+  constexpr int NS = DIM == 3 ? 2 * H + 2 : 1;
+  constexpr int FB = BY * BX;  // elements of one field box
+  constexpr int PLANE = V * FB;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T* ring = reinterpret_cast<T*>(smem);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + sizeof(T) * NS * PLANE);
+
+  const StageParams<T>& s = P.s;
+  const int i0 = (int)(blockIdx.x % P.tiles_x) * TX, j0 = (int)(blockIdx.x / P.tiles_x) * TY;
+  const int k0 = DIM == 3 ? (int)blockIdx.y * P.k_chunk : 0;
+  const int k1 = DIM == 3 ? min(s.nz, k0 + P.k_chunk) : 1;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool active = i < s.nx && j < s.ny;
+  const int plo = DIM == 3 ? max(0, k0 - H) : 0;
+  const int phi = DIM == 3 ? min(s.nz - 1, k1 - 1 + H) : 0;
+
+  if (tid == 0) {
+    for (int q = 0; q < NS; ++q) mbar_init(&bar[q], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int next_issue = plo;  // meaningful in thread 0 only
+  auto issue_upto = [&](int last) {
+    for (; next_issue <= min(phi, last); ++next_issue) {
+      const int rel = next_issue - plo, slot = rel % NS;
+      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * PLANE));
+      for (int v = 0; v < V; ++v)
+        tma_load_3d(ring + slot * PLANE + v * FB, &zm.m[v], i0 - HX, j0 - H, next_issue, &bar[slot]);
+    }
+  };
+  if (tid == 0) issue_upto(plo + NS - 1);
+
+  const int c = (ty + H) * BX + (tx + HX);
+  const int cx = active ? cls_of(i, s.nx, H) : 0;
+  const int cy = active ? cls_of(j, s.ny, H) : 0;
+  int waited = plo;
+  for (int k = k0; k < k1; ++k) {
+    bool failed = false;
+    const int need = DIM == 3 ? min(phi, k + H) : 0;
+    for (; waited <= need; ++waited) {
+      const int rel = waited - plo;
+      if (!mbar_wait(&bar[rel % NS], (unsigned)((rel / NS) & 1))) failed = true;
+    }
+    if (__syncthreads_or(failed)) {
+      if (tid == 0) {
+        atomicExch(P.err, 1);
+        for (int w = waited; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NS], (unsigned)(((w - plo) / NS) & 1));
+      }
+      return;
+    }
+    if (active) {
+      const T* pk = ring + ((k - plo) % NS) * PLANE;
+      const int cz = DIM == 3 ? cls_of(k, s.nz, H) : 0;
+      T D[V][DIM], q[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const T* f = pk + v * FB + c;
+        q[v] = f[0];
+        T dx = T(0), dy = T(0);
+#pragma unroll
+        for (int o = -H; o <= H; ++o) {
+          dx += P.w[cx][o + H] * f[o];
+          dy += P.w[cy][o + H] * f[o * BX];
+        }
+        D[v][0] = dx;
+        D[v][1] = dy;
+        if (DIM == 3) {
+          T dz = T(0);
+#pragma unroll
+          for (int o = -H; o <= H; ++o) {
+            const int kk = k + o;
+            if (kk >= plo && kk <= phi) dz += P.w[cz][o + H] * ring[((kk - plo) % NS) * PLANE + v * FB + c];
+          }
+          D[v][DIM - 1] = dz;
+        }
+      }
+      const long long l = i + (long long)s.nx * (j + (long long)s.ny * k);
+      rhs_update<T, DIM, COMP>(s, l, i, j, k, D, q);
+    }
+    __syncthreads();
+    if (DIM == 3 && tid == 0) issue_upto(k + 1 - H + NS - 1);
+  }
+}
+
+template <typename T, int DIM, bool COMP, int HF>
+__global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ FieldMaps ym,
+                                                    const __grid_constant__ TmaFilterParams<T> P) {
+  constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = 2;
+  constexpr int HX = Box<T, HF>::HX, BX = Box<T, HF>::BX, BY = Box<T, HF>::BY;
+  constexpr int FB = BY * BX;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T* ring = reinterpret_cast<T*>(smem);
+  T* u1 = ring + NSF * FB;  // [BY][TX]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(u1 + BY * TX);
+
+  const int v = blockIdx.z;
+  const int i0 = (int)(blockIdx.x % P.tiles_x) * TX, j0 = (int)(blockIdx.x / P.tiles_x) * TY;
+  const int k0 = DIM == 3 ? (int)blockIdx.y * P.k_chunk : 0;
+  const int k1 = DIM == 3 ? min(P.nz, k0 + P.k_chunk) : 1;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool active = i < P.nx && j < P.ny;
+  const int plo = DIM == 3 ? max(0, k0 - HF) : 0;
+  const int phi = DIM == 3 ? min(P.nz - 1, k1 - 1 + HF) : 0;
+
+  if (tid == 0) {
+    for (int q = 0; q < NSF; ++q) mbar_init(&bar[q], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int next_issue = plo;
+  auto issue_upto = [&](int last) {
+    for (; next_issue <= min(phi, last); ++next_issue) {
+      const int slot = (next_issue - plo) % NSF;
+      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * FB));
+      tma_load_3d(ring + slot * FB, &ym.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
+    }
+  };
+  if (tid == 0) issue_upto(plo + NSF - 1);
+
+  const int cx = cls_of(min(i, P.nx - 1), P.nx, HF);
+  const int cy = cls_of(min(j, P.ny - 1), P.ny, HF);
+  T uq[NQ], dq[HF + 1], xq[HF + 1];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) uq[q] = T(0);
+#pragma unroll
+  for (int q = 0; q <= HF; ++q) dq[q] = xq[q] = T(0);
+  const int pstart = DIM == 3 ? k0 - HF : 0, pend = DIM == 3 ? k1 - 1 + HF : 0;
+  for (int p = pstart; p <= pend; ++p) {
+    T u2 = T(0), d12 = T(0), xc = T(0);
+    if (p >= plo && p <= phi) {
+      const int rel = p - plo;
+      const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1));
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(P.errflag, 1);
+          for (int w = p + 1; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NSF], (unsigned)(((w - plo) / NSF) & 1));
+        }
+        return;
+      }
+      const T* box = ring + (rel % NSF) * FB;
+      for (int r = ty; r < BY; r += TY) {  // F_xi on the tile and its eta halo
+        const T* f = box + r * BX + tx + HX;
+        T d = T(0);
+#pragma unroll
+        for (int o = -HF; o <= HF; ++o) d += P.w[cx][o + HF] * f[o];
+        u1[r * TX + tx] = COMP ? f[0] + d : d;
+      }
+      __syncthreads();
+      const T* fc = box + (ty + HF) * BX + tx + HX;
+      xc = fc[0];
+      T dy = T(0);
+#pragma unroll
+      for (int o = -HF; o <= HF; ++o) dy += P.w[cy][o + HF] * u1[(ty + HF + o) * TX + tx];
+      if (COMP) {
+        T d1 = T(0);
+#pragma unroll
+        for (int o = -HF; o <= HF; ++o) d1 += P.w[cx][o + HF] * fc[o];
+        u2 = u1[(ty + HF) * TX + tx] + dy;
+        d12 = d1 + dy;
+      } else {
+        u2 = dy;
+      }
+      __syncthreads();
+      if (tid == 0) issue_upto(p + NSF);
+    }
+#pragma unroll
+    for (int q = 0; q < NQ - 1; ++q) uq[q] = uq[q + 1];
+    uq[NQ - 1] = u2;
+#pragma unroll
+    for (int q = 0; q < HF; ++q) {
+      dq[q] = dq[q + 1];
+      xq[q] = xq[q + 1];
+    }
+    dq[HF] = d12;
+    xq[HF] = xc;
+    const int k = DIM == 3 ? p - HF : 0;
+    if (!active || k < k0 || k >= k1) continue;
+    T fz, x0, dsum;
+    if (DIM == 3) {
+      const int cz = cls_of(k, P.nz, HF);
+      fz = T(0);
+#pragma unroll
+      for (int o = -HF; o <= HF; ++o) fz += P.w[cz][o + HF] * uq[o + HF];
+      x0 = xq[0];
+      dsum = dq[0];
+    } else {
+      fz = u2;
+      x0 = xc;
+      dsum = d12;
+    }
+    const long long l = i + (long long)P.nx * (j + (long long)P.ny * k);
+    if (!COMP) {
+      P.out[v][l] = (T(1) - P.blend) * x0 + P.blend * fz;
+    } else {
+      const T D = DIM == 3 ? dsum + fz : dsum;
+      const T t = P.blend * D + P.err[v][l];
+      const T sm = x0 + t;
+      const T bb = sm - x0;
+      P.out[v][l] = sm;
+      P.comp[v][l] = (x0 - (sm - bb)) + (t - bb);
+    }
+  }
+}
+
+template <typename T, int DIM, bool COMP>
+size_t stage_smem() {
+  constexpr int NS = DIM == 3 ? 2 * kFdHalf + 2 : 1;
+  return sizeof(T) * NS * (DIM + 2) * Box<T, kFdHalf>::BY * Box<T, kFdHalf>::BX + NS * sizeof(uint64_t);
+}
+
+template <typename T, int HF>
+size_t filter_smem() {
+  return sizeof(T) * (2 * Box<T, HF>::BY * Box<T, HF>::BX + Box<T, HF>::BY * kTileX) + 2 * sizeof(uint64_t);
+}
+
+template <typename T, int DIM, bool COMP>
+cudaError_t go_stage(const FieldMaps& z, const TmaStageParams<T>& p, int tiles, int chunks, cudaStream_t s) {
+  static bool attr = false;
+  const size_t sm = stage_smem<T, DIM, COMP>();
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_stage_tma<T, DIM, COMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_stage_tma<T, DIM, COMP><<<dim3(tiles, chunks), 256, sm, s>>>(z, p);
+  return cudaGetLastError();
+}
+
+template <typename T, int DIM, bool COMP, int HF>
+cudaError_t go_filter(const FieldMaps& in, const TmaFilterParams<T>& p, int tiles, int chunks, cudaStream_t s) {
+  const size_t sm = filter_smem<T, HF>();
+  k_filter_tma<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, sm, s>>>(in, p);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t stage_tma_smem(int dim, size_t esz) {
+  if (esz == 8) return dim == 3 ? stage_smem<double, 3, false>() : stage_smem<double, 2, false>();
+  return dim == 3 ? stage_smem<float, 3, true>() : stage_smem<float, 2, true>();
+}
+
+template <typename T>
+cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int comp, int tiles, int chunks,
+                             cudaStream_t s) {
+  if (p.s.dim == 2) return comp ? go_stage<T, 2, true>(zin, p, tiles, 1, s) : go_stage<T, 2, false>(zin, p, tiles, 1, s);
+  return comp ? go_stage<T, 3, true>(zin, p, tiles, chunks, s) : go_stage<T, 3, false>(zin, p, tiles, chunks, s);
+}
+
+template <typename T>
+cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
+                              int chunks, cudaStream_t s) {
+#define LEE_FILTER_CASE(HF)                                                                     \
+  if (hf == HF) {                                                                               \
+    if (dim == 2)                                                                               \
+      return comp ? go_filter<T, 2, true, HF>(in, p, tiles, 1, s) : go_filter<T, 2, false, HF>(in, p, tiles, 1, s); \
+    return comp ? go_filter<T, 3, true, HF>(in, p, tiles, chunks, s)                            \
+                : go_filter<T, 3, false, HF>(in, p, tiles, chunks, s);                          \
+  }
+  LEE_FILTER_CASE(2)
+  LEE_FILTER_CASE(4)
+  LEE_FILTER_CASE(5)
+#undef LEE_FILTER_CASE
+  return cudaErrorInvalidValue;
+}
+
+template cudaError_t launch_stage_tma<double>(const FieldMaps&, const TmaStageParams<double>&, int, int, int, cudaStream_t);
+template cudaError_t launch_stage_tma<float>(const FieldMaps&, const TmaStageParams<float>&, int, int, int, cudaStream_t);
+template cudaError_t launch_filter_tma<double>(const FieldMaps&, const TmaFilterParams<double>&, int, int, int, int, int,
+                                               cudaStream_t);
+template cudaError_t launch_filter_tma<float>(const FieldMaps&, const TmaFilterParams<float>&, int, int, int, int, int,
+                                              cudaStream_t);
+
+}  // namespace lee

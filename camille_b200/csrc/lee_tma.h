@@ -1,0 +1,59 @@
+// TMA-staged stage and filter kernels (lee_tma.cu): declarations shared with the host.
+#pragma once
+
+#include <cuda.h>
+
+#include "lee_internal.h"
+
+namespace lee {
+
+constexpr int kTileX = 32;  // points along i per CTA (one warp row)
+constexpr int kTileY = 8;   // points along j per CTA
+constexpr int kFdHalf = 2;  // the TMA stage kernel handles the 4th-order difference
+
+// One tensor map per state field of a buffer (passed as a __grid_constant__ parameter).
+struct __align__(64) FieldMaps {
+  CUtensorMap m[kMaxVars];
+};
+
+template <typename T>
+struct TmaStageParams {
+  StageParams<T> s;
+  int tiles_x, k_chunk;
+  // derivative weights by closure class: 0 interior, 1..2 left rows, 3..4 right rows;
+  // offsets -2..2 from the point (the reference's stencil tables rewritten per class)
+  T w[5][5];
+  int* err;  // set when a bounded wait gives up
+};
+
+template <typename T>
+struct TmaFilterParams {
+  int nx, ny, nz, V, tiles_x, k_chunk;
+  // filter weights by class (interior, left rows, right rows), offsets -hf..hf; the
+  // compensated form uses F - I
+  T w[11][11];
+  T blend;
+  const T* err[kMaxVars];  // compensated: rounding error of the pre-filter state
+  T* out[kMaxVars];
+  T* comp[kMaxVars];
+  int* errflag;
+};
+
+// Shared-memory box geometry: halo along i rounded up so every TMA row starts on 16 bytes.
+template <typename T, int H>
+struct Box {
+  static constexpr int A = (int)(16 / sizeof(T));
+  static constexpr int HX = ((H + A - 1) / A) * A;
+  static constexpr int BX = kTileX + 2 * HX;
+  static constexpr int BY = kTileY + 2 * H;
+};
+
+size_t stage_tma_smem(int dim, size_t esz);
+template <typename T>
+cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int comp, int tiles, int chunks,
+                             cudaStream_t s);
+template <typename T>
+cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
+                              int chunks, cudaStream_t s);
+
+}  // namespace lee
