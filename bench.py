@@ -103,10 +103,13 @@ def stage_bytes_per_point(info, comp: bool) -> float:
 
 
 def step_bytes_per_point(info, comp: bool, dim: int) -> float:
-    """Algorithmic bytes per grid point per RK4 step: four stages and the filter passes
-    (FP64: read+write per pass plus the blend input; compensated: the increment sums)."""
+    """Algorithmic bytes per grid point per RK4 step: four stages and the filter. The fused
+    filter reads the pre-filter state once and writes the filtered state once (FP64: 2 V
+    words; compensated: y_pre and its rounding error in, y and its error out, 4 V words)."""
     V, e = info.state_vars, info.bytes_per_value
-    if comp:
+    if info.tma_filter:
+        filt = 4 if comp else 2
+    elif comp:
         filt = {2: 3 + 6, 3: 3 + 4 + 6}[dim]
     else:
         filt = {2: 2 + 3, 3: 2 + 2 + 3}[dim]
@@ -231,7 +234,9 @@ def run_ours(args) -> None:
                          "avg_launch_ms": stage_avg_ms, "dominant": dominant,
                          "filter_avg_launch_ms": filt_avg_ms,
                          "step_gbs": step_gbs, "step_frac": step_gbs / peak,
-                         "step_bytes_per_point": step_bytes_per_point(info, True, 3)},
+                         "step_bytes_per_point": step_bytes_per_point(info, True, 3),
+                         "tma_stage": info.tma_stage, "tma_filter": info.tma_filter,
+                         "stage_chunk": info.stage_chunk, "filter_chunk": info.filter_chunk},
             "e2e": {"value": world * npts * K / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K,
                     "note": "lee_upload_state from pinned host memory, lee_advance(K), lee_download_state"},

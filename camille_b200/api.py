@@ -43,7 +43,9 @@ class LeeConfig(C.Structure):
 
 class LeeInfo(C.Structure):
     _fields_ = [("points", C.c_longlong), ("state_vars", C.c_int), ("bytes_per_value", C.c_int),
-                ("num_coef_fields", C.c_int), ("device_bytes", C.c_longlong)]
+                ("num_coef_fields", C.c_int), ("device_bytes", C.c_longlong),
+                ("tma_stage", C.c_int), ("tma_filter", C.c_int), ("stage_chunk", C.c_int),
+                ("filter_chunk", C.c_int)]
 
 
 class LeeStats(C.Structure):

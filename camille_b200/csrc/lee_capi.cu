@@ -576,18 +576,19 @@ void swap_fields(int V, void** a, void** b) {
 
 // Weights of an operator by closure class for offsets -H..H (see lee_tma.h); false when a
 // nonzero coefficient falls outside the window.
-bool class_weights(const OpTable& op, int H, double* w /* [(1+2nb)][(2H+1)] */) {
-  const int W = 2 * H + 1, nb = op.nb;
-  for (int q = 0; q < (1 + 2 * nb) * W; ++q) w[q] = 0.0;
-  if (op.h > H) return false;
-  for (int o = -op.h; o <= op.h; ++o) w[0 * W + H + o] = op.c[o + op.h];
+// `stride` is the row length of the destination table (>= 2H+1).
+bool class_weights(const OpTable& op, int H, double* w, int stride) {
+  const int nb = op.nb;
+  for (int q = 0; q < (1 + 2 * nb) * stride; ++q) w[q] = 0.0;
+  if (op.h > H || 2 * H + 1 > stride) return false;
+  for (int o = -op.h; o <= op.h; ++o) w[0 * stride + H + o] = op.c[o + op.h];
   for (int r = 0; r < nb; ++r)
     for (int s = 0; s < op.S; ++s) {
       if (op.B[r][s] == 0.0) continue;
       int ol = s - r, orr = r - s;
       if (ol < -H || ol > H || orr < -H || orr > H) return false;
-      w[(1 + r) * W + H + ol] += op.B[r][s];
-      w[(1 + nb + r) * W + H + orr] += op.mfac * op.B[r][s];
+      w[(1 + r) * stride + H + ol] += op.B[r][s];
+      w[(1 + nb + r) * stride + H + orr] += op.mfac * op.B[r][s];
     }
   return true;
 }
@@ -886,9 +887,9 @@ int lee_create(const lee_config* cfg, lee_ctx** out) {
     }
     c->fltd = minus_identity(c->flt);
     c->hf = c->flt.h;
-    c->wfl_ok = c->hf <= 5 && class_weights(c->comp ? c->fltd : c->flt, c->hf, &c->wfl[0][0]);
+    c->wfl_ok = c->hf <= 5 && class_weights(c->comp ? c->fltd : c->flt, c->hf, &c->wfl[0][0], 11);
   }
-  c->wst_ok = c->fd.h == kFdHalf && class_weights(c->fd, kFdHalf, &c->wst[0][0]);
+  c->wst_ok = c->fd.h == kFdHalf && class_weights(c->fd, kFdHalf, &c->wst[0][0], 5);
   c->blk.resize((size_t)cfg->num_blocks);
   e = cudaSetDevice(cfg->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
@@ -1400,6 +1401,14 @@ int lee_get_info(lee_ctx* c, lee_info* info) {
   info->state_vars = c->V;
   info->bytes_per_value = (int)c->esz;
   info->device_bytes = c->device_bytes;
+  info->tma_stage = 1;
+  info->tma_filter = c->cfg.filter_scheme != LEE_FILTER_NONE ? 1 : 0;
+  for (auto& b : c->blk) {
+    info->tma_stage &= b.tma ? 1 : 0;
+    info->tma_filter &= b.tma_filter ? 1 : 0;
+  }
+  info->stage_chunk = c->blk.empty() ? 0 : c->blk[0].stage_chunk;
+  info->filter_chunk = c->blk.empty() ? 0 : c->blk[0].filter_chunk;
   return LEE_OK;
 }
 

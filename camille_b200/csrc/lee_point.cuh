@@ -15,25 +15,49 @@ __device__ __forceinline__ T cval(const Coef<T>& c, long long l) {
   return c.p ? __ldg(c.p + l) : c.c;
 }
 
+// Per-point inputs read from global memory, gathered before the arithmetic so that
+// every load of the point is in flight at once.
+template <typename T, int DIM>
+struct PointIn {
+  T jm[DIM][DIM];     // J * metrics[d][x]
+  T yn[DIM + 2];      // y_n (stages after the first)
+  T av[DIM + 2];      // accumulator (stages after the first) or carried error (compensated, first stage)
+};
+
+template <typename T, int DIM, bool COMP>
+__device__ __forceinline__ void gather(const StageParams<T>& p, long long l, PointIn<T, DIM>& in) {
+  constexpr int V = DIM + 2;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) in.jm[d][x] = cval(p.jm[d * 3 + x], l);
+  const bool need_yn = p.stage > 0 && (COMP || !p.last);
+  const bool need_av = p.stage > 0 || (COMP && p.stage == 0);
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    in.yn[v] = need_yn ? p.yn[v][l] : T(0);
+    in.av[v] = need_av ? (p.stage == 0 ? p.comp[v][l] : p.acc[v][l]) : T(0);
+  }
+}
+
 // D[v][d]: computational-space derivative of field v along direction d; q[v]: the
-// stage input at the point. Writes the next stage input and the accumulator.
+// stage input at the point; in: the gathered inputs. Writes the next stage input and
+// the accumulator.
 template <typename T, int DIM, bool COMP>
 __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l, int i, int j, int k,
-                                           const T (&D)[DIM + 2][DIM], const T (&q)[DIM + 2]) {
+                                           const T (&D)[DIM + 2][DIM], const T (&q)[DIM + 2],
+                                           const PointIn<T, DIM>& in) {
   constexpr int V = DIM + 2;
   constexpr int P = DIM + 1;
   // physical gradients g[v][x] = sum_d JM[d][x] D_d f_v (take_derivative_xyz, :1802-1826)
   T g[V][DIM];
 #pragma unroll
   for (int x = 0; x < DIM; ++x) {
-    T m[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) m[d] = cval(p.jm[d * 3 + x], l);
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       T s = T(0);
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) s += m[d] * D[v][d];
+      for (int d = 0; d < DIM; ++d) s += in.jm[d][x] * D[v][d];
       g[v][x] = s;
     }
   }
@@ -116,17 +140,16 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l,
     const T hk = r[v] * p.h;
     if (!COMP) {
       // y_next = y_n + sum b_i h k_i; the next stage input y_n + a h k_i
-      const T yv = p.stage == 0 ? q[v] : (p.last ? T(0) : p.yn[v][l]);
-      const T prev = p.stage == 0 ? q[v] : p.acc[v][l];
+      const T yv = p.stage == 0 ? q[v] : in.yn[v];
+      const T prev = p.stage == 0 ? q[v] : in.av[v];
       p.acc[v][l] = prev + p.b * hk;
       if (!p.last) p.zout[v][l] = yv + p.a * hk;
     } else {
       // compensated form: acc carries the increment of y since y_n plus the carried
       // rounding error of y; the last stage forms y_pre = y_n + increment as an exact
       // two-float sum (y_pre in zout, its rounding error in acc)
-      const T yv = p.stage == 0 ? q[v] : p.yn[v][l];
-      const T prev = p.stage == 0 ? p.comp[v][l] : p.acc[v][l];
-      const T inc = prev + p.b * hk;
+      const T yv = p.stage == 0 ? q[v] : in.yn[v];
+      const T inc = in.av[v] + p.b * hk;
       if (!p.last) {
         p.acc[v][l] = inc;
         p.zout[v][l] = yv + p.a * hk;

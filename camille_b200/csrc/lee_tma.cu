@@ -121,6 +121,10 @@ __global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ Field
   const int cy = active ? cls_of(j, s.ny, H) : 0;
   int waited = plo;
   for (int k = k0; k < k1; ++k) {
+    // pointwise inputs of this plane: issued before the wait so their latency overlaps it
+    const long long l = i + (long long)s.nx * (j + (long long)s.ny * k);
+    PointIn<T, DIM> in;
+    if (active) gather<T, DIM, COMP>(s, l, in);
     bool failed = false;
     const int need = DIM == 3 ? min(phi, k + H) : 0;
     for (; waited <= need; ++waited) {
@@ -160,8 +164,7 @@ __global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ Field
           D[v][DIM - 1] = dz;
         }
       }
-      const long long l = i + (long long)s.nx * (j + (long long)s.ny * k);
-      rhs_update<T, DIM, COMP>(s, l, i, j, k, D, q);
+      rhs_update<T, DIM, COMP>(s, l, i, j, k, D, q, in);
     }
     __syncthreads();
     if (DIM == 3 && tid == 0) issue_upto(k + 1 - H + NS - 1);
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ Field
 template <typename T, int DIM, bool COMP, int HF>
 __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ FieldMaps ym,
                                                     const __grid_constant__ TmaFilterParams<T> P) {
-  constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = 2;
+  constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = kFilterSlots;
   constexpr int HX = Box<T, HF>::HX, BX = Box<T, HF>::BX, BY = Box<T, HF>::BY;
   constexpr int FB = BY * BX;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -214,6 +217,10 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
   const int pstart = DIM == 3 ? k0 - HF : 0, pend = DIM == 3 ? k1 - 1 + HF : 0;
   for (int p = pstart; p <= pend; ++p) {
     T u2 = T(0), d12 = T(0), xc = T(0);
+    const int kf = DIM == 3 ? p - HF : 0;  // the plane finalized at the end of this iteration
+    const bool fin = active && kf >= k0 && kf < k1;
+    const long long lf = i + (long long)P.nx * (j + (long long)P.ny * kf);
+    const T ef = (COMP && fin) ? P.err[v][lf] : T(0);
     if (p >= plo && p <= phi) {
       const int rel = p - plo;
       const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1));
@@ -260,8 +267,8 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
     }
     dq[HF] = d12;
     xq[HF] = xc;
-    const int k = DIM == 3 ? p - HF : 0;
-    if (!active || k < k0 || k >= k1) continue;
+    const int k = kf;
+    if (!fin) continue;
     T fz, x0, dsum;
     if (DIM == 3) {
       const int cz = cls_of(k, P.nz, HF);
@@ -275,12 +282,12 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
       x0 = xc;
       dsum = d12;
     }
-    const long long l = i + (long long)P.nx * (j + (long long)P.ny * k);
+    const long long l = lf;
     if (!COMP) {
       P.out[v][l] = (T(1) - P.blend) * x0 + P.blend * fz;
     } else {
       const T D = DIM == 3 ? dsum + fz : dsum;
-      const T t = P.blend * D + P.err[v][l];
+      const T t = P.blend * D + ef;
       const T sm = x0 + t;
       const T bb = sm - x0;
       P.out[v][l] = sm;
@@ -297,7 +304,8 @@ size_t stage_smem() {
 
 template <typename T, int HF>
 size_t filter_smem() {
-  return sizeof(T) * (2 * Box<T, HF>::BY * Box<T, HF>::BX + Box<T, HF>::BY * kTileX) + 2 * sizeof(uint64_t);
+  return sizeof(T) * (kFilterSlots * Box<T, HF>::BY * Box<T, HF>::BX + Box<T, HF>::BY * kTileX) +
+         kFilterSlots * sizeof(uint64_t);
 }
 
 template <typename T, int DIM, bool COMP>

@@ -10,6 +10,7 @@ namespace lee {
 constexpr int kTileX = 32;  // points along i per CTA (one warp row)
 constexpr int kTileY = 8;   // points along j per CTA
 constexpr int kFdHalf = 2;  // the TMA stage kernel handles the 4th-order difference
+constexpr int kFilterSlots = 4;  // planes in the filter kernel's ring (three in flight)
 
 // One tensor map per state field of a buffer (passed as a __grid_constant__ parameter).
 struct __align__(64) FieldMaps {

@@ -157,6 +157,10 @@ typedef struct {
   int num_coef_fields;       /* per-point coefficient fields read by every stage; uniform
                                 fields are folded into kernel constants at setup */
   long long device_bytes;    /* device memory held by the context */
+  int tma_stage;             /* 1 when every block runs the TMA-staged stage kernel */
+  int tma_filter;            /* 1 when every block runs the fused TMA-staged filter */
+  int stage_chunk;           /* planes marched per CTA by the stage kernel (autotuned; block 0) */
+  int filter_chunk;          /* planes marched per CTA by the filter kernel (autotuned; block 0) */
 } lee_info;
 int lee_get_info(lee_ctx *ctx, lee_info *info);
 
