@@ -150,8 +150,12 @@ class Solver:
             for bd in case.boundaries:
                 lo = (C.c_int * 3)(*bd.lo)
                 hi = (C.c_int * 3)(*bd.hi)
+                sig = None
+                if bd.sigma is not None:
+                    sarr = np.ascontiguousarray(bd.sigma, np.float64)
+                    sig = _dptr(sarr)
                 self._chk(lib.add_boundary(self.ctx, bd.block, _cases.BC_TYPES[bd.kind], bd.dir, bd.end,
-                                           lo, hi, None))
+                                           lo, hi, sig))
             if case.monopole is not None:
                 p = np.array(case.monopole, np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))

@@ -68,6 +68,7 @@ class Boundary:
     end: int       # 0 left (+dir), 1 right (-dir)
     lo: tuple[int, int, int]
     hi: tuple[int, int, int]
+    sigma: Optional[np.ndarray] = None  # sponge strengths over the box (i fastest), when precomputed
 
     def line(self) -> str:
         sign = "+" if self.end == 0 else "-"
@@ -211,7 +212,7 @@ def curvi3d_grid(n: int, amp: float = 0.1) -> tuple[np.ndarray, np.ndarray, np.n
 
 
 def curvi3d(n: int = 256, seed: int = 2, npulses: int = 8, mach: float = 0.5, nsteps: int = 500,
-            gamma: float = 1.4, halfwidth: float = 4.0) -> Case:
+            gamma: float = 1.4, halfwidth: float = 4.0, sponge: int = 0, sponge_constant: float = 1.0) -> Case:
     x, y, z = curvi3d_grid(n)
     mean = np.zeros((5,) + x.shape)
     mean[1] = mach
@@ -224,5 +225,42 @@ def curvi3d(n: int = 256, seed: int = 2, npulses: int = 8, mach: float = 0.5, ns
     state = np.zeros((5,) + x.shape)
     state[4] = p
     blk = Block(x, y, z, mean, state)
-    return Case(name=f"curvi3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps,
-                notes=f"3-D {n}^3 curvilinear, Mach {mach} along x, {npulses} pulses seed {seed}")
+    bnd = sponge_frame(3, blk.dims, sponge) if sponge > 0 else []
+    return Case(name=f"curvi3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
+                sponge_constant=sponge_constant,
+                notes=f"3-D {n}^3 curvilinear, Mach {mach} along x, {npulses} pulses seed {seed}, "
+                      f"sponge {sponge} (constant {sponge_constant})")
+
+
+def sponge_sigma(case: Case, bd: Boundary) -> np.ndarray:
+    """Freund sponge strengths of one zone, C (d_in / (d_in + d_out))^order, where d_in/d_out are
+    the distances to the nearest grid point of the zone's inner/outer face
+    (Geometry::additionalInit_bufferZones, src/geometry/geometry.cpp:1028-1142). The reference
+    searches every face point for every zone point; an exact nearest-neighbour search over the
+    same points gives the same minimum distance in O(N log N)."""
+    from scipy.spatial import cKDTree
+
+    blk = case.blocks[bd.block]
+    xyz = np.stack([blk.x, blk.y, blk.z], axis=-1)  # (nz, ny, nx, 3)
+    sl = tuple(slice(bd.lo[d], bd.hi[d] + 1) for d in (2, 1, 0))
+    pts = xyz[sl].reshape(-1, 3)
+    ax = 2 - bd.dir  # numpy axis of the zone's direction
+
+    def face(index: int) -> np.ndarray:
+        f = list(sl)
+        f[ax] = slice(index, index + 1)
+        return xyz[tuple(f)].reshape(-1, 3)
+
+    f_in = face(bd.hi[bd.dir] if bd.end == 0 else bd.lo[bd.dir])
+    f_out = face(bd.lo[bd.dir] if bd.end == 0 else bd.hi[bd.dir])
+    d_in = cKDTree(f_in).query(pts)[0]
+    d_out = cKDTree(f_out).query(pts)[0]
+    rel = d_in / (d_in + d_out)
+    return (case.sponge_constant * rel ** case.sponge_order).astype(np.float64)
+
+
+def precompute_sponges(case: Case) -> None:
+    """Fill Boundary.sigma for every sponge of the case (used for large blocks)."""
+    for bd in case.boundaries:
+        if bd.kind == "sponge_freund_ambient" and bd.sigma is None:
+            bd.sigma = sponge_sigma(case, bd)

@@ -79,13 +79,14 @@ __device__ __forceinline__ int cls_of(int pos, int n, int nb) {
 }
 
 template <typename T, int DIM, bool COMP>
-__global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ FieldMaps zm,
-                                                   const __grid_constant__ TmaStageParams<T> P) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
+    k_stage_tma(const __grid_constant__ FieldMaps zm, const __grid_constant__ TmaStageParams<T> P) {
   constexpr int H = kFdHalf, TX = kTileX, TY = kTileY, V = DIM + 2;
-  constexpr int HX = Box<T, H>::HX, BX = Box<T, H>::BX, BY = Box<T, H>::BY;
-  constexpr int NS = DIM == 3 ? 2 * H + 2 : 1;
-  constexpr int FB = BY * BX;  // elements of one field box
-  constexpr int PLANE = V * FB;
+  constexpr int HX = Box<T, H>::HX, BX = Box<T, H>::BX;
+  constexpr int FB = Box<T, H>::FB;    // elements one box load writes
+  constexpr int FBP = Box<T, H>::FBP;  // stride between boxes in shared memory
+  constexpr int NS = DIM == 3 ? 2 * H + 1 + StagePrefetch<T>::P : 1;
+  constexpr int PLANE = V * FBP;
   extern __shared__ __align__(128) unsigned char smem[];
   T* ring = reinterpret_cast<T*>(smem);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + sizeof(T) * NS * PLANE);
@@ -109,9 +110,9 @@ __global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ Field
   auto issue_upto = [&](int last) {
     for (; next_issue <= min(phi, last); ++next_issue) {
       const int rel = next_issue - plo, slot = rel % NS;
-      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * PLANE));
+      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * V * FB));
       for (int v = 0; v < V; ++v)
-        tma_load_3d(ring + slot * PLANE + v * FB, &zm.m[v], i0 - HX, j0 - H, next_issue, &bar[slot]);
+        tma_load_3d(ring + slot * PLANE + v * FBP, &zm.m[v], i0 - HX, j0 - H, next_issue, &bar[slot]);
     }
   };
   if (tid == 0) issue_upto(plo + NS - 1);
@@ -119,12 +120,16 @@ __global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ Field
   const int c = (ty + H) * BX + (tx + HX);
   const int cx = active ? cls_of(i, s.nx, H) : 0;
   const int cy = active ? cls_of(j, s.ny, H) : 0;
+  const long long nxy = (long long)s.nx * s.ny;
+  const long long lij = i + (long long)s.nx * j;
+  // pointwise inputs (y_n, accumulator, J*metrics) are software-pipelined one plane ahead:
+  // the loads for plane k+1 are in flight while plane k is computed
+  PointIn<T, DIM> in;
+  if (active) gather<T, DIM, COMP>(s, lij + nxy * k0, in);
   int waited = plo;
   for (int k = k0; k < k1; ++k) {
-    // pointwise inputs of this plane: issued before the wait so their latency overlaps it
-    const long long l = i + (long long)s.nx * (j + (long long)s.ny * k);
-    PointIn<T, DIM> in;
-    if (active) gather<T, DIM, COMP>(s, l, in);
+    PointIn<T, DIM> in_next;
+    if (active && k + 1 < k1) gather<T, DIM, COMP>(s, lij + nxy * (k + 1), in_next);
     bool failed = false;
     const int need = DIM == 3 ? min(phi, k + H) : 0;
     for (; waited <= need; ++waited) {
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ Field
       T D[V][DIM], q[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const T* f = pk + v * FB + c;
+        const T* f = pk + v * FBP + c;
         q[v] = f[0];
         T dx = T(0), dy = T(0);
 #pragma unroll
@@ -159,13 +164,14 @@ __global__ void __launch_bounds__(256) k_stage_tma(const __grid_constant__ Field
 #pragma unroll
           for (int o = -H; o <= H; ++o) {
             const int kk = k + o;
-            if (kk >= plo && kk <= phi) dz += P.w[cz][o + H] * ring[((kk - plo) % NS) * PLANE + v * FB + c];
+            if (kk >= plo && kk <= phi) dz += P.w[cz][o + H] * ring[((kk - plo) % NS) * PLANE + v * FBP + c];
           }
           D[v][DIM - 1] = dz;
         }
       }
-      rhs_update<T, DIM, COMP>(s, l, i, j, k, D, q, in);
+      rhs_update<T, DIM, COMP>(s, lij + nxy * k, i, j, k, D, q, in);
     }
+    in = in_next;
     __syncthreads();
     if (DIM == 3 && tid == 0) issue_upto(k + 1 - H + NS - 1);
   }
@@ -176,10 +182,11 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
                                                     const __grid_constant__ TmaFilterParams<T> P) {
   constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = kFilterSlots;
   constexpr int HX = Box<T, HF>::HX, BX = Box<T, HF>::BX, BY = Box<T, HF>::BY;
-  constexpr int FB = BY * BX;
+  constexpr int FB = Box<T, HF>::FB;    // elements one box load writes
+  constexpr int FBP = Box<T, HF>::FBP;  // stride between boxes in shared memory
   extern __shared__ __align__(128) unsigned char smem[];
   T* ring = reinterpret_cast<T*>(smem);
-  T* u1 = ring + NSF * FB;  // [BY][TX]
+  T* u1 = ring + NSF * FBP;  // [BY][TX]
   uint64_t* bar = reinterpret_cast<uint64_t*>(u1 + BY * TX);
 
   const int v = blockIdx.z;
@@ -202,7 +209,7 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
     for (; next_issue <= min(phi, last); ++next_issue) {
       const int slot = (next_issue - plo) % NSF;
       mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * FB));
-      tma_load_3d(ring + slot * FB, &ym.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
+      tma_load_3d(ring + slot * FBP, &ym.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
     }
   };
   if (tid == 0) issue_upto(plo + NSF - 1);
@@ -231,7 +238,7 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
         }
         return;
       }
-      const T* box = ring + (rel % NSF) * FB;
+      const T* box = ring + (rel % NSF) * FBP;
       for (int r = ty; r < BY; r += TY) {  // F_xi on the tile and its eta halo
         const T* f = box + r * BX + tx + HX;
         T d = T(0);
@@ -298,13 +305,13 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
 
 template <typename T, int DIM, bool COMP>
 size_t stage_smem() {
-  constexpr int NS = DIM == 3 ? 2 * kFdHalf + 2 : 1;
-  return sizeof(T) * NS * (DIM + 2) * Box<T, kFdHalf>::BY * Box<T, kFdHalf>::BX + NS * sizeof(uint64_t);
+  constexpr int NS = DIM == 3 ? 2 * kFdHalf + 1 + StagePrefetch<T>::P : 1;
+  return sizeof(T) * NS * (DIM + 2) * Box<T, kFdHalf>::FBP + NS * sizeof(uint64_t);
 }
 
 template <typename T, int HF>
 size_t filter_smem() {
-  return sizeof(T) * (kFilterSlots * Box<T, HF>::BY * Box<T, HF>::BX + Box<T, HF>::BY * kTileX) +
+  return sizeof(T) * (kFilterSlots * Box<T, HF>::FBP + Box<T, HF>::BY * kTileX) +
          kFilterSlots * sizeof(uint64_t);
 }
 

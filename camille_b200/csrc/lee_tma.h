@@ -40,13 +40,24 @@ struct TmaFilterParams {
   int* errflag;
 };
 
-// Shared-memory box geometry: halo along i rounded up so every TMA row starts on 16 bytes.
+// Shared-memory box geometry: halo along i rounded up so every TMA row starts on 16 bytes;
+// consecutive boxes in shared memory are FBP elements apart, a multiple of 128 bytes, because
+// a cp.async.bulk.tensor destination must be 128-byte aligned.
 template <typename T, int H>
 struct Box {
   static constexpr int A = (int)(16 / sizeof(T));
   static constexpr int HX = ((H + A - 1) / A) * A;
   static constexpr int BX = kTileX + 2 * HX;
   static constexpr int BY = kTileY + 2 * H;
+  static constexpr int FB = BX * BY;
+  static constexpr int FBP = (int)((((size_t)FB * sizeof(T) + 127) / 128) * 128 / sizeof(T));
+  static_assert((FBP * sizeof(T)) % 128 == 0, "box stride must be a multiple of 128 bytes");
+};
+
+// Planes of prefetch in the stage kernel's ring (beyond the 2h+1 stencil planes).
+template <typename T>
+struct StagePrefetch {
+  static constexpr int P = sizeof(T) == 4 ? 2 : 1;
 };
 
 size_t stage_tma_smem(int dim, size_t esz);
