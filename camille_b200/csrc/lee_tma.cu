@@ -118,8 +118,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
   if (tid == 0) issue_upto(plo + NS - 1);
 
   const int c = (ty + H) * BX + (tx + HX);
-  const int cx = active ? cls_of(i, s.nx, H) : 0;
-  const int cy = active ? cls_of(j, s.ny, H) : 0;
+  // closure-class weights along xi and eta are fixed for a thread: keep them in registers
+  T wx[2 * H + 1], wy[2 * H + 1];
+  {
+    const int cx = active ? cls_of(i, s.nx, H) : 0;
+    const int cy = active ? cls_of(j, s.ny, H) : 0;
+#pragma unroll
+    for (int o = 0; o <= 2 * H; ++o) {
+      wx[o] = P.w[cx][o];
+      wy[o] = P.w[cy][o];
+    }
+  }
   const long long nxy = (long long)s.nx * s.ny;
   const long long lij = i + (long long)s.nx * j;
   // pointwise inputs (y_n, accumulator, J*metrics) are software-pipelined one plane ahead:
@@ -144,8 +153,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
       return;
     }
     if (active) {
-      const T* pk = ring + ((k - plo) % NS) * PLANE;
-      const int cz = DIM == 3 ? cls_of(k, s.nz, H) : 0;
+      // ring slots of planes k-H..k+H; planes outside [plo, phi] map to a loaded plane and
+      // carry zero weight (their closure-class weights are zero)
+      const int sk = (k - plo) % NS;
+      int zoff[2 * H + 1];
+      T wz[2 * H + 1];
+      if (DIM == 3) {
+        const int cz = cls_of(k, s.nz, H);
+#pragma unroll
+        for (int o = -H; o <= H; ++o) {
+          const int kk = min(max(k + o, plo), phi);
+          int sl = sk + (kk - k);
+          sl += sl < 0 ? NS : 0;
+          sl -= sl >= NS ? NS : 0;
+          zoff[o + H] = sl * PLANE + c;
+          wz[o + H] = P.w[cz][o + H];
+        }
+      }
+      const T* pk = ring + sk * PLANE;
       T D[V][DIM], q[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
@@ -154,18 +179,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
         T dx = T(0), dy = T(0);
 #pragma unroll
         for (int o = -H; o <= H; ++o) {
-          dx += P.w[cx][o + H] * f[o];
-          dy += P.w[cy][o + H] * f[o * BX];
+          dx += wx[o + H] * f[o];
+          dy += wy[o + H] * f[o * BX];
         }
         D[v][0] = dx;
         D[v][1] = dy;
         if (DIM == 3) {
           T dz = T(0);
 #pragma unroll
-          for (int o = -H; o <= H; ++o) {
-            const int kk = k + o;
-            if (kk >= plo && kk <= phi) dz += P.w[cz][o + H] * ring[((kk - plo) % NS) * PLANE + v * FBP + c];
-          }
+          for (int o = 0; o <= 2 * H; ++o) dz += wz[o] * ring[zoff[o] + v * FBP];
           D[v][DIM - 1] = dz;
         }
       }
@@ -214,8 +236,17 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
   };
   if (tid == 0) issue_upto(plo + NSF - 1);
 
-  const int cx = cls_of(min(i, P.nx - 1), P.nx, HF);
-  const int cy = cls_of(min(j, P.ny - 1), P.ny, HF);
+  // closure-class weights along xi and eta are fixed for a thread: keep them in registers
+  T wx[NQ], wy[NQ];
+  {
+    const int cx = cls_of(min(i, P.nx - 1), P.nx, HF);
+    const int cy = cls_of(min(j, P.ny - 1), P.ny, HF);
+#pragma unroll
+    for (int o = 0; o < NQ; ++o) {
+      wx[o] = P.w[cx][o];
+      wy[o] = P.w[cy][o];
+    }
+  }
   T uq[NQ], dq[HF + 1], xq[HF + 1];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) uq[q] = T(0);
@@ -239,24 +270,28 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
         return;
       }
       const T* box = ring + (rel % NSF) * FBP;
-      for (int r = ty; r < BY; r += TY) {  // F_xi on the tile and its eta halo
-        const T* f = box + r * BX + tx + HX;
-        T d = T(0);
-#pragma unroll
-        for (int o = -HF; o <= HF; ++o) d += P.w[cx][o + HF] * f[o];
-        u1[r * TX + tx] = COMP ? f[0] + d : d;
-      }
-      __syncthreads();
+      // F_xi on the thread's own row (kept in registers) and on its share of the eta halo rows
       const T* fc = box + (ty + HF) * BX + tx + HX;
       xc = fc[0];
+      T d1 = T(0);
+#pragma unroll
+      for (int o = -HF; o <= HF; ++o) d1 += wx[o + HF] * fc[o];
+      const T u1c = COMP ? xc + d1 : d1;
+      u1[(ty + HF) * TX + tx] = u1c;
+      for (int r = ty; r < 2 * HF; r += TY) {
+        const int row = r < HF ? r : r + TY;
+        const T* f = box + row * BX + tx + HX;
+        T d = T(0);
+#pragma unroll
+        for (int o = -HF; o <= HF; ++o) d += wx[o + HF] * f[o];
+        u1[row * TX + tx] = COMP ? f[0] + d : d;
+      }
+      __syncthreads();
       T dy = T(0);
 #pragma unroll
-      for (int o = -HF; o <= HF; ++o) dy += P.w[cy][o + HF] * u1[(ty + HF + o) * TX + tx];
+      for (int o = -HF; o <= HF; ++o) dy += wy[o + HF] * (o == 0 ? u1c : u1[(ty + HF + o) * TX + tx]);
       if (COMP) {
-        T d1 = T(0);
-#pragma unroll
-        for (int o = -HF; o <= HF; ++o) d1 += P.w[cx][o + HF] * fc[o];
-        u2 = u1[(ty + HF) * TX + tx] + dy;
+        u2 = u1c + dy;
         d12 = d1 + dy;
       } else {
         u2 = dy;
@@ -280,8 +315,14 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
     if (DIM == 3) {
       const int cz = cls_of(k, P.nz, HF);
       fz = T(0);
+      if (cz == 0) {
+        // interior plane: the loop-invariant interior weights
 #pragma unroll
-      for (int o = -HF; o <= HF; ++o) fz += P.w[cz][o + HF] * uq[o + HF];
+        for (int o = 0; o < NQ; ++o) fz += P.w[0][o] * uq[o];
+      } else {
+#pragma unroll
+        for (int o = 0; o < NQ; ++o) fz += P.w[cz][o] * uq[o];
+      }
       x0 = xq[0];
       dsum = dq[0];
     } else {
