@@ -75,6 +75,8 @@ struct BlockData {
   void* rho_next = nullptr;
   // TMA-staged kernels (blocks without holes, 4th-order difference)
   bool tma = false, tma_filter = false;
+  int traits = kTrGeneric;          // coefficient-layout traits of the TMA stage kernel
+  void* d_sigma_field = nullptr;    // summed sponge strengths per point (working precision)
   int tiles_x = 0, tiles_y = 0;
   int stage_chunk = 0, filter_chunk = 0;
 };
@@ -508,6 +510,7 @@ void fill_stage_common(lee_ctx* c, BlockData& b, StageParams<T>& p) {
   for (int d = 0; d < 3; ++d) p.code[d] = b.has_holes ? b.d_code_fd[d] : nullptr;
   p.iblank = b.has_holes ? b.d_iblank : nullptr;
   p.fd = c->fd;
+  p.sigma = (const T*)b.d_sigma_field;
 }
 
 // Amplitude of the monopole at time t (oracle patch P2, modelled on src/solver/source.cpp:60-92).
@@ -657,7 +660,7 @@ int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* co
   int rc = field_maps(c, b, zin, Box<T, kFdHalf>::BX, Box<T, kFdHalf>::BY, &fm);
   if (rc) return rc;
   const int chunks = c->cfg.num_dim == 3 ? (b.nz + tp.k_chunk - 1) / tp.k_chunk : 1;
-  CK(launch_stage_tma<T>(fm, tp, c->comp ? 1 : 0, b.tiles_x * b.tiles_y, chunks, c->stream));
+  CK(launch_stage_tma<T>(fm, tp, b.traits, b.tiles_x * b.tiles_y, chunks, c->stream));
   return LEE_OK;
 }
 
@@ -759,6 +762,41 @@ int autotune(lee_ctx* c, BlockData& b) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return check_device_error(c);
+}
+
+__global__ void k_add_box(int nx, int ny, int lo0, int lo1, int lo2, int b0, int b1, long long nb, const double* sig,
+                          double* field) {
+  for (long long lb = blockIdx.x * (long long)blockDim.x + threadIdx.x; lb < nb; lb += (long long)gridDim.x * blockDim.x) {
+    const int i = lo0 + (int)(lb % b0), j = lo1 + (int)((lb / b0) % b1), k = lo2 + (int)(lb / ((long long)b0 * b1));
+    field[i + (long long)nx * (j + (long long)ny * k)] += sig[lb];
+  }
+}
+
+// Sum of the sponge strengths of every zone at each point (zones are added one after the
+// other, so overlapping corners accumulate as in source::apply_bufferZone), in the working
+// precision of the stage kernels.
+int build_sigma_field(lee_ctx* c, BlockData& b) {
+  double* f = nullptr;
+  int rc = dalloc(c, &f, (size_t)b.N);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(f, 0, (size_t)b.N * 8, c->stream));
+  for (auto& z : b.bnd) {
+    if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+    const int b0 = z.hi[0] - z.lo[0] + 1, b1 = z.hi[1] - z.lo[1] + 1, b2 = z.hi[2] - z.lo[2] + 1;
+    const long long nb = (long long)b0 * b1 * b2;
+    k_add_box<<<grid1d(nb), 256, 0, c->stream>>>(b.nx, b.ny, z.lo[0], z.lo[1], z.lo[2], b0, b1, nb, z.d_sigma, f);
+    CK(cudaGetLastError());
+  }
+  if (!c->comp) {
+    b.d_sigma_field = f;
+    return LEE_OK;
+  }
+  float* g = nullptr;
+  if ((rc = dalloc(c, &g, (size_t)b.N))) return rc;
+  k_convert<float><<<grid1d(b.N), 256, 0, c->stream>>>(b.N, g, f);
+  CK(cudaGetLastError());
+  b.d_sigma_field = g;
+  return LEE_OK;
 }
 
 int check_device_error(lee_ctx* c) {
@@ -1192,6 +1230,22 @@ int lee_prepare(lee_ctx* c) {
     b.tiles_y = (b.ny + kTileY - 1) / kTileY;
     b.tma = c->wst_ok && !b.has_holes && rows16 && !b.need_rho;
     b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE;
+    if (b.tma) {
+      // coefficient-layout traits of the stage kernel
+      bool jmf = false, uni = true, spg = false;
+      for (int q = 0; q < 9; ++q) jmf |= (c->comp ? b.cf_jm[q].p : (const void*)b.cd_jm[q].p) != nullptr;
+      auto is_const = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? !f.p : !d.p; };
+      auto is_zero = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? f.zero : d.zero; };
+      for (int q = 0; q < 3; ++q) {
+        uni &= is_const(b.cd_ub[q], b.cf_ub[q]);
+        uni &= is_zero(b.cd_gs[q], b.cf_gs[q]) != 0 && is_zero(b.cd_gp[q], b.cf_gp[q]) != 0;
+      }
+      for (int q = 0; q < 9; ++q) uni &= is_zero(b.cd_gu[q], b.cf_gu[q]) != 0;
+      uni &= is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi) && !b.need_rho;
+      for (auto& z : b.bnd) spg |= z.kind == LEE_SPONGE_FREUND_AMBIENT;
+      b.traits = (jmf ? kTrJmField : 0) | (uni ? kTrUniform : 0) | (spg ? kTrSponge : 0);
+      if (spg && (rc = build_sigma_field(c, b))) return rc;
+    }
     b.stage_chunk = b.filter_chunk = b.nz;
     if ((b.tma || b.tma_filter) && (rc = ensure_encoder(c))) return rc;
     if ((rc = c->comp ? autotune<float>(c, b) : autotune<double>(c, b))) return rc;

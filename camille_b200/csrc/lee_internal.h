@@ -12,6 +12,12 @@ namespace lee {
 constexpr int kMaxZones = 8;  // sponge zones per block read by the stage kernel
 constexpr int kMaxVars = 5;   // s', u'(1..num_dim), p'
 
+// Compile-time traits of a block's coefficient layout, chosen at setup (stage kernels):
+constexpr int kTrJmField = 1;  // J*metrics vary over the block (else kernel constants)
+constexpr int kTrUniform = 2;  // uniform mean flow: u_bar, p_bar, rho_bar constant, zero gradients
+constexpr int kTrSponge = 4;   // sponge strengths summed into one per-point field (else the zone loop)
+constexpr int kTrGeneric = kTrJmField;  // every coefficient checked at run time
+
 // One directional operator: interior stencil c[l+h] (l = -h..h), closure rows
 // B[row][s] (row < nb, s < S) and the right-boundary sign (-1 difference, +1 filter).
 // Values are those of the reference's StandardCentral / StandardCentralFilter /
@@ -68,9 +74,10 @@ struct StageParams {
   const T* rho_prev;            // rho'/rho_bar from the previous step's last stage (stage 0 input)
   T* rho_next;                  // written on the last stage
   T gamma, inv_gamma;
-  // sponges
+  // sponges: per zone (generic kernels) or summed into one per-point field (TMA kernels)
   int nzones;
   Zone<T> zones[kMaxZones];
+  const T* sigma;
   // monopole source: rhs[p] += src_amp * g, g on a box (src_lo..src_hi), i fastest
   int has_src;
   T src_amp;

@@ -22,15 +22,16 @@ struct PointIn {
   T jm[DIM][DIM];     // J * metrics[d][x]
   T yn[DIM + 2];      // y_n (stages after the first)
   T av[DIM + 2];      // accumulator (stages after the first) or carried error (compensated, first stage)
+  T sg;               // sponge strength (kTrSponge)
 };
 
-template <typename T, int DIM, bool COMP>
+template <typename T, int DIM, bool COMP, int TR>
 __device__ __forceinline__ void gather(const StageParams<T>& p, long long l, PointIn<T, DIM>& in) {
   constexpr int V = DIM + 2;
 #pragma unroll
   for (int d = 0; d < DIM; ++d)
 #pragma unroll
-    for (int x = 0; x < DIM; ++x) in.jm[d][x] = cval(p.jm[d * 3 + x], l);
+    for (int x = 0; x < DIM; ++x) in.jm[d][x] = (TR & kTrJmField) ? cval(p.jm[d * 3 + x], l) : p.jm[d * 3 + x].c;
   const bool need_yn = p.stage > 0 && (COMP || !p.last);
   const bool need_av = p.stage > 0 || (COMP && p.stage == 0);
 #pragma unroll
@@ -38,12 +39,20 @@ __device__ __forceinline__ void gather(const StageParams<T>& p, long long l, Poi
     in.yn[v] = need_yn ? p.yn[v][l] : T(0);
     in.av[v] = need_av ? (p.stage == 0 ? p.comp[v][l] : p.acc[v][l]) : T(0);
   }
+  in.sg = (TR & kTrSponge) ? __ldg(p.sigma + l) : T(0);
 }
+
+template <typename T, int DIM>
+__device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, long long l, const T (&g)[DIM + 2][DIM],
+                                               const T (&q)[DIM + 2], const T (&ub)[DIM], T (&r)[DIM + 2]);
+template <typename T, int DIM, bool COMP>
+__device__ __forceinline__ void rk_update(const StageParams<T>& p, long long l, const T (&q)[DIM + 2],
+                                          const PointIn<T, DIM>& in, const T (&r)[DIM + 2]);
 
 // D[v][d]: computational-space derivative of field v along direction d; q[v]: the
 // stage input at the point; in: the gathered inputs. Writes the next stage input and
 // the accumulator.
-template <typename T, int DIM, bool COMP>
+template <typename T, int DIM, bool COMP, int TR>
 __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l, int i, int j, int k,
                                            const T (&D)[DIM + 2][DIM], const T (&q)[DIM + 2],
                                            const PointIn<T, DIM>& in) {
@@ -61,10 +70,66 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l,
       g[v][x] = s;
     }
   }
+  constexpr bool UNI = (TR & kTrUniform) != 0;
   T ub[DIM];
 #pragma unroll
-  for (int x = 0; x < DIM; ++x) ub[x] = cval(p.ubar[x], l);
+  for (int x = 0; x < DIM; ++x) ub[x] = UNI ? p.ubar[x].c : cval(p.ubar[x], l);
   T r[V];
+  if (UNI) {
+    // uniform mean flow: every mean-gradient term vanishes
+    T rs = T(0);
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) rs -= ub[x] * g[0][x];
+    r[0] = rs;
+    const T rbi = p.rhobar_inv.c;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      T ru = T(0);
+#pragma unroll
+      for (int x = 0; x < DIM; ++x) ru -= ub[x] * g[1 + a][x];
+      ru -= g[P][a] * rbi;
+      r[1 + a] = ru;
+    }
+    T rp = T(0);
+    const T gpb = p.gamma * p.pbar.c;
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) {
+      rp -= ub[x] * g[P][x];
+      rp -= gpb * g[1 + x][x];
+    }
+    r[P] = rp;
+  } else {
+    rhs_mean_terms<T, DIM>(p, l, g, q, ub, r);
+  }
+  if (p.has_src && i >= p.src_lo[0] && i <= p.src_hi[0] && j >= p.src_lo[1] && j <= p.src_hi[1] &&
+      k >= p.src_lo[2] && k <= p.src_hi[2]) {
+    int b0 = p.src_hi[0] - p.src_lo[0] + 1, b1 = p.src_hi[1] - p.src_lo[1] + 1;
+    long long lb = (i - p.src_lo[0]) + (long long)b0 * ((j - p.src_lo[1]) + (long long)b1 * (k - p.src_lo[2]));
+    r[P] += p.src_amp * p.src_g[lb];
+  }
+  if (TR & kTrSponge) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) r[v] += -in.sg * (q[v] - T(0));
+  } else {
+    for (int z = 0; z < p.nzones; ++z) {
+      const Zone<T>& zn = p.zones[z];
+      if (i < zn.lo[0] || i > zn.hi[0] || j < zn.lo[1] || j > zn.hi[1] || k < zn.lo[2] || k > zn.hi[2]) continue;
+      int b0 = zn.hi[0] - zn.lo[0] + 1, b1 = zn.hi[1] - zn.lo[1] + 1;
+      long long lb = (i - zn.lo[0]) + (long long)b0 * ((j - zn.lo[1]) + (long long)b1 * (k - zn.lo[2]));
+      T sg = zn.sig[lb];
+#pragma unroll
+      for (int v = 0; v < V; ++v) r[v] += -sg * (q[v] - T(0));
+    }
+  }
+  rk_update<T, DIM, COMP>(p, l, q, in, r);
+}
+
+// The LEE right-hand side of a non-uniform mean flow: every coefficient is read at the point
+// when it varies, and terms whose mean gradient is identically zero are skipped.
+template <typename T, int DIM>
+__device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, long long l, const T (&g)[DIM + 2][DIM],
+                                               const T (&q)[DIM + 2], const T (&ub)[DIM], T (&r)[DIM + 2]) {
+  constexpr int P = DIM + 1;
   {
     T rs = T(0);
 #pragma unroll
@@ -108,22 +173,13 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l,
     }
     r[P] = rp;
   }
-  if (p.has_src && i >= p.src_lo[0] && i <= p.src_hi[0] && j >= p.src_lo[1] && j <= p.src_hi[1] &&
-      k >= p.src_lo[2] && k <= p.src_hi[2]) {
-    int b0 = p.src_hi[0] - p.src_lo[0] + 1, b1 = p.src_hi[1] - p.src_lo[1] + 1;
-    long long lb = (i - p.src_lo[0]) + (long long)b0 * ((j - p.src_lo[1]) + (long long)b1 * (k - p.src_lo[2]));
-    r[P] += p.src_amp * p.src_g[lb];
-  }
-  for (int z = 0; z < p.nzones; ++z) {
-    const Zone<T>& zn = p.zones[z];
-    if (i < zn.lo[0] || i > zn.hi[0] || j < zn.lo[1] || j > zn.hi[1] || k < zn.lo[2] || k > zn.hi[2]) continue;
-    int b0 = zn.hi[0] - zn.lo[0] + 1, b1 = zn.hi[1] - zn.lo[1] + 1;
-    long long lb = (i - zn.lo[0]) + (long long)b0 * ((j - zn.lo[1]) + (long long)b1 * (k - zn.lo[2]));
-    T sg = zn.sig[lb];
-#pragma unroll
-    for (int v = 0; v < V; ++v) r[v] += -sg * (q[v] - T(0));
-  }
+}
 
+// The Runge-Kutta stage update of one point from its right-hand side r.
+template <typename T, int DIM, bool COMP>
+__device__ __forceinline__ void rk_update(const StageParams<T>& p, long long l, const T (&q)[DIM + 2],
+                                          const PointIn<T, DIM>& in, const T (&r)[DIM + 2]) {
+  constexpr int V = DIM + 2;
   if (p.stage < 0) {  // right-hand side only (spatial::compute_RHS)
 #pragma unroll
     for (int v = 0; v < V; ++v) p.zout[v][l] = r[v];

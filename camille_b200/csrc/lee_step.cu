@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) k_stage(StageParams<T> p) {
   const int nn[3] = {p.nx, p.ny, p.nz};
   const long long sd[3] = {1, p.nx, nxy};
   PointIn<T, DIM> in;
-  gather<T, DIM, COMP>(p, l, in);
+  gather<T, DIM, COMP, kTrGeneric>(p, l, in);
   T D[V][DIM], q[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256) k_stage(StageParams<T> p) {
     for (int d = 0; d < DIM; ++d) D[v][d] = dop<T>(p.fd, p.zin[v], l, pos[d], nn[d], sd[d], p.code[d]);
     q[v] = p.zin[v][l];
   }
-  rhs_update<T, DIM, COMP>(p, l, i, j, k, D, q, in);
+  rhs_update<T, DIM, COMP, kTrGeneric>(p, l, i, j, k, D, q, in);
 }
 
 // One direction of spatial::apply_filter (src/solver/spatial_discretization.cpp:2191-2246).

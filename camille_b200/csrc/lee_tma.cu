@@ -78,7 +78,7 @@ __device__ __forceinline__ int cls_of(int pos, int n, int nb) {
   return pos < nb ? 1 + pos : (pos > n - 1 - nb ? 1 + nb + (n - 1 - pos) : 0);
 }
 
-template <typename T, int DIM, bool COMP>
+template <typename T, int DIM, bool COMP, int TR>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
     k_stage_tma(const __grid_constant__ FieldMaps zm, const __grid_constant__ TmaStageParams<T> P) {
   constexpr int H = kFdHalf, TX = kTileX, TY = kTileY, V = DIM + 2;
@@ -131,14 +131,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
   }
   const long long nxy = (long long)s.nx * s.ny;
   const long long lij = i + (long long)s.nx * j;
-  // pointwise inputs (y_n, accumulator, J*metrics) are software-pipelined one plane ahead:
-  // the loads for plane k+1 are in flight while plane k is computed
+  // pointwise inputs (y_n, accumulator, J*metrics, sponge): in FP32 they are software-pipelined
+  // one plane ahead, so the loads for plane k+1 are in flight while plane k is computed; in
+  // FP64 (twice the registers) they are issued at the top of the plane, before the wait
+  constexpr bool PIPE = sizeof(T) == 4;
   PointIn<T, DIM> in;
-  if (active) gather<T, DIM, COMP>(s, lij + nxy * k0, in);
+  if (PIPE && active) gather<T, DIM, COMP, TR>(s, lij + nxy * k0, in);
   int waited = plo;
   for (int k = k0; k < k1; ++k) {
     PointIn<T, DIM> in_next;
-    if (active && k + 1 < k1) gather<T, DIM, COMP>(s, lij + nxy * (k + 1), in_next);
+    if (PIPE && active && k + 1 < k1) gather<T, DIM, COMP, TR>(s, lij + nxy * (k + 1), in_next);
+    if (!PIPE && active) gather<T, DIM, COMP, TR>(s, lij + nxy * k, in);
     bool failed = false;
     const int need = DIM == 3 ? min(phi, k + H) : 0;
     for (; waited <= need; ++waited) {
@@ -191,9 +194,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
           D[v][DIM - 1] = dz;
         }
       }
-      rhs_update<T, DIM, COMP>(s, lij + nxy * k, i, j, k, D, q, in);
+      rhs_update<T, DIM, COMP, TR>(s, lij + nxy * k, i, j, k, D, q, in);
     }
-    in = in_next;
+    if (PIPE) in = in_next;
     __syncthreads();
     if (DIM == 3 && tid == 0) issue_upto(k + 1 - H + NS - 1);
   }
@@ -356,17 +359,34 @@ size_t filter_smem() {
          kFilterSlots * sizeof(uint64_t);
 }
 
-template <typename T, int DIM, bool COMP>
+template <typename T, int DIM, bool COMP, int TR>
 cudaError_t go_stage(const FieldMaps& z, const TmaStageParams<T>& p, int tiles, int chunks, cudaStream_t s) {
   static bool attr = false;
   const size_t sm = stage_smem<T, DIM, COMP>();
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage_tma<T, DIM, COMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_stage_tma<T, DIM, COMP, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_stage_tma<T, DIM, COMP><<<dim3(tiles, chunks), 256, sm, s>>>(z, p);
+  k_stage_tma<T, DIM, COMP, TR><<<dim3(tiles, chunks), 256, sm, s>>>(z, p);
   return cudaGetLastError();
+}
+
+// Traits are a run-time choice of the host (lee_point.cuh, kTr*) mapped onto instantiations.
+template <typename T, int DIM, bool COMP>
+cudaError_t go_stage_tr(const FieldMaps& z, const TmaStageParams<T>& p, int tr, int tiles, int chunks,
+                        cudaStream_t s) {
+  switch (tr & 7) {
+    case 0: return go_stage<T, DIM, COMP, 0>(z, p, tiles, chunks, s);
+    case 1: return go_stage<T, DIM, COMP, 1>(z, p, tiles, chunks, s);
+    case 2: return go_stage<T, DIM, COMP, 2>(z, p, tiles, chunks, s);
+    case 3: return go_stage<T, DIM, COMP, 3>(z, p, tiles, chunks, s);
+    case 4: return go_stage<T, DIM, COMP, 4>(z, p, tiles, chunks, s);
+    case 5: return go_stage<T, DIM, COMP, 5>(z, p, tiles, chunks, s);
+    case 6: return go_stage<T, DIM, COMP, 6>(z, p, tiles, chunks, s);
+    default: return go_stage<T, DIM, COMP, 7>(z, p, tiles, chunks, s);
+  }
 }
 
 template <typename T, int DIM, bool COMP, int HF>
@@ -383,11 +403,13 @@ size_t stage_tma_smem(int dim, size_t esz) {
   return dim == 3 ? stage_smem<float, 3, true>() : stage_smem<float, 2, true>();
 }
 
+// The FP64 form runs uncompensated and the FP32 form compensated (lee_config.precision).
 template <typename T>
-cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int comp, int tiles, int chunks,
+cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int traits, int tiles, int chunks,
                              cudaStream_t s) {
-  if (p.s.dim == 2) return comp ? go_stage<T, 2, true>(zin, p, tiles, 1, s) : go_stage<T, 2, false>(zin, p, tiles, 1, s);
-  return comp ? go_stage<T, 3, true>(zin, p, tiles, chunks, s) : go_stage<T, 3, false>(zin, p, tiles, chunks, s);
+  constexpr bool COMP = sizeof(T) == 4;
+  if (p.s.dim == 2) return go_stage_tr<T, 2, COMP>(zin, p, traits, tiles, 1, s);
+  return go_stage_tr<T, 3, COMP>(zin, p, traits, tiles, chunks, s);
 }
 
 template <typename T>

@@ -62,7 +62,7 @@ struct StagePrefetch {
 
 size_t stage_tma_smem(int dim, size_t esz);
 template <typename T>
-cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int comp, int tiles, int chunks,
+cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int traits, int tiles, int chunks,
                              cudaStream_t s);
 template <typename T>
 cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
