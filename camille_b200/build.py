@@ -23,6 +23,7 @@ UNITS = {
     "lee_step.cu": [],
     "lee_tma.cu": [],
     "lee_capi.cu": [],
+    "lee_static.cu": [],
 }
 
 

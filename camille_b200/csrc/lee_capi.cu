@@ -891,6 +891,14 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
 
 }  // namespace
 
+namespace lee {
+// Filter coefficient table and the context-free error message, for lee_static.cu.
+bool filter_table(OpTable* o, int scheme, int order, double strength) {
+  return make_filter(o, scheme, order, strength);
+}
+void set_global_error(const char* msg) { snprintf(g_create_error, sizeof g_create_error, "%s", msg); }
+}  // namespace lee
+
 extern "C" {
 
 int lee_create(const lee_config* cfg, lee_ctx** out) {

@@ -114,6 +114,10 @@ cudaError_t launch_filter_pass(const FilterParams<T>& p, int comp, cudaStream_t 
 cudaError_t launch_hole_zero(int n, int V, double** f, const int* iblank, cudaStream_t s);
 cudaError_t launch_hole_zero_f(int n, int V, float** f, const int* iblank, cudaStream_t s);
 
+// lee_capi.cu helpers shared with lee_static.cu
+bool filter_table(OpTable* o, int scheme, int order, double strength);
+void set_global_error(const char* msg);
+
 // lee_setup.cu (FP64, no FMA contraction)
 cudaError_t setup_apply_dir(const OpTable& op, int nx, int ny, int nz, int dir, const double* f, double* out,
                             const int8_t* code, int zero_if_one_cell, cudaStream_t s);

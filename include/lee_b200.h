@@ -177,6 +177,22 @@ typedef struct {
 int lee_set_timing(lee_ctx *ctx, int on);
 int lee_get_stats(lee_ctx *ctx, lee_stats *stats);
 
+/* The filter of one field, with no device allocation (no counterpart in the reference: it
+ * serves callers that cannot call cudaMalloc, such as a framework that owns the device
+ * memory through its own allocator or a time loop that must not allocate). Applies the
+ * dimension-split filter of spatial::apply_filter to one variable of one block without
+ * holes: d_in and d_out are distinct device arrays of nxi*neta*nzeta doubles (i fastest),
+ * owned by the caller; work is enqueued on `stream` (a cudaStream_t, NULL for the default
+ * stream) and the call returns without synchronizing. The intermediate passes use a
+ * scratch array compiled into the library (2 x 2^20 doubles, held by every GPU that loads
+ * the library until exit): fields above 2^20 points are refused with LEE_ERR_ARG. The first
+ * call on each device looks up that array's device address; make it before any stream
+ * capture. Calls share the array, so calls that overlap on the GPU race. Errors are
+ * reported by lee_last_error(NULL). */
+int lee_filter_field_static(int num_dim, int filter_scheme, int filter_order, double filter_strength,
+                            double filter_blend, int nxi, int neta, int nzeta, const double *d_in, double *d_out,
+                            void *stream);
+
 #ifdef __cplusplus
 }
 #endif

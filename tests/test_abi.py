@@ -37,14 +37,20 @@ def test_product_exports_every_declared_symbol(product_lib):
     assert not missing, missing
 
 
+# Entry points that take device pointers: the CPU oracle and the context-based Solver
+# binding do not cover them (tests call them through ctypes directly).
+DEVICE_ONLY = {"lee_filter_field_static"}
+
+
 def test_oracle_exports_the_same_abi(oracle_lib):
-    missing = [n for n in declared_functions() if not hasattr(oracle_lib.dll, "orc_" + n[4:])]
+    missing = [n for n in declared_functions()
+               if n not in DEVICE_ONLY and not hasattr(oracle_lib.dll, "orc_" + n[4:])]
     assert not missing, missing
 
 
 def test_bindings_cover_the_header():
     bound = {"lee_" + n for n in api.SIGNATURES}
-    assert set(declared_functions()) <= bound
+    assert set(declared_functions()) - DEVICE_ONLY <= bound
 
 
 def test_no_cpu_fallback_without_gpu(product_lib):
