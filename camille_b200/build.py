@@ -24,6 +24,7 @@ UNITS = {
     "lee_tma.cu": [],
     "lee_capi.cu": [],
     "lee_static.cu": [],
+    "lee_bc.cu": [],
 }
 
 

@@ -264,3 +264,60 @@ def precompute_sponges(case: Case) -> None:
     for bd in case.boundaries:
         if bd.kind == "sponge_freund_ambient" and bd.sigma is None:
             bd.sigma = sponge_sigma(case, bd)
+
+
+def shear2d(nx: int = 64, ny: int = 48, spacing: float = 0.25, bump: float = 0.3, nsteps: int = 10,
+            sponge: int = 6, gamma: float = 1.4, halfwidth: float = 4.0) -> Case:
+    """2-D block over a bumped slip wall under a parallel tanh shear layer.
+
+    The wall (eta = 0) follows y_w(x) = bump * exp(-x^2 / (ny spacing)^2 * 16) and the grid
+    lines relax to flat at the top; the mean is u_bar = 0.15 (1 + tanh 2 (y - y_c)) with
+    y_c at mid height, a mild entropy layer s_bar = 0.05 tanh(y - y_c) and p_bar = 1/gamma,
+    so every mean-gradient term of the right-hand side, including the rho'/rho_bar one, is
+    active. BC lines: ``wall_slip_kinematic`` on the wall, ``neumann`` on the top, Freund
+    sponges ``sponge`` cells wide at both x ends. A Gaussian p' pulse sits over the bump and a
+    weaker one below the top face."""
+    xs = (np.arange(nx, dtype=np.float64) - 0.5 * (nx - 1)) * spacing
+    eta = np.arange(ny, dtype=np.float64)
+    height = (ny - 1) * spacing
+    yw = bump * np.exp(-16.0 * xs * xs / (height * height))
+    frac = eta / (ny - 1)
+    x = np.broadcast_to(xs[None, :], (ny, nx)).copy()
+    y = yw[None, :] * (1.0 - frac[:, None]) + (eta * spacing)[:, None]
+    x, y = x[None], y[None]
+    z = np.zeros_like(x)
+    yc = 0.5 * height
+    mean = np.zeros((5,) + x.shape)
+    mean[0] = 0.05 * np.tanh(y - yc)
+    mean[1] = 0.15 * (1.0 + np.tanh(2.0 * (y - yc)))
+    mean[4] = 1.0 / gamma
+    state = np.zeros((5,) + x.shape)
+    state[4] = 1e-3 * _gauss(x * x + (y - 0.3 * height) ** 2, halfwidth * spacing)
+    state[4] += 5e-4 * _gauss((x - 0.2 * xs[-1]) ** 2 + (y - 0.85 * height) ** 2, halfwidth * spacing)
+    blk = Block(x, y, z, mean, state)
+    bnd = [Boundary(0, "wall_slip_kinematic", 1, 0, (0, 0, 0), (nx - 1, 0, 0)),
+           Boundary(0, "neumann", 1, 1, (0, ny - 1, 0), (nx - 1, ny - 1, 0))]
+    if sponge > 0:
+        bnd += [b for b in sponge_frame(2, blk.dims, sponge) if b.dir == 0]
+    return Case(name=f"shear2d_{nx}x{ny}", num_dim=2, blocks=[blk], gamma=gamma, nsteps=nsteps,
+                boundaries=bnd, sponge_constant=1.0,
+                notes=f"2-D {nx}x{ny} shear layer over a bumped slip wall, sponge {sponge}")
+
+
+def wall3d(n: int = 16, nsteps: int = 3, gamma: float = 1.4, halfwidth: float = 2.0) -> Case:
+    """3-D curvilinear block (the curvi3d mapping) with a slip wall on zeta = 0, a Neumann
+    face on xi = n-1 and a mean shear u_bar = 0.3 (1 + 0.5 tanh((z - n/2) / 3)) along x,
+    so that the rho'/rho_bar term is active in 3-D too."""
+    x, y, z = curvi3d_grid(n)
+    mean = np.zeros((5,) + x.shape)
+    mean[1] = 0.3 * (1.0 + 0.5 * np.tanh((z - 0.5 * n) / 3.0))
+    mean[4] = 1.0 / gamma
+    state = np.zeros((5,) + x.shape)
+    c = 0.5 * (n - 1)
+    state[4] = 1e-3 * _gauss((x - c) ** 2 + (y - c) ** 2 + (z - 0.3 * n) ** 2, halfwidth)
+    blk = Block(x, y, z, mean, state)
+    m = n - 1
+    bnd = [Boundary(0, "wall_slip_kinematic", 2, 0, (0, 0, 0), (m, m, 0)),
+           Boundary(0, "neumann", 0, 1, (m, 0, 0), (m, m, m))]
+    return Case(name=f"wall3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
+                notes=f"3-D {n}^3 curvilinear, slip wall zeta=0, Neumann xi=max, shear mean")

@@ -71,8 +71,8 @@ struct BlockData {
   void* zb[2][kMaxVars] = {};
   void* comp[kMaxVars] = {};
   void* dsum[kMaxVars] = {};
-  void* rho_prev = nullptr;
-  void* rho_next = nullptr;
+  void* rho = nullptr;      // rho'/rho_bar of the last pre-filter state (non-uniform mean velocity)
+  bool rho_valid = false;   // false until a step or a filter call has written it
   // TMA-staged kernels (blocks without holes, 4th-order difference)
   bool tma = false, tma_filter = false;
   int traits = kTrGeneric;          // coefficient-layout traits of the TMA stage kernel
@@ -314,6 +314,15 @@ template <typename T>
 __global__ void k_convert(long long n, T* out, const double* in) {
   for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
     out[l] = (T)in[l];
+}
+
+// FP64 -> (y, e) with y = fl32(x) and e = fl32(x - y): the compensated pair of an uploaded state
+__global__ void k_split(long long n, float* y, float* e, const double* in) {
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x) {
+    const float r = (float)in[l];
+    y[l] = r;
+    e[l] = (float)(in[l] - (double)r);
+  }
 }
 
 template <typename T>
@@ -810,6 +819,39 @@ int check_device_error(lee_ctx* c) {
   return LEE_OK;
 }
 
+// Every BC line of a block, in the order they were added, on the fields f (with the
+// rounding errors e of a compensated pair, or null).
+template <typename T>
+int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e) {
+  for (auto& z : b.bnd) {
+    if (z.kind != LEE_BC_NEUMANN && z.kind != LEE_BC_WALL_SLIP_KINEMATIC) continue;
+    BcParams<T> p;
+    memset(&p, 0, sizeof p);
+    p.kind = z.kind; p.dir = z.dir; p.end = z.end;
+    p.nd = c->cfg.num_dim; p.V = c->V;
+    for (int d = 0; d < 3; ++d) {
+      p.lo[d] = z.lo[d];
+      p.nb[d] = z.hi[d] - z.lo[d] + 1;
+    }
+    p.lo[z.dir] = z.end == 0 ? z.lo[z.dir] : z.hi[z.dir];
+    p.nb[z.dir] = 1;
+    p.nx = b.nx; p.ny = b.ny;
+    p.sd = z.dir == 0 ? 1 : z.dir == 1 ? (long long)b.nx : (long long)b.nx * b.ny;
+    p.S = c->fd.S;
+    for (int q = 0; q < c->fd.S; ++q) p.c0[q] = c->fd.B[0][q];
+    for (int v = 0; v < c->V; ++v) {
+      p.y[v] = (T*)f[v];
+      p.e[v] = e ? (T*)e[v] : nullptr;
+    }
+    for (int q = 0; q < 9; ++q) { p.met[q] = b.d_met[q]; p.minv[q] = b.d_minv[q]; }
+    p.jac = b.d_jac;
+    p.iblank = b.has_holes ? b.d_iblank : nullptr;
+    CK(launch_bc<T>(p, c->stream));
+    c->stats.kernel_launches += 1;
+  }
+  return LEE_OK;
+}
+
 template <typename T>
 int advance_impl(lee_ctx* c, int nsteps, double dt) {
   const int rk = c->cfg.rk_scheme;
@@ -849,7 +891,7 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
           p.zout[v] = (T*)zout[v];
           p.comp[v] = (T*)b.comp[v];
         }
-        p.rho_prev = (const T*)b.rho_prev;
+        p.rho_prev = b.rho_valid ? (const T*)b.rho : nullptr;
         int e0 = mark(c);
         int rc = launch_stage_any<T>(c, b, p, zin);
         if (rc) return rc;
@@ -858,13 +900,27 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
         c->stats.stage_launches += 1;
         c->stats.kernel_launches += 1;
       }
-      // boundary conditions and overset updates of the stage output come here
+      // boundary update of the stage output (spatial::update_boundary): z, or y_next after the
+      // last stage (FP64: the accumulator; compensated: the pair y_pre, e)
+      const bool last = s == ns - 1;
+      for (auto& b : c->blk) {
+        void** zout = b.zb[s % 2];
+        void** tgt = (last && !c->comp) ? b.acc : zout;
+        void** err = (last && c->comp) ? b.acc : nullptr;
+        int rc = apply_bcs<T>(c, b, tgt, err);
+        if (rc) return rc;
+        if (last && b.need_rho) {
+          // rho'/rho_bar of the pre-filter state, read by the next step's first stage: the
+          // reference recomputes its auxiliary fields after the boundary update and not after
+          // the filter (temporal_discretization.cpp:236-242)
+          CK(launch_rho<T>(b.N, c->V, (T* const*)tgt, (T* const*)err, b.d_mean[4], c->cfg.gamma, (T*)b.rho,
+                           c->stream));
+          b.rho_valid = true;
+          c->stats.kernel_launches += 1;
+        }
+      }
     }
     for (auto& b : c->blk) {
-      if (b.need_rho) {
-        // rho'/rho_bar of the pre-filter state for the next step's first stage (F9 ordering)
-        return fail(c, LEE_ERR_UNSUPPORTED, "non-uniform mean velocity is not supported yet");
-      }
       void** last_out = b.zb[(ns - 1) % 2];
       void** other = b.zb[ns % 2];
       if (c->cfg.filter_scheme != LEE_FILTER_NONE && b.tma_filter) {
@@ -1019,8 +1075,8 @@ int lee_add_boundary(lee_ctx* c, int b, int kind, int dir, int end, const int lo
   if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_add_boundary after lee_prepare");
   if (b < 0 || b >= (int)c->blk.size() || !c->blk[(size_t)b].set) return fail(c, LEE_ERR_STATE, "lee_set_block first");
   BlockData& bk = c->blk[(size_t)b];
-  if (kind != LEE_SPONGE_FREUND_AMBIENT)
-    return fail(c, LEE_ERR_UNSUPPORTED, "boundary kind %d is not supported yet", kind);
+  if (kind != LEE_SPONGE_FREUND_AMBIENT && kind != LEE_BC_NEUMANN && kind != LEE_BC_WALL_SLIP_KINEMATIC)
+    return fail(c, LEE_ERR_UNSUPPORTED, "boundary kind %d is not supported", kind);
   if (dir < 0 || dir >= c->cfg.num_dim || (end != 0 && end != 1)) return fail(c, LEE_ERR_ARG, "dir/end");
   int dims[3] = {bk.nx, bk.ny, bk.nz};
   Boundary z;
@@ -1030,10 +1086,18 @@ int lee_add_boundary(lee_ctx* c, int b, int kind, int dir, int end, const int lo
     z.lo[d] = lo[d];
     z.hi[d] = hi[d];
   }
+  if (kind != LEE_SPONGE_FREUND_AMBIENT) {
+    // the face's closure row reads S-1 points inward along dir
+    const int S = c->fd.S, f = end == 0 ? lo[dir] : hi[dir];
+    if ((end == 0 && f + S - 1 > dims[dir] - 1) || (end == 1 && f - (S - 1) < 0))
+      return fail(c, LEE_ERR_ARG, "boundary face %d in direction %d lacks the %d points its closure row reads", f,
+                  dir, S);
+  }
   int nzones = 0;
   for (auto& q : bk.bnd) nzones += q.kind == LEE_SPONGE_FREUND_AMBIENT;
-  if (nzones >= kMaxZones) return fail(c, LEE_ERR_UNSUPPORTED, "more than %d sponge zones in a block", kMaxZones);
-  if (sigma) {
+  if (kind == LEE_SPONGE_FREUND_AMBIENT && nzones >= kMaxZones)
+    return fail(c, LEE_ERR_UNSUPPORTED, "more than %d sponge zones in a block", kMaxZones);
+  if (sigma && kind == LEE_SPONGE_FREUND_AMBIENT) {
     size_t nb = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
     z.sigma.assign(sigma, sigma + nb);
   }
@@ -1222,7 +1286,8 @@ int lee_prepare(lee_ctx* c) {
     }
     b.need_rho = 0;
     for (int q = 0; q < 9; ++q) b.need_rho |= c->comp ? !b.cf_gu[q].zero : !b.cd_gu[q].zero;
-    if (b.need_rho) return fail(c, LEE_ERR_UNSUPPORTED, "non-uniform mean velocity is not supported yet");
+    if (b.need_rho && (rc = dev_alloc(c, &b.rho, (size_t)b.N * c->esz))) return rc;
+    b.rho_valid = false;
     // state buffers
     if ((rc = alloc_fields(c, b.y, b.N))) return rc;
     if ((rc = alloc_fields(c, b.acc, b.N))) return rc;
@@ -1236,7 +1301,7 @@ int lee_prepare(lee_ctx* c) {
     const bool rows16 = ((size_t)b.nx * c->esz) % 16 == 0;
     b.tiles_x = (b.nx + kTileX - 1) / kTileX;
     b.tiles_y = (b.ny + kTileY - 1) / kTileY;
-    b.tma = c->wst_ok && !b.has_holes && rows16 && !b.need_rho;
+    b.tma = c->wst_ok && !b.has_holes && rows16;
     b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE;
     if (b.tma) {
       // coefficient-layout traits of the stage kernel
@@ -1280,14 +1345,14 @@ int lee_upload_state(lee_ctx* c, int b, const double* const sol[5], int step, do
     if (!c->comp) {
       CK(cudaMemcpyAsync(bk.y[v], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToDevice, c->stream));
     } else {
-      k_convert<float><<<grid1d(bk.N), 256, 0, c->stream>>>(bk.N, (float*)bk.y[v], tmp);
+      k_split<<<grid1d(bk.N), 256, 0, c->stream>>>(bk.N, (float*)bk.y[v], (float*)bk.comp[v], tmp);
       CK(cudaGetLastError());
-      CK(cudaMemsetAsync(bk.comp[v], 0, (size_t)bk.N * 4, c->stream));
     }
   }
   CK(cudaFreeAsync(tmp, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   (void)rc;
+  bk.rho_valid = false;  // the first stage takes rho'/rho_bar from the uploaded state
   c->step = step;
   c->time = time;
   c->uploaded = true;
@@ -1398,6 +1463,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     fill_stage_common<double>(c, bk, p);
     p.stage = -1;
     p.src_amp = c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, time) : 0.0;
+    p.rho_prev = bk.rho_valid ? (const double*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const double*)bk.y[v];
       p.zout[v] = (double*)bk.zb[0][v];
@@ -1411,6 +1477,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     fill_stage_common<float>(c, bk, p);
     p.stage = -1;
     p.src_amp = (float)(c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, time) : 0.0);
+    p.rho_prev = bk.rho_valid ? (const float*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const float*)bk.y[v];
       p.zout[v] = (float*)bk.zb[0][v];
@@ -1434,6 +1501,16 @@ int lee_apply_filter(lee_ctx* c) {
   if (c->cfg.filter_scheme == LEE_FILTER_NONE) return LEE_OK;
   CK(cudaSetDevice(c->cfg.device));
   for (auto& b : c->blk) {
+    if (b.need_rho && !b.rho_valid) {
+      // the auxiliary fields keep describing the state from before the filter
+      if (c->comp)
+        CK(launch_rho<float>(b.N, c->V, (float* const*)b.y, (float* const*)b.comp, b.d_mean[4], c->cfg.gamma,
+                             (float*)b.rho, c->stream));
+      else
+        CK(launch_rho<double>(b.N, c->V, (double* const*)b.y, nullptr, b.d_mean[4], c->cfg.gamma, (double*)b.rho,
+                              c->stream));
+      b.rho_valid = true;
+    }
     if (b.tma_filter) {
       // y (and its carried error) -> zb[0], then the buffers swap roles
       int rc = c->comp ? launch_filter_fused<float>(c, b, b.y, b.comp, b.zb[0], b.comp)

@@ -71,8 +71,8 @@ struct StageParams {
   Coef<T> ubar[3], pbar, rhobar_inv;
   Coef<T> gs[3], gu[9], gp[3];  // mean gradients: d s_bar/dx_j, d u_bar_i/dx_j at i*3+j, d p_bar/dx_j
   int need_rho;                 // 1 when some d u_bar_i/dx_j is nonzero
-  const T* rho_prev;            // rho'/rho_bar from the previous step's last stage (stage 0 input)
-  T* rho_next;                  // written on the last stage
+  const T* rho_prev;            // rho'/rho_bar of the previous step's pre-filter state, read by the
+                                // first stage and by a right-hand-side evaluation (null: from q)
   T gamma, inv_gamma;
   // sponges: per zone (generic kernels) or summed into one per-point field (TMA kernels)
   int nzones;
@@ -105,6 +105,30 @@ struct FilterParams {
   const int* iblank;
   OpTable op;
 };
+
+// One BC line applied to a stage output (lee_bc.cu).
+template <typename T>
+struct BcParams {
+  int kind, dir, end, nd, V;
+  int lo[3], nb[3];           // the end face of the line's box (nb[dir] = 1)
+  int nx, ny;
+  long long sd;               // index stride along dir
+  int S;                      // closure row width
+  double c0[9];               // row 0 of the difference operator's left closure
+  T* y[kMaxVars];
+  T* e[kMaxVars];             // rounding errors of a compensated pair, or null
+  const double* met[9];       // metrics, inverse metrics and Jacobian (slip wall)
+  const double* minv[9];
+  const double* jac;
+  const int* iblank;
+};
+
+template <typename T>
+cudaError_t launch_bc(const BcParams<T>& p, cudaStream_t s);
+// out = p'/(gamma p_bar) - s' of the state y (+ e when e is non-null)
+template <typename T>
+cudaError_t launch_rho(long long n, int V, T* const* y, T* const* e, const double* pbar, double gamma, T* out,
+                       cudaStream_t s);
 
 // lee_step.cu
 template <typename T>

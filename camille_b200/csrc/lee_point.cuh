@@ -141,7 +141,7 @@ __device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, long lon
   }
   T rr = T(0);
   if (p.need_rho) {
-    if (p.stage == 0 && p.rho_prev) {
+    if (p.stage <= 0 && p.rho_prev) {
       rr = p.rho_prev[l];
     } else {
       rr = q[P] * p.inv_gamma * (T(1) / cval(p.pbar, l)) - q[0];

@@ -32,6 +32,11 @@ WORKLOADS = {
     "pulse2d_48": lambda: cases.pulse2d(n=48, length=47 * 100.0 / 255.0, sponge=8, nsteps=20),
     # 3-D curvilinear, Mach 0.5, closures only (the 256^3 workload at 16^3)
     "curvi3d_16": lambda: cases.curvi3d(n=16, seed=2, npulses=8, nsteps=5, halfwidth=2.0),
+    # 2-D shear layer over a bumped slip wall, Neumann top, sponges at both x ends: the
+    # boundary conditions and every non-uniform mean term (rho'/rho_bar included)
+    "shear2d_40x32": lambda: cases.shear2d(nx=40, ny=32, nsteps=20),
+    # 3-D curvilinear block with a slip wall, a Neumann face and a mean shear
+    "wall3d_14": lambda: cases.wall3d(n=14, nsteps=4),
 }
 
 
@@ -57,5 +62,5 @@ def make(name: str) -> str:
 if __name__ == "__main__":
     if not run_ref.available():
         sys.exit("build the reference first: python oracle/build_ref.py")
-    for n in WORKLOADS:
+    for n in (sys.argv[1:] or WORKLOADS):
         print(make(n))

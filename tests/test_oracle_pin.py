@@ -15,7 +15,7 @@ import pytest
 from camille_b200 import api, cases
 from tests.conftest import golden_case, load_golden
 
-NAMES = ["pulse2d_48", "curvi3d_16"]
+NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14"]
 
 
 @pytest.mark.parametrize("name", NAMES)

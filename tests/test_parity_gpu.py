@@ -15,7 +15,7 @@ from camille_b200 import api, cases
 from tests.conftest import golden_case, load_golden
 
 pytestmark = pytest.mark.gpu
-NAMES = ["pulse2d_48", "curvi3d_16"]
+NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14"]
 
 
 def rl2(a, b):
@@ -76,7 +76,10 @@ def _larger():
     c.fd_scheme, c.filter_scheme, c.filter_strength = "FDO11P", "SFO11P", 0.2
     d = cases.pulse2d(n=64, length=63 * 100.0 / 255.0, sponge=10, nsteps=10)
     d.rk, d.filter_order, d.filter_blend = "RUNGE_KUTTA2", 4, 0.6
-    return {"pulse2d_128": a, "curvi3d_40": b, "fdo11p_3d_24": c, "rk2_2d_64": d}
+    e = cases.shear2d(nx=130, ny=96, nsteps=40)
+    f = cases.wall3d(n=40, nsteps=8, halfwidth=3.0)
+    return {"pulse2d_128": a, "curvi3d_40": b, "fdo11p_3d_24": c, "rk2_2d_64": d, "shear2d_130x96": e,
+            "wall3d_40": f}
 
 
 @pytest.mark.parametrize("label", list(_larger().keys()))
@@ -98,7 +101,7 @@ def test_fp64_matches_oracle(product_lib, oracle_lib, label):
     assert rl2(yp, yo) <= 1e-10
 
 
-@pytest.mark.parametrize("label", ["pulse2d_128", "curvi3d_40"])
+@pytest.mark.parametrize("label", ["pulse2d_128", "curvi3d_40", "shear2d_130x96", "wall3d_40"])
 def test_fp32_compensated_error_vs_oracle(product_lib, oracle_lib, label):
     case = _larger()[label]
     o = api.Solver(oracle_lib, case)
@@ -108,3 +111,21 @@ def test_fp32_compensated_error_vs_oracle(product_lib, oracle_lib, label):
     p.advance(case.nsteps, dt)
     err = rl2(p.download(0)[0][4], o.download(0)[0][4])
     assert err <= 1e-5, err
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+def test_rho_ratio_follows_the_pre_filter_state(product_lib, oracle_lib, precision):
+    """With a sheared mean the right-hand side reads rho'/rho_bar, which the reference
+    recomputes after each boundary update and not after the filter: a right-hand side taken
+    after a step, or after a filter call, sees the pre-filter state."""
+    tol = 1e-12 if precision == api.FP64 else 1e-5
+    case = cases.shear2d(nx=48, ny=40, nsteps=3)
+    o = api.Solver(oracle_lib, case)
+    p = api.Solver(product_lib, case, precision=precision)
+    o.apply_filter()
+    p.apply_filter()
+    assert rl2(p.eval_rhs(0, 0.1), o.eval_rhs(0, 0.1)) <= tol
+    dt = o.compute_dt()
+    o.advance(case.nsteps, dt)
+    p.advance(case.nsteps, dt)
+    assert rl2(p.eval_rhs(0, 0.2), o.eval_rhs(0, 0.2)) <= tol
