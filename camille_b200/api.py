@@ -63,6 +63,7 @@ class LeeError(RuntimeError):
 _DP = C.POINTER(C.c_double)
 _IP = C.POINTER(C.c_int)
 _PP = C.POINTER(_DP)
+_LP = C.POINTER(C.c_longlong)
 
 # name -> (restype, argtypes); the first argument of most is the context pointer.
 SIGNATURES = {
@@ -73,6 +74,9 @@ SIGNATURES = {
     "set_mean": (C.c_int, [C.c_void_p, C.c_int, _PP]),
     "add_boundary": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP]),
     "set_source": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
+    "set_overset": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP, _IP, _IP, _IP, _DP, C.c_int, _IP, _IP]),
+    "read_overset_file": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    "get_overset": (C.c_int, [C.c_void_p, _IP, _LP, _IP, _LP, _DP]),
     "prepare": (C.c_int, [C.c_void_p]),
     "upload_state": (C.c_int, [C.c_void_p, C.c_int, _PP, C.c_int, C.c_double]),
     "download_state": (C.c_int, [C.c_void_p, C.c_int, _PP, _IP, _DP]),
@@ -128,7 +132,9 @@ class Solver:
     """A context loaded with one Case: grids, means, boundaries, source and state."""
 
     def __init__(self, lib: Library, case: "_cases.Case", precision: int = FP64, device: int = 0,
-                 upload: bool = True):
+                 upload: bool = True, overset_file: Optional[str] = None):
+        """``overset_file``: read the case's overset maps from this Overture-format file
+        (lee_read_overset_file) instead of passing the arrays (lee_set_overset)."""
         self.lib = lib
         self.case = case
         self.ctx = C.c_void_p()
@@ -159,6 +165,17 @@ class Solver:
             if case.monopole is not None:
                 p = np.array(case.monopole, np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))
+            if overset_file is not None:
+                self._chk(lib.read_overset_file(self.ctx, overset_file.encode(), case.overset.order))
+            elif case.overset is not None:
+                o = case.overset
+                arrs = [np.ascontiguousarray(a, np.int32) for a in
+                        (o.recv_block, o.recv_ijk, o.donor_block, o.donor_ijk, np.asarray(o.width),
+                         o.hole_block, o.hole_ijk)]
+                w = np.ascontiguousarray(o.weights, np.float64)
+                ip = [a.ctypes.data_as(_IP) for a in arrs]
+                self._chk(lib.set_overset(self.ctx, o.num_receivers, ip[0], ip[1], ip[2], ip[3], ip[4], _dptr(w),
+                                          int(o.hole_block.size), ip[5], ip[6]))
             self._chk(lib.prepare(self.ctx))
             if upload:
                 for b, blk in enumerate(case.blocks):
@@ -211,6 +228,19 @@ class Solver:
 
     def apply_filter(self) -> None:
         self._chk(self.lib.apply_filter(self.ctx))
+
+    def get_overset(self) -> dict:
+        """The donor maps the context holds: receiver/donor blocks, linear indices and the
+        normalised weights."""
+        o = self.case.overset
+        n = o.num_receivers if o is not None else 0
+        W = int(np.prod(o.width)) if o is not None else 1
+        rb = np.zeros(n, np.int32); db = np.zeros(n, np.int32)
+        rl = np.zeros(n, np.int64); dl = np.zeros(n, np.int64)
+        wt = np.zeros((n, W), np.float64)
+        self._chk(self.lib.get_overset(self.ctx, rb.ctypes.data_as(_IP), rl.ctypes.data_as(_LP),
+                                       db.ctypes.data_as(_IP), dl.ctypes.data_as(_LP), _dptr(wt)))
+        return {"recv_block": rb, "recv_l0": rl, "donor_block": db, "donor_l0": dl, "weights": wt}
 
     def get_setup(self, b: int, what: int) -> np.ndarray:
         nx, ny, nz = self.case.blocks[b].dims

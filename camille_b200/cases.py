@@ -30,6 +30,7 @@ from typing import Optional
 
 import numpy as np
 
+from . import overset as overset_mod
 from . import plot3d
 
 BC_TYPES = {
@@ -98,6 +99,7 @@ class Case:
     sponge_order: int = 2
     sponge_constant: float = 5.0
     monopole: Optional[tuple[float, float, float, float, float, float, float]] = None
+    overset: Optional["overset_mod.OversetMap"] = None
     notes: str = ""
 
     @property
@@ -136,12 +138,21 @@ class Case:
         lines += [
             f"BUFFER_ZONE POLYNOMIAL_ORDER = {self.sponge_order}, CONSTANT = {self.sponge_constant!r}",
             "METRIC_SCHEME = THOMAS_LOMBARD",
-            "OVERSET = NONE",
+        ]
+        if self.overset is None:
+            lines.append("OVERSET = NONE")
+        else:
+            lines.append(f"OVERSET = OVERTURE, TYPE = EXPLICIT, ORDER_ACCURACY = {self.overset.order}")
+        lines += [
             "DOMAIN_DECOMPOSITION = DECOMP_1D",
             "FILE_FORMAT = PLOT3D",
             f"GRID_FILE = {grid}",
             f"BASESTATE_FILE = {mean}",
             f"BC_FILE = {bc}",
+        ]
+        if self.overset is not None:
+            lines.append(f"OVERSET_FILE = {os.path.join(os.path.dirname(bc), 'overset.bin')}")
+        lines += [
             "SOLUTION_WRITING_TIME = 1.0E+300",
             "HARMONIC_WAVE = NONE",
             "INTERPOLATE_SOLUTION = NONE",
@@ -157,6 +168,8 @@ class Case:
         plot3d.write_function(mean, [b.mean for b in self.blocks])
         plot3d.write_solution(ic, [b.state for b in self.blocks], step=step, time=time)
         plot3d.write_bc(bc, [bd.line() for bd in self.boundaries])
+        if self.overset is not None:
+            self.overset.write(os.path.join(workdir, "overset.bin"))
         plot3d.write_deck(os.path.join(workdir, "camille.in"), self.deck_lines(dt, nsteps, grid, mean, bc))
         return ic
 
@@ -321,3 +334,135 @@ def wall3d(n: int = 16, nsteps: int = 3, gamma: float = 1.4, halfwidth: float = 
            Boundary(0, "neumann", 0, 1, (m, 0, 0), (m, m, m))]
     return Case(name=f"wall3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
                 notes=f"3-D {n}^3 curvilinear, slip wall zeta=0, Neumann xi=max, shear mean")
+
+
+def _tanh_radii(nr: int, r0: float, r1: float, first: float) -> tuple[np.ndarray, float]:
+    """r(s) = r0 + (r1 - r0) (1 + tanh(d (s - 1)) / tanh d), s = j / (nr - 1), with d chosen so
+    that the first cell is ``first`` wide (one-sided tanh clustering at the wall)."""
+    from scipy.optimize import brentq
+
+    def first_cell(d: float) -> float:
+        return (r1 - r0) * (1.0 + math.tanh(d * (1.0 / (nr - 1) - 1.0)) / math.tanh(d)) - first
+
+    d = brentq(first_cell, 1e-6, 50.0, xtol=1e-15, rtol=1e-15)
+    s = np.arange(nr, dtype=np.float64) / (nr - 1)
+    return r0 + (r1 - r0) * (1.0 + np.tanh(d * (s - 1.0)) / math.tanh(d)), d
+
+
+def cylinder2d(nb: int = 512, length: float = 80.0, ntheta: int = 384, nr: int = 96, r_wall: float = 0.5,
+               r_out: float = 5.0, first_cell: float = 0.005, r_cut: float = 1.5, seam_overlap: float = 8.5,
+               fringe: int = 2, sponge: Optional[int] = None, sponge_constant: float = 5.0,
+               source: tuple[float, float] = (2.0, 0.0), omega: float = 0.8 * math.pi, halfwidth: float = 0.2,
+               amplitude: float = 1e-3, ramp: float = 2.5, nsteps: int = 4000, gamma: float = 1.4,
+               pulse: Optional[tuple[float, float, float, float]] = None) -> Case:
+    """Two-block overset workload: a Cartesian background (block 0, nb x nb on [-L/2, L/2]^2)
+    and a body-fitted O-grid (block 1, ntheta x nr) around a cylinder of radius ``r_wall``,
+    radii clustered at the wall by a one-sided tanh (first cell ``first_cell``) out to ``r_out``.
+
+    The reference has no periodic boundary, so the O-grid wraps past 2 pi by ``seam_overlap``
+    cells: its first and last ``fringe`` theta lines are receivers donated by the O-grid's
+    own interior across the seam. The background is blanked inside ``r_cut`` and its
+    ``fringe`` layers of points next to the hole are receivers donated by the O-grid; the
+    O-grid's outer ``fringe`` rings are receivers donated by the background. Donor stencils
+    are 4 x 4 Lagrange (``ORDER_ACCURACY = 3``) in the donor's computational coordinates.
+
+    Mean flow: the parallel shear layer u_bar = 0.15 (1 + tanh 2y) (Mach units, c = 1:
+    rho_bar = 1, p_bar = 1/gamma) on both blocks. Source: monopole at ``source`` with
+    angular frequency ``omega``, Gaussian half-width ``halfwidth`` and a sin^2 ramp over
+    ``ramp``. BC lines: slip wall on the cylinder (O-grid eta = 0) and Freund sponges on the
+    background's four sides (``sponge`` cells, default 20 at nb = 512). The initial state is
+    zero, or a Gaussian p' pulse ``pulse`` = (x0, y0, amplitude, half-width) on both blocks."""
+    # background
+    dx = length / (nb - 1)
+    c1 = -0.5 * length + dx * np.arange(nb, dtype=np.float64)
+    yb, xb = np.meshgrid(c1, c1, indexing="ij")
+    # O-grid: theta decreases with i so that the mapping is right-handed (positive Jacobian)
+    period = ntheta - 1 - seam_overlap
+    dth = 2.0 * math.pi / period
+    radii, delta = _tanh_radii(nr, r_wall, r_out, first_cell)
+    th = -dth * np.arange(ntheta, dtype=np.float64)
+    xo = radii[:, None] * np.cos(th)[None, :]
+    yo = radii[:, None] * np.sin(th)[None, :]
+
+    def block(x2: np.ndarray, y2: np.ndarray) -> Block:
+        x, y = x2[None].copy(), y2[None].copy()
+        mean = np.zeros((5,) + x.shape)
+        mean[1] = 0.15 * (1.0 + np.tanh(2.0 * y))
+        mean[4] = 1.0 / gamma
+        return Block(x, y, np.zeros_like(x), mean, np.zeros((5,) + x.shape))
+
+    bg, og = block(xb, yb), block(xo, yo)
+    if pulse is not None:
+        px, py, pa, pb = pulse
+        for blk in (bg, og):
+            blk.state[4] = pa * _gauss((blk.x - px) ** 2 + (blk.y - py) ** 2, pb)
+
+    # background hole and fringe
+    ib_bg = np.zeros((nb, nb), np.int32)
+    hole = np.hypot(xb, yb) < r_cut
+    ib_bg[hole] = overset_mod.BLANKED
+    near = np.zeros_like(hole)
+    hj, hi = np.nonzero(hole)
+    for dj in range(-fringe, fringe + 1):
+        for di in range(-fringe, fringe + 1):
+            jj, ii = np.clip(hj + dj, 0, nb - 1), np.clip(hi + di, 0, nb - 1)
+            near[jj, ii] = True
+    recv_bg = near & ~hole
+    ib_bg[recv_bg] = overset_mod.INTERPOLATED
+    # O-grid receivers: outer rings, then the seam lines
+    recv_og = np.zeros((nr, ntheta), bool)
+    recv_og[nr - fringe:, :] = True
+    seam = np.zeros_like(recv_og)
+    seam[:nr - fringe, :fringe] = True
+    seam[:nr - fringe, ntheta - fringe:] = True
+    recv_og |= seam
+
+    def inv_bg(x: float, y: float):
+        return [((x + 0.5 * length) / dx, (y + 0.5 * length) / dx)]
+
+    tanh_d = math.tanh(delta)
+
+    def inv_og(x: float, y: float):
+        r = math.hypot(x, y)
+        t = ((r - r_wall) / (r_out - r_wall) - 1.0) * tanh_d
+        if not (-1.0 < t <= 0.0):
+            return []
+        eta = (nr - 1) * (1.0 + math.atanh(t) / delta)
+        xi = ((-math.atan2(y, x)) % (2.0 * math.pi)) / dth
+        return [(xi, eta), (xi + period, eta), (xi - period, eta)]
+
+    donors = [overset_mod.DonorGrid((nb, nb), inv_bg, ib_bg == overset_mod.NOTBLANKED),
+              overset_mod.DonorGrid((ntheta, nr), inv_og, ~recv_og)]
+    rb, rijk, db, dijk, wts = [], [], [], [], []
+
+    def add(block_id: int, mask: np.ndarray, xs: np.ndarray, ys: np.ndarray, donor_of) -> None:
+        jj, ii = np.nonzero(mask)
+        order = np.lexsort((ii, jj))  # i fastest
+        for q in order:
+            j, i = int(jj[q]), int(ii[q])
+            d = donor_of(i, j)
+            found = overset_mod.find_donor(donors[d], float(xs[j, i]), float(ys[j, i]))
+            if found is None:
+                raise ValueError(f"no donor stencil for block {block_id} point ({i}, {j}) in block {d}")
+            i0, j0, w = found
+            rb.append(block_id); rijk.append((i, j, 0)); db.append(d); dijk.append((i0, j0, 0)); wts.append(w)
+
+    add(0, recv_bg, xb, yb, lambda i, j: 1)
+    add(1, recv_og, xo, yo, lambda i, j: 0 if j >= nr - fringe else 1)
+    hj, hi = np.nonzero(hole)
+    order = np.lexsort((hi, hj))
+    ovs = overset_mod.OversetMap(
+        num_dim=2, block_points=[nb * nb, ntheta * nr],
+        recv_block=np.asarray(rb, np.int32), recv_ijk=np.asarray(rijk, np.int32),
+        donor_block=np.asarray(db, np.int32), donor_ijk=np.asarray(dijk, np.int32), width=(4, 4, 1),
+        weights=np.asarray(wts, np.float64), hole_block=np.zeros(order.size, np.int32),
+        hole_ijk=np.stack([hi[order], hj[order], np.zeros(order.size, np.int64)], axis=1).astype(np.int32))
+    if sponge is None:
+        sponge = max(4, int(round(20 * nb / 512)))
+    bnd = [Boundary(1, "wall_slip_kinematic", 1, 0, (0, 0, 0), (ntheta - 1, 0, 0))]
+    bnd += sponge_frame(2, bg.dims, sponge, block=0) if sponge > 0 else []
+    return Case(name=f"cylinder2d_{nb}_{ntheta}x{nr}", num_dim=2, blocks=[bg, og], gamma=gamma, nsteps=nsteps,
+                boundaries=bnd, sponge_constant=sponge_constant, overset=ovs,
+                monopole=(source[0], source[1], 0.0, amplitude, omega, halfwidth, ramp),
+                notes=f"2-D overset: background {nb}^2 on [-{length/2},{length/2}]^2, O-grid {ntheta}x{nr} "
+                      f"r in [{r_wall},{r_out}] first cell {first_cell}, shear layer, monopole at {source}")

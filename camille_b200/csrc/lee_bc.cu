@@ -1,4 +1,5 @@
-// Boundary update of a stage output and the rho'/rho_bar field of the next step's first stage.
+// Boundary update of a stage output (BC lines, then overset interpolation) and the rho'/rho_bar
+// field of the next step's first stage.
 //
 // spatial::update_boundary (camille src/solver/spatial_discretization.cpp:2162-2187) applies
 // bc::apply_BC (src/solver/boundary_condition.cpp:46-209) to the stage output z (or to y_next
@@ -96,6 +97,54 @@ __global__ void k_rho(long long n, const T* ys, const T* yp, const T* es, const 
   }
 }
 
+// overset::interpolate (src/overset/overset.cpp:820-845): compute_weighted_sum (:886-974) sums
+// coeff * y over the stencil, zeta outermost and xi innermost, from 0.0 for every variable;
+// update_each_grid (:1241-1278) overwrites the receivers. One thread per receiver.
+template <typename T, bool PAIR>
+__device__ __forceinline__ double ovs_ld(const OvsParams<T>& p, int b, int v, long long l) {
+  double x = (double)p.y[b][v][l];
+  if (PAIR) x = __dadd_rn(x, (double)p.e[b][v][l]);
+  return x;
+}
+
+template <typename T, bool PAIR>
+__device__ __forceinline__ void ovs_st(const OvsParams<T>& p, int b, int v, long long l, double x) {
+  const T r = (T)x;
+  p.y[b][v][l] = r;
+  if (PAIR) p.e[b][v][l] = (T)__dsub_rn(x, (double)r);
+}
+
+template <typename T, bool PAIR>
+__global__ void k_ovs_gather(OvsParams<T> p) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.n) return;
+  const int d = p.db[r];
+  const long long nx = p.nx[d], nxy = nx * p.ny[d];
+  const long long base = p.dl[r];
+  const double* cf = p.wt + (long long)r * p.W;
+  double acc[kMaxVars] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  int st = 0;
+  for (int w3 = 0; w3 < p.w[2]; ++w3)
+    for (int w2 = 0; w2 < p.w[1]; ++w2)
+      for (int w1 = 0; w1 < p.w[0]; ++w1) {
+        const long long l1 = base + w1 + w2 * nx + w3 * nxy;
+        const double c = cf[st++];
+        for (int v = 0; v < p.V; ++v) acc[v] = __dadd_rn(acc[v], __dmul_rn(c, ovs_ld<T, PAIR>(p, d, v, l1)));
+      }
+  if (p.fused) {
+    for (int v = 0; v < p.V; ++v) ovs_st<T, PAIR>(p, p.rb[r], v, p.rl[r], acc[v]);
+  } else {
+    for (int v = 0; v < p.V; ++v) p.buf[(long long)r * p.V + v] = acc[v];
+  }
+}
+
+template <typename T, bool PAIR>
+__global__ void k_ovs_scatter(OvsParams<T> p) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.n) return;
+  for (int v = 0; v < p.V; ++v) ovs_st<T, PAIR>(p, p.rb[r], v, p.rl[r], p.buf[(long long)r * p.V + v]);
+}
+
 int grid_for(long long n) {
   long long g = (n + 255) / 256;
   return (int)(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
@@ -120,6 +169,22 @@ cudaError_t launch_rho(long long n, int V, T* const* y, T* const* e, const doubl
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_overset(const OvsParams<T>& p, cudaStream_t s) {
+  if (p.n <= 0) return cudaSuccess;
+  const int g = (p.n + 127) / 128;
+  if (p.pair) {
+    k_ovs_gather<T, true><<<g, 128, 0, s>>>(p);
+    if (!p.fused) k_ovs_scatter<T, true><<<g, 128, 0, s>>>(p);
+  } else {
+    k_ovs_gather<T, false><<<g, 128, 0, s>>>(p);
+    if (!p.fused) k_ovs_scatter<T, false><<<g, 128, 0, s>>>(p);
+  }
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_overset<double>(const OvsParams<double>&, cudaStream_t);
+template cudaError_t launch_overset<float>(const OvsParams<float>&, cudaStream_t);
 template cudaError_t launch_bc<double>(const BcParams<double>&, cudaStream_t);
 template cudaError_t launch_bc<float>(const BcParams<float>&, cudaStream_t);
 template cudaError_t launch_rho<double>(long long, int, double* const*, double* const*, const double*, double, double*,

@@ -16,7 +16,9 @@
 #include <utility>
 #include <vector>
 
+#include <algorithm>
 #include <map>
+#include <memory>
 
 #include "lee_internal.h"
 #include "lee_tma.h"
@@ -55,7 +57,8 @@ struct BlockData {
   int* d_iblank = nullptr;
   int8_t* d_code_fd[3] = {};
   int8_t* d_code_flt[3] = {};
-  bool has_holes = false;
+  bool has_holes = false;   // some point is BLANKED: hole closures and hole bypass
+  bool has_iblank = false;  // some point is not NOTBLANKED (holes or receivers): CFL skips them
   // monopole factor on a box
   int src_lo[3] = {0, 0, 0}, src_hi[3] = {-1, -1, -1};
   double* d_src_g = nullptr;
@@ -131,6 +134,17 @@ struct lee_ctx {
   int hf = 0;
   bool wst_ok = false, wfl_ok = false;
   int* d_err = nullptr;
+  // overset maps (host copies, then device arrays from lee_prepare)
+  struct {
+    int n = 0, W = 1, w[3] = {1, 1, 1};
+    bool fused = false;
+    std::vector<int> rb, db;
+    std::vector<long long> rl, dl;
+    std::vector<double> wt;
+    int *d_rb = nullptr, *d_db = nullptr;
+    long long *d_rl = nullptr, *d_dl = nullptr;
+    double *d_wt = nullptr, *d_buf = nullptr;
+  } ovs;
 };
 
 namespace {
@@ -903,12 +917,38 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
       // boundary update of the stage output (spatial::update_boundary): z, or y_next after the
       // last stage (FP64: the accumulator; compensated: the pair y_pre, e)
       const bool last = s == ns - 1;
+      auto target = [&](BlockData& b) -> void** { return (last && !c->comp) ? b.acc : b.zb[s % 2]; };
+      auto errors = [&](BlockData& b) -> void** { return (last && c->comp) ? b.acc : nullptr; };
       for (auto& b : c->blk) {
-        void** zout = b.zb[s % 2];
-        void** tgt = (last && !c->comp) ? b.acc : zout;
-        void** err = (last && c->comp) ? b.acc : nullptr;
-        int rc = apply_bcs<T>(c, b, tgt, err);
+        int rc = apply_bcs<T>(c, b, target(b), errors(b));
         if (rc) return rc;
+      }
+      // overset interpolation over all blocks, from their post-BC values (overset::interpolate)
+      if (c->ovs.n > 0) {
+        OvsParams<T> op;
+        memset(&op, 0, sizeof op);
+        op.n = c->ovs.n; op.W = c->ovs.W; op.V = c->V; op.fused = c->ovs.fused ? 1 : 0;
+        for (int d = 0; d < 3; ++d) op.w[d] = c->ovs.w[d];
+        op.rb = c->ovs.d_rb; op.rl = c->ovs.d_rl; op.db = c->ovs.d_db; op.dl = c->ovs.d_dl;
+        op.wt = c->ovs.d_wt; op.buf = c->ovs.d_buf;
+        op.pair = (last && c->comp) ? 1 : 0;
+        for (size_t bi = 0; bi < c->blk.size(); ++bi) {
+          BlockData& b = c->blk[bi];
+          void** t = target(b);
+          void** e = errors(b);
+          for (int v = 0; v < c->V; ++v) {
+            op.y[bi][v] = (T*)t[v];
+            op.e[bi][v] = e ? (T*)e[v] : nullptr;
+          }
+          op.nx[bi] = b.nx;
+          op.ny[bi] = b.ny;
+        }
+        CK(launch_overset<T>(op, c->stream));
+        c->stats.kernel_launches += op.fused ? 1 : 2;
+      }
+      for (auto& b : c->blk) {
+        void** tgt = target(b);
+        void** err = errors(b);
         if (last && b.need_rho) {
           // rho'/rho_bar of the pre-filter state, read by the next step's first stage: the
           // reference recomputes its auxiliary fields after the boundary update and not after
@@ -1042,12 +1082,13 @@ int lee_set_block(lee_ctx* c, int b, int nx, int ny, int nz, const double* x, co
   bk.hy.assign(y, y + bk.N);
   bk.hz.assign(z, z + bk.N);
   bk.hib.clear();
-  bk.has_holes = false;
+  bk.has_holes = bk.has_iblank = false;
   if (iblank) {
     bk.hib.assign(iblank, iblank + bk.N);
     for (int v : bk.hib) {
       if (v != 0 && v != 1 && v != -1) return fail(c, LEE_ERR_ARG, "iblank values are 0, 1 or -1");
-      if (v != 0) bk.has_holes = true;
+      if (v == 1) bk.has_holes = true;
+      if (v != 0) bk.has_iblank = true;
     }
   }
   bk.set = true;
@@ -1119,6 +1160,172 @@ int lee_set_source(lee_ctx* c, int kind, const double* params, int nparams) {
   return LEE_OK;
 }
 
+int lee_set_overset(lee_ctx* c, int n, const int* recv_block, const int* recv_ijk, const int* donor_block,
+                    const int* donor_ijk, const int width[3], const double* weights, int num_holes,
+                    const int* hole_block, const int* hole_ijk) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_overset after lee_prepare");
+  if (n < 0 || num_holes < 0 || !width) return fail(c, LEE_ERR_ARG, "negative count or null width");
+  if (n > 0 && (!recv_block || !recv_ijk || !donor_block || !donor_ijk || !weights))
+    return fail(c, LEE_ERR_ARG, "null receiver arrays");
+  if (num_holes > 0 && (!hole_block || !hole_ijk)) return fail(c, LEE_ERR_ARG, "null hole arrays");
+  const int nb = (int)c->blk.size();
+  if (nb > kMaxOvsBlocks) return fail(c, LEE_ERR_UNSUPPORTED, "overset over more than %d blocks", kMaxOvsBlocks);
+  for (int d = 0; d < 3; ++d)
+    if (width[d] < 1 || (d >= c->cfg.num_dim && width[d] != 1)) return fail(c, LEE_ERR_ARG, "stencil width");
+  const int W = width[0] * width[1] * width[2];
+  auto& o = c->ovs;
+  // validate everything before touching the blocks
+  for (int q = 0; q < num_holes; ++q) {
+    const int b = hole_block[q];
+    if (b < 0 || b >= nb || !c->blk[(size_t)b].set) return fail(c, LEE_ERR_ARG, "hole %d: block %d", q, b);
+    const BlockData& bk = c->blk[(size_t)b];
+    const int* ijk = hole_ijk + 3 * (size_t)q;
+    if (ijk[0] < 0 || ijk[0] >= bk.nx || ijk[1] < 0 || ijk[1] >= bk.ny || ijk[2] < 0 || ijk[2] >= bk.nz)
+      return fail(c, LEE_ERR_ARG, "hole %d outside its block", q);
+  }
+  std::vector<int> rb((size_t)n), db((size_t)n);
+  std::vector<long long> rl((size_t)n), dl((size_t)n);
+  std::vector<double> wt((size_t)n * W);
+  for (int r = 0; r < n; ++r) {
+    const int b = recv_block[r], d = donor_block[r];
+    if (b < 0 || b >= nb || d < 0 || d >= nb || !c->blk[(size_t)b].set || !c->blk[(size_t)d].set)
+      return fail(c, LEE_ERR_ARG, "receiver %d: block %d or donor block %d", r, b, d);
+    const BlockData &rk = c->blk[(size_t)b], &dk = c->blk[(size_t)d];
+    const int* ri = recv_ijk + 3 * (size_t)r;
+    const int* di = donor_ijk + 3 * (size_t)r;
+    const int rn[3] = {rk.nx, rk.ny, rk.nz}, dn[3] = {dk.nx, dk.ny, dk.nz};
+    for (int q = 0; q < 3; ++q) {
+      if (ri[q] < 0 || ri[q] >= rn[q]) return fail(c, LEE_ERR_ARG, "receiver %d outside its block", r);
+      // the stencil must lie within the donor grid (initialize_donor asserts it, :536-537)
+      if (di[q] < 0 || di[q] + width[q] - 1 >= dn[q])
+        return fail(c, LEE_ERR_ARG, "donor stencil of receiver %d outside block %d", r, d);
+    }
+    rb[(size_t)r] = b;
+    db[(size_t)r] = d;
+    rl[(size_t)r] = ri[0] + (long long)rk.nx * (ri[1] + (long long)rk.ny * ri[2]);
+    dl[(size_t)r] = di[0] + (long long)dk.nx * (di[1] + (long long)dk.ny * di[2]);
+    // normalised by the sum, accumulated left to right (initialize_donor, :516-526)
+    double sum = 0.0;
+    for (int q = 0; q < W; ++q) sum += weights[(size_t)r * W + q];
+    sum = 1.0 / sum;
+    for (int q = 0; q < W; ++q) wt[(size_t)r * W + q] = weights[(size_t)r * W + q] * sum;
+  }
+  // holes BLANKED, then receivers INTERPOLATED (override_iblank_4holeCells / _4interpolatedCells)
+  auto touch = [&](BlockData& bk) {
+    if (bk.hib.empty()) bk.hib.assign((size_t)bk.N, 0);
+  };
+  for (int q = 0; q < num_holes; ++q) {
+    BlockData& bk = c->blk[(size_t)hole_block[q]];
+    touch(bk);
+    const int* ijk = hole_ijk + 3 * (size_t)q;
+    bk.hib[(size_t)(ijk[0] + (long long)bk.nx * (ijk[1] + (long long)bk.ny * ijk[2]))] = 1;
+  }
+  for (int r = 0; r < n; ++r) {
+    BlockData& bk = c->blk[(size_t)rb[(size_t)r]];
+    touch(bk);
+    bk.hib[(size_t)rl[(size_t)r]] = -1;
+  }
+  for (auto& bk : c->blk) {
+    if (bk.hib.empty()) continue;
+    bk.has_holes = bk.has_iblank = false;
+    for (int v : bk.hib) {
+      bk.has_holes |= v == 1;
+      bk.has_iblank |= v != 0;
+    }
+  }
+  o.n = n;
+  o.W = W;
+  for (int d = 0; d < 3; ++d) o.w[d] = width[d];
+  o.rb.swap(rb); o.db.swap(db); o.rl.swap(rl); o.dl.swap(dl); o.wt.swap(wt);
+  return LEE_OK;
+}
+
+int lee_read_overset_file(lee_ctx* c, const char* path, int order_accuracy) {
+  if (!c || !path) return LEE_ERR_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(c, LEE_ERR_ARG, "cannot open overset file %s", path);
+  std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
+  auto rd = [&](void* p, size_t sz, size_t n) { return n == 0 || fread(p, sz, n, f) == n; };
+  int nd = 0, nb = 0;
+  if (!rd(&nd, 4, 1) || !rd(&nb, 4, 1)) return fail(c, LEE_ERR_ARG, "short overset file");
+  if (nd != c->cfg.num_dim || nb != (int)c->blk.size())
+    return fail(c, LEE_ERR_ARG, "overset file has %d dimensions and %d blocks", nd, nb);
+  std::vector<int> cnt((size_t)nb);
+  for (int b = 0; b < nb; ++b) {
+    int np = 0;
+    if (!rd(&np, 4, 1)) return fail(c, LEE_ERR_ARG, "short overset file");
+    if (!c->blk[(size_t)b].set || np != c->blk[(size_t)b].N)
+      return fail(c, LEE_ERR_ARG, "overset file: block %d has %d points", b, np);
+  }
+  if (!rd(cnt.data(), 4, (size_t)nb)) return fail(c, LEE_ERR_ARG, "short overset file");
+  long long R = 0;
+  for (int v : cnt) {
+    if (v < 0) return fail(c, LEE_ERR_ARG, "overset file: negative receiver count");
+    R += v;
+  }
+  if (R > (1LL << 30)) return fail(c, LEE_ERR_ARG, "overset file: too many receivers");
+  std::vector<int> rb((size_t)R), db((size_t)R), rijk((size_t)R * 3, 0), dijk((size_t)R * 3, 0);
+  if (!rd(rb.data(), 4, (size_t)R)) return fail(c, LEE_ERR_ARG, "short overset file");
+  for (long long r = 0; r < R; ++r)
+    if (!rd(&rijk[(size_t)r * 3], 4, (size_t)nd)) return fail(c, LEE_ERR_ARG, "short overset file");
+  if (!rd(db.data(), 4, (size_t)R)) return fail(c, LEE_ERR_ARG, "short overset file");
+  for (long long r = 0; r < R; ++r)
+    if (!rd(&dijk[(size_t)r * 3], 4, (size_t)nd)) return fail(c, LEE_ERR_ARG, "short overset file");
+  int width[3] = {1, 1, 1};
+  std::vector<double> wt;
+  size_t base = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (!rd(width, 4, 3)) return fail(c, LEE_ERR_ARG, "short overset file");
+    for (int d = 0; d < nd; ++d)
+      if (width[d] - 1 != order_accuracy)  // overture.cpp:609
+        return fail(c, LEE_ERR_ARG, "overset stencil width %d does not match order %d", width[d], order_accuracy);
+    for (int d = 0; d < 3; ++d)
+      if (width[d] < 1 || width[d] > 16) return fail(c, LEE_ERR_ARG, "overset stencil width %d", width[d]);
+    const size_t W = (size_t)width[0] * width[1] * width[2];
+    if (wt.empty()) wt.assign((size_t)R * W, 0.0);
+    if (wt.size() != (size_t)R * W) return fail(c, LEE_ERR_UNSUPPORTED, "overset stencil widths differ by block");
+    if (!rd(wt.data() + base * W, 8, (size_t)cnt[(size_t)b] * W)) return fail(c, LEE_ERR_ARG, "short overset file");
+    base += (size_t)cnt[(size_t)b];
+  }
+  std::vector<int> hc((size_t)nb);
+  if (!rd(hc.data(), 4, (size_t)nb)) return fail(c, LEE_ERR_ARG, "short overset file");
+  std::vector<int> hb, hijk;
+  for (int b = 0; b < nb; ++b) {
+    if (hc[(size_t)b] < 0) return fail(c, LEE_ERR_ARG, "overset file: negative hole count");
+    hb.insert(hb.end(), (size_t)hc[(size_t)b], b);
+  }
+  hijk.assign(hb.size() * 3, 0);
+  if (!rd(hijk.data(), 4, hijk.size())) return fail(c, LEE_ERR_ARG, "short overset file");
+  return lee_set_overset(c, (int)R, rb.data(), rijk.data(), db.data(), dijk.data(), width, wt.data(), (int)hb.size(),
+                         hb.data(), hijk.data());
+}
+
+int lee_get_overset(lee_ctx* c, int* recv_block, long long* recv_l0, int* donor_block, long long* donor_l0,
+                    double* weights) {
+  if (!c) return LEE_ERR_ARG;
+  auto& o = c->ovs;
+  const size_t n = (size_t)o.n;
+  if (!c->prepared || n == 0) {
+    // the host copies (no device arrays yet)
+    if (recv_block) std::copy(o.rb.begin(), o.rb.end(), recv_block);
+    if (recv_l0) std::copy(o.rl.begin(), o.rl.end(), recv_l0);
+    if (donor_block) std::copy(o.db.begin(), o.db.end(), donor_block);
+    if (donor_l0) std::copy(o.dl.begin(), o.dl.end(), donor_l0);
+    if (weights) std::copy(o.wt.begin(), o.wt.end(), weights);
+    return LEE_OK;
+  }
+  // what the kernels read
+  CK(cudaSetDevice(c->cfg.device));
+  if (recv_block) CK(cudaMemcpyAsync(recv_block, o.d_rb, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (recv_l0) CK(cudaMemcpyAsync(recv_l0, o.d_rl, n * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  if (donor_block) CK(cudaMemcpyAsync(donor_block, o.d_db, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (donor_l0) CK(cudaMemcpyAsync(donor_l0, o.d_dl, n * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  if (weights) CK(cudaMemcpyAsync(weights, o.d_wt, n * o.W * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return LEE_OK;
+}
+
 int lee_prepare(lee_ctx* c) {
   if (!c) return LEE_ERR_ARG;
   if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare called twice");
@@ -1135,10 +1342,13 @@ int lee_prepare(lee_ctx* c) {
     for (int v = 0; v < 5; ++v)
       if ((rc = upload(c, &b.d_mean[v], b.hmean[v]))) return rc;
     if ((rc = compute_metrics(c, b))) return rc;
-    // hole closures
-    if (b.has_holes) {
+    if (b.has_iblank) {
       if ((rc = dalloc(c, &b.d_iblank, (size_t)N))) return rc;
       CK(cudaMemcpyAsync(b.d_iblank, b.hib.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    // hole closures (receivers alone leave every closure as it is)
+    if (b.has_holes) {
       std::vector<int8_t> code;
       int dims[3] = {b.nx, b.ny, b.nz};
       for (int d = 0; d < dim; ++d) {
@@ -1323,6 +1533,34 @@ int lee_prepare(lee_ctx* c) {
     if ((b.tma || b.tma_filter) && (rc = ensure_encoder(c))) return rc;
     if ((rc = c->comp ? autotune<float>(c, b) : autotune<double>(c, b))) return rc;
   }
+  if (c->ovs.n > 0) {
+    auto& o = c->ovs;
+    const size_t n = (size_t)o.n;
+    if ((rc = dalloc(c, &o.d_rb, n)) || (rc = dalloc(c, &o.d_db, n)) || (rc = dalloc(c, &o.d_rl, n)) ||
+        (rc = dalloc(c, &o.d_dl, n)) || (rc = dalloc(c, &o.d_wt, n * o.W)) || (rc = dalloc(c, &o.d_buf, n * c->V)))
+      return rc;
+    CK(cudaMemcpyAsync(o.d_rb, o.rb.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(o.d_db, o.db.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(o.d_rl, o.rl.data(), n * sizeof(long long), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(o.d_dl, o.dl.data(), n * sizeof(long long), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(o.d_wt, o.wt.data(), n * o.W * sizeof(double), cudaMemcpyHostToDevice, s));
+    // one kernel is enough when no stencil reads a receiver: the sums then cannot see a value
+    // written in the same update
+    o.fused = true;
+    for (size_t r = 0; r < n && o.fused; ++r) {
+      const BlockData& dk = c->blk[(size_t)o.db[r]];
+      if (dk.hib.empty()) continue;
+      for (int w3 = 0; w3 < o.w[2] && o.fused; ++w3)
+        for (int w2 = 0; w2 < o.w[1] && o.fused; ++w2)
+          for (int w1 = 0; w1 < o.w[0]; ++w1) {
+            const long long l1 = o.dl[r] + w1 + (long long)w2 * dk.nx + (long long)w3 * dk.nx * dk.ny;
+            if (dk.hib[(size_t)l1] == -1) {
+              o.fused = false;
+              break;
+            }
+          }
+    }
+  }
   CK(cudaStreamSynchronize(s));
   c->prepared = true;
   return LEE_OK;
@@ -1403,7 +1641,7 @@ int lee_compute_dt(lee_ctx* c, double cfl, double* dt) {
     CK(cudaMemcpyAsync(d_m, b.d_met, 9 * sizeof(double*), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(d_u, b.d_mean + 1, 3 * sizeof(double*), cudaMemcpyHostToDevice, c->stream));
     CK(setup_cfl((int)b.N, c->cfg.num_dim, d_m, b.d_jac, d_u, b.d_mean[4], b.d_mean[0],
-                 b.has_holes ? b.d_iblank : nullptr, c->cfg.gamma, dt0, d_max, c->stream));
+                 b.has_iblank ? b.d_iblank : nullptr, c->cfg.gamma, dt0, d_max, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaFreeAsync(d_m, c->stream));
     CK(cudaFreeAsync(d_u, c->stream));

@@ -123,6 +123,32 @@ struct BcParams {
   const int* iblank;
 };
 
+// Overset interpolation of a stage output over all blocks (lee_bc.cu): receiver r of block
+// rb[r], linear index rl[r], takes the weighted sum of the donor stencil with lower-left
+// corner dl[r] in block db[r] (weights wt[r*W..], zeta outermost, xi innermost). With
+// `fused` (no stencil reads a receiver) the sums are written straight to the receivers;
+// otherwise they go through buf first, as overset::interpolate gathers every sum before it
+// overwrites any receiver.
+constexpr int kMaxOvsBlocks = 8;
+template <typename T>
+struct OvsParams {
+  int n, W, V, fused;
+  int w[3];
+  const int* rb;
+  const long long* rl;
+  const int* db;
+  const long long* dl;
+  const double* wt;
+  double* buf;               // n x V, when not fused
+  T* y[kMaxOvsBlocks][kMaxVars];
+  T* e[kMaxOvsBlocks][kMaxVars];  // compensated pair errors, or null
+  int nx[kMaxOvsBlocks], ny[kMaxOvsBlocks];
+  int pair;
+};
+
+template <typename T>
+cudaError_t launch_overset(const OvsParams<T>& p, cudaStream_t s);
+
 template <typename T>
 cudaError_t launch_bc(const BcParams<T>& p, cudaStream_t s);
 // out = p'/(gamma p_bar) - s' of the state y (+ e when e is non-null)

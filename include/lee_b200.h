@@ -119,6 +119,27 @@ int lee_add_boundary(lee_ctx *ctx, int b, int kind, int dir, int end, const int 
                      const double *sigma);
 /* Physical source (source::apply_physicalSource, src/solver/source.cpp:22-107). */
 int lee_set_source(lee_ctx *ctx, int kind, const double *params, int nparams);
+/* Overset donor maps, replacing overset::initialize_overset (src/overset/overset.cpp:56-84)
+ * with the data of its Overture file (src/io/overture.cpp:473-680). n receivers, grouped by
+ * block in block order: recv_block[r] and recv_ijk[3r..3r+2] (block-level indices), the donor
+ * block and the lower-left corner donor_ijk of its stencil of width[0] x width[1] x width[2]
+ * points, and the stencil weights (width product per receiver, zeta outermost, xi innermost),
+ * which are normalised by their sum as initialize_donor does (:516-526). Holes are set
+ * BLANKED (:683-751), then receivers INTERPOLATED (:755-790). After every boundary update
+ * each receiver is overwritten with its stencil's weighted sum (overset::interpolate,
+ * :820-845). Call after lee_set_block and before lee_prepare. */
+int lee_set_overset(lee_ctx *ctx, int n, const int *recv_block, const int *recv_ijk, const int *donor_block,
+                    const int *donor_ijk, const int width[3], const double *weights, int num_holes,
+                    const int *hole_block, const int *hole_ijk);
+/* Read the Overture overset file as read_overset_at_headrank does (src/io/overture.cpp:473-680;
+ * the stencil width must be order_accuracy + 1, :609), then lee_set_overset. */
+int lee_read_overset_file(lee_ctx *ctx, const char *path, int order_accuracy);
+/* The maps as the time loop holds them (for the donor-map check; no reference counterpart):
+ * per receiver its block and linear index i + nxi (j + neta k), the donor block and the
+ * linear index of the stencil's lower-left corner, and the normalised weights. Any pointer
+ * may be null. Arrays hold n (weights: n times the width product) entries. */
+int lee_get_overset(lee_ctx *ctx, int *recv_block, long long *recv_l0, int *donor_block, long long *donor_l0,
+                    double *weights);
 /* Finish setup on the GPU: metrics, Jacobian, mean gradients (spatial::precompute_something,
  * src/solver/spatial_discretization.cpp:2250-2271), sponge strengths, hole closures,
  * and the per-point coefficient fields the kernels read. */

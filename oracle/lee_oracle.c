@@ -58,6 +58,19 @@ typedef struct {
   bnd_t bnd[MAXBND];
 } blk_t;
 
+/* Overset donor maps as overset::initialize_donor / initialize_receiver hold them
+ * (src/overset/overset.cpp:88-554): per receiver its block and linear index, the donor
+ * block and the linear index of the stencil's lower-left corner, and the weights
+ * normalised by their sum (:516-526), zeta outermost, xi innermost. */
+typedef struct {
+  int n;
+  int *rb, *db;
+  long long *rl, *dl;
+  int w[3], W;
+  double *wt;
+  double *buf; /* n x 5 interpolants */
+} ovs_t;
+
 struct orc_ctx {
   lee_config cfg;
   op_t fd, flt;
@@ -67,6 +80,7 @@ struct orc_ctx {
   double src[7];
   int prepared, step;
   double time;
+  ovs_t ovs;
   char err[512];
 };
 typedef struct orc_ctx orc_ctx;
@@ -596,6 +610,30 @@ static int filter_block(orc_ctx *c, blk_t *bk, double **y) {
   return 0;
 }
 
+/* overset::interpolate (src/overset/overset.cpp:820-845) in its OVERTURE form: every
+ * receiver's weighted sum over its donor stencil, for all five variables
+ * (compute_weighted_sum :886-974), all of them before any receiver is overwritten
+ * (update_each_grid :1241-1278). y[b] is the stage output of block b. */
+static void interpolate(orc_ctx *c, double **y[MAXB]) {
+  ovs_t *o = &c->ovs;
+  for (int r = 0; r < o->n; ++r) {
+    blk_t *dk = &c->blk[o->db[r]];
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double *cf = o->wt + (size_t)r * o->W;
+    int st = 0;
+    for (int w3 = 0; w3 < o->w[2]; ++w3)
+      for (int w2 = 0; w2 < o->w[1]; ++w2)
+        for (int w1 = 0; w1 < o->w[0]; ++w1) {
+          long long l1 = o->dl[r] + (w1 + w2 * dk->nx + (long long)w3 * dk->nx * dk->ny);
+          for (int v = 0; v < 5; ++v) acc[v] += cf[st] * y[o->db[r]][v][l1];
+          st++;
+        }
+    for (int v = 0; v < 5; ++v) o->buf[(size_t)r * 5 + v] = acc[v];
+  }
+  for (int r = 0; r < o->n; ++r)
+    for (int v = 0; v < 5; ++v) y[o->rb[r]][v][o->rl[r]] = o->buf[(size_t)r * 5 + v];
+}
+
 /* ---------------------------------------------------------------------------
  * Exported ABI (orc_ prefix). */
 int orc_create(const lee_config *cfg, orc_ctx **out) {
@@ -633,6 +671,7 @@ void orc_destroy(orc_ctx *c) {
     for (int q = 0; q < 4; ++q) free(bk->aux[q]);
     for (int q = 0; q < bk->nbnd; ++q) free(bk->bnd[q].sigma);
   }
+  free(c->ovs.rb); free(c->ovs.db); free(c->ovs.rl); free(c->ovs.dl); free(c->ovs.wt); free(c->ovs.buf);
   free(c);
 }
 
@@ -685,6 +724,137 @@ int orc_add_boundary(orc_ctx *c, int b, int kind, int dir, int end, const int lo
 int orc_set_source(orc_ctx *c, int kind, const double *params, int np) {
   c->src_kind = kind;
   for (int i = 0; i < 7 && i < np; ++i) c->src[i] = params[i];
+  return LEE_OK;
+}
+
+/* overset::initialize_overset (src/overset/overset.cpp:56-84): the maps of the
+ * Overture file (src/io/overture.cpp:473-680), weights normalised as initialize_donor
+ * does (:516-526), then holes BLANKED (:683-751) and receivers INTERPOLATED (:755-790). */
+int orc_set_overset(orc_ctx *c, int n, const int *recv_block, const int *recv_ijk, const int *donor_block,
+                    const int *donor_ijk, const int width[3], const double *weights, int num_holes,
+                    const int *hole_block, const int *hole_ijk) {
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "set_overset after prepare");
+  if (n < 0 || num_holes < 0) return fail(c, LEE_ERR_ARG, "negative count");
+  int W = width[0] * width[1] * width[2];
+  ovs_t *o = &c->ovs;
+  free(o->rb); free(o->db); free(o->rl); free(o->dl); free(o->wt); free(o->buf);
+  memset(o, 0, sizeof *o);
+  o->rb = (int *)malloc(sizeof(int) * (size_t)(n ? n : 1));
+  o->db = (int *)malloc(sizeof(int) * (size_t)(n ? n : 1));
+  o->rl = (long long *)malloc(sizeof(long long) * (size_t)(n ? n : 1));
+  o->dl = (long long *)malloc(sizeof(long long) * (size_t)(n ? n : 1));
+  o->wt = dalloc((size_t)n * (size_t)W);
+  o->buf = dalloc((size_t)n * 5);
+  for (int d = 0; d < 3; ++d) o->w[d] = width[d];
+  o->W = W;
+  for (int q = 0; q < num_holes; ++q) {
+    int b = hole_block[q];
+    if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_ARG, "hole block");
+    blk_t *bk = &c->blk[b];
+    const int *ijk = hole_ijk + 3 * q;
+    if (ijk[0] < 0 || ijk[0] >= bk->nx || ijk[1] < 0 || ijk[1] >= bk->ny || ijk[2] < 0 || ijk[2] >= bk->nz)
+      return fail(c, LEE_ERR_ARG, "hole outside block");
+    if (!bk->iblank) bk->iblank = (int *)calloc((size_t)bk->N, sizeof(int));
+    bk->iblank[ijk[0] + bk->nx * (ijk[1] + bk->ny * ijk[2])] = BLANKED;
+  }
+  for (int r = 0; r < n; ++r) {
+    int rb = recv_block[r], db = donor_block[r];
+    if (rb < 0 || rb >= c->nblk || db < 0 || db >= c->nblk || !c->blk[rb].set || !c->blk[db].set)
+      return fail(c, LEE_ERR_ARG, "receiver or donor block");
+    blk_t *rk = &c->blk[rb], *dk = &c->blk[db];
+    const int *ri = recv_ijk + 3 * r, *di = donor_ijk + 3 * r;
+    int dn[3] = {dk->nx, dk->ny, dk->nz}, rn[3] = {rk->nx, rk->ny, rk->nz};
+    for (int d = 0; d < 3; ++d) {
+      if (ri[d] < 0 || ri[d] >= rn[d]) return fail(c, LEE_ERR_ARG, "receiver outside block");
+      if (di[d] < 0 || di[d] + width[d] - 1 >= dn[d]) return fail(c, LEE_ERR_ARG, "donor stencil outside block");
+    }
+    o->rb[r] = rb;
+    o->db[r] = db;
+    o->rl[r] = ri[0] + (long long)rk->nx * (ri[1] + (long long)rk->ny * ri[2]);
+    o->dl[r] = di[0] + (long long)dk->nx * (di[1] + (long long)dk->ny * di[2]);
+    double sum = 0.0;
+    for (int q = 0; q < W; ++q) sum += weights[(size_t)r * W + q];
+    sum = 1.0 / sum;
+    for (int q = 0; q < W; ++q) o->wt[(size_t)r * W + q] = weights[(size_t)r * W + q] * sum;
+  }
+  for (int r = 0; r < n; ++r) {
+    blk_t *rk = &c->blk[o->rb[r]];
+    if (!rk->iblank) rk->iblank = (int *)calloc((size_t)rk->N, sizeof(int));
+    rk->iblank[o->rl[r]] = INTERPOLATED;
+  }
+  o->n = n;
+  return LEE_OK;
+}
+
+/* read_overset_at_headrank (src/io/overture.cpp:473-680), then orc_set_overset. */
+int orc_read_overset_file(orc_ctx *c, const char *path, int order_accuracy) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(c, LEE_ERR_ARG, "cannot open %s", path);
+  int rc = LEE_OK, nd = 0, nb = 0, R = 0, H = 0;
+  int *cnt = NULL, *rb = NULL, *rijk = NULL, *db = NULL, *dijk = NULL, *hc = NULL, *hb = NULL, *hijk = NULL;
+  double *wt = NULL;
+  int width[3] = {1, 1, 1};
+#define RD(p, sz, n) do { if (fread((p), (sz), (size_t)(n), f) != (size_t)(n)) { rc = fail(c, LEE_ERR_ARG, "short overset file"); goto done; } } while (0)
+  RD(&nd, 4, 1);
+  RD(&nb, 4, 1);
+  if (nd != c->cfg.num_dim || nb != c->nblk) { rc = fail(c, LEE_ERR_ARG, "overset file dimension/blocks"); goto done; }
+  cnt = (int *)calloc((size_t)nb, sizeof(int));
+  for (int b = 0; b < nb; ++b) {
+    int np;
+    RD(&np, 4, 1);
+    if (np != c->blk[b].N) { rc = fail(c, LEE_ERR_ARG, "overset file points of block %d", b); goto done; }
+  }
+  RD(cnt, 4, nb);
+  for (int b = 0; b < nb; ++b) R += cnt[b];
+  rb = (int *)calloc((size_t)R + 1, sizeof(int));
+  db = (int *)calloc((size_t)R + 1, sizeof(int));
+  rijk = (int *)calloc(3 * (size_t)R + 3, sizeof(int));
+  dijk = (int *)calloc(3 * (size_t)R + 3, sizeof(int));
+  RD(rb, 4, R);
+  for (int r = 0; r < R; ++r) RD(rijk + 3 * r, 4, nd);
+  RD(db, 4, R);
+  for (int r = 0; r < R; ++r) RD(dijk + 3 * r, 4, nd);
+  {
+    int base = 0;
+    for (int b = 0; b < nb; ++b) {
+      RD(width, 4, 3);
+      for (int d = 0; d < nd; ++d)
+        if (width[d] - 1 != order_accuracy) { rc = fail(c, LEE_ERR_ARG, "stencil width vs order"); goto done; }
+      int W = width[0] * width[1] * width[2];
+      if (!wt) wt = dalloc((size_t)R * W + 1);
+      RD(wt + (size_t)base * W, 8, (size_t)cnt[b] * W);
+      base += cnt[b];
+    }
+  }
+  hc = (int *)calloc((size_t)nb, sizeof(int));
+  RD(hc, 4, nb);
+  for (int b = 0; b < nb; ++b) H += hc[b];
+  hb = (int *)calloc((size_t)H + 1, sizeof(int));
+  hijk = (int *)calloc(3 * (size_t)H + 3, sizeof(int));
+  RD(hijk, 4, 3 * (size_t)H);
+  {
+    int q = 0;
+    for (int b = 0; b < nb; ++b)
+      for (int h = 0; h < hc[b]; ++h) hb[q++] = b;
+  }
+  rc = orc_set_overset(c, R, rb, rijk, db, dijk, width, wt, H, hb, hijk);
+#undef RD
+done:
+  fclose(f);
+  free(cnt); free(rb); free(rijk); free(db); free(dijk); free(hc); free(hb); free(hijk); free(wt);
+  return rc;
+}
+
+int orc_get_overset(orc_ctx *c, int *recv_block, long long *recv_l0, int *donor_block, long long *donor_l0,
+                    double *weights) {
+  ovs_t *o = &c->ovs;
+  for (int r = 0; r < o->n; ++r) {
+    if (recv_block) recv_block[r] = o->rb[r];
+    if (recv_l0) recv_l0[r] = o->rl[r];
+    if (donor_block) donor_block[r] = o->db[r];
+    if (donor_l0) donor_l0[r] = o->dl[r];
+  }
+  if (weights) memcpy(weights, o->wt, sizeof(double) * (size_t)o->n * (size_t)o->W);
   return LEE_OK;
 }
 
@@ -825,10 +995,12 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
           }
         }
       }
+      double **tgts[MAXB];
       for (int b = 0; b < nb; ++b) { /* spatial::update_boundary (:2162-2187), then aux */
-        double **tgt = (s < ns - 1) ? zi[b] : ynext[b];
-        apply_bc(c, &c->blk[b], tgt);
+        tgts[b] = (s < ns - 1) ? zi[b] : ynext[b];
+        apply_bc(c, &c->blk[b], tgts[b]);
       }
+      if (c->ovs.n > 0) interpolate(c, tgts);
       for (int b = 0; b < nb; ++b) compute_aux(c, &c->blk[b], (s < ns - 1) ? zi[b] : ynext[b]);
     }
     for (int b = 0; b < nb && !rc; ++b) {

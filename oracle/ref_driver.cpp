@@ -10,10 +10,11 @@
 // LEE auxiliaries, src/core/state.cpp:701-736).
 //
 // Controlled by environment variables (argv[1] stays the reference's restart file):
-//   ORACLE_MODE = run | rhs | filter | setup | step1   (default run)
+//   ORACLE_MODE = run | rhs | filter | setup | overset   (default run)
 //   ORACLE_DUMP = path prefix; each rank writes <prefix>.<rank>.bin
-// Dump layout: int32 magic 0x4C454531, block id, iso_in_parent[3], n_dir[3],
-// nfields, time_step; float64 time_sol, dt; then nfields x N float64 fields,
+// Dump layout: int32 magic 0x4C454532, block id, iso_in_parent[3], n_dir[3],
+// nfields, time_step, is[3], ie[3] (the points this rank owns, local indices
+// without ghost cells); float64 time_sol, dt; then nfields x N float64 fields,
 // i fastest (the reference's idx1D, src/geometry/geometry.h:131-136).
 //
 // The reference exits 0 on fatal errors (src/parallel/parallel.cpp:78-96), so
@@ -26,6 +27,7 @@
 #include <vector>
 
 #include "core/simulation.h"
+#include "overset/overset.h"
 
 namespace {
 
@@ -38,14 +40,16 @@ void dump(const char *prefix, const std::vector<double *> &fields) {
     std::fprintf(stderr, "oracle driver: cannot open %s\n", path.c_str());
     std::exit(3);
   }
-  int hdr[10];
-  hdr[0] = 0x4C454531;
+  int hdr[16];
+  hdr[0] = 0x4C454532;
   hdr[1] = g->id_parent;
   for (int d = 0; d < 3; ++d) hdr[2 + d] = g->iso_in_parent[d];
   for (int d = 0; d < 3; ++d) hdr[5 + d] = g->num_ocells_dir[d];
   hdr[8] = (int)fields.size();
   hdr[9] = simulation::state.time_step;
-  std::fwrite(hdr, sizeof(int), 10, f);
+  for (int d = 0; d < 3; ++d) hdr[10 + d] = g->is[d];
+  for (int d = 0; d < 3; ++d) hdr[13 + d] = g->ie[d];
+  std::fwrite(hdr, sizeof(int), 16, f);
   double td[2] = {simulation::state.time_sol, temporal::dt};
   std::fwrite(td, sizeof(double), 2, f);
   for (double *p : fields) std::fwrite(p, sizeof(double), (size_t)g->num_ocells, f);
@@ -119,6 +123,31 @@ int main(int argc, char *argv[]) {
     if (mpi::irank == 0)
       std::printf("ORACLE_SETUP {\"num_dim\": %d, \"n_mean_grad\": %d, \"n_aux\": %d, \"zones\": %d}\n", nd,
                   st.num_vars_mean * nd, st.num_vars_aux, g->num_bufferZones);
+  } else if (mode == "overset") {
+    // the donor and receiver maps this rank holds after overset::initialize_overset
+    // (src/overset/overset.cpp:436-554): <prefix>.<rank>.ovs with int32 block id, int32
+    // number of donor cells, per donor cell int32 l0, int32 num_coeffs and float64 coeffs
+    // (normalised), then int32 number of receiver cells and their int32 l0
+    if (prefix) {
+      std::string path = std::string(prefix) + "." + std::to_string(mpi::irank) + ".ovs";
+      FILE *f = std::fopen(path.c_str(), "wb");
+      if (!f) return 3;
+      int hdr[2] = {g->id_parent, overset::num_donorCells_in_this_grid};
+      std::fwrite(hdr, sizeof(int), 2, f);
+      for (int d = 0; d < overset::num_donorCells_in_this_grid; ++d) {
+        int rec[2] = {overset::donorCells[d].l0, overset::donorCells[d].num_coeffs};
+        std::fwrite(rec, sizeof(int), 2, f);
+        std::fwrite(overset::donorCells[d].coeff, sizeof(double), (size_t)rec[1], f);
+      }
+      int nr = overset::total_num_donorCells_4mygrid;
+      std::fwrite(&nr, sizeof(int), 1, f);
+      for (int r = 0; r < nr; ++r) std::fwrite(&overset::receiverCells[r].l0, sizeof(int), 1, f);
+      std::fclose(f);
+    }
+    std::vector<double> ib((size_t)N);
+    for (int l = 0; l < N; ++l) ib[(size_t)l] = (double)g->cell[l].iblank;
+    std::vector<double *> f(1, ib.data());
+    dump(prefix, f);
   } else {
     std::fprintf(stderr, "oracle driver: unknown ORACLE_MODE %s\n", mode.c_str());
     return 2;

@@ -24,8 +24,8 @@ def available() -> bool:
 
 def read_dump(path: str) -> dict:
     with open(path, "rb") as f:
-        hdr = np.fromfile(f, "<i4", 10)
-        if int(hdr[0]) != 0x4C454531:
+        hdr = np.fromfile(f, "<i4", 16)
+        if int(hdr[0]) != 0x4C454532:
             raise ValueError(f"{path}: bad oracle dump magic")
         td = np.fromfile(f, "<f8", 2)
         nd = [int(v) for v in hdr[5:8]]
@@ -33,7 +33,24 @@ def read_dump(path: str) -> dict:
         nf = int(hdr[8])
         data = np.fromfile(f, "<f8", nf * n).reshape(nf, nd[2], nd[1], nd[0])
     return {"block": int(hdr[1]), "offset": [int(v) for v in hdr[2:5]], "dims": nd,
+            "owned": ([int(v) for v in hdr[10:13]], [int(v) for v in hdr[13:16]]),
             "step": int(hdr[9]), "time": float(td[0]), "dt": float(td[1]), "fields": data}
+
+
+def read_ovs(path: str) -> dict:
+    """The donor/receiver maps one rank held (ORACLE_MODE=overset of ref_driver.cpp)."""
+    with open(path, "rb") as f:
+        block, nd = (int(v) for v in np.fromfile(f, "<i4", 2))
+        dl0, coeffs = [], []
+        for _ in range(nd):
+            l0, nc = (int(v) for v in np.fromfile(f, "<i4", 2))
+            dl0.append(l0)
+            coeffs.append(np.fromfile(f, "<f8", nc))
+        nr = int(np.fromfile(f, "<i4", 1)[0])
+        rl0 = np.fromfile(f, "<i4", nr)
+    return {"block": block, "donor_l0": np.asarray(dl0, np.int64),
+            "weights": np.asarray(coeffs) if coeffs else np.zeros((0, 0)),
+            "recv_l0": rl0.astype(np.int64)}
 
 
 def run(case, mode: str = "run", nsteps: Optional[int] = None, dt: Optional[float] = None,
@@ -73,6 +90,9 @@ def run(case, mode: str = "run", nsteps: Optional[int] = None, dt: Optional[floa
             if line.startswith("ORACLE_RESULT ") or line.startswith("ORACLE_SETUP "):
                 result.update(json.loads(line.split(" ", 1)[1]))
         ranks = [read_dump(os.path.join(wd, f"dump.{r}.bin")) for r in range(nprocs)]
+        if mode == "overset":
+            for r, d in enumerate(ranks):
+                d["overset"] = read_ovs(os.path.join(wd, f"dump.{r}.ovs"))
         return {"ranks": ranks, "result": result, "stdout": out}
     finally:
         if tmp is not None:
@@ -88,8 +108,10 @@ def assemble(case, ranks: list[dict]) -> list[np.ndarray]:
         nf = parts[0]["fields"].shape[0]
         arr = np.full((nf, nz, ny, nx), np.nan)
         for r in parts:
+            # only the points the rank owns: its ghost cells are not time-advanced
+            (i0, j0, k0), (i1, j1, k1) = r["owned"]
             ox, oy, oz = r["offset"]
-            dx, dy, dz = r["dims"]
-            arr[:, oz:oz + dz, oy:oy + dy, ox:ox + dx] = r["fields"]
+            arr[:, oz + k0:oz + k1 + 1, oy + j0:oy + j1 + 1, ox + i0:ox + i1 + 1] = \
+                r["fields"][:, k0:k1 + 1, j0:j1 + 1, i0:i1 + 1]
         out.append(arr)
     return out

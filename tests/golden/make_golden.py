@@ -39,6 +39,14 @@ WORKLOADS = {
     "wall3d_14": lambda: cases.wall3d(n=14, nsteps=4),
 }
 
+# Two-block overset workloads (run on one reference rank per block).
+OVERSET_WORKLOADS = {
+    # the cylinder workload at 64^2 + 72x24: hole cut, fringes, O-grid seam, slip wall,
+    # sponges, shear layer, monopole, and a pulse that crosses the overlap
+    "cylinder2d_64": lambda: cases.cylinder2d(nb=64, length=16.0, ntheta=72, nr=24, r_out=3.0, first_cell=0.05,
+                                              r_cut=1.0, sponge=4, nsteps=40, pulse=(1.8, 0.6, 1e-3, 0.5)),
+}
+
 
 def make(name: str) -> str:
     case = WORKLOADS[name]()
@@ -59,8 +67,35 @@ def make(name: str) -> str:
     return out
 
 
+def make_overset(name: str) -> str:
+    """Per block: iblank, the donor and receiver maps the reference holds, one RHS, the
+    FIX_CFL dt, and the state after 1 and after `steps` FIX_DT steps."""
+    case = OVERSET_WORKLOADS[name]()
+    nb = len(case.blocks)
+    ovs = run_ref.run(case, mode="overset", nprocs=nb)["ranks"]
+    rhs = run_ref.assemble(case, run_ref.run(case, mode="rhs", nprocs=nb)["ranks"])
+    first = run_ref.run(case, mode="run", nsteps=1, dt=None, nprocs=nb)
+    dt = float(first["result"]["dt"])
+    step1 = run_ref.assemble(case, run_ref.run(case, mode="run", nsteps=1, dt=dt, nprocs=nb)["ranks"])
+    stepn = run_ref.assemble(case, run_ref.run(case, mode="run", nsteps=case.nsteps, dt=dt, nprocs=nb)["ranks"])
+    arrays = {"dt": np.float64(dt), "nsteps": np.int64(case.nsteps)}
+    for r in ovs:
+        b = r["overset"]["block"]
+        arrays[f"iblank_{b}"] = r["fields"][0]
+        arrays[f"donor_l0_{b}"] = r["overset"]["donor_l0"]
+        arrays[f"weights_{b}"] = r["overset"]["weights"]
+        arrays[f"recv_l0_{b}"] = r["overset"]["recv_l0"]
+    for b in range(nb):
+        arrays[f"rhs_{b}"] = rhs[b]
+        arrays[f"step1_{b}"] = step1[b]
+        arrays[f"stepn_{b}"] = stepn[b]
+    out = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(out, **arrays)
+    return out
+
+
 if __name__ == "__main__":
     if not run_ref.available():
         sys.exit("build the reference first: python oracle/build_ref.py")
-    for n in (sys.argv[1:] or WORKLOADS):
-        print(make(n))
+    for n in (sys.argv[1:] or list(WORKLOADS) + list(OVERSET_WORKLOADS)):
+        print(make_overset(n) if n in OVERSET_WORKLOADS else make(n))

@@ -81,3 +81,67 @@ def test_oracle_matches_reference_live(oracle_lib, label):
     ref = run_ref.assemble(case, run_ref.run(case, mode="run", nsteps=case.nsteps, dt=dt)["ranks"])[0]
     s.advance(case.nsteps, dt)
     np.testing.assert_array_equal(s.download(0)[0], ref)
+
+
+def overset_case(name: str):
+    from tests.golden.make_golden import OVERSET_WORKLOADS
+    return OVERSET_WORKLOADS[name]()
+
+
+def check_overset_maps(solver, g, case):
+    """Receiver and donor maps, normalised weights and iblank equal the reference's
+    (per donor block, in file order, as overset::initialize_donor lists them)."""
+    m = solver.get_overset()
+    for b in range(len(case.blocks)):
+        sel = m["donor_block"] == b
+        np.testing.assert_array_equal(m["donor_l0"][sel], g[f"donor_l0_{b}"])
+        np.testing.assert_array_equal(m["weights"][sel], g[f"weights_{b}"])
+        np.testing.assert_array_equal(m["recv_l0"][m["recv_block"] == b], g[f"recv_l0_{b}"])
+
+
+OVERSET_NAMES = ["cylinder2d_64"]
+
+
+@pytest.mark.parametrize("name", OVERSET_NAMES)
+def test_oracle_overset_matches_golden(oracle_lib, name):
+    g = load_golden(name)
+    case = overset_case(name)
+    s = api.Solver(oracle_lib, case)
+    check_overset_maps(s, g, case)
+    assert s.compute_dt() == float(g["dt"])
+    for b in range(len(case.blocks)):
+        np.testing.assert_array_equal(s.eval_rhs(b, 0.0), g[f"rhs_{b}"])
+    dt = float(g["dt"])
+    s.advance(1, dt)
+    for b in range(len(case.blocks)):
+        np.testing.assert_array_equal(s.download(b)[0], g[f"step1_{b}"])
+    s.advance(int(g["nsteps"]) - 1, dt)
+    for b in range(len(case.blocks)):
+        np.testing.assert_array_equal(s.download(b)[0], g[f"stepn_{b}"])
+
+
+def test_oracle_reads_the_overset_file_like_the_arrays(oracle_lib, tmp_path):
+    case = overset_case("cylinder2d_64")
+    path = str(tmp_path / "overset.bin")
+    case.overset.write(path)
+    a = api.Solver(oracle_lib, case).get_overset()
+    b = api.Solver(oracle_lib, case, overset_file=path).get_overset()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_oracle_overset_matches_reference_live(oracle_lib):
+    """A second overset layout run live on two reference ranks: a finer O-grid, a wider seam
+    overlap and three fringe layers."""
+    from oracle import run_ref
+    if not run_ref.available():
+        pytest.skip("oracle/_ref/camille_ref not built here")
+    case = cases.cylinder2d(nb=56, length=14.0, ntheta=80, nr=20, r_out=3.2, first_cell=0.04, r_cut=0.9,
+                            seam_overlap=10.5, fringe=3, sponge=5, nsteps=12, pulse=(-1.5, -0.4, 1e-3, 0.4))
+    s = api.Solver(oracle_lib, case)
+    dt = s.compute_dt()
+    assert dt == run_ref.run(case, mode="run", nsteps=1, dt=None, nprocs=2)["result"]["dt"]
+    ref = run_ref.assemble(case, run_ref.run(case, mode="run", nsteps=case.nsteps, dt=dt, nprocs=2)["ranks"])
+    s.advance(case.nsteps, dt)
+    for b in range(2):
+        np.testing.assert_array_equal(s.download(b)[0], ref[b])
