@@ -354,7 +354,7 @@ def cylinder2d(nb: int = 512, length: float = 80.0, ntheta: int = 384, nr: int =
                fringe: int = 2, sponge: Optional[int] = None, sponge_constant: float = 5.0,
                source: tuple[float, float] = (2.0, 0.0), omega: float = 0.8 * math.pi, halfwidth: float = 0.2,
                amplitude: float = 1e-3, ramp: float = 2.5, nsteps: int = 4000, gamma: float = 1.4,
-               pulse: Optional[tuple[float, float, float, float]] = None) -> Case:
+               pulse: Optional[tuple[float, float, float, float]] = None, wall_damping: float = 0.5) -> Case:
     """Two-block overset workload: a Cartesian background (block 0, nb x nb on [-L/2, L/2]^2)
     and a body-fitted O-grid (block 1, ntheta x nr) around a cylinder of radius ``r_wall``,
     radii clustered at the wall by a one-sided tanh (first cell ``first_cell``) out to ``r_out``.
@@ -367,7 +367,11 @@ def cylinder2d(nb: int = 512, length: float = 80.0, ntheta: int = 384, nr: int =
     are 4 x 4 Lagrange (``ORDER_ACCURACY = 3``) in the donor's computational coordinates.
 
     Mean flow: the parallel shear layer u_bar = 0.15 (1 + tanh 2y) (Mach units, c = 1:
-    rho_bar = 1, p_bar = 1/gamma) on both blocks. Source: monopole at ``source`` with
+    rho_bar = 1, p_bar = 1/gamma) on both blocks, times 1 - exp(-((r - r_wall) / wall_damping)^2)
+    so that it vanishes at the cylinder. A parallel mean taken straight through the body
+    enters the domain through the wall behind the cylinder, where a slip wall cannot be a
+    well-posed boundary; in the reference's arithmetic that run grows without bound after
+    about 1400 steps at the full size. ``wall_damping = 0`` keeps the undamped layer. Source: monopole at ``source`` with
     angular frequency ``omega``, Gaussian half-width ``halfwidth`` and a sin^2 ramp over
     ``ramp``. BC lines: slip wall on the cylinder (O-grid eta = 0) and Freund sponges on the
     background's four sides (``sponge`` cells, default 20 at nb = 512). The initial state is
@@ -388,6 +392,9 @@ def cylinder2d(nb: int = 512, length: float = 80.0, ntheta: int = 384, nr: int =
         x, y = x2[None].copy(), y2[None].copy()
         mean = np.zeros((5,) + x.shape)
         mean[1] = 0.15 * (1.0 + np.tanh(2.0 * y))
+        if wall_damping > 0.0:
+            rr = np.hypot(x, y)
+            mean[1] *= 1.0 - np.exp(-(np.maximum(rr - r_wall, 0.0) / wall_damping) ** 2)
         mean[4] = 1.0 / gamma
         return Block(x, y, np.zeros_like(x), mean, np.zeros((5,) + x.shape))
 
