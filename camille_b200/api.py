@@ -88,6 +88,7 @@ SIGNATURES = {
     "get_info": (C.c_int, [C.c_void_p, C.POINTER(LeeInfo)]),
     "set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "get_stats": (C.c_int, [C.c_void_p, C.POINTER(LeeStats)]),
+    "set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
 }
 
 
@@ -270,6 +271,13 @@ def _solver_timing(self, on: bool) -> None:
 Solver.info = _solver_info
 Solver.stats = _solver_stats
 Solver.set_timing = _solver_timing
+
+
+def _solver_graphs(self, on: bool) -> None:
+    self._chk(self.lib.set_graphs(self.ctx, 1 if on else 0))
+
+
+Solver.set_graphs = _solver_graphs
 
 
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:

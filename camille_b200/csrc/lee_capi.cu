@@ -145,6 +145,19 @@ struct lee_ctx {
     long long *d_rl = nullptr, *d_dl = nullptr;
     double *d_wt = nullptr, *d_buf = nullptr;
   } ovs;
+  // replayed step graph: a few steps captured once (until the buffer roles repeat) and
+  // launched as one graph; keyed by dt, precision and the buffer layout it was captured on
+  struct {
+    bool enabled = true;
+    cudaGraphExec_t exec = nullptr;
+    double dt = 0.0;
+    int steps = 0;                 // steps per replay
+    std::vector<void*> layout;
+    long long launches = 0, stage_launches = 0, filter_launches = 0;  // per replay
+    void* d_amp = nullptr;         // monopole amplitudes, [step][stage], working precision
+    size_t amp_cap = 0;            // entries
+    int* d_ctr = nullptr;          // steps of the current chunk done so far
+  } graph;
 };
 
 namespace {
@@ -866,23 +879,39 @@ int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e) {
   return LEE_OK;
 }
 
-template <typename T>
-int advance_impl(lee_ctx* c, int nsteps, double dt) {
-  const int rk = c->cfg.rk_scheme;
-  double bi[4], ci[4], aij[4];
+// The Butcher tableau of RungeKutta::initialize (src/solver/temporal_discretization.cpp:33-85).
+struct Tableau {
   int ns;
+  double b[4], c[4], a[4];
+};
+
+Tableau tableau(int rk) {
+  Tableau t{};
   if (rk == LEE_RK4) {
-    ns = 4;
-    bi[0] = 1.0 / 6.0; bi[1] = 1.0 / 3.0; bi[2] = 1.0 / 3.0; bi[3] = 1.0 / 6.0;
-    ci[0] = 0.0; ci[1] = 1.0 / 2.0; ci[2] = 1.0 / 2.0; ci[3] = 1.0;
-    aij[0] = 1.0 / 2.0; aij[1] = 1.0 / 2.0; aij[2] = 1.0; aij[3] = 0.0;
+    t.ns = 4;
+    t.b[0] = 1.0 / 6.0; t.b[1] = 1.0 / 3.0; t.b[2] = 1.0 / 3.0; t.b[3] = 1.0 / 6.0;
+    t.c[0] = 0.0; t.c[1] = 1.0 / 2.0; t.c[2] = 1.0 / 2.0; t.c[3] = 1.0;
+    t.a[0] = 1.0 / 2.0; t.a[1] = 1.0 / 2.0; t.a[2] = 1.0; t.a[3] = 0.0;
   } else {
-    ns = 2;
-    bi[0] = 1.0 / 2.0; bi[1] = 1.0 / 2.0;
-    ci[0] = 0.0; ci[1] = 1.0;
-    aij[0] = 1.0; aij[1] = 0.0;
+    t.ns = 2;
+    t.b[0] = 1.0 / 2.0; t.b[1] = 1.0 / 2.0;
+    t.c[0] = 0.0; t.c[1] = 1.0;
+    t.a[0] = 1.0; t.a[1] = 0.0;
   }
-  for (int it = 0; it < nsteps; ++it) {
+  return t;
+}
+
+// One time step (temporal::time_advance with RungeKutta::integrate) enqueued on the context
+// stream: the time is incremented first (solver::solve, src/solver/solver.cpp:72), then every
+// stage runs on every block, the boundary update (BC lines, overset) follows each stage, and
+// the filter closes the step. amp_tab/ctr: the monopole amplitudes of a replayed step graph
+// (null: the amplitude is passed by value).
+template <typename T>
+int step_impl(lee_ctx* c, double dt, const T* amp_tab, const int* ctr) {
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  const int ns = tb.ns;
+  const double *bi = tb.b, *ci = tb.c, *aij = tb.a;
+  {
     c->time += dt;
     c->step += 1;
     const double tn = c->time;
@@ -896,6 +925,9 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
         p.b = (T)bi[s];
         p.a = (T)aij[s];
         p.src_amp = (T)(c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, tn + ci[s] * dt) : 0.0);
+        p.amp_tab = amp_tab;
+        p.step_ctr = ctr;
+        p.nstages = ns;
         void** zin = s == 0 ? b.y : b.zb[(s + 1) % 2];
         void** zout = b.zb[s % 2];
         for (int v = 0; v < c->V; ++v) {
@@ -985,6 +1017,184 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
   return LEE_OK;
 }
 
+__global__ void k_tick(int* ctr) { *ctr += 1; }
+
+// The buffer roles of every block (they rotate when a step ends with a swap) and whether each
+// block's rho'/rho_bar field is live: a captured step sequence replays only on the same layout.
+std::vector<void*> layout_of(lee_ctx* c) {
+  std::vector<void*> l;
+  for (auto& b : c->blk) {
+    for (int v = 0; v < c->V; ++v) {
+      l.push_back(b.y[v]); l.push_back(b.acc[v]); l.push_back(b.zb[0][v]); l.push_back(b.zb[1][v]);
+      l.push_back(b.comp[v]); l.push_back(b.dsum[v]);
+    }
+    l.push_back((void*)(uintptr_t)(b.rho_valid ? 1 : 0));
+  }
+  return l;
+}
+
+struct SavedRoles {
+  std::vector<std::vector<void*>> f;
+};
+
+SavedRoles save_roles(lee_ctx* c) {
+  SavedRoles r;
+  for (auto& b : c->blk) {
+    std::vector<void*> v;
+    for (int q = 0; q < c->V; ++q) {
+      v.push_back(b.y[q]); v.push_back(b.acc[q]); v.push_back(b.zb[0][q]); v.push_back(b.zb[1][q]);
+      v.push_back(b.comp[q]); v.push_back(b.dsum[q]);
+    }
+    r.f.push_back(v);
+  }
+  return r;
+}
+
+void restore_roles(lee_ctx* c, const SavedRoles& r) {
+  for (size_t i = 0; i < c->blk.size(); ++i) {
+    BlockData& b = c->blk[i];
+    const std::vector<void*>& v = r.f[i];
+    for (int q = 0; q < c->V; ++q) {
+      b.y[q] = v[6 * q]; b.acc[q] = v[6 * q + 1]; b.zb[0][q] = v[6 * q + 2]; b.zb[1][q] = v[6 * q + 3];
+      b.comp[q] = v[6 * q + 4]; b.dsum[q] = v[6 * q + 5];
+    }
+  }
+}
+
+// Capture steps into one graph until the buffer roles come back to where they started
+// (at most 4 steps), with the monopole amplitudes read from the device table.
+template <typename T>
+int capture_steps(lee_ctx* c, double dt) {
+  auto& g = c->graph;
+  if (g.exec) {
+    cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+  }
+  const std::vector<void*> start = layout_of(c);
+  const SavedRoles roles = save_roles(c);
+  const double t0 = c->time;
+  const int s0 = c->step;
+  const lee_stats st0 = c->stats;
+  memset(&c->stats, 0, sizeof c->stats);
+  const bool src = c->src_kind == LEE_SOURCE_MONOPOLE;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  int rc = LEE_OK, steps = 0;
+  for (; steps < 4;) {
+    rc = step_impl<T>(c, dt, src ? (const T*)g.d_amp : nullptr, src ? g.d_ctr : nullptr);
+    if (rc) break;
+    if (src) {
+      k_tick<<<1, 1, 0, c->stream>>>(g.d_ctr);
+      c->stats.kernel_launches += 1;
+    }
+    ++steps;
+    if (layout_of(c) == start) break;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  const bool repeat = rc == LEE_OK && layout_of(c) == start;
+  const lee_stats per = c->stats;
+  restore_roles(c, roles);
+  c->time = t0;
+  c->step = s0;
+  c->stats = st0;
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(c, LEE_ERR_CUDA, "stream capture: %s", cudaGetErrorString(e));
+  if (!repeat) {  // buffer roles that never come back: keep launching step by step
+    cudaGraphDestroy(graph);
+    g.steps = 0;
+    return LEE_OK;
+  }
+  e = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g.exec = nullptr;
+    return fail(c, LEE_ERR_CUDA, "graph instantiation: %s", cudaGetErrorString(e));
+  }
+  g.dt = dt;
+  g.steps = steps;
+  g.layout = start;
+  g.launches = per.kernel_launches;
+  g.stage_launches = per.stage_launches;
+  g.filter_launches = per.filter_launches;
+  return LEE_OK;
+}
+
+// lee_advance: step by step when timing kernels (events between launches), else replays of a
+// captured step graph; the remainder, and a first step whose rho'/rho_bar field is not yet
+// live, run step by step.
+template <typename T>
+int advance_impl(lee_ctx* c, int nsteps, double dt) {
+  auto& g = c->graph;
+  int done = 0;
+  auto direct = [&](int n) -> int {
+    for (int k = 0; k < n; ++k) {
+      int rc = step_impl<T>(c, dt, nullptr, nullptr);
+      if (rc) return rc;
+    }
+    done += n;
+    return LEE_OK;
+  };
+  if (!g.enabled || c->timing || nsteps < 2) return direct(nsteps);
+  bool need_rho = false, rho_live = true;
+  for (auto& b : c->blk) {
+    need_rho |= b.need_rho != 0;
+    rho_live &= !b.need_rho || b.rho_valid;
+  }
+  if (need_rho && !rho_live) {
+    int rc = direct(1);
+    if (rc) return rc;
+  }
+  const bool src = c->src_kind == LEE_SOURCE_MONOPOLE;
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  constexpr size_t kTableSteps = 4096;  // amplitude table rows: steps per chunk of replays
+  if (src && !g.d_ctr) {
+    int rc = dalloc(c, &g.d_ctr, 1);
+    if (rc) return rc;
+    void* p = nullptr;
+    if ((rc = dev_alloc(c, &p, kTableSteps * 4 * sizeof(double)))) return rc;
+    g.d_amp = p;
+    g.amp_cap = kTableSteps * 4;
+  }
+  if (!g.exec || g.dt != dt || g.layout != layout_of(c)) {
+    int rc = capture_steps<T>(c, dt);
+    if (rc) return rc;
+  }
+  if (!g.exec || g.steps < 1) return direct(nsteps - done);
+  const int P = g.steps;
+  const size_t chunk_steps = (size_t)P * (kTableSteps / P);
+  std::vector<T> amp;
+  while (nsteps - done >= P) {
+    const int reps = (int)std::min<long long>((nsteps - done) / P, (long long)(chunk_steps / P));
+    const int n = reps * P;
+    if (src) {
+      // amplitudes at the stage times of each step, with the time advanced as the steps do
+      amp.assign((size_t)n * tb.ns, T(0));
+      double t = c->time;
+      for (int k = 0; k < n; ++k) {
+        t += dt;
+        for (int s = 0; s < tb.ns; ++s) amp[(size_t)k * tb.ns + s] = (T)source_amp(c, t + tb.c[s] * dt);
+      }
+      CK(cudaMemcpyAsync(g.d_amp, amp.data(), amp.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemsetAsync(g.d_ctr, 0, sizeof(int), c->stream));
+    }
+    for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(g.exec, c->stream));
+    for (int k = 0; k < n; ++k) {
+      c->time += dt;
+      c->step += 1;
+    }
+    for (auto& b : c->blk)
+      if (b.need_rho) b.rho_valid = true;
+    c->stats.kernel_launches += g.launches * reps;
+    c->stats.stage_launches += g.stage_launches * reps;
+    c->stats.filter_launches += g.filter_launches * reps;
+    done += n;
+  }
+  return direct(nsteps - done);
+}
+
 }  // namespace
 
 namespace lee {
@@ -1052,6 +1262,7 @@ void lee_destroy(lee_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->cfg.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   for (void* p : c->allocs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1792,6 +2003,18 @@ int lee_get_info(lee_ctx* c, lee_info* info) {
 int lee_set_timing(lee_ctx* c, int on) {
   if (!c) return LEE_ERR_ARG;
   c->timing = on != 0;
+  return LEE_OK;
+}
+
+int lee_set_graphs(lee_ctx* c, int on) {
+  if (!c) return LEE_ERR_ARG;
+  c->graph.enabled = on != 0;
+  if (!c->graph.enabled && c->graph.exec) {
+    cudaSetDevice(c->cfg.device);
+    cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(c->graph.exec);
+    c->graph.exec = nullptr;
+  }
   return LEE_OK;
 }
 

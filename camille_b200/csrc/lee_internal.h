@@ -78,9 +78,13 @@ struct StageParams {
   int nzones;
   Zone<T> zones[kMaxZones];
   const T* sigma;
-  // monopole source: rhs[p] += src_amp * g, g on a box (src_lo..src_hi), i fastest
+  // monopole source: rhs[p] += amp * g, g on a box (src_lo..src_hi), i fastest; amp is src_amp,
+  // or, in a replayed step graph, amp_tab[*step_ctr * nstages + stage]
   int has_src;
   T src_amp;
+  const T* amp_tab;
+  const int* step_ctr;
+  int nstages;
   int src_lo[3], src_hi[3];
   const T* src_g;
   // holes and closure codes (nullptr when the block has no holes)

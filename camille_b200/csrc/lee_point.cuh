@@ -105,7 +105,8 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l,
       k >= p.src_lo[2] && k <= p.src_hi[2]) {
     int b0 = p.src_hi[0] - p.src_lo[0] + 1, b1 = p.src_hi[1] - p.src_lo[1] + 1;
     long long lb = (i - p.src_lo[0]) + (long long)b0 * ((j - p.src_lo[1]) + (long long)b1 * (k - p.src_lo[2]));
-    r[P] += p.src_amp * p.src_g[lb];
+    const T amp = p.amp_tab ? p.amp_tab[*p.step_ctr * p.nstages + p.stage] : p.src_amp;
+    r[P] += amp * p.src_g[lb];
   }
   if (TR & kTrSponge) {
 #pragma unroll

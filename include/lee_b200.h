@@ -196,6 +196,11 @@ typedef struct {
   long long kernel_launches; /* every kernel this library launched in the last lee_advance */
 } lee_stats;
 int lee_set_timing(lee_ctx *ctx, int on);
+/* Step graphs (no reference counterpart; on by default): lee_advance captures the launches
+ * of a few steps once, until the buffer roles repeat, and replays them as one CUDA graph per
+ * group of steps. Off, or while kernel timing is on, every launch is issued on its own. The
+ * results are the same either way. */
+int lee_set_graphs(lee_ctx *ctx, int on);
 int lee_get_stats(lee_ctx *ctx, lee_stats *stats);
 
 /* The filter of one field, with no device allocation (no counterpart in the reference: it

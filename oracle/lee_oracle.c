@@ -1079,6 +1079,11 @@ int orc_set_timing(orc_ctx *c, int on) {
   return LEE_OK;
 }
 
+int orc_set_graphs(orc_ctx *c, int on) {
+  (void)c; (void)on;
+  return LEE_OK;
+}
+
 int orc_get_stats(orc_ctx *c, lee_stats *st) {
   (void)c;
   memset(st, 0, sizeof *st);
