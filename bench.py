@@ -120,6 +120,26 @@ SPONGE_FRACTION = 16.0 / 256.0  # sponge width per side, relative to the block s
 SPONGE_CONSTANT = 1.0
 
 
+WORKLOADS = {
+    "curvi3d": "curvi3d {n}^3 Mach 0.5, 8 Gaussian pulses (seed 2), RK4 CFL 0.5, OA4 central FD + OA8 filter, "
+               "Freund sponges n/16 wide (constant 1)",
+    "pulse2d": "pulse2d {n}^2 on [-50,50]^2, quiescent, Gaussian p' pulse, RK4 CFL 0.5, OA4 FD + OA8 filter, "
+               "20-cell Freund sponges (constant 5)",
+    "cylinder": "cylinder2d: background 512^2 on [-40,40]^2 + O-grid 384x96 (first cell 0.005), 4x4 Lagrange "
+                "overset, tanh shear layer damped at the wall, monopole (2,0) omega 0.8 pi, RK4 CFL 0.5",
+}
+
+
+def make_case(workload: str, n: int, nsteps: int) -> cases.Case:
+    if workload == "curvi3d":
+        return bench_case(n, nsteps)
+    if workload == "pulse2d":
+        return cases.pulse2d(n=n, nsteps=nsteps)
+    if workload == "cylinder":
+        return cases.cylinder2d(nsteps=nsteps)
+    raise ValueError(workload)
+
+
 def bench_case(n: int, nsteps: int) -> cases.Case:
     """The 3-D curvilinear workload with a Freund sponge frame: closure-only boundaries
     with the Mach 0.5 mean flow make the reference's scheme unstable, so the pinned
@@ -155,7 +175,9 @@ def run_ours(args) -> None:
         return float(t.item())
 
     n = args.n
-    case = bench_case(n, args.error_steps)
+    case = make_case(args.workload, n, args.error_steps)
+    dim = case.num_dim
+    nblk = len(case.blocks)
     lib = api.product_library()
     K, W = args.steps, args.warmup
     results = {}
@@ -171,42 +193,52 @@ def run_ours(args) -> None:
         if sampler:
             sampler.start()
             time.sleep(0.3)
-        s.set_timing(True)
+        # the product path (replayed step graphs), timed by lee_advance's own CUDA events
         s.advance(K, dt)
         st = s.stats()
-        s.set_timing(False)
         barrier()
         if sampler:
             clocks = sampler.stop()
         ms = max_over_ranks(st.advance_ms)
+        # per-kernel launch times, for the roofline: the same steps launched one by one with
+        # events between the launches
+        s.set_timing(True)
+        s.advance(min(K, args.kernel_steps), dt)
+        kst = s.stats()
+        s.set_timing(False)
         info = s.info()
-        results[form] = {"ms": ms, "stats": st, "info": info, "dt": dt}
+        results[form] = {"ms": ms, "stats": st, "kstats": kst, "info": info, "dt": dt}
     npts = case.npoints
 
     # accuracy of the compensated form against FP64 at the step count of the workload
-    done = W + K
+    done = W + K + min(K, args.kernel_steps)
     for s in solvers.values():
         if args.error_steps > done:
             s.advance(args.error_steps - done, results["fp64"]["dt"])
-    p32 = solvers["fp32c"].download(0)[0][4]
-    p64 = solvers["fp64"].download(0)[0][4]
+    p32 = np.concatenate([solvers["fp32c"].download(b)[0][4].ravel() for b in range(nblk)])
+    p64 = np.concatenate([solvers["fp64"].download(b)[0][4].ravel() for b in range(nblk)])
     err = api.rel_l2(p32, p64)
     solvers["fp64"].close()
 
     # end to end through the C ABI with host buffers: upload from pinned host memory,
     # K steps, download of the state to pinned host memory
     s = solvers["fp32c"]
-    host_in = [torch.from_numpy(np.ascontiguousarray(case.blocks[0].state[v])).pin_memory() for v in range(5)]
-    host_out = [torch.empty_like(host_in[v]).pin_memory() for v in range(5)]
-    pin_in = (C.POINTER(C.c_double) * 5)(*[C.cast(t.data_ptr(), C.POINTER(C.c_double)) for t in host_in])
-    pin_out = (C.POINTER(C.c_double) * 5)(*[C.cast(t.data_ptr(), C.POINTER(C.c_double)) for t in host_out])
+    pins = []
+    for blk in case.blocks:
+        host_in = [torch.from_numpy(np.ascontiguousarray(blk.state[v])).pin_memory() for v in range(5)]
+        host_out = [torch.empty_like(host_in[v]).pin_memory() for v in range(5)]
+        pin_in = (C.POINTER(C.c_double) * 5)(*[C.cast(t.data_ptr(), C.POINTER(C.c_double)) for t in host_in])
+        pin_out = (C.POINTER(C.c_double) * 5)(*[C.cast(t.data_ptr(), C.POINTER(C.c_double)) for t in host_out])
+        pins.append((host_in, host_out, pin_in, pin_out))
     dt = results["fp32c"]["dt"]
     barrier()
     t0 = time.perf_counter()
-    s._chk(lib.upload_state(s.ctx, 0, pin_in, 0, 0.0))
+    for b, (_, _, pin_in, _) in enumerate(pins):
+        s._chk(lib.upload_state(s.ctx, b, pin_in, 0, 0.0))
     s._chk(lib.advance(s.ctx, K, dt))
     stp, tm = C.c_int(), C.c_double()
-    s._chk(lib.download_state(s.ctx, 0, pin_out, C.byref(stp), C.byref(tm)))
+    for b, (_, _, _, pin_out) in enumerate(pins):
+        s._chk(lib.download_state(s.ctx, b, pin_out, C.byref(stp), C.byref(tm)))
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     state_bytes = 5 * npts * 8
@@ -214,14 +246,14 @@ def run_ours(args) -> None:
     r32, r64 = results["fp32c"], results["fp64"]
     value = world * npts * K / (r32["ms"] / 1e3)
     value64 = world * npts * K / (r64["ms"] / 1e3)
-    st = r32["stats"]
+    st = r32["kstats"]
     info = r32["info"]
     peak, peak_kind = measured_hbm_gbs()
     stage_avg_ms = st.stage_ms / max(st.stage_launches, 1)
     filt_avg_ms = st.filter_ms / max(st.filter_launches, 1)
     stage_b = stage_bytes_per_point(info, True) * npts
     achieved = stage_b / (stage_avg_ms / 1e3) / 1e9
-    step_b = step_bytes_per_point(info, True, 3) * npts
+    step_b = step_bytes_per_point(info, True, dim) * npts
     step_gbs = step_b * K / (r32["ms"] / 1e3) / 1e9
     dominant = "stage" if st.stage_ms >= st.filter_ms else "filter"
 
@@ -233,11 +265,12 @@ def run_ours(args) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": r32["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32-compensated (fp64 setup)", "data": "synthetic",
-            "config": {"workload": f"curvi3d {n}^3 Mach 0.5, 8 Gaussian pulses (seed 2), RK4 CFL 0.5, "
-                                   "OA4 central FD + OA8 filter, Freund sponges n/16 wide (constant 1)",
-                       "points_per_gpu": npts, "parallelism": f"replicas x{world} (no sharding)",
-                       "l2": "inputs larger than L2 (state 335 MB fp32 / 671 MB fp64 vs 126 MB L2)",
-                       "dt": dt},
+            "config": {"workload": WORKLOADS[args.workload].format(n=n),
+                       "points_per_gpu": npts, "blocks": nblk, "parallelism": f"replicas x{world} (no sharding)",
+                       "l2": (f"state {5 * npts * 4 / 1e6:.0f} MB fp32 / {5 * npts * 8 / 1e6:.0f} MB fp64 vs "
+                              "126 MB L2" + (" (inputs larger than L2)" if 5 * npts * 4 > 126e6 else
+                                             " (fits in L2: an L2-resident workload)")),
+                       "launch": "replayed CUDA step graphs", "dt": dt},
             "fp64": {"value": value64, "ms_per_step": r64["ms"] / K},
             "mixed_over_fp64": value / value64,
             "p_rel_l2_vs_fp64": {"value": err, "steps": max(args.error_steps, W + K)},
@@ -248,13 +281,13 @@ def run_ours(args) -> None:
                          "avg_launch_ms": stage_avg_ms, "dominant": dominant,
                          "filter_avg_launch_ms": filt_avg_ms,
                          "step_gbs": step_gbs, "step_frac": step_gbs / peak,
-                         "step_bytes_per_point": step_bytes_per_point(info, True, 3),
+                         "step_bytes_per_point": step_bytes_per_point(info, True, dim),
                          "tma_stage": info.tma_stage, "tma_filter": info.tma_filter,
                          "stage_chunk": info.stage_chunk, "filter_chunk": info.filter_chunk},
             "e2e": {"value": world * npts * K / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K,
                     "note": "lee_upload_state from pinned host memory, lee_advance(K), lee_download_state"},
-            "gpu_launches": int(st.kernel_launches),
+            "gpu_launches": int(r32["stats"].kernel_launches),
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
@@ -264,19 +297,36 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def reference_sample(args, workload: str, n: int, steps: int) -> tuple[cases.Case, str]:
+    """A bounded sample of the workload for the compiled reference: the 3-D block at a
+    smaller n, the 2-D workloads at full size."""
+    if workload == "curvi3d":
+        return bench_case(n, steps), f"curvi3d {n}^3 (bounded sample of the {args.n}^3 workload)"
+    case = make_case(workload, args.n, steps)
+    return case, case.name
+
+
+def reference_ranks(case: cases.Case, requested: int) -> int:
+    cores = os.cpu_count() or 1
+    nprocs = requested or min(cores, 8)
+    return max(nprocs, len(case.blocks))  # one rank per block at least (src/parallel/decomp.cpp:19-30)
+
+
 def cpu_baseline(args) -> dict:
-    """The compiled reference (oracle/_ref) on a bounded sample of the workload."""
+    """The compiled reference (oracle/_ref) on a bounded sample of the workload, all host cores."""
     try:
         from oracle import run_ref
         if not run_ref.available():
             return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                     "sample": "oracle/_ref/camille_ref not built"}
-        n, k = args.cpu_n, args.cpu_steps
-        case = bench_case(n, k)
-        r = run_ref.run(case, mode="run", nsteps=k, dt=0.28, timeout=600)
+        k = args.cpu_steps
+        case, desc = reference_sample(args, args.workload, args.cpu_n, k)
+        nprocs = reference_ranks(case, args.ref_ranks)
+        r = run_ref.run(case, mode="run", nsteps=k, dt=None, nprocs=nprocs, timeout=900)
         sec = r["result"]["seconds"]
-        return {"value": n ** 3 * k / sec, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"curvi3d {n}^3, {k} RK4 steps, solver::solve wall time, 1 rank, g++ -O3"}
+        return {"value": case.npoints * k / sec, "unit": UNIT, "cores": nprocs, "kind": "reference",
+                "sample": f"{desc}, {k} RK4 steps (FIX_CFL), solver::solve wall time, {nprocs} MPI ranks "
+                          "(DECOMP_1D), g++ -O3"}
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
@@ -290,21 +340,18 @@ def run_reference(args) -> None:
     if not run_ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/camille_ref is not built"}))
         return
-    cores = os.cpu_count() or 1
-    nprocs = max(1, min(args.ref_ranks or cores, 8))
-    n = args.ref_n
     steps = args.steps + args.warmup
-    case = bench_case(n, steps)
-    r = run_ref.run(case, mode="run", nsteps=steps, dt=0.28, nprocs=nprocs, timeout=1800)
+    case, desc = reference_sample(args, args.workload, args.ref_n, steps)
+    nprocs = reference_ranks(case, args.ref_ranks)
+    r = run_ref.run(case, mode="run", nsteps=steps, dt=None, nprocs=nprocs, timeout=1800)
     sec = r["result"]["seconds"]
-    value = n ** 3 * steps / sec
+    value = case.npoints * steps / sec
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": steps, "warmup": 0, "ms_per_step": sec * 1e3 / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"curvi3d {n}^3 (bounded sample of the 256^3 workload), Mach 0.5, "
-                                   "RK4, OA4 FD + OA8 filter", "ranks": nprocs},
+            "config": {"workload": f"{desc}: " + WORKLOADS[args.workload].format(n=args.n), "ranks": nprocs},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nprocs, "kind": "reference",
-                             "sample": f"curvi3d {n}^3 x {steps} steps, {nprocs} MPI ranks (DECOMP_1D)"},
+                             "sample": f"{desc} x {steps} steps (FIX_CFL), {nprocs} MPI ranks (DECOMP_1D)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -316,12 +363,15 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--workload", default="curvi3d", choices=list(WORKLOADS))
+    ap.add_argument("--kernel-steps", type=int, default=20,
+                    help="steps launched one by one with events between launches (roofline)")
     ap.add_argument("--error-steps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=64)
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--ref-n", type=int, default=48)
-    ap.add_argument("--ref-ranks", type=int, default=1)
+    ap.add_argument("--ref-n", type=int, default=64)
+    ap.add_argument("--ref-ranks", type=int, default=0, help="reference MPI ranks (0: the host's cores, at most 8)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
