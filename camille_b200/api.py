@@ -25,6 +25,7 @@ FD = {"STANDARD_CENTRAL": 1, "FDO11P": 11}
 FILTER = {"NONE": 0, "STANDARD_CENTRAL": 1, "SFO11P": 11}
 RK = {"RUNGE_KUTTA2": 2, "RUNGE_KUTTA4": 4}
 FP64, FP32_COMPENSATED = 0, 1
+SOURCE_DISTRIBUTED = 2
 SETUP_METRICS, SETUP_JACOBIAN, SETUP_MEAN_GRADIENT, SETUP_SPONGE = 0, 1, 2, 3
 SOURCE_MONOPOLE = 1
 
@@ -89,6 +90,10 @@ SIGNATURES = {
     "set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "get_stats": (C.c_int, [C.c_void_p, C.POINTER(LeeStats)]),
     "set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _LP, C.c_double]),
+    "eval_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _DP]),
+    "apply_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "adjoint_gradient": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, _DP, _DP, _LP]),
 }
 
 
@@ -166,6 +171,9 @@ class Solver:
             if case.monopole is not None:
                 p = np.array(case.monopole, np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))
+            if case.distributed is not None:
+                p = np.ascontiguousarray(case.distributed.params(), np.float64)
+                self._chk(lib.set_source(self.ctx, SOURCE_DISTRIBUTED, _dptr(p), len(p)))
             if overset_file is not None:
                 self._chk(lib.read_overset_file(self.ctx, overset_file.encode(), case.overset.order))
             elif case.overset is not None:
@@ -178,6 +186,12 @@ class Solver:
                 self._chk(lib.set_overset(self.ctx, o.num_receivers, ip[0], ip[1], ip[2], ip[3], ip[4], _dptr(w),
                                           int(o.hole_block.size), ip[5], ip[6]))
             self._chk(lib.prepare(self.ctx))
+            if case.microphones is not None:
+                mic = np.ascontiguousarray(case.microphones.l0, np.int64)
+                w = case.microphones.weight
+                if w is None:
+                    w = self.compute_dt()
+                self._chk(lib.set_objective(self.ctx, case.microphones.block, len(mic), mic.ctypes.data_as(_LP), w))
             if upload:
                 for b, blk in enumerate(case.blocks):
                     self.upload(b, blk.state)
@@ -229,6 +243,25 @@ class Solver:
 
     def apply_filter(self) -> None:
         self._chk(self.lib.apply_filter(self.ctx))
+
+    def eval_objective(self, nsteps: int, dt: float) -> float:
+        J = C.c_double()
+        self._chk(self.lib.eval_objective(self.ctx, nsteps, dt, C.byref(J)))
+        return J.value
+
+    def apply_adjoint(self, nsteps: int, dt: float) -> None:
+        self._chk(self.lib.apply_adjoint(self.ctx, nsteps, dt))
+
+    def adjoint_gradient(self, nsteps: int, dt: float, checkpoint_every: int = 100,
+                         recompute: bool = True) -> tuple[float, np.ndarray, int]:
+        """(J, dJ/d amplitudes, recomputed trace values that differ from the first pass)."""
+        d = self.case.distributed
+        grad = np.zeros(d.amplitudes.size, np.float64)
+        J = C.c_double()
+        mism = C.c_longlong()
+        self._chk(self.lib.adjoint_gradient(self.ctx, nsteps, dt, checkpoint_every, 1 if recompute else 0,
+                                            C.byref(J), _dptr(grad), C.byref(mism)))
+        return J.value, grad.reshape(d.amplitudes.shape), mism.value
 
     def get_overset(self) -> dict:
         """The donor maps the context holds: receiver/donor blocks, linear indices and the

@@ -25,6 +25,7 @@ UNITS = {
     "lee_capi.cu": [],
     "lee_static.cu": [],
     "lee_bc.cu": [],
+    "lee_adjoint.cu": [],
 }
 
 

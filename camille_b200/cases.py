@@ -81,6 +81,33 @@ class Boundary:
 
 
 @dataclasses.dataclass
+class DistributedSource:
+    """rhs[p'] += (gamma - 1) sin(omega t) S on block ``block``, S the trilinear prolongation of
+    ``amplitudes`` (shape (cz, cy, cx)) from lattice nodes at grid index origin + node * spacing
+    (LEE_SOURCE_DISTRIBUTED of include/lee_b200.h; the reference has no such source)."""
+    block: int
+    omega: float
+    origin: tuple[float, float, float]
+    spacing: tuple[float, float, float]
+    amplitudes: np.ndarray
+
+    def params(self) -> np.ndarray:
+        cz, cy, cx = self.amplitudes.shape
+        head = [self.block, self.omega, cx, cy, cz, *self.origin, *self.spacing]
+        return np.concatenate([np.asarray(head, np.float64), self.amplitudes.astype(np.float64).ravel()])
+
+
+@dataclasses.dataclass
+class Microphones:
+    """Objective J = weight * sum over steps of sum over microphones of p'^2 at linear
+    indices ``l0`` of block ``block``; weight None takes the FIX_CFL time step (a rectangle-rule
+    time integral)."""
+    block: int
+    l0: np.ndarray
+    weight: Optional[float] = None
+
+
+@dataclasses.dataclass
 class Case:
     name: str
     num_dim: int
@@ -100,6 +127,8 @@ class Case:
     sponge_constant: float = 5.0
     monopole: Optional[tuple[float, float, float, float, float, float, float]] = None
     overset: Optional["overset_mod.OversetMap"] = None
+    distributed: Optional[DistributedSource] = None
+    microphones: Optional[Microphones] = None
     notes: str = ""
 
     @property
@@ -162,6 +191,8 @@ class Case:
     def write_reference_inputs(self, workdir: str, dt: Optional[float], nsteps: int,
                                step: int = 0, time: float = 0.0) -> str:
         """Write grid, mean, restart, BC and deck files; return the restart path."""
+        if self.distributed is not None:
+            raise ValueError("the reference cannot express a distributed source")
         os.makedirs(workdir, exist_ok=True)
         grid, mean, ic, bc = (os.path.join(workdir, n) for n in ("grid.xyz", "mean.q", "ic.q", "bc.in"))
         plot3d.write_grid(grid, [(b.x, b.y, b.z) for b in self.blocks])
@@ -473,3 +504,42 @@ def cylinder2d(nb: int = 512, length: float = 80.0, ntheta: int = 384, nr: int =
                 monopole=(source[0], source[1], 0.0, amplitude, omega, halfwidth, ramp),
                 notes=f"2-D overset: background {nb}^2 on [-{length/2},{length/2}]^2, O-grid {ntheta}x{nr} "
                       f"r in [{r_wall},{r_out}] first cell {first_cell}, shear layer, monopole at {source}")
+
+
+def adjoint3d(n: int = 192, nsteps: int = 2000, seed: int = 5, mach: float = 0.5, lattice: int = 16,
+              omega: float = 0.4 * math.pi, amp_std: float = 1e-3, nmics: int = 64, gamma: float = 1.4,
+              sponge: Optional[int] = None, precompute: bool = False) -> Case:
+    """The adjoint workload: the curvi3d mapping at n^3, Mach ``mach`` along x, zero initial
+    state, a distributed monopole whose lattice x lattice x lattice amplitudes are drawn
+    N(0, amp_std) from ``numpy.random.default_rng(seed)`` and span 60 n/192 grid cells around
+    the block centre (node spacing 4 n/192), at angular frequency ``omega``; ``nmics``
+    microphones on the downstream half circle of radius 60 n/192 cells in the mid-zeta plane;
+    Freund sponges n/16 cells wide (constant 1), as the 256^3 workload."""
+    x, y, z = curvi3d_grid(n)
+    mean = np.zeros((5,) + x.shape)
+    mean[1] = mach
+    mean[4] = 1.0 / gamma
+    blk = Block(x, y, z, mean, np.zeros((5,) + x.shape))
+    width = max(4, int(round(n / 16))) if sponge is None else sponge
+    bnd = sponge_frame(3, blk.dims, width) if width > 0 else []
+    c = 0.5 * (n - 1)
+    h = 4.0 * n / 192.0
+    o = c - 0.5 * (lattice - 1) * h
+    rng = np.random.default_rng(seed)
+    amps = rng.normal(0.0, amp_std, size=(lattice, lattice, lattice))
+    src = DistributedSource(0, omega, (o, o, o), (h, h, h), amps)
+    R = 60.0 * n / 192.0
+    th = np.linspace(-0.5 * math.pi, 0.5 * math.pi, nmics)
+    ii = np.rint(c + R * np.cos(th)).astype(np.int64)
+    jj = np.rint(c + R * np.sin(th)).astype(np.int64)
+    kk = n // 2
+    l0 = ii + n * (jj + n * kk)
+    if np.unique(l0).size != l0.size:
+        raise ValueError("microphones collide at this size")
+    case = Case(name=f"adjoint3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
+                sponge_constant=1.0, distributed=src, microphones=Microphones(0, l0),
+                notes=f"3-D {n}^3 curvilinear, Mach {mach}, distributed source {lattice}^3 (seed {seed}), "
+                      f"{nmics} microphones r = {R:.1f}")
+    if precompute:
+        precompute_sponges(case)
+    return case

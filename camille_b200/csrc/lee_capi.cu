@@ -114,6 +114,7 @@ struct lee_ctx {
   cudaStream_t stream = nullptr;
   int src_kind = LEE_SOURCE_NONE;
   double src[7] = {0, 0, 0, 0, 0, 0, 0};
+  std::vector<double> dsrc;  // distributed source parameters (LEE_SOURCE_DISTRIBUTED)
   bool prepared = false, uploaded = false;
   int step = 0;
   double time = 0.0;
@@ -158,6 +159,24 @@ struct lee_ctx {
     size_t amp_cap = 0;            // entries
     int* d_ctr = nullptr;          // steps of the current chunk done so far
   } graph;
+  // discrete adjoint (single block, uniform mean, no BC lines, holes or overset)
+  struct {
+    bool ready = false;
+    TransOp dT{}, fT{};                    // transposed difference and filter operators
+    void *lam[kMaxVars] = {}, *mu[kMaxVars] = {}, *kb[2][kMaxVars] = {}, *ybar[kMaxVars] = {};
+    int mic_block = 0;
+    double weight = 0.0;
+    std::vector<long long> mic;
+    long long* d_mic = nullptr;
+    bool trace_on = false;
+    double* d_trace = nullptr;             // rows of p' at the microphones, one per step
+    size_t trace_rows = 0;
+    int* d_base = nullptr;                 // trace row of the first step of a replayed chunk
+    int host_row = 0;                      // trace row of the next directly launched step
+    double* d_gbar = nullptr;              // gradient of the distributed source's box field
+    std::vector<void*> ckpt;               // checkpoints: V (+ V carried errors) fields each
+    size_t ckpt_slots = 0;
+  } adj;
 };
 
 namespace {
@@ -350,6 +369,12 @@ __global__ void k_split(long long n, float* y, float* e, const double* in) {
     y[l] = r;
     e[l] = (float)(in[l] - (double)r);
   }
+}
+
+// out = fl32(y + e)
+__global__ void k_add_pair(long long n, float* out, const float* y, const float* e) {
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
+    out[l] = (float)((double)y[l] + (double)e[l]);
 }
 
 template <typename T>
@@ -549,8 +574,88 @@ void fill_stage_common(lee_ctx* c, BlockData& b, StageParams<T>& p) {
   p.sigma = (const T*)b.d_sigma_field;
 }
 
+// Distributed source: the grid box covered by the lattice, and the trilinear prolongation of
+// coarse amplitudes A onto it (box-shaped, i fastest) or its transpose (restriction of a box
+// field onto the lattice). p = block, omega, cx, cy, cz, ox, oy, oz, hx, hy, hz, ...
+bool distributed_box(const std::vector<double>& p, int dim, int nx, int ny, int nz, int lo[3], int hi[3]) {
+  const int n[3] = {nx, ny, nz};
+  for (int d = 0; d < 3; ++d) {
+    if (d >= dim) {
+      lo[d] = hi[d] = 0;
+      continue;
+    }
+    const int cn = (int)p[2 + d];
+    const double o = p[5 + d], h = p[8 + d];
+    lo[d] = std::max(0, (int)std::ceil(o));
+    hi[d] = std::min(n[d] - 1, (int)std::floor(o + (cn - 1) * h));
+    if (hi[d] < lo[d]) return false;
+  }
+  return true;
+}
+
+// Corner weights of fine index i along one lattice direction: node p0 and weight of p0 + 1.
+void lattice_weights(double i, double o, double h, int cn, int* p0, double* f) {
+  const double u = (i - o) / h;
+  int q = (int)std::floor(u);
+  if (q > cn - 2) q = cn - 2;
+  if (q < 0) q = 0;
+  *p0 = q;
+  *f = u - q;
+}
+
+void prolong(const std::vector<double>& p, int dim, const int lo[3], const int hi[3], const double* A,
+             std::vector<double>& g) {
+  const int cx = (int)p[2], cy = (int)p[3], cz = (int)p[4];
+  const size_t nb = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+  g.assign(nb, 0.0);
+  size_t lb = 0;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i, ++lb) {
+        int q[3] = {0, 0, 0};
+        double f[3] = {0.0, 0.0, 0.0};
+        lattice_weights(i, p[5], p[8], cx, &q[0], &f[0]);
+        lattice_weights(j, p[6], p[9], cy, &q[1], &f[1]);
+        if (dim == 3) lattice_weights(k, p[7], p[10], cz, &q[2], &f[2]);
+        double sum = 0.0;
+        for (int c2 = 0; c2 < (dim == 3 ? 2 : 1); ++c2)
+          for (int c1 = 0; c1 < 2; ++c1)
+            for (int c0 = 0; c0 < 2; ++c0) {
+              const double w = (c0 ? f[0] : 1.0 - f[0]) * (c1 ? f[1] : 1.0 - f[1]) *
+                               (dim == 3 ? (c2 ? f[2] : 1.0 - f[2]) : 1.0);
+              sum += w * A[(q[0] + c0) + (size_t)cx * ((q[1] + c1) + (size_t)cy * (q[2] + c2))];
+            }
+        g[lb] = sum;
+      }
+  (void)cz;
+}
+
+void restrict_to_lattice(const std::vector<double>& p, int dim, const int lo[3], const int hi[3], const double* gbar,
+                         double* abar) {
+  const int cx = (int)p[2], cy = (int)p[3], cz = (int)p[4];
+  std::fill(abar, abar + (size_t)cx * cy * cz, 0.0);
+  size_t lb = 0;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i, ++lb) {
+        int q[3] = {0, 0, 0};
+        double f[3] = {0.0, 0.0, 0.0};
+        lattice_weights(i, p[5], p[8], cx, &q[0], &f[0]);
+        lattice_weights(j, p[6], p[9], cy, &q[1], &f[1]);
+        if (dim == 3) lattice_weights(k, p[7], p[10], cz, &q[2], &f[2]);
+        for (int c2 = 0; c2 < (dim == 3 ? 2 : 1); ++c2)
+          for (int c1 = 0; c1 < 2; ++c1)
+            for (int c0 = 0; c0 < 2; ++c0) {
+              const double w = (c0 ? f[0] : 1.0 - f[0]) * (c1 ? f[1] : 1.0 - f[1]) *
+                               (dim == 3 ? (c2 ? f[2] : 1.0 - f[2]) : 1.0);
+              abar[(q[0] + c0) + (size_t)cx * ((q[1] + c1) + (size_t)cy * (q[2] + c2))] += w * gbar[lb];
+            }
+      }
+}
+
 // Amplitude of the monopole at time t (oracle patch P2, modelled on src/solver/source.cpp:60-92).
 double source_amp(const lee_ctx* c, double t) {
+  if (c->src_kind == LEE_SOURCE_DISTRIBUTED) return (c->cfg.gamma - 1.0) * sin(c->dsrc[1] * t);
   double T = c->src[6];
   double ramp = 1.0;
   if (T > 0.0 && t < T) {
@@ -924,7 +1029,7 @@ int step_impl(lee_ctx* c, double dt, const T* amp_tab, const int* ctr) {
         p.h = (T)dt;
         p.b = (T)bi[s];
         p.a = (T)aij[s];
-        p.src_amp = (T)(c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, tn + ci[s] * dt) : 0.0);
+        p.src_amp = (T)(c->src_kind != LEE_SOURCE_NONE ? source_amp(c, tn + ci[s] * dt) : 0.0);
         p.amp_tab = amp_tab;
         p.step_ctr = ctr;
         p.nstages = ns;
@@ -1014,6 +1119,15 @@ int step_impl(lee_ctx* c, double dt, const T* amp_tab, const int* ctr) {
       }
     }
   }
+  if (c->adj.trace_on) {
+    // p' at the microphones after this step (the objective's trace), in FP64
+    BlockData& b = c->blk[(size_t)c->adj.mic_block];
+    const int P = c->V - 1;
+    CK(launch_trace<T>((int)c->adj.mic.size(), c->adj.d_mic, (const T*)b.y[P], c->comp ? (const T*)b.comp[P] : nullptr,
+                       c->adj.d_trace, ctr, ctr ? c->adj.d_base : nullptr, c->adj.host_row, c->stream));
+    c->stats.kernel_launches += 1;
+    if (!ctr) c->adj.host_row += 1;
+  }
   return LEE_OK;
 }
 
@@ -1030,6 +1144,8 @@ std::vector<void*> layout_of(lee_ctx* c) {
     }
     l.push_back((void*)(uintptr_t)(b.rho_valid ? 1 : 0));
   }
+  l.push_back((void*)(uintptr_t)(c->adj.trace_on ? 1 : 0));
+  l.push_back(c->adj.d_trace);
   return l;
 }
 
@@ -1076,13 +1192,14 @@ int capture_steps(lee_ctx* c, double dt) {
   const int s0 = c->step;
   const lee_stats st0 = c->stats;
   memset(&c->stats, 0, sizeof c->stats);
-  const bool src = c->src_kind == LEE_SOURCE_MONOPOLE;
+  const bool src = c->src_kind != LEE_SOURCE_NONE;
+  const bool tick = src || c->adj.trace_on;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
   int rc = LEE_OK, steps = 0;
   for (; steps < 4;) {
-    rc = step_impl<T>(c, dt, src ? (const T*)g.d_amp : nullptr, src ? g.d_ctr : nullptr);
+    rc = step_impl<T>(c, dt, src ? (const T*)g.d_amp : nullptr, tick ? g.d_ctr : nullptr);
     if (rc) break;
-    if (src) {
+    if (tick) {
       k_tick<<<1, 1, 0, c->stream>>>(g.d_ctr);
       c->stats.kernel_launches += 1;
     }
@@ -1147,10 +1264,11 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
     int rc = direct(1);
     if (rc) return rc;
   }
-  const bool src = c->src_kind == LEE_SOURCE_MONOPOLE;
+  const bool src = c->src_kind != LEE_SOURCE_NONE;
+  const bool tick = src || c->adj.trace_on;
   const Tableau tb = tableau(c->cfg.rk_scheme);
   constexpr size_t kTableSteps = 4096;  // amplitude table rows: steps per chunk of replays
-  if (src && !g.d_ctr) {
+  if (tick && !g.d_ctr) {
     int rc = dalloc(c, &g.d_ctr, 1);
     if (rc) return rc;
     void* p = nullptr;
@@ -1178,7 +1296,13 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
         for (int s = 0; s < tb.ns; ++s) amp[(size_t)k * tb.ns + s] = (T)source_amp(c, t + tb.c[s] * dt);
       }
       CK(cudaMemcpyAsync(g.d_amp, amp.data(), amp.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
-      CK(cudaMemsetAsync(g.d_ctr, 0, sizeof(int), c->stream));
+    }
+    if (tick) CK(cudaMemsetAsync(g.d_ctr, 0, sizeof(int), c->stream));
+    if (c->adj.trace_on) {
+      const int base = c->adj.host_row;
+      CK(cudaMemcpyAsync(c->adj.d_base, &base, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaStreamSynchronize(c->stream));  // `base` lives on this frame
+      c->adj.host_row += n;
     }
     for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(g.exec, c->stream));
     for (int k = 0; k < n; ++k) {
@@ -1193,6 +1317,169 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
     done += n;
   }
   return direct(nsteps - done);
+}
+
+// ---- discrete adjoint --------------------------------------------------------------------
+
+// The transpose of a directional operator as dop() applies it (closure row r at the r-th point
+// from either end, the mirrored right rows scaled by mfac, the interior stencil elsewhere),
+// built densely on a line long enough to hold both ends and an interior, then read back as
+// an interior row and E class rows per end within a window of H points on either side.
+bool build_transpose(const OpTable& op, TransOp* t) {
+  const int h = op.h, S = op.S;
+  const int n = 4 * (h + S) + 2 * kTE + 1;
+  std::vector<double> D((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    if (i < h) {
+      for (int s = 0; s < S; ++s) D[(size_t)i * n + s] += op.B[i][s];
+    } else if (i > n - 1 - h) {
+      const int r = n - 1 - i;
+      for (int s = 0; s < S; ++s) D[(size_t)i * n + (n - 1 - s)] += op.mfac * op.B[r][s];
+    } else {
+      for (int l = -h; l <= h; ++l) D[(size_t)i * n + i + l] += op.c[l + h];
+    }
+  }
+  auto DT = [&](int i, int j) { return (j < 0 || j >= n) ? 0.0 : D[(size_t)j * n + i]; };
+  int H = 0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j)
+      if (DT(i, j) != 0.0) H = std::max(H, std::abs(j - i));
+  if (H > kTH) return false;
+  const int mid = n / 2;
+  auto interior_like = [&](int i) {
+    for (int q = -H; q <= H; ++q)
+      if (DT(i, i + q) != DT(mid, mid + q)) return false;
+    return true;
+  };
+  int E = 0;
+  while (E < n / 2 && !interior_like(E)) ++E;
+  int Er = 0;
+  while (Er < n / 2 && !interior_like(n - 1 - Er)) ++Er;
+  E = std::max(std::max(E, Er), H);
+  if (E > kTE) return false;
+  for (int i = E; i <= n - 1 - E; ++i)
+    if (!interior_like(i)) return false;
+  memset(t, 0, sizeof *t);
+  t->H = H;
+  t->E = E;
+  for (int q = -H; q <= H; ++q) t->in[q + H] = DT(mid, mid + q);
+  for (int r = 0; r < E; ++r)
+    for (int q = -H; q <= H; ++q) {
+      t->lt[r][q + H] = DT(r, r + q);
+      t->rt[r][q + H] = DT(n - 1 - r, n - 1 - r + q);
+    }
+  return true;
+}
+
+// Checks and buffers of the adjoint path; the operators it transposes must be the
+// uniform-mean, single-block, hole-free ones.
+int adjoint_setup(lee_ctx* c) {
+  auto& a = c->adj;
+  if (a.ready) return LEE_OK;
+  if (c->blk.size() != 1) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint covers single-block contexts");
+  BlockData& b = c->blk[0];
+  if (b.has_iblank || c->ovs.n > 0) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no holes or overset");
+  for (auto& z : b.bnd)
+    if (z.kind != LEE_SPONGE_FREUND_AMBIENT) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no BC lines");
+  auto is_const = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? !f.p : !d.p; };
+  auto is_zero = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? f.zero != 0 : d.zero != 0; };
+  bool uni = is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi);
+  for (int q = 0; q < 3; ++q)
+    uni = uni && is_const(b.cd_ub[q], b.cf_ub[q]) && is_zero(b.cd_gs[q], b.cf_gs[q]) && is_zero(b.cd_gp[q], b.cf_gp[q]);
+  for (int q = 0; q < 9; ++q) uni = uni && is_zero(b.cd_gu[q], b.cf_gu[q]);
+  if (!uni) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint needs a uniform mean flow");
+  if (!build_transpose(c->fd, &a.dT)) return fail(c, LEE_ERR_UNSUPPORTED, "difference operator too wide to transpose");
+  if (c->cfg.filter_scheme != LEE_FILTER_NONE && !build_transpose(c->flt, &a.fT))
+    return fail(c, LEE_ERR_UNSUPPORTED, "filter too wide to transpose");
+  // a line must keep the two ends' class rows apart, and a class row must only meet closure
+  // rows of its own end: n >= 2E and n >= E + H + h
+  const int n[3] = {b.nx, b.ny, b.nz};
+  int need = std::max(2 * a.dT.E, a.dT.E + a.dT.H + c->fd.h);
+  if (c->cfg.filter_scheme != LEE_FILTER_NONE) need = std::max(need, std::max(2 * a.fT.E, a.fT.E + a.fT.H + c->flt.h));
+  for (int d = 0; d < c->cfg.num_dim; ++d)
+    if (n[d] < need) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint needs %d points per direction", need);
+  int rc;
+  if ((rc = alloc_fields(c, a.lam, b.N)) || (rc = alloc_fields(c, a.mu, b.N)) || (rc = alloc_fields(c, a.kb[0], b.N)) ||
+      (rc = alloc_fields(c, a.kb[1], b.N)) || (rc = alloc_fields(c, a.ybar, b.N)))
+    return rc;
+  bool spg = false;
+  for (auto& z : b.bnd) spg |= z.kind == LEE_SPONGE_FREUND_AMBIENT;
+  if (spg && !b.d_sigma_field && (rc = build_sigma_field(c, b))) return rc;
+  if ((rc = dalloc(c, &a.d_base, 1))) return rc;
+  a.ready = true;
+  return LEE_OK;
+}
+
+// One transposed step: lam (adjoint of y_{n+1}) -> lam (adjoint of y_n); amps[s] are the
+// source amplitudes of the forward step's stages (gbar null: no source gradient).
+template <typename T>
+int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
+  auto& a = c->adj;
+  BlockData& b = c->blk[0];
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  const int V = c->V;
+  // mu = F^T lam: the directions commute, each is transposed, the last pass blends
+  void** mu = a.lam;
+  if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
+    const int n[3] = {b.nx, b.ny, b.nz};
+    int dirs[3], nd = 0;
+    for (int d = 0; d < c->cfg.num_dim; ++d)
+      if (n[d] > 1) dirs[nd++] = d;
+    void** src = a.lam;
+    for (int q = 0; q < nd; ++q) {
+      AdjFilterParams<T> fp;
+      memset(&fp, 0, sizeof fp);
+      fp.nx = b.nx; fp.ny = b.ny; fp.nz = b.nz; fp.V = V; fp.dir = dirs[q]; fp.last = q == nd - 1;
+      void** dst = fp.last ? a.mu : a.kb[q % 2];
+      for (int v = 0; v < V; ++v) {
+        fp.in[v] = (const T*)src[v];
+        fp.out[v] = (T*)dst[v];
+        fp.lam[v] = (const T*)a.lam[v];
+      }
+      fp.blend = (T)c->cfg.filter_blend;
+      fp.op = a.fT;
+      CK(launch_adj_filter<T>(fp, c->stream));
+      c->stats.kernel_launches += 1;
+      src = dst;
+    }
+    mu = a.mu;
+  }
+  const bool dbl = std::is_same<T, double>::value;
+  AdjStageParams<T> p;
+  memset(&p, 0, sizeof p);
+  p.nx = b.nx; p.ny = b.ny; p.nz = b.nz; p.V = V;
+  const Coef<T>* jm = dbl ? (const Coef<T>*)b.cd_jm : (const Coef<T>*)b.cf_jm;
+  for (int q = 0; q < 9; ++q) p.jm[q] = jm[q];
+  for (int x = 0; x < 3; ++x) p.ubar[x] = dbl ? (T)b.cd_ub[x].c : (T)b.cf_ub[x].c;
+  const T pb = dbl ? (T)b.cd_pb.c : (T)b.cf_pb.c;
+  p.gpb = (T)c->cfg.gamma * pb;
+  p.rbi = dbl ? (T)b.cd_rbi.c : (T)b.cf_rbi.c;
+  p.sigma = (const T*)b.d_sigma_field;
+  p.gbar = gbar;
+  for (int d = 0; d < 3; ++d) { p.src_lo[d] = b.src_lo[d]; p.src_hi[d] = b.src_hi[d]; }
+  p.op = a.dT;
+  const int ns = tb.ns;
+  int cur = 0;
+  for (int s = ns - 1; s >= 0; --s) {
+    p.first = s == ns - 1;
+    p.has_next = s > 0;
+    p.hb_in = (T)(dt * tb.b[ns - 1]);
+    p.hb_next = s > 0 ? (T)(dt * tb.b[s - 1]) : T(0);
+    p.ha_next = s > 0 ? (T)(tb.a[s - 1] * dt) : T(0);
+    p.amp = amps ? amps[s] : 0.0;
+    for (int v = 0; v < V; ++v) {
+      p.kin[v] = (const T*)(p.first ? mu[v] : a.kb[cur][v]);
+      p.mu[v] = (const T*)mu[v];
+      p.ybar[v] = (T*)a.ybar[v];
+      p.kout[v] = (T*)a.kb[1 - cur][v];
+    }
+    CK(launch_adj_stage<T>(p, c->cfg.num_dim, c->stream));
+    c->stats.kernel_launches += 1;
+    if (!p.first) cur = 1 - cur;
+    else cur = 1;  // the first processed stage wrote kb[1]
+  }
+  swap_fields(V, a.lam, a.ybar);
+  return LEE_OK;
 }
 
 }  // namespace
@@ -1362,6 +1649,19 @@ int lee_set_source(lee_ctx* c, int kind, const double* params, int nparams) {
   if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_source after lee_prepare");
   if (kind == LEE_SOURCE_NONE) {
     c->src_kind = kind;
+    return LEE_OK;
+  }
+  if (kind == LEE_SOURCE_DISTRIBUTED) {
+    if (!params || nparams < 11) return fail(c, LEE_ERR_ARG, "distributed source takes 11 + lattice params");
+    const int b = (int)params[0], cx = (int)params[2], cy = (int)params[3], cz = (int)params[4];
+    if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "distributed source block");
+    if (cx < 2 || cy < 2 || cz < 1 || (c->cfg.num_dim == 3 && cz < 2) || (c->cfg.num_dim == 2 && cz != 1))
+      return fail(c, LEE_ERR_ARG, "distributed source lattice %d x %d x %d", cx, cy, cz);
+    if ((long long)nparams != 11 + (long long)cx * cy * cz) return fail(c, LEE_ERR_ARG, "distributed source size");
+    if (!(params[8] > 0.0 && params[9] > 0.0 && (cz == 1 || params[10] > 0.0)))
+      return fail(c, LEE_ERR_ARG, "distributed source spacing must be positive");
+    c->src_kind = kind;
+    c->dsrc.assign(params, params + nparams);
     return LEE_OK;
   }
   if (kind != LEE_SOURCE_MONOPOLE || !params || nparams != 7) return fail(c, LEE_ERR_ARG, "monopole takes 7 params");
@@ -1659,6 +1959,22 @@ int lee_prepare(lee_ctx* c) {
         }
       }
     }
+    if (c->src_kind == LEE_SOURCE_DISTRIBUTED && (int)(&b - &c->blk[0]) == (int)c->dsrc[0]) {
+      int lo[3], hi[3];
+      std::vector<double> g;
+      if (!distributed_box(c->dsrc, c->cfg.num_dim, b.nx, b.ny, b.nz, lo, hi))
+        return fail(c, LEE_ERR_ARG, "the distributed source lattice covers no grid point");
+      prolong(c->dsrc, c->cfg.num_dim, lo, hi, c->dsrc.data() + 11, g);
+      if ((rc = upload(c, &b.d_src_g, g))) return rc;
+      for (int d = 0; d < 3; ++d) { b.src_lo[d] = lo[d]; b.src_hi[d] = hi[d]; }
+      if (c->comp) {
+        float* f = nullptr;
+        if ((rc = dalloc(c, &f, g.size()))) return rc;
+        k_convert<float><<<grid1d((long long)g.size()), 256, 0, s>>>((long long)g.size(), f, b.d_src_g);
+        CK(cudaGetLastError());
+        b.d_src_g_t = f;
+      }
+    }
     CK(cudaStreamSynchronize(s));
     // coefficient fields: constant ones become kernel constants
     b.n_coef_fields = 0;
@@ -1911,7 +2227,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     StageParams<double> p;
     fill_stage_common<double>(c, bk, p);
     p.stage = -1;
-    p.src_amp = c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, time) : 0.0;
+    p.src_amp = c->src_kind != LEE_SOURCE_NONE ? source_amp(c, time) : 0.0;
     p.rho_prev = bk.rho_valid ? (const double*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const double*)bk.y[v];
@@ -1925,7 +2241,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     StageParams<float> p;
     fill_stage_common<float>(c, bk, p);
     p.stage = -1;
-    p.src_amp = (float)(c->src_kind == LEE_SOURCE_MONOPOLE ? source_amp(c, time) : 0.0);
+    p.src_amp = (float)(c->src_kind != LEE_SOURCE_NONE ? source_amp(c, time) : 0.0);
     p.rho_prev = bk.rho_valid ? (const float*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const float*)bk.y[v];
@@ -2004,6 +2320,253 @@ int lee_set_timing(lee_ctx* c, int on) {
   if (!c) return LEE_ERR_ARG;
   c->timing = on != 0;
   return LEE_OK;
+}
+
+int lee_set_objective(lee_ctx* c, int b, int n, const long long* l0, double weight) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "objective block");
+  if (n < 1 || !l0) return fail(c, LEE_ERR_ARG, "the objective needs microphones");
+  const BlockData& bk = c->blk[(size_t)b];
+  std::vector<long long> mic(l0, l0 + n);
+  std::vector<long long> sorted = mic;
+  std::sort(sorted.begin(), sorted.end());
+  for (size_t m = 0; m < sorted.size(); ++m) {
+    if (sorted[m] < 0 || sorted[m] >= bk.N) return fail(c, LEE_ERR_ARG, "microphone %zu outside the block", m);
+    if (m && sorted[m] == sorted[m - 1]) return fail(c, LEE_ERR_ARG, "two microphones on one point");
+  }
+  CK(cudaSetDevice(c->cfg.device));
+  auto& a = c->adj;
+  if (a.mic.size() != mic.size()) {
+    int rc = dalloc(c, &a.d_mic, mic.size());
+    if (rc) return rc;
+  }
+  a.mic = mic;
+  a.mic_block = b;
+  a.weight = weight;
+  CK(cudaMemcpyAsync(a.d_mic, a.mic.data(), a.mic.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  if (!a.d_base) {
+    int rc = dalloc(c, &a.d_base, 1);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return LEE_OK;
+}
+
+namespace {
+
+// Trace rows for nsteps steps (reallocated when too short).
+int ensure_trace(lee_ctx* c, size_t rows) {
+  auto& a = c->adj;
+  if (a.trace_rows >= rows) return LEE_OK;
+  int rc = dalloc(c, &a.d_trace, rows * a.mic.size());
+  if (rc) return rc;
+  a.trace_rows = rows;
+  return LEE_OK;
+}
+
+// Advance nsteps with the microphone traces written from row 0.
+int advance_traced(lee_ctx* c, int nsteps, double dt, int row0) {
+  auto& a = c->adj;
+  a.trace_on = true;
+  a.host_row = row0;
+  int rc = c->comp ? advance_impl<float>(c, nsteps, dt) : advance_impl<double>(c, nsteps, dt);
+  a.trace_on = false;
+  return rc;
+}
+
+double objective_of(const lee_ctx* c, const std::vector<double>& tr) {
+  double J = 0.0;
+  for (double v : tr) J += v * v;
+  return c->adj.weight * J;
+}
+
+}  // namespace
+
+int lee_eval_objective(lee_ctx* c, int nsteps, double dt, double* J) {
+  if (!c || !J) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (c->adj.mic.empty()) return fail(c, LEE_ERR_STATE, "lee_set_objective first");
+  if (nsteps < 1 || !(dt > 0.0)) return fail(c, LEE_ERR_ARG, "nsteps >= 1 and dt > 0");
+  CK(cudaSetDevice(c->cfg.device));
+  memset(&c->stats, 0, sizeof c->stats);
+  int rc = ensure_trace(c, (size_t)nsteps);
+  if (rc) return rc;
+  if ((rc = advance_traced(c, nsteps, dt, 0))) return rc;
+  std::vector<double> tr((size_t)nsteps * c->adj.mic.size());
+  CK(cudaMemcpyAsync(tr.data(), c->adj.d_trace, tr.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *J = objective_of(c, tr);
+  return check_device_error(c);
+}
+
+int lee_apply_adjoint(lee_ctx* c, int nsteps, double dt) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (nsteps < 0 || !(dt > 0.0)) return fail(c, LEE_ERR_ARG, "nsteps >= 0 and dt > 0");
+  CK(cudaSetDevice(c->cfg.device));
+  int rc = adjoint_setup(c);
+  if (rc) return rc;
+  BlockData& b = c->blk[0];
+  auto& a = c->adj;
+  const size_t bytes = (size_t)b.N * c->esz;
+  // the state slots hold the adjoint variable (with a compensated state, y + e rounded)
+  for (int v = 0; v < c->V; ++v) {
+    if (c->comp) {
+      k_add_pair<<<grid1d(b.N), 256, 0, c->stream>>>(b.N, (float*)a.lam[v], (const float*)b.y[v],
+                                                      (const float*)b.comp[v]);
+      CK(cudaGetLastError());
+    } else {
+      CK(cudaMemcpyAsync(a.lam[v], b.y[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+  }
+  for (int it = 0; it < nsteps; ++it) {
+    rc = c->comp ? adjoint_step<float>(c, dt, nullptr, nullptr) : adjoint_step<double>(c, dt, nullptr, nullptr);
+    if (rc) return rc;
+  }
+  for (int v = 0; v < c->V; ++v) {
+    CK(cudaMemcpyAsync(b.y[v], a.lam[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->comp) CK(cudaMemsetAsync(b.comp[v], 0, bytes, c->stream));
+  }
+  b.rho_valid = false;
+  CK(cudaStreamSynchronize(c->stream));
+  return check_device_error(c);
+}
+
+int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every, int recompute, double* J,
+                         double* grad, long long* trace_mismatches) {
+  if (!c || !J || !grad) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (c->adj.mic.empty()) return fail(c, LEE_ERR_STATE, "lee_set_objective first");
+  if (c->src_kind != LEE_SOURCE_DISTRIBUTED) return fail(c, LEE_ERR_STATE, "the gradient is for a distributed source");
+  if (nsteps < 1 || checkpoint_every < 1 || !(dt > 0.0)) return fail(c, LEE_ERR_ARG, "nsteps, checkpoint_every, dt");
+  if (c->adj.mic_block != 0) return fail(c, LEE_ERR_ARG, "objective block");
+  CK(cudaSetDevice(c->cfg.device));
+  memset(&c->stats, 0, sizeof c->stats);
+  int rc = adjoint_setup(c);
+  if (rc) return rc;
+  auto& a = c->adj;
+  BlockData& b = c->blk[0];
+  const int V = c->V;
+  const size_t bytes = (size_t)b.N * c->esz;
+  const int K = checkpoint_every;
+  const int nseg = (nsteps + K - 1) / K;
+  const int fields = c->comp ? 2 * V : V;
+  // checkpoint slots: the state at the start of every segment
+  if (a.ckpt_slots < (size_t)nseg) {
+    for (size_t q = a.ckpt.size(); q < (size_t)nseg * fields; ++q) {
+      void* p = nullptr;
+      if ((rc = dev_alloc(c, &p, bytes))) return rc;
+      a.ckpt.push_back(p);
+    }
+    a.ckpt_slots = (size_t)nseg;
+  }
+  if ((rc = ensure_trace(c, (size_t)nsteps))) return rc;
+  auto save = [&](int seg) -> int {
+    for (int v = 0; v < V; ++v) {
+      CK(cudaMemcpyAsync(a.ckpt[(size_t)seg * fields + v], b.y[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      if (c->comp)
+        CK(cudaMemcpyAsync(a.ckpt[(size_t)seg * fields + V + v], b.comp[v], bytes, cudaMemcpyDeviceToDevice,
+                           c->stream));
+    }
+    return LEE_OK;
+  };
+  auto restore = [&](int seg) -> int {
+    for (int v = 0; v < V; ++v) {
+      CK(cudaMemcpyAsync(b.y[v], a.ckpt[(size_t)seg * fields + v], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      if (c->comp)
+        CK(cudaMemcpyAsync(b.comp[v], a.ckpt[(size_t)seg * fields + V + v], bytes, cudaMemcpyDeviceToDevice,
+                           c->stream));
+    }
+    return LEE_OK;
+  };
+  // forward pass: checkpoints, traces, the stage times of every step
+  const int step_start = c->step;
+  std::vector<double> seg_time((size_t)nseg);
+  for (int seg = 0; seg < nseg; ++seg) {
+    const int n = std::min(K, nsteps - seg * K);
+    seg_time[(size_t)seg] = c->time;
+    if ((rc = save(seg))) return rc;
+    if ((rc = advance_traced(c, n, dt, seg * K))) return rc;
+  }
+  const long long fwd_launches = c->stats.kernel_launches;
+  std::vector<double> tr((size_t)nsteps * a.mic.size());
+  CK(cudaMemcpyAsync(tr.data(), a.d_trace, tr.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *J = objective_of(c, tr);
+  // final state, kept aside while segments are recomputed
+  const double t_end = c->time;
+  const int step_end = c->step;
+  std::vector<void*> fin;
+  if (recompute) {
+    for (int q = 0; q < fields; ++q) {
+      void* p = nullptr;
+      CK(cudaMallocAsync(&p, bytes, c->stream));
+      fin.push_back(p);
+      CK(cudaMemcpyAsync(p, q < V ? b.y[q] : b.comp[q - V], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+  }
+  // reverse sweep
+  const size_t nbox = (size_t)(b.src_hi[0] - b.src_lo[0] + 1) * (b.src_hi[1] - b.src_lo[1] + 1) *
+                      (b.src_hi[2] - b.src_lo[2] + 1);
+  if (!a.d_gbar && (rc = dalloc(c, &a.d_gbar, nbox))) return rc;
+  CK(cudaMemsetAsync(a.d_gbar, 0, nbox * sizeof(double), c->stream));
+  for (int v = 0; v < V; ++v) CK(cudaMemsetAsync(a.lam[v], 0, bytes, c->stream));
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  const size_t M = a.mic.size();
+  const double scale = 2.0 * a.weight;
+  const int P = V - 1;
+  long long mismatches = 0;
+  std::vector<double> tr2;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int n0 = seg * K, n = std::min(K, nsteps - n0);
+    if (recompute) {
+      // the segment's forward steps again, from its checkpoint; their traces must repeat
+      if ((rc = restore(seg))) return rc;
+      c->time = seg_time[(size_t)seg];
+      c->step = step_start + n0;
+      if ((rc = advance_traced(c, n, dt, n0))) return rc;
+      tr2.assign((size_t)n * M, 0.0);
+      CK(cudaMemcpyAsync(tr2.data(), a.d_trace + (size_t)n0 * M, tr2.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      for (size_t q = 0; q < tr2.size(); ++q) mismatches += tr2[q] != tr[(size_t)n0 * M + q];
+    }
+    // stage times of each step of the segment, advanced as the forward steps advance them
+    std::vector<double> amps((size_t)n * tb.ns);
+    double t = seg_time[(size_t)seg];
+    for (int k = 0; k < n; ++k) {
+      t += dt;
+      for (int s = 0; s < tb.ns; ++s) amps[(size_t)k * tb.ns + s] = source_amp(c, t + tb.c[s] * dt);
+    }
+    for (int k = n - 1; k >= 0; --k) {
+      const int step = n0 + k;  // 0-based: this transposed step maps the adjoint of y_{step+1} to y_step
+      if (c->comp)
+        CK(launch_mic_force<float>((int)M, a.d_mic, (float*)a.lam[P], a.d_trace, step, scale, c->stream));
+      else
+        CK(launch_mic_force<double>((int)M, a.d_mic, (double*)a.lam[P], a.d_trace, step, scale, c->stream));
+      rc = c->comp ? adjoint_step<float>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar)
+                   : adjoint_step<double>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar);
+      if (rc) return rc;
+    }
+  }
+  // source-box gradient -> lattice gradient
+  std::vector<double> gbox(nbox);
+  CK(cudaMemcpyAsync(gbox.data(), a.d_gbar, nbox * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  restrict_to_lattice(c->dsrc, c->cfg.num_dim, b.src_lo, b.src_hi, gbox.data(), grad);
+  if (recompute) {
+    for (int q = 0; q < fields; ++q) {
+      CK(cudaMemcpyAsync(q < V ? b.y[q] : b.comp[q - V], fin[(size_t)q], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaFreeAsync(fin[(size_t)q], c->stream));
+    }
+    c->time = t_end;
+    c->step = step_end;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  (void)fwd_launches;
+  if (trace_mismatches) *trace_mismatches = mismatches;
+  return check_device_error(c);
 }
 
 int lee_set_graphs(lee_ctx* c, int on) {

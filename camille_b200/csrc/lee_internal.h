@@ -160,6 +160,68 @@ template <typename T>
 cudaError_t launch_rho(long long n, int V, T* const* y, T* const* e, const double* pbar, double gamma, T* out,
                        cudaStream_t s);
 
+// ---- discrete adjoint (lee_adjoint.cu) ----------------------------------------------------
+// The transpose of one directional operator (difference or filter) with its boundary closures:
+// out_i = sum_t w[t] in_{i+t}, t = -H..H, with w the interior row `in`, or a class row for
+// the E outputs nearest each end (lt[r]: position r; rt[r]: position n-1-r).
+constexpr int kTH = 8;
+constexpr int kTE = 16;
+struct TransOp {
+  int H, E;
+  double in[2 * kTH + 1];
+  double lt[kTE][2 * kTH + 1];
+  double rt[kTE][2 * kTH + 1];
+};
+
+// One adjoint RK stage s (processed from the last stage down): zbar = L^T kin, with L the
+// uniform-mean LEE operator (chain rule through J*metrics, sponge); ybar accumulates zbar
+// (first processed stage: ybar = mu + zbar), and the next input is
+// kout = hb_next * mu + ha_next * zbar. The distributed source's box field gathers
+// amp * kin[p'] (kin = hb_in * mu on the first processed stage).
+template <typename T>
+struct AdjStageParams {
+  int nx, ny, nz, V;
+  int first, has_next;
+  T hb_in, hb_next, ha_next;
+  const T* kin[kMaxVars];
+  const T* mu[kMaxVars];
+  T* ybar[kMaxVars];
+  T* kout[kMaxVars];
+  Coef<T> jm[9];
+  T ubar[3];
+  T gpb, rbi;
+  const T* sigma;
+  double* gbar;
+  double amp;
+  int src_lo[3], src_hi[3];
+  TransOp op;
+};
+
+// One direction of the transposed filter; the last pass blends (1 - beta) lam + beta F^T(...).
+template <typename T>
+struct AdjFilterParams {
+  int nx, ny, nz, V, dir, last;
+  const T* in[kMaxVars];
+  T* out[kMaxVars];
+  const T* lam[kMaxVars];
+  T blend;
+  TransOp op;
+};
+
+template <typename T>
+cudaError_t launch_adj_stage(const AdjStageParams<T>& p, int dim, cudaStream_t s);
+template <typename T>
+cudaError_t launch_adj_filter(const AdjFilterParams<T>& p, cudaStream_t s);
+// trace[row * n + m] = p'(l0[m]) (+ its carried error), row = *ctr + *base in a replayed
+// graph, else `row`
+template <typename T>
+cudaError_t launch_trace(int n, const long long* l0, const T* p, const T* e, double* trace, const int* ctr,
+                         const int* base, int row, cudaStream_t s);
+// lam_p[l0[m]] += scale * trace[row * n + m]
+template <typename T>
+cudaError_t launch_mic_force(int n, const long long* l0, T* lam_p, const double* trace, int row, double scale,
+                             cudaStream_t s);
+
 // lee_step.cu
 template <typename T>
 cudaError_t launch_stage(const StageParams<T>& p, int comp, cudaStream_t s);

@@ -69,6 +69,13 @@ extern "C" {
 /* physical sources */
 #define LEE_SOURCE_NONE 0
 #define LEE_SOURCE_MONOPOLE 1  /* params: x0, y0, z0, amplitude, omega, halfwidth, ramp_time */
+/* Distributed monopole (no reference counterpart: the reference cannot express it): on block
+ * `block`, rhs[p'] += (gamma - 1) sin(omega t) S(l), with S the trilinear prolongation of a
+ * coarse amplitude lattice of cx x cy x cz nodes whose node (p, q, r) sits at the fractional
+ * grid index (ox + p hx, oy + q hy, oz + r hz); S is zero outside the lattice's box.
+ * params: block, omega, cx, cy, cz, ox, oy, oz, hx, hy, hz, then cx*cy*cz amplitudes
+ * (p fastest). In 2-D, cz = 1. */
+#define LEE_SOURCE_DISTRIBUTED 2
 
 /* lee_get_setup selectors: products of the one-time setup, per block */
 #define LEE_SETUP_METRICS 0     /* 9 fields, metrics[l][i] = (1/J) dxi_l/dx_i, row-major (l*3+i) */
@@ -201,6 +208,31 @@ int lee_set_timing(lee_ctx *ctx, int on);
  * group of steps. Off, or while kernel timing is on, every launch is issued on its own. The
  * results are the same either way. */
 int lee_set_graphs(lee_ctx *ctx, int on);
+
+/* ---- discrete adjoint (no reference counterpart: the reference has no adjoint) ----------
+ * The step map of lee_advance is linear in the state; these entry points apply its exact
+ * transpose (transposed stencils and closures, transposed filter, reverse RK stages) on a
+ * single-block context with a uniform mean flow, sponges allowed, no BC lines, holes or
+ * overset. */
+/* Objective J = weight * sum over steps n = 1..N of sum over microphones m of p'_n(l[m])^2,
+ * p' of block b at linear indices l[m] (distinct) after every step. */
+int lee_set_objective(lee_ctx *ctx, int b, int n, const long long *l, double weight);
+/* Advance nsteps as lee_advance does and return J over those steps. */
+int lee_eval_objective(lee_ctx *ctx, int nsteps, double dt, double *J);
+/* Replace the uploaded state x by (M^T)^nsteps x, M the source-free step map of lee_advance
+ * (the dot-product test: <l, M x> = <M^T l, x>). */
+int lee_apply_adjoint(lee_ctx *ctx, int nsteps, double dt);
+/* J over nsteps from the uploaded state and its gradient with respect to the amplitudes of
+ * the LEE_SOURCE_DISTRIBUTED lattice (grad: cx*cy*cz values), by the discrete adjoint: the
+ * forward pass records the microphone traces and keeps the state every checkpoint_every
+ * steps; the reverse sweep goes segment by segment from the last. recompute = 1: each
+ * segment's forward steps are run again from its checkpoint before its reverse sweep, and
+ * *trace_mismatches counts recomputed trace values that differ from the first pass (0 when
+ * the replay is bit-identical); recompute = 0: the first pass's traces drive the sweep (the
+ * operator is linear, so the sweep needs no other forward state). On return the context
+ * holds the state after nsteps. */
+int lee_adjoint_gradient(lee_ctx *ctx, int nsteps, double dt, int checkpoint_every, int recompute, double *J,
+                         double *grad, long long *trace_mismatches);
 int lee_get_stats(lee_ctx *ctx, lee_stats *stats);
 
 /* The filter of one field, with no device allocation (no counterpart in the reference: it

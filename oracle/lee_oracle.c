@@ -78,6 +78,12 @@ struct orc_ctx {
   blk_t blk[MAXB];
   int src_kind;
   double src[7];
+  double *dsrc;  /* distributed source parameters */
+  int ndsrc;
+  double *dsrc_g; /* its prolonged field on block dsrc[0] (full grid, zero outside the lattice) */
+  int mic_block, nmic; /* objective: p' at microphones */
+  long long *mic;
+  double mic_weight;
   int prepared, step;
   double time;
   ovs_t ovs;
@@ -480,6 +486,10 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
   free(df);
   free(work);
   if (rc) return rc;
+  if (c->src_kind == LEE_SOURCE_DISTRIBUTED && bk == &c->blk[(int)c->dsrc[0]] && c->dsrc_g) {
+    double fac = (g - 1.0) * sin(c->dsrc[1] * time);
+    for (int p = 0; p < N; ++p) rhs[4][p] += fac * c->dsrc_g[p];
+  }
   if (c->src_kind == LEE_SOURCE_MONOPOLE) { /* oracle patch P2 (oracle/ref_patch_source.cpp) */
     double x0 = c->src[0], y0 = c->src[1], z0 = c->src[2], amp = c->src[3], om = c->src[4];
     double b = c->src[5], T = c->src[6];
@@ -672,6 +682,7 @@ void orc_destroy(orc_ctx *c) {
     for (int q = 0; q < bk->nbnd; ++q) free(bk->bnd[q].sigma);
   }
   free(c->ovs.rb); free(c->ovs.db); free(c->ovs.rl); free(c->ovs.dl); free(c->ovs.wt); free(c->ovs.buf);
+  free(c->dsrc); free(c->dsrc_g); free(c->mic);
   free(c);
 }
 
@@ -723,8 +734,58 @@ int orc_add_boundary(orc_ctx *c, int b, int kind, int dir, int end, const int lo
 
 int orc_set_source(orc_ctx *c, int kind, const double *params, int np) {
   c->src_kind = kind;
+  if (kind == LEE_SOURCE_DISTRIBUTED) {
+    free(c->dsrc);
+    c->dsrc = dalloc((size_t)np);
+    memcpy(c->dsrc, params, sizeof(double) * (size_t)np);
+    c->ndsrc = np;
+    return LEE_OK;
+  }
   for (int i = 0; i < 7 && i < np; ++i) c->src[i] = params[i];
   return LEE_OK;
+}
+
+/* The distributed source's lattice weights and trilinear prolongation (the same arithmetic
+ * as the CUDA library's host setup): node (p,q,r) at grid index (o + p h) per direction. */
+static void lattice_weights(double i, double o, double h, int cn, int *p0, double *f) {
+  double u = (i - o) / h;
+  int q = (int)floor(u);
+  if (q > cn - 2) q = cn - 2;
+  if (q < 0) q = 0;
+  *p0 = q;
+  *f = u - q;
+}
+
+static void prolong_distributed(orc_ctx *c, blk_t *bk) {
+  const double *p = c->dsrc, *A = c->dsrc + 11;
+  int dim = c->cfg.num_dim, cx = (int)p[2], cy = (int)p[3];
+  int n[3] = {bk->nx, bk->ny, bk->nz}, lo[3], hi[3];
+  c->dsrc_g = dalloc((size_t)bk->N);
+  for (int d = 0; d < 3; ++d) {
+    if (d >= dim) { lo[d] = hi[d] = 0; continue; }
+    lo[d] = (int)ceil(p[5 + d]);
+    if (lo[d] < 0) lo[d] = 0;
+    hi[d] = (int)floor(p[5 + d] + ((int)p[2 + d] - 1) * p[8 + d]);
+    if (hi[d] > n[d] - 1) hi[d] = n[d] - 1;
+  }
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i) {
+        int q[3] = {0, 0, 0};
+        double f[3] = {0.0, 0.0, 0.0};
+        lattice_weights(i, p[5], p[8], cx, &q[0], &f[0]);
+        lattice_weights(j, p[6], p[9], cy, &q[1], &f[1]);
+        if (dim == 3) lattice_weights(k, p[7], p[10], (int)p[4], &q[2], &f[2]);
+        double sum = 0.0;
+        for (int c2 = 0; c2 < (dim == 3 ? 2 : 1); ++c2)
+          for (int c1 = 0; c1 < 2; ++c1)
+            for (int c0 = 0; c0 < 2; ++c0) {
+              double w = (c0 ? f[0] : 1.0 - f[0]) * (c1 ? f[1] : 1.0 - f[1]) *
+                         (dim == 3 ? (c2 ? f[2] : 1.0 - f[2]) : 1.0);
+              sum += w * A[(q[0] + c0) + (size_t)cx * ((q[1] + c1) + (size_t)cy * (q[2] + c2))];
+            }
+        c->dsrc_g[i + (size_t)bk->nx * (j + (size_t)bk->ny * k)] = sum;
+      }
 }
 
 /* overset::initialize_overset (src/overset/overset.cpp:56-84): the maps of the
@@ -877,6 +938,7 @@ int orc_prepare(orc_ctx *c) {
       }
     free(work);
     compute_aux(c, bk, bk->sol);
+    if (c->src_kind == LEE_SOURCE_DISTRIBUTED && b == (int)c->dsrc[0]) prolong_distributed(c, bk);
   }
   c->prepared = 1;
   return LEE_OK;
@@ -1077,6 +1139,46 @@ int orc_set_timing(orc_ctx *c, int on) {
   (void)c;
   (void)on;
   return LEE_OK;
+}
+
+/* The microphone objective J = weight * sum_n sum_m p'_n(l_m)^2 (the same definition as the
+ * CUDA library's), evaluated on the oracle's own steps. */
+int orc_set_objective(orc_ctx *c, int b, int n, const long long *l, double weight) {
+  if (b < 0 || b >= c->nblk || n < 1) return fail(c, LEE_ERR_ARG, "objective");
+  free(c->mic);
+  c->mic = (long long *)malloc(sizeof(long long) * (size_t)n);
+  memcpy(c->mic, l, sizeof(long long) * (size_t)n);
+  c->nmic = n;
+  c->mic_block = b;
+  c->mic_weight = weight;
+  return LEE_OK;
+}
+
+int orc_eval_objective(orc_ctx *c, int nsteps, double dt, double *J) {
+  double acc = 0.0;
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = orc_advance(c, 1, dt);
+    if (rc) return rc;
+    for (int m = 0; m < c->nmic; ++m) {
+      double p = c->blk[c->mic_block].sol[4][c->mic[m]];
+      acc += p * p;
+    }
+  }
+  *J = c->mic_weight * acc;
+  return LEE_OK;
+}
+
+/* The adjoint is not restated on the CPU: it is checked against the CUDA forward map
+ * (dot-product test) and against oracle objectives (finite differences). */
+int orc_apply_adjoint(orc_ctx *c, int nsteps, double dt) {
+  (void)nsteps; (void)dt;
+  return fail(c, LEE_ERR_UNSUPPORTED, "the oracle has no adjoint");
+}
+
+int orc_adjoint_gradient(orc_ctx *c, int nsteps, double dt, int k, int recompute, double *J, double *grad,
+                         long long *mism) {
+  (void)nsteps; (void)dt; (void)k; (void)recompute; (void)J; (void)grad; (void)mism;
+  return fail(c, LEE_ERR_UNSUPPORTED, "the oracle has no adjoint");
 }
 
 int orc_set_graphs(orc_ctx *c, int on) {
