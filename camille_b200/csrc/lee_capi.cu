@@ -1145,7 +1145,9 @@ std::vector<void*> layout_of(lee_ctx* c) {
     l.push_back((void*)(uintptr_t)(b.rho_valid ? 1 : 0));
   }
   l.push_back((void*)(uintptr_t)(c->adj.trace_on ? 1 : 0));
-  l.push_back(c->adj.d_trace);
+  l.push_back(c->adj.d_trace);  // buffers a captured step reads through baked-in pointers
+  l.push_back(c->adj.d_base);
+  l.push_back(c->adj.d_mic);
   return l;
 }
 
@@ -1405,7 +1407,7 @@ int adjoint_setup(lee_ctx* c) {
   bool spg = false;
   for (auto& z : b.bnd) spg |= z.kind == LEE_SPONGE_FREUND_AMBIENT;
   if (spg && !b.d_sigma_field && (rc = build_sigma_field(c, b))) return rc;
-  if ((rc = dalloc(c, &a.d_base, 1))) return rc;
+  if (!a.d_base && (rc = dalloc(c, &a.d_base, 1))) return rc;
   a.ready = true;
   return LEE_OK;
 }

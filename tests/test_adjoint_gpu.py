@@ -123,6 +123,24 @@ def test_gradient_central_differences_and_tangent_linear(product_lib, oracle_lib
         assert abs(tl - ad) <= 1e-8 * abs(tl), (tl, ad)
 
 
+def test_objective_then_gradient_on_one_context(product_lib):
+    """A context that evaluated the objective (and captured its step graph) gives the same J
+    from its gradient call, and the recomputed segments replay their traces bit for bit."""
+    case = _grad_case(nsteps=36)
+    s = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
+    dt = s.compute_dt()
+    s.advance(3, dt)
+    s.upload(0, case.blocks[0].state)
+    J0 = s.eval_objective(case.nsteps, dt)
+    s.upload(0, case.blocks[0].state)
+    J, g, mism = s.adjoint_gradient(case.nsteps, dt, checkpoint_every=8, recompute=True)
+    assert mism == 0 and J == J0
+    s.upload(0, case.blocks[0].state)
+    J2, g2, _ = s.adjoint_gradient(case.nsteps, dt, checkpoint_every=8, recompute=False)
+    assert J2 == J0
+    np.testing.assert_array_equal(g, g2)
+
+
 def test_recompute_replays_and_precisions_agree(product_lib):
     case = _grad_case(nsteps=30)
     s64 = api.Solver(product_lib, case)
