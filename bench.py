@@ -125,9 +125,103 @@ WORKLOADS = {
                "Freund sponges n/16 wide (constant 1)",
     "pulse2d": "pulse2d {n}^2 on [-50,50]^2, quiescent, Gaussian p' pulse, RK4 CFL 0.5, OA4 FD + OA8 filter, "
                "20-cell Freund sponges (constant 5)",
+    "batch": "batch2d: 64 independent 2-D Cartesian instances, sides round(exp(U[ln 64, ln 512])) (seed 4, "
+             "5.2M points), Mach U[0,0.6], monopole omega U[pi/10, pi/3], 20 N/256-cell sponges, RK4 CFL 0.5 per "
+             "instance, batched kernels (one launch per stage and per filter for all instances) in step graphs",
     "cylinder": "cylinder2d: background 512^2 on [-40,40]^2 + O-grid 384x96 (first cell 0.005), 4x4 Lagrange "
                 "overset, tanh shear layer damped at the wall, monopole (2,0) omega 0.8 pi, RK4 CFL 0.5",
 }
+
+
+def run_batch(args) -> None:
+    """64 instances advanced together (lee_advance_blocks, FP32-compensated and FP64)
+    and, as the comparison the config asks for, one at a time in plain FP64 (each instance in
+    its own context, its own time step)."""
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    K, W = args.steps, args.warmup
+    case = cases.batch2d(nsteps=K)
+    lib = api.product_library()
+    npts = case.npoints
+    res = {}
+    clocks = None
+    for form, prec in (("fp32c", api.FP32_COMPENSATED), ("fp64", api.FP64)):
+        s = api.Solver(lib, case, precision=prec)
+        dts = s.compute_dt_blocks()
+        s.advance_blocks(W, dts)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) if form == "fp32c" else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        s.advance_blocks(K, dts)
+        st = s.stats()
+        if sampler:
+            clocks = sampler.stop()
+        s.set_timing(True)
+        s.advance_blocks(min(K, args.kernel_steps), dts)
+        kst = s.stats()
+        s.set_timing(False)
+        res[form] = {"ms": st.advance_ms, "launches": st.kernel_launches, "kst": kst, "info": s.info(),
+                     "state": [s.download(b)[0] for b in range(len(case.blocks))], "dts": dts,
+                     "steps_done": W + K + min(K, args.kernel_steps)}
+        s.close()
+    # one at a time, plain FP64, the same steps
+    alone_s, errs = 0.0, []
+    n_done = res["fp32c"]["steps_done"]
+    for b in range(len(case.blocks)):
+        s = api.Solver(lib, cases.instance(case, b), precision=api.FP64)
+        dt = float(res["fp64"]["dts"][b])
+        s.advance(W, dt)
+        s.advance(K, dt)
+        alone_s += s.stats().advance_ms / 1e3
+        s.advance(n_done - W - K, dt)
+        y = s.download(0)[0]
+        errs.append(api.rel_l2(res["fp32c"]["state"][b][4], y[4]))
+        s.close()
+    value = npts * K / (res["fp32c"]["ms"] / 1e3)
+    value64 = npts * K / (res["fp64"]["ms"] / 1e3)
+    alone = npts * K / alone_s
+    kst = res["fp32c"]["kst"]
+    peak, peak_kind = measured_hbm_gbs()
+    stage_avg = kst.stage_ms / max(kst.stage_launches, 1)
+    filt_avg = kst.filter_ms / max(kst.filter_launches, 1)
+    info = res["fp32c"]["info"]
+    # 2-D FP32-compensated: stage words 4,5,5,5 x V (V = 4) + the sigma field + the J*metrics
+    # fields a block keeps (the off-diagonal terms carry rounding noise of 1e-15); filter 4 V words
+    stage_b = ((4 + 5 + 5 + 5) / 4.0 * 4 * 4 + 4 + 4 * info.num_coef_fields) * npts
+    filt_b = 4 * 4 * 4 * npts
+    step_b = 4 * stage_b + filt_b
+    achieved = stage_b / (stage_avg / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value * world, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": res["fp32c"]["ms"] / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32-compensated (fp64 setup)", "data": "synthetic",
+            "config": {"workload": WORKLOADS["batch"], "points_per_gpu": npts, "blocks": len(case.blocks),
+                       "l2": f"state {5 * npts * 4 / 1e6:.0f} MB fp32 vs 126 MB L2 (inputs larger than L2)",
+                       "launch": "batched kernels in replayed CUDA step graphs"},
+            "fp64": {"value": value64, "ms_per_step": res["fp64"]["ms"] / K},
+            "mixed_over_fp64": value / value64,
+            "one_at_a_time_fp64": {"value": alone, "ms_per_step": alone_s * 1e3 / K,
+                                   "batched_fp32c_over_it": value / alone},
+            "p_rel_l2_vs_fp64_alone": {"max": max(errs), "median": float(np.median(errs)), "steps": n_done},
+            "roofline": {"bound": "hbm", "kernel": "batched RK stage (fp32-compensated)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} copy bandwidth", "traffic": None,
+                         "avg_launch_ms": stage_avg, "filter_avg_launch_ms": filt_avg,
+                         "filter_gbs": filt_b / (filt_avg / 1e3) / 1e9,
+                         "step_gbs": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9,
+                         "step_frac": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9 / peak},
+            "e2e": None,
+            "gpu_launches": int(res["fp32c"]["launches"]),
+            "clocks": clocks,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line))
 
 
 def make_case(workload: str, n: int, nsteps: int) -> cases.Case:
@@ -257,6 +351,10 @@ def run_ours(args) -> None:
     step_gbs = step_b * K / (r32["ms"] / 1e3) / 1e9
     dominant = "stage" if st.stage_ms >= st.filter_ms else "filter"
 
+    adjoint = None
+    if args.workload == "curvi3d" and not args.no_adjoint:
+        adjoint = run_adjoint(args, lib, barrier, max_over_ranks)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
@@ -290,11 +388,46 @@ def run_ours(args) -> None:
             "gpu_launches": int(r32["stats"].kernel_launches),
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "adjoint": adjoint,
         }
         print(json.dumps(line))
     solvers["fp32c"].close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_adjoint(args, lib, barrier, max_over_ranks) -> dict:
+    """The adjoint workload: 192^3 curvilinear block, Mach 0.5, a 16^3 distributed
+    source, 64 microphones, FP32-compensated forward of `adjoint_steps` steps checkpointed every
+    100. Times the forward alone (lee_eval_objective) and the gradient (lee_adjoint_gradient)
+    with segment recompute and with the first pass's traces; each timed region is bracketed by
+    device synchronisation (lee_* calls return after their stream drained)."""
+    n, N = args.adjoint_n, args.adjoint_steps
+    case = cases.adjoint3d(n=n, nsteps=N, precompute=True)
+    s = api.Solver(lib, case, precision=api.FP32_COMPENSATED)
+    dt = s.compute_dt()
+    s.eval_objective(min(N, 20), dt)  # warm-up: graph capture, traces
+    out = {"workload": f"adjoint3d {n}^3 Mach 0.5, 16^3 distributed source (seed 5), 64 microphones, "
+                       f"{N} FP32-compensated RK4 steps, checkpoint every 100",
+           "steps": N}
+    s.upload(0, case.blocks[0].state)
+    barrier()
+    t0 = time.perf_counter()
+    J0 = s.eval_objective(N, dt)
+    fwd = max_over_ranks(time.perf_counter() - t0)
+    for label, rec in (("recompute", True), ("traces", False)):
+        s.upload(0, case.blocks[0].state)
+        barrier()
+        t0 = time.perf_counter()
+        J, g, mism = s.adjoint_gradient(N, dt, checkpoint_every=100, recompute=rec)
+        el = max_over_ranks(time.perf_counter() - t0)
+        out[label] = {"seconds": el, "adjoint_over_forward": el / fwd, "trace_mismatches": mism,
+                      "objective_matches_forward": J == J0}
+    out["forward_seconds"] = fwd
+    out["forward_ms_per_step"] = fwd * 1e3 / N
+    out["gradient_norm"] = float(np.linalg.norm(g))
+    s.close()
+    return out
 
 
 def reference_sample(args, workload: str, n: int, steps: int) -> tuple[cases.Case, str]:
@@ -368,6 +501,9 @@ def main() -> int:
                     help="steps launched one by one with events between launches (roofline)")
     ap.add_argument("--error-steps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing (configs[4])")
+    ap.add_argument("--adjoint-n", type=int, default=192)
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--cpu-n", type=int, default=64)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-n", type=int, default=64)
@@ -375,6 +511,8 @@ def main() -> int:
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)
     return 0

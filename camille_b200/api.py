@@ -46,7 +46,8 @@ class LeeInfo(C.Structure):
     _fields_ = [("points", C.c_longlong), ("state_vars", C.c_int), ("bytes_per_value", C.c_int),
                 ("num_coef_fields", C.c_int), ("device_bytes", C.c_longlong),
                 ("tma_stage", C.c_int), ("tma_filter", C.c_int), ("stage_chunk", C.c_int),
-                ("filter_chunk", C.c_int)]
+                ("filter_chunk", C.c_int), ("batched", C.c_int), ("batch_stage_tile", C.c_int * 2),
+                ("batch_filter_tile", C.c_int * 2)]
 
 
 class LeeStats(C.Structure):
@@ -75,6 +76,9 @@ SIGNATURES = {
     "set_mean": (C.c_int, [C.c_void_p, C.c_int, _PP]),
     "add_boundary": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP]),
     "set_source": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
+    "set_block_source": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _DP, C.c_int]),
+    "advance_blocks": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "compute_dt_blocks": (C.c_int, [C.c_void_p, C.c_double, _DP]),
     "set_overset": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP, _IP, _IP, _IP, _DP, C.c_int, _IP, _IP]),
     "read_overset_file": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "get_overset": (C.c_int, [C.c_void_p, _IP, _LP, _IP, _LP, _DP]),
@@ -171,6 +175,10 @@ class Solver:
             if case.monopole is not None:
                 p = np.array(case.monopole, np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))
+            for b, blk in enumerate(case.blocks):
+                if blk.monopole is not None:
+                    p = np.array(blk.monopole, np.float64)
+                    self._chk(lib.set_block_source(self.ctx, b, SOURCE_MONOPOLE, _dptr(p), len(p)))
             if case.distributed is not None:
                 p = np.ascontiguousarray(case.distributed.params(), np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_DISTRIBUTED, _dptr(p), len(p)))
@@ -234,6 +242,15 @@ class Solver:
 
     def advance(self, nsteps: int, dt: float) -> None:
         self._chk(self.lib.advance(self.ctx, nsteps, dt))
+
+    def compute_dt_blocks(self, cfl: Optional[float] = None) -> np.ndarray:
+        out = np.zeros(len(self.case.blocks), np.float64)
+        self._chk(self.lib.compute_dt_blocks(self.ctx, self.case.cfl if cfl is None else cfl, _dptr(out)))
+        return out
+
+    def advance_blocks(self, nsteps: int, dts) -> None:
+        d = np.ascontiguousarray(dts, np.float64)
+        self._chk(self.lib.advance_blocks(self.ctx, nsteps, _dptr(d)))
 
     def eval_rhs(self, b: int = 0, time: float = 0.0) -> np.ndarray:
         nx, ny, nz = self.case.blocks[b].dims

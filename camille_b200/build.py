@@ -26,6 +26,7 @@ UNITS = {
     "lee_static.cu": [],
     "lee_bc.cu": [],
     "lee_adjoint.cu": [],
+    "lee_batch.cu": [],
 }
 
 

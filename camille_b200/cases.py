@@ -49,6 +49,7 @@ class Block:
     mean: np.ndarray       # (5, nz, ny, nx): s_bar, u_bar, v_bar, w_bar, p_bar
     state: np.ndarray      # (5, nz, ny, nx): s', u', v', w', p'
     iblank: Optional[np.ndarray] = None  # (nz, ny, nx) int32: 0 fluid, 1 hole, -1 receiver
+    monopole: Optional[tuple[float, float, float, float, float, float, float]] = None  # this block's own
 
     @property
     def dims(self) -> tuple[int, int, int]:
@@ -543,3 +544,51 @@ def adjoint3d(n: int = 192, nsteps: int = 2000, seed: int = 5, mach: float = 0.5
     if precompute:
         precompute_sponges(case)
     return case
+
+
+def batch2d(count: int = 64, seed: int = 4, nmin: int = 64, nmax: int = 512, nsteps: int = 2000,
+            spacing: float = 100.0 / 255.0, gamma: float = 1.4, sponge_constant: float = 5.0,
+            spacing_spread: float = 1.0) -> Case:
+    """A batch of ``count`` independent square 2-D Cartesian instances (one block each) drawn by
+    ``numpy.random.default_rng(seed)``: side N = round(exp(U[ln nmin, ln nmax])) points at
+    ``spacing``, uniform mean Mach U[0, 0.6] along x, a monopole at a uniform position inside the
+    central half of the instance with angular frequency U[pi/10, pi/3], amplitude 1e-3, Gaussian
+    half-width 3 spacings and a sin^2 ramp over one period, and Freund sponges 20 N/256 cells
+    wide (at least 4) on every side. Each instance advances with its own CFL time step.
+    ``spacing_spread`` > 1 draws each instance's spacing log-uniformly in
+    [spacing / spread, spacing * spread] (after the draws above, so they are unchanged)."""
+    rng = np.random.default_rng(seed)
+    sides = np.rint(np.exp(rng.uniform(math.log(nmin), math.log(nmax), size=count))).astype(int)
+    draws = [(float(rng.uniform(0.0, 0.6)), float(rng.uniform(math.pi / 10.0, math.pi / 3.0)),
+              rng.uniform(-0.25, 0.25, size=2)) for _ in range(count)]
+    spacings = [spacing] * count
+    if spacing_spread > 1.0:
+        spacings = list(spacing * np.exp(rng.uniform(-math.log(spacing_spread), math.log(spacing_spread), count)))
+    blocks, bnd = [], []
+    for b, n in enumerate(sides):
+        n = int(n)
+        spacing = float(spacings[b])
+        mach, omega, pos = draws[b]
+        length = (n - 1) * spacing
+        sx, sy = pos * length
+        c1 = -0.5 * length + spacing * np.arange(n, dtype=np.float64)
+        y, x = np.meshgrid(c1, c1, indexing="ij")
+        x, y = x[None].copy(), y[None].copy()
+        mean = np.zeros((5,) + x.shape)
+        mean[1] = mach
+        mean[4] = 1.0 / gamma
+        blk = Block(x, y, np.zeros_like(x), mean, np.zeros((5,) + x.shape),
+                    monopole=(float(sx), float(sy), 0.0, 1e-3, omega, 3.0 * spacing, 2.0 * math.pi / omega))
+        blocks.append(blk)
+        width = max(4, int(round(20 * n / 256)))
+        bnd += sponge_frame(2, blk.dims, width, block=b)
+    return Case(name=f"batch2d_{count}", num_dim=2, blocks=blocks, gamma=gamma, nsteps=nsteps, boundaries=bnd,
+                sponge_constant=sponge_constant,
+                notes=f"{count} 2-D instances, sides {int(sides.min())}..{int(sides.max())}, seed {seed}")
+
+
+def instance(case: Case, b: int) -> Case:
+    """Block b of a batch as a single-block case of its own (its boundaries renumbered)."""
+    blk = case.blocks[b]
+    bnd = [dataclasses.replace(bd, block=0) for bd in case.boundaries if bd.block == b]
+    return dataclasses.replace(case, name=f"{case.name}_b{b}", blocks=[blk], boundaries=bnd)

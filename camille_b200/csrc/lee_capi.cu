@@ -59,6 +59,12 @@ struct BlockData {
   int8_t* d_code_flt[3] = {};
   bool has_holes = false;   // some point is BLANKED: hole closures and hole bypass
   bool has_iblank = false;  // some point is not NOTBLANKED (holes or receivers): CFL skips them
+  // per-block clock (blocks advanced with their own time steps keep their own time)
+  double time = 0.0;
+  int step = 0;
+  // source of this block: 0 the context's, 1 its own monopole (own_src), 2 none
+  int src_mode = 0;
+  double own_src[7] = {0, 0, 0, 0, 0, 0, 0};
   // monopole factor on a box
   int src_lo[3] = {0, 0, 0}, src_hi[3] = {-1, -1, -1};
   double* d_src_g = nullptr;
@@ -151,7 +157,7 @@ struct lee_ctx {
   struct {
     bool enabled = true;
     cudaGraphExec_t exec = nullptr;
-    double dt = 0.0;
+    std::vector<double> dts;       // the time step of every block
     int steps = 0;                 // steps per replay
     std::vector<void*> layout;
     long long launches = 0, stage_launches = 0, filter_launches = 0;  // per replay
@@ -159,6 +165,19 @@ struct lee_ctx {
     size_t amp_cap = 0;            // entries
     int* d_ctr = nullptr;          // steps of the current chunk done so far
   } graph;
+  // batched kernels for many independent 2-D blocks (lee_advance_blocks)
+  struct {
+    bool active = false;
+    int sshape = 0, fshape = 0, sgrid = 0, fgrid = 0;
+    int4* d_stiles = nullptr;
+    int nst = 0;
+    int4* d_ftiles = nullptr;
+    int nft = 0;
+    void* d_prm_graph = nullptr;   // StageParams [stage][block], monopole amplitudes from the graph table
+    void* d_prm_direct = nullptr;  // the same with the amplitudes of the step being launched
+    void* d_finst = nullptr;       // BatchFilterInst [block]
+    std::vector<double> graph_dts;  // time steps d_prm_graph was built for
+  } batch;
   // discrete adjoint (single block, uniform mean, no BC lines, holes or overset)
   struct {
     bool ready = false;
@@ -654,15 +673,24 @@ void restrict_to_lattice(const std::vector<double>& p, int dim, const int lo[3],
 }
 
 // Amplitude of the monopole at time t (oracle patch P2, modelled on src/solver/source.cpp:60-92).
-double source_amp(const lee_ctx* c, double t) {
+// The monopole parameters that apply to block b, or null when it has no monopole.
+const double* monopole_of(const lee_ctx* c, const BlockData& b) {
+  if (b.src_mode == 1) return b.own_src;
+  if (b.src_mode == 0 && c->src_kind == LEE_SOURCE_MONOPOLE && c->src[5] > 0.0) return c->src;
+  return nullptr;
+}
+
+double source_amp(const lee_ctx* c, const BlockData& b, double t) {
   if (c->src_kind == LEE_SOURCE_DISTRIBUTED) return (c->cfg.gamma - 1.0) * sin(c->dsrc[1] * t);
-  double T = c->src[6];
+  const double* m = monopole_of(c, b);
+  if (!m) return 0.0;
+  double T = m[6];
   double ramp = 1.0;
   if (T > 0.0 && t < T) {
     double sn = sin(0.5 * M_PI * t / T);
     ramp = sn * sn;
   }
-  return c->src[3] * (c->cfg.gamma - 1.0) * ramp * sin(c->src[4] * t);
+  return m[3] * (c->cfg.gamma - 1.0) * ramp * sin(m[4] * t);
 }
 
 // Dimension-split filter of `in` (spatial::apply_filter, src/solver/spatial_discretization.cpp:2191-2246).
@@ -1006,22 +1034,271 @@ Tableau tableau(int rk) {
   return t;
 }
 
+// p' at the microphones after a step (the objective's trace), in FP64.
+template <typename T>
+int trace_step(lee_ctx* c, const int* ctr) {
+  if (!c->adj.trace_on) return LEE_OK;
+  BlockData& b = c->blk[(size_t)c->adj.mic_block];
+  const int P = c->V - 1;
+  CK(launch_trace<T>((int)c->adj.mic.size(), c->adj.d_mic, (const T*)b.y[P], c->comp ? (const T*)b.comp[P] : nullptr,
+                     c->adj.d_trace, ctr, ctr ? c->adj.d_base : nullptr, c->adj.host_row, c->stream));
+  c->stats.kernel_launches += 1;
+  if (!ctr) c->adj.host_row += 1;
+  return LEE_OK;
+}
+
+// ---- batches of independent 2-D blocks ----------------------------------------------------
+
+// Blocks the batched kernels cover: 2-D, uniform mean, no holes,
+// BC lines or overset (sponges allowed), the 4th-order difference and the 8th-order filter.
+bool batch_eligible(const lee_ctx* c) {
+  if (c->cfg.num_dim != 2 || c->ovs.n > 0) return false;
+  if (!(c->fd.h == 2 && c->fd.S == 3)) return false;
+  if (c->cfg.filter_scheme != LEE_FILTER_STANDARD_CENTRAL || c->cfg.filter_order != 8) return false;
+  for (auto& b : c->blk) {
+    if (b.has_iblank || b.need_rho) return false;
+    for (auto& z : b.bnd)
+      if (z.kind != LEE_SPONGE_FREUND_AMBIENT) return false;
+    auto is_const = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? !f.p : !d.p; };
+    auto is_zero = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? f.zero != 0 : d.zero != 0; };
+    bool uni = is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi);
+    for (int q = 0; q < 3; ++q)
+      uni = uni && is_const(b.cd_ub[q], b.cf_ub[q]) && is_zero(b.cd_gs[q], b.cf_gs[q]) && is_zero(b.cd_gp[q], b.cf_gp[q]);
+    for (int q = 0; q < 9; ++q) uni = uni && is_zero(b.cd_gu[q], b.cf_gu[q]);
+    if (!uni) return false;
+  }
+  return true;
+}
+
+std::vector<int4> batch_tiles(const lee_ctx* c, int shape) {
+  int tx, ty;
+  batch_shape(shape, &tx, &ty);
+  std::vector<int4> t;
+  for (size_t b = 0; b < c->blk.size(); ++b)
+    for (int y0 = 0; y0 < c->blk[b].ny; y0 += ty)
+      for (int x0 = 0; x0 < c->blk[b].nx; x0 += tx) t.push_back(make_int4((int)b, x0, y0, 0));
+  return t;
+}
+
+// The stage parameters of every block for every stage, [stage][block]: `stage_override` >= 0
+// builds right-hand-side-only parameters (the autotuner's harmless launches).
+template <typename T>
+std::vector<StageParams<T>> batch_params(lee_ctx* c, const std::vector<double>& dts, bool graph, int rhs_only) {
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  const int ns = tb.ns, nbk = (int)c->blk.size();
+  std::vector<StageParams<T>> out((size_t)ns * nbk);
+  const bool src = c->src_kind != LEE_SOURCE_NONE;
+  for (int s = 0; s < ns; ++s)
+    for (int q = 0; q < nbk; ++q) {
+      BlockData& b = c->blk[(size_t)q];
+      StageParams<T>& p = out[(size_t)s * nbk + q];
+      fill_stage_common<T>(c, b, p);
+      const double dt = dts[(size_t)q];
+      p.stage = rhs_only ? -1 : s;
+      p.last = s == ns - 1;
+      p.h = (T)dt;
+      p.b = (T)tb.b[s];
+      p.a = (T)tb.a[s];
+      p.src_amp = (T)(src ? source_amp(c, b, b.time + tb.c[s] * dt) : 0.0);
+      if (graph && src) {
+        p.amp_tab = (const T*)c->graph.d_amp + (size_t)q * ns;
+        p.step_ctr = c->graph.d_ctr;
+        p.nstages = nbk * ns;
+      }
+      void** zin = s == 0 ? b.y : b.zb[(s + 1) % 2];
+      void** zout = rhs_only ? b.zb[0] : b.zb[s % 2];
+      if (rhs_only) zin = b.y;
+      for (int v = 0; v < c->V; ++v) {
+        p.zin[v] = (const T*)zin[v];
+        p.yn[v] = (const T*)b.y[v];
+        p.acc[v] = (T*)b.acc[v];
+        p.zout[v] = (T*)zout[v];
+        p.comp[v] = (T*)b.comp[v];
+      }
+      p.rho_prev = nullptr;
+    }
+  return out;
+}
+
+// Filter operands of every block; `scratch` sends the outputs to buffers that are free between
+// steps (the autotuner's harmless launches).
+template <typename T>
+std::vector<BatchFilterInst<T>> batch_filter_inst(lee_ctx* c, bool scratch) {
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  std::vector<BatchFilterInst<T>> out;
+  for (auto& b : c->blk) {
+    BatchFilterInst<T> f;
+    memset(&f, 0, sizeof f);
+    f.nx = b.nx;
+    f.ny = b.ny;
+    void** last_out = b.zb[(tb.ns - 1) % 2];
+    void** other = b.zb[tb.ns % 2];
+    for (int v = 0; v < c->V; ++v) {
+      f.x[v] = (const T*)(c->comp ? last_out[v] : b.acc[v]);
+      f.err[v] = c->comp ? (const T*)b.acc[v] : nullptr;
+      f.y[v] = (T*)(scratch ? other[v] : b.y[v]);
+      f.comp[v] = c->comp ? (T*)(scratch ? b.dsum[v] : b.comp[v]) : nullptr;
+    }
+    out.push_back(f);
+  }
+  return out;
+}
+
+template <typename T>
+int batch_launch_stage(lee_ctx* c, const void* prm, const int4* tiles, int nt, int shape, int grid) {
+  CK(launch_batch_stage<T>((const StageParams<T>*)prm, tiles, nt, shape, c->comp ? 1 : 0, grid, c->stream));
+  return LEE_OK;
+}
+
+template <typename T>
+int batch_launch_filter(lee_ctx* c, const void* inst, const int4* tiles, int nt, int shape, int grid) {
+  CK(launch_batch_filter<T>((const BatchFilterInst<T>*)inst, tiles, nt, shape, c->comp ? 1 : 0, grid,
+                            c->comp ? c->fltd : c->flt, c->cfg.filter_blend, c->stream));
+  return LEE_OK;
+}
+
+// Setup of the batched path at lee_prepare: operand arrays, sponge fields, and the tile shapes
+// of the stage and filter launches picked by timing every candidate (right-hand-side-only
+// stage launches and filter launches into scratch buffers, so the state is left alone).
+template <typename T>
+int batch_setup(lee_ctx* c) {
+  auto& bt = c->batch;
+  const int nbk = (int)c->blk.size();
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  int rc;
+  for (auto& b : c->blk)
+    if (!b.d_sigma_field && (rc = build_sigma_field(c, b))) return rc;
+  const size_t pbytes = sizeof(StageParams<T>) * (size_t)tb.ns * nbk;
+  if ((rc = dev_alloc(c, &bt.d_prm_graph, pbytes)) || (rc = dev_alloc(c, &bt.d_prm_direct, pbytes))) return rc;
+  std::vector<BatchFilterInst<T>> fi = batch_filter_inst<T>(c, false);
+  if ((rc = dev_alloc(c, &bt.d_finst, fi.size() * sizeof(fi[0])))) return rc;
+  CK(cudaMemcpyAsync(bt.d_finst, fi.data(), fi.size() * sizeof(fi[0]), cudaMemcpyHostToDevice, c->stream));
+  // scratch operands for the timing runs
+  const std::vector<double> dts((size_t)nbk, 1e-3);
+  std::vector<StageParams<T>> pr = batch_params<T>(c, dts, false, 1);
+  std::vector<BatchFilterInst<T>> fs = batch_filter_inst<T>(c, true);
+  void *d_pr = nullptr, *d_fs = nullptr;
+  int4* d_t = nullptr;
+  CK(cudaMalloc(&d_pr, pr.size() * sizeof(pr[0])));
+  CK(cudaMalloc(&d_fs, fs.size() * sizeof(fs[0])));
+  CK(cudaMemcpy(d_pr, pr.data(), pr.size() * sizeof(pr[0]), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_fs, fs.data(), fs.size() * sizeof(fs[0]), cudaMemcpyHostToDevice));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->cfg.device);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best_s = 1e30f, best_f = 1e30f;
+  std::vector<int4> tiles_s, tiles_f;
+  for (int shape = 0; shape < kBatchShapes; ++shape) {
+    std::vector<int4> t = batch_tiles(c, shape);
+    CK(cudaMalloc(&d_t, t.size() * sizeof(int4)));
+    CK(cudaMemcpy(d_t, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    const int nt = (int)t.size();
+    const int gs = std::min(nt, nsm * batch_stage_occupancy<T>(shape, c->comp ? 1 : 0));
+    const int gf = std::min(nt, nsm * 4);
+    float ms_s = 0.f, ms_f = 0.f;
+    for (int pass = 0; pass < 2; ++pass) {  // the first pass warms up
+      CK(cudaEventRecord(e0, c->stream));
+      for (int r = 0; r < 3; ++r)
+        if ((rc = batch_launch_stage<T>(c, (const StageParams<T>*)d_pr + nbk, d_t, nt, shape, gs))) return rc;
+      CK(cudaEventRecord(e1, c->stream));
+      CK(cudaEventSynchronize(e1));
+      CK(cudaEventElapsedTime(&ms_s, e0, e1));
+      CK(cudaEventRecord(e0, c->stream));
+      for (int r = 0; r < 3; ++r)
+        if ((rc = batch_launch_filter<T>(c, d_fs, d_t, nt, shape, gf))) return rc;
+      CK(cudaEventRecord(e1, c->stream));
+      CK(cudaEventSynchronize(e1));
+      CK(cudaEventElapsedTime(&ms_f, e0, e1));
+    }
+    if (ms_s < best_s) {
+      best_s = ms_s;
+      bt.sshape = shape;
+      bt.sgrid = gs;
+      tiles_s = t;
+    }
+    if (ms_f < best_f) {
+      best_f = ms_f;
+      bt.fshape = shape;
+      bt.fgrid = gf;
+      tiles_f = t;
+    }
+    CK(cudaFree(d_t));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaFree(d_pr));
+  CK(cudaFree(d_fs));
+  if ((rc = dalloc(c, &bt.d_stiles, tiles_s.size())) || (rc = dalloc(c, &bt.d_ftiles, tiles_f.size()))) return rc;
+  CK(cudaMemcpy(bt.d_stiles, tiles_s.data(), tiles_s.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(bt.d_ftiles, tiles_f.data(), tiles_f.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  bt.nst = (int)tiles_s.size();
+  bt.nft = (int)tiles_f.size();
+  // the timing runs wrote right-hand sides and filtered values into scratch buffers only
+  bt.active = true;
+  return LEE_OK;
+}
+
+// One batched step (see step_impl): ns stage launches and one filter launch for every block.
+template <typename T>
+int batch_step(lee_ctx* c, const std::vector<double>& dts, bool graph) {
+  auto& bt = c->batch;
+  const Tableau tb = tableau(c->cfg.rk_scheme);
+  const int nbk = (int)c->blk.size();
+  const void* prm = bt.d_prm_graph;
+  if (!graph) {
+    std::vector<StageParams<T>> pr = batch_params<T>(c, dts, false, 0);
+    CK(cudaMemcpyAsync(bt.d_prm_direct, pr.data(), pr.size() * sizeof(pr[0]), cudaMemcpyHostToDevice, c->stream));
+    prm = bt.d_prm_direct;
+  }
+  for (int s = 0; s < tb.ns; ++s) {
+    int e0 = mark(c);
+    int rc = batch_launch_stage<T>(c, (const StageParams<T>*)prm + (size_t)s * nbk, bt.d_stiles, bt.nst, bt.sshape,
+                                   bt.sgrid);
+    if (rc) return rc;
+    int e1 = mark(c);
+    span(c, 0, e0, e1);
+    c->stats.stage_launches += 1;
+    c->stats.kernel_launches += 1;
+  }
+  int e0 = mark(c);
+  int rc = batch_launch_filter<T>(c, bt.d_finst, bt.d_ftiles, bt.nft, bt.fshape, bt.fgrid);
+  if (rc) return rc;
+  int e1 = mark(c);
+  span(c, 1, e0, e1);
+  c->stats.filter_launches += 1;
+  c->stats.kernel_launches += 1;
+  return LEE_OK;
+}
+
 // One time step (temporal::time_advance with RungeKutta::integrate) enqueued on the context
 // stream: the time is incremented first (solver::solve, src/solver/solver.cpp:72), then every
 // stage runs on every block, the boundary update (BC lines, overset) follows each stage, and
 // the filter closes the step. amp_tab/ctr: the monopole amplitudes of a replayed step graph
 // (null: the amplitude is passed by value).
 template <typename T>
-int step_impl(lee_ctx* c, double dt, const T* amp_tab, const int* ctr) {
+int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, const int* ctr) {
   const Tableau tb = tableau(c->cfg.rk_scheme);
   const int ns = tb.ns;
+  const int nbk = (int)c->blk.size();
   const double *bi = tb.b, *ci = tb.c, *aij = tb.a;
   {
-    c->time += dt;
-    c->step += 1;
-    const double tn = c->time;
+    for (int q = 0; q < nbk; ++q) {
+      c->blk[(size_t)q].time += dts[(size_t)q];
+      c->blk[(size_t)q].step += 1;
+    }
+    c->time = c->blk[0].time;
+    c->step = c->blk[0].step;
+    if (c->batch.active) {
+      int rc = batch_step<T>(c, dts, ctr != nullptr);
+      if (rc) return rc;
+      return trace_step<T>(c, ctr);
+    }
     for (int s = 0; s < ns; ++s) {
       for (auto& b : c->blk) {
+        const size_t bix = (size_t)(&b - &c->blk[0]);
+        const double dt = dts[bix];
         StageParams<T> p;
         fill_stage_common<T>(c, b, p);
         p.stage = s;
@@ -1029,10 +1306,11 @@ int step_impl(lee_ctx* c, double dt, const T* amp_tab, const int* ctr) {
         p.h = (T)dt;
         p.b = (T)bi[s];
         p.a = (T)aij[s];
-        p.src_amp = (T)(c->src_kind != LEE_SOURCE_NONE ? source_amp(c, tn + ci[s] * dt) : 0.0);
-        p.amp_tab = amp_tab;
+        p.src_amp = (T)(c->src_kind != LEE_SOURCE_NONE ? source_amp(c, b, b.time + ci[s] * dt) : 0.0);
+        // the replayed graph's amplitude table holds [step][block][stage]
+        p.amp_tab = amp_tab ? amp_tab + bix * ns : nullptr;
         p.step_ctr = ctr;
-        p.nstages = ns;
+        p.nstages = nbk * ns;
         void** zin = s == 0 ? b.y : b.zb[(s + 1) % 2];
         void** zout = b.zb[s % 2];
         for (int v = 0; v < c->V; ++v) {
@@ -1119,16 +1397,7 @@ int step_impl(lee_ctx* c, double dt, const T* amp_tab, const int* ctr) {
       }
     }
   }
-  if (c->adj.trace_on) {
-    // p' at the microphones after this step (the objective's trace), in FP64
-    BlockData& b = c->blk[(size_t)c->adj.mic_block];
-    const int P = c->V - 1;
-    CK(launch_trace<T>((int)c->adj.mic.size(), c->adj.d_mic, (const T*)b.y[P], c->comp ? (const T*)b.comp[P] : nullptr,
-                       c->adj.d_trace, ctr, ctr ? c->adj.d_base : nullptr, c->adj.host_row, c->stream));
-    c->stats.kernel_launches += 1;
-    if (!ctr) c->adj.host_row += 1;
-  }
-  return LEE_OK;
+  return trace_step<T>(c, ctr);
 }
 
 __global__ void k_tick(int* ctr) { *ctr += 1; }
@@ -1179,10 +1448,43 @@ void restore_roles(lee_ctx* c, const SavedRoles& r) {
   }
 }
 
+struct Clocks {
+  std::vector<double> t;
+  std::vector<int> n;
+};
+
+Clocks save_clocks(const lee_ctx* c) {
+  Clocks k;
+  for (auto& b : c->blk) {
+    k.t.push_back(b.time);
+    k.n.push_back(b.step);
+  }
+  return k;
+}
+
+void restore_clocks(lee_ctx* c, const Clocks& k) {
+  for (size_t i = 0; i < c->blk.size(); ++i) {
+    c->blk[i].time = k.t[i];
+    c->blk[i].step = k.n[i];
+  }
+  c->time = c->blk[0].time;
+  c->step = c->blk[0].step;
+}
+
+// Every block at time t after `step` steps (the context's lockstep clock).
+void set_clock(lee_ctx* c, double t, int step) {
+  for (auto& b : c->blk) {
+    b.time = t;
+    b.step = step;
+  }
+  c->time = t;
+  c->step = step;
+}
+
 // Capture steps into one graph until the buffer roles come back to where they started
 // (at most 4 steps), with the monopole amplitudes read from the device table.
 template <typename T>
-int capture_steps(lee_ctx* c, double dt) {
+int capture_steps(lee_ctx* c, const std::vector<double>& dts) {
   auto& g = c->graph;
   if (g.exec) {
     cudaGraphExecDestroy(g.exec);
@@ -1190,8 +1492,7 @@ int capture_steps(lee_ctx* c, double dt) {
   }
   const std::vector<void*> start = layout_of(c);
   const SavedRoles roles = save_roles(c);
-  const double t0 = c->time;
-  const int s0 = c->step;
+  const Clocks clk = save_clocks(c);
   const lee_stats st0 = c->stats;
   memset(&c->stats, 0, sizeof c->stats);
   const bool src = c->src_kind != LEE_SOURCE_NONE;
@@ -1199,7 +1500,7 @@ int capture_steps(lee_ctx* c, double dt) {
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
   int rc = LEE_OK, steps = 0;
   for (; steps < 4;) {
-    rc = step_impl<T>(c, dt, src ? (const T*)g.d_amp : nullptr, tick ? g.d_ctr : nullptr);
+    rc = step_impl<T>(c, dts, src ? (const T*)g.d_amp : nullptr, tick ? g.d_ctr : nullptr);
     if (rc) break;
     if (tick) {
       k_tick<<<1, 1, 0, c->stream>>>(g.d_ctr);
@@ -1213,8 +1514,7 @@ int capture_steps(lee_ctx* c, double dt) {
   const bool repeat = rc == LEE_OK && layout_of(c) == start;
   const lee_stats per = c->stats;
   restore_roles(c, roles);
-  c->time = t0;
-  c->step = s0;
+  restore_clocks(c, clk);
   c->stats = st0;
   if (rc) {
     if (graph) cudaGraphDestroy(graph);
@@ -1232,7 +1532,7 @@ int capture_steps(lee_ctx* c, double dt) {
     g.exec = nullptr;
     return fail(c, LEE_ERR_CUDA, "graph instantiation: %s", cudaGetErrorString(e));
   }
-  g.dt = dt;
+  g.dts = dts;
   g.steps = steps;
   g.layout = start;
   g.launches = per.kernel_launches;
@@ -1243,14 +1543,14 @@ int capture_steps(lee_ctx* c, double dt) {
 
 // lee_advance: step by step when timing kernels (events between launches), else replays of a
 // captured step graph; the remainder, and a first step whose rho'/rho_bar field is not yet
-// live, run step by step.
+// live, run step by step. dts: the time step of every block.
 template <typename T>
-int advance_impl(lee_ctx* c, int nsteps, double dt) {
+int advance_impl(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
   auto& g = c->graph;
   int done = 0;
   auto direct = [&](int n) -> int {
     for (int k = 0; k < n; ++k) {
-      int rc = step_impl<T>(c, dt, nullptr, nullptr);
+      int rc = step_impl<T>(c, dts, nullptr, nullptr);
       if (rc) return rc;
     }
     done += n;
@@ -1269,17 +1569,24 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
   const bool src = c->src_kind != LEE_SOURCE_NONE;
   const bool tick = src || c->adj.trace_on;
   const Tableau tb = tableau(c->cfg.rk_scheme);
+  const size_t nbk = c->blk.size();
   constexpr size_t kTableSteps = 4096;  // amplitude table rows: steps per chunk of replays
   if (tick && !g.d_ctr) {
     int rc = dalloc(c, &g.d_ctr, 1);
     if (rc) return rc;
     void* p = nullptr;
-    if ((rc = dev_alloc(c, &p, kTableSteps * 4 * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, &p, kTableSteps * 4 * nbk * sizeof(double)))) return rc;
     g.d_amp = p;
-    g.amp_cap = kTableSteps * 4;
+    g.amp_cap = kTableSteps * 4 * nbk;
   }
-  if (!g.exec || g.dt != dt || g.layout != layout_of(c)) {
-    int rc = capture_steps<T>(c, dt);
+  if (!g.exec || g.dts != dts || g.layout != layout_of(c)) {
+    if (c->batch.active) {
+      // the stage parameters the captured batched launches read (amplitudes from the table)
+      std::vector<StageParams<T>> pr = batch_params<T>(c, dts, true, 0);
+      CK(cudaMemcpy(c->batch.d_prm_graph, pr.data(), pr.size() * sizeof(pr[0]), cudaMemcpyHostToDevice));
+      c->batch.graph_dts = dts;
+    }
+    int rc = capture_steps<T>(c, dts);
     if (rc) return rc;
   }
   if (!g.exec || g.steps < 1) return direct(nsteps - done);
@@ -1290,12 +1597,16 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
     const int reps = (int)std::min<long long>((nsteps - done) / P, (long long)(chunk_steps / P));
     const int n = reps * P;
     if (src) {
-      // amplitudes at the stage times of each step, with the time advanced as the steps do
-      amp.assign((size_t)n * tb.ns, T(0));
-      double t = c->time;
-      for (int k = 0; k < n; ++k) {
-        t += dt;
-        for (int s = 0; s < tb.ns; ++s) amp[(size_t)k * tb.ns + s] = (T)source_amp(c, t + tb.c[s] * dt);
+      // amplitudes at the stage times of each step of each block, [step][block][stage], with
+      // every block's time advanced as its steps advance it
+      amp.assign((size_t)n * nbk * tb.ns, T(0));
+      for (size_t q = 0; q < nbk; ++q) {
+        double t = c->blk[q].time;
+        for (int k = 0; k < n; ++k) {
+          t += dts[q];
+          for (int s = 0; s < tb.ns; ++s)
+            amp[((size_t)k * nbk + q) * tb.ns + s] = (T)source_amp(c, c->blk[q], t + tb.c[s] * dts[q]);
+        }
       }
       CK(cudaMemcpyAsync(g.d_amp, amp.data(), amp.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
     }
@@ -1307,10 +1618,13 @@ int advance_impl(lee_ctx* c, int nsteps, double dt) {
       c->adj.host_row += n;
     }
     for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(g.exec, c->stream));
-    for (int k = 0; k < n; ++k) {
-      c->time += dt;
-      c->step += 1;
-    }
+    for (size_t q = 0; q < nbk; ++q)
+      for (int k = 0; k < n; ++k) {
+        c->blk[q].time += dts[q];
+        c->blk[q].step += 1;
+      }
+    c->time = c->blk[0].time;
+    c->step = c->blk[0].step;
     for (auto& b : c->blk)
       if (b.need_rho) b.rho_valid = true;
     c->stats.kernel_launches += g.launches * reps;
@@ -1673,6 +1987,24 @@ int lee_set_source(lee_ctx* c, int kind, const double* params, int nparams) {
   return LEE_OK;
 }
 
+int lee_set_block_source(lee_ctx* c, int b, int kind, const double* params, int nparams) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_block_source after lee_prepare");
+  if (b < 0 || b >= (int)c->blk.size()) return fail(c, LEE_ERR_ARG, "block index");
+  if (c->src_kind == LEE_SOURCE_DISTRIBUTED) return fail(c, LEE_ERR_UNSUPPORTED, "a distributed source is set");
+  BlockData& bk = c->blk[(size_t)b];
+  if (kind == LEE_SOURCE_NONE) {
+    bk.src_mode = 2;
+    return LEE_OK;
+  }
+  if (kind != LEE_SOURCE_MONOPOLE || !params || nparams != 7) return fail(c, LEE_ERR_ARG, "monopole takes 7 params");
+  if (!(params[5] > 0.0)) return fail(c, LEE_ERR_ARG, "monopole half-width must be positive");
+  bk.src_mode = 1;
+  for (int q = 0; q < 7; ++q) bk.own_src[q] = params[q];
+  if (c->src_kind == LEE_SOURCE_NONE) c->src_kind = LEE_SOURCE_MONOPOLE;  // other blocks keep none
+  return LEE_OK;
+}
+
 int lee_set_overset(lee_ctx* c, int n, const int* recv_block, const int* recv_ijk, const int* donor_block,
                     const int* donor_ijk, const int width[3], const double* weights, int num_holes,
                     const int* hole_block, const int* hole_ijk) {
@@ -1933,12 +2265,12 @@ int lee_prepare(lee_ctx* c) {
       }
     }
     // monopole spatial factor on the box where exp() is nonzero in FP64
-    if (c->src_kind == LEE_SOURCE_MONOPOLE) {
-      double ef = -log(2.0) / (c->src[5] * c->src[5]);
+    if (const double* mp = monopole_of(c, b)) {
+      double ef = -log(2.0) / (mp[5] * mp[5]);
       double rmax = sqrt(746.0 / -ef);
       int lo[3] = {b.nx, b.ny, b.nz}, hi[3] = {-1, -1, -1};
       for (long long l = 0; l < b.N; ++l) {
-        double dx = b.hx[(size_t)l] - c->src[0], dy = b.hy[(size_t)l] - c->src[1], dz = b.hz[(size_t)l] - c->src[2];
+        double dx = b.hx[(size_t)l] - mp[0], dy = b.hy[(size_t)l] - mp[1], dz = b.hz[(size_t)l] - mp[2];
         if (dx * dx + dy * dy + dz * dz <= rmax * rmax) {
           int ijk[3] = {(int)(l % b.nx), (int)((l / b.nx) % b.ny), (int)(l / ((long long)b.nx * b.ny))};
           for (int d = 0; d < 3; ++d) {
@@ -1950,7 +2282,7 @@ int lee_prepare(lee_ctx* c) {
       if (hi[0] >= 0) {
         size_t nb = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
         if ((rc = dalloc(c, &b.d_src_g, nb))) return rc;
-        CK(setup_monopole_g(b.nx, b.ny, d_xyzp, lo, hi, c->src[0], c->src[1], c->src[2], ef, b.d_src_g, s));
+        CK(setup_monopole_g(b.nx, b.ny, d_xyzp, lo, hi, mp[0], mp[1], mp[2], ef, b.d_src_g, s));
         for (int d = 0; d < 3; ++d) { b.src_lo[d] = lo[d]; b.src_hi[d] = hi[d]; }
         if (c->comp) {
           float* f = nullptr;
@@ -2062,6 +2394,10 @@ int lee_prepare(lee_ctx* c) {
     if ((b.tma || b.tma_filter) && (rc = ensure_encoder(c))) return rc;
     if ((rc = c->comp ? autotune<float>(c, b) : autotune<double>(c, b))) return rc;
   }
+  if (c->blk.size() > 1 && batch_eligible(c)) {
+    rc = c->comp ? batch_setup<float>(c) : batch_setup<double>(c);
+    if (rc) return rc;
+  }
   if (c->ovs.n > 0) {
     auto& o = c->ovs;
     const size_t n = (size_t)o.n;
@@ -2120,8 +2456,10 @@ int lee_upload_state(lee_ctx* c, int b, const double* const sol[5], int step, do
   CK(cudaStreamSynchronize(c->stream));
   (void)rc;
   bk.rho_valid = false;  // the first stage takes rho'/rho_bar from the uploaded state
-  c->step = step;
-  c->time = time;
+  bk.step = step;
+  bk.time = time;
+  c->step = c->blk[0].step;
+  c->time = c->blk[0].time;
   c->uploaded = true;
   return LEE_OK;
 }
@@ -2147,21 +2485,22 @@ int lee_download_state(lee_ctx* c, int b, double* const sol[5], int* step, doubl
   CK(cudaFreeAsync(tmp, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (c->cfg.num_dim == 2) memset(sol[3], 0, (size_t)bk.N * 8);
-  if (step) *step = c->step;
-  if (time) *time = c->time;
+  if (step) *step = bk.step;
+  if (time) *time = bk.time;
   return LEE_OK;
 }
 
-int lee_compute_dt(lee_ctx* c, double cfl, double* dt) {
-  if (!c || !dt) return LEE_ERR_ARG;
-  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
-  if (!(cfl > 0.0)) return fail(c, LEE_ERR_ARG, "cfl must be positive");
+namespace {
+
+// CFL maxima (temporal::compute_CFL with the dummy dt) of every block, or of all blocks.
+int cfl_max(lee_ctx* c, bool per_block, std::vector<double>& out) {
   CK(cudaSetDevice(c->cfg.device));
   double* d_max = nullptr;
   CK(cudaMallocAsync((void**)&d_max, sizeof(double), c->stream));
-  double init = -1e308;
-  CK(cudaMemcpyAsync(d_max, &init, sizeof init, cudaMemcpyHostToDevice, c->stream));
+  const double init = -1e308;
   const double dt0 = 1e-6;  // the reference's dummy initial dt (src/core/input.cpp:131)
+  out.clear();
+  CK(cudaMemcpyAsync(d_max, &init, sizeof init, cudaMemcpyHostToDevice, c->stream));
   for (auto& b : c->blk) {
     double** d_m = nullptr;
     double** d_u = nullptr;
@@ -2174,22 +2513,61 @@ int lee_compute_dt(lee_ctx* c, double cfl, double* dt) {
     CK(cudaStreamSynchronize(c->stream));
     CK(cudaFreeAsync(d_m, c->stream));
     CK(cudaFreeAsync(d_u, c->stream));
+    if (per_block) {
+      double m = 0.0;
+      CK(cudaMemcpyAsync(&m, d_max, sizeof m, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(d_max, &init, sizeof init, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      out.push_back(m);
+    }
   }
-  double cmax = 0.0;
-  CK(cudaMemcpyAsync(&cmax, d_max, sizeof cmax, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  if (!per_block) {
+    double m = 0.0;
+    CK(cudaMemcpyAsync(&m, d_max, sizeof m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out.push_back(m);
+  }
   CK(cudaFreeAsync(d_max, c->stream));
-  double ratio = cfl / cmax;
-  double d = dt0;
-  d *= ratio;
-  *dt = d;
+  CK(cudaStreamSynchronize(c->stream));
   return LEE_OK;
 }
 
-int lee_advance(lee_ctx* c, int nsteps, double dt) {
-  if (!c) return LEE_ERR_ARG;
-  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
-  if (nsteps < 0 || !(dt > 0.0)) return fail(c, LEE_ERR_ARG, "nsteps >= 0 and dt > 0");
+// The FIX_CFL rescale of solver::solve (src/solver/solver.cpp:58-64).
+double rescale(double cfl, double cmax) {
+  double ratio = cfl / cmax;
+  double d = 1e-6;
+  d *= ratio;
+  return d;
+}
+
+}  // namespace
+
+int lee_compute_dt(lee_ctx* c, double cfl, double* dt) {
+  if (!c || !dt) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (!(cfl > 0.0)) return fail(c, LEE_ERR_ARG, "cfl must be positive");
+  std::vector<double> m;
+  int rc = cfl_max(c, false, m);
+  if (rc) return rc;
+  *dt = rescale(cfl, m[0]);
+  return LEE_OK;
+}
+
+int lee_compute_dt_blocks(lee_ctx* c, double cfl, double* dt) {
+  if (!c || !dt) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (!(cfl > 0.0)) return fail(c, LEE_ERR_ARG, "cfl must be positive");
+  std::vector<double> m;
+  int rc = cfl_max(c, true, m);
+  if (rc) return rc;
+  for (size_t b = 0; b < m.size(); ++b) dt[b] = rescale(cfl, m[b]);
+  return LEE_OK;
+}
+
+namespace {
+
+// lee_advance and lee_advance_blocks: K steps timed by events on the context stream.
+int advance_timed(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
   CK(cudaSetDevice(c->cfg.device));
   memset(&c->stats, 0, sizeof c->stats);
   c->ev_used = 0;
@@ -2198,7 +2576,7 @@ int lee_advance(lee_ctx* c, int nsteps, double dt) {
   CK(cudaEventCreate(&t0));
   CK(cudaEventCreate(&t1));
   CK(cudaEventRecord(t0, c->stream));
-  int rc = c->comp ? advance_impl<float>(c, nsteps, dt) : advance_impl<double>(c, nsteps, dt);
+  int rc = c->comp ? advance_impl<float>(c, nsteps, dts) : advance_impl<double>(c, nsteps, dts);
   CK(cudaEventRecord(t1, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   float ms = 0.f;
@@ -2217,6 +2595,26 @@ int lee_advance(lee_ctx* c, int nsteps, double dt) {
   return check_device_error(c);
 }
 
+}  // namespace
+
+int lee_advance(lee_ctx* c, int nsteps, double dt) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (nsteps < 0 || !(dt > 0.0)) return fail(c, LEE_ERR_ARG, "nsteps >= 0 and dt > 0");
+  return advance_timed(c, nsteps, std::vector<double>(c->blk.size(), dt));
+}
+
+int lee_advance_blocks(lee_ctx* c, int nsteps, const double* dt) {
+  if (!c || !dt) return LEE_ERR_ARG;
+  if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
+  if (nsteps < 0) return fail(c, LEE_ERR_ARG, "nsteps >= 0");
+  if (c->ovs.n > 0) return fail(c, LEE_ERR_UNSUPPORTED, "overset blocks advance with one time step");
+  std::vector<double> dts(dt, dt + c->blk.size());
+  for (double d : dts)
+    if (!(d > 0.0)) return fail(c, LEE_ERR_ARG, "every block needs dt > 0");
+  return advance_timed(c, nsteps, dts);
+}
+
 int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
   if (!c) return LEE_ERR_ARG;
   if (!c->prepared || !c->uploaded) return fail(c, LEE_ERR_STATE, "lee_prepare and lee_upload_state first");
@@ -2229,7 +2627,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     StageParams<double> p;
     fill_stage_common<double>(c, bk, p);
     p.stage = -1;
-    p.src_amp = c->src_kind != LEE_SOURCE_NONE ? source_amp(c, time) : 0.0;
+    p.src_amp = c->src_kind != LEE_SOURCE_NONE ? source_amp(c, bk, time) : 0.0;
     p.rho_prev = bk.rho_valid ? (const double*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const double*)bk.y[v];
@@ -2243,7 +2641,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     StageParams<float> p;
     fill_stage_common<float>(c, bk, p);
     p.stage = -1;
-    p.src_amp = (float)(c->src_kind != LEE_SOURCE_NONE ? source_amp(c, time) : 0.0);
+    p.src_amp = (float)(c->src_kind != LEE_SOURCE_NONE ? source_amp(c, bk, time) : 0.0);
     p.rho_prev = bk.rho_valid ? (const float*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const float*)bk.y[v];
@@ -2315,6 +2713,11 @@ int lee_get_info(lee_ctx* c, lee_info* info) {
   }
   info->stage_chunk = c->blk.empty() ? 0 : c->blk[0].stage_chunk;
   info->filter_chunk = c->blk.empty() ? 0 : c->blk[0].filter_chunk;
+  info->batched = c->batch.active ? 1 : 0;
+  if (c->batch.active) {
+    batch_shape(c->batch.sshape, &info->batch_stage_tile[0], &info->batch_stage_tile[1]);
+    batch_shape(c->batch.fshape, &info->batch_filter_tile[0], &info->batch_filter_tile[1]);
+  }
   return LEE_OK;
 }
 
@@ -2372,7 +2775,8 @@ int advance_traced(lee_ctx* c, int nsteps, double dt, int row0) {
   auto& a = c->adj;
   a.trace_on = true;
   a.host_row = row0;
-  int rc = c->comp ? advance_impl<float>(c, nsteps, dt) : advance_impl<double>(c, nsteps, dt);
+  const std::vector<double> dts(c->blk.size(), dt);
+  int rc = c->comp ? advance_impl<float>(c, nsteps, dts) : advance_impl<double>(c, nsteps, dts);
   a.trace_on = false;
   return rc;
 }
@@ -2525,8 +2929,7 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
     if (recompute) {
       // the segment's forward steps again, from its checkpoint; their traces must repeat
       if ((rc = restore(seg))) return rc;
-      c->time = seg_time[(size_t)seg];
-      c->step = step_start + n0;
+      set_clock(c, seg_time[(size_t)seg], step_start + n0);
       if ((rc = advance_traced(c, n, dt, n0))) return rc;
       tr2.assign((size_t)n * M, 0.0);
       CK(cudaMemcpyAsync(tr2.data(), a.d_trace + (size_t)n0 * M, tr2.size() * sizeof(double), cudaMemcpyDeviceToHost,
@@ -2539,7 +2942,7 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
     double t = seg_time[(size_t)seg];
     for (int k = 0; k < n; ++k) {
       t += dt;
-      for (int s = 0; s < tb.ns; ++s) amps[(size_t)k * tb.ns + s] = source_amp(c, t + tb.c[s] * dt);
+      for (int s = 0; s < tb.ns; ++s) amps[(size_t)k * tb.ns + s] = source_amp(c, b, t + tb.c[s] * dt);
     }
     for (int k = n - 1; k >= 0; --k) {
       const int step = n0 + k;  // 0-based: this transposed step maps the adjoint of y_{step+1} to y_step
@@ -2562,8 +2965,7 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
       CK(cudaMemcpyAsync(q < V ? b.y[q] : b.comp[q - V], fin[(size_t)q], bytes, cudaMemcpyDeviceToDevice, c->stream));
       CK(cudaFreeAsync(fin[(size_t)q], c->stream));
     }
-    c->time = t_end;
-    c->step = step_end;
+    set_clock(c, t_end, step_end);
   }
   CK(cudaStreamSynchronize(c->stream));
   (void)fwd_launches;

@@ -222,6 +222,30 @@ template <typename T>
 cudaError_t launch_mic_force(int n, const long long* l0, T* lam_p, const double* trace, int row, double scale,
                              cudaStream_t s);
 
+// ---- batches of 2-D blocks (lee_batch.cu) ------------------------------------------------
+// Per-block filter operands of the batched filter: pre-filter state x (FP64: y_next;
+// compensated: y_pre, with its rounding error err), outputs y (and the new error comp).
+template <typename T>
+struct BatchFilterInst {
+  int nx, ny;
+  const T* x[4];
+  const T* err[4];
+  T* y[4];
+  T* comp[4];
+};
+
+constexpr int kBatchShapes = 5;
+void batch_shape(int shape, int* tx, int* ty);
+// one launch over the tile list (int4: block, x0, y0, 0) with the blocks' stage parameters
+template <typename T>
+cudaError_t launch_batch_stage(const StageParams<T>* prm, const int4* tiles, int ntiles, int shape, int comp,
+                               int grid, cudaStream_t s);
+template <typename T>
+cudaError_t launch_batch_filter(const BatchFilterInst<T>* inst, const int4* tiles, int ntiles, int shape, int comp,
+                                int grid, const OpTable& op, double blend, cudaStream_t s);
+template <typename T>
+int batch_stage_occupancy(int shape, int comp);
+
 // lee_step.cu
 template <typename T>
 cudaError_t launch_stage(const StageParams<T>& p, int comp, cudaStream_t s);

@@ -126,6 +126,10 @@ int lee_add_boundary(lee_ctx *ctx, int b, int kind, int dir, int end, const int 
                      const double *sigma);
 /* Physical source (source::apply_physicalSource, src/solver/source.cpp:22-107). */
 int lee_set_source(lee_ctx *ctx, int kind, const double *params, int nparams);
+/* A source for block b only (no reference counterpart: the reference applies its source to
+ * every block): LEE_SOURCE_MONOPOLE with the 7 parameters of lee_set_source, or
+ * LEE_SOURCE_NONE for a block without source. Used by batches of independent instances. */
+int lee_set_block_source(lee_ctx *ctx, int b, int kind, const double *params, int nparams);
 /* Overset donor maps, replacing overset::initialize_overset (src/overset/overset.cpp:56-84)
  * with the data of its Overture file (src/io/overture.cpp:473-680). n receivers, grouped by
  * block in block order: recv_block[r] and recv_ijk[3r..3r+2] (block-level indices), the donor
@@ -176,6 +180,16 @@ int lee_apply_filter(lee_ctx *ctx);
  * back to back, each nxi*neta*nzeta long. */
 int lee_get_setup(lee_ctx *ctx, int b, int what, double *out);
 
+/* Batches (no reference counterpart): advance every block nsteps with its own time step
+ * dt[b] and its own clock (lee_download_state returns each block's step and time). For
+ * independent blocks only (no overset). A context whose blocks are all 2-D with a
+ * uniform mean, the 4th-order difference, no BC lines or holes runs them through batched
+ * kernels: one launch per RK stage and one per filter for the whole batch, over a work list
+ * of tiles from every block, replayed as step graphs. */
+int lee_advance_blocks(lee_ctx *ctx, int nsteps, const double *dt);
+/* The FIX_CFL time step of every block on its own (dt[b], as lee_compute_dt would give for a
+ * context holding block b alone). */
+int lee_compute_dt_blocks(lee_ctx *ctx, double cfl, double *dt);
 /* Sizes and coefficient layout chosen by lee_prepare (no reference counterpart: the
  * reference has no timers or counters, finding F13). */
 typedef struct {
@@ -189,6 +203,9 @@ typedef struct {
   int tma_filter;            /* 1 when every block runs the fused TMA-staged filter */
   int stage_chunk;           /* planes marched per CTA by the stage kernel (autotuned; block 0) */
   int filter_chunk;          /* planes marched per CTA by the filter kernel (autotuned; block 0) */
+  int batched;               /* 1 when the blocks run through the batched kernels */
+  int batch_stage_tile[2];   /* tile (xi, eta points) of the batched stage and filter launches, */
+  int batch_filter_tile[2];  /* picked by timing the candidates at lee_prepare */
 } lee_info;
 int lee_get_info(lee_ctx *ctx, lee_info *info);
 

@@ -78,6 +78,8 @@ struct orc_ctx {
   blk_t blk[MAXB];
   int src_kind;
   double src[7];
+  int bsrc_mode[MAXB];     /* per block: 0 the context's source, 1 its own monopole, 2 none */
+  double bsrc[MAXB][7];
   double *dsrc;  /* distributed source parameters */
   int ndsrc;
   double *dsrc_g; /* its prolonged field on block dsrc[0] (full grid, zero outside the lattice) */
@@ -490,9 +492,13 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
     double fac = (g - 1.0) * sin(c->dsrc[1] * time);
     for (int p = 0; p < N; ++p) rhs[4][p] += fac * c->dsrc_g[p];
   }
-  if (c->src_kind == LEE_SOURCE_MONOPOLE) { /* oracle patch P2 (oracle/ref_patch_source.cpp) */
-    double x0 = c->src[0], y0 = c->src[1], z0 = c->src[2], amp = c->src[3], om = c->src[4];
-    double b = c->src[5], T = c->src[6];
+  int bix = (int)(bk - &c->blk[0]);
+  const double *mp = c->bsrc_mode[bix] == 1 ? c->bsrc[bix]
+                   : (c->bsrc_mode[bix] == 0 && c->src_kind == LEE_SOURCE_MONOPOLE && c->src[5] > 0.0) ? c->src
+                   : NULL;
+  if (mp) { /* oracle patch P2 (oracle/ref_patch_source.cpp) */
+    double x0 = mp[0], y0 = mp[1], z0 = mp[2], amp = mp[3], om = mp[4];
+    double b = mp[5], T = mp[6];
     double ramp = 1.0;
     if (T > 0.0 && time < T) {
       double s = sin(0.5 * M_PI * time / T);
@@ -745,6 +751,26 @@ int orc_set_source(orc_ctx *c, int kind, const double *params, int np) {
   return LEE_OK;
 }
 
+int orc_set_block_source(orc_ctx *c, int b, int kind, const double *params, int np) {
+  if (b < 0 || b >= c->nblk) return fail(c, LEE_ERR_ARG, "block index");
+  if (kind == LEE_SOURCE_NONE) {
+    c->bsrc_mode[b] = 2;
+    return LEE_OK;
+  }
+  if (kind != LEE_SOURCE_MONOPOLE || np != 7) return fail(c, LEE_ERR_ARG, "monopole takes 7 params");
+  c->bsrc_mode[b] = 1;
+  for (int i = 0; i < 7; ++i) c->bsrc[b][i] = params[i];
+  if (c->src_kind == LEE_SOURCE_NONE) c->src_kind = LEE_SOURCE_MONOPOLE;
+  return LEE_OK;
+}
+
+/* Blocks advance in lockstep with one clock here, so every dt must be the same. */
+int orc_advance_blocks(orc_ctx *c, int nsteps, const double *dt) {
+  for (int b = 1; b < c->nblk; ++b)
+    if (dt[b] != dt[0]) return fail(c, LEE_ERR_UNSUPPORTED, "the oracle advances blocks with one time step");
+  return orc_advance(c, nsteps, dt[0]);
+}
+
 /* The distributed source's lattice weights and trilinear prolongation (the same arithmetic
  * as the CUDA library's host setup): node (p,q,r) at grid index (o + p h) per direction. */
 static void lattice_weights(double i, double o, double h, int cn, int *p0, double *f) {
@@ -995,6 +1021,20 @@ int orc_compute_dt(orc_ctx *c, double cfl_target, double *dt_out) {
   double ratio = cfl_target / cmax;
   dt *= ratio;
   *dt_out = dt;
+  return LEE_OK;
+}
+
+int orc_compute_dt_blocks(orc_ctx *c, double cfl_target, double *dt_out) {
+  int n = c->nblk;
+  for (int b = 0; b < n; ++b) {
+    c->nblk = 1;
+    blk_t save = c->blk[0];
+    c->blk[0] = c->blk[b];
+    int rc = orc_compute_dt(c, cfl_target, &dt_out[b]);
+    c->blk[0] = save;
+    c->nblk = n;
+    if (rc) return rc;
+  }
   return LEE_OK;
 }
 

@@ -1,0 +1,77 @@
+"""Batches of independent 2-D instances (lee_advance_blocks and the batched kernels).
+
+A context holding several Cartesian instances runs one launch per RK stage and one per filter
+for the whole batch. Each instance is checked against itself run alone in its own single-block
+context (the per-block kernels) and against the CPU oracle, in FP64 within 1e-12 / 1e-10
+relative L2; the FP32-compensated batch against the FP64 one-at-a-time runs within 1e-5 in p';
+replayed step graphs against direct launches, bit for bit.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from camille_b200 import api, cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(nsteps=24):
+    return cases.batch2d(count=6, nmin=40, nmax=96, spacing_spread=2.0, nsteps=nsteps, seed=9)
+
+
+def _alone(lib, case, b, dt, nsteps, precision=api.FP64):
+    s = api.Solver(lib, cases.instance(case, b), precision=precision)
+    s.advance(nsteps, dt)
+    y, step, t = s.download(0)
+    s.close()
+    return y, step, t
+
+
+def test_block_time_steps_are_each_blocks_own(product_lib):
+    case = _batch()
+    s = api.Solver(product_lib, case)
+    dts = s.compute_dt_blocks()
+    for b in range(len(case.blocks)):
+        alone = api.Solver(product_lib, cases.instance(case, b)).compute_dt()
+        assert abs(dts[b] - alone) <= 1e-15 * alone
+    assert np.unique(dts).size == len(case.blocks)
+
+
+def test_fp64_batch_matches_each_instance_alone_and_the_oracle(product_lib, oracle_lib):
+    case = _batch()
+    s = api.Solver(product_lib, case)
+    dts = s.compute_dt_blocks()
+    s.advance_blocks(case.nsteps, dts)
+    for b in range(len(case.blocks)):
+        y, step, t = s.download(b)
+        ya, stepa, ta = _alone(product_lib, case, b, dts[b], case.nsteps)
+        assert step == stepa == case.nsteps and t == ta
+        assert api.rel_l2(y, ya) <= 1e-12
+        yo, _, _ = _alone(oracle_lib, case, b, dts[b], case.nsteps)
+        assert api.rel_l2(y, yo) <= 1e-10
+
+
+def test_fp32_compensated_batch_vs_fp64_alone(product_lib):
+    case = _batch(nsteps=60)
+    s = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
+    dts = s.compute_dt_blocks()
+    s.advance_blocks(case.nsteps, dts)
+    for b in range(len(case.blocks)):
+        y = s.download(b)[0]
+        ya = _alone(product_lib, case, b, dts[b], case.nsteps)[0]
+        assert api.rel_l2(y[4], ya[4]) <= 1e-5
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+def test_batch_graphs_give_the_same_bits(product_lib, precision):
+    case = _batch()
+    a = api.Solver(product_lib, case, precision=precision)
+    b = api.Solver(product_lib, case, precision=precision)
+    b.set_graphs(False)
+    dts = a.compute_dt_blocks()
+    for n in (1, 7, 3):
+        a.advance_blocks(n, dts)
+        b.advance_blocks(n, dts)
+    for q in range(len(case.blocks)):
+        np.testing.assert_array_equal(a.download(q)[0], b.download(q)[0])
