@@ -1,12 +1,13 @@
 // Batched kernels: many independent 2-D blocks (instances of uneven sizes) advance through one
-// launch per RK stage and one per filter, over a work list of tiles drawn from every block.
+// launch per RK stage and one per filter, over a work list of strips drawn from every block.
 //
-// Each CTA is persistent: it walks the tile list with a stride of the grid size. A tile
-// names its block and its origin; the block's stage parameters (pointers, coefficients, time
-// step, source) are copied into shared memory when the CTA moves to another block, and the
-// tile's stage input with its stencil halo is staged in shared memory by coalesced row loads.
-// The arithmetic is that of the per-block kernels (the generic operator order of lee_step.cu
-// and the pointwise update of lee_point.cuh), so a block gives the same bits batched or alone.
+// A work item is a strip of columns of one block and a range of its rows; each CTA takes a
+// run of consecutive items (a block's items are contiguous, so a CTA rarely changes block),
+// copies the block's parameters (pointers, coefficients, time step, source) into shared memory
+// when it does, and marches its strip along eta, streaming rows through a shared-memory ring
+// with asynchronous copies issued a few rows ahead. The arithmetic is that of the per-block
+// kernels (the generic operator order of lee_step.cu and the pointwise update of
+// lee_point.cuh), so a block gives the same bits batched or alone.
 #include <type_traits>
 
 #include "lee_internal.h"
@@ -18,29 +19,76 @@ namespace {
 constexpr int kFdH = 2;   // the 4th-order difference: closure rows read 3 points, inside a halo of 2
 constexpr int kFlH = 4;   // the 8th-order filter: closure rows read 7 points, inside a halo of 4
 
-// dop() of lee_step.cu on a line held in shared memory: f points at the line's element for
-// position `pos`, stride `st`.
-template <typename T>
-__device__ __forceinline__ T dop_sm(const OpTable& op, const T* f, int st, int pos, int n) {
-  int c;
-  if (pos >= op.h && pos <= n - 1 - op.h) c = 0;
-  else if (pos < op.h) c = 1 + pos;
-  else c = -(1 + (n - 1 - pos));
+// An operator's weights in the working precision, converted once per CTA exactly as dop()
+// converts them per use (T(c), T(B), T(mfac * B)), for a compile-time half-width HH and row
+// width SS.
+template <typename T, int HH, int SS>
+struct SmOp {
+  T c[2 * HH + 1];
+  T bl[HH][SS];
+  T br[HH][SS];
+};
+
+template <typename T, int HH, int SS>
+__device__ __forceinline__ void load_op(SmOp<T, HH, SS>& w, const OpTable& op, int tid, int nthr) {
+  for (int q = tid; q < 2 * HH + 1; q += nthr) w.c[q] = T(op.c[q]);
+  for (int q = tid; q < HH * SS; q += nthr) {
+    const int r = q / SS, s = q % SS;
+    w.bl[r][s] = T(op.B[r][s]);
+    w.br[r][s] = T(op.mfac * op.B[r][s]);
+  }
+}
+
+// dop() of lee_step.cu on a line held in shared memory (same terms in the same order): f
+// points at the element of position `pos` on a line of n points, stride ST.
+template <typename T, int HH, int SS, int ST>
+__device__ __forceinline__ T dop_c(const SmOp<T, HH, SS>& w, const T* f, int pos, int n) {
   T acc = T(0);
-  if (c == 0) {
+  if (pos >= HH && pos <= n - 1 - HH) {
 #pragma unroll
-    for (int l = -op.h; l <= op.h; ++l) acc += T(op.c[l + op.h]) * f[l * st];
+    for (int l = -HH; l <= HH; ++l) acc += w.c[l + HH] * f[l * ST];
     return acc;
   }
-  if (c > 0) {
-    const int r = c - 1;
-    const T* a = f - r * st;
-    for (int s = 0; s < op.S; ++s) acc += T(op.B[r][s]) * a[s * st];
+  // closure rows: zero weights are skipped, so a row reads only the points within HH of its
+  // own (the 8th-order filter's rows carry zeros out to 6 points, beyond the staged halo)
+  if (pos < HH) {
+    const int r = pos;
+    const T* a = f - r * ST;
+#pragma unroll
+    for (int s = 0; s < SS; ++s)
+      if (w.bl[r][s] != T(0)) acc += w.bl[r][s] * a[s * ST];
     return acc;
   }
-  const int r = -c - 1;
-  const T* a = f + r * st;
-  for (int s = 0; s < op.S; ++s) acc += T(op.mfac * op.B[r][s]) * a[-s * st];
+  const int r = n - 1 - pos;
+  const T* a = f + r * ST;
+#pragma unroll
+  for (int s = 0; s < SS; ++s)
+    if (w.br[r][s] != T(0)) acc += w.br[r][s] * a[-s * ST];
+  return acc;
+}
+
+// dop() along eta on rows held in a ring of NSL rows: row r of column `col` lives at
+// ring[(r mod NSL) * rs + col]; so[] holds the ring offsets of rows j - HH .. j + HH.
+template <typename T, int HH, int SS, int NSL>
+__device__ __forceinline__ T dop_ring(const SmOp<T, HH, SS>& w, const T* ring, const int (&so)[2 * HH + 1], int rs,
+                                      int col, int j, int n) {
+  T acc = T(0);
+  if (j >= HH && j <= n - 1 - HH) {
+#pragma unroll
+    for (int l = -HH; l <= HH; ++l) acc += w.c[l + HH] * ring[so[l + HH] + col];
+    return acc;
+  }
+  if (j < HH) {
+    const int r = j;
+#pragma unroll
+    for (int s = 0; s < SS; ++s)
+      if (w.bl[r][s] != T(0)) acc += w.bl[r][s] * ring[((j - r + s + NSL) % NSL) * rs + col];
+    return acc;
+  }
+  const int r = n - 1 - j;
+#pragma unroll
+  for (int s = 0; s < SS; ++s)
+    if (w.br[r][s] != T(0)) acc += w.br[r][s] * ring[((j + r - s + 2 * NSL) % NSL) * rs + col];
   return acc;
 }
 
@@ -53,216 +101,343 @@ __device__ __forceinline__ void copy_params(P* dst, const P* src, int tid, int n
   for (int q = tid; q < (int)(sizeof(P) / 4); q += nthr) d[q] = s[q];
 }
 
-template <typename T, bool COMP, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY) k_batch_stage(const StageParams<T>* __restrict__ prm,
-                                                        const int4* __restrict__ tiles, int ntiles) {
+// Asynchronous global -> shared copies of one element (4 or 8 bytes), grouped per row.
+template <typename T>
+__device__ __forceinline__ void cp_async(T* dst, const T* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Row r of a strip (columns x0 - H .. x0 + TX + H - 1) of V fields into ring slot `slot`:
+// cp.async inside the block, zeros outside it; one commit group per row (empty when the row
+// is outside the block, so the group count stays one per row).
+template <typename T, int V, int TX, int H>
+__device__ __forceinline__ void issue_row(T* ring, int slot, const T* const* fields, int r, int x0, int nx, int ny,
+                                          int tid) {
+  constexpr int W = TX + 2 * H;
+  if (r >= 0 && r < ny) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      T* dst = ring + ((long long)slot * V + v) * W;
+      const T* src = fields[v] + (long long)r * nx;
+      for (int cc = tid; cc < W; cc += TX) {
+        const int gx = x0 - H + cc;
+        if (gx >= 0 && gx < nx) cp_async(dst + cc, src + gx);
+        else dst[cc] = T(0);
+      }
+    }
+  }
+  cp_commit();
+}
+
+// The stage kernel of a batch, marching along eta: a CTA of TX threads owns TX columns of a
+// block (one per thread) and rows [ys, ye) of them. Rows of the stage input (with a xi halo)
+// stream through a ring of 2H + 2 + PF rows in shared memory, PF rows ahead of the row being
+// computed; the pointwise inputs of the next row are loaded into registers while this row is
+// computed. A work item is int4 (block, x0, ys, ye); a CTA takes `per` consecutive items.
+template <typename T, bool COMP, int TX, int PF>
+__global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __restrict__ prm,
+                                                    const int4* __restrict__ items, int nitems, int per) {
   constexpr int V = 4;
   constexpr int H = kFdH;
-  constexpr int W = TX + 2 * H, R = TY + 2 * H;
-  // J*metrics read per point where a block keeps them as fields (cval falls back to the
-  // constant otherwise); uniform mean; summed sponge field
+  constexpr int W = TX + 2 * H;
+  constexpr int NS = 2 * H + 2 + PF;
   constexpr int TR = kTrJmField | kTrUniform | kTrSponge;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  T* ring = reinterpret_cast<T*>(dsm);  // [NS][V][W]
   __shared__ __align__(16) StageParams<T> P;
-  __shared__ T sm[V][R][W];
+  __shared__ SmOp<T, kFdH, 3> w;
   __shared__ int cur;
-  const int tid = threadIdx.x, nthr = TX * TY;
-  const int tx = tid % TX, ty = tid / TX;
+  const int tid = threadIdx.x;
   if (tid == 0) cur = -1;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int4 td = tiles[t];
-    __syncthreads();  // the previous tile's readers are done with P and sm
-    if (td.x != cur) {
-      copy_params(&P, prm + td.x, tid, nthr);
+  load_op(w, prm[0].fd, tid, TX);
+  const int t0 = blockIdx.x * per, t1 = min(t0 + per, nitems);
+  for (int t = t0; t < t1; ++t) {
+    const int4 it = items[t];
+    __syncthreads();  // every thread is done with the previous item's ring and parameters
+    if (it.x != cur) {
+      copy_params(&P, prm + it.x, tid, TX);
       __syncthreads();
-      if (tid == 0) cur = td.x;
+      if (tid == 0) cur = it.x;
     }
-    const int nx = P.nx, ny = P.ny, x0 = td.y, y0 = td.z;
-    for (int q = tid; q < V * R * W; q += nthr) {
-      const int v = q / (R * W), rr = (q / W) % R, cc = q % W;
-      const int gx = x0 - H + cc, gy = y0 - H + rr;
-      sm[v][rr][cc] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? P.zin[v][(long long)gy * nx + gx] : T(0);
-    }
-    __syncthreads();
-    const int i = x0 + tx, j = y0 + ty;
-    if (i < nx && j < ny) {
-      const long long l = (long long)j * nx + i;
-      PointIn<T, 2> in;
-      gather<T, 2, COMP, TR>(P, l, in);
-      T D[V][2], q[V];
+    const int nx = P.nx, ny = P.ny, x0 = it.y, ys = it.z, ye = it.w;
+    const T* const* zin = P.zin;
+    // prologue: rows ys - H .. ys + H + PF - 1
+    for (int r = ys - H; r < ys + H + PF; ++r) issue_row<T, V, TX, H>(ring, (r + NS) % NS, zin, r, x0, nx, ny, tid);
+    const int i = x0 + tid;
+    const bool col = i < nx;
+    PointIn<T, 2> in_cur, in_nxt;
+    if (col) gather<T, 2, COMP, TR>(P, (long long)ys * nx + i, in_cur);
+    for (int j = ys; j < ye; ++j) {
+      issue_row<T, V, TX, H>(ring, (j + H + PF + NS) % NS, zin, j + H + PF, x0, nx, ny, tid);
+      if (col && j + 1 < ye) gather<T, 2, COMP, TR>(P, (long long)(j + 1) * nx + i, in_nxt);
+      cp_wait<PF>();
+      __syncthreads();
+      if (col) {
+        T D[V][2], q[V];
+        int so[2 * H + 1];
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const T* c0 = &sm[v][ty + H][tx + H];
-        D[v][0] = dop_sm<T>(P.fd, c0, 1, i, nx);
-        D[v][1] = dop_sm<T>(P.fd, c0, W, j, ny);
-        q[v] = *c0;
+        for (int l = -H; l <= H; ++l) so[l + H] = ((j + l + NS) % NS) * (V * W);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const T* c0 = ring + so[H] + v * W + tid + H;
+          D[v][0] = dop_c<T, kFdH, 3, 1>(w, c0, i, nx);
+          D[v][1] = dop_ring<T, kFdH, 3, NS>(w, ring, so, V * W, v * W + tid + H, j, ny);
+          q[v] = *c0;
+        }
+        rhs_update<T, 2, COMP, TR>(P, (long long)j * nx + i, i, j, 0, D, q, in_cur);
       }
-      rhs_update<T, 2, COMP, TR>(P, l, i, j, 0, D, q, in);
+      in_cur = in_nxt;
     }
+    cp_wait<0>();
   }
 }
 
-template <typename T, bool COMP, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY) k_batch_filter(const BatchFilterInst<T>* __restrict__ inst,
-                                                         const int4* __restrict__ tiles, int ntiles, OpTable op,
-                                                         T blend) {
+// The filter of a batch, marching along eta: rows of the pre-filter state (with a xi halo of
+// 4) stream through a shared-memory ring; each thread applies F_xi to its column of every row
+// as it arrives and keeps the results of the last 2H + 1 rows in a register queue, from which
+// F_eta of the row H behind follows without another pass through shared memory. The
+// arithmetic is that of the per-block passes (xi pass, then eta pass with the blend, or the
+// increment form with the two-float sum), term for term.
+template <typename T, bool COMP, int TX, int PF>
+__global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* __restrict__ inst,
+                                                     const int4* __restrict__ items, int nitems, int per, OpTable op,
+                                                     T blend) {
   constexpr int V = 4;
   constexpr int H = kFlH;
-  constexpr int W = TX + 2 * H, R = TY + 2 * H;
+  constexpr int S = 7;
+  constexpr int W = TX + 2 * H;
+  constexpr int NX = H + PF + 2;  // state rows r - H - 1 .. r + PF around the row r being filtered in xi
   extern __shared__ __align__(16) unsigned char dsm[];
-  T* X = reinterpret_cast<T*>(dsm);              // [V][R][W]: pre-filter state with halo
-  T* O = X + V * R * W;                          // [V][R][TX]: after the xi pass
+  T* X = reinterpret_cast<T*>(dsm);  // [NX][V][W]
   __shared__ __align__(16) BatchFilterInst<T> P;
+  __shared__ SmOp<T, kFlH, S> w;
   __shared__ int cur;
-  const int tid = threadIdx.x, nthr = TX * TY;
-  const int tx = tid % TX, ty = tid / TX;
+  const int tid = threadIdx.x;
   if (tid == 0) cur = -1;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int4 td = tiles[t];
+  load_op(w, op, tid, TX);
+  const int t0 = blockIdx.x * per, t1 = min(t0 + per, nitems);
+  for (int t = t0; t < t1; ++t) {
+    const int4 it = items[t];
     __syncthreads();
-    if (td.x != cur) {
-      copy_params(&P, inst + td.x, tid, nthr);
+    if (it.x != cur) {
+      copy_params(&P, inst + it.x, tid, TX);
       __syncthreads();
-      if (tid == 0) cur = td.x;
+      if (tid == 0) cur = it.x;
     }
-    const int nx = P.nx, ny = P.ny, x0 = td.y, y0 = td.z;
-    for (int q = tid; q < V * R * W; q += nthr) {
-      const int v = q / (R * W), rr = (q / W) % R, cc = q % W;
-      const int gx = x0 - H + cc, gy = y0 - H + rr;
-      X[q] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? P.x[v][(long long)gy * nx + gx] : T(0);
+    const int nx = P.nx, ny = P.ny, x0 = it.y, ys = it.z, ye = it.w;
+    const T* const* xf = P.x;
+    const int i = x0 + tid;
+    const bool col = i < nx;
+    T fq[V][2 * H + 1];  // xi-pass values (x + D_xi x when compensated) of rows r - 2H .. r
+    T dq[V][H + 1];      // compensated: D_xi x of rows r - H .. r
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+#pragma unroll
+      for (int q = 0; q <= 2 * H; ++q) fq[v][q] = T(0);
+#pragma unroll
+      for (int q = 0; q <= H; ++q) dq[v][q] = T(0);
     }
-    __syncthreads();
-    // xi pass on every row of the tile and its eta halo, tile columns only
-    for (int q = tid; q < V * R * TX; q += nthr) {
-      const int v = q / (R * TX), rr = (q / TX) % R, cc = q % TX;
-      const int gx = x0 + cc, gy = y0 - H + rr;
-      T o = T(0);
-      if (gx < nx && gy >= 0 && gy < ny) {
-        const T* f = X + ((long long)v * R + rr) * W + (cc + H);
-        const T fx = dop_sm<T>(op, f, 1, gx, nx);
-        o = COMP ? *f + fx : fx;  // compensated: the increment form, x + (F - I) x
+    T err_nxt[V];
+    for (int r = ys - H; r < ys - H + PF; ++r) issue_row<T, V, TX, H>(X, (r + NX) % NX, xf, r, x0, nx, ny, tid);
+    for (int r = ys - H; r < ye + H; ++r) {
+      issue_row<T, V, TX, H>(X, (r + PF + NX) % NX, xf, r + PF, x0, nx, ny, tid);
+      const int j = r - H;  // the row finished in this iteration
+      if (COMP && col && j >= ys && j < ye) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) err_nxt[v] = P.err[v][(long long)j * nx + i];
       }
-      O[q] = o;
-    }
-    __syncthreads();
-    const int i = x0 + tx, j = y0 + ty;
-    if (i < nx && j < ny) {
-      const long long l = (long long)j * nx + i;
+      cp_wait<PF>();
+      __syncthreads();  // state row r landed for every thread
+      const bool rin = r >= 0 && r < ny;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const T* col = O + ((long long)v * R + (ty + H)) * TX + tx;
-        const T fy = dop_sm<T>(op, col, TX, j, ny);
-        const T xc = X[((long long)v * R + (ty + H)) * W + (tx + H)];
-        if (!COMP) {
-          P.y[v][l] = (T(1) - blend) * xc + blend * fy;
-        } else {
-          // the xi increment again at the centre (as the per-block first pass keeps it), then
-          // y = y_pre + beta (D_xi + D_eta) + err as an exact two-float sum
-          const T dx = dop_sm<T>(op, X + ((long long)v * R + (ty + H)) * W + (tx + H), 1, i, nx);
-          const T dsum = dx + fy;
-          const T tt = blend * dsum + P.err[v][l];
-          const T s = xc + tt;
-          const T bb = s - xc;
-          const T e = (xc - (s - bb)) + (tt - bb);
-          P.y[v][l] = s;
-          P.comp[v][l] = e;
+        T o = T(0), fx = T(0);
+        if (rin && col) {
+          const T* f = X + ((long long)((r + NX) % NX) * V + v) * W + tid + H;
+          fx = dop_c<T, kFlH, S, 1>(w, f, i, nx);
+          o = COMP ? *f + fx : fx;
+        }
+#pragma unroll
+        for (int q = 0; q < 2 * H; ++q) fq[v][q] = fq[v][q + 1];
+        fq[v][2 * H] = o;
+        if (COMP) {
+#pragma unroll
+          for (int q = 0; q < H; ++q) dq[v][q] = dq[v][q + 1];
+          dq[v][H] = fx;
+        }
+      }
+      if (col && j >= ys && j < ye) {
+        const long long l = (long long)j * nx + i;
+        const T* xrow = X + (long long)((j + NX) % NX) * V * W + tid + H;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          // F_eta at row j from the queue (entry H + q holds row j + q), in dop()'s order
+          T fy = T(0);
+          if (j >= H && j <= ny - 1 - H) {
+#pragma unroll
+            for (int q = -H; q <= H; ++q) fy += w.c[q + H] * fq[v][q + H];
+          } else if (j < H) {  // left closure row j reads rows s = 0 .. S-1, i.e. q = s - j
+#pragma unroll
+            for (int q = -H; q <= H; ++q) {
+              const int sidx = j + q;
+              if (sidx >= 0 && sidx < S && w.bl[j][sidx] != T(0)) fy += w.bl[j][sidx] * fq[v][q + H];
+            }
+          } else {  // right closure row rr reads rows ny-1-s, s = 0 .. S-1, i.e. q = rr - s (s ascending)
+            const int rr = ny - 1 - j;
+#pragma unroll
+            for (int q = H; q >= -H; --q) {
+              const int sidx = rr - q;
+              if (sidx >= 0 && sidx < S && w.br[rr][sidx] != T(0)) fy += w.br[rr][sidx] * fq[v][q + H];
+            }
+          }
+          const T xc = xrow[v * W];
+          if (!COMP) {
+            P.y[v][l] = (T(1) - blend) * xc + blend * fy;
+          } else {
+            const T dsum = dq[v][0] + fy;
+            const T tt = blend * dsum + err_nxt[v];
+            const T s2 = xc + tt;
+            const T bb = s2 - xc;
+            const T e = (xc - (s2 - bb)) + (tt - bb);
+            P.y[v][l] = s2;
+            P.comp[v][l] = e;
+          }
         }
       }
     }
+    cp_wait<0>();
   }
 }
 
-template <typename T, bool COMP, int TX, int TY>
-cudaError_t go_stage(const StageParams<T>* prm, const int4* tiles, int ntiles, int grid, cudaStream_t s) {
-  k_batch_stage<T, COMP, TX, TY><<<grid, TX * TY, 0, s>>>(prm, tiles, ntiles);
+template <typename T, int TX>
+size_t stage_smem() {
+  return sizeof(T) * 4 * (2 * kFdH + 2 + 2) * (TX + 2 * kFdH);
+}
+
+template <typename T, bool COMP, int TX>
+cudaError_t go_stage(const StageParams<T>* prm, const int4* items, int n, int grid, cudaStream_t s) {
+  const size_t smem = stage_smem<T, TX>();
+  cudaError_t e =
+      cudaFuncSetAttribute(k_batch_stage<T, COMP, TX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int per = (n + grid - 1) / grid;
+  k_batch_stage<T, COMP, TX, 2><<<(n + per - 1) / per, TX, smem, s>>>(prm, items, n, per);
   return cudaGetLastError();
 }
 
-template <typename T, int TX, int TY>
+template <typename T, int TX>
 size_t filter_smem() {
-  return sizeof(T) * 4 * ((TY + 2 * kFlH) * (TX + 2 * kFlH) + (TY + 2 * kFlH) * TX);
+  return sizeof(T) * 4 * (kFlH + 2 + 2) * (TX + 2 * kFlH);
 }
 
-template <typename T, bool COMP, int TX, int TY>
-cudaError_t go_filter(const BatchFilterInst<T>* inst, const int4* tiles, int ntiles, int grid, const OpTable& op,
-                      T blend, cudaStream_t s) {
-  const size_t smem = filter_smem<T, TX, TY>();
-  cudaError_t e = cudaFuncSetAttribute(k_batch_filter<T, COMP, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+template <typename T, bool COMP, int TX>
+cudaError_t go_filter(const BatchFilterInst<T>* inst, const int4* items, int n, int grid, const OpTable& op, T blend,
+                      cudaStream_t s) {
+  const size_t smem = filter_smem<T, TX>();
+  cudaError_t e =
+      cudaFuncSetAttribute(k_batch_filter<T, COMP, TX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_batch_filter<T, COMP, TX, TY><<<grid, TX * TY, smem, s>>>(inst, tiles, ntiles, op, blend);
+  const int per = (n + grid - 1) / grid;
+  k_batch_filter<T, COMP, TX, 2><<<(n + per - 1) / per, TX, smem, s>>>(inst, items, n, per, op, blend);
   return cudaGetLastError();
 }
 
 template <typename T, bool COMP>
-int occupancy_stage(int shape) {
+int occupancy_stage(int tx) {
   int n = 0;
-  switch (shape) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 32, 8>, 256, 0); break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 64, 4>, 256, 0); break;
-    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 64, 8>, 512, 0); break;
-    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 32, 16>, 512, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 128, 4>, 512, 0); break;
-  }
+  if (tx == 64)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 64, 2>, 64, stage_smem<T, 64>());
+  else if (tx == 128)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 128, 2>, 128, stage_smem<T, 128>());
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 256, 2>, 256, stage_smem<T, 256>());
   return n > 0 ? n : 1;
 }
 
 }  // namespace
 
-// Tile shapes, by index: 0 = 32x8, 1 = 64x4, 2 = 64x8, 3 = 32x16, 4 = 128x4 (stage and filter).
+// Work-item shapes, by index: columns x rows of a strip; the CTA has one thread per column.
 void batch_shape(int shape, int* tx, int* ty) {
-  static const int s[5][2] = {{32, 8}, {64, 4}, {64, 8}, {32, 16}, {128, 4}};
+  static const int s[kBatchShapes][2] = {{64, 16}, {128, 16}, {128, 32}, {256, 16}, {64, 32}};
   *tx = s[shape][0];
   *ty = s[shape][1];
 }
 
 template <typename T>
-cudaError_t launch_batch_stage(const StageParams<T>* prm, const int4* tiles, int ntiles, int shape, int comp,
-                               int grid, cudaStream_t s) {
-  if (ntiles <= 0) return cudaSuccess;
+cudaError_t launch_batch_stage(const StageParams<T>* prm, const int4* items, int n, int shape, int comp, int grid,
+                               cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  int tx, ty;
+  batch_shape(shape, &tx, &ty);
   if (comp) {
-    switch (shape) {
-      case 0: return go_stage<T, true, 32, 8>(prm, tiles, ntiles, grid, s);
-      case 1: return go_stage<T, true, 64, 4>(prm, tiles, ntiles, grid, s);
-      case 2: return go_stage<T, true, 64, 8>(prm, tiles, ntiles, grid, s);
-      case 3: return go_stage<T, true, 32, 16>(prm, tiles, ntiles, grid, s);
-      default: return go_stage<T, true, 128, 4>(prm, tiles, ntiles, grid, s);
-    }
+    if (tx == 64) return go_stage<T, true, 64>(prm, items, n, grid, s);
+    if (tx == 128) return go_stage<T, true, 128>(prm, items, n, grid, s);
+    return go_stage<T, true, 256>(prm, items, n, grid, s);
   }
-  switch (shape) {
-    case 0: return go_stage<T, false, 32, 8>(prm, tiles, ntiles, grid, s);
-    case 1: return go_stage<T, false, 64, 4>(prm, tiles, ntiles, grid, s);
-    case 2: return go_stage<T, false, 64, 8>(prm, tiles, ntiles, grid, s);
-    case 3: return go_stage<T, false, 32, 16>(prm, tiles, ntiles, grid, s);
-    default: return go_stage<T, false, 128, 4>(prm, tiles, ntiles, grid, s);
-  }
+  if (tx == 64) return go_stage<T, false, 64>(prm, items, n, grid, s);
+  if (tx == 128) return go_stage<T, false, 128>(prm, items, n, grid, s);
+  return go_stage<T, false, 256>(prm, items, n, grid, s);
 }
 
 template <typename T>
-cudaError_t launch_batch_filter(const BatchFilterInst<T>* inst, const int4* tiles, int ntiles, int shape, int comp,
+cudaError_t launch_batch_filter(const BatchFilterInst<T>* inst, const int4* items, int n, int shape, int comp,
                                 int grid, const OpTable& op, double blend, cudaStream_t s) {
-  if (ntiles <= 0) return cudaSuccess;
+  if (n <= 0) return cudaSuccess;
+  int tx, ty;
+  batch_shape(shape, &tx, &ty);
   const T b = (T)blend;
   if (comp) {
-    switch (shape) {
-      case 0: return go_filter<T, true, 32, 8>(inst, tiles, ntiles, grid, op, b, s);
-      case 1: return go_filter<T, true, 64, 4>(inst, tiles, ntiles, grid, op, b, s);
-      case 2: return go_filter<T, true, 64, 8>(inst, tiles, ntiles, grid, op, b, s);
-      case 3: return go_filter<T, true, 32, 16>(inst, tiles, ntiles, grid, op, b, s);
-      default: return go_filter<T, true, 128, 4>(inst, tiles, ntiles, grid, op, b, s);
-    }
+    if (tx == 64) return go_filter<T, true, 64>(inst, items, n, grid, op, b, s);
+    if (tx == 128) return go_filter<T, true, 128>(inst, items, n, grid, op, b, s);
+    return go_filter<T, true, 256>(inst, items, n, grid, op, b, s);
   }
-  switch (shape) {
-    case 0: return go_filter<T, false, 32, 8>(inst, tiles, ntiles, grid, op, b, s);
-    case 1: return go_filter<T, false, 64, 4>(inst, tiles, ntiles, grid, op, b, s);
-    case 2: return go_filter<T, false, 64, 8>(inst, tiles, ntiles, grid, op, b, s);
-    case 3: return go_filter<T, false, 32, 16>(inst, tiles, ntiles, grid, op, b, s);
-    default: return go_filter<T, false, 128, 4>(inst, tiles, ntiles, grid, op, b, s);
-  }
+  if (tx == 64) return go_filter<T, false, 64>(inst, items, n, grid, op, b, s);
+  if (tx == 128) return go_filter<T, false, 128>(inst, items, n, grid, op, b, s);
+  return go_filter<T, false, 256>(inst, items, n, grid, op, b, s);
 }
 
 template <typename T>
 int batch_stage_occupancy(int shape, int comp) {
-  return comp ? occupancy_stage<T, true>(shape) : occupancy_stage<T, false>(shape);
+  int tx, ty;
+  batch_shape(shape, &tx, &ty);
+  return comp ? occupancy_stage<T, true>(tx) : occupancy_stage<T, false>(tx);
+}
+
+template <typename T, bool COMP>
+int occupancy_filter(int tx) {
+  int n = 0;
+  if (tx == 64)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 64, 2>, 64, filter_smem<T, 64>());
+  else if (tx == 128)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 128, 2>, 128, filter_smem<T, 128>());
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 256, 2>, 256, filter_smem<T, 256>());
+  return n > 0 ? n : 1;
+}
+
+template <typename T>
+int batch_filter_occupancy(int shape, int comp) {
+  int tx, ty;
+  batch_shape(shape, &tx, &ty);
+  // the dynamic shared memory limit must be raised before the occupancy query counts it
+  const size_t smem = tx == 64 ? filter_smem<T, 64>() : tx == 128 ? filter_smem<T, 128>() : filter_smem<T, 256>();
+  if (comp) {
+    cudaFuncSetAttribute(tx == 64 ? k_batch_filter<T, true, 64, 2> : tx == 128 ? k_batch_filter<T, true, 128, 2>
+                                                                                : k_batch_filter<T, true, 256, 2>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return occupancy_filter<T, true>(tx);
+  }
+  cudaFuncSetAttribute(tx == 64 ? k_batch_filter<T, false, 64, 2> : tx == 128 ? k_batch_filter<T, false, 128, 2>
+                                                                               : k_batch_filter<T, false, 256, 2>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return occupancy_filter<T, false>(tx);
 }
 
 template cudaError_t launch_batch_stage<double>(const StageParams<double>*, const int4*, int, int, int, int,
@@ -275,5 +450,7 @@ template cudaError_t launch_batch_filter<float>(const BatchFilterInst<float>*, c
                                                 const OpTable&, double, cudaStream_t);
 template int batch_stage_occupancy<double>(int, int);
 template int batch_stage_occupancy<float>(int, int);
+template int batch_filter_occupancy<double>(int, int);
+template int batch_filter_occupancy<float>(int, int);
 
 }  // namespace lee

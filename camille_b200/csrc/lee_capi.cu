@@ -1051,10 +1051,21 @@ int trace_step(lee_ctx* c, const int* ctr) {
 
 // Blocks the batched kernels cover: 2-D, uniform mean, no holes,
 // BC lines or overset (sponges allowed), the 4th-order difference and the 8th-order filter.
+// Every nonzero closure weight of row r lies within h points of the row's own point (the batched
+// kernels stage h points of halo and skip zero weights).
+bool closures_within_halo(const OpTable& op) {
+  for (int r = 0; r < op.h; ++r)
+    for (int s = 0; s < op.S; ++s)
+      if (op.B[r][s] != 0.0 && std::abs(s - r) > op.h) return false;
+  return true;
+}
+
 bool batch_eligible(const lee_ctx* c) {
   if (c->cfg.num_dim != 2 || c->ovs.n > 0) return false;
   if (!(c->fd.h == 2 && c->fd.S == 3)) return false;
   if (c->cfg.filter_scheme != LEE_FILTER_STANDARD_CENTRAL || c->cfg.filter_order != 8) return false;
+  if (!(c->flt.h == 4 && c->flt.S == 7 && c->fltd.h == 4 && c->fltd.S == 7)) return false;
+  if (!closures_within_halo(c->fd) || !closures_within_halo(c->flt) || !closures_within_halo(c->fltd)) return false;
   for (auto& b : c->blk) {
     if (b.has_iblank || b.need_rho) return false;
     for (auto& z : b.bnd)
@@ -1070,13 +1081,15 @@ bool batch_eligible(const lee_ctx* c) {
   return true;
 }
 
+// Work items of a shape: (block, x0, ys, ye) strips of tx columns and ty rows.
 std::vector<int4> batch_tiles(const lee_ctx* c, int shape) {
   int tx, ty;
   batch_shape(shape, &tx, &ty);
   std::vector<int4> t;
   for (size_t b = 0; b < c->blk.size(); ++b)
-    for (int y0 = 0; y0 < c->blk[b].ny; y0 += ty)
-      for (int x0 = 0; x0 < c->blk[b].nx; x0 += tx) t.push_back(make_int4((int)b, x0, y0, 0));
+    for (int x0 = 0; x0 < c->blk[b].nx; x0 += tx)
+      for (int y0 = 0; y0 < c->blk[b].ny; y0 += ty)
+        t.push_back(make_int4((int)b, x0, y0, std::min(y0 + ty, c->blk[b].ny)));
   return t;
 }
 
@@ -1196,7 +1209,7 @@ int batch_setup(lee_ctx* c) {
     CK(cudaMemcpy(d_t, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice));
     const int nt = (int)t.size();
     const int gs = std::min(nt, nsm * batch_stage_occupancy<T>(shape, c->comp ? 1 : 0));
-    const int gf = std::min(nt, nsm * 4);
+    const int gf = std::min(nt, nsm * batch_filter_occupancy<T>(shape, c->comp ? 1 : 0));
     float ms_s = 0.f, ms_f = 0.f;
     for (int pass = 0; pass < 2; ++pass) {  // the first pass warms up
       CK(cudaEventRecord(e0, c->stream));
@@ -2971,6 +2984,36 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
   (void)fwd_launches;
   if (trace_mismatches) *trace_mismatches = mismatches;
   return check_device_error(c);
+}
+
+int lee_set_batch_shapes(lee_ctx* c, int stage_shape, int filter_shape) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared || !c->batch.active) return fail(c, LEE_ERR_STATE, "the context does not run batched kernels");
+  if (stage_shape < 0 || stage_shape >= kBatchShapes || filter_shape < 0 || filter_shape >= kBatchShapes)
+    return fail(c, LEE_ERR_ARG, "shape index");
+  CK(cudaSetDevice(c->cfg.device));
+  auto& bt = c->batch;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->cfg.device);
+  const std::vector<int4> ts = batch_tiles(c, stage_shape), tf = batch_tiles(c, filter_shape);
+  int rc;
+  if ((rc = dalloc(c, &bt.d_stiles, ts.size())) || (rc = dalloc(c, &bt.d_ftiles, tf.size()))) return rc;
+  CK(cudaMemcpy(bt.d_stiles, ts.data(), ts.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(bt.d_ftiles, tf.data(), tf.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  bt.nst = (int)ts.size();
+  bt.nft = (int)tf.size();
+  bt.sshape = stage_shape;
+  bt.fshape = filter_shape;
+  const int occs = c->comp ? batch_stage_occupancy<float>(stage_shape, 1) : batch_stage_occupancy<double>(stage_shape, 0);
+  const int occf = c->comp ? batch_filter_occupancy<float>(filter_shape, 1)
+                           : batch_filter_occupancy<double>(filter_shape, 0);
+  bt.sgrid = std::min(bt.nst, nsm * occs);
+  bt.fgrid = std::min(bt.nft, nsm * occf);
+  if (c->graph.exec) {  // captured launches name the old work lists
+    cudaGraphExecDestroy(c->graph.exec);
+    c->graph.exec = nullptr;
+  }
+  return LEE_OK;
 }
 
 int lee_set_graphs(lee_ctx* c, int on) {

@@ -245,6 +245,8 @@ cudaError_t launch_batch_filter(const BatchFilterInst<T>* inst, const int4* tile
                                 int grid, const OpTable& op, double blend, cudaStream_t s);
 template <typename T>
 int batch_stage_occupancy(int shape, int comp);
+template <typename T>
+int batch_filter_occupancy(int shape, int comp);
 
 // lee_step.cu
 template <typename T>

@@ -190,6 +190,9 @@ int lee_advance_blocks(lee_ctx *ctx, int nsteps, const double *dt);
 /* The FIX_CFL time step of every block on its own (dt[b], as lee_compute_dt would give for a
  * context holding block b alone). */
 int lee_compute_dt_blocks(lee_ctx *ctx, double cfl, double *dt);
+/* Override the batched launches' work-item shapes that lee_prepare picked by timing (index
+ * 0..4; lee_info reports them): every shape gives the same results. */
+int lee_set_batch_shapes(lee_ctx *ctx, int stage_shape, int filter_shape);
 /* Sizes and coefficient layout chosen by lee_prepare (no reference counterpart: the
  * reference has no timers or counters, finding F13). */
 typedef struct {

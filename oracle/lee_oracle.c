@@ -1221,6 +1221,11 @@ int orc_adjoint_gradient(orc_ctx *c, int nsteps, double dt, int k, int recompute
   return fail(c, LEE_ERR_UNSUPPORTED, "the oracle has no adjoint");
 }
 
+int orc_set_batch_shapes(orc_ctx *c, int stage_shape, int filter_shape) {
+  (void)stage_shape; (void)filter_shape;
+  return fail(c, LEE_ERR_STATE, "the oracle has no batched kernels");
+}
+
 int orc_set_graphs(orc_ctx *c, int on) {
   (void)c; (void)on;
   return LEE_OK;

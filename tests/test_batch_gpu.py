@@ -63,6 +63,22 @@ def test_fp32_compensated_batch_vs_fp64_alone(product_lib):
         assert api.rel_l2(y[4], ya[4]) <= 1e-5
 
 
+def test_full_size_batch_stays_finite_and_close(product_lib):
+    """The 64-instance workload (5.2M points, the autotuned strip shapes) over 300 steps: the
+    compensated batch stays within 1e-5 of the FP64 batch in p'."""
+    case = cases.batch2d(nsteps=300)
+    a = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
+    b = api.Solver(product_lib, case, precision=api.FP64)
+    assert a.info().batched and b.info().batched
+    dts = b.compute_dt_blocks()
+    a.advance_blocks(case.nsteps, dts)
+    b.advance_blocks(case.nsteps, dts)
+    for q in range(0, len(case.blocks), 7):
+        ya, yb = a.download(q)[0], b.download(q)[0]
+        assert np.isfinite(ya).all()
+        assert api.rel_l2(ya[4], yb[4]) <= 1e-5
+
+
 @pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
 def test_batch_graphs_give_the_same_bits(product_lib, precision):
     case = _batch()
