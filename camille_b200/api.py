@@ -87,6 +87,8 @@ SIGNATURES = {
     "upload_state": (C.c_int, [C.c_void_p, C.c_int, _PP, C.c_int, C.c_double]),
     "download_state": (C.c_int, [C.c_void_p, C.c_int, _PP, _IP, _DP]),
     "compute_dt": (C.c_int, [C.c_void_p, C.c_double, _DP]),
+    "compute_cfl": (C.c_int, [C.c_void_p, C.c_double, _DP]),
+    "state_minmax": (C.c_int, [C.c_void_p, _DP, _DP]),
     "advance": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "eval_rhs": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _PP]),
     "apply_filter": (C.c_int, [C.c_void_p]),
@@ -173,8 +175,8 @@ class Solver:
                     sig = _dptr(sarr)
                 self._chk(lib.add_boundary(self.ctx, bd.block, _cases.BC_TYPES[bd.kind], bd.dir, bd.end,
                                            lo, hi, sig))
-            if case.monopole is not None:
-                p = np.array(case.monopole, np.float64)
+            if case.source_monopole() is not None:
+                p = np.array(case.source_monopole(), np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))
             for b, blk in enumerate(case.blocks):
                 if blk.monopole is not None:
@@ -240,6 +242,16 @@ class Solver:
         dt = C.c_double()
         self._chk(self.lib.compute_dt(self.ctx, self.case.cfl if cfl is None else cfl, C.byref(dt)))
         return dt.value
+
+    def compute_cfl(self, dt: float) -> float:
+        out = C.c_double()
+        self._chk(self.lib.compute_cfl(self.ctx, dt, C.byref(out)))
+        return out.value
+
+    def state_minmax(self) -> tuple[np.ndarray, np.ndarray]:
+        mn, mx = np.zeros(5), np.zeros(5)
+        self._chk(self.lib.state_minmax(self.ctx, _dptr(mn), _dptr(mx)))
+        return mn, mx
 
     def advance(self, nsteps: int, dt: float) -> None:
         self._chk(self.lib.advance(self.ctx, nsteps, dt))

@@ -1,4 +1,5 @@
-"""Build camille_b200/liblee_b200.so: the sm_100a CUDA library behind include/lee_b200.h.
+"""Build camille_b200/liblee_b200.so, the sm_100a CUDA library behind include/lee_b200.h, and
+camille_b200/lee_run, the deck-driven runner linked against it.
 
 nvcc cross-compiles for sm_100a without a GPU. The setup kernels (lee_setup.cu) are
 compiled with --fmad=false so the FP64 metric, Jacobian and mean-gradient generation
@@ -16,6 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "liblee_b200.so")
+RUNNER = os.path.join(PKG, "lee_run")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")] + ARCH
 UNITS = {
@@ -61,8 +63,14 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         list(ex.map(_compile, jobs))
     if jobs or not os.path.isfile(LIB):
         _compile([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"])
+    runner_src = os.path.join(CSRC, "lee_run.cpp")
+    if not os.path.isfile(RUNNER) or os.path.getmtime(RUNNER) < max(os.path.getmtime(LIB), os.path.getmtime(runner_src)):
+        # the deck-driven runner links the library by name and finds it beside itself
+        _compile(["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), runner_src, "-o", RUNNER,
+                  "-L", PKG, "-llee_b200", "-Wl,-rpath,$ORIGIN"])
     if verbose:
         print(LIB)
+        print(RUNNER)
     return LIB
 
 

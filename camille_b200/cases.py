@@ -108,6 +108,12 @@ class Microphones:
     weight: Optional[float] = None
 
 
+# The pressure source of the reference's CASE_SCATTERING_TWOCYLINDER (src/solver/source.cpp:60-92),
+# (gamma - 1) exp(-ln 2 r^2 / 0.2^2) sin(4 * 2 pi t) ramped by sin^2(pi/2 t / 4) up to t = 4, as
+# monopole parameters (x0, y0, z0, amplitude, omega, halfwidth, ramp_time).
+TWOCYLINDER_SOURCE = (0.0, 0.0, 0.0, 1.0, 4.0 * (2.0 * math.pi), 0.2, 16.0 / 4.0)
+
+
 @dataclasses.dataclass
 class Case:
     name: str
@@ -131,27 +137,38 @@ class Case:
     distributed: Optional[DistributedSource] = None
     microphones: Optional[Microphones] = None
     notes: str = ""
+    # the deck's SIMULATION; CASE_SCATTERING_TWOCYLINDER brings the reference's own source
+    simulation: str = "CASE_KBK_COMBUSTOR"
 
     @property
     def npoints(self) -> int:
         return sum(b.npoints for b in self.blocks)
 
+    def source_monopole(self) -> Optional[tuple[float, float, float, float, float, float, float]]:
+        """The monopole that acts on every block: the case's own, else the one SIMULATION implies."""
+        if self.monopole is not None:
+            return self.monopole
+        if self.simulation == "CASE_SCATTERING_TWOCYLINDER":
+            return TWOCYLINDER_SOURCE
+        return None
+
     # ---- reference input files -------------------------------------------------
-    def deck_lines(self, dt: Optional[float], nsteps: int, grid: str, mean: str, bc: str) -> list[str]:
+    def deck_lines(self, dt: Optional[float], nsteps: int, grid: str, mean: str, bc: str,
+                   report: int = 2000000000) -> list[str]:
         fix = "FIX_DT" if dt is not None else "FIX_CFL"
         lines = [
             f"DIMENSION = {self.num_dim}",
             "AXISYMMETRY = FALSE",
             "PHYSICAL_MODEL = LEE",
             "FLUID_MODEL = IDEAL_GAS_CALORIC",
-            "SIMULATION = CASE_KBK_COMBUSTOR",
+            f"SIMULATION = {self.simulation}",
             f"GAMMA_SPECIFICHEAT = {self.gamma!r}",
             f"FIX_DT_OR_CFL = {fix}",
             f"DT = {dt!r}" if dt is not None else "DT = 1.0E-6",
             f"CFL = {self.cfl!r}",
             f"TEMPORAL_SCHEME = {self.rk}",
             f"NUM_TOTAL_TIMESTEP = {nsteps}",
-            "REPORT_TIMESTEP = 2000000000",
+            f"REPORT_TIMESTEP = {report}",
         ]
         if self.fd_scheme == "STANDARD_CENTRAL":
             lines.append(f"SPATIAL_SCHEME = STANDARD_CENTRAL, ORDER_ACCURACY = {self.fd_order}")
@@ -187,13 +204,18 @@ class Case:
             "HARMONIC_WAVE = NONE",
             "INTERPOLATE_SOLUTION = NONE",
         ]
+        if self.monopole is not None:
+            # read by camille_b200/lee_run only; the reference never looks the name up
+            lines.append("SOURCE_MONOPOLE = " + ", ".join(repr(float(v)) for v in self.monopole))
         return lines
 
     def write_reference_inputs(self, workdir: str, dt: Optional[float], nsteps: int,
-                               step: int = 0, time: float = 0.0) -> str:
+                               step: int = 0, time: float = 0.0, report: int = 2000000000) -> str:
         """Write grid, mean, restart, BC and deck files; return the restart path."""
         if self.distributed is not None:
             raise ValueError("the reference cannot express a distributed source")
+        if self.monopole is not None and self.simulation == "CASE_SCATTERING_TWOCYLINDER":
+            raise ValueError("a case-level monopole and the two-cylinder source do not combine")
         os.makedirs(workdir, exist_ok=True)
         grid, mean, ic, bc = (os.path.join(workdir, n) for n in ("grid.xyz", "mean.q", "ic.q", "bc.in"))
         plot3d.write_grid(grid, [(b.x, b.y, b.z) for b in self.blocks])
@@ -202,7 +224,7 @@ class Case:
         plot3d.write_bc(bc, [bd.line() for bd in self.boundaries])
         if self.overset is not None:
             self.overset.write(os.path.join(workdir, "overset.bin"))
-        plot3d.write_deck(os.path.join(workdir, "camille.in"), self.deck_lines(dt, nsteps, grid, mean, bc))
+        plot3d.write_deck(os.path.join(workdir, "camille.in"), self.deck_lines(dt, nsteps, grid, mean, bc, report))
         return ic
 
 

@@ -8,6 +8,7 @@
 //     accumulator), then the boundary conditions of the stage output
 //   filter passes (dimension split, src/solver/spatial_discretization.cpp:2191-2246)
 //   hole mask (temporal::iblank_correction, :380-393)
+#include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -141,6 +142,7 @@ struct lee_ctx {
   int hf = 0;
   bool wst_ok = false, wfl_ok = false;
   int* d_err = nullptr;
+  double* d_report = nullptr;  // -min and max of the five state slots (lee_state_minmax)
   // overset maps (host copies, then device arrays from lee_prepare)
   struct {
     int n = 0, W = 1, w[3] = {1, 1, 1};
@@ -2505,13 +2507,12 @@ int lee_download_state(lee_ctx* c, int b, double* const sol[5], int* step, doubl
 
 namespace {
 
-// CFL maxima (temporal::compute_CFL with the dummy dt) of every block, or of all blocks.
-int cfl_max(lee_ctx* c, bool per_block, std::vector<double>& out) {
+// CFL maxima (temporal::compute_CFL) at time step dt0 of every block, or of all blocks.
+int cfl_max(lee_ctx* c, bool per_block, std::vector<double>& out, double dt0) {
   CK(cudaSetDevice(c->cfg.device));
   double* d_max = nullptr;
   CK(cudaMallocAsync((void**)&d_max, sizeof(double), c->stream));
   const double init = -1e308;
-  const double dt0 = 1e-6;  // the reference's dummy initial dt (src/core/input.cpp:131)
   out.clear();
   CK(cudaMemcpyAsync(d_max, &init, sizeof init, cudaMemcpyHostToDevice, c->stream));
   for (auto& b : c->blk) {
@@ -2545,10 +2546,13 @@ int cfl_max(lee_ctx* c, bool per_block, std::vector<double>& out) {
   return LEE_OK;
 }
 
-// The FIX_CFL rescale of solver::solve (src/solver/solver.cpp:58-64).
+// The reference's dummy initial dt (src/core/input.cpp:131).
+constexpr double kDummyDt = 1e-6;
+
+// The FIX_CFL rescale of solver::solve (src/solver/solver.cpp:58-64) from the dummy dt.
 double rescale(double cfl, double cmax) {
   double ratio = cfl / cmax;
-  double d = 1e-6;
+  double d = kDummyDt;
   d *= ratio;
   return d;
 }
@@ -2560,9 +2564,46 @@ int lee_compute_dt(lee_ctx* c, double cfl, double* dt) {
   if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
   if (!(cfl > 0.0)) return fail(c, LEE_ERR_ARG, "cfl must be positive");
   std::vector<double> m;
-  int rc = cfl_max(c, false, m);
+  int rc = cfl_max(c, false, m, kDummyDt);
   if (rc) return rc;
   *dt = rescale(cfl, m[0]);
+  return LEE_OK;
+}
+
+int lee_compute_cfl(lee_ctx* c, double dt, double* cfl) {
+  if (!c || !cfl) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  if (!(dt > 0.0)) return fail(c, LEE_ERR_ARG, "dt must be positive");
+  std::vector<double> m;
+  int rc = cfl_max(c, false, m, dt);
+  if (rc) return rc;
+  *cfl = m[0];
+  return LEE_OK;
+}
+
+int lee_state_minmax(lee_ctx* c, double* mn, double* mx) {
+  if (!c || !mn || !mx) return LEE_ERR_ARG;
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
+  CK(cudaSetDevice(c->cfg.device));
+  if (!c->d_report) {
+    int rc = dalloc(c, &c->d_report, 10);
+    if (rc) return rc;
+  }
+  double init[10];
+  for (int q = 0; q < 10; ++q) init[q] = -DBL_MAX;
+  CK(cudaMemcpyAsync(c->d_report, init, sizeof init, cudaMemcpyHostToDevice, c->stream));
+  for (auto& bk : c->blk)
+    for (int v = 0; v < c->V; ++v)
+      CK(setup_state_minmax(bk.N, bk.y[v], c->comp ? bk.comp[v] : nullptr, c->comp, c->d_report + 2 * slot_of(c->V, v),
+                            c->stream));
+  double out[10];
+  CK(cudaMemcpyAsync(out, c->d_report, sizeof out, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int q = 0; q < 5; ++q) {
+    mn[q] = -out[2 * q];
+    mx[q] = out[2 * q + 1];
+  }
+  if (c->cfg.num_dim == 2) mn[3] = mx[3] = 0.0;  // the w' slot of a 2-D state holds zeros
   return LEE_OK;
 }
 
@@ -2571,7 +2612,7 @@ int lee_compute_dt_blocks(lee_ctx* c, double cfl, double* dt) {
   if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
   if (!(cfl > 0.0)) return fail(c, LEE_ERR_ARG, "cfl must be positive");
   std::vector<double> m;
-  int rc = cfl_max(c, true, m);
+  int rc = cfl_max(c, true, m, kDummyDt);
   if (rc) return rc;
   for (size_t b = 0; b < m.size(); ++b) dt[b] = rescale(cfl, m[b]);
   return LEE_OK;

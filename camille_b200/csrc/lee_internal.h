@@ -273,6 +273,7 @@ cudaError_t setup_scale(int n, double* out, const double* sum, const double* jac
 cudaError_t setup_sigma(int nx, int ny, int nz, const double* const* xyz, const int lo[3], const int hi[3], int dir,
                         int end, int order, double constant, double* sig, cudaStream_t s);
 cudaError_t setup_minmax(int n, const double* f, double* d_out2, cudaStream_t s);
+cudaError_t setup_state_minmax(long long n, const void* y, const void* e, bool fp32, double* d_out2, cudaStream_t s);
 cudaError_t setup_cfl(int n, int dim, const double* const* met, const double* jac, const double* const* ubar,
                       const double* pbar, const double* sbar, const int* iblank, double gamma, double dt,
                       double* d_max, cudaStream_t s);

@@ -205,6 +205,33 @@ __global__ void k_minmax(long long n, const double* f, double* out2) {
   }
 }
 
+// Minimum and maximum of one state field, the value of a point being y (FP64) or fl64(y) + fl64(e)
+// (a compensated FP32 pair): out2[0] collects -min and out2[1] max, both by atomic maximum.
+template <typename T>
+__global__ void k_state_minmax(long long n, const T* y, const T* e, double* out2) {
+  __shared__ double smin[kThreads], smax[kThreads];
+  double lo = DBL_MAX, hi = -DBL_MAX;
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x) {
+    const double v = e ? (double)y[l] + (double)e[l] : (double)y[l];
+    lo = v < lo ? v : lo;
+    hi = v > hi ? v : hi;
+  }
+  smin[threadIdx.x] = lo;
+  smax[threadIdx.x] = hi;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
+      smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    atomic_max_double(&out2[0], -smin[0]);
+    atomic_max_double(&out2[1], smax[0]);
+  }
+}
+
 // temporal::compute_CFL (src/solver/temporal_discretization.cpp:397-450), including the
 // convective term's truncation to int (abs(double) resolving to int abs(int) at :425).
 __global__ void k_cfl(long long n, int dim, const double* const* met, const double* jac, const double* const* ub,
@@ -326,6 +353,14 @@ cudaError_t setup_sigma(int nx, int ny, int nz, const double* const* xyz, const 
 
 cudaError_t setup_minmax(int n, const double* f, double* d_out2, cudaStream_t s) {
   k_minmax<<<grid_for(n), kThreads, 0, s>>>(n, f, d_out2);
+  return cudaGetLastError();
+}
+
+cudaError_t setup_state_minmax(long long n, const void* y, const void* e, bool fp32, double* d_out2, cudaStream_t s) {
+  if (fp32)
+    k_state_minmax<float><<<grid_for(n), kThreads, 0, s>>>(n, (const float*)y, (const float*)e, d_out2);
+  else
+    k_state_minmax<double><<<grid_for(n), kThreads, 0, s>>>(n, (const double*)y, (const double*)e, d_out2);
   return cudaGetLastError();
 }
 

@@ -163,8 +163,17 @@ int lee_download_state(lee_ctx *ctx, int b, double *const sol[5], int *step, dou
 
 /* Time step for a target CFL (temporal::compute_CFL, src/solver/temporal_discretization.cpp:397-450),
  * including the reference's truncation of the convective term to an int (abs(double) resolving to
- * int abs(int) at :425): dt = cfl / max over non-hole points of the per-unit-dt CFL. */
+ * int abs(int) at :425): the first FIX_CFL step of solver::solve (src/solver/solver.cpp:54-64),
+ * dt = 1e-6 * (cfl / cmax) with cmax the largest CFL over non-hole points at the dummy dt 1e-6. */
 int lee_compute_dt(lee_ctx *ctx, double cfl, double *dt);
+/* Largest CFL over all non-hole points at time step dt (temporal::compute_CFL,
+ * src/solver/temporal_discretization.cpp:397-450): the value solver::solve reports and, under
+ * FIX_CFL, rescales dt by at every step (src/solver/solver.cpp:54-68). */
+int lee_compute_cfl(lee_ctx *ctx, double dt, double *cfl);
+/* Minimum and maximum of each of the five solution slots over every point of every block
+ * (ReportSolution::minmax, src/io/io.cpp:440-499), reduced on the GPU; a 2-D state's w' slot
+ * reports 0 ~ 0. */
+int lee_state_minmax(lee_ctx *ctx, double mn[5], double mx[5]);
 /* Advance every block by nsteps RK steps of size dt (FIX_DT): per step the RK stages with
  * boundary conditions and overset updates, the filter and the hole mask
  * (temporal::time_advance, src/solver/temporal_discretization.cpp:334-374). */

@@ -989,13 +989,12 @@ int orc_download_state(orc_ctx *c, int b, double *const sol[5], int *step, doubl
   return LEE_OK;
 }
 
-/* temporal::compute_CFL (src/solver/temporal_discretization.cpp:397-450) with the
- * reference's dummy initial dt of 1e-6 (src/core/input.cpp:131) and the FIX_CFL
- * rescale of solver::solve (src/solver/solver.cpp:58-64). */
-int orc_compute_dt(orc_ctx *c, double cfl_target, double *dt_out) {
-  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+/* temporal::compute_CFL (src/solver/temporal_discretization.cpp:397-450) at time step dt;
+ * orc_compute_dt applies it at the reference's dummy initial dt of 1e-6
+ * (src/core/input.cpp:131) with the FIX_CFL rescale of solver::solve (src/solver/solver.cpp:58-64). */
+static double cfl_at(orc_ctx *c, double dt) {
   int nd = c->cfg.num_dim;
-  double dt = 1e-6, cmax = -1e99, gm1 = c->cfg.gamma - 1.0;
+  double cmax = -1e99, gm1 = c->cfg.gamma - 1.0;
   for (int b = 0; b < c->nblk; ++b) {
     blk_t *bk = &c->blk[b];
     for (int p = 0; p < bk->N; ++p) {
@@ -1018,9 +1017,38 @@ int orc_compute_dt(orc_ctx *c, double cfl_target, double *dt_out) {
       if (cfl > cmax) cmax = cfl;
     }
   }
-  double ratio = cfl_target / cmax;
+  return cmax;
+}
+
+int orc_compute_dt(orc_ctx *c, double cfl_target, double *dt_out) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  double dt = 1e-6;
+  double ratio = cfl_target / cfl_at(c, dt);
   dt *= ratio;
   *dt_out = dt;
+  return LEE_OK;
+}
+
+int orc_compute_cfl(orc_ctx *c, double dt, double *cfl) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  if (!(dt > 0.0)) return fail(c, LEE_ERR_ARG, "dt must be positive");
+  *cfl = cfl_at(c, dt);
+  return LEE_OK;
+}
+
+/* ReportSolution::minmax (src/io/io.cpp:440-499) over every point of every block. */
+int orc_state_minmax(orc_ctx *c, double *mn, double *mx) {
+  if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
+  for (int q = 0; q < 5; ++q) {
+    mn[q] = 1e300;
+    mx[q] = -1e300;
+    for (int b = 0; b < c->nblk; ++b)
+      for (int p = 0; p < c->blk[b].N; ++p) {
+        double v = c->blk[b].sol[q][p];
+        mn[q] = v < mn[q] ? v : mn[q];
+        mx[q] = v > mx[q] ? v : mx[q];
+      }
+  }
   return LEE_OK;
 }
 

@@ -42,5 +42,5 @@ def load_golden(name: str) -> dict:
 
 
 def golden_case(name: str):
-    from tests.golden.make_golden import WORKLOADS
-    return WORKLOADS[name]()
+    from tests.golden.make_golden import OVERSET_WORKLOADS, WORKLOADS
+    return (WORKLOADS[name] if name in WORKLOADS else OVERSET_WORKLOADS[name])()
