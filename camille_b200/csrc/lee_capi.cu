@@ -85,6 +85,8 @@ struct BlockData {
   bool rho_valid = false;   // false until a step or a filter call has written it
   // TMA-staged kernels (blocks without holes, 4th-order difference)
   bool tma = false, tma_filter = false;
+  bool filter_vec = false;           // the fused filter runs the vectorised kernel (lee_filter.cu)
+  int vtiles_x = 0, vtiles_y = 0;    // its tiles
   int traits = kTrGeneric;          // coefficient-layout traits of the TMA stage kernel
   void* d_sigma_field = nullptr;    // summed sponge strengths per point (working precision)
   int tiles_x = 0, tiles_y = 0;
@@ -141,6 +143,7 @@ struct lee_ctx {
   double wfl[11][11] = {};
   int hf = 0;
   bool wst_ok = false, wfl_ok = false;
+  bool wfl_sym = false;  // symmetric interior filter stencil: the vectorised filter kernel applies
   int* d_err = nullptr;
   double* d_report = nullptr;  // -min and max of the five state slots (lee_state_minmax)
   // overset maps (host copies, then device arrays from lee_prepare)
@@ -402,6 +405,12 @@ template <typename T>
 __global__ void k_to_double(long long n, double* out, const T* y, const T* comp) {
   for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
     out[l] = comp ? (double)y[l] + (double)comp[l] : (double)y[l];
+}
+
+template <typename T>
+__global__ void k_fill_const(long long n, T* out, T v) {
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
+    out[l] = v;
 }
 
 __global__ void k_zero_bytes(long long n, unsigned char* p) {
@@ -831,7 +840,12 @@ int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* co
   int rc = field_maps(c, b, zin, Box<T, kFdHalf>::BX, Box<T, kFdHalf>::BY, &fm);
   if (rc) return rc;
   const int chunks = c->cfg.num_dim == 3 ? (b.nz + tp.k_chunk - 1) / tp.k_chunk : 1;
-  CK(launch_stage_tma<T>(fm, tp, b.traits, b.tiles_x * b.tiles_y, chunks, c->stream));
+  // the stage's kind selects a specialised kernel; a first stage that is also the last (no
+  // such tableau here) reads p.stage and p.last at run time
+  const int kind = p.stage < 0 ? kKindRhs
+                   : p.stage == 0 ? (p.last ? kKindRuntime : kKindFirst)
+                                  : (p.last ? kKindLast : kKindMid);
+  CK(launch_stage_tma<T>(fm, tp, b.traits | (kind << kKindShift), b.tiles_x * b.tiles_y, chunks, c->stream));
   return LEE_OK;
 }
 
@@ -854,14 +868,22 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
     fp.comp[v] = comp_out ? (T*)comp_out[v] : nullptr;
   }
   fp.errflag = c->d_err;
-  int bx, by;
-  filter_box(c, &bx, &by);
+  int bx, by, tx, ty;
+  if (b.filter_vec) {
+    filter_vec_box(c->esz, c->hf, &bx, &by, &tx, &ty);
+    fp.tiles_x = b.vtiles_x;
+  } else {
+    filter_box(c, &bx, &by);
+  }
   FieldMaps fm;
   int rc = field_maps(c, b, in, bx, by, &fm);
   if (rc) return rc;
   const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
   int e0 = mark(c);
-  CK(launch_filter_tma<T>(fm, fp, c->hf, c->cfg.num_dim, c->comp ? 1 : 0, b.tiles_x * b.tiles_y, chunks, c->stream));
+  if (b.filter_vec)
+    CK(launch_filter_vec<T>(fm, fp, c->hf, c->cfg.num_dim, b.vtiles_x * b.vtiles_y, chunks, c->stream));
+  else
+    CK(launch_filter_tma<T>(fm, fp, c->hf, c->cfg.num_dim, c->comp ? 1 : 0, b.tiles_x * b.tiles_y, chunks, c->stream));
   int e1 = mark(c);
   span(c, 1, e0, e1);
   c->stats.filter_launches += 1;
@@ -1858,6 +1880,8 @@ int lee_create(const lee_config* cfg, lee_ctx** out) {
     c->fltd = minus_identity(c->flt);
     c->hf = c->flt.h;
     c->wfl_ok = c->hf <= 5 && class_weights(c->comp ? c->fltd : c->flt, c->hf, &c->wfl[0][0], 11);
+    c->wfl_sym = c->wfl_ok && (c->hf == 2 || c->hf == 4 || c->hf == 5);
+    for (int o = 1; o <= c->hf && c->wfl_sym; ++o) c->wfl_sym = c->wfl[0][c->hf - o] == c->wfl[0][c->hf + o];
   }
   c->wst_ok = c->fd.h == kFdHalf && class_weights(c->fd, kFdHalf, &c->wst[0][0], 5);
   c->blk.resize((size_t)cfg->num_blocks);
@@ -2387,8 +2411,16 @@ int lee_prepare(lee_ctx* c) {
     const bool rows16 = ((size_t)b.nx * c->esz) % 16 == 0;
     b.tiles_x = (b.nx + kTileX - 1) / kTileX;
     b.tiles_y = (b.ny + kTileY - 1) / kTileY;
-    b.tma = c->wst_ok && !b.has_holes && rows16;
+    // (the TMA stage kernel addresses points with 32-bit offsets)
+    b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32);
     b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE;
+    b.filter_vec = b.tma_filter && c->wfl_sym;
+    if (b.filter_vec) {
+      int bx, by, tx, ty;
+      filter_vec_box(c->esz, c->hf, &bx, &by, &tx, &ty);
+      b.vtiles_x = (b.nx + tx - 1) / tx;
+      b.vtiles_y = (b.ny + ty - 1) / ty;
+    }
     if (b.tma) {
       // coefficient-layout traits of the stage kernel
       bool jmf = false, uni = true, spg = false;
@@ -2402,8 +2434,29 @@ int lee_prepare(lee_ctx* c) {
       for (int q = 0; q < 9; ++q) uni &= is_zero(b.cd_gu[q], b.cf_gu[q]) != 0;
       uni &= is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi) && !b.need_rho;
       for (auto& z : b.bnd) spg |= z.kind == LEE_SPONGE_FREUND_AMBIENT;
-      b.traits = (jmf ? kTrJmField : 0) | (uni ? kTrUniform : 0) | (spg ? kTrSponge : 0);
+      b.traits = kTrTma | (jmf ? kTrJmField : 0) | (uni ? kTrUniform : 0) | (spg ? kTrSponge : 0);
       if (spg && (rc = build_sigma_field(c, b))) return rc;
+      if (jmf) {
+        // the TMA kernel reads every J*metrics entry as a field when one is: constant entries
+        // become fields holding their constant
+        for (int l = 0; l < dim; ++l)
+          for (int x = 0; x < dim; ++x) {
+            const int q = l * 3 + x;
+            if (c->comp && !b.cf_jm[q].p) {
+              float* f = nullptr;
+              if ((rc = dalloc(c, &f, (size_t)b.N))) return rc;
+              k_fill_const<float><<<grid1d(b.N), 256, 0, c->stream>>>(b.N, f, b.cf_jm[q].c);
+              CK(cudaGetLastError());
+              b.cf_jm[q].p = f;
+            } else if (!c->comp && !b.cd_jm[q].p) {
+              double* f = nullptr;
+              if ((rc = dalloc(c, &f, (size_t)b.N))) return rc;
+              k_fill_const<double><<<grid1d(b.N), 256, 0, c->stream>>>(b.N, f, b.cd_jm[q].c);
+              CK(cudaGetLastError());
+              b.cd_jm[q].p = f;
+            }
+          }
+      }
     }
     b.stage_chunk = b.filter_chunk = b.nz;
     if ((b.tma || b.tma_filter) && (rc = ensure_encoder(c))) return rc;

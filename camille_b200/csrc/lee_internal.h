@@ -17,6 +17,11 @@ constexpr int kTrJmField = 1;  // J*metrics vary over the block (else kernel con
 constexpr int kTrUniform = 2;  // uniform mean flow: u_bar, p_bar, rho_bar constant, zero gradients
 constexpr int kTrSponge = 4;   // sponge strengths summed into one per-point field (else the zone loop)
 constexpr int kTrGeneric = kTrJmField;  // every coefficient checked at run time
+// Launch-time traits of the TMA stage kernel (blocks without holes), added to the layout traits:
+constexpr int kTrTma = 8;       // no holes; with kTrJmField every J*metrics entry is a per-point field;
+                                // 32-bit point offsets
+constexpr int kKindShift = 4;   // bits 4..6: the stage's kind; 0 reads p.stage and p.last at run time
+constexpr int kKindRuntime = 0, kKindRhs = 1, kKindFirst = 2, kKindMid = 3, kKindLast = 4;
 
 // One directional operator: interior stencil c[l+h] (l = -h..h), closure rows
 // B[row][s] (row < nb, s < S) and the right-boundary sign (-1 difference, +1 filter).

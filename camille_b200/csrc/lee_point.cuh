@@ -10,10 +10,28 @@
 
 namespace lee {
 
-template <typename T>
-__device__ __forceinline__ T cval(const Coef<T>& c, long long l) {
+template <typename T, typename I>
+__device__ __forceinline__ T cval(const Coef<T>& c, I l) {
   return c.p ? __ldg(c.p + l) : c.c;
 }
+
+// The stage's kind: from the traits when they fix it, else from p.stage and p.last.
+template <int TR>
+struct Kind {
+  static constexpr int K = (TR >> kKindShift) & 7;
+  template <typename T>
+  __device__ __forceinline__ static bool rhs(const StageParams<T>& p) {
+    return K == kKindRuntime ? p.stage < 0 : K == kKindRhs;
+  }
+  template <typename T>
+  __device__ __forceinline__ static bool first(const StageParams<T>& p) {
+    return K == kKindRuntime ? p.stage == 0 : K == kKindFirst;
+  }
+  template <typename T>
+  __device__ __forceinline__ static bool last(const StageParams<T>& p) {
+    return K == kKindRuntime ? p.last != 0 : K == kKindLast;
+  }
+};
 
 // Per-point inputs read from global memory, gathered before the arithmetic so that
 // every load of the point is in flight at once.
@@ -25,35 +43,41 @@ struct PointIn {
   T sg;               // sponge strength (kTrSponge)
 };
 
-template <typename T, int DIM, bool COMP, int TR>
-__device__ __forceinline__ void gather(const StageParams<T>& p, long long l, PointIn<T, DIM>& in) {
+template <typename T, int DIM, bool COMP, int TR, typename I>
+__device__ __forceinline__ void gather(const StageParams<T>& p, I l, PointIn<T, DIM>& in) {
   constexpr int V = DIM + 2;
+  using K = Kind<TR>;
 #pragma unroll
   for (int d = 0; d < DIM; ++d)
 #pragma unroll
-    for (int x = 0; x < DIM; ++x) in.jm[d][x] = (TR & kTrJmField) ? cval(p.jm[d * 3 + x], l) : p.jm[d * 3 + x].c;
-  const bool need_yn = p.stage > 0 && (COMP || !p.last);
-  const bool need_av = p.stage > 0 || (COMP && p.stage == 0);
+    for (int x = 0; x < DIM; ++x) {
+      const Coef<T>& c = p.jm[d * 3 + x];
+      // TMA kernels: every entry is a field when any is
+      in.jm[d][x] = (TR & kTrJmField) ? ((TR & kTrTma) ? __ldg(c.p + l) : cval(c, l)) : c.c;
+    }
+  const bool mid = !K::rhs(p) && !K::first(p);
+  const bool need_yn = mid && (COMP || !K::last(p));
+  const bool need_av = mid || (COMP && K::first(p));
 #pragma unroll
   for (int v = 0; v < V; ++v) {
     in.yn[v] = need_yn ? p.yn[v][l] : T(0);
-    in.av[v] = need_av ? (p.stage == 0 ? p.comp[v][l] : p.acc[v][l]) : T(0);
+    in.av[v] = need_av ? (K::first(p) ? p.comp[v][l] : p.acc[v][l]) : T(0);
   }
   in.sg = (TR & kTrSponge) ? __ldg(p.sigma + l) : T(0);
 }
 
-template <typename T, int DIM>
-__device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, long long l, const T (&g)[DIM + 2][DIM],
+template <typename T, int DIM, int TR, typename I>
+__device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, I l, const T (&g)[DIM + 2][DIM],
                                                const T (&q)[DIM + 2], const T (&ub)[DIM], T (&r)[DIM + 2]);
-template <typename T, int DIM, bool COMP>
-__device__ __forceinline__ void rk_update(const StageParams<T>& p, long long l, const T (&q)[DIM + 2],
+template <typename T, int DIM, bool COMP, int TR, typename I>
+__device__ __forceinline__ void rk_update(const StageParams<T>& p, I l, const T (&q)[DIM + 2],
                                           const PointIn<T, DIM>& in, const T (&r)[DIM + 2]);
 
 // D[v][d]: computational-space derivative of field v along direction d; q[v]: the
 // stage input at the point; in: the gathered inputs. Writes the next stage input and
 // the accumulator.
-template <typename T, int DIM, bool COMP, int TR>
-__device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l, int i, int j, int k,
+template <typename T, int DIM, bool COMP, int TR, typename I>
+__device__ __forceinline__ void rhs_update(const StageParams<T>& p, I l, int i, int j, int k,
                                            const T (&D)[DIM + 2][DIM], const T (&q)[DIM + 2],
                                            const PointIn<T, DIM>& in) {
   constexpr int V = DIM + 2;
@@ -99,7 +123,7 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l,
     }
     r[P] = rp;
   } else {
-    rhs_mean_terms<T, DIM>(p, l, g, q, ub, r);
+    rhs_mean_terms<T, DIM, TR>(p, l, g, q, ub, r);
   }
   if (p.has_src && i >= p.src_lo[0] && i <= p.src_hi[0] && j >= p.src_lo[1] && j <= p.src_hi[1] &&
       k >= p.src_lo[2] && k <= p.src_hi[2]) {
@@ -122,13 +146,13 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, long long l,
       for (int v = 0; v < V; ++v) r[v] += -sg * (q[v] - T(0));
     }
   }
-  rk_update<T, DIM, COMP>(p, l, q, in, r);
+  rk_update<T, DIM, COMP, TR>(p, l, q, in, r);
 }
 
 // The LEE right-hand side of a non-uniform mean flow: every coefficient is read at the point
 // when it varies, and terms whose mean gradient is identically zero are skipped.
-template <typename T, int DIM>
-__device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, long long l, const T (&g)[DIM + 2][DIM],
+template <typename T, int DIM, int TR, typename I>
+__device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, I l, const T (&g)[DIM + 2][DIM],
                                                const T (&q)[DIM + 2], const T (&ub)[DIM], T (&r)[DIM + 2]) {
   constexpr int P = DIM + 1;
   {
@@ -142,7 +166,7 @@ __device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, long lon
   }
   T rr = T(0);
   if (p.need_rho) {
-    if (p.stage <= 0 && p.rho_prev) {
+    if ((Kind<TR>::first(p) || Kind<TR>::rhs(p)) && p.rho_prev) {
       rr = p.rho_prev[l];
     } else {
       rr = q[P] * p.inv_gamma * (T(1) / cval(p.pbar, l)) - q[0];
@@ -177,37 +201,39 @@ __device__ __forceinline__ void rhs_mean_terms(const StageParams<T>& p, long lon
 }
 
 // The Runge-Kutta stage update of one point from its right-hand side r.
-template <typename T, int DIM, bool COMP>
-__device__ __forceinline__ void rk_update(const StageParams<T>& p, long long l, const T (&q)[DIM + 2],
+template <typename T, int DIM, bool COMP, int TR, typename I>
+__device__ __forceinline__ void rk_update(const StageParams<T>& p, I l, const T (&q)[DIM + 2],
                                           const PointIn<T, DIM>& in, const T (&r)[DIM + 2]) {
   constexpr int V = DIM + 2;
-  if (p.stage < 0) {  // right-hand side only (spatial::compute_RHS)
+  using K = Kind<TR>;
+  if (K::rhs(p)) {  // right-hand side only (spatial::compute_RHS)
 #pragma unroll
     for (int v = 0; v < V; ++v) p.zout[v][l] = r[v];
     return;
   }
-  const bool hole = p.iblank && p.iblank[l] == 1;
+  const bool first = K::first(p), last = K::last(p);
+  const bool hole = !(TR & kTrTma) && p.iblank && p.iblank[l] == 1;
 #pragma unroll
   for (int v = 0; v < V; ++v) {
     if (hole) {
       p.acc[v][l] = T(0);
-      if (!p.last || COMP) p.zout[v][l] = T(0);
+      if (!last || COMP) p.zout[v][l] = T(0);
       continue;
     }
     const T hk = r[v] * p.h;
     if (!COMP) {
       // y_next = y_n + sum b_i h k_i; the next stage input y_n + a h k_i
-      const T yv = p.stage == 0 ? q[v] : in.yn[v];
-      const T prev = p.stage == 0 ? q[v] : in.av[v];
+      const T yv = first ? q[v] : in.yn[v];
+      const T prev = first ? q[v] : in.av[v];
       p.acc[v][l] = prev + p.b * hk;
-      if (!p.last) p.zout[v][l] = yv + p.a * hk;
+      if (!last) p.zout[v][l] = yv + p.a * hk;
     } else {
       // compensated form: acc carries the increment of y since y_n plus the carried
       // rounding error of y; the last stage forms y_pre = y_n + increment as an exact
       // two-float sum (y_pre in zout, its rounding error in acc)
-      const T yv = p.stage == 0 ? q[v] : in.yn[v];
+      const T yv = first ? q[v] : in.yn[v];
       const T inc = in.av[v] + p.b * hk;
-      if (!p.last) {
+      if (!last) {
         p.acc[v][l] = inc;
         p.zout[v][l] = yv + p.a * hk;
       } else {

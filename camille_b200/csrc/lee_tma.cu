@@ -20,63 +20,10 @@
 // flight and returns, and the host reports LEE_ERR_TIMEOUT.
 #include "lee_point.cuh"
 #include "lee_tma.h"
+#include "lee_tma_util.cuh"
 
 namespace lee {
 namespace {
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned n) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
-}
-
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ unsigned mbar_try(uint64_t* b, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok;
-}
-
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Wait for the phase of the given parity; false after about one second.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
-  if (mbar_try(b, parity)) return true;
-  const unsigned long long t0 = gtimer();
-  for (unsigned it = 1;; ++it) {
-    if (mbar_try(b, parity)) return true;
-    if ((it & 63u) == 0u && gtimer() - t0 > 1000000000ull) return false;
-  }
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-          smem_u32(dst)),
-      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// Closure class of a position along a line with nb closure rows at each end:
-// 0 interior, 1 + p for the left rows, 1 + nb + (n - 1 - p) for the right rows.
-__device__ __forceinline__ int cls_of(int pos, int n, int nb) {
-  return pos < nb ? 1 + pos : (pos > n - 1 - nb ? 1 + nb + (n - 1 - pos) : 0);
-}
 
 template <typename T, int DIM, bool COMP, int TR>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
@@ -118,7 +65,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
   if (tid == 0) issue_upto(plo + NS - 1);
 
   const int c = (ty + H) * BX + (tx + HX);
-  // closure-class weights along xi and eta are fixed for a thread: keep them in registers
+  // closure-class weights along xi and eta are fixed for a thread: kept in registers
   T wx[2 * H + 1], wy[2 * H + 1];
   {
     const int cx = active ? cls_of(i, s.nx, H) : 0;
@@ -129,19 +76,23 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
       wy[o] = P.w[cy][o];
     }
   }
-  const long long nxy = (long long)s.nx * s.ny;
-  const long long lij = i + (long long)s.nx * j;
+  // point offsets fit 32 bits (the host checks the block size)
+  const unsigned nxy = (unsigned)s.nx * (unsigned)s.ny;
+  const unsigned lij = (unsigned)i + (unsigned)s.nx * (unsigned)j;
   // pointwise inputs (y_n, accumulator, J*metrics, sponge): in FP32 they are software-pipelined
   // one plane ahead, so the loads for plane k+1 are in flight while plane k is computed; in
   // FP64 (twice the registers) they are issued at the top of the plane, before the wait
   constexpr bool PIPE = sizeof(T) == 4;
-  PointIn<T, DIM> in;
-  if (PIPE && active) gather<T, DIM, COMP, TR>(s, lij + nxy * k0, in);
+  PointIn<T, DIM> inA, inB;
+  if (PIPE && active) gather<T, DIM, COMP, TR>(s, lij + nxy * (unsigned)k0, inA);
   int waited = plo;
-  for (int k = k0; k < k1; ++k) {
-    PointIn<T, DIM> in_next;
-    if (PIPE && active && k + 1 < k1) gather<T, DIM, COMP, TR>(s, lij + nxy * (k + 1), in_next);
-    if (!PIPE && active) gather<T, DIM, COMP, TR>(s, lij + nxy * k, in);
+  int sk = (k0 - plo) % NS;  // ring slot of plane k
+
+  // one plane: `cur` holds its gathered inputs, `nxt` receives those of the next plane
+  auto plane = [&](int k, PointIn<T, DIM>& cur, PointIn<T, DIM>& nxt) -> bool {
+    const unsigned lk = lij + nxy * (unsigned)k;
+    if (PIPE && active && k + 1 < k1) gather<T, DIM, COMP, TR>(s, lk + nxy, nxt);
+    if (!PIPE && active) gather<T, DIM, COMP, TR>(s, lk, cur);
     bool failed = false;
     const int need = DIM == 3 ? min(phi, k + H) : 0;
     for (; waited <= need; ++waited) {
@@ -153,12 +104,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
         atomicExch(P.err, 1);
         for (int w = waited; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NS], (unsigned)(((w - plo) / NS) & 1));
       }
-      return;
+      return false;
     }
     if (active) {
       // ring slots of planes k-H..k+H; planes outside [plo, phi] map to a loaded plane and
       // carry zero weight (their closure-class weights are zero)
-      const int sk = (k - plo) % NS;
       int zoff[2 * H + 1];
       T wz[2 * H + 1];
       if (DIM == 3) {
@@ -170,8 +120,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
           sl += sl < 0 ? NS : 0;
           sl -= sl >= NS ? NS : 0;
           zoff[o + H] = sl * PLANE + c;
-          wz[o + H] = P.w[cz][o + H];
         }
+#pragma unroll
+        for (int o = 0; o <= 2 * H; ++o) wz[o] = P.w[cz][o];
       }
       const T* pk = ring + sk * PLANE;
       T D[V][DIM], q[V];
@@ -194,11 +145,22 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
           D[v][DIM - 1] = dz;
         }
       }
-      rhs_update<T, DIM, COMP, TR>(s, lij + nxy * k, i, j, k, D, q, in);
+      rhs_update<T, DIM, COMP, TR>(s, lk, i, j, k, D, q, cur);
     }
-    if (PIPE) in = in_next;
     __syncthreads();
     if (DIM == 3 && tid == 0) issue_upto(k + 1 - H + NS - 1);
+    sk = sk + 1 == NS ? 0 : sk + 1;
+    return true;
+  };
+  if (PIPE) {
+    // planes in pairs, the two input sets alternating roles (no copies between them)
+    for (int k = k0; k < k1; k += 2) {
+      if (!plane(k, inA, inB)) return;
+      if (k + 1 < k1 && !plane(k + 1, inB, inA)) return;
+    }
+  } else {
+    for (int k = k0; k < k1; ++k)
+      if (!plane(k, inA, inA)) return;
   }
 }
 
@@ -373,19 +335,32 @@ cudaError_t go_stage(const FieldMaps& z, const TmaStageParams<T>& p, int tiles, 
   return cudaGetLastError();
 }
 
-// Traits are a run-time choice of the host (lee_point.cuh, kTr*) mapped onto instantiations.
+// Traits are a run-time choice of the host (kTr* and the stage kind) mapped onto instantiations.
+template <typename T, int DIM, bool COMP, int KIND>
+cudaError_t go_stage_layout(const FieldMaps& z, const TmaStageParams<T>& p, int tr, int tiles, int chunks,
+                            cudaStream_t s) {
+  constexpr int B = kTrTma | (KIND << kKindShift);
+  switch (tr & 7) {
+    case 0: return go_stage<T, DIM, COMP, B | 0>(z, p, tiles, chunks, s);
+    case 1: return go_stage<T, DIM, COMP, B | 1>(z, p, tiles, chunks, s);
+    case 2: return go_stage<T, DIM, COMP, B | 2>(z, p, tiles, chunks, s);
+    case 3: return go_stage<T, DIM, COMP, B | 3>(z, p, tiles, chunks, s);
+    case 4: return go_stage<T, DIM, COMP, B | 4>(z, p, tiles, chunks, s);
+    case 5: return go_stage<T, DIM, COMP, B | 5>(z, p, tiles, chunks, s);
+    case 6: return go_stage<T, DIM, COMP, B | 6>(z, p, tiles, chunks, s);
+    default: return go_stage<T, DIM, COMP, B | 7>(z, p, tiles, chunks, s);
+  }
+}
+
 template <typename T, int DIM, bool COMP>
 cudaError_t go_stage_tr(const FieldMaps& z, const TmaStageParams<T>& p, int tr, int tiles, int chunks,
                         cudaStream_t s) {
-  switch (tr & 7) {
-    case 0: return go_stage<T, DIM, COMP, 0>(z, p, tiles, chunks, s);
-    case 1: return go_stage<T, DIM, COMP, 1>(z, p, tiles, chunks, s);
-    case 2: return go_stage<T, DIM, COMP, 2>(z, p, tiles, chunks, s);
-    case 3: return go_stage<T, DIM, COMP, 3>(z, p, tiles, chunks, s);
-    case 4: return go_stage<T, DIM, COMP, 4>(z, p, tiles, chunks, s);
-    case 5: return go_stage<T, DIM, COMP, 5>(z, p, tiles, chunks, s);
-    case 6: return go_stage<T, DIM, COMP, 6>(z, p, tiles, chunks, s);
-    default: return go_stage<T, DIM, COMP, 7>(z, p, tiles, chunks, s);
+  switch ((tr >> kKindShift) & 7) {
+    case kKindRhs: return go_stage_layout<T, DIM, COMP, kKindRhs>(z, p, tr, tiles, chunks, s);
+    case kKindFirst: return go_stage_layout<T, DIM, COMP, kKindFirst>(z, p, tr, tiles, chunks, s);
+    case kKindMid: return go_stage_layout<T, DIM, COMP, kKindMid>(z, p, tr, tiles, chunks, s);
+    case kKindLast: return go_stage_layout<T, DIM, COMP, kKindLast>(z, p, tr, tiles, chunks, s);
+    default: return go_stage_layout<T, DIM, COMP, kKindRuntime>(z, p, tr, tiles, chunks, s);
   }
 }
 

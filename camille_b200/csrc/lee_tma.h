@@ -67,5 +67,10 @@ cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, i
 template <typename T>
 cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
                               int chunks, cudaStream_t s);
+// The vectorised fused filter (lee_filter.cu): its TMA box (bx x by) and tile (tx x ty).
+void filter_vec_box(size_t esz, int hf, int* bx, int* by, int* tx, int* ty);
+template <typename T>
+cudaError_t launch_filter_vec(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int tiles, int chunks,
+                              cudaStream_t s);
 
 }  // namespace lee
