@@ -47,7 +47,7 @@ class LeeInfo(C.Structure):
                 ("num_coef_fields", C.c_int), ("device_bytes", C.c_longlong),
                 ("tma_stage", C.c_int), ("tma_filter", C.c_int), ("stage_chunk", C.c_int),
                 ("filter_chunk", C.c_int), ("batched", C.c_int), ("batch_stage_tile", C.c_int * 2),
-                ("batch_filter_tile", C.c_int * 2)]
+                ("batch_filter_tile", C.c_int * 2), ("filter_kernel", C.c_int), ("stage_kernel", C.c_int)]
 
 
 class LeeStats(C.Structure):
@@ -97,6 +97,8 @@ SIGNATURES = {
     "set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "get_stats": (C.c_int, [C.c_void_p, C.POINTER(LeeStats)]),
     "set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_filter_kernel": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_stage_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "set_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _LP, C.c_double]),
     "eval_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _DP]),
     "apply_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
@@ -145,9 +147,12 @@ class Solver:
     """A context loaded with one Case: grids, means, boundaries, source and state."""
 
     def __init__(self, lib: Library, case: "_cases.Case", precision: int = FP64, device: int = 0,
-                 upload: bool = True, overset_file: Optional[str] = None):
+                 upload: bool = True, overset_file: Optional[str] = None, filter_kernel: int = -1,
+                 stage_kernel: int = -1):
         """``overset_file``: read the case's overset maps from this Overture-format file
-        (lee_read_overset_file) instead of passing the arrays (lee_set_overset)."""
+        (lee_read_overset_file) instead of passing the arrays (lee_set_overset).
+        ``filter_kernel``: lee_set_filter_kernel (-1/0 scalar, 2/4 vector width);
+        ``stage_kernel``: lee_set_stage_kernel (-1 default, 1 or 2 points per thread)."""
         self.lib = lib
         self.case = case
         self.ctx = C.c_void_p()
@@ -196,6 +201,10 @@ class Solver:
                 ip = [a.ctypes.data_as(_IP) for a in arrs]
                 self._chk(lib.set_overset(self.ctx, o.num_receivers, ip[0], ip[1], ip[2], ip[3], ip[4], _dptr(w),
                                           int(o.hole_block.size), ip[5], ip[6]))
+            if filter_kernel != -1:
+                self._chk(lib.set_filter_kernel(self.ctx, filter_kernel))
+            if stage_kernel != -1:
+                self._chk(lib.set_stage_kernel(self.ctx, stage_kernel))
             self._chk(lib.prepare(self.ctx))
             if case.microphones is not None:
                 mic = np.ascontiguousarray(case.microphones.l0, np.int64)

@@ -29,6 +29,8 @@ UNITS = {
     "lee_bc.cu": [],
     "lee_adjoint.cu": [],
     "lee_batch.cu": [],
+    "lee_filter.cu": [],
+    "lee_stage_pair.cu": [],
 }
 
 

@@ -85,8 +85,11 @@ struct BlockData {
   bool rho_valid = false;   // false until a step or a filter call has written it
   // TMA-staged kernels (blocks without holes, 4th-order difference)
   bool tma = false, tma_filter = false;
-  bool filter_vec = false;           // the fused filter runs the vectorised kernel (lee_filter.cu)
-  int vtiles_x = 0, vtiles_y = 0;    // its tiles
+  bool filter_vec = false;           // the vectorised fused filter (lee_filter.cu) applies
+  int filter_px = 0;                 // the fused filter's kernel: 0 scalar, else the vector group width
+  int stage_px = 1;                  // points per thread of the TMA stage kernel (2: lee_stage_pair.cu)
+  bool stage_pair = false;           // the two-point stage kernel applies
+  int vtiles_x = 0, vtiles_y = 0;    // tiles of the vectorised kernel at that width
   int traits = kTrGeneric;          // coefficient-layout traits of the TMA stage kernel
   void* d_sigma_field = nullptr;    // summed sponge strengths per point (working precision)
   int tiles_x = 0, tiles_y = 0;
@@ -144,6 +147,8 @@ struct lee_ctx {
   int hf = 0;
   bool wst_ok = false, wfl_ok = false;
   bool wfl_sym = false;  // symmetric interior filter stencil: the vectorised filter kernel applies
+  int filter_kernel = -1;  // lee_set_filter_kernel: -1/0 scalar, else vector group width
+  int stage_kernel = -1;   // lee_set_stage_kernel: -1 default, else points per thread
   int* d_err = nullptr;
   double* d_report = nullptr;  // -min and max of the five state slots (lee_state_minmax)
   // overset maps (host copies, then device arrays from lee_prepare)
@@ -822,6 +827,15 @@ int filter_box(const lee_ctx* c, int* bx, int* by) {
   return LEE_OK;
 }
 
+// Tiles of the vectorised filter at the block's group width.
+void set_filter_tiles(const lee_ctx* c, BlockData& b) {
+  if (b.filter_px <= 0) return;
+  int bx, by, tx, ty;
+  filter_vec_box(c->esz, c->hf, b.filter_px, &bx, &by, &tx, &ty);
+  b.vtiles_x = (b.nx + tx - 1) / tx;
+  b.vtiles_y = (b.ny + ty - 1) / ty;
+}
+
 template <typename T>
 int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* const* zin, int chunk_override = 0) {
   if (!b.tma) {
@@ -845,7 +859,14 @@ int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* co
   const int kind = p.stage < 0 ? kKindRhs
                    : p.stage == 0 ? (p.last ? kKindRuntime : kKindFirst)
                                   : (p.last ? kKindLast : kKindMid);
-  CK(launch_stage_tma<T>(fm, tp, b.traits | (kind << kKindShift), b.tiles_x * b.tiles_y, chunks, c->stream));
+  const int tr = b.traits | (kind << kKindShift);
+  if constexpr (sizeof(T) == 4) {
+    if (b.stage_px == 2 && stage_pair_applies(tr, b.nx)) {
+      CK(launch_stage_pair(fm, tp, tr, b.tiles_x * b.tiles_y, chunks, c->stream));
+      return LEE_OK;
+    }
+  }
+  CK(launch_stage_tma<T>(fm, tp, tr, b.tiles_x * b.tiles_y, chunks, c->stream));
   return LEE_OK;
 }
 
@@ -869,8 +890,8 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
   }
   fp.errflag = c->d_err;
   int bx, by, tx, ty;
-  if (b.filter_vec) {
-    filter_vec_box(c->esz, c->hf, &bx, &by, &tx, &ty);
+  if (b.filter_px > 0) {
+    filter_vec_box(c->esz, c->hf, b.filter_px, &bx, &by, &tx, &ty);
     fp.tiles_x = b.vtiles_x;
   } else {
     filter_box(c, &bx, &by);
@@ -880,8 +901,8 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
   if (rc) return rc;
   const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
   int e0 = mark(c);
-  if (b.filter_vec)
-    CK(launch_filter_vec<T>(fm, fp, c->hf, c->cfg.num_dim, b.vtiles_x * b.vtiles_y, chunks, c->stream));
+  if (b.filter_px > 0)
+    CK(launch_filter_vec<T>(fm, fp, c->hf, b.filter_px, c->cfg.num_dim, b.vtiles_x * b.vtiles_y, chunks, c->stream));
   else
     CK(launch_filter_tma<T>(fm, fp, c->hf, c->cfg.num_dim, c->comp ? 1 : 0, b.tiles_x * b.tiles_y, chunks, c->stream));
   int e1 = mark(c);
@@ -898,57 +919,81 @@ int check_device_error(lee_ctx* c);
 // halo planes. Runs at setup on the (not yet uploaded) state buffers.
 template <typename T>
 int autotune(lee_ctx* c, BlockData& b) {
-  if (c->cfg.num_dim != 3 || (!b.tma && !b.tma_filter)) return LEE_OK;
-  const int cands[] = {8, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+  if (!b.tma && !b.tma_filter) return LEE_OK;
+  const bool d3 = c->cfg.num_dim == 3;
+  const int cands3[] = {8, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+  const int cands2[] = {1};
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   const bool saved = c->timing;
   c->timing = false;
+  // the kernels are fixed at this point (lee_set_stage_kernel, lee_set_filter_kernel or the
+  // defaults); only the plane chunk, which leaves the arithmetic unchanged, is timed
+  const int kinds[1] = {b.filter_px}, nkinds = 1;
+  const int skinds[1] = {b.stage_px}, nskinds = 1;
   for (int which = 0; which < 2; ++which) {
     if ((which == 0 && !b.tma) || (which == 1 && !b.tma_filter)) continue;
+    if (which == 0 && !d3 && nskinds == 1) continue;  // nothing to choose
     float best = 1e30f;
-    int best_chunk = b.nz;
-    for (int ch : cands) {
-      if (ch > b.nz) continue;
-      float tsum = 0.f;
-      for (int rep = 0; rep < 3; ++rep) {
-        CK(cudaEventRecord(e0, c->stream));
-        int rc;
-        if (which == 0) {
-          StageParams<T> p;
-          fill_stage_common<T>(c, b, p);
-          p.stage = 1;
-          p.last = 0;
-          p.h = (T)1e-3;
-          p.b = (T)(1.0 / 3.0);
-          p.a = (T)0.5;
-          for (int v = 0; v < c->V; ++v) {
-            p.zin[v] = (const T*)b.zb[0][v];
-            p.yn[v] = (const T*)b.y[v];
-            p.acc[v] = (T*)b.acc[v];
-            p.zout[v] = (T*)b.zb[1][v];
-            p.comp[v] = (T*)b.comp[v];
-          }
-          rc = launch_stage_any<T>(c, b, p, b.zb[0], ch);
-        } else {
-          rc = c->comp ? launch_filter_fused<T>(c, b, b.zb[1], b.acc, b.zb[0], b.comp, ch)
-                       : launch_filter_fused<T>(c, b, b.acc, nullptr, b.zb[0], nullptr, ch);
-        }
-        if (rc) return rc;
-        CK(cudaEventRecord(e1, c->stream));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        if (rep > 0) tsum += ms;
+    int best_chunk = b.nz, best_kind = which == 0 ? b.stage_px : b.filter_px;
+    for (int kq = 0; kq < (which == 1 ? nkinds : nskinds); ++kq) {
+      if (which == 0) {
+        b.stage_px = skinds[kq];
+      } else {
+        b.filter_px = kinds[kq];
+        set_filter_tiles(c, b);
       }
-      if (tsum < best) {
-        best = tsum;
-        best_chunk = ch;
+      for (int ch : (d3 ? std::vector<int>(std::begin(cands3), std::end(cands3))
+                        : std::vector<int>(std::begin(cands2), std::end(cands2)))) {
+        if (d3 && ch > b.nz) continue;
+        float tsum = 0.f;
+        for (int rep = 0; rep < 3; ++rep) {
+          CK(cudaEventRecord(e0, c->stream));
+          int rc;
+          if (which == 0) {
+            StageParams<T> p;
+            fill_stage_common<T>(c, b, p);
+            p.stage = 1;
+            p.last = 0;
+            p.h = (T)1e-3;
+            p.b = (T)(1.0 / 3.0);
+            p.a = (T)0.5;
+            for (int v = 0; v < c->V; ++v) {
+              p.zin[v] = (const T*)b.zb[0][v];
+              p.yn[v] = (const T*)b.y[v];
+              p.acc[v] = (T*)b.acc[v];
+              p.zout[v] = (T*)b.zb[1][v];
+              p.comp[v] = (T*)b.comp[v];
+            }
+            rc = launch_stage_any<T>(c, b, p, b.zb[0], d3 ? ch : 0);
+          } else {
+            const int chunk = d3 ? ch : 0;
+            rc = c->comp ? launch_filter_fused<T>(c, b, b.zb[1], b.acc, b.zb[0], b.comp, chunk)
+                         : launch_filter_fused<T>(c, b, b.acc, nullptr, b.zb[0], nullptr, chunk);
+          }
+          if (rc) return rc;
+          CK(cudaEventRecord(e1, c->stream));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          if (rep > 0) tsum += ms;
+        }
+        if (tsum < best) {
+          best = tsum;
+          best_chunk = d3 ? ch : b.nz;
+          best_kind = which == 0 ? b.stage_px : b.filter_px;
+        }
       }
     }
-    if (which == 0) b.stage_chunk = best_chunk;
-    else b.filter_chunk = best_chunk;
+    if (which == 0) {
+      b.stage_chunk = best_chunk;
+      b.stage_px = best_kind;
+    } else {
+      b.filter_chunk = best_chunk;
+      b.filter_px = best_kind;
+      set_filter_tiles(c, b);
+    }
   }
   c->timing = saved;
   c->stats = lee_stats{};
@@ -2414,13 +2459,21 @@ int lee_prepare(lee_ctx* c) {
     // (the TMA stage kernel addresses points with 32-bit offsets)
     b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32);
     b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE;
+    // the kernels are a fixed choice (they round differently, and two contexts of one case give
+    // the same bits): the scalar fused filter unless another is asked for
     b.filter_vec = b.tma_filter && c->wfl_sym;
-    if (b.filter_vec) {
-      int bx, by, tx, ty;
-      filter_vec_box(c->esz, c->hf, &bx, &by, &tx, &ty);
-      b.vtiles_x = (b.nx + tx - 1) / tx;
-      b.vtiles_y = (b.ny + ty - 1) / ty;
+    b.filter_px = 0;
+    if (c->filter_kernel >= 0 && b.tma_filter) {
+      int px[2];
+      const int n = filter_vec_widths(c->esz, px);
+      bool ok = c->filter_kernel == 0;
+      for (int q = 0; q < n; ++q) ok |= b.filter_vec && c->filter_kernel == px[q];
+      if (!ok)
+        return fail(c, LEE_ERR_UNSUPPORTED, "filter kernel %d is not available for block %d", c->filter_kernel,
+                    (int)(&b - c->blk.data()));
+      b.filter_px = c->filter_kernel;
     }
+    set_filter_tiles(c, b);
     if (b.tma) {
       // coefficient-layout traits of the stage kernel
       bool jmf = false, uni = true, spg = false;
@@ -2435,6 +2488,14 @@ int lee_prepare(lee_ctx* c) {
       uni &= is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi) && !b.need_rho;
       for (auto& z : b.bnd) spg |= z.kind == LEE_SPONGE_FREUND_AMBIENT;
       b.traits = kTrTma | (jmf ? kTrJmField : 0) | (uni ? kTrUniform : 0) | (spg ? kTrSponge : 0);
+      b.stage_pair = c->comp && uni && b.nx % 2 == 0;
+      b.stage_px = b.stage_pair ? 2 : 1;
+      if (c->stage_kernel > 0) {
+        if (c->stage_kernel != 1 && !(c->stage_kernel == 2 && b.stage_pair))
+          return fail(c, LEE_ERR_UNSUPPORTED, "stage kernel %d is not available for block %d", c->stage_kernel,
+                      (int)(&b - c->blk.data()));
+        b.stage_px = c->stage_kernel;
+      }
       if (spg && (rc = build_sigma_field(c, b))) return rc;
       if (jmf) {
         // the TMA kernel reads every J*metrics entry as a field when one is: constant entries
@@ -2820,6 +2881,8 @@ int lee_get_info(lee_ctx* c, lee_info* info) {
   }
   info->stage_chunk = c->blk.empty() ? 0 : c->blk[0].stage_chunk;
   info->filter_chunk = c->blk.empty() ? 0 : c->blk[0].filter_chunk;
+  info->filter_kernel = c->blk.empty() ? 0 : c->blk[0].filter_px;
+  info->stage_kernel = c->blk.empty() ? 0 : c->blk[0].stage_px;
   info->batched = c->batch.active ? 1 : 0;
   if (c->batch.active) {
     batch_shape(c->batch.sshape, &info->batch_stage_tile[0], &info->batch_stage_tile[1]);
@@ -3107,6 +3170,22 @@ int lee_set_batch_shapes(lee_ctx* c, int stage_shape, int filter_shape) {
     cudaGraphExecDestroy(c->graph.exec);
     c->graph.exec = nullptr;
   }
+  return LEE_OK;
+}
+
+int lee_set_stage_kernel(lee_ctx* c, int kind) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_stage_kernel before lee_prepare");
+  if (kind != -1 && kind != 1 && kind != 2) return fail(c, LEE_ERR_ARG, "stage kernel %d", kind);
+  c->stage_kernel = kind;
+  return LEE_OK;
+}
+
+int lee_set_filter_kernel(lee_ctx* c, int kind) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_filter_kernel before lee_prepare");
+  if (kind < -1) return fail(c, LEE_ERR_ARG, "filter kernel %d", kind);
+  c->filter_kernel = kind;
   return LEE_OK;
 }
 

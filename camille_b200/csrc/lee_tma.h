@@ -67,10 +67,18 @@ cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, i
 template <typename T>
 cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
                               int chunks, cudaStream_t s);
-// The vectorised fused filter (lee_filter.cu): its TMA box (bx x by) and tile (tx x ty).
-void filter_vec_box(size_t esz, int hf, int* bx, int* by, int* tx, int* ty);
-template <typename T>
-cudaError_t launch_filter_vec(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int tiles, int chunks,
+// The FP32 stage kernel with two points per thread (lee_stage_pair.cu): compensated form,
+// uniform mean flow, TMA blocks of even width, a fixed stage kind.
+bool stage_pair_applies(int traits, int nx);
+cudaError_t launch_stage_pair(const FieldMaps& zin, const TmaStageParams<float>& p, int traits, int tiles, int chunks,
                               cudaStream_t s);
+
+// The vectorised fused filter (lee_filter.cu): the group widths (points per thread) it offers for
+// an element size, its TMA box (bx x by) and tile (tx x ty) for one width, and the launch.
+int filter_vec_widths(size_t esz, int* px);
+void filter_vec_box(size_t esz, int hf, int px, int* bx, int* by, int* tx, int* ty);
+template <typename T>
+cudaError_t launch_filter_vec(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int px, int dim, int tiles,
+                              int chunks, cudaStream_t s);
 
 }  // namespace lee

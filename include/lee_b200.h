@@ -218,6 +218,8 @@ typedef struct {
   int batched;               /* 1 when the blocks run through the batched kernels */
   int batch_stage_tile[2];   /* tile (xi, eta points) of the batched stage and filter launches, */
   int batch_filter_tile[2];  /* picked by timing the candidates at lee_prepare */
+  int filter_kernel;         /* fused filter of block 0: 0 scalar, else the vector group width */
+  int stage_kernel;          /* TMA stage kernel of block 0: points per thread */
 } lee_info;
 int lee_get_info(lee_ctx *ctx, lee_info *info);
 
@@ -237,6 +239,17 @@ int lee_set_timing(lee_ctx *ctx, int on);
  * group of steps. Off, or while kernel timing is on, every launch is issued on its own. The
  * results are the same either way. */
 int lee_set_graphs(lee_ctx *ctx, int on);
+/* Kernel of the fused filter (no reference counterpart; results agree to rounding): -1 or 0
+ * (default) the scalar kernel, 2 or 4 the kernel that gives each thread that many neighbouring
+ * points along xi (4: FP32 only). LEE_ERR_UNSUPPORTED from lee_prepare when a block cannot run the
+ * choice. Call before lee_prepare. */
+int lee_set_filter_kernel(lee_ctx *ctx, int kind);
+/* Kernel of the RK stages on blocks that run the TMA stage kernel (no reference counterpart;
+ * results agree to rounding): 1 one point per thread, 2 two neighbouring points per thread with
+ * packed FP32 arithmetic (compensated form, uniform mean flow, even nxi); -1 (default) takes 2
+ * where it applies, else 1. LEE_ERR_UNSUPPORTED from lee_prepare when a block cannot run the
+ * choice. Call before lee_prepare. */
+int lee_set_stage_kernel(lee_ctx *ctx, int kind);
 
 /* ---- discrete adjoint (no reference counterpart: the reference has no adjoint) ----------
  * The step map of lee_advance is linear in the state; these entry points apply its exact

@@ -1254,6 +1254,18 @@ int orc_set_batch_shapes(orc_ctx *c, int stage_shape, int filter_shape) {
   return fail(c, LEE_ERR_STATE, "the oracle has no batched kernels");
 }
 
+int orc_set_stage_kernel(orc_ctx *c, int kind) {
+  (void)c;
+  (void)kind;
+  return LEE_OK; /* one stage path */
+}
+
+int orc_set_filter_kernel(orc_ctx *c, int kind) {
+  (void)c;
+  (void)kind;
+  return LEE_OK; /* one filter path */
+}
+
 int orc_set_graphs(orc_ctx *c, int on) {
   (void)c; (void)on;
   return LEE_OK;

@@ -113,6 +113,71 @@ def test_fp32_compensated_error_vs_oracle(product_lib, oracle_lib, label):
     assert err <= 1e-5, err
 
 
+def _wide():
+    a = cases.curvi3d(n=136, nsteps=1, halfwidth=6.0, sponge=8)
+    b = cases.curvi3d(n=72, nsteps=1, halfwidth=4.0)
+    b.fd_scheme, b.filter_scheme, b.filter_strength = "FDO11P", "SFO11P", 0.3
+    c = cases.pulse2d(n=520, length=519 * 100.0 / 255.0, sponge=20, nsteps=1)
+    d = cases.curvi3d(n=68, nsteps=1, halfwidth=4.0)
+    d.filter_order, d.filter_blend = 4, 0.7
+    return {"curvi3d_136": a, "sfo11p_3d_72": b, "pulse2d_520": c, "filter4_3d_68": d}
+
+
+def _uniform_cases():
+    a = cases.pulse2d(n=128, length=127 * 100.0 / 255.0, sponge=20, nsteps=40)
+    a.monopole = (3.0, -2.0, 0.0, 1e-3, 0.5, 3.0, 20.0)
+    b = cases.curvi3d(n=40, nsteps=12, halfwidth=3.0)
+    c = cases.curvi3d(n=44, nsteps=10, halfwidth=3.0, sponge=4)
+    c.monopole = (20.0, 22.0, 21.0, 1e-3, 0.7, 2.5, 0.0)
+    c.rk = "RUNGE_KUTTA2"
+    return {"pulse2d_128_monopole": a, "curvi3d_40": b, "curvi3d_44_sponge_monopole_rk2": c}
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("label", list(_uniform_cases().keys()))
+def test_stage_kernels_fp32_compensated(product_lib, oracle_lib, label, kernel):
+    """Both TMA stage kernels of the compensated form (one point per thread; two, in packed
+    FP32): the right-hand side against the oracle within 1e-6, and the steps within 1e-5 in p'."""
+    case = _uniform_cases()[label]
+    o = api.Solver(oracle_lib, case)
+    dt = o.compute_dt()
+    p = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED, stage_kernel=kernel)
+    assert p.info().stage_kernel == kernel
+    assert rl2(p.eval_rhs(0, 0.7), o.eval_rhs(0, 0.7)) <= 1e-6
+    o.advance(case.nsteps, dt)
+    p.advance(case.nsteps, dt)
+    err = rl2(p.download(0)[0][4], o.download(0)[0][4])
+    assert err <= 1e-5, err
+
+
+_ORACLE_FILTERED = {}
+
+
+def _oracle_filtered(oracle_lib, label):
+    if label not in _ORACLE_FILTERED:
+        o = api.Solver(oracle_lib, _wide()[label])
+        o.apply_filter()
+        _ORACLE_FILTERED[label] = o.download(0)[0]
+    return _ORACLE_FILTERED[label]
+
+
+@pytest.mark.parametrize("kernel", [0, 2, 4])
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+@pytest.mark.parametrize("label", list(_wide().keys()))
+def test_filter_across_tiles(product_lib, oracle_lib, label, precision, kernel):
+    """Blocks several filter tiles wide and tall (vector tiles of 32 groups along xi, 8 rows,
+    chunks of planes), with the OA8, OA4 and SFO11P filters, on every fused-filter kernel (scalar;
+    groups of 2 or 4 points): the fused filter against the oracle, FP64 within 1e-13 and the
+    compensated form within 1e-6 (one FP32 rounding)."""
+    if precision == api.FP64 and kernel == 4:
+        pytest.skip("FP64 groups hold 2 points")
+    case = _wide()[label]
+    p = api.Solver(product_lib, case, precision=precision, filter_kernel=kernel)
+    p.apply_filter()
+    tol = 1e-13 if precision == api.FP64 else 1e-6
+    assert rl2(p.download(0)[0], _oracle_filtered(oracle_lib, label)) <= tol
+
+
 @pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
 def test_rho_ratio_follows_the_pre_filter_state(product_lib, oracle_lib, precision):
     """With a sheared mean the right-hand side reads rho'/rho_bar, which the reference
