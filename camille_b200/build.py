@@ -31,6 +31,7 @@ UNITS = {
     "lee_batch.cu": [],
     "lee_filter.cu": [],
     "lee_stage_pair.cu": [],
+    "lee_adjoint_tma.cu": [],
 }
 
 

@@ -151,6 +151,7 @@ struct lee_ctx {
   int stage_kernel = -1;   // lee_set_stage_kernel: -1 default, else points per thread
   int* d_err = nullptr;
   double* d_report = nullptr;  // -min and max of the five state slots (lee_state_minmax)
+  double* d_staging = nullptr;  // FP64 field of compensated uploads and downloads
   // overset maps (host copies, then device arrays from lee_prepare)
   struct {
     int n = 0, W = 1, w[3] = {1, 1, 1};
@@ -205,6 +206,8 @@ struct lee_ctx {
     double* d_gbar = nullptr;              // gradient of the distributed source's box field
     std::vector<void*> ckpt;               // checkpoints: V (+ V carried errors) fields each
     size_t ckpt_slots = 0;
+    bool tma = false;                      // the plane-marching stage kernel (lee_adjoint_tma.cu)
+    bool tma_jm = false;                   // ... with J*metrics fields (else constants)
   } adj;
 };
 
@@ -792,12 +795,12 @@ int ensure_encoder(lee_ctx* c) {
   return LEE_OK;
 }
 
-// Tensor maps (box bx x by x 1) of the V fields of a buffer, cached per device pointer.
-int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int by, FieldMaps* out) {
+// Tensor maps (box bx x by x 1) of n fields of a block, cached per device pointer.
+int encode_maps(lee_ctx* c, const BlockData& b, const void* const* fields, int n, int bx, int by, CUtensorMap* out) {
   int rc = ensure_encoder(c);
   if (rc) return rc;
-  for (int v = 0; v < c->V; ++v) {
-    MapKey key{fields[v], bx, by};
+  for (int v = 0; v < n; ++v) {
+    MapKey key{const_cast<void*>(fields[v]), bx, by};
     auto it = c->tmaps.find(key);
     if (it == c->tmaps.end()) {
       CUtensorMap m;
@@ -806,7 +809,7 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
       cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
       cuuint32_t es[3] = {1, 1, 1};
       CUresult r = c->encode(&m, c->esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
-                             fields[v], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             const_cast<void*>(fields[v]), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS) return fail(c, LEE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -814,9 +817,14 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
       memcpy(mb.b, &m, sizeof m);
       it = c->tmaps.emplace(key, mb).first;
     }
-    memcpy(&out->m[v], it->second.b, sizeof(CUtensorMap));
+    memcpy(&out[v], it->second.b, sizeof(CUtensorMap));
   }
   return LEE_OK;
+}
+
+// Tensor maps of the V fields of a buffer.
+int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int by, FieldMaps* out) {
+  return encode_maps(c, b, const_cast<const void* const*>(fields), c->V, bx, by, out->m);
 }
 
 int filter_box(const lee_ctx* c, int* bx, int* by) {
@@ -1796,6 +1804,15 @@ int adjoint_setup(lee_ctx* c) {
   if (c->cfg.filter_scheme != LEE_FILTER_NONE) need = std::max(need, std::max(2 * a.fT.E, a.fT.E + a.fT.H + c->flt.h));
   for (int d = 0; d < c->cfg.num_dim; ++d)
     if (n[d] < need) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint needs %d points per direction", need);
+  // the plane-marching stage kernel: 3-D, transposed stencils within two points, rows of 16-byte
+  // multiples, 32-bit point offsets, J*metrics all fields or all constants
+  {
+    int nf = 0;
+    for (int q = 0; q < 9; ++q) nf += (c->comp ? (const void*)b.cf_jm[q].p : (const void*)b.cd_jm[q].p) != nullptr;
+    a.tma = c->cfg.num_dim == 3 && a.dT.H == 2 && ((size_t)b.nx * c->esz) % 16 == 0 &&
+            (unsigned long long)b.N < (1ull << 32) && (nf == 0 || nf == 9);
+    a.tma_jm = nf == 9;
+  }
   int rc;
   if ((rc = alloc_fields(c, a.lam, b.N)) || (rc = alloc_fields(c, a.mu, b.N)) || (rc = alloc_fields(c, a.kb[0], b.N)) ||
       (rc = alloc_fields(c, a.kb[1], b.N)) || (rc = alloc_fields(c, a.ybar, b.N)))
@@ -1871,7 +1888,26 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
       p.ybar[v] = (T*)a.ybar[v];
       p.kout[v] = (T*)a.kb[1 - cur][v];
     }
-    CK(launch_adj_stage<T>(p, c->cfg.num_dim, c->stream));
+    if (a.tma) {
+      // the plane-marching kernel: maps of w (this stage's input) and the J*metrics fields
+      AdjMaps am;
+      int bx, by, tx, ty;
+      adj_tma_box(c->esz, &bx, &by, &tx, &ty);
+      const void* f[14];
+      for (int v = 0; v < 5; ++v) f[v] = p.kin[v];
+      for (int q = 0; q < 9; ++q) f[5 + q] = p.jm[q].p;
+      int rc = encode_maps(c, b, f, a.tma_jm ? 14 : 5, bx, by, am.m);
+      if (rc) return rc;
+      AdjTmaParams<T> tp;
+      tp.a = p;
+      tp.tiles_x = (b.nx + tx - 1) / tx;
+      tp.k_chunk = std::min(b.nz, 32);
+      tp.err = c->d_err;
+      const int tiles = tp.tiles_x * ((b.ny + ty - 1) / ty);
+      CK(launch_adj_tma<T>(am, tp, a.tma_jm, tiles, (b.nz + tp.k_chunk - 1) / tp.k_chunk, c->stream));
+    } else {
+      CK(launch_adj_stage<T>(p, c->cfg.num_dim, c->stream));
+    }
     c->stats.kernel_launches += 1;
     if (!p.first) cur = 1 - cur;
     else cur = 1;  // the first processed stage wrote kb[1]
@@ -2560,6 +2596,23 @@ int lee_prepare(lee_ctx* c) {
   return LEE_OK;
 }
 
+namespace {
+
+// FP64 staging field of the compensated form's uploads, downloads and right-hand sides, as large
+// as the largest block; allocated once, on first use.
+int staging(lee_ctx* c, double** out) {
+  if (!c->d_staging) {
+    long long n = 0;
+    for (const auto& b : c->blk) n = std::max(n, b.N);
+    const int rc = dalloc(c, &c->d_staging, (size_t)n);
+    if (rc) return rc;
+  }
+  *out = c->d_staging;
+  return LEE_OK;
+}
+
+}  // namespace
+
 int lee_upload_state(lee_ctx* c, int b, const double* const sol[5], int step, double time) {
   if (!c) return LEE_ERR_ARG;
   if (!c->prepared) return fail(c, LEE_ERR_STATE, "lee_prepare first");
@@ -2569,21 +2622,21 @@ int lee_upload_state(lee_ctx* c, int b, const double* const sol[5], int step, do
   if (c->cfg.num_dim == 2)
     for (long long l = 0; l < bk.N; ++l)
       if (sol[3][l] != 0.0) return fail(c, LEE_ERR_ARG, "2-D state must have w' = 0");
-  int rc;
   double* tmp = nullptr;
-  CK(cudaMallocAsync((void**)&tmp, (size_t)bk.N * 8, c->stream));
+  if (c->comp) {
+    const int rc = staging(c, &tmp);
+    if (rc) return rc;
+  }
   for (int v = 0; v < c->V; ++v) {
-    CK(cudaMemcpyAsync(tmp, sol[slot_of(c->V, v)], (size_t)bk.N * 8, cudaMemcpyHostToDevice, c->stream));
     if (!c->comp) {
-      CK(cudaMemcpyAsync(bk.y[v], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(bk.y[v], sol[slot_of(c->V, v)], (size_t)bk.N * 8, cudaMemcpyHostToDevice, c->stream));
     } else {
+      CK(cudaMemcpyAsync(tmp, sol[slot_of(c->V, v)], (size_t)bk.N * 8, cudaMemcpyHostToDevice, c->stream));
       k_split<<<grid1d(bk.N), 256, 0, c->stream>>>(bk.N, (float*)bk.y[v], (float*)bk.comp[v], tmp);
       CK(cudaGetLastError());
     }
   }
-  CK(cudaFreeAsync(tmp, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  (void)rc;
   bk.rho_valid = false;  // the first stage takes rho'/rho_bar from the uploaded state
   bk.step = step;
   bk.time = time;
@@ -2600,7 +2653,10 @@ int lee_download_state(lee_ctx* c, int b, double* const sol[5], int* step, doubl
   BlockData& bk = c->blk[(size_t)b];
   CK(cudaSetDevice(c->cfg.device));
   double* tmp = nullptr;
-  CK(cudaMallocAsync((void**)&tmp, (size_t)bk.N * 8, c->stream));
+  if (c->comp) {
+    const int rc = staging(c, &tmp);
+    if (rc) return rc;
+  }
   for (int v = 0; v < c->V; ++v) {
     if (!c->comp) {
       CK(cudaMemcpyAsync(sol[slot_of(c->V, v)], bk.y[v], (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -2611,7 +2667,6 @@ int lee_download_state(lee_ctx* c, int b, double* const sol[5], int* step, doubl
       CK(cudaMemcpyAsync(sol[slot_of(c->V, v)], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
     }
   }
-  CK(cudaFreeAsync(tmp, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (c->cfg.num_dim == 2) memset(sol[3], 0, (size_t)bk.N * 8);
   if (step) *step = bk.step;
@@ -2790,7 +2845,10 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
   CK(cudaSetDevice(c->cfg.device));
   BlockData& bk = c->blk[(size_t)b];
   double* tmp = nullptr;
-  CK(cudaMallocAsync((void**)&tmp, (size_t)bk.N * 8, c->stream));
+  {
+    const int rc = staging(c, &tmp);
+    if (rc) return rc;
+  }
   if (!c->comp) {
     StageParams<double> p;
     fill_stage_common<double>(c, bk, p);
@@ -2822,7 +2880,6 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
       CK(cudaMemcpyAsync(rhs[slot_of(c->V, v)], tmp, (size_t)bk.N * 8, cudaMemcpyDeviceToHost, c->stream));
     }
   }
-  CK(cudaFreeAsync(tmp, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (c->cfg.num_dim == 2) memset(rhs[3], 0, (size_t)bk.N * 8);
   return LEE_OK;

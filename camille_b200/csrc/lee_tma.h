@@ -67,6 +67,22 @@ cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, i
 template <typename T>
 cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
                               int chunks, cudaStream_t s);
+// The plane-marching adjoint stage (lee_adjoint_tma.cu): tensor maps of w (5 fields) then the
+// nine J*metrics fields, and its parameters.
+struct __align__(64) AdjMaps {
+  CUtensorMap m[14];
+};
+template <typename T>
+struct AdjTmaParams {
+  AdjStageParams<T> a;
+  int tiles_x, k_chunk;
+  int* err;  // set when a bounded wait gives up
+};
+void adj_tma_box(size_t esz, int* bx, int* by, int* tx, int* ty);
+template <typename T>
+cudaError_t launch_adj_tma(const AdjMaps& m, const AdjTmaParams<T>& p, bool jm_fields, int tiles, int chunks,
+                           cudaStream_t s);
+
 // The FP32 stage kernel with two points per thread (lee_stage_pair.cu): compensated form,
 // uniform mean flow, TMA blocks of even width, a fixed stage kind.
 bool stage_pair_applies(int traits, int nx);
