@@ -208,6 +208,7 @@ struct lee_ctx {
     size_t ckpt_slots = 0;
     bool tma = false;                      // the plane-marching stage kernel (lee_adjoint_tma.cu)
     bool tma_jm = false;                   // ... with J*metrics fields (else constants)
+    bool fused_filter = false;             // F^T by the fused filter kernel (lee_tma.cu)
   } adj;
 };
 
@@ -888,6 +889,7 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
   fp.V = c->V;
   fp.tiles_x = b.tiles_x;
   fp.k_chunk = chunk_override ? chunk_override : b.filter_chunk;
+  fp.nb = c->hf;
   for (int a = 0; a < 11; ++a)
     for (int o = 0; o < 11; ++o) fp.w[a][o] = (T)c->wfl[a][o];
   fp.blend = (T)c->cfg.filter_blend;
@@ -1812,6 +1814,11 @@ int adjoint_setup(lee_ctx* c) {
     a.tma = c->cfg.num_dim == 3 && a.dT.H == 2 && ((size_t)b.nx * c->esz) % 16 == 0 &&
             (unsigned long long)b.N < (1ull << 32) && (nf == 0 || nf == 9);
     a.tma_jm = nf == 9;
+    // the transposed filter through the fused filter kernel: its instantiated widths, rows of
+    // 16-byte multiples (the TMA box), class rows within the parameter table
+    const int H = a.fT.H;
+    a.fused_filter = c->cfg.filter_scheme != LEE_FILTER_NONE && (H == 2 || H == 4 || H == 5) &&
+                     a.fT.E <= kTE && ((size_t)b.nx * c->esz) % 16 == 0 && (unsigned long long)b.N < (1ull << 32);
   }
   int rc;
   if ((rc = alloc_fields(c, a.lam, b.N)) || (rc = alloc_fields(c, a.mu, b.N)) || (rc = alloc_fields(c, a.kb[0], b.N)) ||
@@ -1835,7 +1842,37 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
   const int V = c->V;
   // mu = F^T lam: the directions commute, each is transposed, the last pass blends
   void** mu = a.lam;
-  if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
+  if (c->cfg.filter_scheme != LEE_FILTER_NONE && a.fused_filter) {
+    // the fused filter kernel with the transposed rows as its class weights: one read of lam,
+    // one write of mu = (1 - beta) lam + beta F^T lam
+    TmaFilterParams<T> fp;
+    memset(&fp, 0, sizeof fp);
+    fp.nx = b.nx; fp.ny = b.ny; fp.nz = b.nz;
+    fp.V = V;
+    fp.tiles_x = b.tiles_x;
+    fp.k_chunk = b.filter_chunk;
+    fp.nb = a.fT.E;
+    const int H = a.fT.H;
+    for (int o = 0; o <= 2 * H; ++o) {
+      fp.w[0][o] = (T)a.fT.in[o];
+      for (int r = 0; r < a.fT.E; ++r) {
+        fp.w[1 + r][o] = (T)a.fT.lt[r][o];
+        fp.w[1 + a.fT.E + r][o] = (T)a.fT.rt[r][o];
+      }
+    }
+    fp.blend = (T)c->cfg.filter_blend;
+    for (int v = 0; v < V; ++v) fp.out[v] = (T*)a.mu[v];
+    fp.errflag = c->d_err;
+    const int A = (int)(16 / c->esz);
+    const int hx = ((H + A - 1) / A) * A;
+    FieldMaps fm;
+    int rc = field_maps(c, b, a.lam, kTileX + 2 * hx, kTileY + 2 * H, &fm);
+    if (rc) return rc;
+    const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
+    CK(launch_filter_tma<T>(fm, fp, H, c->cfg.num_dim, 0, b.tiles_x * b.tiles_y, chunks, c->stream));
+    c->stats.kernel_launches += 1;
+    mu = a.mu;
+  } else if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
     const int n[3] = {b.nx, b.ny, b.nz};
     int dirs[3], nd = 0;
     for (int d = 0; d < c->cfg.num_dim; ++d)
@@ -2494,7 +2531,8 @@ int lee_prepare(lee_ctx* c) {
     b.tiles_y = (b.ny + kTileY - 1) / kTileY;
     // (the TMA stage kernel addresses points with 32-bit offsets)
     b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32);
-    b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE;
+    b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE &&
+                   (unsigned long long)b.N < (1ull << 32);
     // the kernels are a fixed choice (they round differently, and two contexts of one case give
     // the same bits): the scalar fused filter unless another is asked for
     b.filter_vec = b.tma_filter && c->wfl_sym;

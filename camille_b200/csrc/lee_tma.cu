@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
   // closure-class weights along xi and eta are fixed for a thread: keep them in registers
   T wx[NQ], wy[NQ];
   {
-    const int cx = cls_of(min(i, P.nx - 1), P.nx, HF);
-    const int cy = cls_of(min(j, P.ny - 1), P.ny, HF);
+    const int cx = cls_of(min(i, P.nx - 1), P.nx, P.nb);
+    const int cy = cls_of(min(j, P.ny - 1), P.ny, P.nb);
 #pragma unroll
     for (int o = 0; o < NQ; ++o) {
       wx[o] = P.w[cx][o];
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
     if (!fin) continue;
     T fz, x0, dsum;
     if (DIM == 3) {
-      const int cz = cls_of(k, P.nz, HF);
+      const int cz = cls_of(k, P.nz, P.nb);
       fz = T(0);
       if (cz == 0) {
         // interior plane: the loop-invariant interior weights

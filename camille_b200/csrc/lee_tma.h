@@ -30,9 +30,10 @@ struct TmaStageParams {
 template <typename T>
 struct TmaFilterParams {
   int nx, ny, nz, V, tiles_x, k_chunk;
+  int nb;  // class rows per line end: class 0 interior, 1..nb from the left, nb+1..2nb from the right
   // filter weights by class (interior, left rows, right rows), offsets -hf..hf; the
   // compensated form uses F - I
-  T w[11][11];
+  T w[1 + 2 * kTE][11];
   T blend;
   const T* err[kMaxVars];  // compensated: rounding error of the pre-filter state
   T* out[kMaxVars];
