@@ -19,6 +19,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 PRODUCT_LIB = os.path.join(PKG, "liblee_b200.so")
 
 LEE_OK = 0
+LEE_ERR_ARG, LEE_ERR_STATE, LEE_ERR_UNSUPPORTED = 1, 2, 5
 ERRORS = {1: "LEE_ERR_ARG", 2: "LEE_ERR_STATE", 3: "LEE_ERR_CUDA", 4: "LEE_ERR_NOMEM",
           5: "LEE_ERR_UNSUPPORTED", 6: "LEE_ERR_NONFINITE", 7: "LEE_ERR_NODEVICE", 8: "LEE_ERR_TIMEOUT"}
 FD = {"STANDARD_CENTRAL": 1, "FDO11P": 11}
@@ -28,6 +29,8 @@ FP64, FP32_COMPENSATED = 0, 1
 SOURCE_DISTRIBUTED = 2
 SETUP_METRICS, SETUP_JACOBIAN, SETUP_MEAN_GRADIENT, SETUP_SPONGE = 0, 1, 2, 3
 SOURCE_MONOPOLE = 1
+WAVE_NONE, WAVE_ACOUSTIC, WAVE_ENTROPY = 0, 1, 2
+WAVEFORM_PLANE, WAVEFORM_HOMOGENEOUS, WAVEFORM_GAUSSIAN_ROUNDJET = 0, 1, 2
 
 
 class LeeConfig(C.Structure):
@@ -75,6 +78,7 @@ SIGNATURES = {
     "set_block": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _IP]),
     "set_mean": (C.c_int, [C.c_void_p, C.c_int, _PP]),
     "add_boundary": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP]),
+    "set_harmonic_wave": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]),
     "set_source": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
     "set_block_source": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _DP, C.c_int]),
     "advance_blocks": (C.c_int, [C.c_void_p, C.c_int, _DP]),
@@ -148,11 +152,12 @@ class Solver:
 
     def __init__(self, lib: Library, case: "_cases.Case", precision: int = FP64, device: int = 0,
                  upload: bool = True, overset_file: Optional[str] = None, filter_kernel: int = -1,
-                 stage_kernel: int = -1):
+                 stage_kernel: int = -1, prepare: bool = True):
         """``overset_file``: read the case's overset maps from this Overture-format file
         (lee_read_overset_file) instead of passing the arrays (lee_set_overset).
         ``filter_kernel``: lee_set_filter_kernel (-1/0 scalar, 2/4 vector width);
-        ``stage_kernel``: lee_set_stage_kernel (-1 default, 1 or 2 points per thread)."""
+        ``stage_kernel``: lee_set_stage_kernel (-1 default, 1 or 2 points per thread).
+        ``prepare=False`` stops before lee_prepare (nothing is uploaded)."""
         self.lib = lib
         self.case = case
         self.ctx = C.c_void_p()
@@ -180,6 +185,8 @@ class Solver:
                     sig = _dptr(sarr)
                 self._chk(lib.add_boundary(self.ctx, bd.block, _cases.BC_TYPES[bd.kind], bd.dir, bd.end,
                                            lo, hi, sig))
+            if case.harmonic_wave is not None:
+                self._chk(lib.set_harmonic_wave(self.ctx, *case.harmonic_wave.args()))
             if case.source_monopole() is not None:
                 p = np.array(case.source_monopole(), np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))
@@ -205,6 +212,8 @@ class Solver:
                 self._chk(lib.set_filter_kernel(self.ctx, filter_kernel))
             if stage_kernel != -1:
                 self._chk(lib.set_stage_kernel(self.ctx, stage_kernel))
+            if not prepare:
+                return
             self._chk(lib.prepare(self.ctx))
             if case.microphones is not None:
                 mic = np.ascontiguousarray(case.microphones.l0, np.int64)

@@ -34,11 +34,19 @@ from . import overset as overset_mod
 from . import plot3d
 
 BC_TYPES = {
-    "sponge_freund_ambient": 1000,
+    "dirichlet_allzero": 1,
+    "dirichlet_harmonicwave": 2,
     "neumann": 100,
     "wall_slip_kinematic": 201,
+    "centerline_cart_norm2x": 900,
+    "centerline_cart_norm2y": 901,
+    "centerline_cart_norm2z": 902,
+    "sponge_freund_ambient": 1000,
+    "sponge_freund_harmonicwave": 1002,
 }
 DIRS = {"XI": 0, "ETA": 1, "ZETA": 2}
+WAVE_TYPES = {"WAVE_ACOUSTIC": 1, "WAVE_ENTROPY": 2}
+WAVE_FORMS = {"WAVEFORM_PLANE": 0, "WAVEFORM_HOMOGENEOUS": 1, "WAVEFORM_GAUSSIAN_ROUNDJET": 2}
 
 
 @dataclasses.dataclass
@@ -79,6 +87,30 @@ class Boundary:
         for d in range(3):
             idx += [str(self.lo[d]), str(self.hi[d])]
         return f"{self.block} {self.kind} {sign}{name} " + " ".join(idx)
+
+
+@dataclasses.dataclass
+class HarmonicWave:
+    """The deck's ``HARMONIC_WAVE`` line (src/core/input.cpp:219-231), read by
+    ``dirichlet_harmonicwave`` BC lines and ``sponge_freund_harmonicwave`` zones."""
+    wave_type: str        # key of WAVE_TYPES
+    form: str             # key of WAVE_FORMS
+    direction: int        # 0 X, 1 Y, 2 Z
+    amplitude: float
+    wavelength: float
+    halfwidth: float = 0.0  # WAVEFORM_GAUSSIAN_ROUNDJET only
+
+    def args(self) -> tuple:
+        """Arguments of lee_set_harmonic_wave after the context."""
+        return (WAVE_TYPES[self.wave_type], WAVE_FORMS[self.form], self.direction, float(self.amplitude),
+                float(self.wavelength), float(self.halfwidth))
+
+    def deck_line(self) -> str:
+        line = (f"HARMONIC_WAVE = {self.wave_type}, AMPLITUDE = {self.amplitude!r}, SHAPE = {self.form}, "
+                f"DIRECTION = {'XYZ'[self.direction]}, WAVELENGTH = {self.wavelength!r}")
+        if self.form == "WAVEFORM_GAUSSIAN_ROUNDJET":
+            line += f", HALFWIDTH = {self.halfwidth!r}"
+        return line
 
 
 @dataclasses.dataclass
@@ -136,6 +168,7 @@ class Case:
     overset: Optional["overset_mod.OversetMap"] = None
     distributed: Optional[DistributedSource] = None
     microphones: Optional[Microphones] = None
+    harmonic_wave: Optional[HarmonicWave] = None
     notes: str = ""
     # the deck's SIMULATION; CASE_SCATTERING_TWOCYLINDER brings the reference's own source
     simulation: str = "CASE_KBK_COMBUSTOR"
@@ -201,7 +234,7 @@ class Case:
             lines.append(f"OVERSET_FILE = {os.path.join(os.path.dirname(bc), 'overset.bin')}")
         lines += [
             "SOLUTION_WRITING_TIME = 1.0E+300",
-            "HARMONIC_WAVE = NONE",
+            self.harmonic_wave.deck_line() if self.harmonic_wave is not None else "HARMONIC_WAVE = NONE",
             "INTERPOLATE_SOLUTION = NONE",
         ]
         if self.monopole is not None:
@@ -388,6 +421,72 @@ def wall3d(n: int = 16, nsteps: int = 3, gamma: float = 1.4, halfwidth: float = 
            Boundary(0, "neumann", 0, 1, (m, 0, 0), (m, m, m))]
     return Case(name=f"wall3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
                 notes=f"3-D {n}^3 curvilinear, slip wall zeta=0, Neumann xi=max, shear mean")
+
+
+def waves2d(nx: int = 40, ny: int = 32, spacing: float = 0.25, nsteps: int = 10, gamma: float = 1.4,
+            wave: Optional[HarmonicWave] = None, mach: float = 0.2, sponge: int = 8) -> Case:
+    """2-D Cartesian block on [0, (nx-1) d] x [0, (ny-1) d] driven by a time-harmonic wave
+    (by default an acoustic plane wave along x, amplitude 1e-3, wavelength 16 d) under a
+    uniform mean flow of Mach ``mach`` along x. BC lines: ``dirichlet_harmonicwave`` on xi = 0,
+    ``centerline_cart_norm2y`` on eta = 0, ``dirichlet_allzero`` on eta = max, ``neumann`` on
+    xi = max, and a ``sponge_freund_harmonicwave`` zone ``sponge`` cells wide at the xi = max
+    end that relaxes toward the same wave. A weak Gaussian p' pulse starts inside."""
+    if wave is None:
+        wave = HarmonicWave("WAVE_ACOUSTIC", "WAVEFORM_PLANE", 0, 1e-3, 16.0 * spacing)
+    xs = np.arange(nx, dtype=np.float64) * spacing
+    ys = np.arange(ny, dtype=np.float64) * spacing
+    x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
+    y = np.broadcast_to(ys[None, :, None], (1, ny, nx)).copy()
+    z = np.zeros_like(x)
+    mean = np.zeros((5,) + x.shape)
+    mean[1] = mach
+    mean[4] = 1.0 / gamma
+    state = np.zeros((5,) + x.shape)
+    state[4] = 5e-4 * _gauss((x - 0.5 * xs[-1]) ** 2 + (y - 0.4 * ys[-1]) ** 2, 3.0 * spacing)
+    blk = Block(x, y, z, mean, state)
+    mx, my = nx - 1, ny - 1
+    bnd = [Boundary(0, "dirichlet_harmonicwave", 0, 0, (0, 0, 0), (0, my, 0)),
+           Boundary(0, "centerline_cart_norm2y", 1, 0, (0, 0, 0), (mx, 0, 0)),
+           Boundary(0, "dirichlet_allzero", 1, 1, (0, my, 0), (mx, my, 0)),
+           Boundary(0, "neumann", 0, 1, (mx, 0, 0), (mx, my, 0))]
+    if sponge > 0:
+        bnd.append(Boundary(0, "sponge_freund_harmonicwave", 0, 1, (mx - sponge + 1, 0, 0), (mx, my, 0)))
+    return Case(name=f"waves2d_{nx}x{ny}", num_dim=2, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
+                sponge_constant=2.0, harmonic_wave=wave,
+                notes=f"2-D {nx}x{ny} harmonic wave {wave.wave_type}/{wave.form}, centerline, allzero, sponge")
+
+
+def jet3d(n: int = 14, nsteps: int = 4, gamma: float = 1.4, wave: Optional[HarmonicWave] = None,
+          mach: float = 0.3, sponge: int = 4) -> Case:
+    """3-D curvilinear block (the curvi3d mapping) with the corner eta = zeta = 0 as the axis of
+    a quarter round jet: an entropy wave (by default the Gaussian round jet along x, amplitude
+    1e-3, wavelength 6, half-width 3) enters through a ``dirichlet_harmonicwave`` face on
+    xi = 0 and a ``sponge_freund_harmonicwave`` zone ``sponge`` cells deep behind it, under a
+    uniform mean flow of Mach ``mach`` along x; ``centerline_cart_norm2y`` on eta = 0,
+    ``centerline_cart_norm2z`` on zeta = 0, ``neumann`` on eta = max and zeta = max, and an
+    ambient sponge at the xi = max end."""
+    if wave is None:
+        wave = HarmonicWave("WAVE_ENTROPY", "WAVEFORM_GAUSSIAN_ROUNDJET", 0, 1e-3, 6.0, 3.0)
+    x, y, z = curvi3d_grid(n)
+    mean = np.zeros((5,) + x.shape)
+    mean[1] = mach
+    mean[4] = 1.0 / gamma
+    state = np.zeros((5,) + x.shape)
+    c = 0.5 * (n - 1)
+    state[4] = 5e-4 * _gauss((x - c) ** 2 + (y - 0.3 * n) ** 2 + (z - 0.3 * n) ** 2, 2.0)
+    blk = Block(x, y, z, mean, state)
+    m = n - 1
+    bnd = [Boundary(0, "dirichlet_harmonicwave", 0, 0, (0, 0, 0), (0, m, m)),
+           Boundary(0, "centerline_cart_norm2y", 1, 0, (0, 0, 0), (m, 0, m)),
+           Boundary(0, "centerline_cart_norm2z", 2, 0, (0, 0, 0), (m, m, 0)),
+           Boundary(0, "neumann", 1, 1, (0, m, 0), (m, m, m)),
+           Boundary(0, "neumann", 2, 1, (0, 0, m), (m, m, m))]
+    if sponge > 0:
+        bnd += [Boundary(0, "sponge_freund_harmonicwave", 0, 0, (0, 0, 0), (sponge - 1, m, m)),
+                Boundary(0, "sponge_freund_ambient", 0, 1, (m - sponge + 1, 0, 0), (m, m, m))]
+    return Case(name=f"jet3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
+                sponge_constant=1.0, harmonic_wave=wave,
+                notes=f"3-D {n}^3 quarter jet, harmonic wave {wave.wave_type}/{wave.form}, centerlines")
 
 
 def _tanh_radii(nr: int, r0: float, r1: float, first: float) -> tuple[np.ndarray, float]:

@@ -8,7 +8,12 @@
 //    operator's boundary closure, mirrored on a right end;
 //  - wall_slip_kinematic (:448-494): s' and p' as Neumann; the velocity is taken to the
 //    contravariant components with the metrics, the wall-normal one is set to zero, and it
-//    is brought back with the inverse metrics times J.
+//    is brought back with the inverse metrics times J;
+//  - centerline_cart_norm2x/y/z (:141-148, :498-574): Neumann, then the velocity component
+//    along x/y/z is set to zero;
+//  - dirichlet_allzero (:213-228): every slot zero;
+//  - dirichlet_harmonicwave (:232-344): the time-harmonic wave at the update's time
+//    (tn + c_{min(i+1, last)} h, RungeKutta::integrate, src/solver/temporal_discretization.cpp:232-244).
 // BC lines run one launch each, in the order they were added, so a later line sees what an
 // earlier one wrote (corners). Within one line a face point reads only points off the face
 // (and its own velocity), so the update is in place.
@@ -56,6 +61,21 @@ __global__ void k_bc(BcParams<T> p) {
     double out[kMaxVars];
     if (p.kind == LEE_BC_NEUMANN) {
       for (int v = 0; v < p.V; ++v) out[v] = neumann<T, PAIR>(p, v, l);
+    } else if (p.kind >= LEE_BC_CENTERLINE_CART_NORM2X && p.kind <= LEE_BC_CENTERLINE_CART_NORM2Z) {
+      for (int v = 0; v < p.V; ++v) out[v] = neumann<T, PAIR>(p, v, l);
+      const int d = p.kind - LEE_BC_CENTERLINE_CART_NORM2X;
+      if (d < p.nd) out[1 + d] = 0.0;
+    } else if (p.kind == LEE_BC_DIRICHLET_ALLZERO) {
+      for (int v = 0; v < p.V; ++v) out[v] = 0.0;
+    } else if (p.kind == LEE_BC_DIRICHLET_HARMONICWAVE) {
+      for (int v = 0; v < p.V; ++v) out[v] = 0.0;
+      const double x[3] = {p.xyz[0][l], p.xyz[1][l], p.xyz[2][l]};
+      const double t = p.t_tab ? p.t_tab[(long long)*p.ctr * p.t_stride] : p.t;
+      double ws, wu, wp;
+      wave_eval(p.wave, x, t, &ws, &wu, &wp);
+      out[0] = ws;
+      if (p.wave.dir < p.nd) out[1 + p.wave.dir] = wu;
+      out[P] = wp;
     } else {
       out[0] = neumann<T, PAIR>(p, 0, l);
       out[P] = neumann<T, PAIR>(p, P, l);
@@ -79,6 +99,32 @@ __global__ void k_bc(BcParams<T> p) {
       p.y[v][l] = r;
       if (PAIR) p.e[v][l] = (T)__dsub_rn(out[v], (double)r);
     }
+  }
+}
+
+// The reference state of a harmonic-wave sponge zone (source::apply_bufferZone_Freund_harmonicWave,
+// src/solver/source.cpp:264-320, reading bc::bc_dirichlet_harmonicwave): the wave at the stage
+// time on the zone's box, zero in hole points, in the working precision.
+template <typename T>
+__global__ void k_wave_ref(WaveRefParams<T> p) {
+  const long long n = (long long)p.nb[0] * p.nb[1] * p.nb[2];
+  const double t = p.t_tab ? p.t_tab[(long long)*p.ctr * p.t_stride] : p.t;
+  for (long long lb = blockIdx.x * (long long)blockDim.x + threadIdx.x; lb < n;
+       lb += (long long)gridDim.x * blockDim.x) {
+    const int i = p.lo[0] + (int)(lb % p.nb[0]);
+    const int j = p.lo[1] + (int)((lb / p.nb[0]) % p.nb[1]);
+    const int k = p.lo[2] + (int)(lb / ((long long)p.nb[0] * p.nb[1]));
+    const long long l = i + (long long)p.nx * (j + (long long)p.ny * k);
+    double out[kMaxVars] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!p.iblank || p.iblank[l] != 1) {
+      const double x[3] = {p.xyz[0][l], p.xyz[1][l], p.xyz[2][l]};
+      double ws, wu, wp;
+      wave_eval(p.wave, x, t, &ws, &wu, &wp);
+      out[0] = ws;
+      if (p.wave.dir < p.nd) out[1 + p.wave.dir] = wu;
+      out[p.nd + 1] = wp;
+    }
+    for (int v = 0; v < p.V; ++v) p.out[v * n + lb] = (T)out[v];
   }
 }
 
@@ -185,6 +231,15 @@ cudaError_t launch_overset(const OvsParams<T>& p, cudaStream_t s) {
 
 template cudaError_t launch_overset<double>(const OvsParams<double>&, cudaStream_t);
 template cudaError_t launch_overset<float>(const OvsParams<float>&, cudaStream_t);
+template <typename T>
+cudaError_t launch_wave_ref(const WaveRefParams<T>& p, cudaStream_t s) {
+  const long long n = (long long)p.nb[0] * p.nb[1] * p.nb[2];
+  k_wave_ref<T><<<grid_for(n), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_wave_ref<double>(const WaveRefParams<double>&, cudaStream_t);
+template cudaError_t launch_wave_ref<float>(const WaveRefParams<float>&, cudaStream_t);
 template cudaError_t launch_bc<double>(const BcParams<double>&, cudaStream_t);
 template cudaError_t launch_bc<float>(const BcParams<float>&, cudaStream_t);
 template cudaError_t launch_rho<double>(long long, int, double* const*, double* const*, const double*, double, double*,

@@ -35,6 +35,7 @@ struct Boundary {
   std::vector<double> sigma;  // host copy when given by the caller
   double* d_sigma = nullptr;  // FP64 strengths
   void* d_sigma_t = nullptr;  // strengths in the working precision
+  void* d_ref = nullptr;      // harmonic-wave sponge: the wave on the box, V fields (working precision)
 };
 
 struct BlockData {
@@ -126,6 +127,8 @@ struct lee_ctx {
   cudaStream_t stream = nullptr;
   int src_kind = LEE_SOURCE_NONE;
   double src[7] = {0, 0, 0, 0, 0, 0, 0};
+  Wave wave{};               // lee_set_harmonic_wave (type LEE_WAVE_NONE until set)
+  bool wave_time = false;    // some BC line or sponge zone reads the wave (from lee_prepare)
   std::vector<double> dsrc;  // distributed source parameters (LEE_SOURCE_DISTRIBUTED)
   bool prepared = false, uploaded = false;
   int step = 0;
@@ -175,6 +178,7 @@ struct lee_ctx {
     void* d_amp = nullptr;         // monopole amplitudes, [step][stage], working precision
     size_t amp_cap = 0;            // entries
     int* d_ctr = nullptr;          // steps of the current chunk done so far
+    double* d_ttab = nullptr;      // stage times, [step][block][stage] (harmonic-wave lines and zones)
   } graph;
   // batched kernels for many independent 2-D blocks (lee_advance_blocks)
   struct {
@@ -226,6 +230,20 @@ int fail(lee_ctx* c, int code, const char* fmt, ...) {
     snprintf(g_create_error, sizeof g_create_error, "%s", buf);
   return code;
 }
+
+// Kinds of boundary lines: sponge zones (RHS terms) and BC lines (boundary updates).
+bool is_sponge(int kind) { return kind == LEE_SPONGE_FREUND_AMBIENT || kind == LEE_SPONGE_FREUND_HARMONICWAVE; }
+bool is_bc_line(int kind) {
+  return kind == LEE_BC_NEUMANN || kind == LEE_BC_WALL_SLIP_KINEMATIC || kind == LEE_BC_DIRICHLET_ALLZERO ||
+         kind == LEE_BC_DIRICHLET_HARMONICWAVE ||
+         (kind >= LEE_BC_CENTERLINE_CART_NORM2X && kind <= LEE_BC_CENTERLINE_CART_NORM2Z);
+}
+// BC lines whose face values come from the closure row of the difference operator
+bool reads_inward(int kind) {
+  return kind == LEE_BC_NEUMANN || kind == LEE_BC_WALL_SLIP_KINEMATIC ||
+         (kind >= LEE_BC_CENTERLINE_CART_NORM2X && kind <= LEE_BC_CENTERLINE_CART_NORM2Z);
+}
+bool reads_wave(int kind) { return kind == LEE_BC_DIRICHLET_HARMONICWAVE || kind == LEE_SPONGE_FREUND_HARMONICWAVE; }
 
 #define CK(call)                                                                       \
   do {                                                                                 \
@@ -599,10 +617,11 @@ void fill_stage_common(lee_ctx* c, BlockData& b, StageParams<T>& p) {
   p.inv_gamma = (T)(1.0 / c->cfg.gamma);
   p.nzones = 0;
   for (auto& z : b.bnd) {
-    if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+    if (!is_sponge(z.kind)) continue;
     Zone<T>& zn = p.zones[p.nzones++];
     for (int d = 0; d < 3; ++d) { zn.lo[d] = z.lo[d]; zn.hi[d] = z.hi[d]; }
     zn.sig = dbl ? (const T*)z.d_sigma : (const T*)z.d_sigma_t;
+    zn.ref = (const T*)z.d_ref;
   }
   p.has_src = b.d_src_g != nullptr;
   for (int d = 0; d < 3; ++d) { p.src_lo[d] = b.src_lo[d]; p.src_hi[d] = b.src_hi[d]; }
@@ -1029,7 +1048,7 @@ int build_sigma_field(lee_ctx* c, BlockData& b) {
   if (rc) return rc;
   CK(cudaMemsetAsync(f, 0, (size_t)b.N * 8, c->stream));
   for (auto& z : b.bnd) {
-    if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+    if (!is_sponge(z.kind)) continue;
     const int b0 = z.hi[0] - z.lo[0] + 1, b1 = z.hi[1] - z.lo[1] + 1, b2 = z.hi[2] - z.lo[2] + 1;
     const long long nb = (long long)b0 * b1 * b2;
     k_add_box<<<grid1d(nb), 256, 0, c->stream>>>(b.nx, b.ny, z.lo[0], z.lo[1], z.lo[2], b0, b1, nb, z.d_sigma, f);
@@ -1061,9 +1080,10 @@ int check_device_error(lee_ctx* c) {
 // Every BC line of a block, in the order they were added, on the fields f (with the
 // rounding errors e of a compensated pair, or null).
 template <typename T>
-int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e) {
+int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e, double t, const double* t_tab, const int* ctr,
+              int t_stride) {
   for (auto& z : b.bnd) {
-    if (z.kind != LEE_BC_NEUMANN && z.kind != LEE_BC_WALL_SLIP_KINEMATIC) continue;
+    if (!is_bc_line(z.kind)) continue;
     BcParams<T> p;
     memset(&p, 0, sizeof p);
     p.kind = z.kind; p.dir = z.dir; p.end = z.end;
@@ -1085,7 +1105,41 @@ int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e) {
     for (int q = 0; q < 9; ++q) { p.met[q] = b.d_met[q]; p.minv[q] = b.d_minv[q]; }
     p.jac = b.d_jac;
     p.iblank = b.has_holes ? b.d_iblank : nullptr;
+    p.wave = c->wave;
+    for (int d = 0; d < 3; ++d) p.xyz[d] = b.d_xyz[d];
+    p.t = t;
+    p.t_tab = t_tab;
+    p.ctr = ctr;
+    p.t_stride = t_stride;
     CK(launch_bc<T>(p, c->stream));
+    c->stats.kernel_launches += 1;
+  }
+  return LEE_OK;
+}
+
+// The reference states of the block's harmonic-wave sponge zones at a stage's time (t, or in a
+// replayed step graph t_tab[*ctr * t_stride]), read by the stage kernel's zone loop.
+template <typename T>
+int wave_refs(lee_ctx* c, BlockData& b, double t, const double* t_tab, const int* ctr, int t_stride) {
+  for (auto& z : b.bnd) {
+    if (z.kind != LEE_SPONGE_FREUND_HARMONICWAVE) continue;
+    WaveRefParams<T> p;
+    memset(&p, 0, sizeof p);
+    for (int d = 0; d < 3; ++d) {
+      p.lo[d] = z.lo[d];
+      p.nb[d] = z.hi[d] - z.lo[d] + 1;
+    }
+    p.nx = b.nx; p.ny = b.ny;
+    p.nd = c->cfg.num_dim; p.V = c->V;
+    p.wave = c->wave;
+    for (int d = 0; d < 3; ++d) p.xyz[d] = b.d_xyz[d];
+    p.iblank = b.has_holes ? b.d_iblank : nullptr;
+    p.t = t;
+    p.t_tab = t_tab;
+    p.ctr = ctr;
+    p.t_stride = t_stride;
+    p.out = (T*)z.d_ref;
+    CK(launch_wave_ref<T>(p, c->stream));
     c->stats.kernel_launches += 1;
   }
   return LEE_OK;
@@ -1367,10 +1421,10 @@ int batch_step(lee_ctx* c, const std::vector<double>& dts, bool graph) {
 // One time step (temporal::time_advance with RungeKutta::integrate) enqueued on the context
 // stream: the time is incremented first (solver::solve, src/solver/solver.cpp:72), then every
 // stage runs on every block, the boundary update (BC lines, overset) follows each stage, and
-// the filter closes the step. amp_tab/ctr: the monopole amplitudes of a replayed step graph
-// (null: the amplitude is passed by value).
+// the filter closes the step. amp_tab/t_tab/ctr: the monopole amplitudes and stage times of a
+// replayed step graph, [step][block][stage] (null: passed by value).
 template <typename T>
-int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, const int* ctr) {
+int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, const double* t_tab, const int* ctr) {
   const Tableau tb = tableau(c->cfg.rk_scheme);
   const int ns = tb.ns;
   const int nbk = (int)c->blk.size();
@@ -1403,6 +1457,10 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         p.amp_tab = amp_tab ? amp_tab + bix * ns : nullptr;
         p.step_ctr = ctr;
         p.nstages = nbk * ns;
+        if (c->wave_time) {
+          int rc = wave_refs<T>(c, b, b.time + ci[s] * dt, t_tab ? t_tab + bix * ns + s : nullptr, ctr, nbk * ns);
+          if (rc) return rc;
+        }
         void** zin = s == 0 ? b.y : b.zb[(s + 1) % 2];
         void** zout = b.zb[s % 2];
         for (int v = 0; v < c->V; ++v) {
@@ -1426,8 +1484,13 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
       const bool last = s == ns - 1;
       auto target = [&](BlockData& b) -> void** { return (last && !c->comp) ? b.acc : b.zb[s % 2]; };
       auto errors = [&](BlockData& b) -> void** { return (last && c->comp) ? b.acc : nullptr; };
+      // the update's time is that of the next stage, the last stage's on the last
+      // (RungeKutta::integrate, src/solver/temporal_discretization.cpp:232-244)
+      const int sb = std::min(s + 1, ns - 1);
       for (auto& b : c->blk) {
-        int rc = apply_bcs<T>(c, b, target(b), errors(b));
+        const size_t bix = (size_t)(&b - &c->blk[0]);
+        int rc = apply_bcs<T>(c, b, target(b), errors(b), b.time + ci[sb] * dts[bix],
+                              t_tab ? t_tab + bix * ns + sb : nullptr, ctr, nbk * ns);
         if (rc) return rc;
       }
       // overset interpolation over all blocks, from their post-BC values (overset::interpolate)
@@ -1588,11 +1651,12 @@ int capture_steps(lee_ctx* c, const std::vector<double>& dts) {
   const lee_stats st0 = c->stats;
   memset(&c->stats, 0, sizeof c->stats);
   const bool src = c->src_kind != LEE_SOURCE_NONE;
-  const bool tick = src || c->adj.trace_on;
+  const bool tick = src || c->adj.trace_on || c->wave_time;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
   int rc = LEE_OK, steps = 0;
   for (; steps < 4;) {
-    rc = step_impl<T>(c, dts, src ? (const T*)g.d_amp : nullptr, tick ? g.d_ctr : nullptr);
+    rc = step_impl<T>(c, dts, src ? (const T*)g.d_amp : nullptr, c->wave_time ? g.d_ttab : nullptr,
+                      tick ? g.d_ctr : nullptr);
     if (rc) break;
     if (tick) {
       k_tick<<<1, 1, 0, c->stream>>>(g.d_ctr);
@@ -1642,7 +1706,7 @@ int advance_impl(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
   int done = 0;
   auto direct = [&](int n) -> int {
     for (int k = 0; k < n; ++k) {
-      int rc = step_impl<T>(c, dts, nullptr, nullptr);
+      int rc = step_impl<T>(c, dts, nullptr, nullptr, nullptr);
       if (rc) return rc;
     }
     done += n;
@@ -1659,7 +1723,7 @@ int advance_impl(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
     if (rc) return rc;
   }
   const bool src = c->src_kind != LEE_SOURCE_NONE;
-  const bool tick = src || c->adj.trace_on;
+  const bool tick = src || c->adj.trace_on || c->wave_time;
   const Tableau tb = tableau(c->cfg.rk_scheme);
   const size_t nbk = c->blk.size();
   constexpr size_t kTableSteps = 4096;  // amplitude table rows: steps per chunk of replays
@@ -1670,6 +1734,10 @@ int advance_impl(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
     if ((rc = dev_alloc(c, &p, kTableSteps * 4 * nbk * sizeof(double)))) return rc;
     g.d_amp = p;
     g.amp_cap = kTableSteps * 4 * nbk;
+  }
+  if (c->wave_time && !g.d_ttab) {
+    int rc = dalloc(c, &g.d_ttab, kTableSteps * 4 * nbk);
+    if (rc) return rc;
   }
   if (!g.exec || g.dts != dts || g.layout != layout_of(c)) {
     if (c->batch.active) {
@@ -1685,6 +1753,7 @@ int advance_impl(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
   const int P = g.steps;
   const size_t chunk_steps = (size_t)P * (kTableSteps / P);
   std::vector<T> amp;
+  std::vector<double> ttab;
   while (nsteps - done >= P) {
     const int reps = (int)std::min<long long>((nsteps - done) / P, (long long)(chunk_steps / P));
     const int n = reps * P;
@@ -1701,6 +1770,18 @@ int advance_impl(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
         }
       }
       CK(cudaMemcpyAsync(g.d_amp, amp.data(), amp.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    }
+    if (c->wave_time) {
+      // the stage times themselves, in the same layout, for the harmonic wave
+      ttab.assign((size_t)n * nbk * tb.ns, 0.0);
+      for (size_t q = 0; q < nbk; ++q) {
+        double t = c->blk[q].time;
+        for (int k = 0; k < n; ++k) {
+          t += dts[q];
+          for (int s = 0; s < tb.ns; ++s) ttab[((size_t)k * nbk + q) * tb.ns + s] = t + tb.c[s] * dts[q];
+        }
+      }
+      CK(cudaMemcpyAsync(g.d_ttab, ttab.data(), ttab.size() * 8, cudaMemcpyHostToDevice, c->stream));
     }
     if (tick) CK(cudaMemsetAsync(g.d_ctr, 0, sizeof(int), c->stream));
     if (c->adj.trace_on) {
@@ -1787,8 +1868,11 @@ int adjoint_setup(lee_ctx* c) {
   if (c->blk.size() != 1) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint covers single-block contexts");
   BlockData& b = c->blk[0];
   if (b.has_iblank || c->ovs.n > 0) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no holes or overset");
-  for (auto& z : b.bnd)
+  for (auto& z : b.bnd) {
+    if (z.kind == LEE_SPONGE_FREUND_HARMONICWAVE)
+      return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no harmonic-wave sponge");
     if (z.kind != LEE_SPONGE_FREUND_AMBIENT) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no BC lines");
+  }
   auto is_const = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? !f.p : !d.p; };
   auto is_zero = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? f.zero != 0 : d.zero != 0; };
   bool uni = is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi);
@@ -2087,7 +2171,7 @@ int lee_add_boundary(lee_ctx* c, int b, int kind, int dir, int end, const int lo
   if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_add_boundary after lee_prepare");
   if (b < 0 || b >= (int)c->blk.size() || !c->blk[(size_t)b].set) return fail(c, LEE_ERR_STATE, "lee_set_block first");
   BlockData& bk = c->blk[(size_t)b];
-  if (kind != LEE_SPONGE_FREUND_AMBIENT && kind != LEE_BC_NEUMANN && kind != LEE_BC_WALL_SLIP_KINEMATIC)
+  if (!is_sponge(kind) && !is_bc_line(kind))
     return fail(c, LEE_ERR_UNSUPPORTED, "boundary kind %d is not supported", kind);
   if (dir < 0 || dir >= c->cfg.num_dim || (end != 0 && end != 1)) return fail(c, LEE_ERR_ARG, "dir/end");
   int dims[3] = {bk.nx, bk.ny, bk.nz};
@@ -2098,7 +2182,7 @@ int lee_add_boundary(lee_ctx* c, int b, int kind, int dir, int end, const int lo
     z.lo[d] = lo[d];
     z.hi[d] = hi[d];
   }
-  if (kind != LEE_SPONGE_FREUND_AMBIENT) {
+  if (reads_inward(kind)) {
     // the face's closure row reads S-1 points inward along dir
     const int S = c->fd.S, f = end == 0 ? lo[dir] : hi[dir];
     if ((end == 0 && f + S - 1 > dims[dir] - 1) || (end == 1 && f - (S - 1) < 0))
@@ -2106,14 +2190,45 @@ int lee_add_boundary(lee_ctx* c, int b, int kind, int dir, int end, const int lo
                   dir, S);
   }
   int nzones = 0;
-  for (auto& q : bk.bnd) nzones += q.kind == LEE_SPONGE_FREUND_AMBIENT;
-  if (kind == LEE_SPONGE_FREUND_AMBIENT && nzones >= kMaxZones)
+  for (auto& q : bk.bnd) nzones += is_sponge(q.kind);
+  if (is_sponge(kind) && nzones >= kMaxZones)
     return fail(c, LEE_ERR_UNSUPPORTED, "more than %d sponge zones in a block", kMaxZones);
-  if (sigma && kind == LEE_SPONGE_FREUND_AMBIENT) {
+  if (sigma && is_sponge(kind)) {
     size_t nb = (size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
     z.sigma.assign(sigma, sigma + nb);
   }
   bk.bnd.push_back(std::move(z));
+  return LEE_OK;
+}
+
+int lee_set_harmonic_wave(lee_ctx* c, int type, int form, int dir, double amplitude, double wavelength,
+                          double halfwidth) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_harmonic_wave after lee_prepare");
+  if (type == LEE_WAVE_NONE) {
+    c->wave = Wave{};
+    return LEE_OK;
+  }
+  const bool ok = (type == LEE_WAVE_ACOUSTIC && (form == LEE_WAVEFORM_PLANE || form == LEE_WAVEFORM_HOMOGENEOUS)) ||
+                  (type == LEE_WAVE_ENTROPY &&
+                   (form == LEE_WAVEFORM_HOMOGENEOUS || form == LEE_WAVEFORM_GAUSSIAN_ROUNDJET));
+  if (!ok) return fail(c, LEE_ERR_ARG, "unknown type of wave for this wave form (type %d, form %d)", type, form);
+  if (dir < 0 || dir > 2) return fail(c, LEE_ERR_ARG, "wave direction %d", dir);
+  if (!(amplitude >= 0.0 && amplitude <= 1.0)) return fail(c, LEE_ERR_ARG, "the wave amplitude should be between 0 and 1");
+  if (!(wavelength > 0.0)) return fail(c, LEE_ERR_ARG, "the wavelength must be positive");
+  if (form == LEE_WAVEFORM_GAUSSIAN_ROUNDJET && !(halfwidth > 0.0))
+    return fail(c, LEE_ERR_ARG, "the round jet's half-width must be positive");
+  if (type == LEE_WAVE_ACOUSTIC && dir >= c->cfg.num_dim)
+    return fail(c, LEE_ERR_UNSUPPORTED, "an acoustic wave along direction %d of a %d-D case", dir, c->cfg.num_dim);
+  Wave w{};
+  w.type = type;
+  w.form = form;
+  w.dir = dir;
+  w.amp = amplitude;
+  w.k = 2.0 * acos(-1.0) / wavelength;  // math_constants::twopi (src/math/math.cpp:7-8)
+  w.gfac = form == LEE_WAVEFORM_GAUSSIAN_ROUNDJET ? -log(2.0) / (halfwidth * halfwidth) : 0.0;
+  w.p0 = 1.0 / c->cfg.gamma;
+  c->wave = w;
   return LEE_OK;
 }
 
@@ -2335,6 +2450,11 @@ int lee_prepare(lee_ctx* c) {
   const int dim = c->cfg.num_dim;
   cudaStream_t s = c->stream;
   int rc;
+  c->wave_time = false;
+  for (auto& b : c->blk)
+    for (auto& z : b.bnd) c->wave_time |= reads_wave(z.kind);
+  if (c->wave_time && c->wave.type == LEE_WAVE_NONE)
+    return fail(c, LEE_ERR_STATE, "a harmonic-wave boundary needs lee_set_harmonic_wave");
   for (auto& b : c->blk) {
     if (!b.set || !b.has_mean) return fail(c, LEE_ERR_STATE, "every block needs lee_set_block and lee_set_mean");
     const int N = (int)b.N;
@@ -2404,7 +2524,7 @@ int lee_prepare(lee_ctx* c) {
     if ((rc = dalloc(c, &d_xyzp, 3))) return rc;
     CK(cudaMemcpyAsync(d_xyzp, b.d_xyz, sizeof b.d_xyz, cudaMemcpyHostToDevice, s));
     for (auto& z : b.bnd) {
-      if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+      if (!is_sponge(z.kind)) continue;
       size_t nb = (size_t)(z.hi[0] - z.lo[0] + 1) * (z.hi[1] - z.lo[1] + 1) * (z.hi[2] - z.lo[2] + 1);
       if ((rc = dalloc(c, &z.d_sigma, nb))) return rc;
       if (!z.sigma.empty()) {
@@ -2419,6 +2539,10 @@ int lee_prepare(lee_ctx* c) {
         k_convert<float><<<grid1d((long long)nb), 256, 0, s>>>((long long)nb, f, z.d_sigma);
         CK(cudaGetLastError());
         z.d_sigma_t = f;
+      }
+      if (z.kind == LEE_SPONGE_FREUND_HARMONICWAVE) {
+        if ((rc = dev_alloc(c, &z.d_ref, nb * (size_t)c->V * c->esz))) return rc;
+        CK(cudaMemsetAsync(z.d_ref, 0, nb * (size_t)c->V * c->esz, s));
       }
     }
     // monopole spatial factor on the box where exp() is nonzero in FP64
@@ -2530,7 +2654,10 @@ int lee_prepare(lee_ctx* c) {
     b.tiles_x = (b.nx + kTileX - 1) / kTileX;
     b.tiles_y = (b.ny + kTileY - 1) / kTileY;
     // (the TMA stage kernel addresses points with 32-bit offsets)
-    b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32);
+    // (and the harmonic-wave sponge, an RHS term of the generic kernel's zone loop, is absent)
+    bool wave_zone = false;
+    for (auto& z : b.bnd) wave_zone |= z.kind == LEE_SPONGE_FREUND_HARMONICWAVE;
+    b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32) && !wave_zone;
     b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE &&
                    (unsigned long long)b.N < (1ull << 32);
     // the kernels are a fixed choice (they round differently, and two contexts of one case give
@@ -2560,7 +2687,7 @@ int lee_prepare(lee_ctx* c) {
       }
       for (int q = 0; q < 9; ++q) uni &= is_zero(b.cd_gu[q], b.cf_gu[q]) != 0;
       uni &= is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi) && !b.need_rho;
-      for (auto& z : b.bnd) spg |= z.kind == LEE_SPONGE_FREUND_AMBIENT;
+      for (auto& z : b.bnd) spg |= is_sponge(z.kind);
       b.traits = kTrTma | (jmf ? kTrJmField : 0) | (uni ? kTrUniform : 0) | (spg ? kTrSponge : 0);
       b.stage_pair = c->comp && uni && b.nx % 2 == 0;
       b.stage_px = b.stage_pair ? 2 : 1;
@@ -2892,6 +3019,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     fill_stage_common<double>(c, bk, p);
     p.stage = -1;
     p.src_amp = c->src_kind != LEE_SOURCE_NONE ? source_amp(c, bk, time) : 0.0;
+    if (int rc = wave_refs<double>(c, bk, time, nullptr, nullptr, 0)) return rc;
     p.rho_prev = bk.rho_valid ? (const double*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const double*)bk.y[v];
@@ -2906,6 +3034,7 @@ int lee_eval_rhs(lee_ctx* c, int b, double time, double* const rhs[5]) {
     fill_stage_common<float>(c, bk, p);
     p.stage = -1;
     p.src_amp = (float)(c->src_kind != LEE_SOURCE_NONE ? source_amp(c, bk, time) : 0.0);
+    if (int rc = wave_refs<float>(c, bk, time, nullptr, nullptr, 0)) return rc;
     p.rho_prev = bk.rho_valid ? (const float*)bk.rho : nullptr;
     for (int v = 0; v < c->V; ++v) {
       p.zin[v] = (const float*)bk.y[v];
@@ -3320,7 +3449,7 @@ int lee_get_setup(lee_ctx* c, int b, int what, double* out) {
     CK(cudaStreamSynchronize(c->stream));
     memset(out, 0, N * 8);
     for (auto& z : bk.bnd) {
-      if (z.kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+      if (!is_sponge(z.kind)) continue;
       int b0 = z.hi[0] - z.lo[0] + 1, b1 = z.hi[1] - z.lo[1] + 1, b2 = z.hi[2] - z.lo[2] + 1;
       std::vector<double> h((size_t)b0 * b1 * b2);
       CK(cudaMemcpy(h.data(), z.d_sigma, h.size() * 8, cudaMemcpyDeviceToHost));

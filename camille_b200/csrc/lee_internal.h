@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include "../../include/lee_b200.h"
@@ -52,12 +53,47 @@ struct Coef {
   int zero;
 };
 
-// A sponge zone: inclusive index box and its strengths (box-shaped, i fastest).
+// A sponge zone: inclusive index box and its strengths (box-shaped, i fastest); `ref`, when
+// set, holds the state the zone relaxes toward (V box fields one after the other, the
+// time-harmonic wave at the stage time), else it relaxes toward zero.
 template <typename T>
 struct Zone {
   int lo[3], hi[3];
   const T* sig;
+  const T* ref;
 };
+
+// The time-harmonic wave of lee_set_harmonic_wave: type LEE_WAVE_*, form LEE_WAVEFORM_*, the
+// propagation direction, amplitude, wavenumber k = 2 pi / wavelength, the Gaussian exponent
+// factor -ln 2 / halfwidth^2 and the ambient pressure 1/gamma.
+struct Wave {
+  int type, form, dir;
+  double amp, k, gfac, p0;
+};
+
+// The wave at coordinates x and time t as bc::bc_dirichlet_harmonicwave evaluates it
+// (src/solver/boundary_condition.cpp:232-344): the entropy, velocity (along dir) and pressure
+// fluctuations. Unknown combinations are refused on the host.
+__host__ __device__ inline void wave_eval(const Wave& w, const double x[3], double t, double* s, double* u,
+                                          double* p) {
+  double pf = 0.0, vf = 0.0, sf = 0.0;
+  if (w.form == LEE_WAVEFORM_PLANE) {
+    pf = w.amp * w.p0 * sin(w.k * (x[w.dir] - 1.0 * t));
+    vf = pf;
+  } else if (w.type == LEE_WAVE_ACOUSTIC) {
+    pf = w.amp * w.p0 * sin(w.k * 1.0 * t);
+    vf = pf;
+  } else {
+    sf = w.amp * (1.0 + sin(w.k * 1.0 * t));
+    if (w.form == LEE_WAVEFORM_GAUSSIAN_ROUNDJET) {
+      const double a = x[w.dir == 0 ? 1 : 0], b = x[w.dir == 2 ? 1 : 2];
+      sf *= exp(w.gfac * (a * a + b * b));
+    }
+  }
+  *s = sf;
+  *u = vf / (1.0 * 1.0);
+  *p = pf;
+}
 
 // Everything one stage kernel launch needs for one block.
 template <typename T>
@@ -130,6 +166,28 @@ struct BcParams {
   const double* minv[9];
   const double* jac;
   const int* iblank;
+  // harmonic wave: the wave, the coordinates and the time of the boundary update (t, or in a
+  // replayed step graph t_tab[*ctr * t_stride])
+  Wave wave;
+  const double* xyz[3];
+  double t;
+  const double* t_tab;
+  const int* ctr;
+  int t_stride;
+};
+
+// The time-harmonic wave on a sponge zone's box (lee_bc.cu): V box fields, zero in holes.
+template <typename T>
+struct WaveRefParams {
+  int lo[3], nb[3], nx, ny, nd, V;
+  Wave wave;
+  const double* xyz[3];
+  const int* iblank;
+  double t;                   // the stage time, or in a replayed step graph t_tab[*ctr * t_stride]
+  const double* t_tab;
+  const int* ctr;
+  int t_stride;
+  T* out;
 };
 
 // Overset interpolation of a stage output over all blocks (lee_bc.cu): receiver r of block
@@ -160,6 +218,8 @@ cudaError_t launch_overset(const OvsParams<T>& p, cudaStream_t s);
 
 template <typename T>
 cudaError_t launch_bc(const BcParams<T>& p, cudaStream_t s);
+template <typename T>
+cudaError_t launch_wave_ref(const WaveRefParams<T>& p, cudaStream_t s);
 // out = p'/(gamma p_bar) - s' of the state y (+ e when e is non-null)
 template <typename T>
 cudaError_t launch_rho(long long n, int V, T* const* y, T* const* e, const double* pbar, double gamma, T* out,

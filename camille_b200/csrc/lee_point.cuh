@@ -142,6 +142,14 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, I l, int i, 
       int b0 = zn.hi[0] - zn.lo[0] + 1, b1 = zn.hi[1] - zn.lo[1] + 1;
       long long lb = (i - zn.lo[0]) + (long long)b0 * ((j - zn.lo[1]) + (long long)b1 * (k - zn.lo[2]));
       T sg = zn.sig[lb];
+      if (zn.ref) {
+        // source::apply_bufferZone_Freund_harmonicWave (src/solver/source.cpp:264-320): the
+        // reference state is the wave at the stage time
+        const long long nbz = (long long)b0 * b1 * (zn.hi[2] - zn.lo[2] + 1);
+#pragma unroll
+        for (int v = 0; v < V; ++v) r[v] += -sg * (q[v] - zn.ref[v * nbz + lb]);
+        continue;
+      }
 #pragma unroll
       for (int v = 0; v < V; ++v) r[v] += -sg * (q[v] - T(0));
     }

@@ -240,11 +240,17 @@ struct BcLine {
   int block, kind, dir, end, lo[3], hi[3];
 };
 
-// io::parse_boundary_type (src/io/io.cpp) for the kinds the library implements.
+// io::parse_boundary_type (src/io/io.cpp:1275-1320) for the kinds the library implements.
 int bc_kind(const std::string& s) {
+  if (s == "dirichlet_allzero") return LEE_BC_DIRICHLET_ALLZERO;
+  if (s == "dirichlet_harmonicwave") return LEE_BC_DIRICHLET_HARMONICWAVE;
   if (s == "neumann") return LEE_BC_NEUMANN;
   if (s == "wall_slip_kinematic") return LEE_BC_WALL_SLIP_KINEMATIC;
+  if (s == "centerline_cart_norm2x") return LEE_BC_CENTERLINE_CART_NORM2X;
+  if (s == "centerline_cart_norm2y") return LEE_BC_CENTERLINE_CART_NORM2Y;
+  if (s == "centerline_cart_norm2z") return LEE_BC_CENTERLINE_CART_NORM2Z;
   if (s == "sponge_freund_ambient") return LEE_SPONGE_FREUND_AMBIENT;
+  if (s == "sponge_freund_harmonicwave") return LEE_SPONGE_FREUND_HARMONICWAVE;
   die("boundary type " + s + " is not implemented by the library");
 }
 
@@ -303,13 +309,37 @@ struct Run {
   int num_time_steps = 0, report_freq = 1, overset_order = 0;
   bool has_monopole = false;
   double monopole[7] = {};
+  // HARMONIC_WAVE (type LEE_WAVE_NONE when the deck says NONE)
+  int wave_type = LEE_WAVE_NONE, wave_form = -1, wave_dir = 0;
+  double wave_amp = 0.0, wave_len = 0.0, wave_hw = 0.0;
 };
 
 Run configure(const Deck& d, int precision) {
   Run r;
   if (d.str("PHYSICAL_MODEL") != "LEE") die("PHYSICAL_MODEL " + d.str("PHYSICAL_MODEL") + ": the library runs LEE");
   if (d.has("AXISYMMETRY") && d.str("AXISYMMETRY") != "FALSE") die("AXISYMMETRY is not implemented by the library");
-  if (d.has("HARMONIC_WAVE") && d.str("HARMONIC_WAVE") != "NONE") die("HARMONIC_WAVE is not implemented by the library");
+  if (d.has("HARMONIC_WAVE") && d.str("HARMONIC_WAVE") != "NONE") {
+    // src/core/input.cpp:219-231, then check_consistency_wave (:629-656), whose else clauses
+    // bind to the inner ifs: only an acoustic wave of another shape and the amplitude range
+    // stop the run there; a type or shape without a formula stops it at the first boundary
+    // update that evaluates the wave (src/solver/boundary_condition.cpp:263-307)
+    const std::string type = d.str("HARMONIC_WAVE"), form = d.str("HARMONIC_WAVE", "SHAPE");
+    r.wave_amp = d.d("HARMONIC_WAVE", "AMPLITUDE");
+    std::string dir = d.str("HARMONIC_WAVE", "DIRECTION");
+    for (auto& ch : dir) ch = (char)std::toupper((unsigned char)ch);
+    r.wave_dir = dir == "X" ? 0 : (dir == "Y" || dir == "R") ? 1 : dir == "Z" ? 2 : -1;
+    if (r.wave_dir < 0) die("HARMONIC_WAVE DIRECTION " + dir);
+    r.wave_len = d.d("HARMONIC_WAVE", "WAVELENGTH");
+    if (form == "WAVEFORM_GAUSSIAN_ROUNDJET") r.wave_hw = d.d("HARMONIC_WAVE", "HALFWIDTH");
+    if (type == "WAVE_ACOUSTIC" && form != "WAVEFORM_PLANE" && form != "WAVEFORM_HOMOGENEOUS")
+      die("Unknown spatial distribution of acoustic waves.");
+    if (r.wave_amp < 0.0 || r.wave_amp > 1.0) die("The wave amplitude should be between 0 and 1.");
+    r.wave_type = type == "WAVE_ACOUSTIC" ? LEE_WAVE_ACOUSTIC : type == "WAVE_ENTROPY" ? LEE_WAVE_ENTROPY : -1;
+    r.wave_form = form == "WAVEFORM_PLANE"           ? LEE_WAVEFORM_PLANE
+                  : form == "WAVEFORM_HOMOGENEOUS"   ? LEE_WAVEFORM_HOMOGENEOUS
+                  : form == "WAVEFORM_GAUSSIAN_ROUNDJET" ? LEE_WAVEFORM_GAUSSIAN_ROUNDJET
+                                                     : -1;
+  }
   if (d.has("INTERPOLATE_SOLUTION") && d.str("INTERPOLATE_SOLUTION") != "NONE")
     die("INTERPOLATE_SOLUTION is a pre-processing mode, not a time advance");
   if (d.has("FILE_FORMAT") && d.str("FILE_FORMAT") != "PLOT3D") die("FILE_FORMAT " + d.str("FILE_FORMAT"));
@@ -420,6 +450,8 @@ void print_parse(const Run& r, const std::vector<Block>& blocks, const std::vect
   } else {
     std::printf("null");
   }
+  std::printf(", \"wave\": [%d, %d, %d, %.17g, %.17g, %.17g]", r.wave_type, r.wave_form, r.wave_dir, r.wave_amp,
+              r.wave_len, r.wave_hw);
   std::printf(", \"bc\": [");
   for (size_t q = 0; q < bcs.size(); ++q)
     std::printf("%s[%d, %d, %d, %d, %d, %d, %d, %d, %d, %d]", q ? ", " : "", bcs[q].block, bcs[q].kind, bcs[q].dir,
@@ -475,6 +507,16 @@ int main(int argc, char** argv) {
     check(c, lee_set_mean(c, (int)b, m), "mean flow");
   }
   for (const BcLine& b : bcs) check(c, lee_add_boundary(c, b.block, b.kind, b.dir, b.end, b.lo, b.hi, nullptr), "BC file");
+  bool wave_lines = false;
+  for (const BcLine& b : bcs)
+    wave_lines |= b.kind == LEE_BC_DIRICHLET_HARMONICWAVE || b.kind == LEE_SPONGE_FREUND_HARMONICWAVE;
+  if (wave_lines) {
+    // the reference reads the wave only where a line evaluates it
+    if (r.wave_type == LEE_WAVE_NONE) die("Unknown type of wave form.");
+    if (r.wave_type < 0 || r.wave_form < 0) die("Unknown type of wave for this wave form.");
+    check(c, lee_set_harmonic_wave(c, r.wave_type, r.wave_form, r.wave_dir, r.wave_amp, r.wave_len, r.wave_hw),
+          "HARMONIC_WAVE");
+  }
   if (r.has_monopole) check(c, lee_set_source(c, LEE_SOURCE_MONOPOLE, r.monopole, 7), "source");
   if (r.overset != "NONE") check(c, lee_read_overset_file(c, r.overset_file.c_str(), r.overset_order), "overset file");
   check(c, lee_prepare(c), "lee_prepare");

@@ -61,10 +61,24 @@ extern "C" {
 #define LEE_FP64 0                /* the reference's own FP64 arithmetic */
 #define LEE_FP32_COMPENSATED 1    /* FP32 state/stencils, compensated RK sum */
 
-/* boundary kinds: the reference's codes (src/core/param.h:101-121) */
+/* boundary kinds: the reference's codes (src/core/param.h:99-114) */
+#define LEE_BC_DIRICHLET_ALLZERO 1         /* every slot 0 (bc_dirichlet_allzero) */
+#define LEE_BC_DIRICHLET_HARMONICWAVE 2    /* the harmonic wave of lee_set_harmonic_wave */
 #define LEE_BC_NEUMANN 100
 #define LEE_BC_WALL_SLIP_KINEMATIC 201
+#define LEE_BC_CENTERLINE_CART_NORM2X 900  /* Neumann, then u' = 0 (v' for 901, w' for 902) */
+#define LEE_BC_CENTERLINE_CART_NORM2Y 901
+#define LEE_BC_CENTERLINE_CART_NORM2Z 902
 #define LEE_SPONGE_FREUND_AMBIENT 1000
+#define LEE_SPONGE_FREUND_HARMONICWAVE 1002  /* relaxes toward the harmonic wave */
+
+/* time-harmonic wave (HARMONIC_WAVE deck line, src/core/input.cpp:219-231) */
+#define LEE_WAVE_NONE 0
+#define LEE_WAVE_ACOUSTIC 1             /* WAVE_ACOUSTIC */
+#define LEE_WAVE_ENTROPY 2              /* WAVE_ENTROPY */
+#define LEE_WAVEFORM_PLANE 0            /* WAVEFORM_PLANE (acoustic) */
+#define LEE_WAVEFORM_HOMOGENEOUS 1      /* WAVEFORM_HOMOGENEOUS (acoustic or entropy) */
+#define LEE_WAVEFORM_GAUSSIAN_ROUNDJET 2 /* WAVEFORM_GAUSSIAN_ROUNDJET (entropy) */
 
 /* physical sources */
 #define LEE_SOURCE_NONE 0
@@ -124,6 +138,25 @@ int lee_set_mean(lee_ctx *ctx, int b, const double *const mean[5]);
  * src/geometry/geometry.cpp:1126-1127); NULL computes them on the GPU. */
 int lee_add_boundary(lee_ctx *ctx, int b, int kind, int dir, int end, const int lo[3], const int hi[3],
                      const double *sigma);
+/* The time-harmonic wave read by LEE_BC_DIRICHLET_HARMONICWAVE lines and
+ * LEE_SPONGE_FREUND_HARMONICWAVE zones (the deck's HARMONIC_WAVE line, src/core/input.cpp:219-231;
+ * the wave of bc::bc_dirichlet_harmonicwave, src/solver/boundary_condition.cpp:232-344). type
+ * LEE_WAVE_*, form LEE_WAVEFORM_*, dir 0/1/2 (X/Y/Z) the propagation direction, amplitude in
+ * [0, 1] (check_consistency_wave, src/core/input.cpp:650-652), wavelength > 0, halfwidth > 0
+ * for the Gaussian round jet (ignored otherwise). With k = 2 pi / wavelength, p_0 = 1/gamma and
+ * x the coordinate along dir, the wave at time t is
+ *   acoustic plane:        p' = u'_dir = amplitude p_0 sin(k (x - t)), s' = 0
+ *   acoustic homogeneous:  p' = u'_dir = amplitude p_0 sin(k t),       s' = 0
+ *   entropy homogeneous:   s' = amplitude (1 + sin(k t)),              u' = p' = 0
+ *   entropy round jet:     s' = amplitude (1 + sin(k t)) exp(-ln 2 (a^2 + b^2) / halfwidth^2)
+ * with a, b the two coordinates other than x; every other slot is 0. A BC line writes it on
+ * its face at the time the reference's RungeKutta::integrate passes to update_boundary
+ * (tn + c_{min(i+1, last)} h); a sponge zone adds -sigma (q - wave) at the stage time.
+ * LEE_ERR_ARG for an unknown type or form, a form the type has no formula for, or a value out
+ * of range (the reference stops at its first boundary update on a form the type has no formula
+ * for); LEE_ERR_UNSUPPORTED for an acoustic wave along Z in 2-D (its w' has no slot here). */
+int lee_set_harmonic_wave(lee_ctx *ctx, int type, int form, int dir, double amplitude, double wavelength,
+                          double halfwidth);
 /* Physical source (source::apply_physicalSource, src/solver/source.cpp:22-107). */
 int lee_set_source(lee_ctx *ctx, int kind, const double *params, int nparams);
 /* A source for block b only (no reference counterpart: the reference applies its source to

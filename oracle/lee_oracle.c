@@ -89,6 +89,9 @@ struct orc_ctx {
   int prepared, step;
   double time;
   ovs_t ovs;
+  /* time-harmonic wave (UserInput::harmonicWave_*, src/core/input.cpp:219-231) */
+  int wave_type, wave_form, wave_dir;
+  double wave_amp, wave_len, wave_hw;
   char err[512];
 };
 typedef struct orc_ctx orc_ctx;
@@ -455,6 +458,36 @@ static void compute_sigma(orc_ctx *c, blk_t *bk, bnd_t *z) {
  * Right-hand side: spatial::compute_RHS (src/solver/spatial_discretization.cpp:1963-1990),
  * compute_RHS_linearized_Euler (:2053-2130) and source::add_RHSSourceTerms
  * (src/solver/source.cpp:10-18): physical source, then Freund sponges (:174-201). */
+/* The wave of bc::bc_dirichlet_harmonicwave (src/solver/boundary_condition.cpp:232-344) at
+ * point l0 and the given time, into the five LEE slots (entropy 0, velocity 1 + dir, pressure
+ * 4; every other slot 0), for a point that is not a hole. */
+static const int dir_other[3][2] = {{1, 2}, {0, 2}, {0, 1}}; /* src/core/param.h:133 */
+static void wave_at(const orc_ctx *c, const blk_t *bk, int l0, double time, double out[5]) {
+  double rho_0 = 1.0, p_0 = 1.0 / c->cfg.gamma, c_0 = 1.0;
+  double wavenumber = (2.0 * acos(-1.0)) / c->wave_len;
+  int idir = c->wave_dir;
+  double loc = bk->xyz[idir][l0];
+  double t1 = bk->xyz[dir_other[idir][0]][l0], t2 = bk->xyz[dir_other[idir][1]][l0];
+  double pf = 0.0, vf = 0.0, sf = 0.0;
+  if (c->wave_form == LEE_WAVEFORM_PLANE) {
+    pf = c->wave_amp * p_0 * sin(wavenumber * (loc - c_0 * time));
+    vf = pf;
+  } else if (c->wave_form == LEE_WAVEFORM_HOMOGENEOUS && c->wave_type == LEE_WAVE_ACOUSTIC) {
+    pf = c->wave_amp * p_0 * sin(wavenumber * c_0 * time);
+    vf = pf;
+  } else {
+    sf = c->wave_amp * (1.0 + sin(wavenumber * c_0 * time));
+    if (c->wave_form == LEE_WAVEFORM_GAUSSIAN_ROUNDJET) {
+      double fac = -log(2.0) / pow(c->wave_hw, 2);
+      sf *= exp(fac * (pow(t1, 2) + pow(t2, 2)));
+    }
+  }
+  for (int v = 0; v < 5; ++v) out[v] = 0.0;
+  out[0] = sf;
+  out[1 + idir] = vf / (rho_0 * c_0);
+  out[4] = pf;
+}
+
 static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, double time) {
   int nd = c->cfg.num_dim, N = bk->N;
   double g = c->cfg.gamma;
@@ -513,7 +546,8 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
   }
   for (int zi = 0; zi < bk->nbnd; ++zi) {
     bnd_t *z = &bk->bnd[zi];
-    if (z->kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+    int wave = z->kind == LEE_SPONGE_FREUND_HARMONICWAVE; /* apply_bufferZone_Freund_harmonicWave (:264-320) */
+    if (z->kind != LEE_SPONGE_FREUND_AMBIENT && !wave) continue;
     int bn0 = z->hi[0] - z->lo[0] + 1, bn1 = z->hi[1] - z->lo[1] + 1;
     for (int k = z->lo[2]; k <= z->hi[2]; ++k)
       for (int j = z->lo[1]; j <= z->hi[1]; ++j)
@@ -521,8 +555,10 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
           int lb = (i - z->lo[0]) + bn0 * ((j - z->lo[1]) + bn1 * (k - z->lo[2]));
           int l0 = i + bk->nx * (j + bk->ny * k);
           double sg = z->sigma[lb];
+          double ref[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+          if (wave && !(bk->iblank && bk->iblank[l0] == BLANKED)) wave_at(c, bk, l0, time, ref);
           for (int v = 0; v < 5; ++v) {
-            double relax = -sg * (y[v][l0] - 0.0);
+            double relax = -sg * (y[v][l0] - ref[v]);
             rhs[v][l0] += relax;
           }
         }
@@ -532,15 +568,18 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
 
 /* ---------------------------------------------------------------------------
  * Boundary conditions: bc::apply_BC (src/solver/boundary_condition.cpp:46-209) with
- * bc_neumann (:348-444) and bc_wall_slip_kinematic (:448-494). The boundary is the
- * box's end face in its direction (src/geometry/geometry.cpp:583-645). */
-static void apply_bc(orc_ctx *c, blk_t *bk, double **y) {
+ * bc_dirichlet_allzero (:213-228), bc_dirichlet_harmonicwave (:232-344), bc_neumann
+ * (:348-444), bc_wall_slip_kinematic (:448-494) and bc_centerline (:498-574) at the given
+ * time. The boundary is the box's end face in its direction (src/geometry/geometry.cpp:583-645). */
+static void apply_bc(orc_ctx *c, blk_t *bk, double **y, double time) {
   int nd = c->cfg.num_dim;
   int st[3] = {1, bk->nx, bk->nx * bk->ny};
   const op_t *o = &c->fd;
   for (int zi = 0; zi < bk->nbnd; ++zi) {
     bnd_t *z = &bk->bnd[zi];
-    if (z->kind != LEE_BC_NEUMANN && z->kind != LEE_BC_WALL_SLIP_KINEMATIC) continue;
+    int centerline = z->kind >= LEE_BC_CENTERLINE_CART_NORM2X && z->kind <= LEE_BC_CENTERLINE_CART_NORM2Z;
+    int dirichlet = z->kind == LEE_BC_DIRICHLET_ALLZERO || z->kind == LEE_BC_DIRICHLET_HARMONICWAVE;
+    if (z->kind != LEE_BC_NEUMANN && z->kind != LEE_BC_WALL_SLIP_KINEMATIC && !centerline && !dirichlet) continue;
     int lo[3] = {z->lo[0], z->lo[1], z->lo[2]}, hi[3] = {z->hi[0], z->hi[1], z->hi[2]};
     lo[z->dir] = hi[z->dir] = (z->end == 0) ? z->lo[z->dir] : z->hi[z->dir];
     int sd = st[z->dir];
@@ -549,9 +588,9 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y) {
     double *data[5];
     for (int v = 0; v < 5; ++v) data[v] = dalloc((size_t)nbp);
     int vars_neu[5], nneu = 0;
-    if (z->kind == LEE_BC_NEUMANN) {
+    if (z->kind == LEE_BC_NEUMANN || centerline) {
       for (int v = 0; v < 5; ++v) vars_neu[nneu++] = v;
-    } else {
+    } else if (z->kind == LEE_BC_WALL_SLIP_KINEMATIC) {
       vars_neu[nneu++] = 0;
       vars_neu[nneu++] = 4;
     }
@@ -561,6 +600,14 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y) {
           int lb = (i - lo[0]) + nbx * ((j - lo[1]) + nby * (k - lo[2]));
           int l0 = i + bk->nx * (j + bk->ny * k);
           int hole = bk->iblank && bk->iblank[l0] == BLANKED;
+          if (dirichlet) {
+            for (int v = 0; v < 5; ++v) data[v][lb] = 0.0;
+            if (z->kind == LEE_BC_DIRICHLET_HARMONICWAVE && !hole) {
+              double w[5];
+              wave_at(c, bk, l0, time, w);
+              for (int v = 0; v < 5; ++v) data[v][lb] = w[v];
+            }
+          }
           if (!hole) {
             for (int q = 0; q < nneu; ++q) {
               int v = vars_neu[q];
@@ -591,6 +638,7 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y) {
             }
             for (int q = 0; q < 3; ++q) data[1 + q][lb] = vel[q];
           }
+          if (centerline && !hole) data[1 + (z->kind - LEE_BC_CENTERLINE_CART_NORM2X)][lb] = 0.0;
         }
     for (int k = lo[2]; k <= hi[2]; ++k)
       for (int j = lo[1]; j <= hi[1]; ++j)
@@ -730,11 +778,36 @@ int orc_add_boundary(orc_ctx *c, int b, int kind, int dir, int end, const int lo
   z->kind = kind; z->dir = dir; z->end = end;
   for (int d = 0; d < 3; ++d) { z->lo[d] = lo[d]; z->hi[d] = hi[d]; }
   z->sigma = NULL;
-  if (kind == LEE_SPONGE_FREUND_AMBIENT && sigma) {
+  if ((kind == LEE_SPONGE_FREUND_AMBIENT || kind == LEE_SPONGE_FREUND_HARMONICWAVE) && sigma) {
     int nb = (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
     z->sigma = dalloc((size_t)nb);
     memcpy(z->sigma, sigma, sizeof(double) * (size_t)nb);
   }
+  return LEE_OK;
+}
+
+/* The HARMONIC_WAVE deck line (src/core/input.cpp:219-231) with check_consistency_wave's
+ * amplitude range (:650-652); the forms each type has a formula for
+ * (src/solver/boundary_condition.cpp:263-307). */
+int orc_set_harmonic_wave(orc_ctx *c, int type, int form, int dir, double amplitude, double wavelength,
+                          double halfwidth) {
+  if (type == LEE_WAVE_NONE) {
+    c->wave_type = LEE_WAVE_NONE;
+    return LEE_OK;
+  }
+  int ok = (type == LEE_WAVE_ACOUSTIC && (form == LEE_WAVEFORM_PLANE || form == LEE_WAVEFORM_HOMOGENEOUS)) ||
+           (type == LEE_WAVE_ENTROPY && (form == LEE_WAVEFORM_HOMOGENEOUS || form == LEE_WAVEFORM_GAUSSIAN_ROUNDJET));
+  if (!ok) return fail(c, LEE_ERR_ARG, "unknown type of wave for this wave form");
+  if (dir < 0 || dir > 2) return fail(c, LEE_ERR_ARG, "wave direction");
+  if (amplitude < 0.0 || amplitude > 1.0) return fail(c, LEE_ERR_ARG, "the wave amplitude should be between 0 and 1");
+  if (!(wavelength > 0.0)) return fail(c, LEE_ERR_ARG, "wavelength");
+  if (form == LEE_WAVEFORM_GAUSSIAN_ROUNDJET && !(halfwidth > 0.0)) return fail(c, LEE_ERR_ARG, "halfwidth");
+  c->wave_type = type;
+  c->wave_form = form;
+  c->wave_dir = dir;
+  c->wave_amp = amplitude;
+  c->wave_len = wavelength;
+  c->wave_hw = halfwidth;
   return LEE_OK;
 }
 
@@ -946,13 +1019,21 @@ int orc_get_overset(orc_ctx *c, int *recv_block, long long *recv_l0, int *donor_
 }
 
 int orc_prepare(orc_ctx *c) {
+  for (int b = 0; b < c->nblk; ++b)
+    for (int zi = 0; zi < c->blk[b].nbnd; ++zi) {
+      int k = c->blk[b].bnd[zi].kind;
+      if ((k == LEE_BC_DIRICHLET_HARMONICWAVE || k == LEE_SPONGE_FREUND_HARMONICWAVE) && c->wave_type == LEE_WAVE_NONE)
+        return fail(c, LEE_ERR_STATE, "a harmonic-wave boundary needs a harmonic wave");
+    }
   for (int b = 0; b < c->nblk; ++b) {
     blk_t *bk = &c->blk[b];
     if (!bk->set) return fail(c, LEE_ERR_STATE, "block %d not set", b);
     int rc = compute_metrics(c, bk);
     if (rc) return rc;
     for (int zi = 0; zi < bk->nbnd; ++zi)
-      if (bk->bnd[zi].kind == LEE_SPONGE_FREUND_AMBIENT && !bk->bnd[zi].sigma) compute_sigma(c, bk, &bk->bnd[zi]);
+      if ((bk->bnd[zi].kind == LEE_SPONGE_FREUND_AMBIENT || bk->bnd[zi].kind == LEE_SPONGE_FREUND_HARMONICWAVE) &&
+          !bk->bnd[zi].sigma)
+        compute_sigma(c, bk, &bk->bnd[zi]);
     /* mean gradients: spatial::precompute_something (:2250-2271), with hole closures */
     int nd = c->cfg.num_dim;
     double *work = dalloc((size_t)bk->N);
@@ -1126,9 +1207,12 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
         }
       }
       double **tgts[MAXB];
-      for (int b = 0; b < nb; ++b) { /* spatial::update_boundary (:2162-2187), then aux */
+      /* spatial::update_boundary (:2162-2187) at tn + c_{min(i+1, last)} h
+       * (src/solver/temporal_discretization.cpp:232-244), then aux */
+      int sb = (s + 1 < ns - 1) ? s + 1 : ns - 1;
+      for (int b = 0; b < nb; ++b) {
         tgts[b] = (s < ns - 1) ? zi[b] : ynext[b];
-        apply_bc(c, &c->blk[b], tgts[b]);
+        apply_bc(c, &c->blk[b], tgts[b], tn + ci[sb] * h);
       }
       if (c->ovs.n > 0) interpolate(c, tgts);
       for (int b = 0; b < nb; ++b) compute_aux(c, &c->blk[b], (s < ns - 1) ? zi[b] : ynext[b]);
@@ -1180,7 +1264,7 @@ int orc_get_setup(orc_ctx *c, int b, int what, double *out) {
     memset(out, 0, N * sizeof(double));
     for (int zi = 0; zi < bk->nbnd; ++zi) {
       bnd_t *z = &bk->bnd[zi];
-      if (z->kind != LEE_SPONGE_FREUND_AMBIENT) continue;
+      if (z->kind != LEE_SPONGE_FREUND_AMBIENT && z->kind != LEE_SPONGE_FREUND_HARMONICWAVE) continue;
       int bn0 = z->hi[0] - z->lo[0] + 1, bn1 = z->hi[1] - z->lo[1] + 1;
       for (int k = z->lo[2]; k <= z->hi[2]; ++k)
         for (int j = z->lo[1]; j <= z->hi[1]; ++j)

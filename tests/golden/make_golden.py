@@ -37,6 +37,12 @@ WORKLOADS = {
     "shear2d_40x32": lambda: cases.shear2d(nx=40, ny=32, nsteps=20),
     # 3-D curvilinear block with a slip wall, a Neumann face and a mean shear
     "wall3d_14": lambda: cases.wall3d(n=14, nsteps=4),
+    # 2-D acoustic plane wave: harmonic-wave Dirichlet face, centerline, all-zero face,
+    # Neumann face and a sponge relaxing toward the wave
+    "waves2d_40x32": lambda: cases.waves2d(nx=40, ny=32, nsteps=20),
+    # 3-D quarter round jet: Gaussian entropy wave face and sponge, two centerlines, Neumann
+    # faces, an ambient sponge
+    "jet3d_14": lambda: cases.jet3d(n=14, nsteps=4),
 }
 
 # Two-block overset workloads (run on one reference rank per block).

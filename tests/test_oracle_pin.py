@@ -15,7 +15,7 @@ import pytest
 from camille_b200 import api, cases
 from tests.conftest import golden_case, load_golden
 
-NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14"]
+NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "waves2d_40x32", "jet3d_14"]
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -63,7 +63,15 @@ def _live_cases():
     c3.filter_blend = 0.75
     c4 = cases.curvi3d(n=12, nsteps=2, mach=0.3, halfwidth=2.0)
     c4.filter_scheme = "NONE"
-    return {"fdo11p_sfo11p_3d": c1, "rk2_filter4_2d": c2, "blend_2d": c3, "nofilter_3d": c4}
+    # the wave forms the golden fixtures leave out (acoustic homogeneous along y, entropy
+    # homogeneous along z in 2-D), and the plane wave along y with RK2
+    W = cases.HarmonicWave
+    c5 = cases.waves2d(nx=24, ny=20, nsteps=6, wave=W("WAVE_ACOUSTIC", "WAVEFORM_HOMOGENEOUS", 1, 2e-3, 3.0))
+    c6 = cases.waves2d(nx=24, ny=20, nsteps=6, wave=W("WAVE_ENTROPY", "WAVEFORM_HOMOGENEOUS", 2, 1e-3, 5.0))
+    c7 = cases.jet3d(n=12, nsteps=3, wave=W("WAVE_ACOUSTIC", "WAVEFORM_PLANE", 1, 1e-3, 5.0))
+    c7.rk = "RUNGE_KUTTA2"
+    return {"fdo11p_sfo11p_3d": c1, "rk2_filter4_2d": c2, "blend_2d": c3, "nofilter_3d": c4,
+            "wave_acoustic_homogeneous_2d": c5, "wave_entropy_homogeneous_2d": c6, "wave_plane_rk2_3d": c7}
 
 
 @pytest.mark.parametrize("label", list(_live_cases().keys()))

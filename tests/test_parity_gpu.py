@@ -15,7 +15,7 @@ from camille_b200 import api, cases
 from tests.conftest import golden_case, load_golden
 
 pytestmark = pytest.mark.gpu
-NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14"]
+NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "waves2d_40x32", "jet3d_14"]
 
 
 def rl2(a, b):
@@ -78,8 +78,12 @@ def _larger():
     d.rk, d.filter_order, d.filter_blend = "RUNGE_KUTTA2", 4, 0.6
     e = cases.shear2d(nx=130, ny=96, nsteps=40)
     f = cases.wall3d(n=40, nsteps=8, halfwidth=3.0)
+    g = cases.waves2d(nx=96, ny=64, nsteps=40)
+    h = cases.jet3d(n=40, nsteps=10)
+    i = cases.waves2d(nx=64, ny=48, nsteps=20,
+                      wave=cases.HarmonicWave("WAVE_ENTROPY", "WAVEFORM_HOMOGENEOUS", 2, 1e-3, 4.0))
     return {"pulse2d_128": a, "curvi3d_40": b, "fdo11p_3d_24": c, "rk2_2d_64": d, "shear2d_130x96": e,
-            "wall3d_40": f}
+            "wall3d_40": f, "waves2d_96x64": g, "jet3d_40": h, "entropy2d_64x48": i}
 
 
 @pytest.mark.parametrize("label", list(_larger().keys()))
@@ -101,7 +105,8 @@ def test_fp64_matches_oracle(product_lib, oracle_lib, label):
     assert rl2(yp, yo) <= 1e-10
 
 
-@pytest.mark.parametrize("label", ["pulse2d_128", "curvi3d_40", "shear2d_130x96", "wall3d_40"])
+@pytest.mark.parametrize("label", ["pulse2d_128", "curvi3d_40", "shear2d_130x96", "wall3d_40", "waves2d_96x64",
+                                   "jet3d_40"])
 def test_fp32_compensated_error_vs_oracle(product_lib, oracle_lib, label):
     case = _larger()[label]
     o = api.Solver(oracle_lib, case)
@@ -272,6 +277,9 @@ def _graph_cases():
         "cylinder_nofilter": (lambda c: (setattr(c, "filter_scheme", "NONE"), c)[-1])(
             _overset_golden("cylinder2d_64")),
         "cylinder": _overset_golden("cylinder2d_64"),
+        # stage and update times read from the graph's time table
+        "waves2d": cases.waves2d(nx=64, ny=48, nsteps=11),
+        "jet3d_rk2": (lambda c: (setattr(c, "rk", "RUNGE_KUTTA2"), c)[-1])(cases.jet3d(n=20, nsteps=7)),
     }
 
 
@@ -294,3 +302,37 @@ def test_step_graphs_give_the_same_bits(product_lib, label, precision):
         yb, sb, tb = b.download(blk)
         assert (sa, ta) == (sb, tb)
         np.testing.assert_array_equal(ya, yb)
+
+
+@pytest.mark.parametrize("args,code", [
+    ((api.WAVE_ACOUSTIC, api.WAVEFORM_GAUSSIAN_ROUNDJET, 0, 0.1, 2.0, 1.0), api.LEE_ERR_ARG),
+    ((api.WAVE_ENTROPY, api.WAVEFORM_PLANE, 0, 0.1, 2.0, 0.0), api.LEE_ERR_ARG),
+    ((api.WAVE_ENTROPY, api.WAVEFORM_HOMOGENEOUS, 0, 1.5, 2.0, 0.0), api.LEE_ERR_ARG),
+    ((api.WAVE_ENTROPY, api.WAVEFORM_HOMOGENEOUS, 3, 0.1, 2.0, 0.0), api.LEE_ERR_ARG),
+    ((api.WAVE_ENTROPY, api.WAVEFORM_HOMOGENEOUS, 0, 0.1, 0.0, 0.0), api.LEE_ERR_ARG),
+    ((api.WAVE_ENTROPY, api.WAVEFORM_GAUSSIAN_ROUNDJET, 0, 0.1, 2.0, 0.0), api.LEE_ERR_ARG),
+    ((api.WAVE_ACOUSTIC, api.WAVEFORM_PLANE, 2, 0.1, 2.0, 0.0), api.LEE_ERR_UNSUPPORTED),
+])
+def test_harmonic_wave_arguments_are_checked(product_lib, args, code):
+    """lee_set_harmonic_wave refuses what the reference has no formula for, the amplitude
+    range of check_consistency_wave, and an acoustic wave along z in 2-D; a harmonic-wave
+    line without a wave stops lee_prepare."""
+    case = cases.waves2d(nx=24, ny=20, nsteps=1)
+    case.harmonic_wave = None
+    with pytest.raises(api.LeeError) as e:
+        api.Solver(product_lib, case)
+    assert e.value.code == api.LEE_ERR_STATE
+    case.harmonic_wave = cases.HarmonicWave("WAVE_ENTROPY", "WAVEFORM_HOMOGENEOUS", 0, 0.1, 2.0)
+    s = api.Solver(product_lib, case, upload=False, prepare=False)
+    assert product_lib.set_harmonic_wave(s.ctx, *args) == code
+
+
+def test_harmonic_sponge_blocks_run_the_generic_stage_kernel(product_lib):
+    """A block with a harmonic-wave sponge zone runs the stage kernel with the zone loop (the
+    TMA stage kernels read one summed strength field); the filter stays TMA-staged."""
+    case = cases.waves2d(nx=64, ny=48, nsteps=1)
+    s = api.Solver(product_lib, case)
+    info = s.info()
+    assert info.tma_stage == 0 and info.tma_filter == 1
+    case.boundaries = [b for b in case.boundaries if b.kind != "sponge_freund_harmonicwave"]
+    assert api.Solver(product_lib, case).info().tma_stage == 1

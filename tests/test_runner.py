@@ -108,9 +108,26 @@ def test_parse_only_overset_monopole_and_twocylinder(runner, tmp_path):
     assert info2["monopole"] == list(cases.TWOCYLINDER_SOURCE)
 
 
+def test_parse_only_reads_the_harmonic_wave(runner, tmp_path):
+    for case in (golden_case("waves2d_40x32"), golden_case("jet3d_14")):
+        wd = str(tmp_path / case.name)
+        case.write_reference_inputs(wd, 0.01, 2)
+        info = json.loads(_run(runner, wd, "--parse-only").stdout)
+        w = case.harmonic_wave
+        hw = w.halfwidth if w.form == "WAVEFORM_GAUSSIAN_ROUNDJET" else 0.0
+        assert info["wave"] == [cases.WAVE_TYPES[w.wave_type], cases.WAVE_FORMS[w.form], w.direction, w.amplitude,
+                                w.wavelength, hw]
+        assert [b[1] for b in info["bc"]] == [cases.BC_TYPES[bd.kind] for bd in case.boundaries]
+
+
 @pytest.mark.parametrize("key,value,message", [
     ("PHYSICAL_MODEL", "LINEAR_ACOUSTICS", "the library runs LEE"),
-    ("HARMONIC_WAVE", "PLANE", "HARMONIC_WAVE"),
+    # check_consistency_wave (src/core/input.cpp:629-656): an acoustic wave of another shape,
+    # and the amplitude range
+    ("HARMONIC_WAVE", "WAVE_ACOUSTIC, AMPLITUDE = 0.1, SHAPE = WAVEFORM_GAUSSIAN_ROUNDJET, DIRECTION = X, "
+     "WAVELENGTH = 2.0, HALFWIDTH = 1.0", "Unknown spatial distribution of acoustic waves."),
+    ("HARMONIC_WAVE", "WAVE_ENTROPY, AMPLITUDE = 1.5, SHAPE = WAVEFORM_HOMOGENEOUS, DIRECTION = Y, "
+     "WAVELENGTH = 2.0", "The wave amplitude should be between 0 and 1."),
     ("SIMULATION", "CASE_2DJET_WITH_A_HARMONIC_SOURCE", "CASE_2DJET_WITH_A_HARMONIC_SOURCE"),
     ("FIX_DT_OR_CFL", "FIX_NOTHING", "either DT or CFL"),
 ])
@@ -158,7 +175,8 @@ def _final_solution(wd, counter):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "cylinder2d_64"])
+@pytest.mark.parametrize("name", ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "cylinder2d_64",
+                                  "waves2d_40x32", "jet3d_14"])
 def test_fix_dt_run_matches_reference_and_solver(runner, product_lib, tmp_path, name):
     case = golden_case(name)
     g = load_golden(name)
