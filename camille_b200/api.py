@@ -29,6 +29,7 @@ FP64, FP32_COMPENSATED = 0, 1
 SOURCE_DISTRIBUTED = 2
 SETUP_METRICS, SETUP_JACOBIAN, SETUP_MEAN_GRADIENT, SETUP_SPONGE = 0, 1, 2, 3
 SOURCE_MONOPOLE = 1
+SOURCE_JET2D_HARMONIC = 3
 WAVE_NONE, WAVE_ACOUSTIC, WAVE_ENTROPY = 0, 1, 2
 WAVEFORM_PLANE, WAVEFORM_HOMOGENEOUS, WAVEFORM_GAUSSIAN_ROUNDJET = 0, 1, 2
 
@@ -79,6 +80,7 @@ SIGNATURES = {
     "set_mean": (C.c_int, [C.c_void_p, C.c_int, _PP]),
     "add_boundary": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP]),
     "set_harmonic_wave": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]),
+    "set_axisymmetric": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "set_source": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
     "set_block_source": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _DP, C.c_int]),
     "advance_blocks": (C.c_int, [C.c_void_p, C.c_int, _DP]),
@@ -187,6 +189,10 @@ class Solver:
                                            lo, hi, sig))
             if case.harmonic_wave is not None:
                 self._chk(lib.set_harmonic_wave(self.ctx, *case.harmonic_wave.args()))
+            if case.axisymmetric:
+                self._chk(lib.set_axisymmetric(self.ctx, 1, 0))
+            if case.simulation == "CASE_2DJET_WITH_A_HARMONIC_SOURCE":
+                self._chk(lib.set_source(self.ctx, SOURCE_JET2D_HARMONIC, None, 0))
             if case.source_monopole() is not None:
                 p = np.array(case.source_monopole(), np.float64)
                 self._chk(lib.set_source(self.ctx, SOURCE_MONOPOLE, _dptr(p), len(p)))

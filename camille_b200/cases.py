@@ -41,6 +41,7 @@ BC_TYPES = {
     "centerline_cart_norm2x": 900,
     "centerline_cart_norm2y": 901,
     "centerline_cart_norm2z": 902,
+    "centerline_axisym": 903,
     "sponge_freund_ambient": 1000,
     "sponge_freund_harmonicwave": 1002,
 }
@@ -169,6 +170,7 @@ class Case:
     distributed: Optional[DistributedSource] = None
     microphones: Optional[Microphones] = None
     harmonic_wave: Optional[HarmonicWave] = None
+    axisymmetric: bool = False  # AXISYMMETRY = TRUE, AXIS_OF_SYMMETRY = X (2-D: x axial, y radial)
     notes: str = ""
     # the deck's SIMULATION; CASE_SCATTERING_TWOCYLINDER brings the reference's own source
     simulation: str = "CASE_KBK_COMBUSTOR"
@@ -191,7 +193,7 @@ class Case:
         fix = "FIX_DT" if dt is not None else "FIX_CFL"
         lines = [
             f"DIMENSION = {self.num_dim}",
-            "AXISYMMETRY = FALSE",
+            "AXISYMMETRY = TRUE, AXIS_OF_SYMMETRY = X" if self.axisymmetric else "AXISYMMETRY = FALSE",
             "PHYSICAL_MODEL = LEE",
             "FLUID_MODEL = IDEAL_GAS_CALORIC",
             f"SIMULATION = {self.simulation}",
@@ -247,8 +249,9 @@ class Case:
         """Write grid, mean, restart, BC and deck files; return the restart path."""
         if self.distributed is not None:
             raise ValueError("the reference cannot express a distributed source")
-        if self.monopole is not None and self.simulation == "CASE_SCATTERING_TWOCYLINDER":
-            raise ValueError("a case-level monopole and the two-cylinder source do not combine")
+        if self.monopole is not None and self.simulation in ("CASE_SCATTERING_TWOCYLINDER",
+                                                             "CASE_2DJET_WITH_A_HARMONIC_SOURCE"):
+            raise ValueError("a case-level monopole and the case's own source do not combine")
         os.makedirs(workdir, exist_ok=True)
         grid, mean, ic, bc = (os.path.join(workdir, n) for n in ("grid.xyz", "mean.q", "ic.q", "bc.in"))
         plot3d.write_grid(grid, [(b.x, b.y, b.z) for b in self.blocks])
@@ -487,6 +490,69 @@ def jet3d(n: int = 14, nsteps: int = 4, gamma: float = 1.4, wave: Optional[Harmo
     return Case(name=f"jet3d_{n}", num_dim=3, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
                 sponge_constant=1.0, harmonic_wave=wave,
                 notes=f"3-D {n}^3 quarter jet, harmonic wave {wave.wave_type}/{wave.form}, centerlines")
+
+
+def axisym2d(nx: int = 48, nr: int = 32, spacing: float = 0.125, nsteps: int = 10, gamma: float = 1.4,
+             mach: float = 0.3, sponge: int = 6, halfwidth: float = 3.0) -> Case:
+    """Axisymmetric round jet in the (x, r) half-plane (AXISYMMETRY = TRUE, axis x): x on
+    [-(nx-1) d / 2, (nx-1) d / 2], r = y on [0, (nr-1) d] with the axis as the eta = 0 line;
+    mean u_bar = mach (1 - tanh((r - 1) / 0.25)) / 2 and an entropy layer of the same shape
+    (s_bar = 0.05 times it), v_bar = 0, p_bar = 1/gamma. BC lines: ``centerline_axisym`` on the
+    axis, ``neumann`` on eta = max, Freund sponges ``sponge`` cells wide at both x ends. A
+    Gaussian p' pulse sits on the axis."""
+    xs = (np.arange(nx, dtype=np.float64) - 0.5 * (nx - 1)) * spacing
+    rs = np.arange(nr, dtype=np.float64) * spacing
+    x = np.broadcast_to(xs[None, None, :], (1, nr, nx)).copy()
+    y = np.broadcast_to(rs[None, :, None], (1, nr, nx)).copy()
+    z = np.zeros_like(x)
+    prof = 0.5 * (1.0 - np.tanh((y - 1.0) / 0.25))
+    mean = np.zeros((5,) + x.shape)
+    mean[0] = 0.05 * prof
+    mean[1] = mach * prof
+    mean[4] = 1.0 / gamma
+    state = np.zeros((5,) + x.shape)
+    state[4] = 1e-3 * _gauss((x + 0.1 * xs[-1]) ** 2 + y * y, halfwidth * spacing)
+    blk = Block(x, y, z, mean, state)
+    mx, my = nx - 1, nr - 1
+    bnd = [Boundary(0, "centerline_axisym", 1, 0, (0, 0, 0), (mx, 0, 0)),
+           Boundary(0, "neumann", 1, 1, (0, my, 0), (mx, my, 0))]
+    if sponge > 0:
+        bnd += [b for b in sponge_frame(2, blk.dims, sponge) if b.dir == 0]
+    return Case(name=f"axisym2d_{nx}x{nr}", num_dim=2, blocks=[blk], gamma=gamma, nsteps=nsteps, boundaries=bnd,
+                sponge_constant=1.0, axisymmetric=True,
+                notes=f"2-D axisymmetric round jet {nx}x{nr}, axis centerline, sponges at both x ends")
+
+
+def jet2d_source(nx: int = 64, ny: int = 48, spacing: float = 0.25, nsteps: int = 10, gamma: float = 1.4,
+                 sponge: int = 8) -> Case:
+    """SIMULATION = CASE_2DJET_WITH_A_HARMONIC_SOURCE: the reference's own harmonic pressure
+    source (src/solver/source.cpp:27-58) in its parallel hot jet, on a Cartesian block centred on
+    the source with Freund sponges on all four sides. The mean is the one the reference's
+    initializer gives (State::initialize_state_linearizedEuler_2Djet_with_a_harmonic_source,
+    src/core/state.cpp:376-464: T_j = 600 K over 300 K ambient, M_j = 0.756, u_bar = u_j
+    exp(-ln 2 y^2), the Crocco-Busemann density of its eq. (19)); the state starts at zero."""
+    xs = (np.arange(nx, dtype=np.float64) - 0.5 * (nx - 1)) * spacing
+    ys = (np.arange(ny, dtype=np.float64) - 0.5 * (ny - 1)) * spacing
+    x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
+    y = np.broadcast_to(ys[None, :, None], (1, ny, nx)).copy()
+    z = np.zeros_like(x)
+    pbar = 1.0 / gamma
+    tj = 600.0 / ((gamma - 1.0) * 300.0)
+    cj = math.sqrt((gamma - 1.0) * tj)
+    uj = 0.756 * cj
+    rhoj = pbar * gamma / (gamma - 1.0) / tj
+    ubar = uj * np.exp(-math.log(2.0) * y ** 2)
+    rhobar = 1.0 / (-0.5 * (gamma - 1.0) * (ubar - uj) * ubar + ubar / (rhoj * uj) + (uj - ubar) / uj)
+    mean = np.zeros((5,) + x.shape)
+    mean[0] = (0.0 - gamma * np.log(rhobar)) / gamma
+    mean[1] = ubar
+    mean[4] = pbar
+    state = np.zeros((5,) + x.shape)
+    blk = Block(x, y, z, mean, state)
+    bnd = sponge_frame(2, blk.dims, sponge) if sponge > 0 else []
+    return Case(name=f"jet2d_source_{nx}x{ny}", num_dim=2, blocks=[blk], gamma=gamma, nsteps=nsteps,
+                boundaries=bnd, sponge_constant=1.0, simulation="CASE_2DJET_WITH_A_HARMONIC_SOURCE",
+                notes=f"2-D {nx}x{ny} hot jet with the reference's harmonic pressure source")
 
 
 def _tanh_radii(nr: int, r0: float, r1: float, first: float) -> tuple[np.ndarray, float]:

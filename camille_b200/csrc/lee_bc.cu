@@ -9,8 +9,8 @@
 //  - wall_slip_kinematic (:448-494): s' and p' as Neumann; the velocity is taken to the
 //    contravariant components with the metrics, the wall-normal one is set to zero, and it
 //    is brought back with the inverse metrics times J;
-//  - centerline_cart_norm2x/y/z (:141-148, :498-574): Neumann, then the velocity component
-//    along x/y/z is set to zero;
+//  - centerline_cart_norm2x/y/z and centerline_axisym (:141-156, :498-574): Neumann, then the
+//    velocity component along x/y/z (u_r', the second one, on the axis) is set to zero;
 //  - dirichlet_allzero (:213-228): every slot zero;
 //  - dirichlet_harmonicwave (:232-344): the time-harmonic wave at the update's time
 //    (tn + c_{min(i+1, last)} h, RungeKutta::integrate, src/solver/temporal_discretization.cpp:232-244).
@@ -61,9 +61,10 @@ __global__ void k_bc(BcParams<T> p) {
     double out[kMaxVars];
     if (p.kind == LEE_BC_NEUMANN) {
       for (int v = 0; v < p.V; ++v) out[v] = neumann<T, PAIR>(p, v, l);
-    } else if (p.kind >= LEE_BC_CENTERLINE_CART_NORM2X && p.kind <= LEE_BC_CENTERLINE_CART_NORM2Z) {
+    } else if (p.kind >= LEE_BC_CENTERLINE_CART_NORM2X && p.kind <= LEE_BC_CENTERLINE_AXISYM) {
       for (int v = 0; v < p.V; ++v) out[v] = neumann<T, PAIR>(p, v, l);
-      const int d = p.kind - LEE_BC_CENTERLINE_CART_NORM2X;
+      // the velocity along x/y/z, or u_r' (IVAR_UR, the second component) on the axis
+      const int d = p.kind == LEE_BC_CENTERLINE_AXISYM ? 1 : p.kind - LEE_BC_CENTERLINE_CART_NORM2X;
       if (d < p.nd) out[1 + d] = 0.0;
     } else if (p.kind == LEE_BC_DIRICHLET_ALLZERO) {
       for (int v = 0; v < p.V; ++v) out[v] = 0.0;

@@ -129,6 +129,7 @@ struct lee_ctx {
   double src[7] = {0, 0, 0, 0, 0, 0, 0};
   Wave wave{};               // lee_set_harmonic_wave (type LEE_WAVE_NONE until set)
   bool wave_time = false;    // some BC line or sponge zone reads the wave (from lee_prepare)
+  bool axisym = false;       // lee_set_axisymmetric
   std::vector<double> dsrc;  // distributed source parameters (LEE_SOURCE_DISTRIBUTED)
   bool prepared = false, uploaded = false;
   int step = 0;
@@ -236,12 +237,12 @@ bool is_sponge(int kind) { return kind == LEE_SPONGE_FREUND_AMBIENT || kind == L
 bool is_bc_line(int kind) {
   return kind == LEE_BC_NEUMANN || kind == LEE_BC_WALL_SLIP_KINEMATIC || kind == LEE_BC_DIRICHLET_ALLZERO ||
          kind == LEE_BC_DIRICHLET_HARMONICWAVE ||
-         (kind >= LEE_BC_CENTERLINE_CART_NORM2X && kind <= LEE_BC_CENTERLINE_CART_NORM2Z);
+         (kind >= LEE_BC_CENTERLINE_CART_NORM2X && kind <= LEE_BC_CENTERLINE_AXISYM);
 }
 // BC lines whose face values come from the closure row of the difference operator
 bool reads_inward(int kind) {
   return kind == LEE_BC_NEUMANN || kind == LEE_BC_WALL_SLIP_KINEMATIC ||
-         (kind >= LEE_BC_CENTERLINE_CART_NORM2X && kind <= LEE_BC_CENTERLINE_CART_NORM2Z);
+         (kind >= LEE_BC_CENTERLINE_CART_NORM2X && kind <= LEE_BC_CENTERLINE_AXISYM);
 }
 bool reads_wave(int kind) { return kind == LEE_BC_DIRICHLET_HARMONICWAVE || kind == LEE_SPONGE_FREUND_HARMONICWAVE; }
 
@@ -623,6 +624,8 @@ void fill_stage_common(lee_ctx* c, BlockData& b, StageParams<T>& p) {
     zn.sig = dbl ? (const T*)z.d_sigma : (const T*)z.d_sigma_t;
     zn.ref = (const T*)z.d_ref;
   }
+  p.axisym = c->axisym ? 1 : 0;
+  p.ry = b.d_xyz[1];
   p.has_src = b.d_src_g != nullptr;
   for (int d = 0; d < 3; ++d) { p.src_lo[d] = b.src_lo[d]; p.src_hi[d] = b.src_hi[d]; }
   p.src_g = dbl ? (const T*)b.d_src_g : (const T*)b.d_src_g_t;
@@ -719,8 +722,30 @@ const double* monopole_of(const lee_ctx* c, const BlockData& b) {
   return nullptr;
 }
 
+// The constants of CASE_2DJET_WITH_A_HARMONIC_SOURCE's source (src/solver/source.cpp:30-49), in
+// the reference's order: amplitude, angular frequency, Bx, By.
+void jet2d_constants(double gamma, double* amp, double* omega, double* bx, double* by) {
+  const double twopi = 2.0 * acos(-1.0), inverse_twopi = 1.0 / twopi;  // src/math/math.cpp:7-10
+  double amplitude = 0.001, frequency = 76.0, Bx = 0.04 * log(2.0), By = 0.32 * log(2.0);
+  const double b = 1.3, R = 287.0, rhoinfty = 1.184, Tinfty = 300.0;
+  const double cinfty = sqrt(gamma * R * Tinfty);
+  amplitude /= rhoinfty * pow(cinfty, 2) / (b / cinfty);
+  frequency *= inverse_twopi * (b / cinfty);
+  Bx *= pow(b, 2);
+  By *= pow(b, 2);
+  *amp = amplitude;
+  *omega = frequency * twopi;
+  *bx = Bx;
+  *by = By;
+}
+
 double source_amp(const lee_ctx* c, const BlockData& b, double t) {
   if (c->src_kind == LEE_SOURCE_DISTRIBUTED) return (c->cfg.gamma - 1.0) * sin(c->dsrc[1] * t);
+  if (c->src_kind == LEE_SOURCE_JET2D_HARMONIC && b.src_mode == 0) {
+    double amp, om, bx, by;
+    jet2d_constants(c->cfg.gamma, &amp, &om, &bx, &by);
+    return amp * cos(om * t);
+  }
   const double* m = monopole_of(c, b);
   if (!m) return 0.0;
   double T = m[6];
@@ -1194,7 +1219,7 @@ bool closures_within_halo(const OpTable& op) {
 }
 
 bool batch_eligible(const lee_ctx* c) {
-  if (c->cfg.num_dim != 2 || c->ovs.n > 0) return false;
+  if (c->cfg.num_dim != 2 || c->ovs.n > 0 || c->axisym) return false;
   if (!(c->fd.h == 2 && c->fd.S == 3)) return false;
   if (c->cfg.filter_scheme != LEE_FILTER_STANDARD_CENTRAL || c->cfg.filter_order != 8) return false;
   if (!(c->flt.h == 4 && c->flt.S == 7 && c->fltd.h == 4 && c->fltd.S == 7)) return false;
@@ -1868,6 +1893,7 @@ int adjoint_setup(lee_ctx* c) {
   if (c->blk.size() != 1) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint covers single-block contexts");
   BlockData& b = c->blk[0];
   if (b.has_iblank || c->ovs.n > 0) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no holes or overset");
+  if (c->axisym) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no axisymmetric term");
   for (auto& z : b.bnd) {
     if (z.kind == LEE_SPONGE_FREUND_HARMONICWAVE)
       return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no harmonic-wave sponge");
@@ -2232,10 +2258,29 @@ int lee_set_harmonic_wave(lee_ctx* c, int type, int form, int dir, double amplit
   return LEE_OK;
 }
 
+int lee_set_axisymmetric(lee_ctx* c, int on, int axis) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_axisymmetric after lee_prepare");
+  if (!on) {
+    c->axisym = false;
+    return LEE_OK;
+  }
+  if (c->cfg.num_dim != 2) return fail(c, LEE_ERR_ARG, "Axisymmetry requires 2-D.");
+  if (axis != 0) return fail(c, LEE_ERR_ARG, "The axis of symmetry should be x by definition of the coordinate system.");
+  c->axisym = true;
+  return LEE_OK;
+}
+
 int lee_set_source(lee_ctx* c, int kind, const double* params, int nparams) {
   if (!c) return LEE_ERR_ARG;
   if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_source after lee_prepare");
   if (kind == LEE_SOURCE_NONE) {
+    c->src_kind = kind;
+    return LEE_OK;
+  }
+  if (kind == LEE_SOURCE_JET2D_HARMONIC) {
+    for (auto& b : c->blk)
+      if (b.src_mode == 1) return fail(c, LEE_ERR_UNSUPPORTED, "a block has its own monopole");
     c->src_kind = kind;
     return LEE_OK;
   }
@@ -2271,6 +2316,7 @@ int lee_set_block_source(lee_ctx* c, int b, int kind, const double* params, int 
   }
   if (kind != LEE_SOURCE_MONOPOLE || !params || nparams != 7) return fail(c, LEE_ERR_ARG, "monopole takes 7 params");
   if (!(params[5] > 0.0)) return fail(c, LEE_ERR_ARG, "monopole half-width must be positive");
+  if (c->src_kind == LEE_SOURCE_JET2D_HARMONIC) return fail(c, LEE_ERR_UNSUPPORTED, "the 2-D jet source is set");
   bk.src_mode = 1;
   for (int q = 0; q < 7; ++q) bk.own_src[q] = params[q];
   if (c->src_kind == LEE_SOURCE_NONE) c->src_kind = LEE_SOURCE_MONOPOLE;  // other blocks keep none
@@ -2574,6 +2620,40 @@ int lee_prepare(lee_ctx* c) {
         }
       }
     }
+    if (c->src_kind == LEE_SOURCE_JET2D_HARMONIC && b.src_mode == 0) {
+      // exp(-(Bx x x + By y y)) on the box where it is nonzero in FP64, computed here in FP64
+      double amp, om, bx, by;
+      jet2d_constants(c->cfg.gamma, &amp, &om, &bx, &by);
+      auto arg = [&](long long l) {
+        const double x = b.hx[(size_t)l], y = b.hy[(size_t)l];
+        return -(bx * x * x + by * y * y);
+      };
+      int lo[3] = {b.nx, b.ny, b.nz}, hi[3] = {-1, -1, -1};
+      for (long long l = 0; l < b.N; ++l)
+        if (exp(arg(l)) != 0.0) {
+          int ijk[3] = {(int)(l % b.nx), (int)((l / b.nx) % b.ny), (int)(l / ((long long)b.nx * b.ny))};
+          for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], ijk[d]);
+            hi[d] = std::max(hi[d], ijk[d]);
+          }
+        }
+      if (hi[0] >= 0) {
+        std::vector<double> g((size_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1));
+        size_t q = 0;
+        for (int k = lo[2]; k <= hi[2]; ++k)
+          for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) g[q++] = exp(arg(i + (long long)b.nx * (j + (long long)b.ny * k)));
+        if ((rc = upload(c, &b.d_src_g, g))) return rc;
+        for (int d = 0; d < 3; ++d) { b.src_lo[d] = lo[d]; b.src_hi[d] = hi[d]; }
+        if (c->comp) {
+          float* f = nullptr;
+          if ((rc = dalloc(c, &f, g.size()))) return rc;
+          k_convert<float><<<grid1d((long long)g.size()), 256, 0, s>>>((long long)g.size(), f, b.d_src_g);
+          CK(cudaGetLastError());
+          b.d_src_g_t = f;
+        }
+      }
+    }
     if (c->src_kind == LEE_SOURCE_DISTRIBUTED && (int)(&b - &c->blk[0]) == (int)c->dsrc[0]) {
       int lo[3], hi[3];
       std::vector<double> g;
@@ -2657,7 +2737,8 @@ int lee_prepare(lee_ctx* c) {
     // (and the harmonic-wave sponge, an RHS term of the generic kernel's zone loop, is absent)
     bool wave_zone = false;
     for (auto& z : b.bnd) wave_zone |= z.kind == LEE_SPONGE_FREUND_HARMONICWAVE;
-    b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32) && !wave_zone;
+    b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32) && !wave_zone &&
+            !c->axisym;
     b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE &&
                    (unsigned long long)b.N < (1ull << 32);
     // the kernels are a fixed choice (they round differently, and two contexts of one case give

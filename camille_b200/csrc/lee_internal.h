@@ -119,6 +119,9 @@ struct StageParams {
   int nzones;
   Zone<T> zones[kMaxZones];
   const T* sigma;
+  // axisymmetric term of the pressure equation (2-D): the r coordinate (y) when on
+  int axisym;
+  const double* ry;
   // monopole source: rhs[p] += amp * g, g on a box (src_lo..src_hi), i fastest; amp is src_amp,
   // or, in a replayed step graph, amp_tab[*step_ctr * nstages + stage]
   int has_src;

@@ -125,6 +125,15 @@ __device__ __forceinline__ void rhs_update(const StageParams<T>& p, I l, int i, 
   } else {
     rhs_mean_terms<T, DIM, TR>(p, l, g, q, ub, r);
   }
+  if constexpr (DIM == 2 && !(TR & kTrTma)) {
+    if (p.axisym) {
+      // -gamma (p_bar u_r' + p' u_r_bar) / (r + DUMMY_SMALL), in FP64 in the reference's order
+      // (src/solver/spatial_discretization.cpp:2118-2126)
+      const double pb = (double)cval(p.pbar, l), ur = (double)cval(p.ubar[1], l);
+      const double num = __dadd_rn(__dmul_rn(pb, (double)q[2]), __dmul_rn((double)q[P], ur));
+      r[P] -= (T)__ddiv_rn(__dmul_rn((double)p.gamma, num), __dadd_rn(p.ry[l], 1e-99));
+    }
+  }
   if (p.has_src && i >= p.src_lo[0] && i <= p.src_hi[0] && j >= p.src_lo[1] && j <= p.src_hi[1] &&
       k >= p.src_lo[2] && k <= p.src_hi[2]) {
     int b0 = p.src_hi[0] - p.src_lo[0] + 1, b1 = p.src_hi[1] - p.src_lo[1] + 1;

@@ -249,6 +249,7 @@ int bc_kind(const std::string& s) {
   if (s == "centerline_cart_norm2x") return LEE_BC_CENTERLINE_CART_NORM2X;
   if (s == "centerline_cart_norm2y") return LEE_BC_CENTERLINE_CART_NORM2Y;
   if (s == "centerline_cart_norm2z") return LEE_BC_CENTERLINE_CART_NORM2Z;
+  if (s == "centerline_axisym") return LEE_BC_CENTERLINE_AXISYM;
   if (s == "sponge_freund_ambient") return LEE_SPONGE_FREUND_AMBIENT;
   if (s == "sponge_freund_harmonicwave") return LEE_SPONGE_FREUND_HARMONICWAVE;
   die("boundary type " + s + " is not implemented by the library");
@@ -309,6 +310,8 @@ struct Run {
   int num_time_steps = 0, report_freq = 1, overset_order = 0;
   bool has_monopole = false;
   double monopole[7] = {};
+  bool axisym = false;
+  bool jet2d = false;  // SIMULATION = CASE_2DJET_WITH_A_HARMONIC_SOURCE
   // HARMONIC_WAVE (type LEE_WAVE_NONE when the deck says NONE)
   int wave_type = LEE_WAVE_NONE, wave_form = -1, wave_dir = 0;
   double wave_amp = 0.0, wave_len = 0.0, wave_hw = 0.0;
@@ -317,7 +320,19 @@ struct Run {
 Run configure(const Deck& d, int precision) {
   Run r;
   if (d.str("PHYSICAL_MODEL") != "LEE") die("PHYSICAL_MODEL " + d.str("PHYSICAL_MODEL") + ": the library runs LEE");
-  if (d.has("AXISYMMETRY") && d.str("AXISYMMETRY") != "FALSE") die("AXISYMMETRY is not implemented by the library");
+  std::string axisym = d.has("AXISYMMETRY") ? d.str("AXISYMMETRY") : "FALSE";
+  for (auto& ch : axisym) ch = (char)std::toupper((unsigned char)ch);  // truefalse_2int (:786-799)
+  if (axisym == "TRUE") {
+    // src/core/input.cpp:105-108 and check_consistency_dimension (:519-535)
+    std::string axis = d.str("AXISYMMETRY", "AXIS_OF_SYMMETRY");
+    for (auto& ch : axis) ch = (char)std::toupper((unsigned char)ch);
+    if (axis != "X" && axis != "Y" && axis != "R" && axis != "Z") die("AXIS_OF_SYMMETRY " + axis);
+    if (d.i("DIMENSION") != 2) die("Axisymmetry requires 2-D.");
+    if (axis != "X") die("The axis of symmetry should be x by definition of the coordinate system.");
+    r.axisym = true;
+  } else if (axisym != "FALSE") {
+    die("AXISYMMETRY " + axisym);
+  }
   if (d.has("HARMONIC_WAVE") && d.str("HARMONIC_WAVE") != "NONE") {
     // src/core/input.cpp:219-231, then check_consistency_wave (:629-656), whose else clauses
     // bind to the inner ifs: only an acoustic wave of another shape and the amplitude range
@@ -351,8 +366,8 @@ Run configure(const Deck& d, int precision) {
   c.precision = precision;
   // physical source by case (source::apply_physicalSource, src/solver/source.cpp:22-107)
   r.simulation = d.has("SIMULATION") ? d.str("SIMULATION") : "NONE";
-  if (r.simulation == "CASE_2DJET_WITH_A_HARMONIC_SOURCE")
-    die("the source of CASE_2DJET_WITH_A_HARMONIC_SOURCE is not implemented by the library");
+  // the 2-D jet's harmonic pressure source (src/solver/source.cpp:27-58): LEE_SOURCE_JET2D_HARMONIC
+  r.jet2d = r.simulation == "CASE_2DJET_WITH_A_HARMONIC_SOURCE";
   if (r.simulation == "CASE_SCATTERING_TWOCYLINDER") {
     // (gamma - 1) exp(-ln 2 r^2 / 0.2^2) sin(4 2pi t), ramped by sin^2(pi t / 8) up to t = 4
     // (src/solver/source.cpp:60-92): the library's monopole at the origin.
@@ -365,6 +380,7 @@ Run configure(const Deck& d, int precision) {
     if (b.size() != 7) die("SOURCE_MONOPOLE takes x0, y0, z0, amplitude, omega, halfwidth, ramp_time");
     for (int q = 0; q < 7; ++q) r.monopole[q] = std::atof(b[(size_t)q].c_str());
     r.has_monopole = true;
+    if (r.jet2d) die("SOURCE_MONOPOLE does not combine with the source of CASE_2DJET_WITH_A_HARMONIC_SOURCE");
   }
   // time advance (src/core/input.cpp:129-139)
   r.fix = d.str("FIX_DT_OR_CFL");
@@ -450,8 +466,9 @@ void print_parse(const Run& r, const std::vector<Block>& blocks, const std::vect
   } else {
     std::printf("null");
   }
-  std::printf(", \"wave\": [%d, %d, %d, %.17g, %.17g, %.17g]", r.wave_type, r.wave_form, r.wave_dir, r.wave_amp,
-              r.wave_len, r.wave_hw);
+  std::printf(", \"wave\": [%d, %d, %d, %.17g, %.17g, %.17g], \"axisym\": %s, \"jet2d\": %s", r.wave_type,
+              r.wave_form, r.wave_dir, r.wave_amp, r.wave_len, r.wave_hw, r.axisym ? "true" : "false",
+              r.jet2d ? "true" : "false");
   std::printf(", \"bc\": [");
   for (size_t q = 0; q < bcs.size(); ++q)
     std::printf("%s[%d, %d, %d, %d, %d, %d, %d, %d, %d, %d]", q ? ", " : "", bcs[q].block, bcs[q].kind, bcs[q].dir,
@@ -517,7 +534,9 @@ int main(int argc, char** argv) {
     check(c, lee_set_harmonic_wave(c, r.wave_type, r.wave_form, r.wave_dir, r.wave_amp, r.wave_len, r.wave_hw),
           "HARMONIC_WAVE");
   }
+  if (r.axisym) check(c, lee_set_axisymmetric(c, 1, 0), "AXISYMMETRY");
   if (r.has_monopole) check(c, lee_set_source(c, LEE_SOURCE_MONOPOLE, r.monopole, 7), "source");
+  if (r.jet2d) check(c, lee_set_source(c, LEE_SOURCE_JET2D_HARMONIC, nullptr, 0), "source");
   if (r.overset != "NONE") check(c, lee_read_overset_file(c, r.overset_file.c_str(), r.overset_order), "overset file");
   check(c, lee_prepare(c), "lee_prepare");
   for (size_t b = 0; b < blocks.size(); ++b) {

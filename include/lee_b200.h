@@ -69,6 +69,7 @@ extern "C" {
 #define LEE_BC_CENTERLINE_CART_NORM2X 900  /* Neumann, then u' = 0 (v' for 901, w' for 902) */
 #define LEE_BC_CENTERLINE_CART_NORM2Y 901
 #define LEE_BC_CENTERLINE_CART_NORM2Z 902
+#define LEE_BC_CENTERLINE_AXISYM 903       /* Neumann, then u_r' (v') = 0 */
 #define LEE_SPONGE_FREUND_AMBIENT 1000
 #define LEE_SPONGE_FREUND_HARMONICWAVE 1002  /* relaxes toward the harmonic wave */
 
@@ -90,6 +91,12 @@ extern "C" {
  * params: block, omega, cx, cy, cz, ox, oy, oz, hx, hy, hz, then cx*cy*cz amplitudes
  * (p fastest). In 2-D, cz = 1. */
 #define LEE_SOURCE_DISTRIBUTED 2
+/* The pressure source of SIMULATION = CASE_2DJET_WITH_A_HARMONIC_SOURCE (source::apply_physicalSource,
+ * src/solver/source.cpp:27-58), no params: rhs[p'] += exp(-(Bx x^2 + By y^2)) A cos(2 pi f t) with
+ * the reference's constants made non-dimensional by b = 1.3, c_inf = sqrt(gamma 287 300),
+ * rho_inf = 1.184 (A = 0.001 b / (rho_inf c_inf^3), f = 76 b / (2 pi c_inf), Bx = 0.04 ln 2 b^2,
+ * By = 0.32 ln 2 b^2). */
+#define LEE_SOURCE_JET2D_HARMONIC 3
 
 /* lee_get_setup selectors: products of the one-time setup, per block */
 #define LEE_SETUP_METRICS 0     /* 9 fields, metrics[l][i] = (1/J) dxi_l/dx_i, row-major (l*3+i) */
@@ -157,6 +164,13 @@ int lee_add_boundary(lee_ctx *ctx, int b, int kind, int dir, int end, const int 
  * for); LEE_ERR_UNSUPPORTED for an acoustic wave along Z in 2-D (its w' has no slot here). */
 int lee_set_harmonic_wave(lee_ctx *ctx, int type, int form, int dir, double amplitude, double wavelength,
                           double halfwidth);
+/* AXISYMMETRY = TRUE with AXIS_OF_SYMMETRY = axis (src/core/input.cpp:105-108): the 2-D block is
+ * the (x, r) half-plane with r = y, v' = u_r', and the pressure right-hand side gains
+ * -gamma (p_bar v' + p' v_bar) / (y + 1e-99) (compute_RHS_linearized_Euler,
+ * src/solver/spatial_discretization.cpp:2118-2126). Before lee_prepare; on = 0 turns it off.
+ * LEE_ERR_ARG unless num_dim is 2 and axis is 0 (X) (check_consistency_dimension,
+ * src/core/input.cpp:519-535). */
+int lee_set_axisymmetric(lee_ctx *ctx, int on, int axis);
 /* Physical source (source::apply_physicalSource, src/solver/source.cpp:22-107). */
 int lee_set_source(lee_ctx *ctx, int kind, const double *params, int nparams);
 /* A source for block b only (no reference counterpart: the reference applies its source to

@@ -92,6 +92,7 @@ struct orc_ctx {
   /* time-harmonic wave (UserInput::harmonicWave_*, src/core/input.cpp:219-231) */
   int wave_type, wave_form, wave_dir;
   double wave_amp, wave_len, wave_hw;
+  int axisym; /* UserInput::axisym (src/core/input.cpp:105-108) */
   char err[512];
 };
 typedef struct orc_ctx orc_ctx;
@@ -521,11 +522,30 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
   free(df);
   free(work);
   if (rc) return rc;
+  if (c->axisym) /* additional terms due to axisymmetry (:2118-2126), IVAR_UR = 2, RDIR = 1 */
+    for (int p = 0; p < N; ++p)
+      rhs[4][p] -= g * (bk->mean[4][p] * y[2][p] + y[4][p] * bk->mean[2][p]) / (bk->xyz[1][p] + 1e-99);
   if (c->src_kind == LEE_SOURCE_DISTRIBUTED && bk == &c->blk[(int)c->dsrc[0]] && c->dsrc_g) {
     double fac = (g - 1.0) * sin(c->dsrc[1] * time);
     for (int p = 0; p < N; ++p) rhs[4][p] += fac * c->dsrc_g[p];
   }
   int bix = (int)(bk - &c->blk[0]);
+  if (c->src_kind == LEE_SOURCE_JET2D_HARMONIC && c->bsrc_mode[bix] == 0) { /* source.cpp:27-58 */
+    double twopi = 2.0 * acos(-1.0), inverse_twopi = 1.0 / twopi;
+    double amplitude = 0.001, frequency = 76.0, Bx = 0.04 * log(2.0), By = 0.32 * log(2.0);
+    double b = 1.3, R = 287.0, rhoinfty = 1.184, Tinfty = 300.0;
+    double cinfty = sqrt(g * R * Tinfty);
+    amplitude /= rhoinfty * pow(cinfty, 2) / (b / cinfty);
+    frequency *= inverse_twopi * (b / cinfty);
+    Bx *= pow(b, 2);
+    By *= pow(b, 2);
+    double angular_frequency = frequency * twopi;
+    double amp_cos_wt = amplitude * cos(angular_frequency * time);
+    for (int p = 0; p < N; ++p) {
+      double xloc = bk->xyz[0][p], yloc = bk->xyz[1][p];
+      rhs[4][p] += exp(-(Bx * xloc * xloc + By * yloc * yloc)) * amp_cos_wt;
+    }
+  }
   const double *mp = c->bsrc_mode[bix] == 1 ? c->bsrc[bix]
                    : (c->bsrc_mode[bix] == 0 && c->src_kind == LEE_SOURCE_MONOPOLE && c->src[5] > 0.0) ? c->src
                    : NULL;
@@ -577,7 +597,7 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y, double time) {
   const op_t *o = &c->fd;
   for (int zi = 0; zi < bk->nbnd; ++zi) {
     bnd_t *z = &bk->bnd[zi];
-    int centerline = z->kind >= LEE_BC_CENTERLINE_CART_NORM2X && z->kind <= LEE_BC_CENTERLINE_CART_NORM2Z;
+    int centerline = z->kind >= LEE_BC_CENTERLINE_CART_NORM2X && z->kind <= LEE_BC_CENTERLINE_AXISYM;
     int dirichlet = z->kind == LEE_BC_DIRICHLET_ALLZERO || z->kind == LEE_BC_DIRICHLET_HARMONICWAVE;
     if (z->kind != LEE_BC_NEUMANN && z->kind != LEE_BC_WALL_SLIP_KINEMATIC && !centerline && !dirichlet) continue;
     int lo[3] = {z->lo[0], z->lo[1], z->lo[2]}, hi[3] = {z->hi[0], z->hi[1], z->hi[2]};
@@ -638,7 +658,8 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y, double time) {
             }
             for (int q = 0; q < 3; ++q) data[1 + q][lb] = vel[q];
           }
-          if (centerline && !hole) data[1 + (z->kind - LEE_BC_CENTERLINE_CART_NORM2X)][lb] = 0.0;
+          if (centerline && !hole) /* IVAR_UX + which_dir, or IVAR_UR on the axis */
+            data[z->kind == LEE_BC_CENTERLINE_AXISYM ? 2 : 1 + (z->kind - LEE_BC_CENTERLINE_CART_NORM2X)][lb] = 0.0;
         }
     for (int k = lo[2]; k <= hi[2]; ++k)
       for (int j = lo[1]; j <= hi[1]; ++j)
@@ -808,6 +829,18 @@ int orc_set_harmonic_wave(orc_ctx *c, int type, int form, int dir, double amplit
   c->wave_amp = amplitude;
   c->wave_len = wavelength;
   c->wave_hw = halfwidth;
+  return LEE_OK;
+}
+
+/* AXISYMMETRY (src/core/input.cpp:105-108) with check_consistency_dimension (:519-535). */
+int orc_set_axisymmetric(orc_ctx *c, int on, int axis) {
+  if (!on) {
+    c->axisym = 0;
+    return LEE_OK;
+  }
+  if (c->cfg.num_dim != 2) return fail(c, LEE_ERR_ARG, "Axisymmetry requires 2-D.");
+  if (axis != 0) return fail(c, LEE_ERR_ARG, "The axis of symmetry should be x by definition of the coordinate system.");
+  c->axisym = 1;
   return LEE_OK;
 }
 

@@ -43,6 +43,8 @@ WORKLOADS = {
     # 3-D quarter round jet: Gaussian entropy wave face and sponge, two centerlines, Neumann
     # faces, an ambient sponge
     "jet3d_14": lambda: cases.jet3d(n=14, nsteps=4),
+    # axisymmetric round jet: the 1/r pressure term, the axis centerline, a sheared mean
+    "axisym2d_48x32": lambda: cases.axisym2d(nx=48, nr=32, nsteps=20),
 }
 
 # Two-block overset workloads (run on one reference rank per block).

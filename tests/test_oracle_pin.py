@@ -15,7 +15,7 @@ import pytest
 from camille_b200 import api, cases
 from tests.conftest import golden_case, load_golden
 
-NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "waves2d_40x32", "jet3d_14"]
+NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "waves2d_40x32", "jet3d_14", "axisym2d_48x32"]
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -70,7 +70,10 @@ def _live_cases():
     c6 = cases.waves2d(nx=24, ny=20, nsteps=6, wave=W("WAVE_ENTROPY", "WAVEFORM_HOMOGENEOUS", 2, 1e-3, 5.0))
     c7 = cases.jet3d(n=12, nsteps=3, wave=W("WAVE_ACOUSTIC", "WAVEFORM_PLANE", 1, 1e-3, 5.0))
     c7.rk = "RUNGE_KUTTA2"
-    return {"fdo11p_sfo11p_3d": c1, "rk2_filter4_2d": c2, "blend_2d": c3, "nofilter_3d": c4,
+    c8 = cases.axisym2d(nx=32, nr=20, nsteps=6)
+    c8.rk, c8.filter_scheme, c8.filter_strength = "RUNGE_KUTTA2", "SFO11P", 0.25
+    c9 = cases.jet2d_source(nx=40, ny=32, nsteps=8)
+    return {"axisym_rk2_sfo11p_2d": c8, "jet2d_source_2d": c9, "fdo11p_sfo11p_3d": c1, "rk2_filter4_2d": c2, "blend_2d": c3, "nofilter_3d": c4,
             "wave_acoustic_homogeneous_2d": c5, "wave_entropy_homogeneous_2d": c6, "wave_plane_rk2_3d": c7}
 
 

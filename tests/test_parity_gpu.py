@@ -15,7 +15,7 @@ from camille_b200 import api, cases
 from tests.conftest import golden_case, load_golden
 
 pytestmark = pytest.mark.gpu
-NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "waves2d_40x32", "jet3d_14"]
+NAMES = ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "waves2d_40x32", "jet3d_14", "axisym2d_48x32"]
 
 
 def rl2(a, b):
@@ -82,8 +82,11 @@ def _larger():
     h = cases.jet3d(n=40, nsteps=10)
     i = cases.waves2d(nx=64, ny=48, nsteps=20,
                       wave=cases.HarmonicWave("WAVE_ENTROPY", "WAVEFORM_HOMOGENEOUS", 2, 1e-3, 4.0))
+    j = cases.axisym2d(nx=128, nr=80, nsteps=40)
+    k = cases.jet2d_source(nx=160, ny=96, nsteps=40)
     return {"pulse2d_128": a, "curvi3d_40": b, "fdo11p_3d_24": c, "rk2_2d_64": d, "shear2d_130x96": e,
-            "wall3d_40": f, "waves2d_96x64": g, "jet3d_40": h, "entropy2d_64x48": i}
+            "wall3d_40": f, "waves2d_96x64": g, "jet3d_40": h, "entropy2d_64x48": i, "axisym2d_128x80": j,
+            "jet2d_source_160x96": k}
 
 
 @pytest.mark.parametrize("label", list(_larger().keys()))
@@ -106,7 +109,7 @@ def test_fp64_matches_oracle(product_lib, oracle_lib, label):
 
 
 @pytest.mark.parametrize("label", ["pulse2d_128", "curvi3d_40", "shear2d_130x96", "wall3d_40", "waves2d_96x64",
-                                   "jet3d_40"])
+                                   "jet3d_40", "axisym2d_128x80"])
 def test_fp32_compensated_error_vs_oracle(product_lib, oracle_lib, label):
     case = _larger()[label]
     o = api.Solver(oracle_lib, case)
@@ -280,6 +283,8 @@ def _graph_cases():
         # stage and update times read from the graph's time table
         "waves2d": cases.waves2d(nx=64, ny=48, nsteps=11),
         "jet3d_rk2": (lambda c: (setattr(c, "rk", "RUNGE_KUTTA2"), c)[-1])(cases.jet3d(n=20, nsteps=7)),
+        "axisym2d": cases.axisym2d(nx=64, nr=40, nsteps=9),
+        "jet2d_source": cases.jet2d_source(nx=64, ny=48, nsteps=9),
     }
 
 
@@ -336,3 +341,13 @@ def test_harmonic_sponge_blocks_run_the_generic_stage_kernel(product_lib):
     assert info.tma_stage == 0 and info.tma_filter == 1
     case.boundaries = [b for b in case.boundaries if b.kind != "sponge_freund_harmonicwave"]
     assert api.Solver(product_lib, case).info().tma_stage == 1
+
+
+def test_axisymmetry_arguments_are_checked(product_lib):
+    """check_consistency_dimension (src/core/input.cpp:519-535): 2-D and the x axis only."""
+    s2 = api.Solver(product_lib, cases.axisym2d(nx=24, nr=16, nsteps=1), upload=False, prepare=False)
+    assert product_lib.set_axisymmetric(s2.ctx, 1, 1) == api.LEE_ERR_ARG
+    assert product_lib.set_axisymmetric(s2.ctx, 1, 0) == api.LEE_OK
+    s3 = api.Solver(product_lib, cases.curvi3d(n=12, nsteps=1), upload=False, prepare=False)
+    assert product_lib.set_axisymmetric(s3.ctx, 1, 0) == api.LEE_ERR_ARG
+    assert product_lib.set_axisymmetric(s3.ctx, 0, 0) == api.LEE_OK

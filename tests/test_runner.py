@@ -118,6 +118,28 @@ def test_parse_only_reads_the_harmonic_wave(runner, tmp_path):
         assert info["wave"] == [cases.WAVE_TYPES[w.wave_type], cases.WAVE_FORMS[w.form], w.direction, w.amplitude,
                                 w.wavelength, hw]
         assert [b[1] for b in info["bc"]] == [cases.BC_TYPES[bd.kind] for bd in case.boundaries]
+        assert info["axisym"] is False
+
+
+def test_parse_only_reads_the_jet_source(runner, tmp_path):
+    case = cases.jet2d_source(nx=40, ny=32, nsteps=2)
+    wd = str(tmp_path)
+    case.write_reference_inputs(wd, 0.01, 2)
+    info = json.loads(_run(runner, wd, "--parse-only").stdout)
+    assert info["jet2d"] is True and info["monopole"] is None
+
+
+def test_parse_only_reads_axisymmetry(runner, tmp_path):
+    case = golden_case("axisym2d_48x32")
+    wd = str(tmp_path)
+    case.write_reference_inputs(wd, 0.01, 2)
+    info = json.loads(_run(runner, wd, "--parse-only").stdout)
+    assert info["axisym"] is True
+    assert 903 in [b[1] for b in info["bc"]]
+    _rewrite_deck(wd, lambda lines: ["AXISYMMETRY = TRUE, AXIS_OF_SYMMETRY = Y" if ln.startswith("AXISYMMETRY")
+                                     else ln for ln in lines])
+    p = _run(runner, wd, "--parse-only", check=False)
+    assert p.returncode != 0 and "The axis of symmetry should be x" in p.stderr
 
 
 @pytest.mark.parametrize("key,value,message", [
@@ -128,7 +150,6 @@ def test_parse_only_reads_the_harmonic_wave(runner, tmp_path):
      "WAVELENGTH = 2.0, HALFWIDTH = 1.0", "Unknown spatial distribution of acoustic waves."),
     ("HARMONIC_WAVE", "WAVE_ENTROPY, AMPLITUDE = 1.5, SHAPE = WAVEFORM_HOMOGENEOUS, DIRECTION = Y, "
      "WAVELENGTH = 2.0", "The wave amplitude should be between 0 and 1."),
-    ("SIMULATION", "CASE_2DJET_WITH_A_HARMONIC_SOURCE", "CASE_2DJET_WITH_A_HARMONIC_SOURCE"),
     ("FIX_DT_OR_CFL", "FIX_NOTHING", "either DT or CFL"),
 ])
 def test_refuses_what_the_library_does_not_implement(runner, tmp_path, key, value, message):
@@ -176,7 +197,7 @@ def _final_solution(wd, counter):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["pulse2d_48", "curvi3d_16", "shear2d_40x32", "wall3d_14", "cylinder2d_64",
-                                  "waves2d_40x32", "jet3d_14"])
+                                  "waves2d_40x32", "jet3d_14", "axisym2d_48x32"])
 def test_fix_dt_run_matches_reference_and_solver(runner, product_lib, tmp_path, name):
     case = golden_case(name)
     g = load_golden(name)
