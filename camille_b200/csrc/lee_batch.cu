@@ -204,18 +204,20 @@ __global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __rest
 // as it arrives and keeps the results of the last 2H + 1 rows in a register queue, from which
 // F_eta of the row H behind follows without another pass through shared memory. The
 // arithmetic is that of the per-block passes (xi pass, then eta pass with the blend, or the
-// increment form with the two-float sum), term for term.
-template <typename T, bool COMP, int TX, int PF>
+// increment form with the two-float sum), term for term. Fields are independent: a CTA takes
+// VF of them (fields blockIdx.y * VF ...), which keeps the register queues short.
+template <typename T, bool COMP, int TX, int PF, int VF>
 __global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* __restrict__ inst,
                                                      const int4* __restrict__ items, int nitems, int per, OpTable op,
                                                      T blend) {
-  constexpr int V = 4;
+  constexpr int V = VF;
   constexpr int H = kFlH;
   constexpr int S = 7;
   constexpr int W = TX + 2 * H;
   constexpr int NX = H + PF + 2;  // state rows r - H - 1 .. r + PF around the row r being filtered in xi
+  const int vb = blockIdx.y * VF;  // the CTA's first field
   extern __shared__ __align__(16) unsigned char dsm[];
-  T* X = reinterpret_cast<T*>(dsm);  // [NX][V][W]
+  T* X = reinterpret_cast<T*>(dsm);  // [NX][VF][W]
   __shared__ __align__(16) BatchFilterInst<T> P;
   __shared__ SmOp<T, kFlH, S> w;
   __shared__ int cur;
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* _
       if (tid == 0) cur = it.x;
     }
     const int nx = P.nx, ny = P.ny, x0 = it.y, ys = it.z, ye = it.w;
-    const T* const* xf = P.x;
+    const T* const* xf = P.x + vb;
     const int i = x0 + tid;
     const bool col = i < nx;
     T fq[V][2 * H + 1];  // xi-pass values (x + D_xi x when compensated) of rows r - 2H .. r
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* _
       const int j = r - H;  // the row finished in this iteration
       if (COMP && col && j >= ys && j < ye) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) err_nxt[v] = P.err[v][(long long)j * nx + i];
+        for (int v = 0; v < V; ++v) err_nxt[v] = P.err[vb + v][(long long)j * nx + i];
       }
       cp_wait<PF>();
       __syncthreads();  // state row r landed for every thread
@@ -299,15 +301,15 @@ __global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* _
           }
           const T xc = xrow[v * W];
           if (!COMP) {
-            P.y[v][l] = (T(1) - blend) * xc + blend * fy;
+            P.y[vb + v][l] = (T(1) - blend) * xc + blend * fy;
           } else {
             const T dsum = dq[v][0] + fy;
             const T tt = blend * dsum + err_nxt[v];
             const T s2 = xc + tt;
             const T bb = s2 - xc;
             const T e = (xc - (s2 - bb)) + (tt - bb);
-            P.y[v][l] = s2;
-            P.comp[v][l] = e;
+            P.y[vb + v][l] = s2;
+            P.comp[vb + v][l] = e;
           }
         }
       }
@@ -332,20 +334,27 @@ cudaError_t go_stage(const StageParams<T>* prm, const int4* items, int n, int gr
   return cudaGetLastError();
 }
 
+// Fields per filter CTA (of the four of a 2-D block).
+constexpr int kFilterVF = 1;
+
 template <typename T, int TX>
 size_t filter_smem() {
-  return sizeof(T) * 4 * (kFlH + 2 + 2) * (TX + 2 * kFlH);
+  return sizeof(T) * kFilterVF * (kFlH + 2 + 2) * (TX + 2 * kFlH);
 }
 
 template <typename T, bool COMP, int TX>
 cudaError_t go_filter(const BatchFilterInst<T>* inst, const int4* items, int n, int grid, const OpTable& op, T blend,
                       cudaStream_t s) {
   const size_t smem = filter_smem<T, TX>();
-  cudaError_t e =
-      cudaFuncSetAttribute(k_batch_filter<T, COMP, TX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k_batch_filter<T, COMP, TX, 2, kFilterVF>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const int per = (n + grid - 1) / grid;
-  k_batch_filter<T, COMP, TX, 2><<<(n + per - 1) / per, TX, smem, s>>>(inst, items, n, per, op, blend);
+  // `grid` CTAs in all: the items are shared out over grid / (4 / VF) CTAs per field group
+  constexpr int G = 4 / kFilterVF;
+  const int gx = std::max(1, grid / G);
+  const int per = (n + gx - 1) / gx;
+  k_batch_filter<T, COMP, TX, 2, kFilterVF><<<dim3((n + per - 1) / per, G), TX, smem, s>>>(inst, items, n, per, op,
+                                                                                          blend);
   return cudaGetLastError();
 }
 
@@ -414,11 +423,11 @@ template <typename T, bool COMP>
 int occupancy_filter(int tx) {
   int n = 0;
   if (tx == 64)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 64, 2>, 64, filter_smem<T, 64>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 64, 2, kFilterVF>, 64, filter_smem<T, 64>());
   else if (tx == 128)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 128, 2>, 128, filter_smem<T, 128>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 128, 2, kFilterVF>, 128, filter_smem<T, 128>());
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 256, 2>, 256, filter_smem<T, 256>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_filter<T, COMP, 256, 2, kFilterVF>, 256, filter_smem<T, 256>());
   return n > 0 ? n : 1;
 }
 
@@ -429,13 +438,13 @@ int batch_filter_occupancy(int shape, int comp) {
   // the dynamic shared memory limit must be raised before the occupancy query counts it
   const size_t smem = tx == 64 ? filter_smem<T, 64>() : tx == 128 ? filter_smem<T, 128>() : filter_smem<T, 256>();
   if (comp) {
-    cudaFuncSetAttribute(tx == 64 ? k_batch_filter<T, true, 64, 2> : tx == 128 ? k_batch_filter<T, true, 128, 2>
-                                                                                : k_batch_filter<T, true, 256, 2>,
+    cudaFuncSetAttribute(tx == 64 ? k_batch_filter<T, true, 64, 2, kFilterVF> : tx == 128 ? k_batch_filter<T, true, 128, 2, kFilterVF>
+                                                                                : k_batch_filter<T, true, 256, 2, kFilterVF>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     return occupancy_filter<T, true>(tx);
   }
-  cudaFuncSetAttribute(tx == 64 ? k_batch_filter<T, false, 64, 2> : tx == 128 ? k_batch_filter<T, false, 128, 2>
-                                                                               : k_batch_filter<T, false, 256, 2>,
+  cudaFuncSetAttribute(tx == 64 ? k_batch_filter<T, false, 64, 2, kFilterVF> : tx == 128 ? k_batch_filter<T, false, 128, 2, kFilterVF>
+                                                                               : k_batch_filter<T, false, 256, 2, kFilterVF>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return occupancy_filter<T, false>(tx);
 }

@@ -1367,7 +1367,8 @@ int batch_setup(lee_ctx* c) {
     CK(cudaMemcpy(d_t, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice));
     const int nt = (int)t.size();
     const int gs = std::min(nt, nsm * batch_stage_occupancy<T>(shape, c->comp ? 1 : 0));
-    const int gf = std::min(nt, nsm * batch_filter_occupancy<T>(shape, c->comp ? 1 : 0));
+    // (the filter's CTAs each take a share of the items for some of the four fields)
+    const int gf = std::min(4 * nt, nsm * batch_filter_occupancy<T>(shape, c->comp ? 1 : 0));
     float ms_s = 0.f, ms_f = 0.f;
     for (int pass = 0; pass < 2; ++pass) {  // the first pass warms up
       CK(cudaEventRecord(e0, c->stream));
@@ -3470,7 +3471,7 @@ int lee_set_batch_shapes(lee_ctx* c, int stage_shape, int filter_shape) {
   const int occf = c->comp ? batch_filter_occupancy<float>(filter_shape, 1)
                            : batch_filter_occupancy<double>(filter_shape, 0);
   bt.sgrid = std::min(bt.nst, nsm * occs);
-  bt.fgrid = std::min(bt.nft, nsm * occf);
+  bt.fgrid = std::min(4 * bt.nft, nsm * occf);
   if (c->graph.exec) {  // captured launches name the old work lists
     cudaGraphExecDestroy(c->graph.exec);
     c->graph.exec = nullptr;
