@@ -215,7 +215,8 @@ def run_batch(args) -> None:
                          "avg_launch_ms": stage_avg, "filter_avg_launch_ms": filt_avg,
                          "filter_gbs": filt_b / (filt_avg / 1e3) / 1e9,
                          "step_gbs": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9,
-                         "step_frac": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9 / peak},
+                         "step_frac": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9 / peak,
+                         "stage_strip": list(info.batch_stage_tile), "filter_strip": list(info.batch_filter_tile)},
             "e2e": None,
             "gpu_launches": int(res["fp32c"]["launches"]),
             "clocks": clocks,

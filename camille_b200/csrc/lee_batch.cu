@@ -114,10 +114,10 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Row r of a strip (columns x0 - H .. x0 + TX + H - 1) of V fields into ring slot `slot`:
-// cp.async inside the block, zeros outside it; one commit group per row (empty when the row
-// is outside the block, so the group count stays one per row).
-template <typename T, int V, int TX, int H>
+// Row r of a strip (columns x0 - H .. x0 + TX + H - 1) of V fields into ring slot `slot`, by
+// NT threads: cp.async inside the block, zeros outside it; one commit group per row (empty
+// when the row is outside the block, so the group count stays one per row).
+template <typename T, int V, int TX, int H, int NT = TX>
 __device__ __forceinline__ void issue_row(T* ring, int slot, const T* const* fields, int r, int x0, int nx, int ny,
                                           int tid) {
   constexpr int W = TX + 2 * H;
@@ -126,7 +126,7 @@ __device__ __forceinline__ void issue_row(T* ring, int slot, const T* const* fie
     for (int v = 0; v < V; ++v) {
       T* dst = ring + ((long long)slot * V + v) * W;
       const T* src = fields[v] + (long long)r * nx;
-      for (int cc = tid; cc < W; cc += TX) {
+      for (int cc = tid; cc < W; cc += NT) {
         const int gx = x0 - H + cc;
         if (gx >= 0 && gx < nx) cp_async(dst + cc, src + gx);
         else dst[cc] = T(0);
@@ -136,17 +136,18 @@ __device__ __forceinline__ void issue_row(T* ring, int slot, const T* const* fie
   cp_commit();
 }
 
-// The stage kernel of a batch, marching along eta: a CTA of TX threads owns TX columns of a
-// block (one per thread) and rows [ys, ye) of them. Rows of the stage input (with a xi halo)
+// The stage kernel of a batch, marching along eta: a CTA of TX threads owns CX * TX columns of
+// a block (columns tid + m TX of the strip for m < CX) and rows [ys, ye) of them. Rows of the stage input (with a xi halo)
 // stream through a ring of 2H + 2 + PF rows in shared memory, PF rows ahead of the row being
 // computed; the pointwise inputs of the next row are loaded into registers while this row is
 // computed. A work item is int4 (block, x0, ys, ye); a CTA takes `per` consecutive items.
-template <typename T, bool COMP, int TX, int PF>
+template <typename T, bool COMP, int TX, int PF, int CX>
 __global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __restrict__ prm,
                                                     const int4* __restrict__ items, int nitems, int per) {
   constexpr int V = 4;
   constexpr int H = kFdH;
-  constexpr int W = TX + 2 * H;
+  constexpr int SW = CX * TX;  // strip width
+  constexpr int W = SW + 2 * H;
   constexpr int NS = 2 * H + 2 + PF;
   constexpr int TR = kTrJmField | kTrUniform | kTrSponge;
   extern __shared__ __align__(16) unsigned char dsm[];
@@ -169,31 +170,39 @@ __global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __rest
     const int nx = P.nx, ny = P.ny, x0 = it.y, ys = it.z, ye = it.w;
     const T* const* zin = P.zin;
     // prologue: rows ys - H .. ys + H + PF - 1
-    for (int r = ys - H; r < ys + H + PF; ++r) issue_row<T, V, TX, H>(ring, (r + NS) % NS, zin, r, x0, nx, ny, tid);
-    const int i = x0 + tid;
-    const bool col = i < nx;
-    PointIn<T, 2> in_cur, in_nxt;
-    if (col) gather<T, 2, COMP, TR>(P, (long long)ys * nx + i, in_cur);
+    for (int r = ys - H; r < ys + H + PF; ++r)
+      issue_row<T, V, SW, H, TX>(ring, (r + NS) % NS, zin, r, x0, nx, ny, tid);
+    PointIn<T, 2> in_cur[CX], in_nxt[CX];
+#pragma unroll
+    for (int m = 0; m < CX; ++m)
+      if (x0 + tid + m * TX < nx) gather<T, 2, COMP, TR>(P, (long long)ys * nx + x0 + tid + m * TX, in_cur[m]);
     for (int j = ys; j < ye; ++j) {
-      issue_row<T, V, TX, H>(ring, (j + H + PF + NS) % NS, zin, j + H + PF, x0, nx, ny, tid);
-      if (col && j + 1 < ye) gather<T, 2, COMP, TR>(P, (long long)(j + 1) * nx + i, in_nxt);
+      issue_row<T, V, SW, H, TX>(ring, (j + H + PF + NS) % NS, zin, j + H + PF, x0, nx, ny, tid);
+#pragma unroll
+      for (int m = 0; m < CX; ++m)
+        if (x0 + tid + m * TX < nx && j + 1 < ye)
+          gather<T, 2, COMP, TR>(P, (long long)(j + 1) * nx + x0 + tid + m * TX, in_nxt[m]);
       cp_wait<PF>();
       __syncthreads();
-      if (col) {
-        T D[V][2], q[V];
-        int so[2 * H + 1];
+      int so[2 * H + 1];
 #pragma unroll
-        for (int l = -H; l <= H; ++l) so[l + H] = ((j + l + NS) % NS) * (V * W);
+      for (int l = -H; l <= H; ++l) so[l + H] = ((j + l + NS) % NS) * (V * W);
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const T* c0 = ring + so[H] + v * W + tid + H;
-          D[v][0] = dop_c<T, kFdH, 3, 1>(w, c0, i, nx);
-          D[v][1] = dop_ring<T, kFdH, 3, NS>(w, ring, so, V * W, v * W + tid + H, j, ny);
-          q[v] = *c0;
+      for (int m = 0; m < CX; ++m) {
+        const int cl = tid + m * TX, i = x0 + cl;
+        if (i < nx) {
+          T D[V][2], q[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const T* c0 = ring + so[H] + v * W + cl + H;
+            D[v][0] = dop_c<T, kFdH, 3, 1>(w, c0, i, nx);
+            D[v][1] = dop_ring<T, kFdH, 3, NS>(w, ring, so, V * W, v * W + cl + H, j, ny);
+            q[v] = *c0;
+          }
+          rhs_update<T, 2, COMP, TR>(P, (long long)j * nx + i, i, j, 0, D, q, in_cur[m]);
         }
-        rhs_update<T, 2, COMP, TR>(P, (long long)j * nx + i, i, j, 0, D, q, in_cur);
+        in_cur[m] = in_nxt[m];
       }
-      in_cur = in_nxt;
     }
     cp_wait<0>();
   }
@@ -318,19 +327,20 @@ __global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* _
   }
 }
 
-template <typename T, int TX>
+template <typename T, int SW>
 size_t stage_smem() {
-  return sizeof(T) * 4 * (2 * kFdH + 2 + 2) * (TX + 2 * kFdH);
+  return sizeof(T) * 4 * (2 * kFdH + 2 + 2) * (SW + 2 * kFdH);
 }
 
-template <typename T, bool COMP, int TX>
+// TX threads, each with CX columns of the strip
+template <typename T, bool COMP, int TX, int CX>
 cudaError_t go_stage(const StageParams<T>* prm, const int4* items, int n, int grid, cudaStream_t s) {
-  const size_t smem = stage_smem<T, TX>();
-  cudaError_t e =
-      cudaFuncSetAttribute(k_batch_stage<T, COMP, TX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = stage_smem<T, TX * CX>();
+  cudaError_t e = cudaFuncSetAttribute(k_batch_stage<T, COMP, TX, 2, CX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
   if (e != cudaSuccess) return e;
   const int per = (n + grid - 1) / grid;
-  k_batch_stage<T, COMP, TX, 2><<<(n + per - 1) / per, TX, smem, s>>>(prm, items, n, per);
+  k_batch_stage<T, COMP, TX, 2, CX><<<(n + per - 1) / per, TX, smem, s>>>(prm, items, n, per);
   return cudaGetLastError();
 }
 
@@ -358,25 +368,35 @@ cudaError_t go_filter(const BatchFilterInst<T>* inst, const int4* items, int n, 
   return cudaGetLastError();
 }
 
-template <typename T, bool COMP>
-int occupancy_stage(int tx) {
+template <typename T, bool COMP, int TX, int CX>
+int occupancy_stage_of() {
+  const size_t smem = stage_smem<T, TX * CX>();
+  cudaFuncSetAttribute(k_batch_stage<T, COMP, TX, 2, CX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int n = 0;
-  if (tx == 64)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 64, 2>, 64, stage_smem<T, 64>());
-  else if (tx == 128)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 128, 2>, 128, stage_smem<T, 128>());
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, 256, 2>, 256, stage_smem<T, 256>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<T, COMP, TX, 2, CX>, TX, smem);
   return n > 0 ? n : 1;
+}
+
+template <typename T, bool COMP>
+int occupancy_stage(int width, int cx) {
+  if (cx == 2) return width == 128 ? occupancy_stage_of<T, COMP, 64, 2>() : occupancy_stage_of<T, COMP, 128, 2>();
+  if (width == 64) return occupancy_stage_of<T, COMP, 64, 1>();
+  if (width == 128) return occupancy_stage_of<T, COMP, 128, 1>();
+  return occupancy_stage_of<T, COMP, 256, 1>();
 }
 
 }  // namespace
 
-// Work-item shapes, by index: columns x rows of a strip; the CTA has one thread per column.
+// Work-item shapes, by index: columns x rows of a strip, and the stage kernel's columns per
+// thread (the filter has one thread per column).
+namespace {
+const int kShapes[kBatchShapes][3] = {{64, 16, 1}, {128, 16, 1}, {128, 32, 1}, {256, 16, 1},
+                                      {64, 32, 1},  {128, 16, 2}, {256, 16, 2}};
+}  // namespace
+
 void batch_shape(int shape, int* tx, int* ty) {
-  static const int s[kBatchShapes][2] = {{64, 16}, {128, 16}, {128, 32}, {256, 16}, {64, 32}};
-  *tx = s[shape][0];
-  *ty = s[shape][1];
+  *tx = kShapes[shape][0];
+  *ty = kShapes[shape][1];
 }
 
 template <typename T>
@@ -385,14 +405,19 @@ cudaError_t launch_batch_stage(const StageParams<T>* prm, const int4* items, int
   if (n <= 0) return cudaSuccess;
   int tx, ty;
   batch_shape(shape, &tx, &ty);
+  const int cx = kShapes[shape][2];
   if (comp) {
-    if (tx == 64) return go_stage<T, true, 64>(prm, items, n, grid, s);
-    if (tx == 128) return go_stage<T, true, 128>(prm, items, n, grid, s);
-    return go_stage<T, true, 256>(prm, items, n, grid, s);
+    if (cx == 2) return tx == 128 ? go_stage<T, true, 64, 2>(prm, items, n, grid, s)
+                                  : go_stage<T, true, 128, 2>(prm, items, n, grid, s);
+    if (tx == 64) return go_stage<T, true, 64, 1>(prm, items, n, grid, s);
+    if (tx == 128) return go_stage<T, true, 128, 1>(prm, items, n, grid, s);
+    return go_stage<T, true, 256, 1>(prm, items, n, grid, s);
   }
-  if (tx == 64) return go_stage<T, false, 64>(prm, items, n, grid, s);
-  if (tx == 128) return go_stage<T, false, 128>(prm, items, n, grid, s);
-  return go_stage<T, false, 256>(prm, items, n, grid, s);
+  if (cx == 2) return tx == 128 ? go_stage<T, false, 64, 2>(prm, items, n, grid, s)
+                                : go_stage<T, false, 128, 2>(prm, items, n, grid, s);
+  if (tx == 64) return go_stage<T, false, 64, 1>(prm, items, n, grid, s);
+  if (tx == 128) return go_stage<T, false, 128, 1>(prm, items, n, grid, s);
+  return go_stage<T, false, 256, 1>(prm, items, n, grid, s);
 }
 
 template <typename T>
@@ -416,7 +441,8 @@ template <typename T>
 int batch_stage_occupancy(int shape, int comp) {
   int tx, ty;
   batch_shape(shape, &tx, &ty);
-  return comp ? occupancy_stage<T, true>(tx) : occupancy_stage<T, false>(tx);
+  const int cx = kShapes[shape][2];
+  return comp ? occupancy_stage<T, true>(tx, cx) : occupancy_stage<T, false>(tx, cx);
 }
 
 template <typename T, bool COMP>

@@ -302,7 +302,7 @@ struct BatchFilterInst {
   T* comp[4];
 };
 
-constexpr int kBatchShapes = 5;
+constexpr int kBatchShapes = 7;
 void batch_shape(int shape, int* tx, int* ty);
 // one launch over the tile list (int4: block, x0, y0, 0) with the blocks' stage parameters
 template <typename T>

@@ -247,7 +247,7 @@ int lee_advance_blocks(lee_ctx *ctx, int nsteps, const double *dt);
  * context holding block b alone). */
 int lee_compute_dt_blocks(lee_ctx *ctx, double cfl, double *dt);
 /* Override the batched launches' work-item shapes that lee_prepare picked by timing (index
- * 0..4; lee_info reports them): every shape gives the same results. */
+ * 0..6; lee_info reports the strip of each): every shape gives the same results. */
 int lee_set_batch_shapes(lee_ctx *ctx, int stage_shape, int filter_shape);
 /* Sizes and coefficient layout chosen by lee_prepare (no reference counterpart: the
  * reference has no timers or counters, finding F13). */

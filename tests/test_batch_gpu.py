@@ -91,3 +91,22 @@ def test_batch_graphs_give_the_same_bits(product_lib, precision):
         b.advance_blocks(n, dts)
     for q in range(len(case.blocks)):
         np.testing.assert_array_equal(a.download(q)[0], b.download(q)[0])
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+def test_every_work_item_shape_gives_the_same_bits(product_lib, precision):
+    """The strip shapes the autotuner picks from (one or two columns per stage thread, one
+    field per filter CTA) change the launch, not the arithmetic of any point."""
+    case = _batch(nsteps=5)
+    ref = None
+    for shape in range(7):
+        s = api.Solver(product_lib, case, precision=precision)
+        assert product_lib.set_batch_shapes(s.ctx, shape, (shape + 3) % 7) == api.LEE_OK
+        dts = s.compute_dt_blocks()
+        s.advance_blocks(case.nsteps, dts)
+        out = [s.download(b)[0] for b in range(len(case.blocks))]
+        s.close()
+        if ref is None:
+            ref = out
+        for a, b in zip(out, ref):
+            np.testing.assert_array_equal(a, b)
