@@ -383,7 +383,8 @@ def run_ours(args) -> None:
                          "step_bytes_per_point": step_bytes_per_point(info, True, dim),
                          "tma_stage": info.tma_stage, "tma_filter": info.tma_filter,
                          "stage_chunk": info.stage_chunk, "filter_chunk": info.filter_chunk,
-                         "filter_kernel": info.filter_kernel, "stage_kernel": info.stage_kernel},
+                         "filter_kernel": info.filter_kernel, "stage_kernel": info.stage_kernel,
+                         "filter_rows": info.filter_rows},
             "e2e": {"value": world * npts * K / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K,
                     "note": "lee_upload_state from pinned host memory, lee_advance(K), lee_download_state"},

@@ -95,6 +95,7 @@ struct BlockData {
   void* d_sigma_field = nullptr;    // summed sponge strengths per point (working precision)
   int tiles_x = 0, tiles_y = 0;
   int stage_chunk = 0, filter_chunk = 0;
+  int filter_ry = 1;                  // rows per thread row of the scalar fused filter (1 or 2)
 };
 
 struct MapKey {
@@ -872,13 +873,16 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
   return encode_maps(c, b, const_cast<const void* const*>(fields), c->V, bx, by, out->m);
 }
 
-int filter_box(const lee_ctx* c, int* bx, int* by) {
+// The fused filter's box (tile of kTileX x kTileY * ry points with a halo of h) and its tiles.
+int filter_box(const lee_ctx* c, int h, int ry, int* bx, int* by) {
   const int A = (int)(16 / c->esz);
-  const int hx = ((c->hf + A - 1) / A) * A;
+  const int hx = ((h + A - 1) / A) * A;
   *bx = kTileX + 2 * hx;
-  *by = kTileY + 2 * c->hf;
+  *by = kTileY * ry + 2 * h;
   return LEE_OK;
 }
+
+int filter_tiles(const BlockData& b) { return b.tiles_x * ((b.ny + kTileY * b.filter_ry - 1) / (kTileY * b.filter_ry)); }
 
 // Tiles of the vectorised filter at the block's group width.
 void set_filter_tiles(const lee_ctx* c, BlockData& b) {
@@ -948,7 +952,7 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
     filter_vec_box(c->esz, c->hf, b.filter_px, &bx, &by, &tx, &ty);
     fp.tiles_x = b.vtiles_x;
   } else {
-    filter_box(c, &bx, &by);
+    filter_box(c, c->hf, b.filter_ry, &bx, &by);
   }
   FieldMaps fm;
   int rc = field_maps(c, b, in, bx, by, &fm);
@@ -958,7 +962,8 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
   if (b.filter_px > 0)
     CK(launch_filter_vec<T>(fm, fp, c->hf, b.filter_px, c->cfg.num_dim, b.vtiles_x * b.vtiles_y, chunks, c->stream));
   else
-    CK(launch_filter_tma<T>(fm, fp, c->hf, c->cfg.num_dim, c->comp ? 1 : 0, b.tiles_x * b.tiles_y, chunks, c->stream));
+    CK(launch_filter_tma<T>(fm, fp, c->hf, c->cfg.num_dim, c->comp ? 1 : 0, b.filter_ry, filter_tiles(b), chunks,
+                            c->stream));
   int e1 = mark(c);
   span(c, 1, e0, e1);
   c->stats.filter_launches += 1;
@@ -990,19 +995,24 @@ int autotune(lee_ctx* c, BlockData& b) {
     if ((which == 0 && !b.tma) || (which == 1 && !b.tma_filter)) continue;
     if (which == 0 && !d3 && nskinds == 1) continue;  // nothing to choose
     float best = 1e30f;
-    int best_chunk = b.nz, best_kind = which == 0 ? b.stage_px : b.filter_px;
-    for (int kq = 0; kq < (which == 1 ? nkinds : nskinds); ++kq) {
+    int best_chunk = b.nz, best_kind = which == 0 ? b.stage_px : b.filter_px, best_ry = b.filter_ry;
+    // the scalar filter's rows per thread row are timed with the chunk: each point's
+    // arithmetic is the same for either
+    const int nry = which == 1 ? 2 : 1;
+    for (int kq = 0; kq < (which == 1 ? nkinds : nskinds) * nry; ++kq) {
       if (which == 0) {
         b.stage_px = skinds[kq];
       } else {
-        b.filter_px = kinds[kq];
+        b.filter_px = kinds[kq / nry];
+        b.filter_ry = 1 + kq % nry;
+        if (b.filter_px > 0 && b.filter_ry > 1) continue;
         set_filter_tiles(c, b);
       }
       for (int ch : (d3 ? std::vector<int>(std::begin(cands3), std::end(cands3))
                         : std::vector<int>(std::begin(cands2), std::end(cands2)))) {
         if (d3 && ch > b.nz) continue;
         float tsum = 0.f;
-        for (int rep = 0; rep < 3; ++rep) {
+        for (int rep = 0; rep < 4; ++rep) {  // the first run warms up
           CK(cudaEventRecord(e0, c->stream));
           int rc;
           if (which == 0) {
@@ -1037,6 +1047,7 @@ int autotune(lee_ctx* c, BlockData& b) {
           best = tsum;
           best_chunk = d3 ? ch : b.nz;
           best_kind = which == 0 ? b.stage_px : b.filter_px;
+          best_ry = b.filter_ry;
         }
       }
     }
@@ -1046,6 +1057,7 @@ int autotune(lee_ctx* c, BlockData& b) {
     } else {
       b.filter_chunk = best_chunk;
       b.filter_px = best_kind;
+      b.filter_ry = best_ry;
       set_filter_tiles(c, b);
     }
   }
@@ -1974,13 +1986,13 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
     fp.blend = (T)c->cfg.filter_blend;
     for (int v = 0; v < V; ++v) fp.out[v] = (T*)a.mu[v];
     fp.errflag = c->d_err;
-    const int A = (int)(16 / c->esz);
-    const int hx = ((H + A - 1) / A) * A;
+    int bx, by;
+    filter_box(c, H, b.filter_ry, &bx, &by);
     FieldMaps fm;
-    int rc = field_maps(c, b, a.lam, kTileX + 2 * hx, kTileY + 2 * H, &fm);
+    int rc = field_maps(c, b, a.lam, bx, by, &fm);
     if (rc) return rc;
     const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
-    CK(launch_filter_tma<T>(fm, fp, H, c->cfg.num_dim, 0, b.tiles_x * b.tiles_y, chunks, c->stream));
+    CK(launch_filter_tma<T>(fm, fp, H, c->cfg.num_dim, 0, b.filter_ry, filter_tiles(b), chunks, c->stream));
     c->stats.kernel_launches += 1;
     mu = a.mu;
   } else if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
@@ -3189,6 +3201,7 @@ int lee_get_info(lee_ctx* c, lee_info* info) {
   info->filter_chunk = c->blk.empty() ? 0 : c->blk[0].filter_chunk;
   info->filter_kernel = c->blk.empty() ? 0 : c->blk[0].filter_px;
   info->stage_kernel = c->blk.empty() ? 0 : c->blk[0].stage_px;
+  info->filter_rows = c->blk.empty() ? 0 : c->blk[0].filter_ry;
   info->batched = c->batch.active ? 1 : 0;
   if (c->batch.active) {
     batch_shape(c->batch.sshape, &info->batch_stage_tile[0], &info->batch_stage_tile[1]);

@@ -164,8 +164,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
   }
 }
 
+// One tile row per thread row (the form of k_filter_tma with RY = 1, scheduled by the compiler
+// without the per-row arrays).
 template <typename T, int DIM, bool COMP, int HF>
-__global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ FieldMaps ym,
+__global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ FieldMaps ym,
                                                     const __grid_constant__ TmaFilterParams<T> P) {
   constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = kFilterSlots;
   constexpr int HX = Box<T, HF>::HX, BX = Box<T, HF>::BX, BY = Box<T, HF>::BY;
@@ -309,15 +311,190 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
   }
 }
 
+template <typename T, int DIM, bool COMP, int HF, int RY>
+__global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ FieldMaps ym,
+                                                    const __grid_constant__ TmaFilterParams<T> P) {
+  constexpr int TX = kTileX, TY = kTileY, TYE = kTileY * RY, NQ = 2 * HF + 1, NSF = kFilterSlots;
+  using FBox = Box<T, HF, RY>;
+  constexpr int HX = FBox::HX, BX = FBox::BX, BY = FBox::BY;
+  constexpr int FB = FBox::FB;    // elements one box load writes
+  constexpr int FBP = FBox::FBP;  // stride between boxes in shared memory
+  extern __shared__ __align__(128) unsigned char smem[];
+  T* ring = reinterpret_cast<T*>(smem);
+  T* u1 = ring + NSF * FBP;  // [BY][TX]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(u1 + BY * TX);
+
+  const int v = blockIdx.z;
+  const int i0 = (int)(blockIdx.x % P.tiles_x) * TX, j0 = (int)(blockIdx.x / P.tiles_x) * TYE;
+  const int k0 = DIM == 3 ? (int)blockIdx.y * P.k_chunk : 0;
+  const int k1 = DIM == 3 ? min(P.nz, k0 + P.k_chunk) : 1;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int i = i0 + tx;
+  // the thread's rows j0 + ty + TY r, r < RY
+  int jr[RY];
+  bool active[RY];
+#pragma unroll
+  for (int r = 0; r < RY; ++r) {
+    jr[r] = j0 + ty + TY * r;
+    active[r] = i < P.nx && jr[r] < P.ny;
+  }
+  const int plo = DIM == 3 ? max(0, k0 - HF) : 0;
+  const int phi = DIM == 3 ? min(P.nz - 1, k1 - 1 + HF) : 0;
+
+  if (tid == 0) {
+    for (int q = 0; q < NSF; ++q) mbar_init(&bar[q], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int next_issue = plo;
+  auto issue_upto = [&](int last) {
+    for (; next_issue <= min(phi, last); ++next_issue) {
+      const int slot = (next_issue - plo) % NSF;
+      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * FB));
+      tma_load_3d(ring + slot * FBP, &ym.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
+    }
+  };
+  if (tid == 0) issue_upto(plo + NSF - 1);
+
+  // closure-class weights along xi and eta are fixed for a thread: keep them in registers
+  T wx[NQ], wy[RY][NQ];
+  {
+    const int cx = cls_of(min(i, P.nx - 1), P.nx, P.nb);
+#pragma unroll
+    for (int o = 0; o < NQ; ++o) wx[o] = P.w[cx][o];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+      const int cy = cls_of(min(jr[r], P.ny - 1), P.ny, P.nb);
+#pragma unroll
+      for (int o = 0; o < NQ; ++o) wy[r][o] = P.w[cy][o];
+    }
+  }
+  T uq[RY][NQ], dq[RY][HF + 1], xq[RY][HF + 1];
+#pragma unroll
+  for (int r = 0; r < RY; ++r) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) uq[r][q] = T(0);
+#pragma unroll
+    for (int q = 0; q <= HF; ++q) dq[r][q] = xq[r][q] = T(0);
+  }
+  const int pstart = DIM == 3 ? k0 - HF : 0, pend = DIM == 3 ? k1 - 1 + HF : 0;
+  for (int p = pstart; p <= pend; ++p) {
+    T u2[RY], d12[RY], xc[RY];
+    const int kf = DIM == 3 ? p - HF : 0;  // the plane finalized at the end of this iteration
+    const bool kin = kf >= k0 && kf < k1;
+    T ef[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+      u2[r] = d12[r] = xc[r] = T(0);
+      ef[r] = (COMP && active[r] && kin) ? P.err[v][i + (long long)P.nx * (jr[r] + (long long)P.ny * kf)] : T(0);
+    }
+    if (p >= plo && p <= phi) {
+      const int rel = p - plo;
+      const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1));
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(P.errflag, 1);
+          for (int w = p + 1; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NSF], (unsigned)(((w - plo) / NSF) & 1));
+        }
+        return;
+      }
+      const T* box = ring + (rel % NSF) * FBP;
+      // F_xi on the thread's own rows (kept in registers) and on its share of the eta halo rows
+      T d1[RY], u1c[RY];
+#pragma unroll
+      for (int r = 0; r < RY; ++r) {
+        const T* fc = box + (ty + TY * r + HF) * BX + tx + HX;
+        xc[r] = fc[0];
+        T d = T(0);
+#pragma unroll
+        for (int o = -HF; o <= HF; ++o) d += wx[o + HF] * fc[o];
+        d1[r] = d;
+        u1c[r] = COMP ? xc[r] + d : d;
+        u1[(ty + TY * r + HF) * TX + tx] = u1c[r];
+      }
+      for (int rr = ty; rr < 2 * HF; rr += TY) {
+        const int row = rr < HF ? rr : rr + TYE;
+        const T* f = box + row * BX + tx + HX;
+        T d = T(0);
+#pragma unroll
+        for (int o = -HF; o <= HF; ++o) d += wx[o + HF] * f[o];
+        u1[row * TX + tx] = COMP ? f[0] + d : d;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < RY; ++r) {
+        T dy = T(0);
+#pragma unroll
+        for (int o = -HF; o <= HF; ++o)
+          dy += wy[r][o + HF] * (o == 0 ? u1c[r] : u1[(ty + TY * r + HF + o) * TX + tx]);
+        if (COMP) {
+          u2[r] = u1c[r] + dy;
+          d12[r] = d1[r] + dy;
+        } else {
+          u2[r] = dy;
+        }
+      }
+      __syncthreads();
+      if (tid == 0) issue_upto(p + NSF);
+    }
+    const int k = kf;
+    int cz = 0;
+    if (DIM == 3 && kin) cz = cls_of(k, P.nz, P.nb);
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+#pragma unroll
+      for (int q = 0; q < NQ - 1; ++q) uq[r][q] = uq[r][q + 1];
+      uq[r][NQ - 1] = u2[r];
+#pragma unroll
+      for (int q = 0; q < HF; ++q) {
+        dq[r][q] = dq[r][q + 1];
+        xq[r][q] = xq[r][q + 1];
+      }
+      dq[r][HF] = d12[r];
+      xq[r][HF] = xc[r];
+      if (!(active[r] && kin)) continue;
+      T fz, x0, dsum;
+      if (DIM == 3) {
+        fz = T(0);
+        if (cz == 0) {
+          // interior plane: the loop-invariant interior weights
+#pragma unroll
+          for (int o = 0; o < NQ; ++o) fz += P.w[0][o] * uq[r][o];
+        } else {
+#pragma unroll
+          for (int o = 0; o < NQ; ++o) fz += P.w[cz][o] * uq[r][o];
+        }
+        x0 = xq[r][0];
+        dsum = dq[r][0];
+      } else {
+        fz = u2[r];
+        x0 = xc[r];
+        dsum = d12[r];
+      }
+      const long long l = i + (long long)P.nx * (jr[r] + (long long)P.ny * k);
+      if (!COMP) {
+        P.out[v][l] = (T(1) - P.blend) * x0 + P.blend * fz;
+      } else {
+        const T D = DIM == 3 ? dsum + fz : dsum;
+        const T t = P.blend * D + ef[r];
+        const T sm = x0 + t;
+        const T bb = sm - x0;
+        P.out[v][l] = sm;
+        P.comp[v][l] = (x0 - (sm - bb)) + (t - bb);
+      }
+    }
+  }
+}
+
 template <typename T, int DIM, bool COMP>
 size_t stage_smem() {
   constexpr int NS = DIM == 3 ? 2 * kFdHalf + 1 + StagePrefetch<T>::P : 1;
   return sizeof(T) * NS * (DIM + 2) * Box<T, kFdHalf>::FBP + NS * sizeof(uint64_t);
 }
 
-template <typename T, int HF>
+template <typename T, int HF, int RY>
 size_t filter_smem() {
-  return sizeof(T) * (kFilterSlots * Box<T, HF>::FBP + Box<T, HF>::BY * kTileX) +
+  return sizeof(T) * (kFilterSlots * Box<T, HF, RY>::FBP + Box<T, HF, RY>::BY * kTileX) +
          kFilterSlots * sizeof(uint64_t);
 }
 
@@ -365,9 +542,12 @@ cudaError_t go_stage_tr(const FieldMaps& z, const TmaStageParams<T>& p, int tr, 
 }
 
 template <typename T, int DIM, bool COMP, int HF>
-cudaError_t go_filter(const FieldMaps& in, const TmaFilterParams<T>& p, int tiles, int chunks, cudaStream_t s) {
-  const size_t sm = filter_smem<T, HF>();
-  k_filter_tma<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, sm, s>>>(in, p);
+cudaError_t go_filter(const FieldMaps& in, const TmaFilterParams<T>& p, int ry, int tiles, int chunks, cudaStream_t s) {
+  if (ry == 2) {
+    k_filter_tma<T, DIM, COMP, HF, 2><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 2>(), s>>>(in, p);
+  } else {
+    k_filter_tma_row<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 1>(), s>>>(in, p);
+  }
   return cudaGetLastError();
 }
 
@@ -388,14 +568,16 @@ cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, i
 }
 
 template <typename T>
-cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
-                              int chunks, cudaStream_t s) {
-#define LEE_FILTER_CASE(HF)                                                                     \
-  if (hf == HF) {                                                                               \
-    if (dim == 2)                                                                               \
-      return comp ? go_filter<T, 2, true, HF>(in, p, tiles, 1, s) : go_filter<T, 2, false, HF>(in, p, tiles, 1, s); \
-    return comp ? go_filter<T, 3, true, HF>(in, p, tiles, chunks, s)                            \
-                : go_filter<T, 3, false, HF>(in, p, tiles, chunks, s);                          \
+cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int ry,
+                              int tiles, int chunks, cudaStream_t s) {
+  if (ry != 1 && ry != 2) return cudaErrorInvalidValue;
+#define LEE_FILTER_CASE(HF)                                                                      \
+  if (hf == HF) {                                                                                \
+    if (dim == 2)                                                                                \
+      return comp ? go_filter<T, 2, true, HF>(in, p, ry, tiles, 1, s)                            \
+                  : go_filter<T, 2, false, HF>(in, p, ry, tiles, 1, s);                          \
+    return comp ? go_filter<T, 3, true, HF>(in, p, ry, tiles, chunks, s)                         \
+                : go_filter<T, 3, false, HF>(in, p, ry, tiles, chunks, s);                       \
   }
   LEE_FILTER_CASE(2)
   LEE_FILTER_CASE(4)
@@ -406,9 +588,9 @@ cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, 
 
 template cudaError_t launch_stage_tma<double>(const FieldMaps&, const TmaStageParams<double>&, int, int, int, cudaStream_t);
 template cudaError_t launch_stage_tma<float>(const FieldMaps&, const TmaStageParams<float>&, int, int, int, cudaStream_t);
-template cudaError_t launch_filter_tma<double>(const FieldMaps&, const TmaFilterParams<double>&, int, int, int, int, int,
+template cudaError_t launch_filter_tma<double>(const FieldMaps&, const TmaFilterParams<double>&, int, int, int, int, int, int,
                                                cudaStream_t);
-template cudaError_t launch_filter_tma<float>(const FieldMaps&, const TmaFilterParams<float>&, int, int, int, int, int,
+template cudaError_t launch_filter_tma<float>(const FieldMaps&, const TmaFilterParams<float>&, int, int, int, int, int, int,
                                               cudaStream_t);
 
 }  // namespace lee

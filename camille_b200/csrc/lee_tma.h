@@ -44,12 +44,13 @@ struct TmaFilterParams {
 // Shared-memory box geometry: halo along i rounded up so every TMA row starts on 16 bytes;
 // consecutive boxes in shared memory are FBP elements apart, a multiple of 128 bytes, because
 // a cp.async.bulk.tensor destination must be 128-byte aligned.
-template <typename T, int H>
+// RY: rows of the tile per thread row (the tile is kTileY * RY rows high).
+template <typename T, int H, int RY = 1>
 struct Box {
   static constexpr int A = (int)(16 / sizeof(T));
   static constexpr int HX = ((H + A - 1) / A) * A;
   static constexpr int BX = kTileX + 2 * HX;
-  static constexpr int BY = kTileY + 2 * H;
+  static constexpr int BY = kTileY * RY + 2 * H;
   static constexpr int FB = BX * BY;
   static constexpr int FBP = (int)((((size_t)FB * sizeof(T) + 127) / 128) * 128 / sizeof(T));
   static_assert((FBP * sizeof(T)) % 128 == 0, "box stride must be a multiple of 128 bytes");
@@ -65,9 +66,10 @@ size_t stage_tma_smem(int dim, size_t esz);
 template <typename T>
 cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int traits, int tiles, int chunks,
                              cudaStream_t s);
+// ry: tile rows per thread row, 1 or 2 (the same arithmetic for every point either way)
 template <typename T>
-cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int tiles,
-                              int chunks, cudaStream_t s);
+cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int ry,
+                              int tiles, int chunks, cudaStream_t s);
 // The plane-marching adjoint stage (lee_adjoint_tma.cu): tensor maps of w (5 fields) then the
 // nine J*metrics fields, and its parameters.
 struct __align__(64) AdjMaps {
