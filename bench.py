@@ -34,6 +34,7 @@ from camille_b200 import api, cases  # noqa: E402
 
 METRIC = "grid-point RK steps/s, mixed vs FP64 @<=1e-5 rel L2 p'; adjoint/forward time"
 UNIT = "grid-point RK steps/s"
+STAGE_PAIR_DRAM_BYTES_PER_POINT = 130.7
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -348,6 +349,13 @@ def run_ours(args) -> None:
     filt_avg_ms = st.filter_ms / max(st.filter_launches, 1)
     stage_b = stage_bytes_per_point(info, True) * npts
     achieved = stage_b / (stage_avg_ms / 1e3) / 1e9
+    # DRAM bytes of the two-point stage kernel measured by ncu (dram__bytes_read.sum +
+    # dram__bytes_write.sum of one step's four launches at 160^3: 130.7 bytes per point on
+    # average), scaled to this launch by its points; other kernels and workloads have no capture
+    traffic, traffic_src = None, None
+    if args.workload == "curvi3d" and info.stage_kernel == 2 and dim == 3:
+        traffic = STAGE_PAIR_DRAM_BYTES_PER_POINT * npts
+        traffic_src = "ncu at 160^3 (mean of the four stage launches of a step), scaled by points"
     step_b = step_bytes_per_point(info, True, dim) * npts
     step_gbs = step_b * K / (r32["ms"] / 1e3) / 1e9
     dominant = "stage" if st.stage_ms >= st.filter_ms else "filter"
@@ -375,7 +383,8 @@ def run_ours(args) -> None:
             "p_rel_l2_vs_fp64": {"value": err, "steps": max(args.error_steps, W + K)},
             "roofline": {"bound": "hbm", "kernel": "fused RK stage (fp32-compensated)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": f"{peak_kind} copy bandwidth", "traffic": None,
+                         "peak_source": f"{peak_kind} copy bandwidth", "traffic": traffic,
+                         "traffic_source": traffic_src,
                          "bytes_per_point": stage_bytes_per_point(info, True),
                          "avg_launch_ms": stage_avg_ms, "dominant": dominant,
                          "filter_avg_launch_ms": filt_avg_ms,
