@@ -135,9 +135,9 @@ WORKLOADS = {
 
 
 def run_batch(args) -> None:
-    """64 instances advanced together (lee_advance_blocks, FP32-compensated and FP64)
-    and, as the comparison the config asks for, one at a time in plain FP64 (each instance in
-    its own context, its own time step)."""
+    """The batch workload: 64 instances of uneven sizes advanced together (lee_advance_blocks,
+    FP32-compensated and FP64) and, for comparison, one at a time in plain FP64 (each instance
+    in its own context, its own time step)."""
     import torch
 
     rank = int(os.environ.get("RANK", "0"))
@@ -409,7 +409,7 @@ def run_ours(args) -> None:
 
 
 def run_adjoint(args, lib, barrier, max_over_ranks) -> dict:
-    """The adjoint workload (configs[4]): 192^3 curvilinear block, Mach 0.5, a 16^3 distributed
+    """The adjoint workload: 192^3 curvilinear block, Mach 0.5, a 16^3 distributed
     source, 64 microphones, FP32-compensated forward of `adjoint_steps` steps checkpointed every
     100. Times the forward alone (lee_eval_objective) and the gradient (lee_adjoint_gradient)
     with segment recompute and with the first pass's traces; each timed region is bracketed by
@@ -513,7 +513,7 @@ def main() -> int:
                     help="steps launched one by one with events between launches (roofline)")
     ap.add_argument("--error-steps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing (configs[4])")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing (the 192^3 adjoint workload)")
     ap.add_argument("--adjoint-n", type=int, default=192)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--cpu-n", type=int, default=64)
