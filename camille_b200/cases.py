@@ -779,3 +779,85 @@ def instance(case: Case, b: int) -> Case:
     blk = case.blocks[b]
     bnd = [dataclasses.replace(bd, block=0) for bd in case.boundaries if bd.block == b]
     return dataclasses.replace(case, name=f"{case.name}_b{b}", blocks=[blk], boundaries=bnd)
+
+
+def _boxes_mask(dims: tuple[int, int, int], boxes) -> np.ndarray:
+    """(nz, ny, nx) bool mask of the union of inclusive index boxes ((i0, i1), (j0, j1), (k0, k1))."""
+    nx, ny, nz = dims
+    m = np.zeros((nz, ny, nx), bool)
+    for (i0, i1), (j0, j1), (k0, k1) in boxes:
+        m[k0:k1 + 1, j0:j1 + 1, i0:i1 + 1] = True
+    return m
+
+
+def holes(num_dim: int = 2, nsteps: int = 12, seed: int = 11, gamma: float = 1.4) -> Case:
+    """A single Cartesian block (64 x 56 in 2-D, 24^3 in 3-D, unit spacing) with a hand-set pattern of
+    holes and receivers, so that every branch of the reference's hole closures
+    (StandardCentral::iblank_correction, src/solver/spatial_discretization.cpp:1356-1652) occurs
+    along every direction: a hole after a plain fluid point (the ``last_iblank /= BLANKED``
+    branch that inserts no closure), a hole after a receiver (right closure rows anchored at
+    the receiver), a hole after a hole (zero), fluid and receivers after a hole (left closure
+    rows), holes at the start and at the end of lines, and a seven-point run between a hole at a
+    line start and a hole after receivers (the filter closure's whole support).
+
+    Receivers are donated by the block itself (4-point stencils in every direction, positive
+    seeded weights) from a fluid region away from holes and receivers. Uniform mean flow
+    (Mach 0.3, 0.2, 0.1 along x, y, z), a Gaussian p' pulse over the holes, closures at the block
+    edges and no BC lines. The maps go to both sides through the reference's overset file."""
+    rng = np.random.default_rng(seed)
+    if num_dim == 2:
+        dims = (64, 56, 1)
+        z1 = (0, 0)
+        hole_boxes = [((20, 24), (10, 14), z1), ((40, 44), (10, 14), z1), ((0, 3), (26, 30), z1),
+                      ((58, 63), (26, 30), z1), ((20, 26), (52, 55), z1), ((40, 46), (0, 2), z1)]
+        recv_boxes = [((38, 39), (10, 14), z1), ((45, 46), (10, 14), z1), ((40, 44), (8, 9), z1),
+                      ((40, 44), (15, 16), z1), ((56, 57), (26, 30), z1), ((20, 26), (50, 51), z1)]
+        region, width = ((28, 8), (36, 8), (0, 1)), (4, 4, 1)
+        centre = (30.0, 22.0, 0.0)
+    elif num_dim == 3:
+        dims = (24, 24, 24)
+        hole_boxes = [((4, 7), (4, 7), (4, 7)), ((13, 16), (13, 16), (13, 16)),
+                      ((0, 3), (13, 16), (0, 2)), ((0, 3), (13, 16), (21, 23)),
+                      ((20, 23), (0, 2), (0, 3)), ((20, 23), (21, 23), (20, 23))]
+        recv_boxes = [((11, 12), (13, 16), (13, 16)), ((17, 18), (13, 16), (13, 16)),
+                      ((13, 16), (11, 12), (13, 16)), ((13, 16), (17, 18), (13, 16)),
+                      ((13, 16), (13, 16), (11, 12)), ((13, 16), (13, 16), (17, 18)),
+                      ((0, 3), (13, 16), (19, 20)), ((20, 23), (19, 20), (20, 23))]
+        region, width = ((8, 5), (18, 3), (4, 5)), (4, 4, 4)
+        centre = (11.0, 12.0, 12.0)
+    else:
+        raise ValueError("num_dim must be 2 or 3")
+    nx, ny, nz = dims
+    hole = _boxes_mask(dims, hole_boxes)
+    recv = _boxes_mask(dims, recv_boxes) & ~hole
+    c = [np.arange(n, dtype=np.float64) for n in dims]
+    zz, yy, xx = np.meshgrid(c[2], c[1], c[0], indexing="ij")
+    mean = np.zeros((5,) + xx.shape)
+    mean[1], mean[2] = 0.3, 0.2
+    if num_dim == 3:
+        mean[3] = 0.1
+    mean[4] = 1.0 / gamma
+    state = np.zeros((5,) + xx.shape)
+    r2 = (xx - centre[0]) ** 2 + (yy - centre[1]) ** 2 + (zz - centre[2]) ** 2
+    state[4] = 1e-3 * _gauss(r2, 6.0)
+    state[1] = 2e-4 * _gauss(r2, 8.0)
+    blk = Block(xx, yy, zz if num_dim == 3 else np.zeros_like(xx), mean, state)
+    kk, jj, ii = np.nonzero(recv)
+    order = np.lexsort((ii, jj, kk))  # i fastest
+    ii, jj, kk = ii[order], jj[order], kk[order]
+    (ri, rn), (rj, rm), (rk, rl) = region
+    donor = np.stack([ri + ii % rn, rj + jj % rm, (rk + kk % rl) if num_dim == 3 else np.zeros_like(kk)], axis=1)
+    W = width[0] * width[1] * width[2]
+    ovs = overset_mod.OversetMap(
+        num_dim=num_dim, block_points=[nx * ny * nz], recv_block=np.zeros(ii.size, np.int32),
+        recv_ijk=np.stack([ii, jj, kk], axis=1).astype(np.int32), donor_block=np.zeros(ii.size, np.int32),
+        donor_ijk=donor.astype(np.int32), width=width, weights=rng.uniform(0.5, 1.5, size=(ii.size, W)),
+        hole_block=np.zeros(int(hole.sum()), np.int32), hole_ijk=_hole_ijk(hole))
+    return Case(name=f"holes{num_dim}d", num_dim=num_dim, blocks=[blk], gamma=gamma, nsteps=nsteps,
+                overset=ovs, notes=f"{num_dim}-D block {dims} with hand-set holes and receivers")
+
+
+def _hole_ijk(hole: np.ndarray) -> np.ndarray:
+    kk, jj, ii = np.nonzero(hole)
+    order = np.lexsort((ii, jj, kk))
+    return np.stack([ii[order], jj[order], kk[order]], axis=1).astype(np.int32)

@@ -1,7 +1,8 @@
 """Compile the C restatement (oracle/lee_oracle.c) into oracle/liblee_oracle.so.
 
 Test infrastructure only. Built without FMA contraction, like the reference's
-own x86-64 -O3 build, so the restatement's rounding follows the reference's.
+own x86-64 -O3 build, so the restatement's rounding follows the reference's. The point
+and line loops run on all host threads (OpenMP); each point's arithmetic is unchanged.
 """
 from __future__ import annotations
 
@@ -17,7 +18,7 @@ def build() -> str:
     src = os.path.join(HERE, "lee_oracle.c")
     if os.path.isfile(LIB) and os.path.getmtime(LIB) >= os.path.getmtime(src):
         return LIB
-    cmd = ["gcc", "-O2", "-std=c11", "-D_GNU_SOURCE", "-fPIC", "-shared", "-ffp-contract=off",
+    cmd = ["gcc", "-O2", "-std=c11", "-D_GNU_SOURCE", "-fPIC", "-shared", "-ffp-contract=off", "-fopenmp",
            "-Wall", "-Wno-unused-variable", "-o", LIB, src, "-lm"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

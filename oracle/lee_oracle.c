@@ -21,6 +21,11 @@
 
 #include "../include/lee_b200.h"
 
+/* The point loops of the time advance run on all host threads (OpenMP): every point, and
+ * every line of a directional pass, is computed by the same operations in the same order
+ * whichever thread takes it, so the results are the same bits as a serial run. */
+#define PAR_FOR _Pragma("omp parallel for schedule(static)")
+
 #define NOTBLANKED 0
 #define BLANKED 1
 #define INTERPOLATED (-1)
@@ -93,6 +98,8 @@ struct orc_ctx {
   int wave_type, wave_form, wave_dir;
   double wave_amp, wave_len, wave_hw;
   int axisym; /* UserInput::axisym (src/core/input.cpp:105-108) */
+  double *scr[3]; /* work fields of the right-hand side, scrn points each */
+  size_t scrn;
   char err[512];
 };
 typedef struct orc_ctx orc_ctx;
@@ -185,6 +192,81 @@ static int make_filter(op_t *o, int scheme, int order, double strength) {
   return 1;
 }
 
+/* One line of apply_dir: the line at (b1, b2) across the operator's direction. Returns -1
+ * where the reference's fluid-support assert would fire. */
+static int apply_line(const op_t *o, const int *iblank, const double *f, double *out, int b1, int b2, int st1,
+                      int st2, int nd, int sd, int h, int nb, int S) {
+  int base = b1 * st1 + b2 * st2;
+  for (int i = 0; i < nd; ++i) out[base + i * sd] = 0.0;
+  for (int i = h; i <= nd - 1 - h; ++i) {
+    int l0 = base + i * sd;
+    double acc = out[l0];
+    for (int l = -h; l <= h; ++l) acc += o->c[l + h] * f[l0 + l * sd];
+    out[l0] = acc;
+  }
+  for (int i = 0; i < h; ++i) { /* left boundary rows anchored at the first point */
+    int l0 = base + i * sd;
+    double acc = out[l0];
+    for (int s = 0; s < S; ++s) acc += o->B[i][s] * f[base + s * sd];
+    out[l0] = acc;
+  }
+  for (int i = nd - 1; i > nd - 1 - h; --i) { /* right rows mirrored from the last point */
+    int r = nd - 1 - i;
+    int l0 = base + i * sd, le = base + (nd - 1) * sd;
+    double acc = out[l0];
+    for (int s = 0; s < S; ++s) acc += o->mfac * o->B[r][s] * f[le - s * sd];
+    out[l0] = acc;
+  }
+  if (!iblank) return 0;
+  int last = iblank[base];
+  for (int i = 0; i < nd; ++i) {
+    int l0 = base + i * sd;
+    int my = iblank[l0];
+    if (my == BLANKED) {
+      if (last == BLANKED) {
+        out[l0] = 0.0;
+      } else if (last / BLANKED) { /* `last_iblank /= BLANKED` (:1391): true only after an INTERPOLATED point */
+        if (i > 0) {
+          for (int ib = 0; ib < nb; ++ib) {
+            int p = i - 1 - ib;
+            if (p < 0) return -1;
+            if (iblank[base + p * sd] > 0) return -1;
+          }
+          if (i - 1 - (S - 1) < 0) return -1; /* the rows would read outside the line */
+          int lref = base + (i - 1) * sd;
+          for (int ib = 0; ib < nb; ++ib) {
+            int p = i - 1 - ib;
+            if (p >= 0 && p <= nd - 1) {
+              int l1 = base + p * sd;
+              out[l1] = 0.0;
+              for (int s = 0; s < S; ++s) out[l1] += o->mfac * o->B[ib][s] * f[lref - s * sd];
+            }
+          }
+        }
+      }
+    } else {
+      if (last == BLANKED && i <= nd - 1) {
+        for (int ib = 0; ib < nb; ++ib) {
+          int p = i + ib;
+          if (p > nd - 1) return -1;
+          if (iblank[base + p * sd] > 0) return -1;
+        }
+        if (i + S - 1 > nd - 1) return -1; /* the rows would read outside the line */
+        for (int ib = 0; ib < nb; ++ib) {
+          int p = i + ib;
+          if (p >= 0 && p <= nd - 1) {
+            int l1 = base + p * sd;
+            out[l1] = 0.0;
+            for (int s = 0; s < S; ++s) out[l1] += o->B[ib][s] * f[l0 + s * sd];
+          }
+        }
+      }
+    }
+    last = my;
+  }
+  return 0;
+}
+
 /* ---------------------------------------------------------------------------
  * One directional application of an operator to f, written to out:
  * StandardCentral::apply_spatial_discretization (src/solver/spatial_discretization.cpp:1078-1290)
@@ -199,78 +281,15 @@ static int apply_dir(const op_t *o, const blk_t *bk, const int *iblank, const do
   int nd = n[d], sd = st[d];
   int o1 = (d == 0) ? 1 : 0, o2 = (d == 2) ? 1 : 2;
   int h = o->h, nb = o->nb, S = o->S;
-  for (int b2 = 0; b2 < n[o2]; ++b2)
-    for (int b1 = 0; b1 < n[o1]; ++b1) {
-      int base = b1 * st[o1] + b2 * st[o2];
-      for (int i = 0; i < nd; ++i) out[base + i * sd] = 0.0;
-      for (int i = h; i <= nd - 1 - h; ++i) {
-        int l0 = base + i * sd;
-        double acc = out[l0];
-        for (int l = -h; l <= h; ++l) acc += o->c[l + h] * f[l0 + l * sd];
-        out[l0] = acc;
-      }
-      for (int i = 0; i < h; ++i) { /* left boundary rows anchored at the first point */
-        int l0 = base + i * sd;
-        double acc = out[l0];
-        for (int s = 0; s < S; ++s) acc += o->B[i][s] * f[base + s * sd];
-        out[l0] = acc;
-      }
-      for (int i = nd - 1; i > nd - 1 - h; --i) { /* right rows mirrored from the last point */
-        int r = nd - 1 - i;
-        int l0 = base + i * sd, le = base + (nd - 1) * sd;
-        double acc = out[l0];
-        for (int s = 0; s < S; ++s) acc += o->mfac * o->B[r][s] * f[le - s * sd];
-        out[l0] = acc;
-      }
-      if (!iblank) continue;
-      int last = iblank[base];
-      for (int i = 0; i < nd; ++i) {
-        int l0 = base + i * sd;
-        int my = iblank[l0];
-        if (my == BLANKED) {
-          if (last == BLANKED) {
-            out[l0] = 0.0;
-          } else if (last / BLANKED) { /* `last_iblank /= BLANKED` (:1391): true only after an INTERPOLATED point */
-            if (i > 0) {
-              for (int ib = 0; ib < nb; ++ib) {
-                int p = i - 1 - ib;
-                if (p < 0) return -1;
-                if (iblank[base + p * sd] > 0) return -1;
-              }
-              if (i - 1 - (S - 1) < 0) return -1; /* the rows would read outside the line */
-              int lref = base + (i - 1) * sd;
-              for (int ib = 0; ib < nb; ++ib) {
-                int p = i - 1 - ib;
-                if (p >= 0 && p <= nd - 1) {
-                  int l1 = base + p * sd;
-                  out[l1] = 0.0;
-                  for (int s = 0; s < S; ++s) out[l1] += o->mfac * o->B[ib][s] * f[lref - s * sd];
-                }
-              }
-            }
-          }
-        } else {
-          if (last == BLANKED && i <= nd - 1) {
-            for (int ib = 0; ib < nb; ++ib) {
-              int p = i + ib;
-              if (p > nd - 1) return -1;
-              if (iblank[base + p * sd] > 0) return -1;
-            }
-            if (i + S - 1 > nd - 1) return -1; /* the rows would read outside the line */
-            for (int ib = 0; ib < nb; ++ib) {
-              int p = i + ib;
-              if (p >= 0 && p <= nd - 1) {
-                int l1 = base + p * sd;
-                out[l1] = 0.0;
-                for (int s = 0; s < S; ++s) out[l1] += o->B[ib][s] * f[l0 + s * sd];
-              }
-            }
-          }
-        }
-        last = my;
-      }
+  int nlines = n[o1] * n[o2], bad = 0;
+  PAR_FOR
+  for (int line = 0; line < nlines; ++line) {
+    if (apply_line(o, iblank, f, out, line % n[o1], line / n[o1], st[o1], st[o2], nd, sd, h, nb, S)) {
+#pragma omp atomic write
+      bad = 1;
     }
-  return 0;
+  }
+  return bad ? -1 : 0;
 }
 
 /* take_derivative_xi_eta_zeta (:1322-1336): dflux <- 0, then the operator; a
@@ -286,18 +305,32 @@ static int d_xi(orc_ctx *c, const blk_t *bk, const int *ib, const double *f, dou
 }
 
 /* take_derivative_xyz (:1802-1826): dflux = J * sum_l metrics[l][i] * d/dxi_l f. */
-static int d_x(orc_ctx *c, const blk_t *bk, const double *f, double *out, int i, double *work) {
+static int d_x(orc_ctx *c, const blk_t *bk, const double *f, double *out, int i, double *work, double *sum) {
   int nd = c->cfg.num_dim, N = bk->N;
-  double *sum = dalloc((size_t)N);
+  PAR_FOR
+  for (int p = 0; p < N; ++p) sum[p] = 0.0;
   for (int l = 0; l < nd; ++l) {
     int rc = d_xi(c, bk, bk->iblank, f, work, l);
-    if (rc) { free(sum); return rc; }
+    if (rc) return rc;
     const double *m = bk->met[l * 3 + i];
+    PAR_FOR
     for (int p = 0; p < N; ++p) sum[p] += m[p] * work[p];
   }
+  PAR_FOR
   for (int p = 0; p < N; ++p) out[p] = sum[p] * bk->jac[p];
-  free(sum);
   return 0;
+}
+
+/* Three work fields of at least n points, kept by the context between calls. */
+static double **scratch(orc_ctx *c, size_t n) {
+  if (c->scrn < n) {
+    for (int k = 0; k < 3; ++k) {
+      free(c->scr[k]);
+      c->scr[k] = dalloc(n);
+    }
+    c->scrn = n;
+  }
+  return c->scr;
 }
 
 /* ---------------------------------------------------------------------------
@@ -403,6 +436,7 @@ static int compute_metrics(orc_ctx *c, blk_t *bk) {
 /* State::compute_auxiliary_variables_linear_Euler (src/core/state.cpp:701-736). */
 static void compute_aux(orc_ctx *c, blk_t *bk, double *const *y) {
   double g = c->cfg.gamma, gi = 1.0 / g, gg = g / (g - 1.0);
+  PAR_FOR
   for (int p = 0; p < bk->N; ++p) {
     double sbar = bk->mean[0][p], pbar = bk->mean[4][p];
     double pbi = 1.0 / pbar;
@@ -492,41 +526,51 @@ static void wave_at(const orc_ctx *c, const blk_t *bk, int l0, double time, doub
 static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, double time) {
   int nd = c->cfg.num_dim, N = bk->N;
   double g = c->cfg.gamma;
-  double *df = dalloc((size_t)N), *work = dalloc((size_t)N);
+  double **scr = scratch(c, (size_t)N);
+  double *df = scr[0], *work = scr[1], *sum = scr[2];
   int rc = 0;
   for (int v = 0; v < 5; ++v) memset(rhs[v], 0, sizeof(double) * (size_t)N);
   for (int j = 0; j < nd && !rc; ++j) { /* entropy */
-    rc = d_x(c, bk, y[0], df, j, work);
+    rc = d_x(c, bk, y[0], df, j, work, sum);
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[0][p] -= bk->mean[1 + j][p] * df[p];
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[0][p] -= y[1 + j][p] * bk->grad[0 * nd + j][p];
   }
   for (int i = 0; i < nd && !rc; ++i) { /* velocity */
     for (int j = 0; j < nd && !rc; ++j) {
-      rc = d_x(c, bk, y[1 + i], df, j, work);
+      rc = d_x(c, bk, y[1 + i], df, j, work, sum);
+      PAR_FOR
       for (int p = 0; p < N; ++p) rhs[1 + i][p] -= bk->mean[1 + j][p] * df[p];
+      PAR_FOR
       for (int p = 0; p < N; ++p)
         rhs[1 + i][p] -= (y[1 + j][p] + bk->aux[0][p] / bk->aux[1][p] * bk->mean[1 + j][p]) *
                          bk->grad[(1 + i) * nd + j][p];
     }
-    if (!rc) rc = d_x(c, bk, y[4], df, i, work);
+    if (!rc) rc = d_x(c, bk, y[4], df, i, work, sum);
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[1 + i][p] -= df[p] / bk->aux[1][p];
   }
   for (int j = 0; j < nd && !rc; ++j) { /* pressure */
-    rc = d_x(c, bk, y[4], df, j, work);
+    rc = d_x(c, bk, y[4], df, j, work, sum);
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[4][p] -= bk->mean[1 + j][p] * df[p];
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[4][p] -= y[1 + j][p] * bk->grad[4 * nd + j][p];
-    if (!rc) rc = d_x(c, bk, y[1 + j], df, j, work);
+    if (!rc) rc = d_x(c, bk, y[1 + j], df, j, work, sum);
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[4][p] -= g * bk->mean[4][p] * df[p];
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[4][p] -= g * y[4][p] * bk->grad[(1 + j) * nd + j][p];
   }
-  free(df);
-  free(work);
   if (rc) return rc;
   if (c->axisym) /* additional terms due to axisymmetry (:2118-2126), IVAR_UR = 2, RDIR = 1 */
+    PAR_FOR
     for (int p = 0; p < N; ++p)
       rhs[4][p] -= g * (bk->mean[4][p] * y[2][p] + y[4][p] * bk->mean[2][p]) / (bk->xyz[1][p] + 1e-99);
   if (c->src_kind == LEE_SOURCE_DISTRIBUTED && bk == &c->blk[(int)c->dsrc[0]] && c->dsrc_g) {
     double fac = (g - 1.0) * sin(c->dsrc[1] * time);
+    PAR_FOR
     for (int p = 0; p < N; ++p) rhs[4][p] += fac * c->dsrc_g[p];
   }
   int bix = (int)(bk - &c->blk[0]);
@@ -541,6 +585,7 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
     By *= pow(b, 2);
     double angular_frequency = frequency * twopi;
     double amp_cos_wt = amplitude * cos(angular_frequency * time);
+    PAR_FOR
     for (int p = 0; p < N; ++p) {
       double xloc = bk->xyz[0][p], yloc = bk->xyz[1][p];
       rhs[4][p] += exp(-(Bx * xloc * xloc + By * yloc * yloc)) * amp_cos_wt;
@@ -559,6 +604,7 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
     }
     double fac = amp * (g - 1.0) * ramp * sin(om * time);
     double ef = -log(2.0) / (b * b);
+    PAR_FOR
     for (int p = 0; p < N; ++p) {
       double dx = bk->xyz[0][p] - x0, dy = bk->xyz[1][p] - y0, dz = bk->xyz[2][p] - z0;
       rhs[4][p] += fac * exp(ef * (dx * dx + dy * dy + dz * dz));
@@ -689,6 +735,7 @@ static int filter_block(orc_ctx *c, blk_t *bk, double **y) {
       }
       memcpy(func, out, sizeof(double) * (size_t)N);
     }
+    PAR_FOR
     for (int p = 0; p < N; ++p) y[v][p] = rem * func0[p] + blend * func[p];
   }
   free(func0); free(func); free(out);
@@ -756,6 +803,7 @@ void orc_destroy(orc_ctx *c) {
     for (int q = 0; q < 4; ++q) free(bk->aux[q]);
     for (int q = 0; q < bk->nbnd; ++q) free(bk->bnd[q].sigma);
   }
+  for (int k = 0; k < 3; ++k) free(c->scr[k]);
   free(c->ovs.rb); free(c->ovs.db); free(c->ovs.rl); free(c->ovs.dl); free(c->ovs.wt); free(c->ovs.buf);
   free(c->dsrc); free(c->dsrc_g); free(c->mic);
   free(c);
@@ -1069,14 +1117,15 @@ int orc_prepare(orc_ctx *c) {
         compute_sigma(c, bk, &bk->bnd[zi]);
     /* mean gradients: spatial::precompute_something (:2250-2271), with hole closures */
     int nd = c->cfg.num_dim;
-    double *work = dalloc((size_t)bk->N);
+    double *work = dalloc((size_t)bk->N), *sum = dalloc((size_t)bk->N);
     for (int v = 0; v < 5; ++v)
       for (int j = 0; j < nd; ++j) {
         bk->grad[v * nd + j] = dalloc((size_t)bk->N);
-        rc = d_x(c, bk, bk->mean[v], bk->grad[v * nd + j], j, work);
-        if (rc) { free(work); return rc; }
+        rc = d_x(c, bk, bk->mean[v], bk->grad[v * nd + j], j, work, sum);
+        if (rc) { free(work); free(sum); return rc; }
       }
     free(work);
+    free(sum);
     compute_aux(c, bk, bk->sol);
     if (c->src_kind == LEE_SOURCE_DISTRIBUTED && b == (int)c->dsrc[0]) prolong_distributed(c, bk);
   }
@@ -1223,6 +1272,7 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
       for (int b = 0; b < nb && !rc; ++b) {
         blk_t *bk = &c->blk[b];
         rc = rhs_block(c, bk, zi[b], rhs[b], tn + ci[s] * h);
+        PAR_FOR
         for (int p = 0; p < bk->N; ++p) {
           if (!(bk->iblank && bk->iblank[p] == BLANKED)) {
             for (int v = 0; v < 5; ++v) {

@@ -53,6 +53,11 @@ OVERSET_WORKLOADS = {
     # sponges, shear layer, monopole, and a pulse that crosses the overlap
     "cylinder2d_64": lambda: cases.cylinder2d(nb=64, length=16.0, ntheta=72, nr=24, r_out=3.0, first_cell=0.05,
                                               r_cut=1.0, sponge=4, nsteps=40, pulse=(1.8, 0.6, 1e-3, 0.5)),
+    # one block with hand-set holes and self-donated receivers: every hole-closure branch of
+    # iblank_correction (a hole after fluid, after a receiver, after a hole; fluid and receivers
+    # after a hole; holes at line starts and ends) along every direction, in 2-D and 3-D
+    "holes2d": lambda: cases.holes(2, nsteps=12),
+    "holes3d": lambda: cases.holes(3, nsteps=8),
 }
 
 

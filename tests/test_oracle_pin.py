@@ -110,7 +110,7 @@ def check_overset_maps(solver, g, case):
         np.testing.assert_array_equal(m["recv_l0"][m["recv_block"] == b], g[f"recv_l0_{b}"])
 
 
-OVERSET_NAMES = ["cylinder2d_64"]
+OVERSET_NAMES = ["cylinder2d_64", "holes2d", "holes3d"]
 
 
 @pytest.mark.parametrize("name", OVERSET_NAMES)
@@ -156,3 +156,36 @@ def test_oracle_overset_matches_reference_live(oracle_lib):
     s.advance(case.nsteps, dt)
     for b in range(2):
         np.testing.assert_array_equal(s.download(b)[0], ref[b])
+
+
+def _transitions(iblank: np.ndarray, axis: int) -> set:
+    """The hole-closure branches that occur along one axis of an (nz, ny, nx) iblank array, as the
+    reference's per-line scan meets them (src/solver/spatial_discretization.cpp:1356-1652)."""
+    BL, RC, FL = 1, -1, 0
+    lines = np.moveaxis(iblank, axis, -1).reshape(-1, iblank.shape[axis])
+    seen = set()
+    for ln in lines:
+        if ln[0] == BL:
+            seen.add("hole at line start")
+        if ln[-1] == BL:
+            seen.add("hole at line end")
+        for a, b in zip(ln[:-1], ln[1:]):
+            if b == BL:
+                seen.add({FL: "hole after fluid", RC: "hole after receiver", BL: "hole after hole"}[int(a)])
+            elif a == BL:
+                seen.add("fluid after hole" if b == FL else "receiver after hole")
+    return seen
+
+
+@pytest.mark.parametrize("name", ["holes2d", "holes3d"])
+def test_hole_layouts_exercise_every_closure_branch(name):
+    """The hand-set hole workloads meet every branch of the hole scan along every direction
+    (the F8 branch, a hole after a plain fluid point, among them), on the iblank the reference
+    itself built from the overset file."""
+    g = load_golden(name)
+    ib = np.rint(g["iblank_0"]).astype(int)
+    nd = 3 if ib.shape[0] > 1 else 2
+    want = {"hole after fluid", "hole after receiver", "hole after hole", "fluid after hole",
+            "receiver after hole", "hole at line start", "hole at line end"}
+    for axis in range(3 - nd, 3):
+        assert _transitions(ib, axis) == want, (name, axis, want - _transitions(ib, axis))

@@ -211,11 +211,15 @@ def _overset_golden(name):
     return OVERSET_WORKLOADS[name]()
 
 
-def test_overset_maps_are_bit_exact(product_lib):
+OVERSET_NAMES = ["cylinder2d_64", "holes2d", "holes3d"]
+
+
+@pytest.mark.parametrize("name", OVERSET_NAMES)
+def test_overset_maps_are_bit_exact(product_lib, name):
     """The receiver and donor indices and the normalised weights the GPU holds equal the
     reference's overset::receiverCells / donorCells, to the last bit."""
-    g = load_golden("cylinder2d_64")
-    case = _overset_golden("cylinder2d_64")
+    g = load_golden(name)
+    case = _overset_golden(name)
     m = api.Solver(product_lib, case).get_overset()
     for b in range(len(case.blocks)):
         sel = m["donor_block"] == b
@@ -224,28 +228,34 @@ def test_overset_maps_are_bit_exact(product_lib):
         np.testing.assert_array_equal(m["recv_l0"][m["recv_block"] == b], g[f"recv_l0_{b}"])
 
 
-def test_overset_fp64_steps(product_lib):
-    g = load_golden("cylinder2d_64")
-    case = _overset_golden("cylinder2d_64")
+@pytest.mark.parametrize("name", OVERSET_NAMES)
+def test_overset_fp64_steps(product_lib, name):
+    """holes2d / holes3d: a hole after fluid (no closure, the reference's `last_iblank /=
+    BLANKED`), after a receiver (right closure), after a hole (zero), fluid and receivers after a
+    hole (left closure), holes at line starts and ends, along every direction."""
+    g = load_golden(name)
+    case = _overset_golden(name)
+    nb = len(case.blocks)
     s = api.Solver(product_lib, case)
     dt = float(g["dt"])
     assert abs(s.compute_dt() - dt) <= 1e-14 * dt
-    for b in range(2):
+    for b in range(nb):
         assert rl2(s.eval_rhs(b, 0.0), g[f"rhs_{b}"]) <= 1e-12
     s.advance(1, dt)
-    for b in range(2):
+    for b in range(nb):
         assert rl2(s.download(b)[0], g[f"step1_{b}"]) <= 1e-12
     s.advance(int(g["nsteps"]) - 1, dt)
-    for b in range(2):
+    for b in range(nb):
         assert rl2(s.download(b)[0], g[f"stepn_{b}"]) <= 1e-10
 
 
-def test_overset_fp32_compensated_steps(product_lib):
-    g = load_golden("cylinder2d_64")
-    case = _overset_golden("cylinder2d_64")
+@pytest.mark.parametrize("name", OVERSET_NAMES)
+def test_overset_fp32_compensated_steps(product_lib, name):
+    g = load_golden(name)
+    case = _overset_golden(name)
     s = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
     s.advance(int(g["nsteps"]), float(g["dt"]))
-    for b in range(2):
+    for b in range(len(case.blocks)):
         assert rl2(s.download(b)[0][4], g[f"stepn_{b}"][4]) <= 1e-5
 
 
