@@ -91,8 +91,11 @@ __global__ void __launch_bounds__(256) k_filter(FilterParams<T> p) {
   const int n = p.dir == 0 ? p.nx : (p.dir == 1 ? p.ny : p.nz);
   const long long sd = p.dir == 0 ? 1 : (p.dir == 1 ? (long long)p.nx : nxy);
   const bool hole = p.last && p.iblank && p.iblank[l] == 1;
+  // a hole after a hole: the reference writes F = 0 there, so the increment is D = -x, and a
+  // later pass of a 3-D block reads the zero (the other codes give D = F - I directly)
+  const bool zero = COMP && p.code && p.code[l] == kCodeZero;
   for (int v = 0; v < p.V; ++v) {
-    const T f = dop<T>(p.op, p.in[v], l, pos, n, sd, p.code);
+    const T f = zero ? -p.in[v][l] : dop<T>(p.op, p.in[v], l, pos, n, sd, p.code);
     if (!COMP) {
       T o = f;
       if (p.last) o = (T(1) - p.blend) * p.y0[v][l] + p.blend * f;
