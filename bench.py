@@ -93,20 +93,21 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def stage_bytes_per_point(info, comp: bool) -> float:
+def stage_bytes_per_point(info, comp: bool, sponge_field: bool) -> float:
     """Algorithmic HBM bytes per grid point of one fused stage launch, averaged over the
     four RK4 stages: every stage reads its input, y_n and the accumulator once and writes
     the next input and the accumulator once (words per stage: FP64 3,5,5,3 x V;
-    compensated 4,5,5,5 x V), plus the non-uniform coefficient fields."""
+    compensated 4,5,5,5 x V), plus the non-uniform coefficient fields (J*metrics) and the
+    summed sponge-strength field the TMA stage kernels read where sponges exist."""
     V, e = info.state_vars, info.bytes_per_value
     words = (4 + 5 + 5 + 5) / 4.0 if comp else (3 + 5 + 5 + 3) / 4.0
-    return words * V * e + info.num_coef_fields * e
+    return words * V * e + (info.num_coef_fields + (1 if sponge_field else 0)) * e
 
 
-def step_bytes_per_point(info, comp: bool, dim: int) -> float:
-    """Algorithmic bytes per grid point per RK4 step: four stages and the filter. The fused
-    filter reads the pre-filter state once and writes the filtered state once (FP64: 2 V
-    words; compensated: y_pre and its rounding error in, y and its error out, 4 V words)."""
+def filter_bytes_per_point(info, comp: bool, dim: int) -> float:
+    """The fused filter reads the pre-filter state once and writes the filtered state once
+    (FP64: 2 V words; compensated: y_pre and its rounding error in, y and its error out, 4 V
+    words); the per-direction passes move more."""
     V, e = info.state_vars, info.bytes_per_value
     if info.tma_filter:
         filt = 4 if comp else 2
@@ -114,7 +115,21 @@ def step_bytes_per_point(info, comp: bool, dim: int) -> float:
         filt = {2: 3 + 6, 3: 3 + 4 + 6}[dim]
     else:
         filt = {2: 2 + 3, 3: 2 + 2 + 3}[dim]
-    return 4 * stage_bytes_per_point(info, comp) + filt * V * e
+    return filt * V * e
+
+
+def step_bytes_per_point(info, comp: bool, dim: int, sponge_field: bool) -> float:
+    """Algorithmic bytes per grid point per RK4 step as this build schedules it: four stages
+    and the filter."""
+    return 4 * stage_bytes_per_point(info, comp, sponge_field) + filter_bytes_per_point(info, comp, dim)
+
+
+def contract_bytes_per_point(info, comp: bool, sponge_field: bool) -> float:
+    """The byte contract of a classic RK4 step, independent of this build's schedule: 18 V state
+    words (plain FP64) or 20 V (FP32 with a persistent compensation word read and written once
+    per step), plus every per-point coefficient field read once per stage."""
+    V, e = info.state_vars, info.bytes_per_value
+    return (20 if comp else 18) * V * e + 4 * (info.num_coef_fields + (1 if sponge_field else 0)) * e
 
 
 SPONGE_FRACTION = 16.0 / 256.0  # sponge width per side, relative to the block size
@@ -123,7 +138,8 @@ SPONGE_CONSTANT = 1.0
 
 WORKLOADS = {
     "curvi3d": "curvi3d {n}^3 Mach 0.5, 8 Gaussian pulses (seed 2), RK4 CFL 0.5, OA4 central FD + OA8 filter, "
-               "Freund sponges n/16 wide (constant 1)",
+               "plus an added Freund sponge frame n/16 wide (constant 1) that the plain curvilinear workload "
+               "does not have",
     "pulse2d": "pulse2d {n}^2 on [-50,50]^2, quiescent, Gaussian p' pulse, RK4 CFL 0.5, OA4 FD + OA8 filter, "
                "20-cell Freund sponges (constant 5)",
     "batch": "batch2d: 64 independent 2-D Cartesian instances, sides round(exp(U[ln 64, ln 512])) (seed 4, "
@@ -134,16 +150,12 @@ WORKLOADS = {
 }
 
 
-def run_batch(args) -> None:
+def batch_result(args, K: int, W: int, sample_clocks: bool) -> dict:
     """The batch workload: 64 instances of uneven sizes advanced together (lee_advance_blocks,
     FP32-compensated and FP64) and, for comparison, one at a time in plain FP64 (each instance
-    in its own context, its own time step)."""
+    in its own context, its own time step). Returns the measured figures."""
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    K, W = args.steps, args.warmup
     case = cases.batch2d(nsteps=K)
     lib = api.product_library()
     npts = case.npoints
@@ -154,7 +166,7 @@ def run_batch(args) -> None:
         dts = s.compute_dt_blocks()
         s.advance_blocks(W, dts)
         torch.cuda.synchronize()
-        sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) if form == "fp32c" else None
+        sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) if form == "fp32c" and sample_clocks else None
         if sampler:
             sampler.start()
             time.sleep(0.3)
@@ -197,30 +209,44 @@ def run_batch(args) -> None:
     filt_b = 4 * 4 * 4 * npts
     step_b = 4 * stage_b + filt_b
     achieved = stage_b / (stage_avg / 1e3) / 1e9
+    return {
+        "workload": WORKLOADS["batch"], "points": npts, "blocks": len(case.blocks), "steps": K,
+        "value": value, "ms_per_step": res["fp32c"]["ms"] / K,
+        "fp64": {"value": value64, "ms_per_step": res["fp64"]["ms"] / K},
+        "mixed_over_fp64": value / value64,
+        "one_at_a_time_fp64": {"value": alone, "ms_per_step": alone_s * 1e3 / K, "batched_fp32c_over_it": value / alone},
+        "p_rel_l2_vs_fp64_alone": {"max": max(errs), "median": float(np.median(errs)), "steps": n_done},
+        "roofline": {"bound": "hbm", "kernel": "batched RK stage (fp32-compensated)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} copy bandwidth", "traffic": None,
+                     "avg_launch_ms": stage_avg, "filter_avg_launch_ms": filt_avg,
+                     "filter_gbs": filt_b / (filt_avg / 1e3) / 1e9,
+                     "step_gbs": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9,
+                     "step_frac": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9 / peak,
+                     "stage_strip": list(info.batch_stage_tile), "filter_strip": list(info.batch_filter_tile)},
+        "gpu_launches": int(res["fp32c"]["launches"]), "clocks": clocks,
+    }
+
+
+def run_batch(args) -> None:
+    """`--workload batch`: the batch figures as the bench line."""
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    r = batch_result(args, args.steps, args.warmup, sample_clocks=True)
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value * world, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": res["fp32c"]["ms"] / K, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": r["value"] * world, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32-compensated (fp64 setup)", "data": "synthetic",
-            "config": {"workload": WORKLOADS["batch"], "points_per_gpu": npts, "blocks": len(case.blocks),
-                       "l2": f"state {5 * npts * 4 / 1e6:.0f} MB fp32 vs 126 MB L2 (inputs larger than L2)",
+            "config": {"workload": r["workload"], "points_per_gpu": r["points"], "blocks": r["blocks"],
+                       "l2": f"state {5 * r['points'] * 4 / 1e6:.0f} MB fp32 vs 126 MB L2",
                        "launch": "batched kernels in replayed CUDA step graphs"},
-            "fp64": {"value": value64, "ms_per_step": res["fp64"]["ms"] / K},
-            "mixed_over_fp64": value / value64,
-            "one_at_a_time_fp64": {"value": alone, "ms_per_step": alone_s * 1e3 / K,
-                                   "batched_fp32c_over_it": value / alone},
-            "p_rel_l2_vs_fp64_alone": {"max": max(errs), "median": float(np.median(errs)), "steps": n_done},
-            "roofline": {"bound": "hbm", "kernel": "batched RK stage (fp32-compensated)", "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": f"{peak_kind} copy bandwidth", "traffic": None,
-                         "avg_launch_ms": stage_avg, "filter_avg_launch_ms": filt_avg,
-                         "filter_gbs": filt_b / (filt_avg / 1e3) / 1e9,
-                         "step_gbs": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9,
-                         "step_frac": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9 / peak,
-                         "stage_strip": list(info.batch_stage_tile), "filter_strip": list(info.batch_filter_tile)},
-            "e2e": None,
-            "gpu_launches": int(res["fp32c"]["launches"]),
-            "clocks": clocks,
+            "fp64": r["fp64"], "mixed_over_fp64": r["mixed_over_fp64"],
+            "one_at_a_time_fp64": r["one_at_a_time_fp64"], "p_rel_l2_vs_fp64_alone": r["p_rel_l2_vs_fp64_alone"],
+            "roofline": r["roofline"], "e2e": None, "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
             "cpu_baseline": None,
         }
         print(json.dumps(line))
@@ -347,8 +373,11 @@ def run_ours(args) -> None:
     peak, peak_kind = measured_hbm_gbs()
     stage_avg_ms = st.stage_ms / max(st.stage_launches, 1)
     filt_avg_ms = st.filter_ms / max(st.filter_launches, 1)
-    stage_b = stage_bytes_per_point(info, True) * npts
+    sponge_field = info.tma_stage == 1 and any(bd.kind.startswith("sponge") for bd in case.boundaries)
+    stage_b = stage_bytes_per_point(info, True, sponge_field) * npts
     achieved = stage_b / (stage_avg_ms / 1e3) / 1e9
+    filt_b = filter_bytes_per_point(info, True, dim) * npts
+    filt_gbs = filt_b / (filt_avg_ms / 1e3) / 1e9
     # DRAM bytes of the two-point stage kernel measured by ncu (dram__bytes_read.sum +
     # dram__bytes_write.sum of one step's four launches at 160^3: 130.7 bytes per point on
     # average), scaled to this launch by its points; other kernels and workloads have no capture
@@ -356,17 +385,24 @@ def run_ours(args) -> None:
     if args.workload == "curvi3d" and info.stage_kernel == 2 and dim == 3:
         traffic = STAGE_PAIR_DRAM_BYTES_PER_POINT * npts
         traffic_src = "ncu at 160^3 (mean of the four stage launches of a step), scaled by points"
-    step_b = step_bytes_per_point(info, True, dim) * npts
+    step_b = step_bytes_per_point(info, True, dim, sponge_field) * npts
     step_gbs = step_b * K / (r32["ms"] / 1e3) / 1e9
+    contract_gbs = contract_bytes_per_point(info, True, sponge_field) * npts * K / (r32["ms"] / 1e3) / 1e9
     dominant = "stage" if st.stage_ms >= st.filter_ms else "filter"
 
     adjoint = None
     if args.workload == "curvi3d" and not args.no_adjoint:
         adjoint = run_adjoint(args, lib, barrier, max_over_ranks)
 
+    # the batch workload (64 uneven 2-D instances), FP32-compensated and FP64 batched and FP64
+    # one instance at a time, K steps each
+    batch = None
+    if args.workload == "curvi3d" and not args.no_batch:
+        batch = batch_result(args, args.batch_steps, W, sample_clocks=False)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args)
+        cpu = cpu_baseline(args, lib, local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -385,11 +421,14 @@ def run_ours(args) -> None:
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} copy bandwidth", "traffic": traffic,
                          "traffic_source": traffic_src,
-                         "bytes_per_point": stage_bytes_per_point(info, True),
+                         "bytes_per_point": stage_bytes_per_point(info, True, sponge_field),
                          "avg_launch_ms": stage_avg_ms, "dominant": dominant,
-                         "filter_avg_launch_ms": filt_avg_ms,
+                         "filter": {"achieved": filt_gbs, "frac": filt_gbs / peak, "avg_launch_ms": filt_avg_ms,
+                                    "bytes_per_point": filter_bytes_per_point(info, True, dim)},
                          "step_gbs": step_gbs, "step_frac": step_gbs / peak,
-                         "step_bytes_per_point": step_bytes_per_point(info, True, dim),
+                         "step_bytes_per_point": step_bytes_per_point(info, True, dim, sponge_field),
+                         "contract_bytes_per_point": contract_bytes_per_point(info, True, sponge_field),
+                         "contract_frac": contract_gbs / peak,
                          "tma_stage": info.tma_stage, "tma_filter": info.tma_filter,
                          "stage_chunk": info.stage_chunk, "filter_chunk": info.filter_chunk,
                          "filter_kernel": info.filter_kernel, "stage_kernel": info.stage_kernel,
@@ -401,6 +440,7 @@ def run_ours(args) -> None:
             "clocks": clocks,
             "cpu_baseline": cpu,
             "adjoint": adjoint,
+            "batch": batch,
         }
         print(json.dumps(line))
     solvers["fp32c"].close()
@@ -457,8 +497,11 @@ def reference_ranks(case: cases.Case, requested: int) -> int:
     return max(nprocs, len(case.blocks))  # one rank per block at least (src/parallel/decomp.cpp:19-30)
 
 
-def cpu_baseline(args) -> dict:
-    """The compiled reference (oracle/_ref) on a bounded sample of the workload, all host cores."""
+def cpu_baseline(args, lib=None, device: int = 0) -> dict:
+    """The compiled reference (oracle/_ref) on a bounded sample of the workload, all host cores,
+    at the FIX_CFL time step of the sample's first step. With `lib`, the CUDA library advances
+    the same sample in both forms and the errors against the reference's own state are
+    reported beside the timing."""
     try:
         from oracle import run_ref
         if not run_ref.available():
@@ -467,11 +510,29 @@ def cpu_baseline(args) -> dict:
         k = args.cpu_steps
         case, desc = reference_sample(args, args.workload, args.cpu_n, k)
         nprocs = reference_ranks(case, args.ref_ranks)
-        r = run_ref.run(case, mode="run", nsteps=k, dt=None, nprocs=nprocs, timeout=900)
+        dt = None
+        ours = {}
+        if lib is not None:
+            for form, prec in (("fp32c", api.FP32_COMPENSATED), ("fp64", api.FP64)):
+                s = api.Solver(lib, case, precision=prec, device=device)
+                dt = s.compute_dt(case.cfl)
+                s.advance(k, dt)
+                ours[form] = [s.download(b)[0] for b in range(len(case.blocks))]
+                s.close()
+        r = run_ref.run(case, mode="run", nsteps=k, dt=dt, nprocs=nprocs, timeout=900)
         sec = r["result"]["seconds"]
-        return {"value": case.npoints * k / sec, "unit": UNIT, "cores": nprocs, "kind": "reference",
-                "sample": f"{desc}, {k} RK4 steps (FIX_CFL), solver::solve wall time, {nprocs} MPI ranks "
-                          "(DECOMP_1D), g++ -O3"}
+        out = {"value": case.npoints * k / sec, "unit": UNIT, "cores": nprocs, "kind": "reference",
+               "sample": f"{desc}, {k} RK4 steps ({'FIX_DT at the CFL time step' if dt else 'FIX_CFL'}), "
+                         f"solver::solve wall time, {nprocs} MPI ranks (DECOMP_1D), g++ -O3"}
+        if ours:
+            ref = run_ref.assemble(case, r["ranks"])
+            pr = np.concatenate([y[4].ravel() for y in ref])
+            out["errors_vs_reference"] = {
+                "steps": k,
+                "fp32c_p_rel_l2": api.rel_l2(np.concatenate([y[4].ravel() for y in ours["fp32c"]]), pr),
+                "fp64_rel_l2": api.rel_l2(np.concatenate([y.ravel() for y in ours["fp64"]]),
+                                          np.concatenate([y.ravel() for y in ref]))}
+        return out
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
@@ -517,7 +578,9 @@ def main() -> int:
     ap.add_argument("--adjoint-n", type=int, default=192)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--cpu-n", type=int, default=64)
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch workload's figures in the default line")
+    ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--ref-n", type=int, default=64)
     ap.add_argument("--ref-ranks", type=int, default=0, help="reference MPI ranks (0: the host's cores, at most 8)")
     args = ap.parse_args()

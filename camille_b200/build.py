@@ -25,6 +25,13 @@ UNITS = {
     "lee_step.cu": [],
     "lee_tma.cu": [],
     "lee_capi.cu": [],
+    "lee_host_core.cu": [],
+    "lee_host_setup.cu": [],
+    "lee_host_kernels.cu": [],
+    "lee_host_batch.cu": [],
+    "lee_host_step.cu": [],
+    "lee_host_adjoint.cu": [],
+    "lee_host_overset.cu": [],
     "lee_static.cu": [],
     "lee_bc.cu": [],
     "lee_adjoint.cu": [],

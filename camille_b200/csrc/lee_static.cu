@@ -12,6 +12,7 @@
 // the library image: a file-scope __device__ array of kStaticFilterPoints doubles per pass
 // (2 x 8 MiB), which every GPU that loads the library holds until the process exits.
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -32,12 +33,33 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_scratch_addr[kMaxDevices] = {};
 
-int scratch_for_current_device(double** out) {
+// The device a pointer's memory lives on, or -1 when CUDA does not know it as device memory.
+int device_of(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();  // the lookup's error is not sticky: clear it
+    return -1;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) ? a.device : -1;
+}
+
+int scratch_for_current_device(const void* d_in, const void* d_out, double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (e != cudaSuccess || dev < 0) {
     set_global_error("lee_filter_field_static: no current CUDA device");
     return LEE_ERR_NODEVICE;
+  }
+  if (dev >= kMaxDevices) {
+    char msg[128];
+    snprintf(msg, sizeof msg, "lee_filter_field_static: device %d is beyond the %d devices the library serves", dev,
+             kMaxDevices);
+    set_global_error(msg);
+    return LEE_ERR_UNSUPPORTED;
+  }
+  if (device_of(d_in) != dev || device_of(d_out) != dev) {
+    set_global_error("lee_filter_field_static: d_in and d_out must be device memory of the current device");
+    return LEE_ERR_ARG;
   }
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_scratch_addr[dev]) {
@@ -97,8 +119,16 @@ extern "C" int lee_filter_field_static(int num_dim, int filter_scheme, int filte
     set_global_error(msg);
     return LEE_ERR_ARG;
   }
+  // input and output ranges must not share any element: the passes read neighbours of
+  // every point of d_in while the last one writes d_out
+  const uintptr_t a0 = (uintptr_t)d_in, a1 = a0 + (uintptr_t)n * sizeof(double);
+  const uintptr_t b0 = (uintptr_t)d_out, b1 = b0 + (uintptr_t)n * sizeof(double);
+  if (a0 < b1 && b0 < a1) {
+    set_global_error("lee_filter_field_static: the input and output ranges overlap");
+    return LEE_ERR_ARG;
+  }
   double* scratch = nullptr;
-  int rc = scratch_for_current_device(&scratch);
+  int rc = scratch_for_current_device(d_in, d_out, &scratch);
   if (rc) return rc;
   // Every pass writes each scratch element it hands to the next pass, so nothing needs
   // clearing between calls. Calls that overlap on the GPU share the scratch and race.

@@ -127,7 +127,8 @@ typedef struct {
 int lee_create(const lee_config *cfg, lee_ctx **out);
 /* Release every device and host resource of the context. */
 void lee_destroy(lee_ctx *ctx);
-/* Message of the last failure on ctx (or of the last failed lee_create when ctx is NULL). */
+/* Message of the last failure on ctx; with ctx NULL, of the calling thread's last failed call
+ * without a context (lee_create, lee_filter_field_static). */
 const char *lee_last_error(const lee_ctx *ctx);
 
 /* Grid of block b: coordinates (io::read_grid, src/io/plot3d.cpp:443-671) and the
@@ -329,9 +330,10 @@ int lee_get_stats(lee_ctx *ctx, lee_stats *stats);
  * serves callers that cannot call cudaMalloc, such as a framework that owns the device
  * memory through its own allocator or a time loop that must not allocate). Applies the
  * dimension-split filter of spatial::apply_filter to one variable of one block without
- * holes: d_in and d_out are distinct device arrays of nxi*neta*nzeta doubles (i fastest),
- * owned by the caller; work is enqueued on `stream` (a cudaStream_t, NULL for the default
- * stream) and the call returns without synchronizing. The intermediate passes use a
+ * holes: d_in and d_out are device arrays of nxi*neta*nzeta doubles (i fastest) that do not
+ * overlap, owned by the caller and on the current device (as is `stream`); work is enqueued
+ * on `stream` (a cudaStream_t, NULL for the default stream) and the call returns without
+ * synchronizing. The intermediate passes use a
  * scratch array compiled into the library (2 x 2^20 doubles, held by every GPU that loads
  * the library until exit): fields above 2^20 points are refused with LEE_ERR_ARG. The first
  * call on each device looks up that array's device address; make it before any stream

@@ -18,6 +18,7 @@ Patches (each a small edit made by this script, not a stored diff):
       skipped when ORACLE_NO_WRITE is set (they write GBs at 256^3).
 
 Usage: python oracle/build_ref.py [--src /path/to/reference] [--jobs N]
+(the default source is $CAMILLE_REFERENCE, else the read-only checkout, see reference_root)
 """
 from __future__ import annotations
 
@@ -146,9 +147,15 @@ def build(src_root: str, jobs: int = 8) -> str:
     return exe
 
 
+def reference_root() -> str:
+    """Where the reference checkout lies: $CAMILLE_REFERENCE, else the read-only checkout this
+    recipe was written against."""
+    return os.environ.get("CAMILLE_REFERENCE", "/root/reference")
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=reference_root())
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     a = ap.parse_args()
     print(build(a.src, a.jobs))

@@ -61,3 +61,22 @@ def test_no_cpu_fallback_without_gpu(product_lib):
     with pytest.raises(api.LeeError) as e:
         api.Solver(product_lib, cases.pulse2d(n=32, sponge=0))
     assert e.value.code == 7  # LEE_ERR_NODEVICE
+
+
+@pytest.mark.parametrize("shift", [8, 8 * 50, -8 * 99])
+def test_static_filter_refuses_overlapping_ranges(shift):
+    """lee_filter_field_static reads stencil neighbours of every input point while its last pass
+    writes the output: input and output ranges that share any element are refused with
+    LEE_ERR_ARG before any device work (so this needs no GPU)."""
+    dll = C.CDLL(api.PRODUCT_LIB)
+    fn = dll.lee_filter_field_static
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                   C.c_void_p, C.c_void_p, C.c_void_p]
+    dll.lee_last_error.restype = C.c_char_p
+    dll.lee_last_error.argtypes = [C.c_void_p]
+    base = 1 << 20
+    rc = fn(2, api.FILTER["STANDARD_CENTRAL"], 8, 1.0, 1.0, 10, 10, 1, C.c_void_p(base), C.c_void_p(base + shift),
+            None)
+    assert rc == api.LEE_ERR_ARG
+    assert b"overlap" in dll.lee_last_error(None)

@@ -6,7 +6,8 @@ allocate -- and filters one field that the caller already holds on the device, k
 its intermediate passes in a scratch array compiled into the library. This test calls it
 through the C ABI on device buffers owned by torch and checks its output against
 lee_apply_filter (the context-based entry point) on two calls in a row, the second call
-reusing the scratch the first one left behind. It runs last (file name) so that a
+reusing the scratch the first one left behind, on a stream of its own, with neither torch's
+memory pool nor the device's free memory changing across it. It runs last (file name) so that a
 failure here cannot hide the other tests.
 """
 from __future__ import annotations
@@ -66,15 +67,24 @@ def test_static_filter_matches_context_filter(product_lib, label):
     blk = case.blocks[0]
     nx, ny, nz = blk.dims
     cfg = api.config_for(case)
-    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     variables = [0, 1, 2, 4] if case.num_dim == 2 else [0, 1, 2, 3, 4]
-    for call, v in enumerate(variables[:2]):  # two calls in a row on the shared scratch
+    side = torch.cuda.Stream()
+    # two calls in a row on the shared scratch: the first on torch's current stream, the second on
+    # a stream of its own; around the second (the library's kernels and its scratch are loaded by
+    # then) neither torch's pool nor the device's free memory may change
+    for call, v in enumerate(variables[:2]):
         d_in = torch.from_numpy(np.ascontiguousarray(blk.state[v])).cuda()
         d_out = torch.full_like(d_in, float("nan"))
-        rc = fn(case.num_dim, cfg.filter_scheme, cfg.filter_order, cfg.filter_strength, cfg.filter_blend,
-                nx, ny, nz, C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), stream)
-        assert rc == 0, err(None).decode()
+        strm = torch.cuda.current_stream() if call == 0 else side
         torch.cuda.synchronize()
+        reserved, (free, _) = torch.cuda.memory_reserved(), torch.cuda.mem_get_info()
+        rc = fn(case.num_dim, cfg.filter_scheme, cfg.filter_order, cfg.filter_strength, cfg.filter_blend,
+                nx, ny, nz, C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), C.c_void_p(strm.cuda_stream))
+        assert rc == 0, err(None).decode()
+        strm.synchronize()
+        if call == 1:
+            assert torch.cuda.memory_reserved() == reserved
+            assert torch.cuda.mem_get_info()[0] == free
         got = d_out.cpu().numpy()
         rel = api.rel_l2(got, ref[v])
         assert rel <= TOL, f"call {call}: relative L2 {rel:.3e}"
