@@ -104,6 +104,8 @@ SIGNATURES = {
     "set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "get_stats": (C.c_int, [C.c_void_p, C.POINTER(LeeStats)]),
     "set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_finite_check": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_wait_limit": (C.c_int, [C.c_void_p, C.c_double]),
     "set_filter_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "set_stage_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "set_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _LP, C.c_double]),

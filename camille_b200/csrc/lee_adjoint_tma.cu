@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
     T wc[5] = {T(0), T(0), T(0), T(0), T(0)};
     if (in_blk) {
       const int rel = pl - plo;
-      failed = !mbar_wait(&bar[rel % G::NSL], (unsigned)((rel / G::NSL) & 1));
+      failed = !mbar_wait(&bar[rel % G::NSL], (unsigned)((rel / G::NSL) & 1), P.wait_ns);
       const T* slot = ring + (rel % G::NSL) * NF * FBP;
       T w[5], jm[3], g[5];
       // G^zeta at the tile point, and w there

@@ -130,8 +130,8 @@ int lee_create(const lee_config* cfg, lee_ctx** out) {
   c->blk.resize((size_t)cfg->num_blocks);
   e = cudaSetDevice(cfg->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_err, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_err, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 2 * sizeof(int));
   if (e != cudaSuccess) {
     if (c->d_err) cudaFree(c->d_err);
     if (c->stream) cudaStreamDestroy(c->stream);

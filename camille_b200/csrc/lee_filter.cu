@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(256, PX * sizeof(T) == 16 ? 2 : 3)
     bool failed = false;
     if (in_blk) {
       const int rel = p - plo;
-      failed = !mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1));
+      failed = !mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1), P.wait_ns);
       // A: F_xi on the own rows (r = HF + wy_row) and the eta halo rows
       xi_rows(box, u1b, db);
     }

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -21,6 +22,9 @@
 using namespace lee;
 
 namespace lee {
+
+// the kernels' default limit of a wait on staged data: one second
+constexpr unsigned long long kDefaultWaitNs = 1000000000ull;
 
 struct Boundary {
   int kind, dir, end, lo[3], hi[3];
@@ -146,7 +150,9 @@ struct lee_ctx {
   bool wfl_sym = false;  // symmetric interior filter stencil: the vectorised filter kernel applies
   int filter_kernel = -1;  // lee_set_filter_kernel: -1/0 scalar, else vector group width
   int stage_kernel = -1;   // lee_set_stage_kernel: -1 default, else points per thread
-  int* d_err = nullptr;
+  int* d_err = nullptr;          // [0] a bounded wait gave up, [1] a non-finite state value was found
+  unsigned long long wait_ns = kDefaultWaitNs;  // limit of the kernels' waits on staged data
+  int finite_every = 0;          // lee_set_finite_check: steps between checks (0: end of each advance, -1: off)
   double* d_report = nullptr;  // -min and max of the five state slots (lee_state_minmax)
   double* d_staging = nullptr;  // FP64 field of compensated uploads and downloads
   // overset maps (host copies, then device arrays from lee_prepare)
@@ -290,6 +296,7 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
 template <typename T>
 int autotune(lee_ctx* c, BlockData& b);
 int check_device_error(lee_ctx* c);
+int check_finite(lee_ctx* c);
 template <typename T>
 int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e, double t, const double* t_tab, const int* ctr,
               int t_stride);
@@ -348,5 +355,9 @@ template <typename T>
 void launch_convert(cudaStream_t s, long long n, T* out, const double* in);
 template <typename T>
 void launch_to_double(cudaStream_t s, long long n, double* out, const T* y, const T* comp);
+// flag = 1 when some value of the V fields f (and e, when given) of n elements of esz bytes is
+// not finite
+cudaError_t launch_nonfinite(cudaStream_t s, long long n, int V, size_t esz, void* const* f, void* const* e,
+                             int* flag);
 
 }  // namespace lee

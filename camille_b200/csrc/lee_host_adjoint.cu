@@ -157,6 +157,7 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
     fp.blend = (T)c->cfg.filter_blend;
     for (int v = 0; v < V; ++v) fp.out[v] = (T*)a.mu[v];
     fp.errflag = c->d_err;
+    fp.wait_ns = c->wait_ns;
     int bx, by;
     filter_box(c, H, b.filter_ry, &bx, &by);
     FieldMaps fm;
@@ -234,6 +235,7 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
       tp.tiles_x = (b.nx + tx - 1) / tx;
       tp.k_chunk = std::min(b.nz, 32);
       tp.err = c->d_err;
+      tp.wait_ns = c->wait_ns;
       const int tiles = tp.tiles_x * ((b.ny + ty - 1) / ty);
       CK(launch_adj_tma<T>(am, tp, a.tma_jm, tiles, (b.nz + tp.k_chunk - 1) / tp.k_chunk, c->stream));
     } else {

@@ -14,6 +14,31 @@ __global__ void k_convert(long long n, T* out, const double* in) {
     out[l] = (T)in[l];
 }
 
+// flag = 1 when some element of the fields is not finite (vector loads: the fields are
+// cudaMalloc'd, and n is a multiple of the vector width or the tail is read one by one)
+template <typename T>
+__global__ void k_nonfinite(long long n, int nf, const T* f0, const T* f1, const T* f2, const T* f3, const T* f4,
+                            const T* f5, const T* f6, const T* f7, const T* f8, const T* f9, int* flag) {
+  const T* f[10] = {f0, f1, f2, f3, f4, f5, f6, f7, f8, f9};
+  using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  constexpr int W = (int)(sizeof(V4) / sizeof(T));
+  const long long nv = n / W;
+  bool bad = false;
+  for (int q = 0; q < nf; ++q) {
+    const V4* v = reinterpret_cast<const V4*>(f[q]);
+    for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nv; l += (long long)gridDim.x * blockDim.x) {
+      const V4 x = v[l];
+      const T* e = reinterpret_cast<const T*>(&x);
+#pragma unroll
+      for (int w = 0; w < W; ++w) bad |= !isfinite(e[w]);
+    }
+    for (long long l = nv * W + blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n;
+         l += (long long)gridDim.x * blockDim.x)
+      bad |= !isfinite(f[q][l]);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(flag, 1);
+}
+
 template <typename T>
 __global__ void k_to_double(long long n, double* out, const T* y, const T* comp) {
   for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < n; l += (long long)gridDim.x * blockDim.x)
@@ -500,5 +525,25 @@ template void launch_convert<float>(cudaStream_t, long long, float*, const doubl
 template void launch_convert<double>(cudaStream_t, long long, double*, const double*);
 template void launch_to_double<float>(cudaStream_t, long long, double*, const float*, const float*);
 template void launch_to_double<double>(cudaStream_t, long long, double*, const double*, const double*);
+
+cudaError_t launch_nonfinite(cudaStream_t s, long long n, int V, size_t esz, void* const* f, void* const* e,
+                             int* flag) {
+  const void* p[10] = {};
+  int nf = 0;
+  for (int v = 0; v < V; ++v) p[nf++] = f[v];
+  if (e)
+    for (int v = 0; v < V; ++v) p[nf++] = e[v];
+  const int grid = grid1d(n / 4 + 1);
+  if (esz == 4) {
+    const float* q[10];
+    for (int k = 0; k < 10; ++k) q[k] = static_cast<const float*>(p[k]);
+    k_nonfinite<float><<<grid, 256, 0, s>>>(n, nf, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], q[9], flag);
+  } else {
+    const double* q[10];
+    for (int k = 0; k < 10; ++k) q[k] = static_cast<const double*>(p[k]);
+    k_nonfinite<double><<<grid, 256, 0, s>>>(n, nf, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], q[9], flag);
+  }
+  return cudaGetLastError();
+}
 
 }  // namespace lee

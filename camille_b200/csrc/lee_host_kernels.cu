@@ -137,6 +137,7 @@ int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* co
   for (int a = 0; a < 5; ++a)
     for (int o = 0; o < 5; ++o) tp.w[a][o] = (T)c->wst[a][o];
   tp.err = c->d_err;
+  tp.wait_ns = c->wait_ns;
   FieldMaps fm;
   int rc = field_maps(c, b, zin, Box<T, kFdHalf>::BX, Box<T, kFdHalf>::BY, &fm);
   if (rc) return rc;
@@ -177,6 +178,7 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
     fp.comp[v] = comp_out ? (T*)comp_out[v] : nullptr;
   }
   fp.errflag = c->d_err;
+  fp.wait_ns = c->wait_ns;
   int bx, by, tx, ty;
   if (b.filter_px > 0) {
     filter_vec_box(c->esz, c->hf, b.filter_px, &bx, &by, &tx, &ty);
@@ -297,13 +299,22 @@ int autotune(lee_ctx* c, BlockData& b) {
 }
 
 int check_device_error(lee_ctx* c) {
-  int h = 0;
-  CK(cudaMemcpyAsync(&h, c->d_err, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  int h[2] = {0, 0};
+  CK(cudaMemcpyAsync(h, c->d_err, sizeof h, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (h) {
-    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
-    return fail(c, LEE_ERR_TIMEOUT, "a bounded wait on a TMA transfer gave up (device flag %d)", h);
+  if (h[0] || h[1]) {
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof h, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (h[0]) return fail(c, LEE_ERR_TIMEOUT, "a bounded wait on a TMA transfer gave up (device flag %d)", h[0]);
+    return fail(c, LEE_ERR_NONFINITE, "the state holds a non-finite value after step %d", c->step);
   }
+  return LEE_OK;
+}
+
+// The non-finite sentinel: every value of the state is checked (the carried rounding error of
+// the compensated form follows the state); any NaN or infinity sets d_err[1].
+int check_finite(lee_ctx* c) {
+  for (auto& b : c->blk) CK(launch_nonfinite(c->stream, b.N, c->V, c->esz, b.y, nullptr, c->d_err + 1));
   return LEE_OK;
 }
 

@@ -410,7 +410,23 @@ int advance_timed(lee_ctx* c, int nsteps, const std::vector<double>& dts) {
   CK(cudaEventCreate(&t0));
   CK(cudaEventCreate(&t1));
   CK(cudaEventRecord(t0, c->stream));
-  int rc = c->comp ? advance_impl<float>(c, nsteps, dts) : advance_impl<double>(c, nsteps, dts);
+  // chunks of lee_set_finite_check's interval, each followed by the non-finite sentinel; a
+  // chunk that finds a NaN or an infinity ends the call (at the end of each call by default)
+  const int every = c->finite_every > 0 ? c->finite_every : std::max(nsteps, 1);
+  int rc = LEE_OK;
+  for (int done = 0; done < nsteps && !rc;) {
+    const int n = std::min(every, nsteps - done);
+    rc = c->comp ? advance_impl<float>(c, n, dts) : advance_impl<double>(c, n, dts);
+    done += n;
+    if (rc || c->finite_every < 0) continue;
+    rc = check_finite(c);
+    if (!rc && done < nsteps) {
+      int bad = 0;
+      CK(cudaMemcpyAsync(&bad, c->d_err + 1, sizeof bad, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (bad) break;
+    }
+  }
   CK(cudaEventRecord(t1, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   float ms = 0.f;
@@ -557,6 +573,28 @@ int lee_set_graphs(lee_ctx* c, int on) {
     cudaGraphExecDestroy(c->graph.exec);
     c->graph.exec = nullptr;
   }
+  return LEE_OK;
+}
+
+int lee_set_wait_limit(lee_ctx* c, double seconds) {
+  if (!c) return LEE_ERR_ARG;
+  if (!(seconds <= 10.0)) return fail(c, LEE_ERR_ARG, "wait limit %g s: at most 10 s", seconds);
+  const unsigned long long ns = seconds < 0.0 ? kDefaultWaitNs : (unsigned long long)(seconds * 1e9);
+  if (ns != c->wait_ns && c->graph.exec) {
+    // captured launches hold the old limit in their parameters
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGraphExecDestroy(c->graph.exec));
+    c->graph.exec = nullptr;
+  }
+  c->wait_ns = ns;
+  return LEE_OK;
+}
+
+int lee_set_finite_check(lee_ctx* c, int every) {
+  if (!c) return LEE_ERR_ARG;
+  if (every < -1) return fail(c, LEE_ERR_ARG, "finite-check interval %d", every);
+  c->finite_every = every;
   return LEE_OK;
 }
 

@@ -134,9 +134,13 @@ __global__ void __launch_bounds__(128, 3)
     if (active && k + 1 < k1) gather_pair<DIM, TR>(s, lk + nxy, nxt);
     bool failed = false;
     const int need = DIM == 3 ? min(phi, k + H) : 0;
+    // `waited` stays at a plane whose wait gave up, so the drain below starts there
     for (; waited <= need; ++waited) {
       const int rel = waited - plo;
-      if (!mbar_wait(&bar[rel % NS], (unsigned)((rel / NS) & 1))) failed = true;
+      if (!mbar_wait(&bar[rel % NS], (unsigned)((rel / NS) & 1), P.wait_ns)) {
+        failed = true;
+        break;
+      }
     }
     if (__syncthreads_or(failed)) {
       if (tid == 0) {

@@ -95,9 +95,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
     if (!PIPE && active) gather<T, DIM, COMP, TR>(s, lk, cur);
     bool failed = false;
     const int need = DIM == 3 ? min(phi, k + H) : 0;
+    // `waited` stays at a plane whose wait gave up, so the drain below starts there
     for (; waited <= need; ++waited) {
       const int rel = waited - plo;
-      if (!mbar_wait(&bar[rel % NS], (unsigned)((rel / NS) & 1))) failed = true;
+      if (!mbar_wait(&bar[rel % NS], (unsigned)((rel / NS) & 1), P.wait_ns)) {
+        failed = true;
+        break;
+      }
     }
     if (__syncthreads_or(failed)) {
       if (tid == 0) {
@@ -228,11 +232,12 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
     const T ef = (COMP && fin) ? P.err[v][lf] : T(0);
     if (p >= plo && p <= phi) {
       const int rel = p - plo;
-      const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1));
+      const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1), P.wait_ns);
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
           atomicExch(P.errflag, 1);
-          for (int w = p + 1; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NSF], (unsigned)(((w - plo) / NSF) & 1));
+          // every copy still in flight, the one whose wait gave up included
+          for (int w = p; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NSF], (unsigned)(((w - plo) / NSF) & 1));
         }
         return;
       }
@@ -390,11 +395,12 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
     }
     if (p >= plo && p <= phi) {
       const int rel = p - plo;
-      const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1));
+      const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1), P.wait_ns);
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
           atomicExch(P.errflag, 1);
-          for (int w = p + 1; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NSF], (unsigned)(((w - plo) / NSF) & 1));
+          // every copy still in flight, the one whose wait gave up included
+          for (int w = p; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NSF], (unsigned)(((w - plo) / NSF) & 1));
         }
         return;
       }

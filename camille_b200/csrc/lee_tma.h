@@ -25,6 +25,7 @@ struct TmaStageParams {
   // offsets -2..2 from the point (the reference's stencil tables rewritten per class)
   T w[5][5];
   int* err;  // set when a bounded wait gives up
+  unsigned long long wait_ns;  // limit of the waits on staged data (the drains keep the default)
 };
 
 template <typename T>
@@ -39,6 +40,7 @@ struct TmaFilterParams {
   T* out[kMaxVars];
   T* comp[kMaxVars];
   int* errflag;
+  unsigned long long wait_ns;  // limit of the waits on staged data (the drains keep the default)
 };
 
 // Shared-memory box geometry: halo along i rounded up so every TMA row starts on 16 bytes;
@@ -80,6 +82,7 @@ struct AdjTmaParams {
   AdjStageParams<T> a;
   int tiles_x, k_chunk;
   int* err;  // set when a bounded wait gives up
+  unsigned long long wait_ns;  // limit of the waits on staged data (the drains keep the default)
 };
 void adj_tma_box(size_t esz, int* bx, int* by, int* tx, int* ty);
 template <typename T>

@@ -39,13 +39,19 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
-// Wait for the phase of the given parity; false after about one second.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+// The default limit of a bounded wait: one second of %globaltimer.
+constexpr unsigned long long kWaitNs = 1000000000ull;
+
+// Wait for the phase of the given parity; false once `limit_ns` nanoseconds have passed (a limit
+// of 0 gives up at the first try that finds the phase still open). The drains that follow a
+// failed wait always use the default limit, so a CTA never exits with a copy in flight.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity, unsigned long long limit_ns = kWaitNs) {
   if (mbar_try(b, parity)) return true;
+  if (limit_ns == 0) return false;
   const unsigned long long t0 = gtimer();
   for (unsigned it = 1;; ++it) {
     if (mbar_try(b, parity)) return true;
-    if ((it & 63u) == 0u && gtimer() - t0 > 1000000000ull) return false;
+    if ((it & 63u) == 0u && gtimer() - t0 > limit_ns) return false;
   }
 }
 

@@ -288,6 +288,19 @@ int lee_set_timing(lee_ctx *ctx, int on);
  * group of steps. Off, or while kernel timing is on, every launch is issued on its own. The
  * results are the same either way. */
 int lee_set_graphs(lee_ctx *ctx, int on);
+/* Failure detection (no reference counterpart: camille keeps going on NaN, and its waits are MPI
+ * calls, src/parallel/parallel.cpp:78-96).
+ * lee_set_finite_check: after every `every` steps of lee_advance / lee_advance_blocks a sentinel
+ * kernel checks that every state value is finite; a NaN or an infinity ends the call with
+ * LEE_ERR_NONFINITE, the state left as it is (lee_download_state still works). 0 (default):
+ * one check at the end of each call; -1: no check.
+ * lee_set_wait_limit: the kernels stage their inputs with TMA copies and wait on them for at most
+ * `seconds` (default 1 s, restored by a negative value; at most 10 s); a wait that gives up
+ * ends the call with LEE_ERR_TIMEOUT after its CTA has drained its copies in flight, and the
+ * context stays usable. 0 gives up at the first look at a copy that has not landed yet: it
+ * exercises that path in tests. */
+int lee_set_finite_check(lee_ctx *ctx, int every);
+int lee_set_wait_limit(lee_ctx *ctx, double seconds);
 /* Kernel of the fused filter (no reference counterpart; results agree to rounding): -1 or 0
  * (default) the scalar kernel, 2 or 4 the kernel that gives each thread that many neighbouring
  * points along xi (4: FP32 only). LEE_ERR_UNSUPPORTED from lee_prepare when a block cannot run the

@@ -99,6 +99,7 @@ struct orc_ctx {
   double wave_amp, wave_len, wave_hw;
   int axisym; /* UserInput::axisym (src/core/input.cpp:105-108) */
   double *scr[3]; /* work fields of the right-hand side, scrn points each */
+  int finite_every; /* steps between non-finite checks (0: end of each advance, -1: none) */
   size_t scrn;
   char err[512];
 };
@@ -1308,6 +1309,16 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
           for (int v = 0; v < 5; ++v) ynext[b][v][p] = 0.0;
       for (int v = 0; v < 5; ++v) memcpy(bk->sol[v], ynext[b][v], sizeof(double) * (size_t)bk->N);
     }
+    /* the non-finite sentinel of lee_set_finite_check (the reference has none) */
+    int last = it == nsteps - 1;
+    if (!rc && c->finite_every >= 0 && (last || (c->finite_every > 0 && (it + 1) % c->finite_every == 0)))
+      for (int b = 0; b < nb && !rc; ++b)
+        for (int v = 0; v < 5 && !rc; ++v)
+          for (int p = 0; p < c->blk[b].N; ++p)
+            if (!isfinite(c->blk[b].sol[v][p])) {
+              rc = fail(c, LEE_ERR_NONFINITE, "the state holds a non-finite value after step %d", c->step);
+              break;
+            }
   }
   for (int b = 0; b < nb; ++b)
     for (int v = 0; v < 5; ++v) { free(yn[b][v]); free(ynext[b][v]); free(zi[b][v]); free(rhs[b][v]); }
@@ -1435,6 +1446,18 @@ int orc_set_filter_kernel(orc_ctx *c, int kind) {
 
 int orc_set_graphs(orc_ctx *c, int on) {
   (void)c; (void)on;
+  return LEE_OK;
+}
+
+int orc_set_finite_check(orc_ctx *c, int every) {
+  if (every < -1) return fail(c, LEE_ERR_ARG, "finite-check interval %d", every);
+  c->finite_every = every;
+  return LEE_OK;
+}
+
+/* The oracle stages nothing and waits on nothing: the limit is accepted and has no effect. */
+int orc_set_wait_limit(orc_ctx *c, double seconds) {
+  if (!(seconds <= 10.0)) return fail(c, LEE_ERR_ARG, "wait limit %g s: at most 10 s", seconds);
   return LEE_OK;
 }
 
