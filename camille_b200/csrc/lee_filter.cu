@@ -146,15 +146,6 @@ struct Grp<double, 2> {
   __device__ __forceinline__ static Grp fma(Grp x, W w, Grp c) { return {__fma_rn(x.a, w, c.a), __fma_rn(x.b, w, c.b)}; }
 };
 
-template <int N, typename F, int... I>
-__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
-  (f(std::integral_constant<int, I>{}), ...);
-}
-// f(integral_constant<0>) ... f(integral_constant<N-1>), in order
-template <int N, typename F>
-__device__ __forceinline__ void static_for(F&& f) {
-  static_for_impl<N>(f, std::make_integer_sequence<int, N>{});
-}
 
 // The symmetric interior stencil along xi for the group whose points sit at win[C .. C+PX-1] of a
 // row window: w0 x_c + sum_o w_o (x_{c-o} + x_{c+o}). FP32 pairs neighbouring points where the

@@ -4,6 +4,9 @@
 
 #include <stdint.h>
 
+#include <type_traits>
+#include <utility>
+
 #include <cuda.h>
 
 namespace lee {
@@ -42,12 +45,13 @@ __device__ __forceinline__ unsigned long long gtimer() {
 // The default limit of a bounded wait: one second of %globaltimer.
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
-// Wait for the phase of the given parity; false once `limit_ns` nanoseconds have passed (a limit
-// of 0 gives up at the first try that finds the phase still open). The drains that follow a
-// failed wait always use the default limit, so a CTA never exits with a copy in flight.
+// Wait for the phase of the given parity; false once `limit_ns` nanoseconds have passed. A limit
+// of 0 gives up at once, without looking: it drives the failure path in tests, whether or not the
+// copy has landed. The drains that follow a failed wait always use the default limit, so a CTA
+// never exits with a copy in flight.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity, unsigned long long limit_ns = kWaitNs) {
-  if (mbar_try(b, parity)) return true;
   if (limit_ns == 0) return false;
+  if (mbar_try(b, parity)) return true;
   const unsigned long long t0 = gtimer();
   for (unsigned it = 1;; ++it) {
     if (mbar_try(b, parity)) return true;
@@ -61,6 +65,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
           smem_u32(dst)),
       "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
+}
+
+template <int N, typename F, int... I>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+// f(integral_constant<0>) ... f(integral_constant<N-1>), in order
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl<N>(f, std::make_integer_sequence<int, N>{});
 }
 
 // Closure class of a position along a line with nb closure rows at each end:

@@ -297,8 +297,8 @@ int lee_set_graphs(lee_ctx *ctx, int on);
  * lee_set_wait_limit: the kernels stage their inputs with TMA copies and wait on them for at most
  * `seconds` (default 1 s, restored by a negative value; at most 10 s); a wait that gives up
  * ends the call with LEE_ERR_TIMEOUT after its CTA has drained its copies in flight, and the
- * context stays usable. 0 gives up at the first look at a copy that has not landed yet: it
- * exercises that path in tests. */
+ * context stays usable. 0 makes every such wait give up at once, landed or not: it exercises
+ * that path in tests. */
 int lee_set_finite_check(lee_ctx *ctx, int every);
 int lee_set_wait_limit(lee_ctx *ctx, double seconds);
 /* Kernel of the fused filter (no reference counterpart; results agree to rounding): -1 or 0

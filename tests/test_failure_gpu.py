@@ -3,9 +3,9 @@
 - The non-finite sentinel (lee_set_finite_check): a NaN uploaded from the host ends lee_advance
   with LEE_ERR_NONFINITE, at the end of the call by default or after the first chunk of the
   chosen interval; the context stays usable.
-- The bounded waits of the TMA-staged kernels (lee_set_wait_limit): with a limit of 0 a wait gives
-  up at its first look at a copy that has not landed, the CTA drains its copies in flight and
-  returns, and lee_advance reports LEE_ERR_TIMEOUT; with the default limit restored the same
+- The bounded waits of the TMA-staged kernels (lee_set_wait_limit): with a limit of 0 every wait
+  gives up at once, the CTA drains its copies in flight and returns, and lee_advance reports
+  LEE_ERR_TIMEOUT; with the default limit restored the same
   context advances again and gives the bits of a fresh context.
 
 Nothing here faults, traps or hangs a GPU: the NaN is data, and every wait that gives up is
