@@ -306,7 +306,9 @@ def run_ours(args) -> None:
     solvers = {}
     clocks = None
     for form, prec in (("fp32c", api.FP32_COMPENSATED), ("fp64", api.FP64)):
-        s = api.Solver(lib, case, precision=prec, device=local)
+        kinds = {"filter_kernel": args.filter_kernel} if form == "fp32c" or args.filter_kernel in (-1, 0, 2) else {}
+        s = api.Solver(lib, case, precision=prec, device=local, stage_kernel=args.stage_kernel if form == "fp32c" else -1,
+                       **kinds)
         solvers[form] = s
         dt = s.compute_dt(case.cfl)
         s.advance(W, dt)
@@ -580,6 +582,10 @@ def main() -> int:
     ap.add_argument("--cpu-n", type=int, default=64)
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-batch", action="store_true", help="skip the batch workload's figures in the default line")
+    ap.add_argument("--filter-kernel", type=int, default=-1,
+                    help="lee_set_filter_kernel for the run (-1: the library's default; 2, 4: the vectorised filter)")
+    ap.add_argument("--stage-kernel", type=int, default=-1,
+                    help="lee_set_stage_kernel for the FP32-compensated run (-1: the library's default)")
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--ref-n", type=int, default=64)
     ap.add_argument("--ref-ranks", type=int, default=0, help="reference MPI ranks (0: the host's cores, at most 8)")

@@ -149,6 +149,12 @@ void lee_destroy(lee_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
   for (auto e : c->ev_pool) cudaEventDestroy(e);
+  if (c->adj.rev) {
+    cudaStreamSynchronize(c->adj.rev);
+    cudaStreamDestroy(c->adj.rev);
+  }
+  if (c->adj.ev_fwd) cudaEventDestroy(c->adj.ev_fwd);
+  if (c->adj.ev_rev) cudaEventDestroy(c->adj.ev_rev);
   for (void* p : c->allocs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

@@ -91,7 +91,8 @@ struct BlockData {
   void* d_sigma_field = nullptr;    // summed sponge strengths per point (working precision)
   int tiles_x = 0, tiles_y = 0;
   int stage_chunk = 0, filter_chunk = 0;
-  int filter_ry = 1;                  // rows per thread row of the scalar fused filter (1 or 2)
+  int filter_ry = 1;                  // form of the scalar fused filter: 1 or 2 tile rows per thread
+                                      // row, 3 one row with the plane loop unrolled (same bits)
 };
 
 struct MapKey {
@@ -213,6 +214,8 @@ struct lee_ctx {
     bool tma = false;                      // the plane-marching stage kernel (lee_adjoint_tma.cu)
     bool tma_jm = false;                   // ... with J*metrics fields (else constants)
     bool fused_filter = false;             // F^T by the fused filter kernel (lee_tma.cu)
+    cudaStream_t rev = nullptr;            // the reverse sweep's stream when segments are recomputed
+    cudaEvent_t ev_fwd = nullptr, ev_rev = nullptr;
   } adj;
 };
 
@@ -285,7 +288,8 @@ void swap_fields(int V, void** a, void** b);
 int ensure_encoder(lee_ctx* c);
 int encode_maps(lee_ctx* c, const BlockData& b, const void* const* fields, int n, int bx, int by, CUtensorMap* out);
 int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int by, FieldMaps* out);
-int filter_box(const lee_ctx* c, int h, int ry, int* bx, int* by);
+int filter_form_rows(int form);
+int filter_box(const lee_ctx* c, int h, int form, int* bx, int* by);
 int filter_tiles(const BlockData& b);
 void set_filter_tiles(const lee_ctx* c, BlockData& b);
 template <typename T>

@@ -449,19 +449,29 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
   const double scale = 2.0 * a.weight;
   const int P = V - 1;
   long long mismatches = 0;
-  std::vector<double> tr2;
+  // With recompute, the reverse sweep runs on a stream of its own: segment s's reverse steps
+  // wait for s's recomputed traces, and the recompute of segment s - 1 (forward buffers, its
+  // own trace rows) runs beside them. The reverse sweep reads the adjoint buffers, the
+  // coefficient fields and trace rows of its segment only, and the forward steps never touch
+  // those, so the two overlap on the GPU with no other ordering.
+  cudaStream_t main_stream = c->stream;
+  if (recompute) {
+    if (!a.rev) CK(cudaStreamCreateWithFlags(&a.rev, cudaStreamNonBlocking));
+    if (!a.ev_fwd) CK(cudaEventCreateWithFlags(&a.ev_fwd, cudaEventDisableTiming));
+    if (!a.ev_rev) CK(cudaEventCreateWithFlags(&a.ev_rev, cudaEventDisableTiming));
+    CK(cudaEventRecord(a.ev_fwd, main_stream));  // lam and gbar zeroed above
+    CK(cudaStreamWaitEvent(a.rev, a.ev_fwd, 0));
+  }
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int n0 = seg * K, n = std::min(K, nsteps - n0);
     if (recompute) {
-      // the segment's forward steps again, from its checkpoint; their traces must repeat
+      // the segment's forward steps again, from its checkpoint; their traces must repeat (checked
+      // against the first pass once every segment is done)
       if ((rc = restore(seg))) return rc;
       set_clock(c, seg_time[(size_t)seg], step_start + n0);
       if ((rc = advance_traced(c, n, dt, n0))) return rc;
-      tr2.assign((size_t)n * M, 0.0);
-      CK(cudaMemcpyAsync(tr2.data(), a.d_trace + (size_t)n0 * M, tr2.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                         c->stream));
-      CK(cudaStreamSynchronize(c->stream));
-      for (size_t q = 0; q < tr2.size(); ++q) mismatches += tr2[q] != tr[(size_t)n0 * M + q];
+      CK(cudaEventRecord(a.ev_fwd, main_stream));
+      CK(cudaStreamWaitEvent(a.rev, a.ev_fwd, 0));
     }
     // stage times of each step of the segment, advanced as the forward steps advance them
     std::vector<double> amps((size_t)n * tb.ns);
@@ -470,16 +480,33 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
       t += dt;
       for (int s = 0; s < tb.ns; ++s) amps[(size_t)k * tb.ns + s] = source_amp(c, b, t + tb.c[s] * dt);
     }
-    for (int k = n - 1; k >= 0; --k) {
+    // the reverse steps go to the reverse stream (every launch below reads c->stream)
+    if (recompute) c->stream = a.rev;
+    for (int k = n - 1; k >= 0 && !rc; --k) {
       const int step = n0 + k;  // 0-based: this transposed step maps the adjoint of y_{step+1} to y_step
-      if (c->comp)
-        CK(launch_mic_force<float>((int)M, a.d_mic, (float*)a.lam[P], a.d_trace, step, scale, c->stream));
-      else
-        CK(launch_mic_force<double>((int)M, a.d_mic, (double*)a.lam[P], a.d_trace, step, scale, c->stream));
-      rc = c->comp ? adjoint_step<float>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar)
-                   : adjoint_step<double>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar);
-      if (rc) return rc;
+      cudaError_t e = c->comp
+                          ? launch_mic_force<float>((int)M, a.d_mic, (float*)a.lam[P], a.d_trace, step, scale, c->stream)
+                          : launch_mic_force<double>((int)M, a.d_mic, (double*)a.lam[P], a.d_trace, step, scale,
+                                                     c->stream);
+      if (e != cudaSuccess) rc = fail(c, LEE_ERR_CUDA, "microphone forcing: %s", cudaGetErrorString(e));
+      if (!rc)
+        rc = c->comp ? adjoint_step<float>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar)
+                     : adjoint_step<double>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar);
     }
+    c->stream = main_stream;
+    if (rc) {
+      if (recompute) cudaStreamSynchronize(a.rev);
+      return rc;
+    }
+  }
+  if (recompute) {
+    // the reverse sweep ends before the gradient is read and the final state put back
+    CK(cudaEventRecord(a.ev_rev, a.rev));
+    CK(cudaStreamWaitEvent(main_stream, a.ev_rev, 0));
+    std::vector<double> tr2(tr.size());
+    CK(cudaMemcpyAsync(tr2.data(), a.d_trace, tr2.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t q = 0; q < tr2.size(); ++q) mismatches += tr2[q] != tr[q];
   }
   // source-box gradient -> lattice gradient
   std::vector<double> gbox(nbox);
