@@ -105,6 +105,8 @@ SIGNATURES = {
     "get_stats": (C.c_int, [C.c_void_p, C.POINTER(LeeStats)]),
     "set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "set_finite_check": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_block_streams": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_batching": (C.c_int, [C.c_void_p, C.c_int]),
     "set_wait_limit": (C.c_int, [C.c_void_p, C.c_double]),
     "set_filter_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "set_stage_kernel": (C.c_int, [C.c_void_p, C.c_int]),
@@ -157,11 +159,12 @@ class Solver:
 
     def __init__(self, lib: Library, case: "_cases.Case", precision: int = FP64, device: int = 0,
                  upload: bool = True, overset_file: Optional[str] = None, filter_kernel: int = -1,
-                 stage_kernel: int = -1, prepare: bool = True):
+                 stage_kernel: int = -1, prepare: bool = True, batching: bool = True):
         """``overset_file``: read the case's overset maps from this Overture-format file
         (lee_read_overset_file) instead of passing the arrays (lee_set_overset).
         ``filter_kernel``: lee_set_filter_kernel (-1/0 scalar, 2/4 vector width);
         ``stage_kernel``: lee_set_stage_kernel (-1 default, 1 or 2 points per thread).
+        ``batching=False``: lee_set_batching(0), every block runs its own kernels;
         ``prepare=False`` stops before lee_prepare (nothing is uploaded)."""
         self.lib = lib
         self.case = case
@@ -221,6 +224,8 @@ class Solver:
                 self._chk(lib.set_filter_kernel(self.ctx, filter_kernel))
             if stage_kernel != -1:
                 self._chk(lib.set_stage_kernel(self.ctx, stage_kernel))
+            if not batching:
+                self._chk(lib.set_batching(self.ctx, 0))
             if not prepare:
                 return
             self._chk(lib.prepare(self.ctx))

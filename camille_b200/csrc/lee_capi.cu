@@ -153,6 +153,11 @@ void lee_destroy(lee_ctx* c) {
     cudaStreamSynchronize(c->adj.rev);
     cudaStreamDestroy(c->adj.rev);
   }
+  for (auto sd : c->side) {
+    cudaStreamSynchronize(sd);
+    cudaStreamDestroy(sd);
+  }
+  for (auto e : c->side_ev) cudaEventDestroy(e);
   if (c->adj.ev_fwd) cudaEventDestroy(c->adj.ev_fwd);
   if (c->adj.ev_rev) cudaEventDestroy(c->adj.ev_rev);
   for (void* p : c->allocs) cudaFree(p);

@@ -151,6 +151,12 @@ struct lee_ctx {
   bool wfl_sym = false;  // symmetric interior filter stencil: the vectorised filter kernel applies
   int filter_kernel = -1;  // lee_set_filter_kernel: -1/0 scalar, else vector group width
   int stage_kernel = -1;   // lee_set_stage_kernel: -1 default, else points per thread
+  // blocks of a multi-block context run their stage and filter launches on side streams, forked
+  // from the context stream and joined before whatever couples the blocks (overset, the clock)
+  bool concurrent = true;       // lee_set_block_streams
+  bool batching = true;         // lee_set_batching: eligible batches run the batched kernels
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;  // [0] the fork, [1 + q] the join of side stream q
   int* d_err = nullptr;          // [0] a bounded wait gave up, [1] a non-finite state value was found
   unsigned long long wait_ns = kDefaultWaitNs;  // limit of the kernels' waits on staged data
   int finite_every = 0;          // lee_set_finite_check: steps between checks (0: end of each advance, -1: off)
@@ -301,6 +307,8 @@ template <typename T>
 int autotune(lee_ctx* c, BlockData& b);
 int check_device_error(lee_ctx* c);
 int check_finite(lee_ctx* c);
+int fork_sides(lee_ctx* c);
+int join_sides(lee_ctx* c);
 template <typename T>
 int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e, double t, const double* t_tab, const int* ctr,
               int t_stride);

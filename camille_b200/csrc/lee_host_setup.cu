@@ -449,7 +449,7 @@ int lee_prepare(lee_ctx* c) {
     if ((b.tma || b.tma_filter) && (rc = ensure_encoder(c))) return rc;
     if ((rc = c->comp ? autotune<float>(c, b) : autotune<double>(c, b))) return rc;
   }
-  if (c->blk.size() > 1 && batch_eligible(c)) {
+  if (c->blk.size() > 1 && c->batching && batch_eligible(c)) {
     rc = c->comp ? batch_setup<float>(c) : batch_setup<double>(c);
     if (rc) return rc;
   }
@@ -482,6 +482,19 @@ int lee_prepare(lee_ctx* c) {
     }
   }
   CK(cudaStreamSynchronize(s));
+  if (c->blk.size() > 1 && c->side.empty()) {
+    const size_t S = std::min<size_t>(c->blk.size(), 8);
+    for (size_t q = 0; q < S; ++q) {
+      cudaStream_t sd = nullptr;
+      CK(cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking));
+      c->side.push_back(sd);
+    }
+    for (size_t q = 0; q <= S; ++q) {
+      cudaEvent_t e = nullptr;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      c->side_ev.push_back(e);
+    }
+  }
   c->prepared = true;
   return LEE_OK;
 }

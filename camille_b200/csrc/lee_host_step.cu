@@ -21,6 +21,22 @@ __global__ void k_tick(int* ctr) { *ctr += 1; }
 
 namespace lee {
 
+// The fork of the side streams from the context stream, and their join back into it (in a
+// captured step graph these become the graph's parallel branches).
+int fork_sides(lee_ctx* c) {
+  CK(cudaEventRecord(c->side_ev[0], c->stream));
+  for (auto sd : c->side) CK(cudaStreamWaitEvent(sd, c->side_ev[0], 0));
+  return LEE_OK;
+}
+
+int join_sides(lee_ctx* c) {
+  for (size_t q = 0; q < c->side.size(); ++q) {
+    CK(cudaEventRecord(c->side_ev[1 + q], c->side[q]));
+    CK(cudaStreamWaitEvent(c->stream, c->side_ev[1 + q], 0));
+  }
+  return LEE_OK;
+}
+
 // One time step (temporal::time_advance with RungeKutta::integrate) enqueued on the context
 // stream: the time is incremented first (solver::solve, src/solver/solver.cpp:72), then every
 // stage runs on every block, the boundary update (BC lines, overset) follows each stage, and
@@ -44,10 +60,25 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
       if (rc) return rc;
       return trace_step<T>(c, ctr);
     }
+    // blocks are independent within a stage (their BC lines included) and within the filter:
+    // with several blocks each one's launches go to a side stream of their own
+    const bool conc = c->concurrent && nbk > 1 && !c->timing && !c->side.empty();
+    cudaStream_t origin = c->stream;
     for (int s = 0; s < ns; ++s) {
+      const bool last = s == ns - 1;
+      auto target = [&](BlockData& b) -> void** { return (last && !c->comp) ? b.acc : b.zb[s % 2]; };
+      auto errors = [&](BlockData& b) -> void** { return (last && c->comp) ? b.acc : nullptr; };
+      // the update's time is that of the next stage, the last stage's on the last
+      // (RungeKutta::integrate, src/solver/temporal_discretization.cpp:232-244)
+      const int sb = std::min(s + 1, ns - 1);
+      if (conc) {
+        int rc = fork_sides(c);
+        if (rc) return rc;
+      }
       for (auto& b : c->blk) {
         const size_t bix = (size_t)(&b - &c->blk[0]);
         const double dt = dts[bix];
+        if (conc) c->stream = c->side[bix % c->side.size()];
         StageParams<T> p;
         fill_stage_common<T>(c, b, p);
         p.stage = s;
@@ -62,7 +93,10 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         p.nstages = nbk * ns;
         if (c->wave_time) {
           int rc = wave_refs<T>(c, b, b.time + ci[s] * dt, t_tab ? t_tab + bix * ns + s : nullptr, ctr, nbk * ns);
-          if (rc) return rc;
+          if (rc) {
+            c->stream = origin;
+            return rc;
+          }
         }
         void** zin = s == 0 ? b.y : b.zb[(s + 1) % 2];
         void** zout = b.zb[s % 2];
@@ -76,24 +110,24 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         p.rho_prev = b.rho_valid ? (const T*)b.rho : nullptr;
         int e0 = mark(c);
         int rc = launch_stage_any<T>(c, b, p, zin);
-        if (rc) return rc;
+        if (rc) {
+          c->stream = origin;
+          return rc;
+        }
         int e1 = mark(c);
         span(c, 0, e0, e1);
         c->stats.stage_launches += 1;
         c->stats.kernel_launches += 1;
+        // boundary update of the stage output (spatial::update_boundary): z, or y_next after the
+        // last stage (FP64: the accumulator; compensated: the pair y_pre, e); BC lines touch their
+        // own block only
+        rc = apply_bcs<T>(c, b, target(b), errors(b), b.time + ci[sb] * dts[bix],
+                          t_tab ? t_tab + bix * ns + sb : nullptr, ctr, nbk * ns);
+        c->stream = origin;
+        if (rc) return rc;
       }
-      // boundary update of the stage output (spatial::update_boundary): z, or y_next after the
-      // last stage (FP64: the accumulator; compensated: the pair y_pre, e)
-      const bool last = s == ns - 1;
-      auto target = [&](BlockData& b) -> void** { return (last && !c->comp) ? b.acc : b.zb[s % 2]; };
-      auto errors = [&](BlockData& b) -> void** { return (last && c->comp) ? b.acc : nullptr; };
-      // the update's time is that of the next stage, the last stage's on the last
-      // (RungeKutta::integrate, src/solver/temporal_discretization.cpp:232-244)
-      const int sb = std::min(s + 1, ns - 1);
-      for (auto& b : c->blk) {
-        const size_t bix = (size_t)(&b - &c->blk[0]);
-        int rc = apply_bcs<T>(c, b, target(b), errors(b), b.time + ci[sb] * dts[bix],
-                              t_tab ? t_tab + bix * ns + sb : nullptr, ctr, nbk * ns);
+      if (conc) {
+        int rc = join_sides(c);
         if (rc) return rc;
       }
       // overset interpolation over all blocks, from their post-BC values (overset::interpolate)
@@ -133,19 +167,30 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         }
       }
     }
+    if (conc) {
+      int rc = fork_sides(c);
+      if (rc) return rc;
+    }
     for (auto& b : c->blk) {
       void** last_out = b.zb[(ns - 1) % 2];
       void** other = b.zb[ns % 2];
+      if (conc) c->stream = c->side[(size_t)(&b - &c->blk[0]) % c->side.size()];
       if (c->cfg.filter_scheme != LEE_FILTER_NONE && b.tma_filter) {
         // pre-filter state (FP64: acc; compensated: y_pre with its error in acc) -> y
         int rc = c->comp ? launch_filter_fused<T>(c, b, last_out, b.acc, b.y, b.comp)
                          : launch_filter_fused<T>(c, b, b.acc, nullptr, b.y, nullptr);
-        if (rc) return rc;
+        if (rc) {
+          c->stream = origin;
+          return rc;
+        }
       } else if (c->cfg.filter_scheme != LEE_FILTER_NONE) {
         void** res = nullptr;
         int rc = c->comp ? run_filter<T>(c, b, last_out, b.acc, b.comp, other, b.y, &res)
                          : run_filter<T>(c, b, b.acc, nullptr, nullptr, last_out, other, &res);
-        if (rc) return rc;
+        if (rc) {
+          c->stream = origin;
+          return rc;
+        }
         swap_fields(c->V, b.y, res);
       } else if (!c->comp) {
         swap_fields(c->V, b.y, b.acc);
@@ -153,6 +198,11 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         swap_fields(c->V, b.y, last_out);
         swap_fields(c->V, b.comp, b.acc);
       }
+      c->stream = origin;
+    }
+    if (conc) {
+      int rc = join_sides(c);
+      if (rc) return rc;
     }
   }
   return trace_step<T>(c, ctr);
@@ -588,6 +638,25 @@ int lee_set_wait_limit(lee_ctx* c, double seconds) {
     c->graph.exec = nullptr;
   }
   c->wait_ns = ns;
+  return LEE_OK;
+}
+
+int lee_set_block_streams(lee_ctx* c, int on) {
+  if (!c) return LEE_ERR_ARG;
+  if ((on != 0) != c->concurrent && c->graph.exec) {  // captured graphs hold the old branches
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGraphExecDestroy(c->graph.exec));
+    c->graph.exec = nullptr;
+  }
+  c->concurrent = on != 0;
+  return LEE_OK;
+}
+
+int lee_set_batching(lee_ctx* c, int on) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_batching before lee_prepare");
+  c->batching = on != 0;
   return LEE_OK;
 }
 

@@ -289,6 +289,16 @@ int lee_set_timing(lee_ctx *ctx, int on);
  * group of steps. Off, or while kernel timing is on, every launch is issued on its own. The
  * results are the same either way. */
 int lee_set_graphs(lee_ctx *ctx, int on);
+/* Multi-block contexts (no reference counterpart; results are the same bits either way):
+ * lee_set_block_streams: on (default), the blocks' stage launches (with their BC lines) and filter
+ * launches of one step go to side streams forked from the context stream and joined before the
+ * overset update and the next stage, so blocks run side by side (parallel branches of a step
+ * graph); off, one stream.
+ * lee_set_batching (before lee_prepare): on (default), a context of 2-D uniform-mean blocks without
+ * holes, BC lines or overset runs the batched kernels (one launch per stage for all blocks); off,
+ * every block runs its own kernels (TMA-staged where the block allows), side by side. */
+int lee_set_block_streams(lee_ctx *ctx, int on);
+int lee_set_batching(lee_ctx *ctx, int on);
 /* Failure detection (no reference counterpart: camille keeps going on NaN, and its waits are MPI
  * calls, src/parallel/parallel.cpp:78-96).
  * lee_set_finite_check: after every `every` steps of lee_advance / lee_advance_blocks a sentinel

@@ -1449,6 +1449,17 @@ int orc_set_graphs(orc_ctx *c, int on) {
   return LEE_OK;
 }
 
+/* The oracle runs its blocks one after the other: both switches are accepted and change nothing. */
+int orc_set_block_streams(orc_ctx *c, int on) {
+  (void)c; (void)on;
+  return LEE_OK;
+}
+
+int orc_set_batching(orc_ctx *c, int on) {
+  (void)c; (void)on;
+  return LEE_OK;
+}
+
 int orc_set_finite_check(orc_ctx *c, int every) {
   if (every < -1) return fail(c, LEE_ERR_ARG, "finite-check interval %d", every);
   c->finite_every = every;

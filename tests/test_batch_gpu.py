@@ -110,3 +110,36 @@ def test_every_work_item_shape_gives_the_same_bits(product_lib, precision):
             ref = out
         for a, b in zip(out, ref):
             np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+def test_block_streams_give_the_same_bits(product_lib, precision):
+    """Blocks on side streams (the default for several blocks: the two-block overset layout with
+    its slip wall, sponges and overset gathers between stages) and on one stream give the same
+    bits, replayed in step graphs or launched directly."""
+    from tests.golden.make_golden import OVERSET_WORKLOADS
+    case = OVERSET_WORKLOADS["cylinder2d_64"]()
+    a = api.Solver(product_lib, case, precision=precision)
+    b = api.Solver(product_lib, case, precision=precision)
+    assert product_lib.set_block_streams(b.ctx, 0) == api.LEE_OK
+    dt = a.compute_dt()
+    for n in (1, 7, 2):
+        a.advance(n, dt)
+        b.advance(n, dt)
+    for blk in range(2):
+        np.testing.assert_array_equal(a.download(blk)[0], b.download(blk)[0])
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+def test_batch_without_batched_kernels_matches_instances(product_lib, precision):
+    """lee_set_batching(0): the instances run their own (TMA-staged) kernels side by side, each on
+    its own clock; every instance matches the same instance run alone, bit for bit."""
+    case = cases.batch2d(count=6, nmin=48, nmax=96, nsteps=9)
+    s = api.Solver(product_lib, case, precision=precision, batching=False)
+    assert s.info().batched == 0
+    dts = s.compute_dt_blocks()
+    s.advance_blocks(case.nsteps, dts)
+    for b in range(len(case.blocks)):
+        alone = api.Solver(product_lib, cases.instance(case, b), precision=precision)
+        alone.advance(case.nsteps, float(dts[b]))
+        np.testing.assert_array_equal(s.download(b)[0], alone.download(0)[0])
