@@ -91,8 +91,7 @@ struct BlockData {
   void* d_sigma_field = nullptr;    // summed sponge strengths per point (working precision)
   int tiles_x = 0, tiles_y = 0;
   int stage_chunk = 0, filter_chunk = 0;
-  int filter_ry = 1;                  // form of the scalar fused filter: 1 or 2 tile rows per thread
-                                      // row, 3 one row with the plane loop unrolled (same bits)
+  int filter_ry = 1;                  // rows per thread row of the scalar fused filter (1 or 2)
 };
 
 struct MapKey {

@@ -103,7 +103,7 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
   return encode_maps(c, b, const_cast<const void* const*>(fields), c->V, bx, by, out->m);
 }
 
-// Tile rows per thread row of a form of the scalar fused filter (1 and 3: one; 2: two).
+// Tile rows per thread row of a form of the scalar fused filter (1 or 2).
 int filter_form_rows(int form) { return form == 2 ? 2 : 1; }
 
 // The fused filter's box (tile of kTileX x kTileY * rows points with a halo of h) and its tiles.
@@ -232,9 +232,9 @@ int autotune(lee_ctx* c, BlockData& b) {
     if (which == 0 && !d3 && nskinds == 1) continue;  // nothing to choose
     float best = 1e30f;
     int best_chunk = b.nz, best_kind = which == 0 ? b.stage_px : b.filter_px, best_ry = b.filter_ry;
-    // the scalar filter's forms (one or two tile rows per thread row, one row with the plane
-    // loop unrolled) are timed with the chunk: each point's arithmetic is the same in all three
-    const int nry = which == 1 ? 3 : 1;
+    // the scalar filter's forms (one or two tile rows per thread row) are timed with the chunk:
+    // each point's arithmetic is the same in both
+    const int nry = which == 1 ? 2 : 1;
     for (int kq = 0; kq < (which == 1 ? nkinds : nskinds) * nry; ++kq) {
       if (which == 0) {
         b.stage_px = skinds[kq];

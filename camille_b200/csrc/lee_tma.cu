@@ -316,175 +316,6 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
   }
 }
 
-// The one-row filter with the same arithmetic as k_filter_tma_row (the same operations in the same
-// order, so the same bits), scheduled differently: the F_xi results of a plane go to one of two
-// shared buffers, so a single CTA barrier per plane suffices (it also frees the plane's ring slot
-// for the next copy), point offsets are 32-bit, and the plane loop is unrolled by the 2h+1 planes
-// of the F_zeta queue, which therefore rotates by renaming instead of by register moves. Held to
-// four CTAs per SM like the plain form; lee_prepare times both and keeps the faster.
-template <typename T, int DIM, bool COMP, int HF>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_filter_tma_unrolled(
-    const __grid_constant__ FieldMaps ym, const __grid_constant__ TmaFilterParams<T> P) {
-  constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = kFilterSlots;
-  constexpr int HX = Box<T, HF>::HX, BX = Box<T, HF>::BX, BY = Box<T, HF>::BY;
-  constexpr int FB = Box<T, HF>::FB;    // elements one box load writes
-  constexpr int FBP = Box<T, HF>::FBP;  // stride between boxes in shared memory
-  extern __shared__ __align__(128) unsigned char smem[];
-  T* ring = reinterpret_cast<T*>(smem);
-  T* u1s = ring + NSF * FBP;  // [2][BY][TX]: F_xi of the tile and its eta halo, two planes
-  uint64_t* bar = reinterpret_cast<uint64_t*>(u1s + 2 * BY * TX);
-
-  const int v = blockIdx.z;
-  const int i0 = (int)(blockIdx.x % P.tiles_x) * TX, j0 = (int)(blockIdx.x / P.tiles_x) * TY;
-  const int k0 = DIM == 3 ? (int)blockIdx.y * P.k_chunk : 0;
-  const int k1 = DIM == 3 ? min(P.nz, k0 + P.k_chunk) : 1;
-  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool active = i < P.nx && j < P.ny;
-  const int plo = DIM == 3 ? max(0, k0 - HF) : 0;
-  const int phi = DIM == 3 ? min(P.nz - 1, k1 - 1 + HF) : 0;
-
-  if (tid == 0) {
-    for (int q = 0; q < NSF; ++q) mbar_init(&bar[q], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  int next_issue = plo;  // meaningful in thread 0 only
-  auto issue_upto = [&](int last) {
-    for (; next_issue <= min(phi, last); ++next_issue) {
-      const int slot = (next_issue - plo) % NSF;
-      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * FB));
-      tma_load_3d(ring + slot * FBP, &ym.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
-    }
-  };
-  if (tid == 0) issue_upto(plo + NSF - 1);
-
-  // closure-class weights along xi and eta are fixed for a thread: keep them in registers
-  T wx[NQ], wy[NQ];
-  {
-    const int cx = cls_of(min(i, P.nx - 1), P.nx, P.nb);
-    const int cy = cls_of(min(j, P.ny - 1), P.ny, P.nb);
-#pragma unroll
-    for (int o = 0; o < NQ; ++o) {
-      wx[o] = P.w[cx][o];
-      wy[o] = P.w[cy][o];
-    }
-  }
-  // uq: F_xi F_eta of the last NQ planes, plane p in entry (p - pstart) % NQ; dq, xq: the
-  // increments and pre-filter values of the last HF + 1 planes, oldest first
-  T uq[NQ], dq[HF + 1], xq[HF + 1];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) uq[q] = T(0);
-#pragma unroll
-  for (int q = 0; q <= HF; ++q) dq[q] = xq[q] = T(0);
-  const int pstart = DIM == 3 ? k0 - HF : 0, pend = DIM == 3 ? k1 - 1 + HF : 0;
-  bool stop = false;
-
-  // one plane p; R = (p - pstart) % NQ is a compile-time constant in the unrolled loop below
-  auto plane = [&](int p, auto Rc) {
-    constexpr int R = decltype(Rc)::value;
-    T u2 = T(0), d12 = T(0), xc = T(0);
-    const int kf = DIM == 3 ? p - HF : 0;  // the plane finalized at the end of this iteration
-    const bool fin = active && kf >= k0 && kf < k1;
-    // point offsets fit 32 bits (the host checks the block size)
-    const unsigned lf = (unsigned)i + (unsigned)P.nx * ((unsigned)j + (unsigned)P.ny * (unsigned)kf);
-    const T ef = (COMP && fin) ? P.err[v][lf] : T(0);
-    if (p >= plo && p <= phi) {
-      const int rel = p - plo;
-      const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1), P.wait_ns);
-      const T* box = ring + (rel % NSF) * FBP;
-      T* u1 = u1s + (p & 1) * (BY * TX);
-      T d1 = T(0), u1c = T(0);
-      if (ok) {
-        // F_xi on the thread's own row (kept in registers) and on its share of the eta halo rows
-        const T* fc = box + (ty + HF) * BX + tx + HX;
-        xc = fc[0];
-#pragma unroll
-        for (int o = -HF; o <= HF; ++o) d1 += wx[o + HF] * fc[o];
-        u1c = COMP ? xc + d1 : d1;
-        u1[(ty + HF) * TX + tx] = u1c;
-        for (int r = ty; r < 2 * HF; r += TY) {
-          const int row = r < HF ? r : r + TY;
-          const T* f = box + row * BX + tx + HX;
-          T d = T(0);
-#pragma unroll
-          for (int o = -HF; o <= HF; ++o) d += wx[o + HF] * f[o];
-          u1[row * TX + tx] = COMP ? f[0] + d : d;
-        }
-      }
-      // one barrier: F_xi of the plane is complete, and its ring slot is free again
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) {
-          atomicExch(P.errflag, 1);
-          // every copy still in flight, the one whose wait gave up included
-          for (int w = p; w < next_issue; ++w) mbar_wait(&bar[(w - plo) % NSF], (unsigned)(((w - plo) / NSF) & 1));
-        }
-        stop = true;
-        return;
-      }
-      if (tid == 0) issue_upto(p + NSF);
-      T dy = T(0);
-#pragma unroll
-      for (int o = -HF; o <= HF; ++o) dy += wy[o + HF] * (o == 0 ? u1c : u1[(ty + HF + o) * TX + tx]);
-      if (COMP) {
-        u2 = u1c + dy;
-        d12 = d1 + dy;
-      } else {
-        u2 = dy;
-      }
-    }
-    uq[R] = u2;
-#pragma unroll
-    for (int q = 0; q < HF; ++q) {
-      dq[q] = dq[q + 1];
-      xq[q] = xq[q + 1];
-    }
-    dq[HF] = d12;
-    xq[HF] = xc;
-    if (!fin) return;
-    T fz, x0, dsum;
-    if (DIM == 3) {
-      // the queue holds planes kf - HF .. kf + HF in entries R + 1 .. R + NQ (mod NQ)
-      const int cz = cls_of(kf, P.nz, P.nb);
-      fz = T(0);
-      if (cz == 0) {
-#pragma unroll
-        for (int o = 0; o < NQ; ++o) fz += P.w[0][o] * uq[(R + 1 + o) % NQ];
-      } else {
-#pragma unroll
-        for (int o = 0; o < NQ; ++o) fz += P.w[cz][o] * uq[(R + 1 + o) % NQ];
-      }
-      x0 = xq[0];
-      dsum = dq[0];
-    } else {
-      fz = u2;
-      x0 = xc;
-      dsum = d12;
-    }
-    if (!COMP) {
-      P.out[v][lf] = (T(1) - P.blend) * x0 + P.blend * fz;
-    } else {
-      const T D = DIM == 3 ? dsum + fz : dsum;
-      const T t = P.blend * D + ef;
-      const T sm = x0 + t;
-      const T bb = sm - x0;
-      P.out[v][lf] = sm;
-      P.comp[v][lf] = (x0 - (sm - bb)) + (t - bb);
-    }
-  };
-
-  if (DIM == 2) {
-    plane(0, std::integral_constant<int, 0>{});
-  } else {
-    for (int p0 = pstart; p0 <= pend && !stop; p0 += NQ) {
-      static_for<NQ>([&](auto Rc) {
-        constexpr int R = decltype(Rc)::value;
-        if (!stop && p0 + R <= pend) plane(p0 + R, Rc);
-      });
-    }
-  }
-}
-
 template <typename T, int DIM, bool COMP, int HF, int RY>
 __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ FieldMaps ym,
                                                     const __grid_constant__ TmaFilterParams<T> P) {
@@ -718,11 +549,7 @@ cudaError_t go_stage_tr(const FieldMaps& z, const TmaStageParams<T>& p, int tr, 
 
 template <typename T, int DIM, bool COMP, int HF>
 cudaError_t go_filter(const FieldMaps& in, const TmaFilterParams<T>& p, int ry, int tiles, int chunks, cudaStream_t s) {
-  if (ry == 3) {
-    const size_t sm = sizeof(T) * (kFilterSlots * Box<T, HF, 1>::FBP + 2 * Box<T, HF, 1>::BY * kTileX) +
-                      kFilterSlots * sizeof(uint64_t);
-    k_filter_tma_unrolled<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, sm, s>>>(in, p);
-  } else if (ry == 2) {
+  if (ry == 2) {
     k_filter_tma<T, DIM, COMP, HF, 2><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 2>(), s>>>(in, p);
   } else {
     k_filter_tma_row<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 1>(), s>>>(in, p);
@@ -749,7 +576,7 @@ cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, i
 template <typename T>
 cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int ry,
                               int tiles, int chunks, cudaStream_t s) {
-  if (ry < 1 || ry > 3) return cudaErrorInvalidValue;
+  if (ry != 1 && ry != 2) return cudaErrorInvalidValue;
 #define LEE_FILTER_CASE(HF)                                                                      \
   if (hf == HF) {                                                                                \
     if (dim == 2)                                                                                \

@@ -68,8 +68,7 @@ size_t stage_tma_smem(int dim, size_t esz);
 template <typename T>
 cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, int traits, int tiles, int chunks,
                              cudaStream_t s);
-// ry: the form, 1 or 2 tile rows per thread row, or 3 one row with the plane loop unrolled (the
-// same arithmetic for every point in each form)
+// ry: tile rows per thread row, 1 or 2 (the same arithmetic for every point either way)
 template <typename T>
 cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int ry,
                               int tiles, int chunks, cudaStream_t s);

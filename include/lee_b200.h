@@ -268,8 +268,7 @@ typedef struct {
   int batch_filter_tile[2];  /* picked by timing the candidates at lee_prepare */
   int filter_kernel;         /* fused filter of block 0: 0 scalar, else the vector group width */
   int stage_kernel;          /* TMA stage kernel of block 0: points per thread */
-  int filter_rows;           /* scalar fused filter of block 0: 1 or 2 tile rows per thread row, 3 one
-                                row with the plane loop unrolled (the same bits in every form) */
+  int filter_rows;           /* scalar fused filter of block 0: tile rows per thread row (1 or 2) */
 } lee_info;
 int lee_get_info(lee_ctx *ctx, lee_info *info);
 
