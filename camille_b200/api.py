@@ -106,6 +106,7 @@ SIGNATURES = {
     "set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "set_finite_check": (C.c_int, [C.c_void_p, C.c_int]),
     "set_block_streams": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_increment_step": (C.c_int, [C.c_void_p, C.c_int]),
     "set_batching": (C.c_int, [C.c_void_p, C.c_int]),
     "set_wait_limit": (C.c_int, [C.c_void_p, C.c_double]),
     "set_filter_kernel": (C.c_int, [C.c_void_p, C.c_int]),

@@ -154,6 +154,7 @@ struct lee_ctx {
   // from the context stream and joined before whatever couples the blocks (overset, the clock)
   bool concurrent = true;       // lee_set_block_streams
   bool batching = true;         // lee_set_batching: eligible batches run the batched kernels
+  bool increment_step = true;   // lee_set_increment_step
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> side_ev;  // [0] the fork, [1 + q] the join of side stream q
   int* d_err = nullptr;          // [0] a bounded wait gave up, [1] a non-finite state value was found
@@ -301,7 +302,10 @@ template <typename T>
 int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* const* zin, int chunk_override = 0);
 template <typename T>
 int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* err, void* const* out,
-                        void* const* comp_out, int chunk_override = 0);
+                        void* const* comp_out, int chunk_override = 0, void* const* inc = nullptr);
+// the compensated form's last stage may write the step's increment alone and leave y_pre to the
+// fused filter (lee_set_increment_step): on blocks where nothing acts between the two
+bool increment_step_applies(const lee_ctx* c, const BlockData& b);
 template <typename T>
 int autotune(lee_ctx* c, BlockData& b);
 int check_device_error(lee_ctx* c);

@@ -464,9 +464,10 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
   }
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int n0 = seg * K, n = std::min(K, nsteps - n0);
-    if (recompute) {
+    if (recompute && seg < nseg - 1) {
       // the segment's forward steps again, from its checkpoint; their traces must repeat (checked
-      // against the first pass once every segment is done)
+      // against the first pass once every segment is done). The last segment is where the
+      // forward pass ended: its traces were just recorded, so the reverse sweep starts on them.
       if ((rc = restore(seg))) return rc;
       set_clock(c, seg_time[(size_t)seg], step_start + n0);
       if ((rc = advance_traced(c, n, dt, n0))) return rc;

@@ -103,6 +103,16 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
   return encode_maps(c, b, const_cast<const void* const*>(fields), c->V, bx, by, out->m);
 }
 
+bool increment_step_applies(const lee_ctx* c, const BlockData& b) {
+  if (!c->comp || !c->increment_step || c->batch.active || c->ovs.n > 0) return false;
+  if (c->cfg.filter_scheme == LEE_FILTER_NONE || !b.tma || !b.tma_filter || b.filter_px > 0 || b.filter_ry != 1)
+    return false;
+  if (b.need_rho) return false;  // rho'/rho_bar is formed from y_pre after the last stage
+  for (const auto& z : b.bnd)
+    if (is_bc_line(z.kind)) return false;  // BC lines update y_pre after the last stage
+  return true;
+}
+
 // Tile rows per thread row of a form of the scalar fused filter (1 or 2).
 int filter_form_rows(int form) { return form == 2 ? 2 : 1; }
 
@@ -152,7 +162,7 @@ int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* co
   // such tableau here) reads p.stage and p.last at run time
   const int kind = p.stage < 0 ? kKindRhs
                    : p.stage == 0 ? (p.last ? kKindRuntime : kKindFirst)
-                                  : (p.last ? kKindLast : kKindMid);
+                                  : (p.last ? (p.increment ? kKindLastIncrement : kKindLast) : kKindMid);
   const int tr = b.traits | (kind << kKindShift);
   if constexpr (sizeof(T) == 4) {
     if (b.stage_px == 2 && stage_pair_applies(tr, b.nx)) {
@@ -167,7 +177,7 @@ int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* co
 // Fused filter (all directions, one read and one write of the state): in -> out.
 template <typename T>
 int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* err, void* const* out,
-                        void* const* comp_out, int chunk_override) {
+                        void* const* comp_out, int chunk_override, void* const* inc) {
   TmaFilterParams<T> fp;
   memset(&fp, 0, sizeof fp);
   fp.nx = b.nx; fp.ny = b.ny; fp.nz = b.nz;
@@ -196,12 +206,21 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
   int rc = field_maps(c, b, in, bx, by, &fm);
   if (rc) return rc;
   const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
+  FieldMaps im;
+  if (inc && (rc = field_maps(c, b, inc, bx, by, &im))) return rc;
   int e0 = mark(c);
-  if (b.filter_px > 0)
+  if (inc) {
+    if constexpr (sizeof(T) == 4) {
+      CK(launch_filter_tma_inc(fm, im, fp, c->hf, c->cfg.num_dim, filter_tiles(b), chunks, c->stream));
+    } else {
+      return fail(c, LEE_ERR_UNSUPPORTED, "the increment step is the compensated form's");
+    }
+  } else if (b.filter_px > 0) {
     CK(launch_filter_vec<T>(fm, fp, c->hf, b.filter_px, c->cfg.num_dim, b.vtiles_x * b.vtiles_y, chunks, c->stream));
-  else
+  } else {
     CK(launch_filter_tma<T>(fm, fp, c->hf, c->cfg.num_dim, c->comp ? 1 : 0, b.filter_ry, filter_tiles(b), chunks,
                             c->stream));
+  }
   int e1 = mark(c);
   span(c, 1, e0, e1);
   c->stats.filter_launches += 1;
@@ -413,9 +432,9 @@ template int run_filter<double>(lee_ctx* c, BlockData& b, void** in, void** err,
 template int launch_stage_any<float>(lee_ctx* c, BlockData& b, const StageParams<float>& p, void* const* zin, int chunk_override);
 template int launch_stage_any<double>(lee_ctx* c, BlockData& b, const StageParams<double>& p, void* const* zin, int chunk_override);
 template int launch_filter_fused<float>(lee_ctx* c, BlockData& b, void* const* in, void* const* err, void* const* out,
-                        void* const* comp_out, int chunk_override);
+                        void* const* comp_out, int chunk_override, void* const* inc);
 template int launch_filter_fused<double>(lee_ctx* c, BlockData& b, void* const* in, void* const* err, void* const* out,
-                        void* const* comp_out, int chunk_override);
+                        void* const* comp_out, int chunk_override, void* const* inc);
 template int autotune<float>(lee_ctx* c, BlockData& b);
 template int autotune<double>(lee_ctx* c, BlockData& b);
 template int apply_bcs<float>(lee_ctx* c, BlockData& b, void** f, void** e, double t, const double* t_tab, const int* ctr,

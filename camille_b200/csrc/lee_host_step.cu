@@ -83,6 +83,7 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         fill_stage_common<T>(c, b, p);
         p.stage = s;
         p.last = s == ns - 1;
+        p.increment = p.last && increment_step_applies(c, b) ? 1 : 0;
         p.h = (T)dt;
         p.b = (T)bi[s];
         p.a = (T)aij[s];
@@ -175,7 +176,16 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
       void** last_out = b.zb[(ns - 1) % 2];
       void** other = b.zb[ns % 2];
       if (conc) c->stream = c->side[(size_t)(&b - &c->blk[0]) % c->side.size()];
-      if (c->cfg.filter_scheme != LEE_FILTER_NONE && b.tma_filter) {
+      if (increment_step_applies(c, b)) {
+        // the last stage left the increment in acc: y_n and the increment in, the filtered state
+        // and its rounding error out (into the free stage buffer, which becomes y)
+        int rc = launch_filter_fused<T>(c, b, b.y, nullptr, last_out, b.comp, 0, b.acc);
+        if (rc) {
+          c->stream = origin;
+          return rc;
+        }
+        swap_fields(c->V, b.y, last_out);
+      } else if (c->cfg.filter_scheme != LEE_FILTER_NONE && b.tma_filter) {
         // pre-filter state (FP64: acc; compensated: y_pre with its error in acc) -> y
         int rc = c->comp ? launch_filter_fused<T>(c, b, last_out, b.acc, b.y, b.comp)
                          : launch_filter_fused<T>(c, b, b.acc, nullptr, b.y, nullptr);
@@ -638,6 +648,18 @@ int lee_set_wait_limit(lee_ctx* c, double seconds) {
     c->graph.exec = nullptr;
   }
   c->wait_ns = ns;
+  return LEE_OK;
+}
+
+int lee_set_increment_step(lee_ctx* c, int on) {
+  if (!c) return LEE_ERR_ARG;
+  if ((on != 0) != c->increment_step && c->graph.exec) {  // captured steps hold the old launches
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGraphExecDestroy(c->graph.exec));
+    c->graph.exec = nullptr;
+  }
+  c->increment_step = on != 0;
   return LEE_OK;
 }
 

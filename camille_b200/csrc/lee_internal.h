@@ -23,6 +23,10 @@ constexpr int kTrTma = 8;       // no holes; with kTrJmField every J*metrics ent
                                 // 32-bit point offsets
 constexpr int kKindShift = 4;   // bits 4..6: the stage's kind; 0 reads p.stage and p.last at run time
 constexpr int kKindRuntime = 0, kKindRhs = 1, kKindFirst = 2, kKindMid = 3, kKindLast = 4;
+// the last stage of the compensated form writing the step's increment alone (no y_n read, no
+// y_pre / error written): the fused filter forms y_pre = y_n + increment as the exact two-float
+// sum itself (TMA kernels only)
+constexpr int kKindLastIncrement = 5;
 
 // One directional operator: interior stencil c[l+h] (l = -h..h), closure rows
 // B[row][s] (row < nb, s < S) and the right-boundary sign (-1 difference, +1 filter).
@@ -112,6 +116,7 @@ struct StageParams {
   Coef<T> ubar[3], pbar, rhobar_inv;
   Coef<T> gs[3], gu[9], gp[3];  // mean gradients: d s_bar/dx_j, d u_bar_i/dx_j at i*3+j, d p_bar/dx_j
   int need_rho;                 // 1 when some d u_bar_i/dx_j is nonzero
+  int increment;                // last stage of the compensated form: write the increment alone
   const T* rho_prev;            // rho'/rho_bar of the previous step's pre-filter state, read by the
                                 // first stage and by a right-hand-side evaluation (null: from q)
   T gamma, inv_gamma;

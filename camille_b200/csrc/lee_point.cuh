@@ -29,8 +29,10 @@ struct Kind {
   }
   template <typename T>
   __device__ __forceinline__ static bool last(const StageParams<T>& p) {
-    return K == kKindRuntime ? p.last != 0 : K == kKindLast;
+    return K == kKindRuntime ? p.last != 0 : (K == kKindLast || K == kKindLastIncrement);
   }
+  // the last stage writes the increment alone (compile-time kinds only)
+  static constexpr bool increment = K == kKindLastIncrement;
 };
 
 // Per-point inputs read from global memory, gathered before the arithmetic so that
@@ -56,7 +58,7 @@ __device__ __forceinline__ void gather(const StageParams<T>& p, I l, PointIn<T, 
       in.jm[d][x] = (TR & kTrJmField) ? ((TR & kTrTma) ? __ldg(c.p + l) : cval(c, l)) : c.c;
     }
   const bool mid = !K::rhs(p) && !K::first(p);
-  const bool need_yn = mid && (COMP || !K::last(p));
+  const bool need_yn = mid && (COMP || !K::last(p)) && !K::increment;
   const bool need_av = mid || (COMP && K::first(p));
 #pragma unroll
   for (int v = 0; v < V; ++v) {
@@ -253,6 +255,8 @@ __device__ __forceinline__ void rk_update(const StageParams<T>& p, I l, const T 
       if (!last) {
         p.acc[v][l] = inc;
         p.zout[v][l] = yv + p.a * hk;
+      } else if (K::increment) {
+        p.acc[v][l] = inc;  // the filter forms y_pre and its rounding error
       } else {
         const T s = yv + inc;
         const T bb = s - yv;

@@ -53,7 +53,7 @@ __device__ __forceinline__ void gather_pair(const StageParams<float>& p, unsigne
   const bool need_av = mid || K::first(p);
 #pragma unroll
   for (int v = 0; v < V; ++v) {
-    in.yn[v] = mid ? ld2(p.yn[v] + l) : f2(0.f);
+    in.yn[v] = (mid && !K::increment) ? ld2(p.yn[v] + l) : f2(0.f);
     in.av[v] = need_av ? (K::first(p) ? ld2(p.comp[v] + l) : ld2(p.acc[v] + l)) : f2(0.f);
   }
   in.sg = (TR & kTrSponge) ? ldg2(p.sigma + l) : f2(0.f);
@@ -270,6 +270,8 @@ __global__ void __launch_bounds__(128, 3)
           if (!last) {
             st2(s.acc[v] + lk, inc);
             st2(s.zout[v] + lk, fma2(aa, hk, yv));
+          } else if (K::increment) {
+            st2(s.acc[v] + lk, inc);  // the filter forms y_pre and its rounding error
           } else {
             const F2 sm = add(yv, inc);
             const F2 bv = sub(sm, yv);
@@ -326,6 +328,7 @@ cudaError_t go_pair_kind(const FieldMaps& z, const TmaStageParams<float>& p, int
     case kKindFirst: return go_pair_layout<DIM, kKindFirst>(z, p, tr, tiles, chunks, s);
     case kKindMid: return go_pair_layout<DIM, kKindMid>(z, p, tr, tiles, chunks, s);
     case kKindLast: return go_pair_layout<DIM, kKindLast>(z, p, tr, tiles, chunks, s);
+    case kKindLastIncrement: return go_pair_layout<DIM, kKindLastIncrement>(z, p, tr, tiles, chunks, s);
     default: return cudaErrorInvalidValue;
   }
 }

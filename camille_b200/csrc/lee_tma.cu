@@ -170,16 +170,26 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 
 // One tile row per thread row (the form of k_filter_tma with RY = 1, scheduled by the compiler
 // without the per-row arrays).
-template <typename T, int DIM, bool COMP, int HF>
+// INC (compensated form): the step's last stage wrote its increment alone, and the filter's input
+// is the pair y_n (ym) and increment (dm): each incoming plane's two boxes land in one ring slot,
+// each thread forms its point's y_pre = y_n + increment and rounding error as the exact two-float
+// sum the last stage would have formed, the other box points become fl(y_n + increment) (the same
+// y_pre), and the rest is the filter of y_pre with its error: the same bits as the pair written by
+// the last stage, with one read of y_n in place of the last stage's read of y_n and writes of
+// y_pre and its error.
+template <typename T, int DIM, bool COMP, int HF, bool INC = false>
 __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ FieldMaps ym,
+                                                    const __grid_constant__ FieldMaps dm,
                                                     const __grid_constant__ TmaFilterParams<T> P) {
+  static_assert(!INC || COMP, "the increment input is the compensated form's");
+  constexpr int NB = INC ? 2 : 1;  // boxes per ring slot
   constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = kFilterSlots;
   constexpr int HX = Box<T, HF>::HX, BX = Box<T, HF>::BX, BY = Box<T, HF>::BY;
   constexpr int FB = Box<T, HF>::FB;    // elements one box load writes
   constexpr int FBP = Box<T, HF>::FBP;  // stride between boxes in shared memory
   extern __shared__ __align__(128) unsigned char smem[];
   T* ring = reinterpret_cast<T*>(smem);
-  T* u1 = ring + NSF * FBP;  // [BY][TX]
+  T* u1 = ring + NSF * NB * FBP;  // [BY][TX]
   uint64_t* bar = reinterpret_cast<uint64_t*>(u1 + BY * TX);
 
   const int v = blockIdx.z;
@@ -201,8 +211,9 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
   auto issue_upto = [&](int last) {
     for (; next_issue <= min(phi, last); ++next_issue) {
       const int slot = (next_issue - plo) % NSF;
-      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * FB));
-      tma_load_3d(ring + slot * FBP, &ym.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
+      mbar_expect_tx(&bar[slot], (unsigned)(sizeof(T) * FB * NB));
+      tma_load_3d(ring + slot * NB * FBP, &ym.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
+      if (INC) tma_load_3d(ring + (slot * NB + 1) * FBP, &dm.m[v], i0 - HX, j0 - HF, next_issue, &bar[slot]);
     }
   };
   if (tid == 0) issue_upto(plo + NSF - 1);
@@ -218,18 +229,21 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
       wy[o] = P.w[cy][o];
     }
   }
-  T uq[NQ], dq[HF + 1], xq[HF + 1];
+  T uq[NQ], dq[HF + 1], xq[HF + 1], eq[INC ? HF + 1 : 1];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) uq[q] = T(0);
 #pragma unroll
   for (int q = 0; q <= HF; ++q) dq[q] = xq[q] = T(0);
+#pragma unroll
+  for (int q = 0; q < (INC ? HF + 1 : 1); ++q) eq[q] = T(0);
   const int pstart = DIM == 3 ? k0 - HF : 0, pend = DIM == 3 ? k1 - 1 + HF : 0;
   for (int p = pstart; p <= pend; ++p) {
     T u2 = T(0), d12 = T(0), xc = T(0);
     const int kf = DIM == 3 ? p - HF : 0;  // the plane finalized at the end of this iteration
     const bool fin = active && kf >= k0 && kf < k1;
     const long long lf = i + (long long)P.nx * (j + (long long)P.ny * kf);
-    const T ef = (COMP && fin) ? P.err[v][lf] : T(0);
+    const T ef = (COMP && !INC && fin) ? P.err[v][lf] : T(0);
+    T ein = T(0);  // INC: the rounding error of y_pre at this thread's point of plane p
     if (p >= plo && p <= phi) {
       const int rel = p - plo;
       const bool ok = mbar_wait(&bar[rel % NSF], (unsigned)((rel / NSF) & 1), P.wait_ns);
@@ -241,7 +255,24 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
         }
         return;
       }
-      const T* box = ring + (rel % NSF) * FBP;
+      T* box = ring + (rel % NSF) * NB * FBP;
+      if (INC) {
+        // y_pre = y_n + increment and its rounding error at the thread's own point; fl(y_n +
+        // increment) at the box's other points (the halo), then one barrier
+        const T* dbox = box + FBP;
+        const int c0 = (ty + HF) * BX + tx + HX;
+        const T yv = box[c0], dv = dbox[c0];
+        const T sm = yv + dv;
+        const T bb = sm - yv;
+        ein = (yv - (sm - bb)) + (dv - bb);
+        box[c0] = sm;
+        for (int q = tid; q < FB; q += TX * TY) {
+          const int r = q / BX, cc = q - r * BX;
+          if (r >= HF && r < HF + TY && cc >= HX && cc < HX + TX) continue;  // a tile point: its owner's
+          box[q] = box[q] + dbox[q];
+        }
+        __syncthreads();
+      }
       // F_xi on the thread's own row (kept in registers) and on its share of the eta halo rows
       const T* fc = box + (ty + HF) * BX + tx + HX;
       xc = fc[0];
@@ -281,6 +312,11 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
     }
     dq[HF] = d12;
     xq[HF] = xc;
+    if (INC) {
+#pragma unroll
+      for (int q = 0; q < HF; ++q) eq[q] = eq[q + 1];
+      eq[HF] = ein;
+    }
     const int k = kf;
     if (!fin) continue;
     T fz, x0, dsum;
@@ -302,12 +338,13 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
       x0 = xc;
       dsum = d12;
     }
+    const T e0 = INC ? (DIM == 3 ? eq[0] : ein) : ef;
     const long long l = lf;
     if (!COMP) {
       P.out[v][l] = (T(1) - P.blend) * x0 + P.blend * fz;
     } else {
       const T D = DIM == 3 ? dsum + fz : dsum;
-      const T t = P.blend * D + ef;
+      const T t = P.blend * D + e0;
       const T sm = x0 + t;
       const T bb = sm - x0;
       P.out[v][l] = sm;
@@ -498,9 +535,9 @@ size_t stage_smem() {
   return sizeof(T) * NS * (DIM + 2) * Box<T, kFdHalf>::FBP + NS * sizeof(uint64_t);
 }
 
-template <typename T, int HF, int RY>
+template <typename T, int HF, int RY, int NB = 1>
 size_t filter_smem() {
-  return sizeof(T) * (kFilterSlots * Box<T, HF, RY>::FBP + Box<T, HF, RY>::BY * kTileX) +
+  return sizeof(T) * (kFilterSlots * NB * Box<T, HF, RY>::FBP + Box<T, HF, RY>::BY * kTileX) +
          kFilterSlots * sizeof(uint64_t);
 }
 
@@ -543,6 +580,9 @@ cudaError_t go_stage_tr(const FieldMaps& z, const TmaStageParams<T>& p, int tr, 
     case kKindFirst: return go_stage_layout<T, DIM, COMP, kKindFirst>(z, p, tr, tiles, chunks, s);
     case kKindMid: return go_stage_layout<T, DIM, COMP, kKindMid>(z, p, tr, tiles, chunks, s);
     case kKindLast: return go_stage_layout<T, DIM, COMP, kKindLast>(z, p, tr, tiles, chunks, s);
+    case kKindLastIncrement:
+      if constexpr (COMP) return go_stage_layout<T, DIM, COMP, kKindLastIncrement>(z, p, tr, tiles, chunks, s);
+      return cudaErrorInvalidValue;
     default: return go_stage_layout<T, DIM, COMP, kKindRuntime>(z, p, tr, tiles, chunks, s);
   }
 }
@@ -552,7 +592,7 @@ cudaError_t go_filter(const FieldMaps& in, const TmaFilterParams<T>& p, int ry, 
   if (ry == 2) {
     k_filter_tma<T, DIM, COMP, HF, 2><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 2>(), s>>>(in, p);
   } else {
-    k_filter_tma_row<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 1>(), s>>>(in, p);
+    k_filter_tma_row<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 1>(), s>>>(in, in, p);
   }
   return cudaGetLastError();
 }
@@ -589,6 +629,26 @@ cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, 
   LEE_FILTER_CASE(4)
   LEE_FILTER_CASE(5)
 #undef LEE_FILTER_CASE
+  return cudaErrorInvalidValue;
+}
+
+// The compensated one-row filter whose input is y_n and the last stage's increment.
+cudaError_t launch_filter_tma_inc(const FieldMaps& y, const FieldMaps& inc, const TmaFilterParams<float>& p, int hf,
+                                  int dim, int tiles, int chunks, cudaStream_t s) {
+#define LEE_FILTER_INC(HF)                                                                                   \
+  if (hf == HF) {                                                                                            \
+    if (dim == 2)                                                                                            \
+      k_filter_tma_row<float, 2, true, HF, true><<<dim3(tiles, 1, p.V), 256, filter_smem<float, HF, 1, 2>(), s>>>( \
+          y, inc, p);                                                                                        \
+    else                                                                                                     \
+      k_filter_tma_row<float, 3, true, HF, true><<<dim3(tiles, chunks, p.V), 256, filter_smem<float, HF, 1, 2>(), \
+                                                   s>>>(y, inc, p);                                          \
+    return cudaGetLastError();                                                                               \
+  }
+  LEE_FILTER_INC(2)
+  LEE_FILTER_INC(4)
+  LEE_FILTER_INC(5)
+#undef LEE_FILTER_INC
   return cudaErrorInvalidValue;
 }
 

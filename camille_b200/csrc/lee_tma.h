@@ -72,6 +72,10 @@ cudaError_t launch_stage_tma(const FieldMaps& zin, const TmaStageParams<T>& p, i
 template <typename T>
 cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, int hf, int dim, int comp, int ry,
                               int tiles, int chunks, cudaStream_t s);
+// The compensated one-row fused filter with the input y_n and the last stage's increment (the
+// kernel forms y_pre and its rounding error; same bits as the pair the last stage would write).
+cudaError_t launch_filter_tma_inc(const FieldMaps& y, const FieldMaps& inc, const TmaFilterParams<float>& p, int hf,
+                                  int dim, int tiles, int chunks, cudaStream_t s);
 // The plane-marching adjoint stage (lee_adjoint_tma.cu): tensor maps of w (5 fields) then the
 // nine J*metrics fields, and its parameters.
 struct __align__(64) AdjMaps {

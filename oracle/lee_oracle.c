@@ -1455,6 +1455,11 @@ int orc_set_block_streams(orc_ctx *c, int on) {
   return LEE_OK;
 }
 
+int orc_set_increment_step(orc_ctx *c, int on) {
+  (void)c; (void)on;
+  return LEE_OK;
+}
+
 int orc_set_batching(orc_ctx *c, int on) {
   (void)c; (void)on;
   return LEE_OK;

@@ -361,3 +361,28 @@ def test_axisymmetry_arguments_are_checked(product_lib):
     s3 = api.Solver(product_lib, cases.curvi3d(n=12, nsteps=1), upload=False, prepare=False)
     assert product_lib.set_axisymmetric(s3.ctx, 1, 0) == api.LEE_ERR_ARG
     assert product_lib.set_axisymmetric(s3.ctx, 0, 0) == api.LEE_OK
+
+
+@pytest.mark.parametrize("label", ["curvi3d_40_sponge", "pulse2d_96", "curvi3d_36_rk2_monopole"])
+def test_increment_step_gives_the_same_bits(product_lib, label):
+    """The compensated step whose last stage writes the increment alone (the fused filter forms
+    y_pre = y_n + increment and its rounding error) gives the bits of the step whose last stage
+    writes y_pre and its error, over replayed step graphs and direct launches."""
+    case = {
+        "curvi3d_40_sponge": lambda: cases.curvi3d(n=40, nsteps=11, halfwidth=3.0, sponge=4),
+        "pulse2d_96": lambda: cases.pulse2d(n=96, length=95 * 100.0 / 255.0, sponge=10, nsteps=11),
+        "curvi3d_36_rk2_monopole": lambda: (lambda c: (setattr(c, "rk", "RUNGE_KUTTA2"),
+                                                       setattr(c, "monopole", (17.0, 18.0, 16.0, 1e-3, 0.6, 2.5, 0.0)),
+                                                       c)[-1])(cases.curvi3d(n=36, nsteps=11, halfwidth=3.0, sponge=4)),
+    }[label]()
+    a = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
+    b = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
+    assert product_lib.set_increment_step(b.ctx, 0) == api.LEE_OK
+    dt = a.compute_dt()
+    for n in (1, case.nsteps, 3):
+        a.advance(n, dt)
+        b.advance(n, dt)
+    ya, sa, ta = a.download(0)
+    yb, sb, tb = b.download(0)
+    assert (sa, ta) == (sb, tb)
+    np.testing.assert_array_equal(ya, yb)
