@@ -97,17 +97,19 @@ def stage_bytes_per_point(info, comp: bool, sponge_field: bool) -> float:
     """Algorithmic HBM bytes per grid point of one fused stage launch, averaged over the
     four RK4 stages: every stage reads its input, y_n and the accumulator once and writes
     the next input and the accumulator once (words per stage: FP64 3,5,5,3 x V;
-    compensated 4,5,5,5 x V), plus the non-uniform coefficient fields (J*metrics) and the
-    summed sponge-strength field the TMA stage kernels read where sponges exist."""
+    compensated 4,5,5,5 x V, or 4,5,5,3 x V when the last stage writes the increment alone),
+    plus the non-uniform coefficient fields (J*metrics) and the summed sponge-strength field
+    the TMA stage kernels read where sponges exist."""
     V, e = info.state_vars, info.bytes_per_value
-    words = (4 + 5 + 5 + 5) / 4.0 if comp else (3 + 5 + 5 + 3) / 4.0
+    last = 3 if getattr(info, "increment_step", 0) else 5
+    words = (4 + 5 + 5 + last) / 4.0 if comp else (3 + 5 + 5 + 3) / 4.0
     return words * V * e + (info.num_coef_fields + (1 if sponge_field else 0)) * e
 
 
 def filter_bytes_per_point(info, comp: bool, dim: int) -> float:
     """The fused filter reads the pre-filter state once and writes the filtered state once
-    (FP64: 2 V words; compensated: y_pre and its rounding error in, y and its error out, 4 V
-    words); the per-direction passes move more."""
+    (FP64: 2 V words; compensated: y_pre and its rounding error in -- or y_n and the last stage's
+    increment -- and y and its error out, 4 V words); the per-direction passes move more."""
     V, e = info.state_vars, info.bytes_per_value
     if info.tma_filter:
         filt = 4 if comp else 2

@@ -52,7 +52,7 @@ class LeeInfo(C.Structure):
                 ("tma_stage", C.c_int), ("tma_filter", C.c_int), ("stage_chunk", C.c_int),
                 ("filter_chunk", C.c_int), ("batched", C.c_int), ("batch_stage_tile", C.c_int * 2),
                 ("batch_filter_tile", C.c_int * 2), ("filter_kernel", C.c_int), ("stage_kernel", C.c_int),
-                ("filter_rows", C.c_int)]
+                ("filter_rows", C.c_int), ("increment_step", C.c_int)]
 
 
 class LeeStats(C.Structure):

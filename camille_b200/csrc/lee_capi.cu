@@ -491,6 +491,8 @@ int lee_get_info(lee_ctx* c, lee_info* info) {
   info->filter_kernel = c->blk.empty() ? 0 : c->blk[0].filter_px;
   info->stage_kernel = c->blk.empty() ? 0 : c->blk[0].stage_px;
   info->filter_rows = c->blk.empty() ? 0 : c->blk[0].filter_ry;
+  info->increment_step = c->blk.empty() ? 0 : 1;
+  for (const auto& b : c->blk) info->increment_step &= increment_step_applies(c, b) ? 1 : 0;
   info->batched = c->batch.active ? 1 : 0;
   if (c->batch.active) {
     batch_shape(c->batch.sshape, &info->batch_stage_tile[0], &info->batch_stage_tile[1]);

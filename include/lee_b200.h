@@ -269,6 +269,7 @@ typedef struct {
   int filter_kernel;         /* fused filter of block 0: 0 scalar, else the vector group width */
   int stage_kernel;          /* TMA stage kernel of block 0: points per thread */
   int filter_rows;           /* scalar fused filter of block 0: tile rows per thread row (1 or 2) */
+  int increment_step;        /* 1 when every block's compensated step hands the increment to the filter */
 } lee_info;
 int lee_get_info(lee_ctx *ctx, lee_info *info);
 
