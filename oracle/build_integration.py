@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
 OBJ = os.path.join(OUT, "obj")
+OWN = os.path.join(OUT, "integration_obj")   # kept apart: oracle/build_ref.py links every object in OBJ
 WORK = os.path.join(OUT, "src")
 MINIMPI = os.path.join(HERE, "minimpi")
 EXE = os.path.join(OUT, "camille_b200_solve")
@@ -43,12 +44,13 @@ def build() -> str:
     lib = os.path.join(LIBDIR, "liblee_b200.so")
     if not os.path.isfile(lib):
         raise FileNotFoundError("build the library first: python camille_b200/build.py")
-    main_o = os.path.join(OBJ, "integration_main.o")
-    solve_o = os.path.join(OBJ, "integration_solve.o")
+    os.makedirs(OWN, exist_ok=True)
+    main_o = os.path.join(OWN, "main.o")
+    solve_o = os.path.join(OWN, "solve.o")
     _run(CXX + ["-c", os.path.join(WORK, "core", "main.cpp"), "-o", main_o])
     _run(CXX + ["-I", os.path.join(WORK, "solver"), "-I", os.path.join(ROOT, "include"), "-c",
                 os.path.join(HERE, "ref_solve_b200.cpp"), "-o", solve_o])
-    skip = {"driver.o", "solver_solver.o", "integration_main.o", "integration_solve.o"}
+    skip = {"driver.o", "solver_solver.o"}
     objs = sorted(os.path.join(OBJ, o) for o in os.listdir(OBJ) if o.endswith(".o") and o not in skip)
     rel = os.path.relpath(LIBDIR, OUT)
     _run(["g++", "-O3", "-o", EXE, main_o, solve_o] + objs +
