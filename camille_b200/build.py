@@ -39,6 +39,8 @@ UNITS = {
     "lee_filter.cu": [],
     "lee_stage_pair.cu": [],
     "lee_adjoint_tma.cu": [],
+    "lee_adjoint_gen.cu": [],
+    "lee_host_adjoint_gen.cu": [],
 }
 
 

@@ -215,6 +215,7 @@ struct lee_ctx {
     int* d_base = nullptr;                 // trace row of the first step of a replayed chunk
     int host_row = 0;                      // trace row of the next directly launched step
     double* d_gbar = nullptr;              // gradient of the distributed source's box field
+    size_t gbar_n = 0;
     std::vector<void*> ckpt;               // checkpoints: V (+ V carried errors) fields each
     size_t ckpt_slots = 0;
     bool tma = false;                      // the plane-marching stage kernel (lee_adjoint_tma.cu)
@@ -222,6 +223,20 @@ struct lee_ctx {
     bool fused_filter = false;             // F^T by the fused filter kernel (lee_tma.cu)
     cudaStream_t rev = nullptr;            // the reverse sweep's stream when segments are recomputed
     cudaEvent_t ev_fwd = nullptr, ev_rev = nullptr;
+    // the general path (lee_adjoint_gen.cu): every block, holes, BC lines, overset, any mean flow
+    bool gen = false;
+    struct GenBlock {
+      void *lam[kMaxVars] = {}, *mu[kMaxVars] = {}, *kb[2][kMaxVars] = {}, *ybar[kMaxVars] = {};
+      void *nu[kMaxVars] = {}, *g[3][kMaxVars] = {};
+      void* rb[2] = {};                    // adjoint of rho'/rho_bar: [0] carried in, [1] produced
+    };
+    std::vector<GenBlock> gb;
+    bool rb_live = false;                  // gb[].rb[0] holds the next step's rho' adjoint
+    int ovs_nd = 0;                        // donor points of the transposed overset gather
+    int *d_ub = nullptr, *d_off = nullptr, *d_cr = nullptr;
+    long long* d_ul = nullptr;
+    double *d_cw = nullptr, *d_otmp = nullptr;
+    std::vector<void*> rho_ckpt;           // rho'/rho_bar at each checkpoint (blocks that need it)
   } adj;
 };
 
@@ -313,6 +328,8 @@ int check_finite(lee_ctx* c);
 int fork_sides(lee_ctx* c);
 int join_sides(lee_ctx* c);
 template <typename T>
+void fill_bc_params(lee_ctx* c, const BlockData& b, const Boundary& z, void** f, void** e, BcParams<T>& p);
+template <typename T>
 int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e, double t, const double* t_tab, const int* ctr,
               int t_stride);
 template <typename T>
@@ -349,6 +366,13 @@ int advance_timed(lee_ctx* c, int nsteps, const std::vector<double>& dts);
 int adjoint_setup(lee_ctx* c);
 template <typename T>
 int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar);
+// the general path (lee_host_adjoint_gen.cu)
+bool adjoint_fast_applies(lee_ctx* c, const char** why);
+int adjoint_gen_setup(lee_ctx* c);
+// one transposed step of every block; rho_in: the forward step's first stage read rho'/rho_bar
+// of the previous step (its adjoint is produced and carried to the next transposed step)
+template <typename T>
+int adjoint_step_gen(lee_ctx* c, double dt, const double* amps, double* gbar, bool rho_in);
 int ensure_trace(lee_ctx* c, size_t rows);
 int advance_traced(lee_ctx* c, int nsteps, double dt, int row0);
 double objective_of(const lee_ctx* c, const std::vector<double>& tr);

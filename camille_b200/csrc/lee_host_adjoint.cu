@@ -69,37 +69,22 @@ bool build_transpose(const OpTable& op, TransOp* t) {
   return true;
 }
 
-// Checks and buffers of the adjoint path; the operators it transposes must be the
-// uniform-mean, single-block, hole-free ones.
+// Checks and buffers of the adjoint path: the uniform-mean single-block path when it applies,
+// else the general path (lee_host_adjoint_gen.cu).
 int adjoint_setup(lee_ctx* c) {
   auto& a = c->adj;
   if (a.ready) return LEE_OK;
-  if (c->blk.size() != 1) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint covers single-block contexts");
+  if (!adjoint_fast_applies(c, nullptr)) return adjoint_gen_setup(c);
   BlockData& b = c->blk[0];
-  if (b.has_iblank || c->ovs.n > 0) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no holes or overset");
-  if (c->axisym) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no axisymmetric term");
-  for (auto& z : b.bnd) {
-    if (z.kind == LEE_SPONGE_FREUND_HARMONICWAVE)
-      return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no harmonic-wave sponge");
-    if (z.kind != LEE_SPONGE_FREUND_AMBIENT) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no BC lines");
-  }
-  auto is_const = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? !f.p : !d.p; };
-  auto is_zero = [&](const Coef<double>& d, const Coef<float>& f) { return c->comp ? f.zero != 0 : d.zero != 0; };
-  bool uni = is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi);
-  for (int q = 0; q < 3; ++q)
-    uni = uni && is_const(b.cd_ub[q], b.cf_ub[q]) && is_zero(b.cd_gs[q], b.cf_gs[q]) && is_zero(b.cd_gp[q], b.cf_gp[q]);
-  for (int q = 0; q < 9; ++q) uni = uni && is_zero(b.cd_gu[q], b.cf_gu[q]);
-  if (!uni) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint needs a uniform mean flow");
-  if (!build_transpose(c->fd, &a.dT)) return fail(c, LEE_ERR_UNSUPPORTED, "difference operator too wide to transpose");
-  if (c->cfg.filter_scheme != LEE_FILTER_NONE && !build_transpose(c->flt, &a.fT))
-    return fail(c, LEE_ERR_UNSUPPORTED, "filter too wide to transpose");
-  // a line must keep the two ends' class rows apart, and a class row must only meet closure
-  // rows of its own end: n >= 2E and n >= E + H + h
+  // the class-row transposes need rows within reach and lines that keep the two ends' class
+  // rows apart (n >= 2E, n >= E + H + h); otherwise the general path's per-point rows serve
+  if (!build_transpose(c->fd, &a.dT)) return adjoint_gen_setup(c);
+  if (c->cfg.filter_scheme != LEE_FILTER_NONE && !build_transpose(c->flt, &a.fT)) return adjoint_gen_setup(c);
   const int n[3] = {b.nx, b.ny, b.nz};
   int need = std::max(2 * a.dT.E, a.dT.E + a.dT.H + c->fd.h);
   if (c->cfg.filter_scheme != LEE_FILTER_NONE) need = std::max(need, std::max(2 * a.fT.E, a.fT.E + a.fT.H + c->flt.h));
   for (int d = 0; d < c->cfg.num_dim; ++d)
-    if (n[d] < need) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint needs %d points per direction", need);
+    if (n[d] < need) return adjoint_gen_setup(c);
   // the plane-marching stage kernel: 3-D, transposed stencils within two points, rows of 16-byte
   // multiples, 32-bit point offsets, J*metrics all fields or all constants
   {
@@ -276,6 +261,16 @@ double objective_of(const lee_ctx* c, const std::vector<double>& tr) {
   return c->adj.weight * J;
 }
 
+// The adjoint fields of block bi (the uniform path keeps one block's).
+void** lam_of(lee_ctx* c, int bi) { return c->adj.gen ? c->adj.gb[(size_t)bi].lam : c->adj.lam; }
+
+// One transposed step on whichever path the context set up, in its working precision.
+int adjoint_step_any(lee_ctx* c, double dt, const double* amps, double* gbar, bool rho_in) {
+  if (c->adj.gen)
+    return c->comp ? adjoint_step_gen<float>(c, dt, amps, gbar, rho_in) : adjoint_step_gen<double>(c, dt, amps, gbar, rho_in);
+  return c->comp ? adjoint_step<float>(c, dt, amps, gbar) : adjoint_step<double>(c, dt, amps, gbar);
+}
+
 // the host translation units use both precisions
 template int adjoint_step<float>(lee_ctx* c, double dt, const double* amps, double* gbar);
 template int adjoint_step<double>(lee_ctx* c, double dt, const double* amps, double* gbar);
@@ -339,28 +334,40 @@ int lee_apply_adjoint(lee_ctx* c, int nsteps, double dt) {
   CK(cudaSetDevice(c->cfg.device));
   int rc = adjoint_setup(c);
   if (rc) return rc;
-  BlockData& b = c->blk[0];
   auto& a = c->adj;
-  const size_t bytes = (size_t)b.N * c->esz;
-  // the state slots hold the adjoint variable (with a compensated state, y + e rounded)
-  for (int v = 0; v < c->V; ++v) {
-    if (c->comp) {
-      k_add_pair<<<grid1d(b.N), 256, 0, c->stream>>>(b.N, (float*)a.lam[v], (const float*)b.y[v],
-                                                      (const float*)b.comp[v]);
-      CK(cudaGetLastError());
-    } else {
-      CK(cudaMemcpyAsync(a.lam[v], b.y[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  // the state slots of every block hold the adjoint variable (with a compensated state, y + e rounded)
+  for (size_t bi = 0; bi < c->blk.size(); ++bi) {
+    BlockData& b = c->blk[bi];
+    void** lam = lam_of(c, (int)bi);
+    const size_t bytes = (size_t)b.N * c->esz;
+    for (int v = 0; v < c->V; ++v) {
+      if (c->comp) {
+        k_add_pair<<<grid1d(b.N), 256, 0, c->stream>>>(b.N, (float*)lam[v], (const float*)b.y[v],
+                                                        (const float*)b.comp[v]);
+        CK(cudaGetLastError());
+      } else {
+        CK(cudaMemcpyAsync(lam[v], b.y[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      }
     }
   }
+  a.rb_live = false;
+  // the transposed map of nsteps forward steps from an uploaded state: the first of them reads no
+  // rho'/rho_bar of a previous step
   for (int it = 0; it < nsteps; ++it) {
-    rc = c->comp ? adjoint_step<float>(c, dt, nullptr, nullptr) : adjoint_step<double>(c, dt, nullptr, nullptr);
+    const bool rho_in = nsteps - it >= 2;
+    rc = adjoint_step_any(c, dt, nullptr, nullptr, rho_in);
     if (rc) return rc;
   }
-  for (int v = 0; v < c->V; ++v) {
-    CK(cudaMemcpyAsync(b.y[v], a.lam[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
-    if (c->comp) CK(cudaMemsetAsync(b.comp[v], 0, bytes, c->stream));
+  for (size_t bi = 0; bi < c->blk.size(); ++bi) {
+    BlockData& b = c->blk[bi];
+    void** lam = lam_of(c, (int)bi);
+    const size_t bytes = (size_t)b.N * c->esz;
+    for (int v = 0; v < c->V; ++v) {
+      CK(cudaMemcpyAsync(b.y[v], lam[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      if (c->comp) CK(cudaMemsetAsync(b.comp[v], 0, bytes, c->stream));
+    }
+    b.rho_valid = false;
   }
-  b.rho_valid = false;
   CK(cudaStreamSynchronize(c->stream));
   return check_device_error(c);
 }
@@ -372,44 +379,64 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
   if (c->adj.mic.empty()) return fail(c, LEE_ERR_STATE, "lee_set_objective first");
   if (c->src_kind != LEE_SOURCE_DISTRIBUTED) return fail(c, LEE_ERR_STATE, "the gradient is for a distributed source");
   if (nsteps < 1 || checkpoint_every < 1 || !(dt > 0.0)) return fail(c, LEE_ERR_ARG, "nsteps, checkpoint_every, dt");
-  if (c->adj.mic_block != 0) return fail(c, LEE_ERR_ARG, "objective block");
   CK(cudaSetDevice(c->cfg.device));
   memset(&c->stats, 0, sizeof c->stats);
   int rc = adjoint_setup(c);
   if (rc) return rc;
   auto& a = c->adj;
-  BlockData& b = c->blk[0];
   const int V = c->V;
-  const size_t bytes = (size_t)b.N * c->esz;
+  const int nbk = (int)c->blk.size();
+  const int sb = (int)c->dsrc[0];
+  BlockData& bs = c->blk[(size_t)sb];
   const int K = checkpoint_every;
   const int nseg = (nsteps + K - 1) / K;
-  const int fields = c->comp ? 2 * V : V;
-  // checkpoint slots: the state at the start of every segment
-  if (a.ckpt_slots < (size_t)nseg) {
+  // what a checkpoint holds: every block's state (and carried errors), and rho'/rho_bar of the
+  // blocks whose first stage reads it
+  struct Slot {
+    int b, kind, v;  // kind 0 y, 1 comp, 2 rho
+  };
+  std::vector<Slot> slots;
+  bool rho0 = false;
+  std::vector<char> rho_start((size_t)nbk, 0);
+  for (int bi = 0; bi < nbk; ++bi) {
+    BlockData& b = c->blk[(size_t)bi];
+    for (int v = 0; v < V; ++v) slots.push_back({bi, 0, v});
+    if (c->comp)
+      for (int v = 0; v < V; ++v) slots.push_back({bi, 1, v});
+    if (b.need_rho) {
+      slots.push_back({bi, 2, 0});
+      rho_start[(size_t)bi] = b.rho_valid ? 1 : 0;
+      rho0 |= b.rho_valid;
+    }
+  }
+  auto field = [&](const Slot& q) -> void* {
+    BlockData& b = c->blk[(size_t)q.b];
+    return q.kind == 0 ? b.y[q.v] : q.kind == 1 ? b.comp[q.v] : b.rho;
+  };
+  auto bytes_of = [&](const Slot& q) { return (size_t)c->blk[(size_t)q.b].N * c->esz; };
+  const size_t fields = slots.size();
+  if (a.ckpt_slots < (size_t)nseg || a.ckpt.size() < (size_t)nseg * fields) {
     for (size_t q = a.ckpt.size(); q < (size_t)nseg * fields; ++q) {
       void* p = nullptr;
-      if ((rc = dev_alloc(c, &p, bytes))) return rc;
+      if ((rc = dev_alloc(c, &p, bytes_of(slots[q % fields])))) return rc;
       a.ckpt.push_back(p);
     }
     a.ckpt_slots = (size_t)nseg;
   }
   if ((rc = ensure_trace(c, (size_t)nsteps))) return rc;
   auto save = [&](int seg) -> int {
-    for (int v = 0; v < V; ++v) {
-      CK(cudaMemcpyAsync(a.ckpt[(size_t)seg * fields + v], b.y[v], bytes, cudaMemcpyDeviceToDevice, c->stream));
-      if (c->comp)
-        CK(cudaMemcpyAsync(a.ckpt[(size_t)seg * fields + V + v], b.comp[v], bytes, cudaMemcpyDeviceToDevice,
-                           c->stream));
-    }
+    for (size_t q = 0; q < fields; ++q)
+      CK(cudaMemcpyAsync(a.ckpt[(size_t)seg * fields + q], field(slots[q]), bytes_of(slots[q]), cudaMemcpyDeviceToDevice,
+                         c->stream));
     return LEE_OK;
   };
   auto restore = [&](int seg) -> int {
-    for (int v = 0; v < V; ++v) {
-      CK(cudaMemcpyAsync(b.y[v], a.ckpt[(size_t)seg * fields + v], bytes, cudaMemcpyDeviceToDevice, c->stream));
-      if (c->comp)
-        CK(cudaMemcpyAsync(b.comp[v], a.ckpt[(size_t)seg * fields + V + v], bytes, cudaMemcpyDeviceToDevice,
-                           c->stream));
-    }
+    for (size_t q = 0; q < fields; ++q)
+      CK(cudaMemcpyAsync(field(slots[q]), a.ckpt[(size_t)seg * fields + q], bytes_of(slots[q]), cudaMemcpyDeviceToDevice,
+                         c->stream));
+    // a segment after the first starts on the rho'/rho_bar its previous step wrote
+    for (int bi = 0; bi < nbk; ++bi)
+      if (c->blk[(size_t)bi].need_rho) c->blk[(size_t)bi].rho_valid = seg > 0 || rho_start[(size_t)bi];
     return LEE_OK;
   };
   // forward pass: checkpoints, traces, the stage times of every step
@@ -421,7 +448,6 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
     if ((rc = save(seg))) return rc;
     if ((rc = advance_traced(c, n, dt, seg * K))) return rc;
   }
-  const long long fwd_launches = c->stats.kernel_launches;
   std::vector<double> tr((size_t)nsteps * a.mic.size());
   CK(cudaMemcpyAsync(tr.data(), a.d_trace, tr.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -430,20 +456,29 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
   const double t_end = c->time;
   const int step_end = c->step;
   std::vector<void*> fin;
+  std::vector<char> rho_end((size_t)nbk, 0);
   if (recompute) {
-    for (int q = 0; q < fields; ++q) {
+    for (size_t q = 0; q < fields; ++q) {
       void* p = nullptr;
-      CK(cudaMallocAsync(&p, bytes, c->stream));
+      CK(cudaMallocAsync(&p, bytes_of(slots[q]), c->stream));
       fin.push_back(p);
-      CK(cudaMemcpyAsync(p, q < V ? b.y[q] : b.comp[q - V], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(p, field(slots[q]), bytes_of(slots[q]), cudaMemcpyDeviceToDevice, c->stream));
     }
+    for (int bi = 0; bi < nbk; ++bi) rho_end[(size_t)bi] = c->blk[(size_t)bi].rho_valid ? 1 : 0;
   }
   // reverse sweep
-  const size_t nbox = (size_t)(b.src_hi[0] - b.src_lo[0] + 1) * (b.src_hi[1] - b.src_lo[1] + 1) *
-                      (b.src_hi[2] - b.src_lo[2] + 1);
-  if (!a.d_gbar && (rc = dalloc(c, &a.d_gbar, nbox))) return rc;
+  const size_t nbox = (size_t)(bs.src_hi[0] - bs.src_lo[0] + 1) * (bs.src_hi[1] - bs.src_lo[1] + 1) *
+                      (bs.src_hi[2] - bs.src_lo[2] + 1);
+  if (a.gbar_n < nbox) {
+    if ((rc = dalloc(c, &a.d_gbar, nbox))) return rc;
+    a.gbar_n = nbox;
+  }
   CK(cudaMemsetAsync(a.d_gbar, 0, nbox * sizeof(double), c->stream));
-  for (int v = 0; v < V; ++v) CK(cudaMemsetAsync(a.lam[v], 0, bytes, c->stream));
+  for (int bi = 0; bi < nbk; ++bi) {
+    void** lam = lam_of(c, bi);
+    for (int v = 0; v < V; ++v) CK(cudaMemsetAsync(lam[v], 0, (size_t)c->blk[(size_t)bi].N * c->esz, c->stream));
+  }
+  a.rb_live = false;
   const Tableau tb = tableau(c->cfg.rk_scheme);
   const size_t M = a.mic.size();
   const double scale = 2.0 * a.weight;
@@ -479,20 +514,20 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
     double t = seg_time[(size_t)seg];
     for (int k = 0; k < n; ++k) {
       t += dt;
-      for (int s = 0; s < tb.ns; ++s) amps[(size_t)k * tb.ns + s] = source_amp(c, b, t + tb.c[s] * dt);
+      for (int s = 0; s < tb.ns; ++s) amps[(size_t)k * tb.ns + s] = source_amp(c, bs, t + tb.c[s] * dt);
     }
     // the reverse steps go to the reverse stream (every launch below reads c->stream)
     if (recompute) c->stream = a.rev;
+    void** lam_mic = lam_of(c, a.mic_block);
     for (int k = n - 1; k >= 0 && !rc; --k) {
       const int step = n0 + k;  // 0-based: this transposed step maps the adjoint of y_{step+1} to y_step
       cudaError_t e = c->comp
-                          ? launch_mic_force<float>((int)M, a.d_mic, (float*)a.lam[P], a.d_trace, step, scale, c->stream)
-                          : launch_mic_force<double>((int)M, a.d_mic, (double*)a.lam[P], a.d_trace, step, scale,
+                          ? launch_mic_force<float>((int)M, a.d_mic, (float*)lam_mic[P], a.d_trace, step, scale, c->stream)
+                          : launch_mic_force<double>((int)M, a.d_mic, (double*)lam_mic[P], a.d_trace, step, scale,
                                                      c->stream);
       if (e != cudaSuccess) rc = fail(c, LEE_ERR_CUDA, "microphone forcing: %s", cudaGetErrorString(e));
-      if (!rc)
-        rc = c->comp ? adjoint_step<float>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar)
-                     : adjoint_step<double>(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar);
+      if (!rc) rc = adjoint_step_any(c, dt, &amps[(size_t)k * tb.ns], a.d_gbar, step > 0 || rho0);
+      lam_mic = lam_of(c, a.mic_block);
     }
     c->stream = main_stream;
     if (rc) {
@@ -513,16 +548,16 @@ int lee_adjoint_gradient(lee_ctx* c, int nsteps, double dt, int checkpoint_every
   std::vector<double> gbox(nbox);
   CK(cudaMemcpyAsync(gbox.data(), a.d_gbar, nbox * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  restrict_to_lattice(c->dsrc, c->cfg.num_dim, b.src_lo, b.src_hi, gbox.data(), grad);
+  restrict_to_lattice(c->dsrc, c->cfg.num_dim, bs.src_lo, bs.src_hi, gbox.data(), grad);
   if (recompute) {
-    for (int q = 0; q < fields; ++q) {
-      CK(cudaMemcpyAsync(q < V ? b.y[q] : b.comp[q - V], fin[(size_t)q], bytes, cudaMemcpyDeviceToDevice, c->stream));
-      CK(cudaFreeAsync(fin[(size_t)q], c->stream));
+    for (size_t q = 0; q < fields; ++q) {
+      CK(cudaMemcpyAsync(field(slots[q]), fin[q], bytes_of(slots[q]), cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaFreeAsync(fin[q], c->stream));
     }
+    for (int bi = 0; bi < nbk; ++bi) c->blk[(size_t)bi].rho_valid = rho_end[(size_t)bi] != 0;
     set_clock(c, t_end, step_end);
   }
   CK(cudaStreamSynchronize(c->stream));
-  (void)fwd_launches;
   if (trace_mismatches) *trace_mismatches = mismatches;
   return check_device_error(c);
 }

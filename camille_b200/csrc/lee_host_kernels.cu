@@ -343,6 +343,34 @@ int check_finite(lee_ctx* c) {
   return LEE_OK;
 }
 
+// The launch parameters of one BC line on the fields f (e: the errors of a compensated pair);
+// the update's time is the caller's.
+template <typename T>
+void fill_bc_params(lee_ctx* c, const BlockData& b, const Boundary& z, void** f, void** e, BcParams<T>& p) {
+  memset(&p, 0, sizeof p);
+  p.kind = z.kind; p.dir = z.dir; p.end = z.end;
+  p.nd = c->cfg.num_dim; p.V = c->V;
+  for (int d = 0; d < 3; ++d) {
+    p.lo[d] = z.lo[d];
+    p.nb[d] = z.hi[d] - z.lo[d] + 1;
+  }
+  p.lo[z.dir] = z.end == 0 ? z.lo[z.dir] : z.hi[z.dir];
+  p.nb[z.dir] = 1;
+  p.nx = b.nx; p.ny = b.ny;
+  p.sd = z.dir == 0 ? 1 : z.dir == 1 ? (long long)b.nx : (long long)b.nx * b.ny;
+  p.S = c->fd.S;
+  for (int q = 0; q < c->fd.S; ++q) p.c0[q] = c->fd.B[0][q];
+  for (int v = 0; v < c->V; ++v) {
+    p.y[v] = (T*)f[v];
+    p.e[v] = e ? (T*)e[v] : nullptr;
+  }
+  for (int q = 0; q < 9; ++q) { p.met[q] = b.d_met[q]; p.minv[q] = b.d_minv[q]; }
+  p.jac = b.d_jac;
+  p.iblank = b.has_holes ? b.d_iblank : nullptr;
+  p.wave = c->wave;
+  for (int d = 0; d < 3; ++d) p.xyz[d] = b.d_xyz[d];
+}
+
 // Every BC line of a block, in the order they were added, on the fields f (with the
 // rounding errors e of a compensated pair, or null).
 template <typename T>
@@ -351,28 +379,7 @@ int apply_bcs(lee_ctx* c, BlockData& b, void** f, void** e, double t, const doub
   for (auto& z : b.bnd) {
     if (!is_bc_line(z.kind)) continue;
     BcParams<T> p;
-    memset(&p, 0, sizeof p);
-    p.kind = z.kind; p.dir = z.dir; p.end = z.end;
-    p.nd = c->cfg.num_dim; p.V = c->V;
-    for (int d = 0; d < 3; ++d) {
-      p.lo[d] = z.lo[d];
-      p.nb[d] = z.hi[d] - z.lo[d] + 1;
-    }
-    p.lo[z.dir] = z.end == 0 ? z.lo[z.dir] : z.hi[z.dir];
-    p.nb[z.dir] = 1;
-    p.nx = b.nx; p.ny = b.ny;
-    p.sd = z.dir == 0 ? 1 : z.dir == 1 ? (long long)b.nx : (long long)b.nx * b.ny;
-    p.S = c->fd.S;
-    for (int q = 0; q < c->fd.S; ++q) p.c0[q] = c->fd.B[0][q];
-    for (int v = 0; v < c->V; ++v) {
-      p.y[v] = (T*)f[v];
-      p.e[v] = e ? (T*)e[v] : nullptr;
-    }
-    for (int q = 0; q < 9; ++q) { p.met[q] = b.d_met[q]; p.minv[q] = b.d_minv[q]; }
-    p.jac = b.d_jac;
-    p.iblank = b.has_holes ? b.d_iblank : nullptr;
-    p.wave = c->wave;
-    for (int d = 0; d < 3; ++d) p.xyz[d] = b.d_xyz[d];
+    fill_bc_params<T>(c, b, z, f, e, p);
     p.t = t;
     p.t_tab = t_tab;
     p.ctr = ctr;
@@ -437,6 +444,8 @@ template int launch_filter_fused<double>(lee_ctx* c, BlockData& b, void* const* 
                         void* const* comp_out, int chunk_override, void* const* inc);
 template int autotune<float>(lee_ctx* c, BlockData& b);
 template int autotune<double>(lee_ctx* c, BlockData& b);
+template void fill_bc_params<float>(lee_ctx*, const BlockData&, const Boundary&, void**, void**, BcParams<float>&);
+template void fill_bc_params<double>(lee_ctx*, const BlockData&, const Boundary&, void**, void**, BcParams<double>&);
 template int apply_bcs<float>(lee_ctx* c, BlockData& b, void** f, void** e, double t, const double* t_tab, const int* ctr,
               int t_stride);
 template int apply_bcs<double>(lee_ctx* c, BlockData& b, void** f, void** e, double t, const double* t_tab, const int* ctr,

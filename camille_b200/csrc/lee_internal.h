@@ -295,6 +295,82 @@ template <typename T>
 cudaError_t launch_mic_force(int n, const long long* l0, T* lam_p, const double* trace, int row, double scale,
                              cudaStream_t s);
 
+// ---- the general discrete adjoint (lee_adjoint_gen.cu) ------------------------------------
+// One transposed RK stage of one block: zbar = L^T w, w = scale * kin, with the forward stage's
+// coefficients, sponge zones, closure codes and source box in `f` (fill_stage_common).
+template <typename T>
+struct AdjGenParams {
+  StageParams<T> f;
+  T scale;
+  const T* kin[kMaxVars];
+  T* g[3][kMaxVars];         // the fluxes G^d (flux kernel out, stage kernel in)
+  T* zbar[kMaxVars];
+  T* rbar;                   // the adjoint of rho_prev when the forward stage read it, else null
+  double* gbar;              // the source box's gradient (null: none)
+  double amp;
+};
+
+// One transposed filter pass (reverse order of the forward's passes): the first reads M lam
+// (mask_in), the last blends (1 - beta) M lam + beta F^T(...) and adds R^T rb.
+template <typename T>
+struct AdjGenFilterParams {
+  int nx, ny, nz, V, dir, last, mask_in;
+  const T* in[kMaxVars];
+  T* out[kMaxVars];
+  const T* lam[kMaxVars];
+  T blend;
+  OpTable op;
+  const int8_t* code;        // the filter's closure codes along dir (null: by position)
+  const int* iblank;         // holes (null: none)
+  const T* rb;               // adjoint of rho'/rho_bar of Y (null: none)
+  const double* pbar;
+  T inv_gamma;
+};
+
+// Pointwise operands: mask (and R^T rb) of `in` into `out`, or the stage combine
+// nu = M in; ybar += nu; out = hb mu + ha nu (out[0] null: ybar += in unmasked).
+template <typename T>
+struct AdjGenPoint {
+  const T* in[kMaxVars];
+  T* out[kMaxVars];
+  const T* mu[kMaxVars];
+  T* ybar[kMaxVars];
+  const int* iblank;
+  const T* rb;
+  const double* pbar;
+  T inv_gamma;
+};
+
+// The transposed overset interpolation: n receivers (block rb, point rl) are taken out into
+// tmp (n x V), then nd donor points (block ub, point ul) gather cw * tmp over their receiver
+// lists off[u]..off[u+1] (receiver cr).
+template <typename T>
+struct AdjGenOvs {
+  int n, nd, V;
+  const int* rb;
+  const long long* rl;
+  const int* ub;
+  const long long* ul;
+  const int* off;
+  const double* cw;
+  const int* cr;
+  double* tmp;
+  T* y[kMaxOvsBlocks][kMaxVars];
+};
+
+template <typename T>
+cudaError_t launch_adjg_stage(const AdjGenParams<T>& p, cudaStream_t s);
+template <typename T>
+cudaError_t launch_adjg_filter(const AdjGenFilterParams<T>& p, cudaStream_t s);
+template <typename T>
+cudaError_t launch_adjg_mask(long long n, int V, const AdjGenPoint<T>& p, cudaStream_t s);
+template <typename T>
+cudaError_t launch_adjg_combine(long long n, int V, const AdjGenPoint<T>& p, double hb, double ha, cudaStream_t s);
+template <typename T>
+cudaError_t launch_adjg_bc(const BcParams<T>& p, cudaStream_t s);
+template <typename T>
+cudaError_t launch_adjg_overset(const AdjGenOvs<T>& p, cudaStream_t s);
+
 // ---- batches of 2-D blocks (lee_batch.cu) ------------------------------------------------
 // Per-block filter operands of the batched filter: pre-filter state x (FP64: y_next;
 // compensated: y_pre, with its rounding error err), outputs y (and the new error comp).

@@ -332,20 +332,25 @@ int lee_set_filter_kernel(lee_ctx *ctx, int kind);
 int lee_set_stage_kernel(lee_ctx *ctx, int kind);
 
 /* ---- discrete adjoint (no reference counterpart: the reference has no adjoint) ----------
- * The step map of lee_advance is linear in the state; these entry points apply its exact
- * transpose (transposed stencils and closures, transposed filter, reverse RK stages) on a
- * single-block context with a uniform mean flow, sponges allowed, no BC lines, holes or
- * overset. */
+ * The step map of lee_advance is affine in the state; these entry points apply the exact
+ * transpose of its linear part (transposed stencils and closures, transposed filter, reverse
+ * RK stages) on any context lee_advance steps with one time step: every block, holes and their
+ * closures, BC lines, sponges, overset interpolation (transposed receiver gather), non-uniform
+ * mean flow and the axisymmetric term. A single-block, uniform-mean context without BC lines,
+ * holes or overset runs the uniform-mean transposed kernels (plane-marching in 3-D); any other
+ * the general per-point kernels. Sources and harmonic waves are the affine part and have no transpose. */
 /* Objective J = weight * sum over steps n = 1..N of sum over microphones m of p'_n(l[m])^2,
  * p' of block b at linear indices l[m] (distinct) after every step. */
 int lee_set_objective(lee_ctx *ctx, int b, int n, const long long *l, double weight);
 /* Advance nsteps as lee_advance does and return J over those steps. */
 int lee_eval_objective(lee_ctx *ctx, int nsteps, double dt, double *J);
-/* Replace the uploaded state x by (M^T)^nsteps x, M the source-free step map of lee_advance
- * (the dot-product test: <l, M x> = <M^T l, x>). */
+/* Replace the uploaded state x (every block) by (M^T)^nsteps x, M^nsteps the linear part of
+ * nsteps steps of lee_advance from an uploaded state (the dot-product test:
+ * <l, M x> = <M^T l, x>; the first of those steps reads no rho'/rho_bar of a previous step). */
 int lee_apply_adjoint(lee_ctx *ctx, int nsteps, double dt);
 /* J over nsteps from the uploaded state and its gradient with respect to the amplitudes of
- * the LEE_SOURCE_DISTRIBUTED lattice (grad: cx*cy*cz values), by the discrete adjoint: the
+ * the LEE_SOURCE_DISTRIBUTED lattice (grad: cx*cy*cz values; the source's block and the
+ * microphones' block may differ), by the discrete adjoint: the
  * forward pass records the microphone traces and keeps the state every checkpoint_every
  * steps; the reverse sweep goes segment by segment from the last. recompute = 1: each
  * segment's forward steps are run again from its checkpoint before its reverse sweep, and
