@@ -115,6 +115,10 @@ SIGNATURES = {
     "eval_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _DP]),
     "apply_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "adjoint_gradient": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, _DP, _DP, _LP]),
+    "set_scalars": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_mean_scalars": (C.c_int, [C.c_void_p, C.c_int, _PP]),
+    "upload_scalars": (C.c_int, [C.c_void_p, C.c_int, _PP]),
+    "download_scalars": (C.c_int, [C.c_void_p, C.c_int, _PP]),
 }
 
 
@@ -175,6 +179,8 @@ class Solver:
         if rc != LEE_OK:
             raise LeeError(rc, lib.last_error(None).decode())
         try:
+            if case.num_scalars:
+                self._chk(lib.set_scalars(self.ctx, case.num_scalars))
             for b, blk in enumerate(case.blocks):
                 nx, ny, nz = blk.dims
                 xs = [np.ascontiguousarray(a, np.float64) for a in (blk.x, blk.y, blk.z)]
@@ -185,6 +191,9 @@ class Solver:
                 self._chk(lib.set_block(self.ctx, b, nx, ny, nz, *[_dptr(a) for a in xs], ib))
                 mean = [np.ascontiguousarray(blk.mean[v], np.float64) for v in range(5)]
                 self._chk(lib.set_mean(self.ctx, b, _fields_ptrs(mean)))
+                if case.num_scalars:
+                    zm = [np.ascontiguousarray(z, np.float64) for z in blk.zmean]
+                    self._chk(lib.set_mean_scalars(self.ctx, b, _fields_ptrs(zm)))
             for bd in case.boundaries:
                 lo = (C.c_int * 3)(*bd.lo)
                 hi = (C.c_int * 3)(*bd.hi)
@@ -259,8 +268,24 @@ class Solver:
             pass
 
     def upload(self, b: int, state: np.ndarray, step: int = 0, time: float = 0.0) -> None:
+        """The five LEE slots of block b, and with passive scalars the slots after them: a state
+        of 5 + n fields uploads both (lee_upload_state, lee_upload_scalars)."""
         f = [np.ascontiguousarray(state[v], np.float64) for v in range(5)]
         self._chk(self.lib.upload_state(self.ctx, b, _fields_ptrs(f), step, time))
+        n = self.case.num_scalars
+        if n:
+            blk = self.case.blocks[b]
+            z = state[5:5 + n] if state.shape[0] >= 5 + n else blk.zstate
+            zf = [np.ascontiguousarray(z[k], np.float64) for k in range(n)]
+            self._chk(self.lib.upload_scalars(self.ctx, b, _fields_ptrs(zf)))
+
+    def download_scalars(self, b: int = 0) -> np.ndarray:
+        """The passive scalars Z_k' of block b, (n, nz, ny, nx)."""
+        n = self.case.num_scalars
+        nx, ny, nz = self.case.blocks[b].dims
+        out = np.zeros((n, nz, ny, nx))
+        self._chk(self.lib.download_scalars(self.ctx, b, _fields_ptrs([out[k] for k in range(n)])))
+        return out
 
     def download(self, b: int = 0) -> tuple[np.ndarray, int, float]:
         nx, ny, nz = self.case.blocks[b].dims

@@ -59,6 +59,8 @@ class Block:
     state: np.ndarray      # (5, nz, ny, nx): s', u', v', w', p'
     iblank: Optional[np.ndarray] = None  # (nz, ny, nx) int32: 0 fluid, 1 hole, -1 receiver
     monopole: Optional[tuple[float, float, float, float, float, float, float]] = None  # this block's own
+    zmean: Optional[np.ndarray] = None   # (n, nz, ny, nx): mean passive scalars Z_bar_k (LEE_SCALAR)
+    zstate: Optional[np.ndarray] = None  # (n, nz, ny, nx): Z_k'
 
     @property
     def dims(self) -> tuple[int, int, int]:
@@ -179,6 +181,12 @@ class Case:
     def npoints(self) -> int:
         return sum(b.npoints for b in self.blocks)
 
+    @property
+    def num_scalars(self) -> int:
+        """Passive scalars of PHYSICAL_MODEL = LEE_SCALAR (0: plain LEE)."""
+        z = self.blocks[0].zmean
+        return 0 if z is None else int(z.shape[0])
+
     def source_monopole(self) -> Optional[tuple[float, float, float, float, float, float, float]]:
         """The monopole that acts on every block: the case's own, else the one SIMULATION implies."""
         if self.monopole is not None:
@@ -194,9 +202,12 @@ class Case:
         lines = [
             f"DIMENSION = {self.num_dim}",
             "AXISYMMETRY = TRUE, AXIS_OF_SYMMETRY = X" if self.axisymmetric else "AXISYMMETRY = FALSE",
-            "PHYSICAL_MODEL = LEE",
+            (f"PHYSICAL_MODEL = LEE_SCALAR, NUMBER_SCALAR = {self.num_scalars}" if self.num_scalars
+             else "PHYSICAL_MODEL = LEE"),
             "FLUID_MODEL = IDEAL_GAS_CALORIC",
-            f"SIMULATION = {self.simulation}",
+            # the reference takes LEE_SCALAR only with CASE_LINEAR_NOZZLE (src/core/input.cpp:596-606);
+            # its initial and mean states are replaced by the restart and base-state files
+            f"SIMULATION = {'CASE_LINEAR_NOZZLE' if self.num_scalars else self.simulation}",
             f"GAMMA_SPECIFICHEAT = {self.gamma!r}",
             f"FIX_DT_OR_CFL = {fix}",
             f"DT = {dt!r}" if dt is not None else "DT = 1.0E-6",
@@ -255,8 +266,13 @@ class Case:
         os.makedirs(workdir, exist_ok=True)
         grid, mean, ic, bc = (os.path.join(workdir, n) for n in ("grid.xyz", "mean.q", "ic.q", "bc.in"))
         plot3d.write_grid(grid, [(b.x, b.y, b.z) for b in self.blocks])
-        plot3d.write_function(mean, [b.mean for b in self.blocks])
-        plot3d.write_solution(ic, [b.state for b in self.blocks], step=step, time=time)
+        if self.num_scalars:
+            plot3d.write_function(mean, [np.concatenate([b.mean, b.zmean]) for b in self.blocks])
+            plot3d.write_solution(ic, [np.concatenate([b.state, b.zstate]) for b in self.blocks], step=step,
+                                  time=time)
+        else:
+            plot3d.write_function(mean, [b.mean for b in self.blocks])
+            plot3d.write_solution(ic, [b.state for b in self.blocks], step=step, time=time)
         plot3d.write_bc(bc, [bd.line() for bd in self.boundaries])
         if self.overset is not None:
             self.overset.write(os.path.join(workdir, "overset.bin"))
@@ -861,3 +877,38 @@ def _hole_ijk(hole: np.ndarray) -> np.ndarray:
     kk, jj, ii = np.nonzero(hole)
     order = np.lexsort((ii, jj, kk))
     return np.stack([ii[order], jj[order], kk[order]], axis=1).astype(np.int32)
+
+
+def with_scalars(case: Case, n: int = 2, seed: int = 21, amplitude: float = 1e-2) -> Case:
+    """``case`` with ``n`` passive scalars (PHYSICAL_MODEL = LEE_SCALAR): on every block mean
+    fields Z_bar_k = 1 + 0.5 tanh((x cos a_k + y sin a_k) / L) with seed-drawn directions a_k
+    (L a quarter of the domain's extent, so that grad Z_bar is non-zero and varies), and Gaussian
+    blobs Z_k' of ``amplitude`` at seed-drawn centres, zero in holes. The reference runs
+    LEE_SCALAR under SIMULATION = CASE_LINEAR_NOZZLE, whose branch of
+    source::apply_physicalSource adds nothing, so the case's monopole is dropped."""
+    if case.simulation != "CASE_KBK_COMBUSTOR":
+        raise ValueError("LEE_SCALAR runs under CASE_LINEAR_NOZZLE: the case's own source would be lost")
+    case.monopole = None
+    rng = np.random.default_rng(seed)
+    xs = np.concatenate([b.x.ravel() for b in case.blocks])
+    ys = np.concatenate([b.y.ravel() for b in case.blocks])
+    zs = np.concatenate([b.z.ravel() for b in case.blocks])
+    ext = max(np.ptp(xs), np.ptp(ys), 1e-12)
+    L = 0.25 * ext
+    ang = rng.uniform(0.0, 2.0 * math.pi, size=n)
+    centres = [(rng.uniform(xs.min(), xs.max()), rng.uniform(ys.min(), ys.max()), rng.uniform(zs.min(), zs.max()))
+               for _ in range(n)]
+    hw = 0.15 * ext
+    for blk in case.blocks:
+        zm = np.empty((n,) + blk.x.shape)
+        zq = np.empty((n,) + blk.x.shape)
+        for k in range(n):
+            zm[k] = 1.0 + 0.5 * np.tanh((blk.x * math.cos(ang[k]) + blk.y * math.sin(ang[k])) / L)
+            cx, cy, cz = centres[k]
+            r2 = (blk.x - cx) ** 2 + (blk.y - cy) ** 2 + (case.num_dim == 3) * (blk.z - cz) ** 2
+            zq[k] = amplitude * _gauss(r2, hw)
+        if blk.iblank is not None:
+            zq[:, blk.iblank == 1] = 0.0
+        blk.zmean, blk.zstate = zm, zq
+    case.name += f"_scalars{n}"
+    return case

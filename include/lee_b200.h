@@ -209,6 +209,20 @@ int lee_upload_state(lee_ctx *ctx, int b, const double *const sol[5], int step, 
 /* Current state of block b (State::sol, src/core/state.h:39). */
 int lee_download_state(lee_ctx *ctx, int b, double *const sol[5], int *step, double *time);
 
+/* Passive scalars (PHYSICAL_MODEL = LEE_SCALAR with NUMBER_SCALAR = n, src/core/input.cpp:113-119,
+ * :768-773): n state slots Z_k' after p', with mean fields Z_bar_k, advanced by
+ * dZ'/dt = -u_bar . grad Z' - u' . grad Z_bar (compute_RHS_linearized_Euler_scalar,
+ * src/solver/spatial_discretization.cpp:2134-2158) plus the sponges (relaxing to zero); they
+ * take the Neumann rows of every Neumann, slip-wall and centerline BC line, zero on Dirichlet
+ * lines, and go through the overset interpolation, the filter and the hole mask with the other
+ * slots. lee_set_scalars (0 <= n <= 8) comes before lee_set_block; the mean scalars before
+ * lee_prepare; the state slots after it. Pointers: n fields of the block's points each. The
+ * adjoint and the batched kernels do not take scalars. */
+int lee_set_scalars(lee_ctx *ctx, int n);
+int lee_set_mean_scalars(lee_ctx *ctx, int b, const double *const *zbar);
+int lee_upload_scalars(lee_ctx *ctx, int b, const double *const *z);
+int lee_download_scalars(lee_ctx *ctx, int b, double *const *z);
+
 /* Time step for a target CFL (temporal::compute_CFL, src/solver/temporal_discretization.cpp:397-450),
  * including the reference's truncation of the convective term to an int (abs(double) resolving to
  * int abs(int) at :425): the first FIX_CFL step of solver::solve (src/solver/solver.cpp:54-64),

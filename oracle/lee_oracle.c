@@ -31,6 +31,8 @@
 #define INTERPOLATED (-1)
 #define MAXB 8
 #define MAXBND 64
+#define MAXSC 8          /* passive scalars (PHYSICAL_MODEL = LEE_SCALAR) */
+#define MAXV (5 + MAXSC) /* state slots: s', u', v', w', p', then the scalars Z_k' */
 
 /* One directional operator: interior stencil c[l+h] for l = -h..h, boundary rows
  * B[row][s] for row < nb, s < S, and the right-boundary sign (-1 for the
@@ -55,10 +57,10 @@ typedef struct {
   double *met[9];  /* metrics[l][i] at l*3+i */
   double *minv[9]; /* metricsInverse[i][l] at i*3+l */
   double *jac, *invjac;
-  double *mean[5];
-  double *grad[15]; /* d mean_v / dx_j at v*ndim + j */
+  double *mean[MAXV];
+  double *grad[3 * MAXV]; /* d mean_v / dx_j at v*ndim + j */
   double *aux[4];   /* rho', rho_bar, T', T_bar (IAUX_*, src/core/param.h:77-80) */
-  double *sol[5];
+  double *sol[MAXV];
   int nbnd;
   bnd_t bnd[MAXBND];
 } blk_t;
@@ -73,12 +75,13 @@ typedef struct {
   long long *rl, *dl;
   int w[3], W;
   double *wt;
-  double *buf; /* n x 5 interpolants */
+  double *buf; /* n x MAXV interpolants */
 } ovs_t;
 
 struct orc_ctx {
   lee_config cfg;
   op_t fd, flt;
+  int nsc, nv; /* passive scalars (UserInput::num_scalar, src/core/input.cpp:113-119) and state slots */
   int nblk;
   blk_t blk[MAXB];
   int src_kind;
@@ -530,7 +533,7 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
   double **scr = scratch(c, (size_t)N);
   double *df = scr[0], *work = scr[1], *sum = scr[2];
   int rc = 0;
-  for (int v = 0; v < 5; ++v) memset(rhs[v], 0, sizeof(double) * (size_t)N);
+  for (int v = 0; v < c->nv; ++v) memset(rhs[v], 0, sizeof(double) * (size_t)N);
   for (int j = 0; j < nd && !rc; ++j) { /* entropy */
     rc = d_x(c, bk, y[0], df, j, work, sum);
     PAR_FOR
@@ -569,6 +572,18 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
     PAR_FOR
     for (int p = 0; p < N; ++p)
       rhs[4][p] -= g * (bk->mean[4][p] * y[2][p] + y[4][p] * bk->mean[2][p]) / (bk->xyz[1][p] + 1e-99);
+  /* compute_RHS_linearized_Euler_scalar (:2134-2158): dZ'/dt = -u_bar . grad Z' - u' . grad Z_bar */
+  for (int k = 0; k < c->nsc && !rc; ++k) {
+    int v = 5 + k;
+    for (int j = 0; j < nd && !rc; ++j) {
+      rc = d_x(c, bk, y[v], df, j, work, sum);
+      PAR_FOR
+      for (int p = 0; p < N; ++p) rhs[v][p] -= bk->mean[1 + j][p] * df[p];
+      PAR_FOR
+      for (int p = 0; p < N; ++p) rhs[v][p] -= y[1 + j][p] * bk->grad[v * nd + j][p];
+    }
+  }
+  if (rc) return rc;
   if (c->src_kind == LEE_SOURCE_DISTRIBUTED && bk == &c->blk[(int)c->dsrc[0]] && c->dsrc_g) {
     double fac = (g - 1.0) * sin(c->dsrc[1] * time);
     PAR_FOR
@@ -622,9 +637,9 @@ static int rhs_block(orc_ctx *c, blk_t *bk, double *const *y, double **rhs, doub
           int lb = (i - z->lo[0]) + bn0 * ((j - z->lo[1]) + bn1 * (k - z->lo[2]));
           int l0 = i + bk->nx * (j + bk->ny * k);
           double sg = z->sigma[lb];
-          double ref[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+          double ref[MAXV] = {0.0};
           if (wave && !(bk->iblank && bk->iblank[l0] == BLANKED)) wave_at(c, bk, l0, time, ref);
-          for (int v = 0; v < 5; ++v) {
+          for (int v = 0; v < c->nv; ++v) { /* the scalars relax to zero (sol_ref, src/core/state.cpp:361-363) */
             double relax = -sg * (y[v][l0] - ref[v]);
             rhs[v][l0] += relax;
           }
@@ -652,14 +667,17 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y, double time) {
     int sd = st[z->dir];
     int nbx = hi[0] - lo[0] + 1, nby = hi[1] - lo[1] + 1, nbz = hi[2] - lo[2] + 1;
     int nbp = nbx * nby * nbz;
-    double *data[5];
-    for (int v = 0; v < 5; ++v) data[v] = dalloc((size_t)nbp);
-    int vars_neu[5], nneu = 0;
+    int nv = c->nv;
+    double *data[MAXV];
+    for (int v = 0; v < nv; ++v) data[v] = dalloc((size_t)nbp);
+    int vars_neu[MAXV], nneu = 0;
     if (z->kind == LEE_BC_NEUMANN || centerline) {
-      for (int v = 0; v < 5; ++v) vars_neu[nneu++] = v;
+      for (int v = 0; v < nv; ++v) vars_neu[nneu++] = v;
     } else if (z->kind == LEE_BC_WALL_SLIP_KINEMATIC) {
+      /* every non-velocity slot, the scalars included (:122-133) */
       vars_neu[nneu++] = 0;
       vars_neu[nneu++] = 4;
+      for (int v = 5; v < nv; ++v) vars_neu[nneu++] = v;
     }
     for (int k = lo[2]; k <= hi[2]; ++k)
       for (int j = lo[1]; j <= hi[1]; ++j)
@@ -668,7 +686,7 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y, double time) {
           int l0 = i + bk->nx * (j + bk->ny * k);
           int hole = bk->iblank && bk->iblank[l0] == BLANKED;
           if (dirichlet) {
-            for (int v = 0; v < 5; ++v) data[v][lb] = 0.0;
+            for (int v = 0; v < nv; ++v) data[v][lb] = 0.0;
             if (z->kind == LEE_BC_DIRICHLET_HARMONICWAVE && !hole) {
               double w[5];
               wave_at(c, bk, l0, time, w);
@@ -714,9 +732,9 @@ static void apply_bc(orc_ctx *c, blk_t *bk, double **y, double time) {
           int lb = (i - lo[0]) + nbx * ((j - lo[1]) + nby * (k - lo[2]));
           int l0 = i + bk->nx * (j + bk->ny * k);
           if (bk->iblank && bk->iblank[l0] == BLANKED) continue;
-          for (int v = 0; v < 5; ++v) y[v][l0] = data[v][lb];
+          for (int v = 0; v < nv; ++v) y[v][l0] = data[v][lb];
         }
-    for (int v = 0; v < 5; ++v) free(data[v]);
+    for (int v = 0; v < nv; ++v) free(data[v]);
   }
 }
 
@@ -725,7 +743,7 @@ static int filter_block(orc_ctx *c, blk_t *bk, double **y) {
   int N = bk->N, n[3] = {bk->nx, bk->ny, bk->nz};
   double *func0 = dalloc((size_t)N), *func = dalloc((size_t)N), *out = dalloc((size_t)N);
   double blend = c->cfg.filter_blend, rem = 1.0 - blend;
-  for (int v = 0; v < 5; ++v) {
+  for (int v = 0; v < c->nv; ++v) {
     memcpy(func0, y[v], sizeof(double) * (size_t)N);
     memcpy(func, func0, sizeof(double) * (size_t)N);
     for (int d = 0; d < c->cfg.num_dim; ++d) {
@@ -751,20 +769,20 @@ static void interpolate(orc_ctx *c, double **y[MAXB]) {
   ovs_t *o = &c->ovs;
   for (int r = 0; r < o->n; ++r) {
     blk_t *dk = &c->blk[o->db[r]];
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double acc[MAXV] = {0.0};
     const double *cf = o->wt + (size_t)r * o->W;
     int st = 0;
     for (int w3 = 0; w3 < o->w[2]; ++w3)
       for (int w2 = 0; w2 < o->w[1]; ++w2)
         for (int w1 = 0; w1 < o->w[0]; ++w1) {
           long long l1 = o->dl[r] + (w1 + w2 * dk->nx + (long long)w3 * dk->nx * dk->ny);
-          for (int v = 0; v < 5; ++v) acc[v] += cf[st] * y[o->db[r]][v][l1];
+          for (int v = 0; v < c->nv; ++v) acc[v] += cf[st] * y[o->db[r]][v][l1];
           st++;
         }
-    for (int v = 0; v < 5; ++v) o->buf[(size_t)r * 5 + v] = acc[v];
+    for (int v = 0; v < c->nv; ++v) o->buf[(size_t)r * MAXV + v] = acc[v];
   }
   for (int r = 0; r < o->n; ++r)
-    for (int v = 0; v < 5; ++v) y[o->rb[r]][v][o->rl[r]] = o->buf[(size_t)r * 5 + v];
+    for (int v = 0; v < c->nv; ++v) y[o->rb[r]][v][o->rl[r]] = o->buf[(size_t)r * MAXV + v];
 }
 
 /* ---------------------------------------------------------------------------
@@ -787,6 +805,7 @@ int orc_create(const lee_config *cfg, orc_ctx **out) {
     }
   }
   c->nblk = cfg->num_blocks;
+  c->nv = 5;
   *out = c;
   return LEE_OK;
 }
@@ -799,8 +818,8 @@ void orc_destroy(orc_ctx *c) {
     free(bk->iblank);
     for (int q = 0; q < 9; ++q) { free(bk->met[q]); free(bk->minv[q]); }
     free(bk->jac); free(bk->invjac);
-    for (int q = 0; q < 5; ++q) { free(bk->mean[q]); free(bk->sol[q]); }
-    for (int q = 0; q < 15; ++q) free(bk->grad[q]);
+    for (int q = 0; q < MAXV; ++q) { free(bk->mean[q]); free(bk->sol[q]); }
+    for (int q = 0; q < 3 * MAXV; ++q) free(bk->grad[q]);
     for (int q = 0; q < 4; ++q) free(bk->aux[q]);
     for (int q = 0; q < bk->nbnd; ++q) free(bk->bnd[q].sigma);
   }
@@ -827,7 +846,7 @@ int orc_set_block(orc_ctx *c, int b, int nx, int ny, int nz, const double *x, co
     bk->iblank = (int *)malloc(sizeof(int) * (size_t)bk->N);
     memcpy(bk->iblank, iblank, sizeof(int) * (size_t)bk->N);
   }
-  for (int q = 0; q < 5; ++q) { bk->mean[q] = dalloc((size_t)bk->N); bk->sol[q] = dalloc((size_t)bk->N); }
+  for (int q = 0; q < c->nv; ++q) { bk->mean[q] = dalloc((size_t)bk->N); bk->sol[q] = dalloc((size_t)bk->N); }
   for (int q = 0; q < 4; ++q) bk->aux[q] = dalloc((size_t)bk->N);
   bk->set = 1;
   return LEE_OK;
@@ -986,7 +1005,7 @@ int orc_set_overset(orc_ctx *c, int n, const int *recv_block, const int *recv_ij
   o->rl = (long long *)malloc(sizeof(long long) * (size_t)(n ? n : 1));
   o->dl = (long long *)malloc(sizeof(long long) * (size_t)(n ? n : 1));
   o->wt = dalloc((size_t)n * (size_t)W);
-  o->buf = dalloc((size_t)n * 5);
+  o->buf = dalloc((size_t)n * MAXV);
   for (int d = 0; d < 3; ++d) o->w[d] = width[d];
   o->W = W;
   for (int q = 0; q < num_holes; ++q) {
@@ -1119,7 +1138,7 @@ int orc_prepare(orc_ctx *c) {
     /* mean gradients: spatial::precompute_something (:2250-2271), with hole closures */
     int nd = c->cfg.num_dim;
     double *work = dalloc((size_t)bk->N), *sum = dalloc((size_t)bk->N);
-    for (int v = 0; v < 5; ++v)
+    for (int v = 0; v < c->nv; ++v)
       for (int j = 0; j < nd; ++j) {
         bk->grad[v * nd + j] = dalloc((size_t)bk->N);
         rc = d_x(c, bk, bk->mean[v], bk->grad[v * nd + j], j, work, sum);
@@ -1150,6 +1169,38 @@ int orc_download_state(orc_ctx *c, int b, double *const sol[5], int *step, doubl
   for (int q = 0; q < 5; ++q) memcpy(sol[q], bk->sol[q], sizeof(double) * (size_t)bk->N);
   if (step) *step = c->step;
   if (time) *time = c->time;
+  return LEE_OK;
+}
+
+/* Passive scalars: n slots Z_k' after p' (PHYSICAL_MODEL = LEE_SCALAR, NUMBER_SCALAR = n;
+ * src/core/input.cpp:113-119, :768-773), before any block is set. */
+int orc_set_scalars(orc_ctx *c, int n) {
+  if (n < 0 || n > MAXSC) return fail(c, LEE_ERR_ARG, "0 <= n <= %d scalars", MAXSC);
+  for (int b = 0; b < c->nblk; ++b)
+    if (c->blk[b].set) return fail(c, LEE_ERR_STATE, "lee_set_scalars before lee_set_block");
+  c->nsc = n;
+  c->nv = 5 + n;
+  return LEE_OK;
+}
+
+int orc_set_mean_scalars(orc_ctx *c, int b, const double *const *zbar) {
+  if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_STATE, "set_block first");
+  if (!c->nsc || !zbar) return fail(c, LEE_ERR_ARG, "no scalars");
+  for (int k = 0; k < c->nsc; ++k) memcpy(c->blk[b].mean[5 + k], zbar[k], sizeof(double) * (size_t)c->blk[b].N);
+  return LEE_OK;
+}
+
+int orc_upload_scalars(orc_ctx *c, int b, const double *const *z) {
+  if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_STATE, "set_block first");
+  if (!c->nsc || !z) return fail(c, LEE_ERR_ARG, "no scalars");
+  for (int k = 0; k < c->nsc; ++k) memcpy(c->blk[b].sol[5 + k], z[k], sizeof(double) * (size_t)c->blk[b].N);
+  return LEE_OK;
+}
+
+int orc_download_scalars(orc_ctx *c, int b, double *const *z) {
+  if (b < 0 || b >= c->nblk || !c->blk[b].set) return fail(c, LEE_ERR_STATE, "set_block first");
+  if (!c->nsc || !z) return fail(c, LEE_ERR_ARG, "no scalars");
+  for (int k = 0; k < c->nsc; ++k) memcpy(z[k], c->blk[b].sol[5 + k], sizeof(double) * (size_t)c->blk[b].N);
   return LEE_OK;
 }
 
@@ -1251,9 +1302,10 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
     return fail(c, LEE_ERR_UNSUPPORTED, "rk scheme");
   }
   int nb = c->nblk;
-  double *yn[MAXB][5], *ynext[MAXB][5], *zi[MAXB][5], *rhs[MAXB][5];
+  int nv = c->nv;
+  double *yn[MAXB][MAXV], *ynext[MAXB][MAXV], *zi[MAXB][MAXV], *rhs[MAXB][MAXV];
   for (int b = 0; b < nb; ++b)
-    for (int v = 0; v < 5; ++v) {
+    for (int v = 0; v < nv; ++v) {
       size_t N = (size_t)c->blk[b].N;
       yn[b][v] = dalloc(N); ynext[b][v] = dalloc(N); zi[b][v] = dalloc(N); rhs[b][v] = dalloc(N);
     }
@@ -1263,7 +1315,7 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
     c->step += 1;
     double tn = c->time, h = dt;
     for (int b = 0; b < nb; ++b)
-      for (int v = 0; v < 5; ++v) {
+      for (int v = 0; v < nv; ++v) {
         size_t N = (size_t)c->blk[b].N;
         memcpy(yn[b][v], c->blk[b].sol[v], N * sizeof(double));
         memcpy(ynext[b][v], yn[b][v], N * sizeof(double));
@@ -1276,13 +1328,13 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
         PAR_FOR
         for (int p = 0; p < bk->N; ++p) {
           if (!(bk->iblank && bk->iblank[p] == BLANKED)) {
-            for (int v = 0; v < 5; ++v) {
+            for (int v = 0; v < nv; ++v) {
               rhs[b][v][p] *= h;
               ynext[b][v][p] += bi[s] * rhs[b][v][p];
               if (s < ns - 1) zi[b][v][p] = yn[b][v][p] + aij[s] * rhs[b][v][p];
             }
           } else {
-            for (int v = 0; v < 5; ++v) {
+            for (int v = 0; v < nv; ++v) {
               rhs[b][v][p] = 0.0;
               ynext[b][v][p] = 0.0;
               zi[b][v][p] = 0.0;
@@ -1306,14 +1358,14 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
       if (c->cfg.filter_scheme != LEE_FILTER_NONE) rc = filter_block(c, bk, ynext[b]);
       for (int p = 0; p < bk->N; ++p) /* temporal::iblank_correction (:380-393) */
         if (bk->iblank && bk->iblank[p] == BLANKED)
-          for (int v = 0; v < 5; ++v) ynext[b][v][p] = 0.0;
-      for (int v = 0; v < 5; ++v) memcpy(bk->sol[v], ynext[b][v], sizeof(double) * (size_t)bk->N);
+          for (int v = 0; v < nv; ++v) ynext[b][v][p] = 0.0;
+      for (int v = 0; v < nv; ++v) memcpy(bk->sol[v], ynext[b][v], sizeof(double) * (size_t)bk->N);
     }
     /* the non-finite sentinel of lee_set_finite_check (the reference has none) */
     int last = it == nsteps - 1;
     if (!rc && c->finite_every >= 0 && (last || (c->finite_every > 0 && (it + 1) % c->finite_every == 0)))
       for (int b = 0; b < nb && !rc; ++b)
-        for (int v = 0; v < 5 && !rc; ++v)
+        for (int v = 0; v < nv && !rc; ++v)
           for (int p = 0; p < c->blk[b].N; ++p)
             if (!isfinite(c->blk[b].sol[v][p])) {
               rc = fail(c, LEE_ERR_NONFINITE, "the state holds a non-finite value after step %d", c->step);
@@ -1321,16 +1373,19 @@ int orc_advance(orc_ctx *c, int nsteps, double dt) {
             }
   }
   for (int b = 0; b < nb; ++b)
-    for (int v = 0; v < 5; ++v) { free(yn[b][v]); free(ynext[b][v]); free(zi[b][v]); free(rhs[b][v]); }
+    for (int v = 0; v < nv; ++v) { free(yn[b][v]); free(ynext[b][v]); free(zi[b][v]); free(rhs[b][v]); }
   return rc;
 }
 
 int orc_eval_rhs(orc_ctx *c, int b, double time, double *const rhs[5]) {
   if (!c->prepared) return fail(c, LEE_ERR_STATE, "prepare first");
   blk_t *bk = &c->blk[b];
-  double *r[5];
+  double *r[MAXV];
   for (int v = 0; v < 5; ++v) r[v] = rhs[v];
-  return rhs_block(c, bk, bk->sol, r, time);
+  for (int v = 5; v < c->nv; ++v) r[v] = dalloc((size_t)bk->N); /* the scalars' right-hand sides are dropped */
+  int rc = rhs_block(c, bk, bk->sol, r, time);
+  for (int v = 5; v < c->nv; ++v) free(r[v]);
+  return rc;
 }
 
 int orc_apply_filter(orc_ctx *c) {

@@ -45,6 +45,10 @@ WORKLOADS = {
     "jet3d_14": lambda: cases.jet3d(n=14, nsteps=4),
     # axisymmetric round jet: the 1/r pressure term, the axis centerline, a sheared mean
     "axisym2d_48x32": lambda: cases.axisym2d(nx=48, nr=32, nsteps=20),
+    # PHYSICAL_MODEL = LEE_SCALAR: two passive scalars on the shear layer (slip wall, Neumann,
+    # sponges, non-uniform mean) and one on the 3-D wall block
+    "scalar2d_40x32": lambda: cases.with_scalars(cases.shear2d(nx=40, ny=32, nsteps=20), n=2),
+    "scalar3d_14": lambda: cases.with_scalars(cases.wall3d(n=14, nsteps=4), n=1, seed=22),
 }
 
 # Two-block overset workloads (run on one reference rank per block).
@@ -58,12 +62,17 @@ OVERSET_WORKLOADS = {
     # after a hole; holes at line starts and ends) along every direction, in 2-D and 3-D
     "holes2d": lambda: cases.holes(2, nsteps=12),
     "holes3d": lambda: cases.holes(3, nsteps=8),
+    # two passive scalars through the cylinder layout's hole cut, fringes and seam
+    "scalar_cylinder2d_64": lambda: cases.with_scalars(
+        cases.cylinder2d(nb=64, length=16.0, ntheta=72, nr=24, r_out=3.0, first_cell=0.05, r_cut=1.0, sponge=4,
+                         nsteps=40, pulse=(1.8, 0.6, 1e-3, 0.5)), n=2, seed=23),
 }
 
 
 def make(name: str) -> str:
     case = WORKLOADS[name]()
     nd = case.num_dim
+    nv = 5 + case.num_scalars
     setup = run_ref.assemble(case, run_ref.run(case, mode="setup")["ranks"])[0]
     rhs = run_ref.assemble(case, run_ref.run(case, mode="rhs")["ranks"])[0]
     filt = run_ref.assemble(case, run_ref.run(case, mode="filter")["ranks"])[0]
@@ -74,8 +83,8 @@ def make(name: str) -> str:
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(
         out,
-        metrics=setup[0:9], jacobian=setup[9], mean_gradient=setup[12:12 + 5 * nd],
-        sponge=setup[12 + 5 * nd + 4], rhs=rhs, filter=filt, dt=np.float64(dt),
+        metrics=setup[0:9], jacobian=setup[9], mean_gradient=setup[12:12 + nv * nd],
+        sponge=setup[12 + nv * nd + 4], rhs=rhs, filter=filt, dt=np.float64(dt),
         step1=step1, stepn=stepn, nsteps=np.int64(case.nsteps))
     return out
 

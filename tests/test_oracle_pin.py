@@ -189,3 +189,51 @@ def test_hole_layouts_exercise_every_closure_branch(name):
             "receiver after hole", "hole at line start", "hole at line end"}
     for axis in range(3 - nd, 3):
         assert _transitions(ib, axis) == want, (name, axis, want - _transitions(ib, axis))
+
+
+# ---- passive scalars (PHYSICAL_MODEL = LEE_SCALAR) ------------------------------------------
+
+SCALAR_NAMES = ["scalar2d_40x32", "scalar3d_14"]
+
+
+def full_state(solver, b):
+    """The 5 + n slots of block b: the LEE slots, then the passive scalars."""
+    return np.concatenate([solver.download(b)[0], solver.download_scalars(b)])
+
+
+@pytest.mark.parametrize("name", SCALAR_NAMES)
+def test_oracle_scalars_match_golden(oracle_lib, name):
+    """Two (2-D) and one (3-D) passive scalars through the slip wall, Neumann faces, sponges
+    and the sheared mean: the LEE slots' setup and right-hand side are unchanged by them, the
+    filter and every step match the reference on all 5 + n slots."""
+    g = load_golden(name)
+    case = golden_case(name)
+    nd = case.num_dim
+    s = api.Solver(oracle_lib, case)
+    np.testing.assert_array_equal(s.get_setup(0, api.SETUP_MEAN_GRADIENT), g["mean_gradient"][:5 * nd])
+    assert s.compute_dt() == float(g["dt"])
+    np.testing.assert_array_equal(s.eval_rhs(0, 0.0), g["rhs"][:5])
+    s.apply_filter()
+    np.testing.assert_array_equal(full_state(s, 0), g["filter"])
+    dt = float(g["dt"])
+    s = api.Solver(oracle_lib, case)
+    s.advance(1, dt)
+    np.testing.assert_array_equal(full_state(s, 0), g["step1"])
+    s.advance(int(g["nsteps"]) - 1, dt)
+    np.testing.assert_array_equal(full_state(s, 0), g["stepn"])
+
+
+def test_oracle_scalars_through_overset_match_golden(oracle_lib):
+    name = "scalar_cylinder2d_64"
+    g = load_golden(name)
+    case = overset_case(name)
+    s = api.Solver(oracle_lib, case)
+    check_overset_maps(s, g, case)
+    dt = float(g["dt"])
+    assert s.compute_dt() == dt
+    s.advance(1, dt)
+    for b in range(len(case.blocks)):
+        np.testing.assert_array_equal(full_state(s, b), g[f"step1_{b}"])
+    s.advance(int(g["nsteps"]) - 1, dt)
+    for b in range(len(case.blocks)):
+        np.testing.assert_array_equal(full_state(s, b), g[f"stepn_{b}"])
