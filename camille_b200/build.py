@@ -41,6 +41,7 @@ UNITS = {
     "lee_adjoint_tma.cu": [],
     "lee_adjoint_gen.cu": [],
     "lee_host_adjoint_gen.cu": [],
+    "lee_host_scalar.cu": [],
 }
 
 

@@ -92,6 +92,20 @@ struct BlockData {
   int tiles_x = 0, tiles_y = 0;
   int stage_chunk = 0, filter_chunk = 0;
   int filter_ry = 1;                  // rows per thread row of the scalar fused filter (1 or 2)
+  // passive scalars (LEE_SCALAR): mean fields and their gradients, and the slots' buffers with
+  // the LEE slots' roles (y, acc, two stage buffers, carried error, filter increments) plus a
+  // filter scratch; fixed roles, nothing swaps
+  std::vector<double> hzmean;         // n x N host copy
+  double* d_zmean[kMaxScalars] = {};
+  double* d_zgrad[kMaxScalars * 3] = {};
+  Coef<double> cd_gz[kMaxScalars][3];
+  Coef<float> cf_gz[kMaxScalars][3];
+  void* zy[kMaxScalars] = {};
+  void* zacc[kMaxScalars] = {};
+  void* zzb[2][kMaxScalars] = {};
+  void* zcomp[kMaxScalars] = {};
+  void* zdsum[kMaxScalars] = {};
+  void* zf[kMaxScalars] = {};
 };
 
 struct MapKey {
@@ -127,6 +141,7 @@ struct lee_ctx {
   Wave wave{};               // lee_set_harmonic_wave (type LEE_WAVE_NONE until set)
   bool wave_time = false;    // some BC line or sponge zone reads the wave (from lee_prepare)
   bool axisym = false;       // lee_set_axisymmetric
+  int nsc = 0;               // lee_set_scalars: passive scalar slots
   std::vector<double> dsrc;  // distributed source parameters (LEE_SOURCE_DISTRIBUTED)
   bool prepared = false, uploaded = false;
   int step = 0;
@@ -366,6 +381,17 @@ int advance_timed(lee_ctx* c, int nsteps, const std::vector<double>& dts);
 int adjoint_setup(lee_ctx* c);
 template <typename T>
 int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar);
+// passive scalars (lee_host_scalar.cu): setup at lee_prepare, and per stage s of ns the update,
+// BC rows and overset of the scalar slots (lee_zin: the LEE stage input, for u'), then the filter
+int scalar_setup(lee_ctx* c, BlockData& b);
+template <typename T>
+int scalar_stage(lee_ctx* c, BlockData& b, int s, int ns, double h, double bcoef, double acoef, void* const* lee_zin);
+template <typename T>
+int scalar_bcs(lee_ctx* c, BlockData& b, int s, int ns);
+template <typename T>
+int scalar_overset(lee_ctx* c, int s, int ns);
+template <typename T>
+int scalar_filter(lee_ctx* c, BlockData& b, int ns);
 // the general path (lee_host_adjoint_gen.cu)
 bool adjoint_fast_applies(lee_ctx* c, const char** why);
 int adjoint_gen_setup(lee_ctx* c);

@@ -74,6 +74,7 @@ bool build_transpose(const OpTable& op, TransOp* t) {
 int adjoint_setup(lee_ctx* c) {
   auto& a = c->adj;
   if (a.ready) return LEE_OK;
+  if (c->nsc) return fail(c, LEE_ERR_UNSUPPORTED, "the adjoint has no passive scalars");
   if (!adjoint_fast_applies(c, nullptr)) return adjoint_gen_setup(c);
   BlockData& b = c->blk[0];
   // the class-row transposes need rows within reach and lines that keep the two ends' class

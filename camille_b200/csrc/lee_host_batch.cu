@@ -20,7 +20,7 @@ bool closures_within_halo(const OpTable& op) {
 }
 
 bool batch_eligible(const lee_ctx* c) {
-  if (c->cfg.num_dim != 2 || c->ovs.n > 0 || c->axisym) return false;
+  if (c->cfg.num_dim != 2 || c->ovs.n > 0 || c->axisym || c->nsc > 0) return false;
   if (!(c->fd.h == 2 && c->fd.S == 3)) return false;
   if (c->cfg.filter_scheme != LEE_FILTER_STANDARD_CENTRAL || c->cfg.filter_order != 8) return false;
   if (!(c->flt.h == 4 && c->flt.S == 7 && c->fltd.h == 4 && c->fltd.S == 7)) return false;

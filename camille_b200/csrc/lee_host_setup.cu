@@ -364,6 +364,7 @@ int lee_prepare(lee_ctx* c) {
     for (int q = 0; q < 9; ++q) b.need_rho |= c->comp ? !b.cf_gu[q].zero : !b.cd_gu[q].zero;
     if (b.need_rho && (rc = dev_alloc(c, &b.rho, (size_t)b.N * c->esz))) return rc;
     b.rho_valid = false;
+    if ((rc = scalar_setup(c, b))) return rc;
     // state buffers
     if ((rc = alloc_fields(c, b.y, b.N))) return rc;
     if ((rc = alloc_fields(c, b.acc, b.N))) return rc;

@@ -119,11 +119,17 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         span(c, 0, e0, e1);
         c->stats.stage_launches += 1;
         c->stats.kernel_launches += 1;
+        // the passive scalars' stage reads u' of this stage's input
+        if ((rc = scalar_stage<T>(c, b, s, ns, dt, bi[s], aij[s], zin))) {
+          c->stream = origin;
+          return rc;
+        }
         // boundary update of the stage output (spatial::update_boundary): z, or y_next after the
         // last stage (FP64: the accumulator; compensated: the pair y_pre, e); BC lines touch their
         // own block only
         rc = apply_bcs<T>(c, b, target(b), errors(b), b.time + ci[sb] * dts[bix],
                           t_tab ? t_tab + bix * ns + sb : nullptr, ctr, nbk * ns);
+        if (!rc) rc = scalar_bcs<T>(c, b, s, ns);
         c->stream = origin;
         if (rc) return rc;
       }
@@ -153,6 +159,8 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         }
         CK(launch_overset<T>(op, c->stream));
         c->stats.kernel_launches += op.fused ? 1 : 2;
+        int rc = scalar_overset<T>(c, s, ns);
+        if (rc) return rc;
       }
       for (auto& b : c->blk) {
         void** tgt = target(b);
@@ -208,7 +216,9 @@ int step_impl(lee_ctx* c, const std::vector<double>& dts, const T* amp_tab, cons
         swap_fields(c->V, b.y, last_out);
         swap_fields(c->V, b.comp, b.acc);
       }
+      int rc = scalar_filter<T>(c, b, ns);
       c->stream = origin;
+      if (rc) return rc;
     }
     if (conc) {
       int rc = join_sides(c);
@@ -599,6 +609,18 @@ int lee_apply_filter(lee_ctx* c) {
         CK(launch_rho<double>(b.N, c->V, (double* const*)b.y, nullptr, b.d_mean[4], c->cfg.gamma, (double*)b.rho,
                               c->stream));
       b.rho_valid = true;
+    }
+    if (c->nsc) {
+      // the scalar slots: y (and its carried error) take the pre-filter roles, then the filter
+      const int ns = tableau(c->cfg.rk_scheme).ns;
+      const size_t bytes = (size_t)b.N * c->esz;
+      for (int k = 0; k < c->nsc; ++k) {
+        CK(cudaMemcpyAsync(c->comp ? b.zzb[(ns - 1) % 2][k] : b.zacc[k], b.zy[k], bytes, cudaMemcpyDeviceToDevice,
+                           c->stream));
+        if (c->comp) CK(cudaMemcpyAsync(b.zacc[k], b.zcomp[k], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      }
+      int rc = c->comp ? scalar_filter<float>(c, b, ns) : scalar_filter<double>(c, b, ns);
+      if (rc) return rc;
     }
     if (b.tma_filter) {
       // y (and its carried error) -> zb[0], then the buffers swap roles

@@ -12,6 +12,7 @@ namespace lee {
 
 constexpr int kMaxZones = 8;  // sponge zones per block read by the stage kernel
 constexpr int kMaxVars = 5;   // s', u'(1..num_dim), p'
+constexpr int kMaxScalars = 8;  // passive scalars Z_k' (PHYSICAL_MODEL = LEE_SCALAR)
 
 // Compile-time traits of a block's coefficient layout, chosen at setup (stage kernels):
 constexpr int kTrJmField = 1;  // J*metrics vary over the block (else kernel constants)
@@ -294,6 +295,33 @@ cudaError_t launch_trace(int n, const long long* l0, const T* p, const T* e, dou
 template <typename T>
 cudaError_t launch_mic_force(int n, const long long* l0, T* lam_p, const double* trace, int row, double scale,
                              cudaStream_t s);
+
+// ---- passive scalars (lee_scalar.cu) -------------------------------------------------------
+// One RK stage of the n scalar slots of a block: dZ'/dt = -u_bar . grad Z' - u' . grad Z_bar
+// minus the sponges, with the stage update of the LEE slots (hole bypass, FP64 or compensated).
+// u' is the LEE stage input at the point.
+template <typename T>
+struct ScalarParams {
+  int nx, ny, nz, dim, n;
+  int stage, last;
+  T h, b, a;
+  const T* zin[kMaxScalars];
+  const T* yn[kMaxScalars];
+  T* acc[kMaxScalars];
+  T* zout[kMaxScalars];
+  T* comp[kMaxScalars];
+  const T* uin[3];
+  Coef<T> jm[9], ubar[3];
+  Coef<T> gz[kMaxScalars][3];   // d Z_bar_k / dx_j
+  int nzones;
+  Zone<T> zones[kMaxZones];
+  const int8_t* code[3];
+  const int* iblank;
+  OpTable fd;
+};
+
+template <typename T>
+cudaError_t launch_scalar_stage(const ScalarParams<T>& p, int comp, cudaStream_t s);
 
 // ---- the general discrete adjoint (lee_adjoint_gen.cu) ------------------------------------
 // One transposed RK stage of one block: zbar = L^T w, w = scale * kin, with the forward stage's

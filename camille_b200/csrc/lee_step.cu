@@ -127,7 +127,96 @@ __global__ void k_hole_zero(long long n, int V, T* f0, T* f1, T* f2, T* f3, T* f
       for (int v = 0; v < V; ++v) f[v][l] = T(0);
 }
 
+// One RK stage of a block's passive scalars (compute_RHS_linearized_Euler_scalar,
+// src/solver/spatial_discretization.cpp:2134-2158): per direction x, r -= u_bar_x dZ/dx_x, then
+// r -= u'_x dZ_bar/dx_x; the sponges (relaxing to zero, src/solver/source.cpp:174-201); then the
+// stage update of the LEE slots (RungeKutta::integrate with the hole bypass).
+template <typename T, int DIM, bool COMP>
+__global__ void __launch_bounds__(256) k_scalar_stage(ScalarParams<T> p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= p.nx || j >= p.ny) return;
+  const long long nxy = (long long)p.nx * p.ny;
+  const long long l = i + (long long)p.nx * j + nxy * k;
+  const int pos[3] = {i, j, k};
+  const int nn[3] = {p.nx, p.ny, p.nz};
+  const long long sd[3] = {1, p.nx, nxy};
+  const bool first = p.stage == 0, last = p.last != 0;
+  const bool hole = p.iblank && p.iblank[l] == 1;
+  T jm[DIM][DIM], ub[DIM], u[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) jm[d][x] = p.jm[d * 3 + x].p ? __ldg(p.jm[d * 3 + x].p + l) : p.jm[d * 3 + x].c;
+#pragma unroll
+  for (int x = 0; x < DIM; ++x) {
+    ub[x] = p.ubar[x].p ? __ldg(p.ubar[x].p + l) : p.ubar[x].c;
+    u[x] = p.uin[x][l];
+  }
+  for (int q = 0; q < p.n; ++q) {
+    const T z = p.zin[q][l];
+    T r = T(0);
+    T D[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) D[d] = dop<T>(p.fd, p.zin[q], l, pos[d], nn[d], sd[d], p.code[d]);
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) {
+      T g = T(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) g += jm[d][x] * D[d];
+      r -= ub[x] * g;
+      const Coef<T>& gz = p.gz[q][x];
+      if (!gz.zero) r -= u[x] * (gz.p ? __ldg(gz.p + l) : gz.c);
+    }
+    for (int zi = 0; zi < p.nzones; ++zi) {
+      const Zone<T>& zn = p.zones[zi];
+      if (i < zn.lo[0] || i > zn.hi[0] || j < zn.lo[1] || j > zn.hi[1] || k < zn.lo[2] || k > zn.hi[2]) continue;
+      const int b0 = zn.hi[0] - zn.lo[0] + 1, b1 = zn.hi[1] - zn.lo[1] + 1;
+      const long long lb = (i - zn.lo[0]) + (long long)b0 * ((j - zn.lo[1]) + (long long)b1 * (k - zn.lo[2]));
+      r += -zn.sig[lb] * (z - T(0));
+    }
+    if (hole) {
+      p.acc[q][l] = T(0);
+      if (!last || COMP) p.zout[q][l] = T(0);
+      continue;
+    }
+    const T hk = r * p.h;
+    const T yv = first ? z : p.yn[q][l];
+    if (!COMP) {
+      const T prev = first ? z : p.acc[q][l];
+      p.acc[q][l] = prev + p.b * hk;
+      if (!last) p.zout[q][l] = yv + p.a * hk;
+    } else {
+      const T inc = (first ? p.comp[q][l] : p.acc[q][l]) + p.b * hk;
+      if (!last) {
+        p.acc[q][l] = inc;
+        p.zout[q][l] = yv + p.a * hk;
+      } else {
+        const T s = yv + inc;
+        const T bb = s - yv;
+        p.zout[q][l] = s;
+        p.acc[q][l] = (yv - (s - bb)) + (inc - bb);
+      }
+    }
+  }
+}
+
 }  // namespace
+
+template <typename T>
+cudaError_t launch_scalar_stage(const ScalarParams<T>& p, int comp, cudaStream_t s) {
+  dim3 blk(32, 8, 1);
+  dim3 grd((p.nx + 31) / 32, (p.ny + 7) / 8, p.nz);
+  if (p.dim == 2) {
+    if (comp) k_scalar_stage<T, 2, true><<<grd, blk, 0, s>>>(p);
+    else k_scalar_stage<T, 2, false><<<grd, blk, 0, s>>>(p);
+  } else {
+    if (comp) k_scalar_stage<T, 3, true><<<grd, blk, 0, s>>>(p);
+    else k_scalar_stage<T, 3, false><<<grd, blk, 0, s>>>(p);
+  }
+  return cudaGetLastError();
+}
 
 template <typename T>
 cudaError_t launch_stage(const StageParams<T>& p, int comp, cudaStream_t s) {
@@ -166,5 +255,7 @@ template cudaError_t launch_stage<double>(const StageParams<double>&, int, cudaS
 template cudaError_t launch_stage<float>(const StageParams<float>&, int, cudaStream_t);
 template cudaError_t launch_filter_pass<double>(const FilterParams<double>&, int, cudaStream_t);
 template cudaError_t launch_filter_pass<float>(const FilterParams<float>&, int, cudaStream_t);
+template cudaError_t launch_scalar_stage<double>(const ScalarParams<double>&, int, cudaStream_t);
+template cudaError_t launch_scalar_stage<float>(const ScalarParams<float>&, int, cudaStream_t);
 
 }  // namespace lee

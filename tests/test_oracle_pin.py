@@ -237,3 +237,11 @@ def test_oracle_scalars_through_overset_match_golden(oracle_lib):
     s.advance(int(g["nsteps"]) - 1, dt)
     for b in range(len(case.blocks)):
         np.testing.assert_array_equal(full_state(s, b), g[f"stepn_{b}"])
+
+
+def test_scalars_are_set_before_the_blocks(oracle_lib):
+    """lee_set_scalars after lee_set_block is refused (the slots are laid out with the block)."""
+    case = golden_case("pulse2d_48")
+    s = api.Solver(oracle_lib, case, prepare=False)
+    with pytest.raises(api.LeeError, match="before lee_set_block"):
+        s._chk(oracle_lib.set_scalars(s.ctx, 2))
