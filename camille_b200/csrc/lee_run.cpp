@@ -134,10 +134,14 @@ class Deck {
 // PLOT3D whole-multiblock files: int32 counts, float64 data, i fastest
 // ---------------------------------------------------------------------------------------------
 
+// state slots: the five LEE slots, then the passive scalars of LEE_SCALAR (at most eight)
+constexpr int kMaxSlots = 13;
+int g_nv = 5;
+
 struct Block {
   int n[3] = {1, 1, 1};
   long long N = 0;
-  std::vector<double> xyz[3], mean[5], sol[5];
+  std::vector<double> xyz[3], mean[kMaxSlots], sol[kMaxSlots];
 };
 
 void read_ints(std::ifstream& f, int* dst, size_t n, const std::string& what) {
@@ -183,10 +187,10 @@ void read_mean(const std::string& path, std::vector<Block>& blocks) {
   for (size_t b = 0; b < blocks.size(); ++b) {
     for (int d = 0; d < 3; ++d)
       if (dims[4 * b + (size_t)d] != blocks[b].n[d]) die("mean-flow file " + path + ": dimensions differ");
-    if (dims[4 * b + 3] != 5) die("mean-flow file " + path + ": five variables expected");
+    if (dims[4 * b + 3] != g_nv) die("mean-flow file " + path + ": " + std::to_string(g_nv) + " variables expected");
   }
   for (auto& k : blocks)
-    for (int v = 0; v < 5; ++v) {
+    for (int v = 0; v < g_nv; ++v) {
       k.mean[v].resize((size_t)k.N);
       read_doubles(f, k.mean[v].data(), (size_t)k.N, path);
     }
@@ -209,7 +213,7 @@ void read_solution(const std::string& path, std::vector<Block>& blocks, int* ste
     read_doubles(f, tau, 4, path);
     *step = (int)tau[2];
     *time = tau[3];
-    for (int v = 0; v < 5; ++v) {
+    for (int v = 0; v < g_nv; ++v) {
       k.sol[v].resize((size_t)k.N);
       read_doubles(f, k.sol[v].data(), (size_t)k.N, path);
     }
@@ -226,7 +230,7 @@ void write_solution(const std::string& path, const std::vector<Block>& blocks, i
   for (auto& k : blocks) {
     const double tau[4] = {0.0, 1.0, (double)step, time};
     f.write(reinterpret_cast<const char*>(tau), 32);
-    for (int v = 0; v < 5; ++v)
+    for (int v = 0; v < g_nv; ++v)
       f.write(reinterpret_cast<const char*>(k.sol[v].data()), (std::streamsize)(k.N * 8));
   }
   if (!f) die("short write to " + path);
@@ -315,11 +319,24 @@ struct Run {
   // HARMONIC_WAVE (type LEE_WAVE_NONE when the deck says NONE)
   int wave_type = LEE_WAVE_NONE, wave_form = -1, wave_dir = 0;
   double wave_amp = 0.0, wave_len = 0.0, wave_hw = 0.0;
+  int nsc = 0;  // PHYSICAL_MODEL = LEE_SCALAR: NUMBER_SCALAR
 };
 
 Run configure(const Deck& d, int precision) {
   Run r;
-  if (d.str("PHYSICAL_MODEL") != "LEE") die("PHYSICAL_MODEL " + d.str("PHYSICAL_MODEL") + ": the library runs LEE");
+  const std::string model = d.str("PHYSICAL_MODEL");
+  if (model == "LEE_SCALAR") {
+    // src/core/input.cpp:113-117, and check_consistency_simulation (:596-606): LEE_SCALAR runs the
+    // linear nozzle only
+    r.nsc = d.i("PHYSICAL_MODEL", "NUMBER_SCALAR");
+    if (!(r.nsc >= 1)) die("For PHYSICAL_MODEL = " + model + ", at least one scalar should be solved for.");
+    if (r.nsc > kMaxSlots - 5) die("NUMBER_SCALAR above " + std::to_string(kMaxSlots - 5));
+    if (d.str("SIMULATION") != "CASE_LINEAR_NOZZLE")
+      die("SIMULATION " + d.str("SIMULATION") + " is not implemented for PHYSICAL_MODEL = " + model + ".");
+  } else if (model != "LEE") {
+    die("PHYSICAL_MODEL " + model + ": the library runs LEE and LEE_SCALAR");
+  }
+  g_nv = 5 + r.nsc;
   std::string axisym = d.has("AXISYMMETRY") ? d.str("AXISYMMETRY") : "FALSE";
   for (auto& ch : axisym) ch = (char)std::toupper((unsigned char)ch);  // truefalse_2int (:786-799)
   if (axisym == "TRUE") {
@@ -469,6 +486,7 @@ void print_parse(const Run& r, const std::vector<Block>& blocks, const std::vect
   std::printf(", \"wave\": [%d, %d, %d, %.17g, %.17g, %.17g], \"axisym\": %s, \"jet2d\": %s", r.wave_type,
               r.wave_form, r.wave_dir, r.wave_amp, r.wave_len, r.wave_hw, r.axisym ? "true" : "false",
               r.jet2d ? "true" : "false");
+  std::printf(", \"scalars\": %d", r.nsc);
   std::printf(", \"bc\": [");
   for (size_t q = 0; q < bcs.size(); ++q)
     std::printf("%s[%d, %d, %d, %d, %d, %d, %d, %d, %d, %d]", q ? ", " : "", bcs[q].block, bcs[q].kind, bcs[q].dir,
@@ -516,12 +534,18 @@ int main(int argc, char** argv) {
 
   lee_ctx* c = nullptr;
   if (lee_create(&r.cfg, &c) != LEE_OK) die(std::string("lee_create: ") + lee_last_error(nullptr));
+  if (r.nsc) check(c, lee_set_scalars(c, r.nsc), "NUMBER_SCALAR");
   for (size_t b = 0; b < blocks.size(); ++b) {
     Block& k = blocks[b];
     check(c, lee_set_block(c, (int)b, k.n[0], k.n[1], k.n[2], k.xyz[0].data(), k.xyz[1].data(), k.xyz[2].data(), nullptr),
           "grid");
     const double* m[5] = {k.mean[0].data(), k.mean[1].data(), k.mean[2].data(), k.mean[3].data(), k.mean[4].data()};
     check(c, lee_set_mean(c, (int)b, m), "mean flow");
+    if (r.nsc) {
+      const double* zm[kMaxSlots];
+      for (int q = 0; q < r.nsc; ++q) zm[q] = k.mean[5 + q].data();
+      check(c, lee_set_mean_scalars(c, (int)b, zm), "mean scalars");
+    }
   }
   for (const BcLine& b : bcs) check(c, lee_add_boundary(c, b.block, b.kind, b.dir, b.end, b.lo, b.hi, nullptr), "BC file");
   bool wave_lines = false;
@@ -543,6 +567,11 @@ int main(int argc, char** argv) {
     const double* s[5] = {blocks[b].sol[0].data(), blocks[b].sol[1].data(), blocks[b].sol[2].data(),
                           blocks[b].sol[3].data(), blocks[b].sol[4].data()};
     check(c, lee_upload_state(c, (int)b, s, step, time), "restart");
+    if (r.nsc) {
+      const double* z[kMaxSlots];
+      for (int q = 0; q < r.nsc; ++q) z[q] = blocks[b].sol[5 + q].data();
+      check(c, lee_upload_scalars(c, (int)b, z), "restart scalars");
+    }
   }
 
   int counter = 0;
@@ -600,6 +629,28 @@ int main(int argc, char** argv) {
       if (!f) die("cannot append to report/solution/solution");
       std::fprintf(f, "Time step: %10d, time: %e", e, time);
       for (int v = 0; v < 5; ++v) std::fprintf(f, ", %s: %e ~ %e", kNames[v], mn[v], mx[v]);
+      if (r.nsc) {
+        // the scalar slots over every point of every block; their names grow as
+        // State::initialize_state_linearizedEuler_scalar builds them with one stringstream
+        // (src/core/state.cpp:350-357): Z0', Z01', Z012', ...
+        std::string digits;
+        for (int q = 0; q < r.nsc; ++q) {
+          double lo = HUGE_VAL, hi = -HUGE_VAL;
+          for (size_t b = 0; b < blocks.size(); ++b) {
+            if (q == 0) {
+              double* z[kMaxSlots];
+              for (int w = 0; w < r.nsc; ++w) z[w] = blocks[b].sol[5 + w].data();
+              check(c, lee_download_scalars(c, (int)b, z), "lee_download_scalars");
+            }
+            for (double v : blocks[b].sol[5 + q]) {
+              lo = std::min(lo, v);
+              hi = std::max(hi, v);
+            }
+          }
+          digits += std::to_string(q);
+          std::fprintf(f, ", Z%s': %e ~ %e", digits.c_str(), lo, hi);
+        }
+      }
       std::fprintf(f, "\n");
       std::fclose(f);
       const bool by_time = (int)((time - time_lastrun) / r.writing_time) > counter;
@@ -609,6 +660,11 @@ int main(int argc, char** argv) {
           double* sol[5] = {blocks[b].sol[0].data(), blocks[b].sol[1].data(), blocks[b].sol[2].data(),
                             blocks[b].sol[3].data(), blocks[b].sol[4].data()};
           check(c, lee_download_state(c, (int)b, sol, &step, nullptr), "lee_download_state");
+          if (r.nsc) {
+            double* z[kMaxSlots];
+            for (int q = 0; q < r.nsc; ++q) z[q] = blocks[b].sol[5 + q].data();
+            check(c, lee_download_scalars(c, (int)b, z), "lee_download_scalars");
+          }
         }
         write_solution(solution_name(counter), blocks, step, time);
       }

@@ -61,8 +61,10 @@ int wave_form(const std::string &s) {
 void solve(UserInput *myinput, Geometry::StructuredGrid *mygrid, Geometry::StructuredBlock *block, State *mystate) {
   if (mpi::nprocs != 1 || myinput->do_overset)
     mpi::graceful_exit("lee_b200 binding: one rank holding one block (no overset) is supported");
-  if (myinput->model_pde != "LEE")
-    mpi::graceful_exit("lee_b200 binding: PHYSICAL_MODEL = LEE only");
+  if (myinput->model_pde != "LEE" && myinput->model_pde != "LEE_SCALAR")
+    mpi::graceful_exit("lee_b200 binding: PHYSICAL_MODEL = LEE or LEE_SCALAR");
+  const int nsc = myinput->model_pde == "LEE_SCALAR" ? myinput->num_scalar : 0;  // slots after p'
+
 
   lee_config cfg = {};
   cfg.num_dim = myinput->num_dim;
@@ -84,6 +86,7 @@ void solve(UserInput *myinput, Geometry::StructuredGrid *mygrid, Geometry::Struc
   cfg.device = 0;
   lee_ctx *ctx = nullptr;
   check(nullptr, lee_create(&cfg, &ctx), "lee_create");
+  if (nsc) check(ctx, lee_set_scalars(ctx, nsc), "lee_set_scalars");
 
   // the block: one rank owns it whole, so the grid has no ghost cells (src/geometry/geometry.cpp:109-132)
   const int nx = mygrid->nXi, ny = mygrid->nEta, nz = mygrid->nZeta;
@@ -100,6 +103,7 @@ void solve(UserInput *myinput, Geometry::StructuredGrid *mygrid, Geometry::Struc
   }
   check(ctx, lee_set_block(ctx, 0, nx, ny, nz, x.data(), y.data(), z.data(), ib.data()), "lee_set_block");
   check(ctx, lee_set_mean(ctx, 0, mystate->sol_mean), "lee_set_mean");
+  if (nsc) check(ctx, lee_set_mean_scalars(ctx, 0, mystate->sol_mean + 5), "lee_set_mean_scalars");
   // BC lines and sponge zones in the BC file's order; sponges pass the strengths the reference
   // computed (Geometry::StructuredBufferZone::buffer_strength, the zone box, xi fastest)
   for (int q = 0; q < mygrid->num_boundaryCondition_nonperiodic; ++q) {
@@ -125,6 +129,7 @@ void solve(UserInput *myinput, Geometry::StructuredGrid *mygrid, Geometry::Struc
     check(ctx, lee_set_source(ctx, LEE_SOURCE_JET2D_HARMONIC, nullptr, 0), "lee_set_source");
   check(ctx, lee_prepare(ctx), "lee_prepare");
   check(ctx, lee_upload_state(ctx, 0, mystate->sol, mystate->time_step, mystate->time_sol), "lee_upload_state");
+  if (nsc) check(ctx, lee_upload_scalars(ctx, 0, mystate->sol + 5), "lee_upload_scalars");
 
   // solver::solve's loop (src/solver/solver.cpp:41-89): FIX_CFL rescales dt every step from the
   // CFL of the previous dt; FIX_DT advances whole runs of steps between reports
@@ -147,6 +152,7 @@ void solve(UserInput *myinput, Geometry::StructuredGrid *mygrid, Geometry::Struc
     if (done % myinput->report_freq == 0 || done == temporal::num_time_steps) {
       check(ctx, lee_download_state(ctx, 0, mystate->sol, &mystate->time_step, &mystate->time_sol),
             "lee_download_state");
+      if (nsc) check(ctx, lee_download_scalars(ctx, 0, mystate->sol + 5), "lee_download_scalars");
       temporal::time_step = mystate->time_step;
       temporal::time_sol = mystate->time_sol;
       if (done % myinput->report_freq == 0) {

@@ -40,10 +40,10 @@ def _run(wd, ic, env_extra=None):
     return subprocess.run([_binary(), ic], cwd=wd, env=env, capture_output=True, text=True, timeout=600)
 
 
-def _written_solution(wd):
+def _written_solution(wd, nvar=5):
     out = sorted(f for f in glob.glob(os.path.join(wd, "*.q")) if os.path.basename(f) not in ("ic.q", "mean.q"))
     assert out, f"no solution file written in {sorted(os.listdir(wd))}"
-    fields, _ = plot3d.read_solution(out[-1])
+    fields, _ = plot3d.read_solution(out[-1], nvar=nvar)
     return fields[0]
 
 
@@ -75,6 +75,29 @@ def test_reference_driver_through_the_c_abi(tmp_path, name, precision):
         assert api.rel_l2(y, g["stepn"]) <= 1e-10
     else:
         assert api.rel_l2(y[4], g["stepn"][4]) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_lee_scalar_deck_through_the_c_abi(tmp_path, precision):
+    """PHYSICAL_MODEL = LEE_SCALAR: the reference's driver hands its 5 + n slots to the library
+    (lee_set_scalars, lee_set_mean_scalars, lee_upload_scalars, lee_download_scalars) and writes
+    them with its own solution writer."""
+    name = "scalar2d_40x32"
+    g = load_golden(name)
+    case = golden_case(name)
+    n = int(g["nsteps"])
+    nv = 5 + case.num_scalars
+    wd = str(tmp_path)
+    ic = case.write_reference_inputs(wd, float(g["dt"]), n, report=n)
+    p = _run(wd, ic, {"LEE_B200_PRECISION": precision})
+    assert p.returncode == 0 and "lee_b200:" not in p.stdout, p.stdout[-2000:] + p.stderr[-2000:]
+    y = _written_solution(wd, nvar=nv)
+    if precision == "fp64":
+        assert api.rel_l2(y, g["stepn"]) <= 1e-10
+    else:
+        for v in range(4, nv):
+            assert api.rel_l2(y[v], g["stepn"][v]) <= 1e-5
 
 
 @pytest.mark.gpu

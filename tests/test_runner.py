@@ -171,6 +171,25 @@ def test_refuses_an_unimplemented_boundary_type(runner, tmp_path):
     assert p.returncode != 0 and "dirichlet_harmonic_wave" in p.stderr
 
 
+def test_parse_only_reads_lee_scalar(runner, tmp_path):
+    """PHYSICAL_MODEL = LEE_SCALAR, NUMBER_SCALAR = n with the 5 + n slot mean and restart files;
+    the reference's own checks on n and on SIMULATION (src/core/input.cpp:113-117, :596-606)."""
+    case = golden_case("scalar2d_40x32")
+    wd = str(tmp_path)
+    case.write_reference_inputs(wd, 0.01, 2)
+    info = json.loads(_run(runner, wd, "--parse-only").stdout)
+    assert info["scalars"] == 2
+    _rewrite_deck(wd, lambda lines: ["SIMULATION = CASE_KBK_COMBUSTOR" if ln.startswith("SIMULATION") else ln
+                                     for ln in lines])
+    p = _run(runner, wd, "--parse-only", check=False)
+    assert p.returncode != 0 and "is not implemented for PHYSICAL_MODEL = LEE_SCALAR" in p.stderr
+    case.write_reference_inputs(wd, 0.01, 2)
+    _rewrite_deck(wd, lambda lines: ["PHYSICAL_MODEL = LEE_SCALAR, NUMBER_SCALAR = 0"
+                                     if ln.startswith("PHYSICAL_MODEL") else ln for ln in lines])
+    p = _run(runner, wd, "--parse-only", check=False)
+    assert p.returncode != 0 and "at least one scalar should be solved for" in p.stderr
+
+
 def test_twocylinder_monopole_is_the_reference_source(oracle_lib):
     """The monopole lee_run sets for CASE_SCATTERING_TWOCYLINDER, run in the oracle, against the
     compiled reference applying its own source (src/solver/source.cpp:60-92)."""
@@ -190,8 +209,8 @@ def test_twocylinder_monopole_is_the_reference_source(oracle_lib):
 # GPU: running the case
 # ---------------------------------------------------------------------------------------------
 
-def _final_solution(wd, counter):
-    qs, taus = plot3d.read_solution(os.path.join(wd, f"camille.{counter:06d}.q"))
+def _final_solution(wd, counter, nvar=5):
+    qs, taus = plot3d.read_solution(os.path.join(wd, f"camille.{counter:06d}.q"), nvar=nvar)
     return qs, taus
 
 
@@ -286,3 +305,33 @@ def test_twocylinder_source_matches_the_live_reference(runner, product_lib, tmp_
     s = api.Solver(product_lib, plain)
     s.advance(24, dt)
     assert api.rel_l2(s.download(0)[0], ref) > 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["scalar2d_40x32", "scalar3d_14", "scalar_cylinder2d_64"])
+def test_lee_scalar_run_matches_reference_and_solver(runner, product_lib, tmp_path, name):
+    """A LEE_SCALAR deck: the 5 + n slot solution file equals the Solver's state bit for bit and the
+    reference's within 1e-10; the report line carries the scalars under the reference's names."""
+    from tests.test_oracle_pin import full_state
+    case = golden_case(name)
+    g = load_golden(name)
+    dt, nsteps = float(g["dt"]), int(g["nsteps"])
+    nv = 5 + case.num_scalars
+    wd = str(tmp_path)
+    case.write_reference_inputs(wd, dt, nsteps, report=nsteps)
+    _run(runner, wd)
+    qs, taus = _final_solution(wd, 1, nvar=nv)
+    s = api.Solver(product_lib, case)
+    s.advance(nsteps, dt)
+    for b in range(len(case.blocks)):
+        np.testing.assert_array_equal(qs[b], full_state(s, b))
+        ref = g["stepn"] if "stepn" in g else g[f"stepn_{b}"]
+        assert api.rel_l2(qs[b], ref) <= 1e-10
+    rep = open(os.path.join(wd, "report", "solution", "solution")).read().splitlines()[-1]
+    names = [part.split(": ")[0] for part in rep.split(", ")[2:]]
+    assert names[5:] == ["Z0'", "Z01'", "Z012'"][:case.num_scalars]
+    for k in range(case.num_scalars):
+        lo, hi = (float(x) for x in rep.split(", ")[2 + 5 + k].split(": ")[1].split(" ~ "))
+        allv = np.concatenate([q[5 + k].ravel() for q in qs])
+        assert lo == pytest.approx(allv.min(), rel=1e-6, abs=1e-300)
+        assert hi == pytest.approx(allv.max(), rel=1e-6, abs=1e-300)
