@@ -169,7 +169,7 @@ struct lee_ctx {
   // from the context stream and joined before whatever couples the blocks (overset, the clock)
   bool concurrent = true;       // lee_set_block_streams
   bool batching = true;         // lee_set_batching: eligible batches run the batched kernels
-  bool increment_step = true;   // lee_set_increment_step
+  bool increment_step = false;  // lee_set_increment_step (measured slower on the B200: off)
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> side_ev;  // [0] the fork, [1 + q] the join of side stream q
   int* d_err = nullptr;          // [0] a bounded wait gave up, [1] a non-finite state value was found

@@ -220,16 +220,22 @@ void read_solution(const std::string& path, std::vector<Block>& blocks, int* ste
   }
 }
 
-// tau = {0, 1, step, time} (src/io/plot3d.cpp:1289).
+// tau = {0, 1, step, time} (src/io/plot3d.cpp:1289). With more than five slots (LEE_SCALAR) the
+// reference writes the PLOT3D function format instead: (nxi, neta, nzeta, nvar) per block and no
+// tau (io::write_solution, src/io/io.cpp:740-760); it still reads restarts as solution files.
 void write_solution(const std::string& path, const std::vector<Block>& blocks, int step, double time) {
   std::ofstream f(path, std::ios::binary | std::ios::trunc);
   if (!f) die("cannot write " + path);
   const int nb = (int)blocks.size();
+  const bool function_form = g_nv != 5;
   f.write(reinterpret_cast<const char*>(&nb), 4);
-  for (auto& k : blocks) f.write(reinterpret_cast<const char*>(k.n), 12);
+  for (auto& k : blocks) {
+    f.write(reinterpret_cast<const char*>(k.n), 12);
+    if (function_form) f.write(reinterpret_cast<const char*>(&g_nv), 4);
+  }
   for (auto& k : blocks) {
     const double tau[4] = {0.0, 1.0, (double)step, time};
-    f.write(reinterpret_cast<const char*>(tau), 32);
+    if (!function_form) f.write(reinterpret_cast<const char*>(tau), 32);
     for (int v = 0; v < g_nv; ++v)
       f.write(reinterpret_cast<const char*>(k.sol[v].data()), (std::streamsize)(k.N * 8));
   }

@@ -312,12 +312,13 @@ int lee_set_graphs(lee_ctx *ctx, int on);
  * holes, BC lines or overset runs the batched kernels (one launch per stage for all blocks); off,
  * every block runs its own kernels (TMA-staged where the block allows), side by side. */
 int lee_set_block_streams(lee_ctx *ctx, int on);
-/* The compensated form's step (no reference counterpart; the same bits either way): on (default),
- * on blocks where nothing acts between the last RK stage and the filter (TMA-staged kernels, the
- * one-row fused filter, no BC lines, no overset, a uniform mean), the last stage writes the step's
+/* The compensated form's step (no reference counterpart; the same bits either way): on, on blocks
+ * where nothing acts between the last RK stage and the filter (TMA-staged kernels, the one-row
+ * fused filter, no BC lines, no overset, a uniform mean), the last stage writes the step's
  * increment alone and the fused filter forms y_pre = y_n + increment and its rounding error
- * itself: 2V fewer words of 4 bytes per point and step. Off: the last stage writes y_pre and its
- * error. */
+ * itself: 2V fewer words of 4 bytes per point and step, but the filter then stages y_n and the
+ * increment with their halos (twice the shared memory per plane), which costs it more time than
+ * the stage saves on the B200. Off (default): the last stage writes y_pre and its error. */
 int lee_set_increment_step(lee_ctx *ctx, int on);
 int lee_set_batching(lee_ctx *ctx, int on);
 /* Failure detection (no reference counterpart: camille keeps going on NaN, and its waits are MPI

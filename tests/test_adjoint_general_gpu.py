@@ -88,17 +88,21 @@ def test_fp32_transpose_agrees_with_fp64(product_lib):
         assert api.rel_l2(b, a) <= 1e-5
 
 
-def _cylinder_gradient_case(nsteps=30):
-    case = golden_case("cylinder2d_64")
-    case = copy.deepcopy(case)
+def _cylinder_gradient_case(nsteps=120):
+    """The cylinder layout from rest (J is then a quadratic form in the amplitudes, so central
+    differences are exact up to rounding) with a 4 x 4 lattice source on the background just
+    left of the O-grid, and microphones on an O-grid ring that its waves reach within the run."""
+    case = copy.deepcopy(golden_case("cylinder2d_64"))
     case.nsteps = nsteps
     case.monopole = None
+    for blk in case.blocks:
+        blk.state = np.zeros_like(blk.state)
     rng = np.random.default_rng(9)
     amps = rng.normal(0.0, 1e-3, size=(1, 4, 4))
-    case.distributed = cases.DistributedSource(0, 0.8 * np.pi, (16.0, 28.0, 0.0), (3.0, 3.0, 1.0), amps)
+    case.distributed = cases.DistributedSource(0, 0.8 * np.pi, (18.0, 28.0, 0.0), (2.0, 2.0, 1.0), amps)
     nx = case.blocks[1].dims[0]
     ii = np.arange(4, nx - 4, 5)
-    case.microphones = cases.Microphones(1, (ii + nx * 10).astype(np.int64), 0.05)
+    case.microphones = cases.Microphones(1, (ii + nx * 8).astype(np.int64), 0.05)
     return case
 
 
@@ -113,11 +117,11 @@ def test_overset_gradient_central_differences(product_lib):
     a0 = case.distributed.amplitudes
     s = api.Solver(product_lib, case)
     dt = s.compute_dt()
-    J, g, mism = s.adjoint_gradient(case.nsteps, dt, checkpoint_every=7, recompute=True)
+    J, g, mism = s.adjoint_gradient(case.nsteps, dt, checkpoint_every=25, recompute=True)
     assert mism == 0
     assert abs(J - api.Solver(product_lib, case).eval_objective(case.nsteps, dt)) <= 1e-13 * J
     s2 = api.Solver(product_lib, case)
-    J2, g2, _ = s2.adjoint_gradient(case.nsteps, dt, checkpoint_every=7, recompute=False)
+    J2, g2, _ = s2.adjoint_gradient(case.nsteps, dt, checkpoint_every=25, recompute=False)
     assert J2 == J
     np.testing.assert_array_equal(g, g2)
     assert np.linalg.norm(g) > 0.0

@@ -41,8 +41,12 @@ def _run(wd, ic, env_extra=None):
 
 
 def _written_solution(wd, nvar=5):
+    """The last solution file; with more than five slots the reference writes it in the PLOT3D
+    function format (io::write_solution, src/io/io.cpp:740-760)."""
     out = sorted(f for f in glob.glob(os.path.join(wd, "*.q")) if os.path.basename(f) not in ("ic.q", "mean.q"))
     assert out, f"no solution file written in {sorted(os.listdir(wd))}"
+    if nvar != 5:
+        return plot3d.read_function(out[-1])[0]
     fields, _ = plot3d.read_solution(out[-1], nvar=nvar)
     return fields[0]
 

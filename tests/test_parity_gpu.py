@@ -377,7 +377,8 @@ def test_increment_step_gives_the_same_bits(product_lib, label):
     }[label]()
     a = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
     b = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
-    assert product_lib.set_increment_step(b.ctx, 0) == api.LEE_OK
+    assert product_lib.set_increment_step(a.ctx, 1) == api.LEE_OK
+    assert a.info().increment_step == 1 and b.info().increment_step == 0
     dt = a.compute_dt()
     for n in (1, case.nsteps, 3):
         a.advance(n, dt)

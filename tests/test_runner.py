@@ -209,8 +209,8 @@ def test_twocylinder_monopole_is_the_reference_source(oracle_lib):
 # GPU: running the case
 # ---------------------------------------------------------------------------------------------
 
-def _final_solution(wd, counter, nvar=5):
-    qs, taus = plot3d.read_solution(os.path.join(wd, f"camille.{counter:06d}.q"), nvar=nvar)
+def _final_solution(wd, counter):
+    qs, taus = plot3d.read_solution(os.path.join(wd, f"camille.{counter:06d}.q"))
     return qs, taus
 
 
@@ -310,8 +310,9 @@ def test_twocylinder_source_matches_the_live_reference(runner, product_lib, tmp_
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["scalar2d_40x32", "scalar3d_14", "scalar_cylinder2d_64"])
 def test_lee_scalar_run_matches_reference_and_solver(runner, product_lib, tmp_path, name):
-    """A LEE_SCALAR deck: the 5 + n slot solution file equals the Solver's state bit for bit and the
-    reference's within 1e-10; the report line carries the scalars under the reference's names."""
+    """A LEE_SCALAR deck: the 5 + n slot solution file (function format) equals the Solver's state bit
+    for bit and the reference's within 1e-10; the report line carries the scalars under the
+    reference's names."""
     from tests.test_oracle_pin import full_state
     case = golden_case(name)
     g = load_golden(name)
@@ -320,7 +321,8 @@ def test_lee_scalar_run_matches_reference_and_solver(runner, product_lib, tmp_pa
     wd = str(tmp_path)
     case.write_reference_inputs(wd, dt, nsteps, report=nsteps)
     _run(runner, wd)
-    qs, taus = _final_solution(wd, 1, nvar=nv)
+    # more than five slots: the PLOT3D function format, as the reference writes it
+    qs = plot3d.read_function(os.path.join(wd, "camille.000001.q"))
     s = api.Solver(product_lib, case)
     s.advance(nsteps, dt)
     for b in range(len(case.blocks)):
