@@ -378,7 +378,11 @@ def test_increment_step_gives_the_same_bits(product_lib, label):
     a = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
     b = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED)
     assert product_lib.set_increment_step(a.ctx, 1) == api.LEE_OK
-    assert a.info().increment_step == 1 and b.info().increment_step == 0
+    assert b.info().increment_step == 0
+    if label.startswith("curvi3d"):
+        # 3-D FP32 blocks run the one-row fused filter, which takes the increment; a 2-D block may
+        # be autotuned to the two-row form, which does not
+        assert a.info().increment_step == 1
     dt = a.compute_dt()
     for n in (1, case.nsteps, 3):
         a.advance(n, dt)
