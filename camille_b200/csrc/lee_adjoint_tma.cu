@@ -6,10 +6,12 @@
 // stencil tap; here a CTA owns a 32 x 8 tile in (i, j), marches along k, and builds each flux once:
 // for every incoming plane (a TMA box of w and J*metrics with a two-point halo) it writes
 //   G^xi  on the tile's rows, two columns beyond the tile on both sides,
-//   G^eta on the tile's columns, two rows beyond the tile on both sides,
-//   G^zeta on the tile, into a ring of planes,
-// then applies the transposed xi and eta stencils at the tile (kept per point in registers) and
-// completes the plane two behind the incoming one with the transposed zeta stencil. Each point's
+//   G^eta on the tile's columns, two rows beyond the tile on both sides
+// into shared memory (one loop over both sets, so no thread takes more than one item beyond
+// the others), keeps G^zeta at its own point in a register queue of five planes (the zeta
+// stencil only ever reads the thread's own column), then applies the transposed xi and eta
+// stencils at the tile (kept per point in registers) and completes the plane two behind the
+// incoming one with the transposed zeta stencil. Each point's
 // own work (the sponge, the ybar and next-input updates, the source gradient) is that of
 // k_adj_stage. The transposed stencils must lie within two points of the row (TransOp.H == 2: the
 // 4th-order difference); the host checks.
@@ -36,11 +38,11 @@ struct AGeo {
   static constexpr int NSL = 2;        // TMA slots: the plane in work and the next
   static constexpr int GXW = TX + 2 * kAH;  // G^xi row width
   static constexpr int GYH = TY + 2 * kAH;  // G^eta column height
-  static constexpr int NZ = 2 * kAH + 2;    // G^zeta ring planes (one beyond the stencil)
+  static constexpr int NGX = TY * GXW, NGY = GYH * TX;  // G^xi and G^eta items of a plane
+  static_assert(NGX % 32 == 0, "the G^xi items end on a warp boundary");
   static constexpr int OFF_GX = NSL * NF * FBP;             // [2][5][TY][GXW]
   static constexpr int OFF_GY = OFF_GX + 2 * 5 * TY * GXW;  // [2][5][GYH][TX]
-  static constexpr int OFF_GZ = OFF_GY + 2 * 5 * GYH * TX;  // [NZ][5][TY][TX]
-  static constexpr int OFF_BAR = OFF_GZ + NZ * 5 * TY * TX;
+  static constexpr int OFF_BAR = OFF_GY + 2 * 5 * GYH * TX;
   static constexpr size_t BYTES = (size_t)OFF_BAR * sizeof(T) + NSL * sizeof(uint64_t);
   static_assert((OFF_BAR * sizeof(T)) % 8 == 0, "mbarrier alignment");
   static_assert((FBP * sizeof(T)) % 128 == 0, "box stride must be a multiple of 128 bytes");
@@ -66,12 +68,11 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
                                                  const __grid_constant__ AdjTmaParams<T> P) {
   using G = AGeo<T>;
   constexpr int TX = G::TX, TY = G::TY, HX = G::HX, BX = G::BX, FBP = G::FBP, NF = G::NF;
-  constexpr int GXW = G::GXW, GYH = G::GYH, NZ = G::NZ;
+  constexpr int GXW = G::GXW, GYH = G::GYH;
   extern __shared__ __align__(128) unsigned char smem[];
   T* ring = reinterpret_cast<T*>(smem);
   T* gxs = ring + G::OFF_GX;
   T* gys = ring + G::OFF_GY;
-  T* gzs = ring + G::OFF_GZ;
   uint64_t* bar = reinterpret_cast<uint64_t*>(ring + G::OFF_BAR);
   const AdjStageParams<T>& p = P.a;
 
@@ -124,12 +125,17 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
 
   const unsigned nxy = (unsigned)p.nx * (unsigned)p.ny;
   const unsigned lij = (unsigned)i + (unsigned)p.nx * (unsigned)j;
-  // per-point results of the last planes: L^T restricted to xi and eta, and w at the point
-  T rq[kAH + 1][5], wq[kAH + 1][5];
+  // per-point results of the last planes: L^T restricted to xi and eta, and w at the point; and
+  // G^zeta at the point over the planes the zeta stencil reads (zq[0] the oldest)
+  T rq[kAH + 1][5], wq[kAH + 1][5], zq[2 * kAH + 1][5];
 #pragma unroll
   for (int a = 0; a <= kAH; ++a)
 #pragma unroll
     for (int v = 0; v < 5; ++v) rq[a][v] = wq[a][v] = T(0);
+#pragma unroll
+  for (int a = 0; a <= 2 * kAH; ++a)
+#pragma unroll
+    for (int v = 0; v < 5; ++v) zq[a][v] = T(0);
 
   for (int pl = k0 - kAH; pl <= k1 - 1 + kAH; ++pl) {
     const bool in_blk = pl >= plo && pl <= phi;
@@ -152,9 +158,9 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
     const int buf = pl & 1;
     T* gx = gxs + buf * (5 * TY * GXW);
     T* gy = gys + buf * (5 * GYH * TX);
-    T* gz = gzs + (((pl % NZ) + NZ) % NZ) * (5 * TY * TX);
     bool failed = false;
     T wc[5] = {T(0), T(0), T(0), T(0), T(0)};
+    T gzc[5] = {T(0), T(0), T(0), T(0), T(0)};  // G^zeta at the point (zero beyond the block)
     if (in_blk) {
       const int rel = pl - plo;
       failed = !mbar_wait(&bar[rel % G::NSL], (unsigned)((rel / G::NSL) & 1), P.wait_ns);
@@ -162,28 +168,26 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
       T w[5], jm[3], g[5];
       // G^zeta at the tile point, and w there
       point(slot, HX + tx, kAH + ty, 2, w, jm);
-      flux(w, jm, ub, p.gpb, p.rbi, g);
+      flux(w, jm, ub, p.gpb, p.rbi, gzc);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        gz[(v * TY + ty) * TX + tx] = g[v];
-        wc[v] = w[v];
-      }
+      for (int v = 0; v < 5; ++v) wc[v] = w[v];
       if (out_plane) {
-        // G^xi on rows j0..j0+TY-1, columns i0-2..i0+TX+1
-        for (int q = tid; q < TY * GXW; q += 256) {
-          const int r = q / GXW, cc = q % GXW;
-          point(slot, HX - kAH + cc, kAH + r, 0, w, jm);
-          flux(w, jm, ub, p.gpb, p.rbi, g);
+        // G^xi on rows j0..j0+TY-1, columns i0-2..i0+TX+1, then G^eta on rows j0-2..j0+TY+1,
+        // columns i0..i0+TX-1, as one list of items
+        for (int q = tid; q < G::NGX + G::NGY; q += 256) {
+          if (q < G::NGX) {
+            const int r = q / GXW, cc = q % GXW;
+            point(slot, HX - kAH + cc, kAH + r, 0, w, jm);
+            flux(w, jm, ub, p.gpb, p.rbi, g);
 #pragma unroll
-          for (int v = 0; v < 5; ++v) gx[(v * TY + r) * GXW + cc] = g[v];
-        }
-        // G^eta on rows j0-2..j0+TY+1, columns i0..i0+TX-1
-        for (int q = tid; q < GYH * TX; q += 256) {
-          const int r = q / TX, cc = q % TX;
-          point(slot, HX + cc, r, 1, w, jm);
-          flux(w, jm, ub, p.gpb, p.rbi, g);
+            for (int v = 0; v < 5; ++v) gx[(v * TY + r) * GXW + cc] = g[v];
+          } else {
+            const int r = (q - G::NGX) / TX, cc = (q - G::NGX) % TX;
+            point(slot, HX + cc, r, 1, w, jm);
+            flux(w, jm, ub, p.gpb, p.rbi, g);
 #pragma unroll
-          for (int v = 0; v < 5; ++v) gy[(v * GYH + r) * TX + cc] = g[v];
+            for (int v = 0; v < 5; ++v) gy[(v * GYH + r) * TX + cc] = g[v];
+          }
         }
       }
     }
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
     }
     // the slot of this plane has been read: load the plane after next into it
     if (tid == 0) issue_upto(pl + G::NSL);
-    // shift the per-point queues; the new entry holds this plane's xi and eta terms
+    // shift the per-point queues; the new entries hold this plane's xi and eta terms and G^zeta
 #pragma unroll
     for (int a = 0; a < kAH; ++a)
 #pragma unroll
@@ -205,6 +209,12 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
         rq[a][v] = rq[a + 1][v];
         wq[a][v] = wq[a + 1][v];
       }
+#pragma unroll
+    for (int a = 0; a < 2 * kAH; ++a)
+#pragma unroll
+      for (int v = 0; v < 5; ++v) zq[a][v] = zq[a + 1][v];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) zq[2 * kAH][v] = gzc[v];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       T acc = T(0);
@@ -224,14 +234,12 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
       T acc[5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) acc[v] = rq[0][v];
+      // planes kf-2..kf+2 are zq[0..4] (entries beyond the block are zero and carry zero weight)
 #pragma unroll
       for (int t = 0; t <= 2 * kAH; ++t) {
         const T r = (T)az[t + p.op.H - kAH];
-        if (r == T(0)) continue;  // a tap beyond the block (never written in the ring)
-        const int zq = kf + t - kAH;
-        const T* gp = gzs + (((zq % NZ) + NZ) % NZ) * (5 * TY * TX) + ty * TX + tx;
 #pragma unroll
-        for (int v = 0; v < 5; ++v) acc[v] += r * gp[v * TY * TX];
+        for (int v = 0; v < 5; ++v) acc[v] += r * zq[t][v];
       }
       const T(&wf)[5] = wq[0];
       if (p.sigma) {

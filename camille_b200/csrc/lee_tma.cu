@@ -290,6 +290,10 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
         u1[row * TX + tx] = COMP ? f[0] + d : d;
       }
       __syncthreads();
+      // every thread is done with this plane's box: its slot takes the plane NSF ahead. The
+      // eta pass below reads u1 only, and the next plane writes u1 after its own wait barrier,
+      // which every thread reaches only once this pass is done
+      if (tid == 0) issue_upto(p + NSF);
       T dy = T(0);
 #pragma unroll
       for (int o = -HF; o <= HF; ++o) dy += wy[o + HF] * (o == 0 ? u1c : u1[(ty + HF + o) * TX + tx]);
@@ -299,8 +303,6 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
       } else {
         u2 = dy;
       }
-      __syncthreads();
-      if (tid == 0) issue_upto(p + NSF);
     }
 #pragma unroll
     for (int q = 0; q < NQ - 1; ++q) uq[q] = uq[q + 1];
@@ -464,6 +466,8 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
         u1[row * TX + tx] = COMP ? f[0] + d : d;
       }
       __syncthreads();
+      // the box is free for the plane NSF ahead; u1 is next written after the next wait barrier
+      if (tid == 0) issue_upto(p + NSF);
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
         T dy = T(0);
@@ -477,8 +481,6 @@ __global__ void __launch_bounds__(256) k_filter_tma(const __grid_constant__ Fiel
           u2[r] = dy;
         }
       }
-      __syncthreads();
-      if (tid == 0) issue_upto(p + NSF);
     }
     const int k = kf;
     int cz = 0;
