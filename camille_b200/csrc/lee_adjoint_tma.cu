@@ -4,14 +4,13 @@
 // zbar = L^T w with (L^T w)_v = sum_d D_d^T G^d_v(w) - sigma w_v (the fluxes G^d of lee_adjoint.cu,
 // uniform mean flow). The generic kernel (k_adj_stage) rebuilds every neighbour's flux for every
 // stencil tap; here a CTA owns a 32 x 8 tile in (i, j), marches along k, and builds each flux once:
-// for every incoming plane (a TMA box of w and J*metrics with a two-point halo) it writes
-//   G^xi  on the tile's rows, two columns beyond the tile on both sides,
-//   G^eta on the tile's columns, two rows beyond the tile on both sides
-// into shared memory (one loop over both sets, so no thread takes more than one item beyond
-// the others), keeps G^zeta at its own point in a register queue of five planes (the zeta
-// stencil only ever reads the thread's own column), then applies the transposed xi and eta
-// stencils at the tile (kept per point in registers) and completes the plane two behind the
-// incoming one with the transposed zeta stencil. Each point's
+// for every incoming plane (a TMA box of w and J*metrics with a two-point halo) each thread
+// reads w and the nine J*metrics at its own tile point once and builds all three fluxes there;
+// G^xi and G^eta go to shared memory, G^zeta to a register queue of five planes (the zeta
+// stencil only reads the thread's own column). One warp adds G^xi two columns beyond the tile
+// on each side of its rows and four warps G^eta two rows beyond it on each side of its columns.
+// Then the transposed xi and eta stencils at the tile (kept per point in registers), and the
+// plane two behind the incoming one is completed with the transposed zeta stencil. Each point's
 // own work (the sponge, the ybar and next-input updates, the source gradient) is that of
 // k_adj_stage. The transposed stencils must lie within two points of the row (TransOp.H == 2: the
 // 4th-order difference); the host checks.
@@ -38,8 +37,9 @@ struct AGeo {
   static constexpr int NSL = 2;        // TMA slots: the plane in work and the next
   static constexpr int GXW = TX + 2 * kAH;  // G^xi row width
   static constexpr int GYH = TY + 2 * kAH;  // G^eta column height
-  static constexpr int NGX = TY * GXW, NGY = GYH * TX;  // G^xi and G^eta items of a plane
-  static_assert(NGX % 32 == 0, "the G^xi items end on a warp boundary");
+  // the halo fluxes: G^xi at 2 kAH columns of the TY rows (one warp), G^eta at 2 kAH rows of the
+  // TX columns (four warps)
+  static_assert(2 * kAH * TY == 32 && 2 * kAH * TX == 128, "halo items of one and four warps");
   static constexpr int OFF_GX = NSL * NF * FBP;             // [2][5][TY][GXW]
   static constexpr int OFF_GY = OFF_GX + 2 * 5 * TY * GXW;  // [2][5][GYH][TX]
   static constexpr int OFF_BAR = OFF_GY + 2 * 5 * GYH * TX;
@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
 
   const T scale = p.first ? p.hb_in : T(1);
   const T ub[3] = {p.ubar[0], p.ubar[1], p.ubar[2]};
-  // transposed stencil rows along xi and eta: fixed for a thread
-  T rx[2 * kAH + 1], ry[2 * kAH + 1];
+  // transposed stencil rows along xi and eta: fixed for a thread; the interior zeta row
+  T rx[2 * kAH + 1], ry[2 * kAH + 1], rzi[2 * kAH + 1];
   {
     const int ci = min(i, p.nx - 1), cj = min(j, p.ny - 1);
     const double* ax = ci < p.op.E ? p.op.lt[ci] : (ci > p.nx - 1 - p.op.E ? p.op.rt[p.nx - 1 - ci] : p.op.in);
@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
     for (int t = 0; t <= 2 * kAH; ++t) {
       rx[t] = (T)ax[t + p.op.H - kAH];
       ry[t] = (T)ay[t + p.op.H - kAH];
+      rzi[t] = (T)p.op.in[t + p.op.H - kAH];
     }
   }
   // w at a box point (scaled) and the J*metrics row of direction d there
@@ -165,29 +166,43 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
       const int rel = pl - plo;
       failed = !mbar_wait(&bar[rel % G::NSL], (unsigned)((rel / G::NSL) & 1), P.wait_ns);
       const T* slot = ring + (rel % G::NSL) * NF * FBP;
-      T w[5], jm[3], g[5];
-      // G^zeta at the tile point, and w there
-      point(slot, HX + tx, kAH + ty, 2, w, jm);
-      flux(w, jm, ub, p.gpb, p.rbi, gzc);
+      T g[5];
+      {
+        // the tile point: w and the J*metrics rows of the three directions, read once
+        const int o = (kAH + ty) * BX + HX + tx;
+        T jm[3][3];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) wc[v] = w[v];
-      if (out_plane) {
-        // G^xi on rows j0..j0+TY-1, columns i0-2..i0+TX+1, then G^eta on rows j0-2..j0+TY+1,
-        // columns i0..i0+TX-1, as one list of items
-        for (int q = tid; q < G::NGX + G::NGY; q += 256) {
-          if (q < G::NGX) {
-            const int r = q / GXW, cc = q % GXW;
-            point(slot, HX - kAH + cc, kAH + r, 0, w, jm);
-            flux(w, jm, ub, p.gpb, p.rbi, g);
+        for (int v = 0; v < 5; ++v) wc[v] = scale * slot[v * FBP + o];
 #pragma unroll
-            for (int v = 0; v < 5; ++v) gx[(v * TY + r) * GXW + cc] = g[v];
-          } else {
-            const int r = (q - G::NGX) / TX, cc = (q - G::NGX) % TX;
-            point(slot, HX + cc, r, 1, w, jm);
-            flux(w, jm, ub, p.gpb, p.rbi, g);
+        for (int d = 0; d < 3; ++d)
 #pragma unroll
-            for (int v = 0; v < 5; ++v) gy[(v * GYH + r) * TX + cc] = g[v];
-          }
+          for (int x = 0; x < 3; ++x) jm[d][x] = JMF ? slot[(5 + d * 3 + x) * FBP + o] : p.jm[d * 3 + x].c;
+        flux(wc, jm[2], ub, p.gpb, p.rbi, gzc);
+        if (out_plane) {
+          flux(wc, jm[0], ub, p.gpb, p.rbi, g);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) gx[(v * TY + ty) * GXW + tx + kAH] = g[v];
+          flux(wc, jm[1], ub, p.gpb, p.rbi, g);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) gy[(v * GYH + ty + kAH) * TX + tx] = g[v];
+        }
+      }
+      if (out_plane && tid < 2 * kAH * (TY + TX)) {
+        T w[5], jm[3];
+        if (tid < 2 * kAH * TY) {
+          // G^xi at columns i0-2, i0-1, i0+TX, i0+TX+1 of row r
+          const int r = tid >> 2, c = tid & 3, cc = c < kAH ? c : TX + c;
+          point(slot, HX - kAH + cc, kAH + r, 0, w, jm);
+          flux(w, jm, ub, p.gpb, p.rbi, g);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) gx[(v * TY + r) * GXW + cc] = g[v];
+        } else {
+          // G^eta at rows j0-2, j0-1, j0+TY, j0+TY+1 of column c
+          const int q = tid - 2 * kAH * TY, r = q >> 5, c = q & 31, rr = r < kAH ? r : TY + r;
+          point(slot, HX + c, rr, 1, w, jm);
+          flux(w, jm, ub, p.gpb, p.rbi, g);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) gy[(v * GYH + rr) * TX + c] = g[v];
         }
       }
     }
@@ -230,6 +245,7 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
     }
     if (fin) {
       // the zeta stencil of plane kf, then the point's own terms (k_adj_stage)
+      const bool zin = kf >= p.op.E && kf <= p.nz - 1 - p.op.E;
       const double* az = kf < p.op.E ? p.op.lt[kf] : (kf > p.nz - 1 - p.op.E ? p.op.rt[p.nz - 1 - kf] : p.op.in);
       T acc[5];
 #pragma unroll
@@ -237,7 +253,7 @@ __global__ void __launch_bounds__(256) k_adj_tma(const __grid_constant__ AdjMaps
       // planes kf-2..kf+2 are zq[0..4] (entries beyond the block are zero and carry zero weight)
 #pragma unroll
       for (int t = 0; t <= 2 * kAH; ++t) {
-        const T r = (T)az[t + p.op.H - kAH];
+        const T r = zin ? rzi[t] : (T)az[t + p.op.H - kAH];
 #pragma unroll
         for (int v = 0; v < 5; ++v) acc[v] += r * zq[t][v];
       }
