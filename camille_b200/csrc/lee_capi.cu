@@ -123,6 +123,8 @@ int lee_create(const lee_config* cfg, lee_ctx** out) {
     c->fltd = minus_identity(c->flt);
     c->hf = c->flt.h;
     c->wfl_ok = c->hf <= 5 && class_weights(c->comp ? c->fltd : c->flt, c->hf, &c->wfl[0][0], 11);
+    // the zero class of a hole after a hole: F = 0, so the increment form's row is -1 at the point
+    if (c->wfl_ok) c->wfl[1 + 2 * c->flt.nb][c->hf] = c->comp ? -1.0 : 0.0;
     c->wfl_sym = c->wfl_ok && (c->hf == 2 || c->hf == 4 || c->hf == 5);
     for (int o = 1; o <= c->hf && c->wfl_sym; ++o) c->wfl_sym = c->wfl[0][c->hf - o] == c->wfl[0][c->hf + o];
   }

@@ -158,8 +158,8 @@ struct lee_ctx {
   // TMA: tensor maps per field buffer, weight tables by closure class, device error flag
   EncodeTiledFn encode = nullptr;
   std::map<MapKey, MapBytes> tmaps;
-  double wst[5][5] = {};
-  double wfl[11][11] = {};
+  double wst[6][5] = {};   // stage classes: interior, 2 left, 2 right, the zero class (holes)
+  double wfl[12][11] = {};  // filter classes: interior, nb left, nb right, the zero class (holes)
   int hf = 0;
   bool wst_ok = false, wfl_ok = false;
   bool wfl_sym = false;  // symmetric interior filter stencil: the vectorised filter kernel applies

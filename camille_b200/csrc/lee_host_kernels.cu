@@ -104,7 +104,7 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
 }
 
 bool increment_step_applies(const lee_ctx* c, const BlockData& b) {
-  if (!c->comp || !c->increment_step || c->batch.active || c->ovs.n > 0) return false;
+  if (!c->comp || !c->increment_step || c->batch.active || c->ovs.n > 0 || b.has_holes) return false;
   if (c->cfg.filter_scheme == LEE_FILTER_NONE || !b.tma || !b.tma_filter || b.filter_px > 0 || b.filter_ry != 1)
     return false;
   if (b.need_rho) return false;  // rho'/rho_bar is formed from y_pre after the last stage
@@ -150,7 +150,7 @@ int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* co
   tp.s = p;
   tp.tiles_x = b.tiles_x;
   tp.k_chunk = chunk_override ? chunk_override : b.stage_chunk;
-  for (int a = 0; a < 5; ++a)
+  for (int a = 0; a < 6; ++a)
     for (int o = 0; o < 5; ++o) tp.w[a][o] = (T)c->wst[a][o];
   tp.err = c->d_err;
   tp.wait_ns = c->wait_ns;
@@ -185,8 +185,12 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
   fp.tiles_x = b.tiles_x;
   fp.k_chunk = chunk_override ? chunk_override : b.filter_chunk;
   fp.nb = c->hf;
-  for (int a = 0; a < 11; ++a)
+  for (int a = 0; a < 12; ++a)
     for (int o = 0; o < 11; ++o) fp.w[a][o] = (T)c->wfl[a][o];
+  if (b.has_holes) {
+    for (int d = 0; d < 3; ++d) fp.code[d] = b.d_code_flt[d];
+    fp.iblank = b.d_iblank;
+  }
   fp.blend = (T)c->cfg.filter_blend;
   for (int v = 0; v < c->V; ++v) {
     fp.err[v] = err ? (const T*)err[v] : nullptr;
@@ -260,7 +264,8 @@ int autotune(lee_ctx* c, BlockData& b) {
       } else {
         b.filter_px = kinds[kq / nry];
         b.filter_ry = 1 + kq % nry;
-        if (b.filter_px > 0 && b.filter_ry > 1) continue;
+        // the one-row form alone takes holes and the increment step's input
+        if ((b.filter_px > 0 || b.has_holes || (c->comp && c->increment_step)) && b.filter_ry > 1) continue;
         set_filter_tiles(c, b);
       }
       for (int ch : (d3 ? std::vector<int>(std::begin(cands3), std::end(cands3))

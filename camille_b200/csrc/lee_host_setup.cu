@@ -374,7 +374,8 @@ int lee_prepare(lee_ctx* c) {
       if ((rc = alloc_fields(c, b.comp, b.N))) return rc;
       if ((rc = alloc_fields(c, b.dsum, b.N))) return rc;
     }
-    // TMA-staged kernels: no holes, the 4th-order difference, rows of 16-byte multiples
+    // TMA-staged kernels: the 4th-order difference, rows of 16-byte multiples; on a block with
+    // holes the classes come from the closure codes (one-point stage kernel, one-row filter)
     const bool rows16 = ((size_t)b.nx * c->esz) % 16 == 0;
     b.tiles_x = (b.nx + kTileX - 1) / kTileX;
     b.tiles_y = (b.ny + kTileY - 1) / kTileY;
@@ -382,13 +383,12 @@ int lee_prepare(lee_ctx* c) {
     // (and the harmonic-wave sponge, an RHS term of the generic kernel's zone loop, is absent)
     bool wave_zone = false;
     for (auto& z : b.bnd) wave_zone |= z.kind == LEE_SPONGE_FREUND_HARMONICWAVE;
-    b.tma = c->wst_ok && !b.has_holes && rows16 && (unsigned long long)b.N < (1ull << 32) && !wave_zone &&
-            !c->axisym;
-    b.tma_filter = c->wfl_ok && !b.has_holes && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE &&
-                   (unsigned long long)b.N < (1ull << 32);
+    b.tma = c->wst_ok && rows16 && (unsigned long long)b.N < (1ull << 32) && !wave_zone && !c->axisym;
+    b.tma_filter = c->wfl_ok && rows16 && c->cfg.filter_scheme != LEE_FILTER_NONE &&
+                   (unsigned long long)b.N < (1ull << 32) && (!b.has_holes || 1 + 2 * c->flt.nb < 12);
     // the kernels are a fixed choice (they round differently, and two contexts of one case give
     // the same bits): the scalar fused filter unless another is asked for
-    b.filter_vec = b.tma_filter && c->wfl_sym;
+    b.filter_vec = b.tma_filter && c->wfl_sym && !b.has_holes;
     b.filter_px = 0;
     if (c->filter_kernel >= 0 && b.tma_filter) {
       int px[2];
@@ -415,7 +415,7 @@ int lee_prepare(lee_ctx* c) {
       uni &= is_const(b.cd_pb, b.cf_pb) && is_const(b.cd_rbi, b.cf_rbi) && !b.need_rho;
       for (auto& z : b.bnd) spg |= is_sponge(z.kind);
       b.traits = kTrTma | (jmf ? kTrJmField : 0) | (uni ? kTrUniform : 0) | (spg ? kTrSponge : 0);
-      b.stage_pair = c->comp && uni && b.nx % 2 == 0;
+      b.stage_pair = c->comp && uni && b.nx % 2 == 0 && !b.has_holes;
       b.stage_px = b.stage_pair ? 2 : 1;
       if (c->stage_kernel > 0) {
         if (c->stage_kernel != 1 && !(c->stage_kernel == 2 && b.stage_pair))

@@ -231,7 +231,7 @@ __device__ __forceinline__ void rk_update(const StageParams<T>& p, I l, const T 
     return;
   }
   const bool first = K::first(p), last = K::last(p);
-  const bool hole = !(TR & kTrTma) && p.iblank && p.iblank[l] == 1;
+  const bool hole = p.iblank && p.iblank[l] == 1;  // null on blocks without holes
 #pragma unroll
   for (int v = 0; v < V; ++v) {
     if (hole) {

@@ -1,4 +1,6 @@
-// TMA-staged, k-marching kernels for blocks without holes (sm_100a).
+// TMA-staged, k-marching kernels (sm_100a). On a block with holes the closure class of each
+// point along each direction comes from its closure code rather than its position, and the
+// RK update and the filter's output take the hole mask.
 //
 // Stage kernel: a CTA owns a 32 x 8 tile in (i, j) and marches along k through a
 // chunk of planes. Each plane of every state field arrives in shared memory as one
@@ -65,11 +67,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
   if (tid == 0) issue_upto(plo + NS - 1);
 
   const int c = (ty + H) * BX + (tx + HX);
-  // closure-class weights along xi and eta are fixed for a thread: kept in registers
+  // closure-class weights along xi and eta: fixed for a thread by its position (kept in
+  // registers), or on a block with holes read per plane from the closure codes
+  const bool holes = s.code[0] != nullptr;
   T wx[2 * H + 1], wy[2 * H + 1];
   {
-    const int cx = active ? cls_of(i, s.nx, H) : 0;
-    const int cy = active ? cls_of(j, s.ny, H) : 0;
+    const int cx = active && !holes ? cls_of(i, s.nx, H) : 0;
+    const int cy = active && !holes ? cls_of(j, s.ny, H) : 0;
 #pragma unroll
     for (int o = 0; o <= 2 * H; ++o) {
       wx[o] = P.w[cx][o];
@@ -111,12 +115,20 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
       return false;
     }
     if (active) {
+      if (holes) {
+        const int cx = cls_of_code(s.code[0][lk], H), cy = cls_of_code(s.code[1][lk], H);
+#pragma unroll
+        for (int o = 0; o <= 2 * H; ++o) {
+          wx[o] = P.w[cx][o];
+          wy[o] = P.w[cy][o];
+        }
+      }
       // ring slots of planes k-H..k+H; planes outside [plo, phi] map to a loaded plane and
       // carry zero weight (their closure-class weights are zero)
       int zoff[2 * H + 1];
       T wz[2 * H + 1];
       if (DIM == 3) {
-        const int cz = cls_of(k, s.nz, H);
+        const int cz = holes ? cls_of_code(s.code[2][lk], H) : cls_of(k, s.nz, H);
 #pragma unroll
         for (int o = -H; o <= H; ++o) {
           const int kk = min(max(k + o, plo), phi);
@@ -218,7 +230,9 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
   };
   if (tid == 0) issue_upto(plo + NSF - 1);
 
-  // closure-class weights along xi and eta are fixed for a thread: keep them in registers
+  // closure-class weights along xi and eta: fixed for a thread by its position (kept in
+  // registers), or on a block with holes read per plane from the closure codes
+  const bool holes = P.code[0] != nullptr;
   T wx[NQ], wy[NQ];
   {
     const int cx = cls_of(min(i, P.nx - 1), P.nx, P.nb);
@@ -229,6 +243,12 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
       wy[o] = P.w[cy][o];
     }
   }
+  // the class of a point of plane kp from its code (0 outside the block: those box values are
+  // the zero fill and feed nothing)
+  auto code_cls = [&](int d, int ii, int jj, int kp) -> int {
+    if (ii >= P.nx || jj < 0 || jj >= P.ny) return 0;
+    return cls_of_code(P.code[d][ii + (long long)P.nx * (jj + (long long)P.ny * kp)], P.nb);
+  };
   T uq[NQ], dq[HF + 1], xq[HF + 1], eq[INC ? HF + 1 : 1];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) uq[q] = T(0);
@@ -273,6 +293,14 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
         }
         __syncthreads();
       }
+      if (holes) {
+        const int cx = code_cls(0, i, j, p), cy = code_cls(1, i, j, p);
+#pragma unroll
+        for (int o = 0; o < NQ; ++o) {
+          wx[o] = P.w[cx][o];
+          wy[o] = P.w[cy][o];
+        }
+      }
       // F_xi on the thread's own row (kept in registers) and on its share of the eta halo rows
       const T* fc = box + (ty + HF) * BX + tx + HX;
       xc = fc[0];
@@ -284,9 +312,13 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
       for (int r = ty; r < 2 * HF; r += TY) {
         const int row = r < HF ? r : r + TY;
         const T* f = box + row * BX + tx + HX;
+        T wh[NQ];
+        const int ch = holes ? code_cls(0, i, j0 - HF + row, p) : -1;
+#pragma unroll
+        for (int o = 0; o < NQ; ++o) wh[o] = ch < 0 ? wx[o] : P.w[ch][o];
         T d = T(0);
 #pragma unroll
-        for (int o = -HF; o <= HF; ++o) d += wx[o + HF] * f[o];
+        for (int o = -HF; o <= HF; ++o) d += wh[o + HF] * f[o];
         u1[row * TX + tx] = COMP ? f[0] + d : d;
       }
       __syncthreads();
@@ -323,7 +355,7 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
     if (!fin) continue;
     T fz, x0, dsum;
     if (DIM == 3) {
-      const int cz = cls_of(k, P.nz, P.nb);
+      const int cz = holes ? code_cls(2, i, j, k) : cls_of(k, P.nz, P.nb);
       fz = T(0);
       if (cz == 0) {
         // interior plane: the loop-invariant interior weights
@@ -342,15 +374,16 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
     }
     const T e0 = INC ? (DIM == 3 ? eq[0] : ein) : ef;
     const long long l = lf;
+    const bool hole = P.iblank && P.iblank[l] == 1;  // temporal::iblank_correction
     if (!COMP) {
-      P.out[v][l] = (T(1) - P.blend) * x0 + P.blend * fz;
+      P.out[v][l] = hole ? T(0) : (T(1) - P.blend) * x0 + P.blend * fz;
     } else {
       const T D = DIM == 3 ? dsum + fz : dsum;
       const T t = P.blend * D + e0;
       const T sm = x0 + t;
       const T bb = sm - x0;
-      P.out[v][l] = sm;
-      P.comp[v][l] = (x0 - (sm - bb)) + (t - bb);
+      P.out[v][l] = hole ? T(0) : sm;
+      P.comp[v][l] = hole ? T(0) : (x0 - (sm - bb)) + (t - bb);
     }
   }
 }

@@ -21,9 +21,11 @@ template <typename T>
 struct TmaStageParams {
   StageParams<T> s;
   int tiles_x, k_chunk;
-  // derivative weights by closure class: 0 interior, 1..2 left rows, 3..4 right rows;
-  // offsets -2..2 from the point (the reference's stencil tables rewritten per class)
-  T w[5][5];
+  // derivative weights by closure class: 0 interior, 1..2 left rows, 3..4 right rows, 5 zero
+  // (a hole after a hole); offsets -2..2 from the point (the reference's stencil tables
+  // rewritten per class). On a block with holes (s.code set) each point's class along each
+  // direction comes from its closure code, else from its position.
+  T w[6][5];
   int* err;  // set when a bounded wait gives up
   unsigned long long wait_ns;  // limit of the waits on staged data (the drains keep the default)
 };
@@ -32,9 +34,13 @@ template <typename T>
 struct TmaFilterParams {
   int nx, ny, nz, V, tiles_x, k_chunk;
   int nb;  // class rows per line end: class 0 interior, 1..nb from the left, nb+1..2nb from the right
-  // filter weights by class (interior, left rows, right rows), offsets -hf..hf; the
-  // compensated form uses F - I
+  // filter weights by class (interior, left rows, right rows, then the zero class 1 + 2 nb of a
+  // hole after a hole), offsets -hf..hf; the compensated form uses F - I
   T w[1 + 2 * kTE][11];
+  // a block with holes: the filter's closure codes per direction (classes from them, not from
+  // positions) and the hole mask of the output; null otherwise
+  const int8_t* code[3];
+  const int* iblank;
   T blend;
   const T* err[kMaxVars];  // compensated: rounding error of the pre-filter state
   T* out[kMaxVars];

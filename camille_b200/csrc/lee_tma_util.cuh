@@ -83,5 +83,12 @@ __device__ __forceinline__ int cls_of(int pos, int n, int nb) {
   return pos < nb ? 1 + pos : (pos > n - 1 - nb ? 1 + nb + (n - 1 - pos) : 0);
 }
 
+// The same classes from a closure code (closure_codes on the host: 0 interior, 1 + r the left
+// row r, -(1 + r) the mirrored right row r, kCodeZero a zero value), the zero class 1 + 2 nb.
+__device__ __forceinline__ int cls_of_code(int code, int nb) {
+  if (code == kCodeZero) return 1 + 2 * nb;
+  return code >= 0 ? code : 1 + nb + (-code - 1);
+}
+
 }  // namespace
 }  // namespace lee

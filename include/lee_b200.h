@@ -318,7 +318,8 @@ int lee_set_block_streams(lee_ctx *ctx, int on);
  * increment alone and the fused filter forms y_pre = y_n + increment and its rounding error
  * itself: 2V fewer words of 4 bytes per point and step, but the filter then stages y_n and the
  * increment with their halos (twice the shared memory per plane), which costs it more time than
- * the stage saves on the B200. Off (default): the last stage writes y_pre and its error. */
+ * the stage saves on the B200. Off (default): the last stage writes y_pre and its error. On before
+ * lee_prepare also keeps the fused filter to its one-row form (the form that takes the increment). */
 int lee_set_increment_step(lee_ctx *ctx, int on);
 int lee_set_batching(lee_ctx *ctx, int on);
 /* Failure detection (no reference counterpart: camille keeps going on NaN, and its waits are MPI
