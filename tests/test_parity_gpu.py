@@ -232,11 +232,15 @@ def test_overset_maps_are_bit_exact(product_lib, name):
 def test_overset_fp64_steps(product_lib, name):
     """holes2d / holes3d: a hole after fluid (no closure, the reference's `last_iblank /=
     BLANKED`), after a receiver (right closure), after a hole (zero), fluid and receivers after a
-    hole (left closure), holes at line starts and ends, along every direction."""
+    hole (left closure), holes at line starts and ends, along every direction; through the
+    TMA-staged kernels."""
     g = load_golden(name)
     case = _overset_golden(name)
     nb = len(case.blocks)
     s = api.Solver(product_lib, case)
+    # the hole blocks run the TMA-staged kernels, their closure classes from the closure codes
+    info = s.info()
+    assert info.tma_stage == 1 and info.tma_filter == 1
     dt = float(g["dt"])
     assert abs(s.compute_dt() - dt) <= 1e-14 * dt
     for b in range(nb):
