@@ -25,7 +25,21 @@ from tests.conftest import golden_case
 pytestmark = pytest.mark.gpu
 
 DOT_CASES = ["shear2d_40x32", "wall3d_14", "waves2d_40x32", "jet3d_14", "axisym2d_48x32", "cylinder2d_64",
-             "holes2d", "holes3d", "curvi3d_16"]
+             "holes2d", "holes3d", "curvi3d_16", "holes2d_rk2_nofilter", "cylinder2d_64_filter4_blend"]
+
+
+def _dot_case(name):
+    """A golden workload, or one of two variants: the 2-D hole layout with RK2 and no filter (the
+    hole mask then acts alone), and the cylinder with the 4th-order filter blended at 0.6."""
+    if name == "holes2d_rk2_nofilter":
+        case = golden_case("holes2d")
+        case.rk, case.filter_scheme = "RUNGE_KUTTA2", "NONE"
+        return case
+    if name == "cylinder2d_64_filter4_blend":
+        case = golden_case("cylinder2d_64")
+        case.filter_order, case.filter_blend = 4, 0.6
+        return case
+    return golden_case(name)
 
 
 def _fields(case, rng):
@@ -60,7 +74,7 @@ def _adjoint(s, case, lam, nsteps, dt):
 @pytest.mark.parametrize("nsteps", [1, 4])
 @pytest.mark.parametrize("name", DOT_CASES)
 def test_dot_product(product_lib, name, nsteps):
-    case = golden_case(name)
+    case = _dot_case(name)
     rng = np.random.default_rng(17)
     x = _fields(case, rng)
     lam = _fields(case, rng)
