@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(128, 3)
   constexpr int HX = Box<T, H>::HX, BX = Box<T, H>::BX;
   constexpr int FB = Box<T, H>::FB, FBP = Box<T, H>::FBP;
   constexpr int NS = DIM == 3 ? 2 * H + 1 + StagePrefetch<T>::P : 1;
+  static_assert(DIM == 2 || NS >= 2 * H + 2, "one barrier per plane needs a slot beyond the stencil");
   constexpr int PLANE = V * FBP;
   constexpr int LX = TX / 2;  // threads per row
   static_assert(HX % 2 == 0 && BX % 2 == 0, "pairs start on 8 bytes");
@@ -149,6 +150,11 @@ __global__ void __launch_bounds__(128, 3)
       }
       return false;
     }
+    // every thread is past plane k-1, so the slot of plane k-1-H is free and takes the plane
+    // NS ahead (the planes a barrier at the end of each plane would issue, one barrier per plane
+    // fewer); with NS >= 2H+2 every plane up to k+H was issued at plane k-1, and the last plane
+    // of the chunk issues nothing that it does not wait for
+    if (DIM == 3 && tid == 0) issue_upto(k - H + NS - 1);
     if (active) {
       int zoff[2 * H + 1];
       F2 wz[2 * H + 1];
@@ -282,8 +288,6 @@ __global__ void __launch_bounds__(128, 3)
         }
       }
     }
-    __syncthreads();
-    if (DIM == 3 && tid == 0) issue_upto(k + 1 - H + NS - 1);
     sk = sk + 1 == NS ? 0 : sk + 1;
     return true;
   };

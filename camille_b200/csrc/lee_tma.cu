@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
   constexpr int FB = Box<T, H>::FB;    // elements one box load writes
   constexpr int FBP = Box<T, H>::FBP;  // stride between boxes in shared memory
   constexpr int NS = DIM == 3 ? 2 * H + 1 + StagePrefetch<T>::P : 1;
+  static_assert(DIM == 2 || NS >= 2 * H + 2, "one barrier per plane needs a slot beyond the stencil");
   constexpr int PLANE = V * FBP;
   extern __shared__ __align__(128) unsigned char smem[];
   T* ring = reinterpret_cast<T*>(smem);
@@ -114,6 +115,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
       }
       return false;
     }
+    // every thread is past plane k-1, so the slot of plane k-1-H is free and takes the plane
+    // NS ahead; with NS >= 2H+2 every plane up to k+H was issued at plane k-1, and the last
+    // plane of the chunk issues nothing that it does not wait for
+    if (DIM == 3 && tid == 0) issue_upto(k - H + NS - 1);
     if (active) {
       if (holes) {
         const int cx = cls_of_code(s.code[0][lk], H), cy = cls_of_code(s.code[1][lk], H);
@@ -163,8 +168,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
       }
       rhs_update<T, DIM, COMP, TR>(s, lk, i, j, k, D, q, cur);
     }
-    __syncthreads();
-    if (DIM == 3 && tid == 0) issue_upto(k + 1 - H + NS - 1);
     sk = sk + 1 == NS ? 0 : sk + 1;
     return true;
   };
@@ -189,11 +192,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 // y_pre), and the rest is the filter of y_pre with its error: the same bits as the pair written by
 // the last stage, with one read of y_n in place of the last stage's read of y_n and writes of
 // y_pre and its error.
-template <typename T, int DIM, bool COMP, int HF, bool INC = false>
+template <typename T, int DIM, bool COMP, int HF, bool INC = false, bool HOLES = false>
 __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ FieldMaps ym,
                                                     const __grid_constant__ FieldMaps dm,
                                                     const __grid_constant__ TmaFilterParams<T> P) {
   static_assert(!INC || COMP, "the increment input is the compensated form's");
+  static_assert(!(INC && HOLES), "the increment input is not taken on blocks with holes");
   constexpr int NB = INC ? 2 : 1;  // boxes per ring slot
   constexpr int TX = kTileX, TY = kTileY, NQ = 2 * HF + 1, NSF = kFilterSlots;
   constexpr int HX = Box<T, HF>::HX, BX = Box<T, HF>::BX, BY = Box<T, HF>::BY;
@@ -231,8 +235,9 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
   if (tid == 0) issue_upto(plo + NSF - 1);
 
   // closure-class weights along xi and eta: fixed for a thread by its position (kept in
-  // registers), or on a block with holes read per plane from the closure codes
-  const bool holes = P.code[0] != nullptr;
+  // registers), or on a block with holes (HOLES: P.code and P.iblank set) read per plane from
+  // the closure codes; the form without holes keeps none of that code
+  constexpr bool holes = HOLES;
   T wx[NQ], wy[NQ];
   {
     const int cx = cls_of(min(i, P.nx - 1), P.nx, P.nb);
@@ -374,7 +379,7 @@ __global__ void __launch_bounds__(256) k_filter_tma_row(const __grid_constant__ 
     }
     const T e0 = INC ? (DIM == 3 ? eq[0] : ein) : ef;
     const long long l = lf;
-    const bool hole = P.iblank && P.iblank[l] == 1;  // temporal::iblank_correction
+    const bool hole = HOLES && P.iblank[l] == 1;  // temporal::iblank_correction
     if (!COMP) {
       P.out[v][l] = hole ? T(0) : (T(1) - P.blend) * x0 + P.blend * fz;
     } else {
@@ -624,7 +629,12 @@ cudaError_t go_stage_tr(const FieldMaps& z, const TmaStageParams<T>& p, int tr, 
 
 template <typename T, int DIM, bool COMP, int HF>
 cudaError_t go_filter(const FieldMaps& in, const TmaFilterParams<T>& p, int ry, int tiles, int chunks, cudaStream_t s) {
-  if (ry == 2) {
+  if (p.code[0]) {
+    // a block with holes: the one-row form with per-point classes and the hole mask
+    if (ry != 1 || !p.iblank) return cudaErrorInvalidValue;
+    k_filter_tma_row<T, DIM, COMP, HF, false, true><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 1>(), s>>>(
+        in, in, p);
+  } else if (ry == 2) {
     k_filter_tma<T, DIM, COMP, HF, 2><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 2>(), s>>>(in, p);
   } else {
     k_filter_tma_row<T, DIM, COMP, HF><<<dim3(tiles, chunks, p.V), 256, filter_smem<T, HF, 1>(), s>>>(in, in, p);
