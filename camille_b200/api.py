@@ -111,6 +111,7 @@ SIGNATURES = {
     "set_wait_limit": (C.c_int, [C.c_void_p, C.c_double]),
     "set_filter_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "set_stage_kernel": (C.c_int, [C.c_void_p, C.c_int]),
+    "set_filter_form": (C.c_int, [C.c_void_p, C.c_int]),
     "set_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _LP, C.c_double]),
     "eval_objective": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _DP]),
     "apply_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
@@ -164,11 +165,12 @@ class Solver:
 
     def __init__(self, lib: Library, case: "_cases.Case", precision: int = FP64, device: int = 0,
                  upload: bool = True, overset_file: Optional[str] = None, filter_kernel: int = -1,
-                 stage_kernel: int = -1, prepare: bool = True, batching: bool = True):
+                 stage_kernel: int = -1, prepare: bool = True, batching: bool = True, filter_form: int = 0):
         """``overset_file``: read the case's overset maps from this Overture-format file
         (lee_read_overset_file) instead of passing the arrays (lee_set_overset).
         ``filter_kernel``: lee_set_filter_kernel (-1/0 scalar, 2/4 vector width);
-        ``stage_kernel``: lee_set_stage_kernel (-1 default, 1 or 2 points per thread).
+        ``stage_kernel``: lee_set_stage_kernel (-1 default, 1 or 2 points per thread);
+        ``filter_form``: lee_set_filter_form (0 timed, else the scalar fused filter's form 1 or 2).
         ``batching=False``: lee_set_batching(0), every block runs its own kernels;
         ``prepare=False`` stops before lee_prepare (nothing is uploaded)."""
         self.lib = lib
@@ -234,6 +236,8 @@ class Solver:
                 self._chk(lib.set_filter_kernel(self.ctx, filter_kernel))
             if stage_kernel != -1:
                 self._chk(lib.set_stage_kernel(self.ctx, stage_kernel))
+            if filter_form:
+                self._chk(lib.set_filter_form(self.ctx, filter_form))
             if not batching:
                 self._chk(lib.set_batching(self.ctx, 0))
             if not prepare:

@@ -511,6 +511,14 @@ int lee_set_stage_kernel(lee_ctx* c, int kind) {
   return LEE_OK;
 }
 
+int lee_set_filter_form(lee_ctx* c, int form) {
+  if (!c) return LEE_ERR_ARG;
+  if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_filter_form before lee_prepare");
+  if (form < 0 || form > 2) return fail(c, LEE_ERR_ARG, "filter form %d", form);
+  c->filter_form = form;
+  return LEE_OK;
+}
+
 int lee_set_filter_kernel(lee_ctx* c, int kind) {
   if (!c) return LEE_ERR_ARG;
   if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_filter_kernel before lee_prepare");

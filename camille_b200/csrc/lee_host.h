@@ -165,6 +165,7 @@ struct lee_ctx {
   bool wfl_sym = false;  // symmetric interior filter stencil: the vectorised filter kernel applies
   int filter_kernel = -1;  // lee_set_filter_kernel: -1/0 scalar, else vector group width
   int stage_kernel = -1;   // lee_set_stage_kernel: -1 default, else points per thread
+  int filter_form = 0;     // lee_set_filter_form: 0 timed at setup, else the scalar filter's form
   // blocks of a multi-block context run their stage and filter launches on side streams, forked
   // from the context stream and joined before whatever couples the blocks (overset, the clock)
   bool concurrent = true;       // lee_set_block_streams

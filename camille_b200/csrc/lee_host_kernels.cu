@@ -257,15 +257,18 @@ int autotune(lee_ctx* c, BlockData& b) {
     int best_chunk = b.nz, best_kind = which == 0 ? b.stage_px : b.filter_px, best_ry = b.filter_ry;
     // the scalar filter's forms (one or two tile rows per thread row) are timed with the chunk:
     // each point's arithmetic is the same in both
-    const int nry = which == 1 ? 2 : 1;
+    const int nry = which == 1 && c->filter_form == 0 ? 2 : 1;
     for (int kq = 0; kq < (which == 1 ? nkinds : nskinds) * nry; ++kq) {
       if (which == 0) {
         b.stage_px = skinds[kq];
       } else {
         b.filter_px = kinds[kq / nry];
-        b.filter_ry = 1 + kq % nry;
-        // the one-row form alone takes holes and the increment step's input
-        if ((b.filter_px > 0 || b.has_holes || (c->comp && c->increment_step)) && b.filter_ry > 1) continue;
+        b.filter_ry = c->filter_form > 0 ? c->filter_form : 1 + kq % nry;
+        // the one-row form alone takes holes and the increment step's input (a form set by
+        // lee_set_filter_form is kept, and the increment step then does not apply)
+        if (c->filter_form == 0 && (b.filter_px > 0 || b.has_holes || (c->comp && c->increment_step)) &&
+            b.filter_ry > 1)
+          continue;
         set_filter_tiles(c, b);
       }
       for (int ch : (d3 ? std::vector<int>(std::begin(cands3), std::end(cands3))

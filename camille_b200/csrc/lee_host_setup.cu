@@ -400,6 +400,14 @@ int lee_prepare(lee_ctx* c) {
                     (int)(&b - c->blk.data()));
       b.filter_px = c->filter_kernel;
     }
+    b.filter_ry = 1;
+    if (c->filter_form > 0 && b.tma_filter) {
+      // the two-row form takes neither holes nor the vector kernel's groups
+      if (c->filter_form > 1 && (b.filter_px > 0 || b.has_holes))
+        return fail(c, LEE_ERR_UNSUPPORTED, "filter form %d is not available for block %d", c->filter_form,
+                    (int)(&b - c->blk.data()));
+      b.filter_ry = c->filter_form;
+    }
     set_filter_tiles(c, b);
     if (b.tma) {
       // coefficient-layout traits of the stage kernel

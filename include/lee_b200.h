@@ -282,7 +282,7 @@ typedef struct {
   int batch_filter_tile[2];  /* picked by timing the candidates at lee_prepare */
   int filter_kernel;         /* fused filter of block 0: 0 scalar, else the vector group width */
   int stage_kernel;          /* TMA stage kernel of block 0: points per thread */
-  int filter_rows;           /* scalar fused filter of block 0: tile rows per thread row (1 or 2) */
+  int filter_rows;           /* scalar fused filter of block 0: its form (lee_set_filter_form) */
   int increment_step;        /* 1 when every block's compensated step hands the increment to the filter */
 } lee_info;
 int lee_get_info(lee_ctx *ctx, lee_info *info);
@@ -340,6 +340,12 @@ int lee_set_wait_limit(lee_ctx *ctx, double seconds);
  * points along xi (4: FP32 only). LEE_ERR_UNSUPPORTED from lee_prepare when a block cannot run the
  * choice. Call before lee_prepare. */
 int lee_set_filter_kernel(lee_ctx *ctx, int kind);
+/* Form of the scalar fused filter (no reference counterpart; both forms give the same bits):
+ * 0 (default) the faster form, timed at lee_prepare; 1 one tile row per thread on tiles of 8
+ * rows; 2 two rows per thread on tiles of 16 rows. Form 2 takes no block with holes and not the
+ * vector kernel (LEE_ERR_UNSUPPORTED from lee_prepare), and with it the increment step does not
+ * apply. Call before lee_prepare. */
+int lee_set_filter_form(lee_ctx *ctx, int form);
 /* Kernel of the RK stages on blocks that run the TMA stage kernel (no reference counterpart;
  * results agree to rounding): 1 one point per thread, 2 two neighbouring points per thread with
  * packed FP32 arithmetic (compensated form, uniform mean flow, even nxi); -1 (default) takes 2

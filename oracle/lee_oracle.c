@@ -1499,6 +1499,12 @@ int orc_set_filter_kernel(orc_ctx *c, int kind) {
   return LEE_OK; /* one filter path */
 }
 
+int orc_set_filter_form(orc_ctx *c, int form) {
+  (void)c;
+  (void)form;
+  return LEE_OK; /* one filter path */
+}
+
 int orc_set_graphs(orc_ctx *c, int on) {
   (void)c; (void)on;
   return LEE_OK;

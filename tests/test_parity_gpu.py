@@ -187,6 +187,39 @@ def test_filter_across_tiles(product_lib, oracle_lib, label, precision, kernel):
 
 
 @pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+@pytest.mark.parametrize("label", ["curvi3d_136", "sfo11p_3d_72", "pulse2d_520", "filter4_3d_68"])
+def test_filter_forms_same_bits(product_lib, oracle_lib, label, precision):
+    """The two forms of the scalar fused filter (one row per thread on 8-row tiles, two rows per
+    thread on 16-row tiles) do the same arithmetic per point: identical bits, within 1e-13 (FP64)
+    or 1e-6 (compensated) of the oracle, and the same bits again after two RK steps with each
+    form."""
+    case = _wide()[label]
+    out, steps = [], []
+    for form in (1, 2):
+        p = api.Solver(product_lib, case, precision=precision, filter_kernel=0, filter_form=form)
+        assert p.info().filter_rows == form
+        p.apply_filter()
+        out.append(p.download(0)[0])
+        q = api.Solver(product_lib, case, precision=precision, filter_kernel=0, filter_form=form)
+        dt = q.compute_dt()
+        q.advance(2, dt)
+        steps.append(q.download(0)[0])
+    tol = 1e-13 if precision == api.FP64 else 1e-6
+    assert rl2(out[0], _oracle_filtered(oracle_lib, label)) <= tol
+    np.testing.assert_array_equal(out[1], out[0])
+    np.testing.assert_array_equal(steps[1], steps[0])
+
+
+def test_filter_form_refusals(product_lib):
+    """The two-row form takes no block with holes and not the vector kernel's groups."""
+    with pytest.raises(api.LeeError, match="filter form"):
+        api.Solver(product_lib, cases.holes(2, nsteps=1), filter_form=2)
+    with pytest.raises(api.LeeError, match="filter form"):
+        api.Solver(product_lib, cases.curvi3d(n=40, nsteps=1, halfwidth=3.0), precision=api.FP32_COMPENSATED,
+                   filter_kernel=4, filter_form=2)
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
 def test_rho_ratio_follows_the_pre_filter_state(product_lib, oracle_lib, precision):
     """With a sheared mean the right-hand side reads rho'/rho_bar, which the reference
     recomputes after each boundary update and not after the filter: a right-hand side taken
