@@ -463,6 +463,12 @@ def run_adjoint(args, lib, barrier, max_over_ranks) -> dict:
     s = api.Solver(lib, case, precision=api.FP32_COMPENSATED)
     dt = s.compute_dt()
     s.eval_objective(min(N, 20), dt)  # warm-up: graph capture, traces
+    # warm-up of the gradient: as many checkpoint segments as the timed calls (the checkpoint
+    # buffers are allocated on first use) and the reverse step's graphs, both modes
+    nseg = max(1, -(-N // 100))
+    for rec in (True, False):
+        s.upload(0, case.blocks[0].state)
+        s.adjoint_gradient(min(N, 10 * nseg), dt, checkpoint_every=10, recompute=rec)
     out = {"workload": f"adjoint3d {n}^3 Mach 0.5, 16^3 distributed source (seed 5), 64 microphones, "
                        f"{N} FP32-compensated RK4 steps, checkpoint every 100",
            "steps": N}
