@@ -309,7 +309,7 @@ def run_ours(args) -> None:
     clocks = None
     for form, prec in (("fp32c", api.FP32_COMPENSATED), ("fp64", api.FP64)):
         kinds = {"filter_kernel": args.filter_kernel} if form == "fp32c" or args.filter_kernel in (-1, 0, 2) else {}
-        if args.filter_form:
+        if args.filter_form and (form == "fp32c" or args.filter_form < 3):
             kinds["filter_form"] = args.filter_form
         s = api.Solver(lib, case, precision=prec, device=local, stage_kernel=args.stage_kernel if form == "fp32c" else -1,
                        **kinds)
@@ -595,7 +595,8 @@ def main() -> int:
     ap.add_argument("--filter-kernel", type=int, default=-1,
                     help="lee_set_filter_kernel for the run (-1: the library's default; 2, 4: the vectorised filter)")
     ap.add_argument("--filter-form", type=int, default=0,
-                    help="lee_set_filter_form for both runs (0: timed at setup; 1, 2: one or two rows per thread)")
+                    help="lee_set_filter_form (0: timed at setup; 1, 2: one or two rows per thread, both runs; "
+                         "3: two points per thread, the FP32-compensated run)")
     ap.add_argument("--stage-kernel", type=int, default=-1,
                     help="lee_set_stage_kernel for the FP32-compensated run (-1: the library's default)")
     ap.add_argument("--batch-steps", type=int, default=200)

@@ -170,7 +170,7 @@ class Solver:
         (lee_read_overset_file) instead of passing the arrays (lee_set_overset).
         ``filter_kernel``: lee_set_filter_kernel (-1/0 scalar, 2/4 vector width);
         ``stage_kernel``: lee_set_stage_kernel (-1 default, 1 or 2 points per thread);
-        ``filter_form``: lee_set_filter_form (0 timed, else the scalar fused filter's form 1 or 2).
+        ``filter_form``: lee_set_filter_form (0 timed, else the scalar fused filter's form 1, 2 or 3).
         ``batching=False``: lee_set_batching(0), every block runs its own kernels;
         ``prepare=False`` stops before lee_prepare (nothing is uploaded)."""
         self.lib = lib

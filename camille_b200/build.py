@@ -37,6 +37,7 @@ UNITS = {
     "lee_adjoint.cu": [],
     "lee_batch.cu": [],
     "lee_filter.cu": [],
+    "lee_filter_pair.cu": [],
     "lee_stage_pair.cu": [],
     "lee_adjoint_tma.cu": [],
     "lee_adjoint_gen.cu": [],

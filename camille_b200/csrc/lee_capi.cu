@@ -492,7 +492,7 @@ int lee_get_info(lee_ctx* c, lee_info* info) {
   info->filter_chunk = c->blk.empty() ? 0 : c->blk[0].filter_chunk;
   info->filter_kernel = c->blk.empty() ? 0 : c->blk[0].filter_px;
   info->stage_kernel = c->blk.empty() ? 0 : c->blk[0].stage_px;
-  info->filter_rows = c->blk.empty() ? 0 : c->blk[0].filter_ry;
+  info->filter_rows = c->blk.empty() ? 0 : (c->blk[0].filter_pair ? 3 : c->blk[0].filter_ry);
   info->increment_step = c->blk.empty() ? 0 : 1;
   for (const auto& b : c->blk) info->increment_step &= increment_step_applies(c, b) ? 1 : 0;
   info->batched = c->batch.active ? 1 : 0;
@@ -514,7 +514,7 @@ int lee_set_stage_kernel(lee_ctx* c, int kind) {
 int lee_set_filter_form(lee_ctx* c, int form) {
   if (!c) return LEE_ERR_ARG;
   if (c->prepared) return fail(c, LEE_ERR_STATE, "lee_set_filter_form before lee_prepare");
-  if (form < 0 || form > 2) return fail(c, LEE_ERR_ARG, "filter form %d", form);
+  if (form < 0 || form > 3) return fail(c, LEE_ERR_ARG, "filter form %d", form);
   c->filter_form = form;
   return LEE_OK;
 }

@@ -92,6 +92,9 @@ struct BlockData {
   int tiles_x = 0, tiles_y = 0;
   int stage_chunk = 0, filter_chunk = 0;
   int filter_ry = 1;                  // rows per thread row of the scalar fused filter (1 or 2)
+  bool filter_pair_ok = false;        // the two-point compensated filter (lee_filter_pair.cu) applies
+  bool filter_pair = false;           // ... and runs the block's fused filter (form 3)
+  int ptiles_x = 0, ptiles_y = 0;     // its tiles
   // passive scalars (LEE_SCALAR): mean fields and their gradients, and the slots' buffers with
   // the LEE slots' roles (y, acc, two stage buffers, carried error, filter increments) plus a
   // filter scratch; fixed roles, nothing swaps

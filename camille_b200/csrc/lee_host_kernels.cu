@@ -105,7 +105,8 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
 
 bool increment_step_applies(const lee_ctx* c, const BlockData& b) {
   if (!c->comp || !c->increment_step || c->batch.active || c->ovs.n > 0 || b.has_holes) return false;
-  if (c->cfg.filter_scheme == LEE_FILTER_NONE || !b.tma || !b.tma_filter || b.filter_px > 0 || b.filter_ry != 1)
+  if (c->cfg.filter_scheme == LEE_FILTER_NONE || !b.tma || !b.tma_filter || b.filter_px > 0 || b.filter_ry != 1 ||
+      b.filter_pair)
     return false;
   if (b.need_rho) return false;  // rho'/rho_bar is formed from y_pre after the last stage
   for (const auto& z : b.bnd)
@@ -130,8 +131,14 @@ int filter_tiles(const BlockData& b) {
   return b.tiles_x * ((b.ny + ty - 1) / ty);
 }
 
-// Tiles of the vectorised filter at the block's group width.
+// Tiles of the vectorised filter at the block's group width, and of the two-point filter.
 void set_filter_tiles(const lee_ctx* c, BlockData& b) {
+  if (b.filter_pair_ok) {
+    int bx, by, tx, ty;
+    filter_pair_box(c->hf, &bx, &by, &tx, &ty);
+    b.ptiles_x = (b.nx + tx - 1) / tx;
+    b.ptiles_y = (b.ny + ty - 1) / ty;
+  }
   if (b.filter_px <= 0) return;
   int bx, by, tx, ty;
   filter_vec_box(c->esz, c->hf, b.filter_px, &bx, &by, &tx, &ty);
@@ -200,7 +207,11 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
   fp.errflag = c->d_err;
   fp.wait_ns = c->wait_ns;
   int bx, by, tx, ty;
-  if (b.filter_px > 0) {
+  const bool pair = b.filter_pair && !inc;
+  if (pair) {
+    filter_pair_box(c->hf, &bx, &by, &tx, &ty);
+    fp.tiles_x = b.ptiles_x;
+  } else if (b.filter_px > 0) {
     filter_vec_box(c->esz, c->hf, b.filter_px, &bx, &by, &tx, &ty);
     fp.tiles_x = b.vtiles_x;
   } else {
@@ -218,6 +229,12 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
       CK(launch_filter_tma_inc(fm, im, fp, c->hf, c->cfg.num_dim, filter_tiles(b), chunks, c->stream));
     } else {
       return fail(c, LEE_ERR_UNSUPPORTED, "the increment step is the compensated form's");
+    }
+  } else if (pair) {
+    if constexpr (sizeof(T) == 4) {
+      CK(launch_filter_pair(fm, fp, c->hf, b.ptiles_x * b.ptiles_y, chunks, c->stream));
+    } else {
+      return fail(c, LEE_ERR_UNSUPPORTED, "the two-point filter is the compensated form's");
     }
   } else if (b.filter_px > 0) {
     CK(launch_filter_vec<T>(fm, fp, c->hf, b.filter_px, c->cfg.num_dim, b.vtiles_x * b.vtiles_y, chunks, c->stream));
@@ -255,20 +272,23 @@ int autotune(lee_ctx* c, BlockData& b) {
     if (which == 0 && !d3 && nskinds == 1) continue;  // nothing to choose
     float best = 1e30f;
     int best_chunk = b.nz, best_kind = which == 0 ? b.stage_px : b.filter_px, best_ry = b.filter_ry;
-    // the scalar filter's forms (one or two tile rows per thread row) are timed with the chunk:
-    // each point's arithmetic is the same in both
-    const int nry = which == 1 && c->filter_form == 0 ? 2 : 1;
+    bool best_pair = b.filter_pair;
+    // the scalar filter's forms (1: one tile row per thread row, 2: two rows, 3: two points per
+    // thread) are timed with the chunk: each point's arithmetic is the same in all three
+    const int nry = which == 1 && c->filter_form == 0 ? 3 : 1;
     for (int kq = 0; kq < (which == 1 ? nkinds : nskinds) * nry; ++kq) {
       if (which == 0) {
         b.stage_px = skinds[kq];
       } else {
         b.filter_px = kinds[kq / nry];
-        b.filter_ry = c->filter_form > 0 ? c->filter_form : 1 + kq % nry;
+        const int form = c->filter_form > 0 ? c->filter_form : 1 + kq % nry;
         // the one-row form alone takes holes and the increment step's input (a form set by
         // lee_set_filter_form is kept, and the increment step then does not apply)
-        if (c->filter_form == 0 && (b.filter_px > 0 || b.has_holes || (c->comp && c->increment_step)) &&
-            b.filter_ry > 1)
+        if (c->filter_form == 0 && (b.filter_px > 0 || b.has_holes || (c->comp && c->increment_step)) && form > 1)
           continue;
+        if (form == 3 && !b.filter_pair_ok) continue;
+        b.filter_ry = form == 2 ? 2 : 1;
+        b.filter_pair = form == 3;
         set_filter_tiles(c, b);
       }
       for (int ch : (d3 ? std::vector<int>(std::begin(cands3), std::end(cands3))
@@ -311,6 +331,7 @@ int autotune(lee_ctx* c, BlockData& b) {
           best_chunk = d3 ? ch : b.nz;
           best_kind = which == 0 ? b.stage_px : b.filter_px;
           best_ry = b.filter_ry;
+          best_pair = b.filter_pair;
         }
       }
     }
@@ -321,6 +342,7 @@ int autotune(lee_ctx* c, BlockData& b) {
       b.filter_chunk = best_chunk;
       b.filter_px = best_kind;
       b.filter_ry = best_ry;
+      b.filter_pair = best_pair;
       set_filter_tiles(c, b);
     }
   }

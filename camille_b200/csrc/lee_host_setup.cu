@@ -401,12 +401,17 @@ int lee_prepare(lee_ctx* c) {
       b.filter_px = c->filter_kernel;
     }
     b.filter_ry = 1;
+    // the two-point form: compensated FP32, 3-D, no holes, even nxi, the scalar kernel's place
+    b.filter_pair_ok = b.tma_filter && c->comp && c->cfg.num_dim == 3 && !b.has_holes && b.nx % 2 == 0 &&
+                       b.filter_px == 0 && filter_pair_half_width(c->hf);
+    b.filter_pair = false;
     if (c->filter_form > 0 && b.tma_filter) {
-      // the two-row form takes neither holes nor the vector kernel's groups
-      if (c->filter_form > 1 && (b.filter_px > 0 || b.has_holes))
+      // the two-row and two-point forms take neither holes nor the vector kernel's groups
+      if ((c->filter_form == 2 && (b.filter_px > 0 || b.has_holes)) || (c->filter_form == 3 && !b.filter_pair_ok))
         return fail(c, LEE_ERR_UNSUPPORTED, "filter form %d is not available for block %d", c->filter_form,
                     (int)(&b - c->blk.data()));
-      b.filter_ry = c->filter_form;
+      b.filter_ry = c->filter_form == 2 ? 2 : 1;
+      b.filter_pair = c->filter_form == 3;
     }
     set_filter_tiles(c, b);
     if (b.tma) {

@@ -340,11 +340,13 @@ int lee_set_wait_limit(lee_ctx *ctx, double seconds);
  * points along xi (4: FP32 only). LEE_ERR_UNSUPPORTED from lee_prepare when a block cannot run the
  * choice. Call before lee_prepare. */
 int lee_set_filter_kernel(lee_ctx *ctx, int kind);
-/* Form of the scalar fused filter (no reference counterpart; both forms give the same bits):
- * 0 (default) the faster form, timed at lee_prepare; 1 one tile row per thread on tiles of 8
- * rows; 2 two rows per thread on tiles of 16 rows. Form 2 takes no block with holes and not the
- * vector kernel (LEE_ERR_UNSUPPORTED from lee_prepare), and with it the increment step does not
- * apply. Call before lee_prepare. */
+/* Form of the scalar fused filter (no reference counterpart; all forms give the same bits):
+ * 0 (default) the fastest form, timed at lee_prepare; 1 one tile row per thread on tiles of 8
+ * rows; 2 two rows per thread on tiles of 16 rows; 3 two neighbouring points per thread along xi
+ * on tiles of 64 x 8 points (packed FP32 arithmetic: the compensated form on 3-D blocks of even
+ * nxi). Forms 2 and 3 take no block with holes and not the vector kernel, form 3 nothing else
+ * than its own case (LEE_ERR_UNSUPPORTED from lee_prepare), and with either the increment step
+ * does not apply. Call before lee_prepare. */
 int lee_set_filter_form(lee_ctx *ctx, int form);
 /* Kernel of the RK stages on blocks that run the TMA stage kernel (no reference counterpart;
  * results agree to rounding): 1 one point per thread, 2 two neighbouring points per thread with

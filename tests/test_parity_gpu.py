@@ -189,13 +189,14 @@ def test_filter_across_tiles(product_lib, oracle_lib, label, precision, kernel):
 @pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
 @pytest.mark.parametrize("label", ["curvi3d_136", "sfo11p_3d_72", "pulse2d_520", "filter4_3d_68"])
 def test_filter_forms_same_bits(product_lib, oracle_lib, label, precision):
-    """The two forms of the scalar fused filter (one row per thread on 8-row tiles, two rows per
-    thread on 16-row tiles) do the same arithmetic per point: identical bits, within 1e-13 (FP64)
-    or 1e-6 (compensated) of the oracle, and the same bits again after two RK steps with each
-    form."""
+    """The forms of the scalar fused filter (one row per thread on 8-row tiles, two rows per
+    thread on 16-row tiles, and for the compensated form on 3-D blocks two points per thread on
+    64 x 8 tiles) do the same arithmetic per point: identical bits, within 1e-13 (FP64) or 1e-6
+    (compensated) of the oracle, and the same bits again after two RK steps with each form."""
     case = _wide()[label]
     out, steps = [], []
-    for form in (1, 2):
+    forms = (1, 2, 3) if precision == api.FP32_COMPENSATED and "3d" in label else (1, 2)
+    for form in forms:
         p = api.Solver(product_lib, case, precision=precision, filter_kernel=0, filter_form=form)
         assert p.info().filter_rows == form
         p.apply_filter()
@@ -206,12 +207,20 @@ def test_filter_forms_same_bits(product_lib, oracle_lib, label, precision):
         steps.append(q.download(0)[0])
     tol = 1e-13 if precision == api.FP64 else 1e-6
     assert rl2(out[0], _oracle_filtered(oracle_lib, label)) <= tol
-    np.testing.assert_array_equal(out[1], out[0])
-    np.testing.assert_array_equal(steps[1], steps[0])
+    for q in range(1, len(forms)):
+        np.testing.assert_array_equal(out[q], out[0])
+        np.testing.assert_array_equal(steps[q], steps[0])
 
 
 def test_filter_form_refusals(product_lib):
-    """The two-row form takes no block with holes and not the vector kernel's groups."""
+    """The two-row form takes no block with holes and not the vector kernel's groups; the
+    two-point form takes only compensated 3-D blocks without holes."""
+    with pytest.raises(api.LeeError, match="filter form"):
+        api.Solver(product_lib, cases.curvi3d(n=40, nsteps=1, halfwidth=3.0), precision=api.FP64, filter_form=3)
+    with pytest.raises(api.LeeError, match="filter form"):
+        api.Solver(product_lib, cases.pulse2d(n=48, nsteps=1), precision=api.FP32_COMPENSATED, filter_form=3)
+    with pytest.raises(api.LeeError, match="filter form"):
+        api.Solver(product_lib, cases.holes(3, nsteps=1), precision=api.FP32_COMPENSATED, filter_form=3)
     with pytest.raises(api.LeeError, match="filter form"):
         api.Solver(product_lib, cases.holes(2, nsteps=1), filter_form=2)
     with pytest.raises(api.LeeError, match="filter form"):
