@@ -4,9 +4,9 @@
 // xi, then eta, then zeta, and the blend with the pre-filter state follows. This kernel fuses the
 // three passes as k_filter_tma_row (lee_tma.cu) does, with each point's arithmetic in the same
 // order (the same bits), but every thread owns two neighbouring points along xi:
-//   - the pair's xi taps come from 8-byte shared-memory words, and the taps whose two values lie
-//     in one word, every eta and zeta tap and the blend run as packed FP32 instructions
-//     (__ffma2_rn, __fadd2_rn), one instruction for both points;
+//   - the pair's xi taps come from 8-byte shared-memory words, and the xi taps whose two values
+//     lie in one word run as packed FP32 instructions (__ffma2_rn, with the pair's two weights
+//     held in a register pair), as do the sums of pairs (__fadd2_rn);
 //   - the per-plane work (the wait on the plane's copy, the barrier, addressing) is shared by the
 //     two points, and the output moves in 8-byte words.
 //
@@ -35,11 +35,11 @@ namespace {
 
 using F2 = float2;
 
-__device__ __forceinline__ F2 f2(float x) { return make_float2(x, x); }
 __device__ __forceinline__ F2 add2(F2 a, F2 b) { return __fadd2_rn(a, b); }
-// a - b, exactly one rounding
-__device__ __forceinline__ F2 sub2(F2 a, F2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return __ffma2_rn(a, b, c); }
+// w * a + c and a - b lane by lane (scalar instructions)
+__device__ __forceinline__ F2 fmas(float w, F2 a, F2 c) { return make_float2(fmaf(w, a.x, c.x), fmaf(w, a.y, c.y)); }
+__device__ __forceinline__ F2 subs(F2 a, F2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ F2 ld2(const float* p) { return *reinterpret_cast<const F2*>(p); }
 __device__ __forceinline__ void st2(float* p, F2 v) { *reinterpret_cast<F2*>(p) = v; }
 
@@ -145,7 +145,6 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
   const float* errp = P.err[v];
   float* outp = P.out[v];
   float* cmpp = P.comp[v];
-  const F2 blend = f2(P.blend);
 
   F2 uq[NQ];
 #pragma unroll
@@ -194,14 +193,16 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
         return;
       }
       if (tid == 0) issue_upto(p + G::PF);
+      // (eta and zeta taps as two scalar FMAs whose weight is an operand from the constant bank:
+      // a packed FMA would first need the weight copied into both halves of a register pair)
       const float* col = u1 + (ty + HF) * kPairTX + 2 * tx;
       F2 dy = make_float2(0.f, 0.f);
       if (cy == 0) {
 #pragma unroll
-        for (int o = -HF; o <= HF; ++o) dy = fma2(f2(P.w[0][o + HF]), o == 0 ? u1c : ld2(col + o * kPairTX), dy);
+        for (int o = -HF; o <= HF; ++o) dy = fmas(P.w[0][o + HF], o == 0 ? u1c : ld2(col + o * kPairTX), dy);
       } else {
 #pragma unroll
-        for (int o = -HF; o <= HF; ++o) dy = fma2(f2(P.w[cy][o + HF]), o == 0 ? u1c : ld2(col + o * kPairTX), dy);
+        for (int o = -HF; o <= HF; ++o) dy = fmas(P.w[cy][o + HF], o == 0 ? u1c : ld2(col + o * kPairTX), dy);
       }
       u2 = add2(u1c, dy);
       d12 = add2(d1, dy);
@@ -216,18 +217,18 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
     F2 fz = make_float2(0.f, 0.f);
     if (cz == 0) {
 #pragma unroll
-      for (int o = 0; o < NQ; ++o) fz = fma2(f2(P.w[0][o]), uq[o], fz);
+      for (int o = 0; o < NQ; ++o) fz = fmas(P.w[0][o], uq[o], fz);
     } else {
 #pragma unroll
-      for (int o = 0; o < NQ; ++o) fz = fma2(f2(P.w[cz][o]), uq[o], fz);
+      for (int o = 0; o < NQ; ++o) fz = fmas(P.w[cz][o], uq[o], fz);
     }
     // the pre-filter pair of plane kf, still in its ring slot (kf >= plo)
     const F2 x0 = ld2(ring + ((rel - HF) % NS) * FBP + (ty + HF) * BX + c);
     const F2 D = add2(ld2(dme + ds * G::DP), fz);
-    const F2 t = fma2(blend, D, e0);
+    const F2 t = fmas(P.blend, D, e0);
     const F2 sm = add2(x0, t);
-    const F2 bb = sub2(sm, x0);
-    const F2 cm = add2(sub2(x0, sub2(sm, bb)), sub2(t, bb));
+    const F2 bb = subs(sm, x0);
+    const F2 cm = add2(subs(x0, subs(sm, bb)), subs(t, bb));
     st2(outp + lf, sm);
     st2(cmpp + lf, cm);
   }
