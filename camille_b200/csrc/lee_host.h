@@ -95,6 +95,7 @@ struct BlockData {
   bool filter_pair_ok = false;        // the two-point compensated filter (lee_filter_pair.cu) applies
   bool filter_pair = false;           // ... and runs the block's fused filter (form 3)
   int ptiles_x = 0, ptiles_y = 0;     // its tiles
+  int tfilter_ry = 1, tfilter_chunk = 0;  // the scalar form and chunk of the adjoint's transposed filter
   // passive scalars (LEE_SCALAR): mean fields and their gradients, and the slots' buffers with
   // the LEE slots' roles (y, acc, two stage buffers, carried error, filter increments) plus a
   // filter scratch; fixed roles, nothing swaps
@@ -331,6 +332,7 @@ int field_maps(lee_ctx* c, const BlockData& b, void* const* fields, int bx, int 
 int filter_form_rows(int form);
 int filter_box(const lee_ctx* c, int h, int form, int* bx, int* by);
 int filter_tiles(const BlockData& b);
+int filter_tiles_form(const BlockData& b, int ry);  // the scalar fused filter's tiles in form ry (1 or 2)
 void set_filter_tiles(const lee_ctx* c, BlockData& b);
 template <typename T>
 int launch_stage_any(lee_ctx* c, BlockData& b, const StageParams<T>& p, void* const* zin, int chunk_override = 0);

@@ -130,7 +130,9 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
     fp.nx = b.nx; fp.ny = b.ny; fp.nz = b.nz;
     fp.V = V;
     fp.tiles_x = b.tiles_x;
-    fp.k_chunk = b.filter_chunk;
+    // the scalar fused filter's form and chunk (the forward filter may run the two-point kernel)
+    const int ry = b.tfilter_ry;
+    fp.k_chunk = b.tfilter_chunk > 0 ? b.tfilter_chunk : (b.filter_chunk > 0 ? b.filter_chunk : b.nz);
     fp.nb = a.fT.E;
     const int H = a.fT.H;
     for (int o = 0; o <= 2 * H; ++o) {
@@ -145,12 +147,12 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
     fp.errflag = c->d_err;
     fp.wait_ns = c->wait_ns;
     int bx, by;
-    filter_box(c, H, b.filter_ry, &bx, &by);
+    filter_box(c, H, ry, &bx, &by);
     FieldMaps fm;
     int rc = field_maps(c, b, a.lam, bx, by, &fm);
     if (rc) return rc;
     const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
-    CK(launch_filter_tma<T>(fm, fp, H, c->cfg.num_dim, 0, b.filter_ry, filter_tiles(b), chunks, c->stream));
+    CK(launch_filter_tma<T>(fm, fp, H, c->cfg.num_dim, 0, ry, filter_tiles_form(b, ry), chunks, c->stream));
     c->stats.kernel_launches += 1;
     mu = a.mu;
   } else if (c->cfg.filter_scheme != LEE_FILTER_NONE) {

@@ -1,6 +1,7 @@
 // Kernel selection and launch: tensor maps of the TMA-staged kernels, the stage and filter
 // launches of one block (TMA, two-point or generic), the plane-chunk autotuner, boundary-line
 // and harmonic-wave updates, microphone traces, and the device error flag of the bounded waits.
+#include <algorithm>
 #include "lee_host.h"
 
 using namespace lee;
@@ -126,10 +127,12 @@ int filter_box(const lee_ctx* c, int h, int form, int* bx, int* by) {
   return LEE_OK;
 }
 
-int filter_tiles(const BlockData& b) {
-  const int ty = kTileY * filter_form_rows(b.filter_ry);
+int filter_tiles_form(const BlockData& b, int ry) {
+  const int ty = kTileY * filter_form_rows(ry);
   return b.tiles_x * ((b.ny + ty - 1) / ty);
 }
+
+int filter_tiles(const BlockData& b) { return filter_tiles_form(b, b.filter_ry); }
 
 // Tiles of the vectorised filter at the block's group width, and of the two-point filter.
 void set_filter_tiles(const lee_ctx* c, BlockData& b) {
@@ -256,8 +259,15 @@ template <typename T>
 int autotune(lee_ctx* c, BlockData& b) {
   if (!b.tma && !b.tma_filter) return LEE_OK;
   const bool d3 = c->cfg.num_dim == 3;
-  const int cands3[] = {8, 16, 24, 32, 48, 64, 96, 128, 192, 256};
-  const int cands2[] = {1};
+  // plane chunks: a fixed ladder (stage kernels), and for the filter also the near-equal splits
+  // of the block's planes into 1..24 chunks (ceil(nz / c): every chunk but the last of the same
+  // length, so that CTA counts that fill whole waves of the GPU are among the candidates)
+  const std::vector<int> ladder = {8, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+  std::vector<int> splits = ladder;
+  for (int q = 1; q <= 24; ++q) splits.push_back((b.nz + q - 1) / q);
+  std::sort(splits.begin(), splits.end());
+  splits.erase(std::unique(splits.begin(), splits.end()), splits.end());
+  const std::vector<int> cands2 = {1};
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -273,6 +283,10 @@ int autotune(lee_ctx* c, BlockData& b) {
     float best = 1e30f;
     int best_chunk = b.nz, best_kind = which == 0 ? b.stage_px : b.filter_px, best_ry = b.filter_ry;
     bool best_pair = b.filter_pair;
+    // the best scalar form (one or two rows) and its chunk, kept for the transposed filter of
+    // the adjoint, which the two-point kernel does not run
+    float best_scalar = 1e30f;
+    int best_scalar_chunk = b.nz, best_scalar_ry = b.filter_ry;
     // the scalar filter's forms (1: one tile row per thread row, 2: two rows, 3: two points per
     // thread) are timed with the chunk: each point's arithmetic is the same in all three
     const int nry = which == 1 && c->filter_form == 0 ? 3 : 1;
@@ -291,8 +305,7 @@ int autotune(lee_ctx* c, BlockData& b) {
         b.filter_pair = form == 3;
         set_filter_tiles(c, b);
       }
-      for (int ch : (d3 ? std::vector<int>(std::begin(cands3), std::end(cands3))
-                        : std::vector<int>(std::begin(cands2), std::end(cands2)))) {
+      for (int ch : (d3 ? (which == 1 ? splits : ladder) : cands2)) {
         if (d3 && ch > b.nz) continue;
         float tsum = 0.f;
         for (int rep = 0; rep < 4; ++rep) {  // the first run warms up
@@ -326,6 +339,11 @@ int autotune(lee_ctx* c, BlockData& b) {
           CK(cudaEventElapsedTime(&ms, e0, e1));
           if (rep > 0) tsum += ms;
         }
+        if (which == 1 && !b.filter_pair && tsum < best_scalar) {
+          best_scalar = tsum;
+          best_scalar_chunk = d3 ? ch : b.nz;
+          best_scalar_ry = b.filter_ry;
+        }
         if (tsum < best) {
           best = tsum;
           best_chunk = d3 ? ch : b.nz;
@@ -343,6 +361,8 @@ int autotune(lee_ctx* c, BlockData& b) {
       b.filter_px = best_kind;
       b.filter_ry = best_ry;
       b.filter_pair = best_pair;
+      b.tfilter_chunk = best_scalar < 1e30f ? best_scalar_chunk : best_chunk;
+      b.tfilter_ry = best_scalar < 1e30f ? best_scalar_ry : (best_pair ? 1 : best_ry);
       set_filter_tiles(c, b);
     }
   }

@@ -413,6 +413,8 @@ int lee_prepare(lee_ctx* c) {
       b.filter_ry = c->filter_form == 2 ? 2 : 1;
       b.filter_pair = c->filter_form == 3;
     }
+    b.tfilter_ry = b.filter_ry;
+    b.tfilter_chunk = 0;
     set_filter_tiles(c, b);
     if (b.tma) {
       // coefficient-layout traits of the stage kernel
