@@ -69,7 +69,10 @@ struct PairGeo {
   static_assert(((size_t)NS * FBP + 2 * U1 + ND * DP) * 4 % 8 == 0, "mbarriers need 8-byte alignment");
 };
 
-template <int HF>
+// COMP: the compensated form (the increments F - I, the carried rounding error in and out);
+// otherwise the plain filter and blend (out = (1 - blend) x + blend F x, the adjoint's transposed
+// filter, whose class rows are the transposed operator's).
+template <int HF, bool COMP>
 __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __grid_constant__ FieldMaps ym,
                                                      const __grid_constant__ TmaFilterParams<float> P) {
   using G = PairGeo<HF>;
@@ -158,7 +161,7 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
     const bool fin = active && kf >= k0 && kf < k1;
     const unsigned lf = lij + nxy * (unsigned)kf;
     F2 e0 = make_float2(0.f, 0.f);
-    if (fin) e0 = ld2(errp + lf);
+    if (COMP && fin) e0 = ld2(errp + lf);
     F2 u2 = make_float2(0.f, 0.f), d12 = make_float2(0.f, 0.f);
     if (p >= plo && p <= phi) {
       const int slot = rel % NS;
@@ -168,7 +171,7 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
       float* u1 = u1s + (rel & 1) * G::U1;
       F2 xc;
       const F2 d1 = xi(box + (ty + HF) * BX, xc);
-      const F2 u1c = add2(xc, d1);
+      const F2 u1c = COMP ? add2(xc, d1) : d1;
       st2(u1 + (ty + HF) * kPairTX + 2 * tx, u1c);
       // the eta halo rows, one per thread row (more than one for half-widths above 4)
 #pragma unroll
@@ -178,7 +181,7 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
           const int row = r < HF ? r : r + TY;
           F2 xh;
           const F2 dh = xi(box + row * BX, xh);
-          st2(u1 + row * kPairTX + 2 * tx, add2(xh, dh));
+          st2(u1 + row * kPairTX + 2 * tx, COMP ? add2(xh, dh) : dh);
         }
       }
       // every thread is past plane p - 1 (so the ring slot of plane p - 1 - h, finished there, is
@@ -204,14 +207,20 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
 #pragma unroll
         for (int o = -HF; o <= HF; ++o) dy = fmas(P.w[cy][o + HF], o == 0 ? u1c : ld2(col + o * kPairTX), dy);
       }
-      u2 = add2(u1c, dy);
-      d12 = add2(d1, dy);
+      if (COMP) {
+        u2 = add2(u1c, dy);
+        d12 = add2(d1, dy);
+      } else {
+        u2 = dy;
+      }
     }
 #pragma unroll
     for (int q = 0; q < NQ - 1; ++q) uq[q] = uq[q + 1];
     uq[NQ - 1] = u2;
-    st2(dme + ds * G::DP, d12);
-    ds = ds == HF ? 0 : ds + 1;
+    if (COMP) {
+      st2(dme + ds * G::DP, d12);
+      ds = ds == HF ? 0 : ds + 1;
+    }
     if (!fin) continue;
     const int cz = cls_of(kf, P.nz, P.nb);
     F2 fz = make_float2(0.f, 0.f);
@@ -224,6 +233,11 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
     }
     // the pre-filter pair of plane kf, still in its ring slot (kf >= plo)
     const F2 x0 = ld2(ring + ((rel - HF) % NS) * FBP + (ty + HF) * BX + c);
+    if (!COMP) {
+      // the one-row kernel's expression, lane by lane
+      st2(outp + lf, make_float2((1.f - P.blend) * x0.x + P.blend * fz.x, (1.f - P.blend) * x0.y + P.blend * fz.y));
+      continue;
+    }
     const F2 D = add2(ld2(dme + ds * G::DP), fz);
     const F2 t = fmas(P.blend, D, e0);
     const F2 sm = add2(x0, t);
@@ -234,18 +248,18 @@ __global__ void __launch_bounds__(256, HF <= 4 ? 4 : 3) k_filter_pair(const __gr
   }
 }
 
-template <int HF>
+template <int HF, bool COMP>
 cudaError_t go_filter_pair(const FieldMaps& in, const TmaFilterParams<float>& p, int tiles, int chunks,
                            cudaStream_t s) {
   using G = PairGeo<HF>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e =
-        cudaFuncSetAttribute(k_filter_pair<HF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES);
+        cudaFuncSetAttribute(k_filter_pair<HF, COMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_filter_pair<HF><<<dim3(tiles, chunks, p.V), 256, G::BYTES, s>>>(in, p);
+  k_filter_pair<HF, COMP><<<dim3(tiles, chunks, p.V), 256, G::BYTES, s>>>(in, p);
   return cudaGetLastError();
 }
 
@@ -261,15 +275,17 @@ void filter_pair_box(int hf, int* bx, int* by, int* tx, int* ty) {
   *ty = kTileY;
 }
 
-cudaError_t launch_filter_pair(const FieldMaps& in, const TmaFilterParams<float>& p, int hf, int tiles, int chunks,
-                               cudaStream_t s) {
-  if (p.nx % 2 != 0 || p.code[0] || !p.err[0] || !p.comp[0]) return cudaErrorInvalidValue;
-  switch (hf) {
-    case 2: return go_filter_pair<2>(in, p, tiles, chunks, s);
-    case 4: return go_filter_pair<4>(in, p, tiles, chunks, s);
-    case 5: return go_filter_pair<5>(in, p, tiles, chunks, s);
-    default: return cudaErrorInvalidValue;
-  }
+cudaError_t launch_filter_pair(const FieldMaps& in, const TmaFilterParams<float>& p, int hf, int comp, int tiles,
+                               int chunks, cudaStream_t s) {
+  if (p.nx % 2 != 0 || p.code[0] || (comp && (!p.err[0] || !p.comp[0]))) return cudaErrorInvalidValue;
+#define LEE_PAIR_CASE(HF)                                                                            \
+  if (hf == HF)                                                                                      \
+    return comp ? go_filter_pair<HF, true>(in, p, tiles, chunks, s) : go_filter_pair<HF, false>(in, p, tiles, chunks, s);
+  LEE_PAIR_CASE(2)
+  LEE_PAIR_CASE(4)
+  LEE_PAIR_CASE(5)
+#undef LEE_PAIR_CASE
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace lee

@@ -146,13 +146,29 @@ int adjoint_step(lee_ctx* c, double dt, const double* amps, double* gbar) {
     for (int v = 0; v < V; ++v) fp.out[v] = (T*)a.mu[v];
     fp.errflag = c->d_err;
     fp.wait_ns = c->wait_ns;
-    int bx, by;
-    filter_box(c, H, ry, &bx, &by);
+    // where the forward filter runs the two-point kernel (FP32, 3-D, no holes, even nxi), so does
+    // the transposed filter, in its plain form, with the forward's tuned chunk
+    const bool pair = sizeof(T) == 4 && b.filter_pair && filter_pair_half_width(H);
+    int bx, by, ptx, pty;
+    if (pair) {
+      filter_pair_box(H, &bx, &by, &ptx, &pty);
+      fp.tiles_x = b.ptiles_x;
+      fp.k_chunk = b.filter_chunk > 0 ? b.filter_chunk : b.nz;
+    } else {
+      filter_box(c, H, ry, &bx, &by);
+    }
     FieldMaps fm;
     int rc = field_maps(c, b, a.lam, bx, by, &fm);
     if (rc) return rc;
     const int chunks = c->cfg.num_dim == 3 ? (b.nz + fp.k_chunk - 1) / fp.k_chunk : 1;
-    CK(launch_filter_tma<T>(fm, fp, H, c->cfg.num_dim, 0, ry, filter_tiles_form(b, ry), chunks, c->stream));
+    bool done = false;
+    if constexpr (sizeof(T) == 4) {
+      if (pair) {
+        CK(launch_filter_pair(fm, fp, H, 0, b.ptiles_x * b.ptiles_y, chunks, c->stream));
+        done = true;
+      }
+    }
+    if (!done) CK(launch_filter_tma<T>(fm, fp, H, c->cfg.num_dim, 0, ry, filter_tiles_form(b, ry), chunks, c->stream));
     c->stats.kernel_launches += 1;
     mu = a.mu;
   } else if (c->cfg.filter_scheme != LEE_FILTER_NONE) {

@@ -235,7 +235,7 @@ int launch_filter_fused(lee_ctx* c, BlockData& b, void* const* in, void* const* 
     }
   } else if (pair) {
     if constexpr (sizeof(T) == 4) {
-      CK(launch_filter_pair(fm, fp, c->hf, b.ptiles_x * b.ptiles_y, chunks, c->stream));
+      CK(launch_filter_pair(fm, fp, c->hf, 1, b.ptiles_x * b.ptiles_y, chunks, c->stream));
     } else {
       return fail(c, LEE_ERR_UNSUPPORTED, "the two-point filter is the compensated form's");
     }

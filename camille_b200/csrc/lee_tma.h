@@ -82,13 +82,14 @@ cudaError_t launch_filter_tma(const FieldMaps& in, const TmaFilterParams<T>& p, 
 // kernel forms y_pre and its rounding error; same bits as the pair the last stage would write).
 cudaError_t launch_filter_tma_inc(const FieldMaps& y, const FieldMaps& inc, const TmaFilterParams<float>& p, int hf,
                                   int dim, int tiles, int chunks, cudaStream_t s);
-// The compensated FP32 fused filter with two neighbouring points per thread along xi
-// (lee_filter_pair.cu): 3-D blocks without holes of even nx, half-widths 2, 4 and 5; the same bits
-// as the one-row scalar filter. Its TMA box (bx x by) and tile (tx x ty), and the launch.
+// The FP32 fused filter with two neighbouring points per thread along xi (lee_filter_pair.cu):
+// 3-D blocks without holes of even nx, half-widths 2, 4 and 5; the compensated form gives the same
+// bits as the one-row scalar filter. Its TMA box (bx x by) and tile (tx x ty), and the launch.
 bool filter_pair_half_width(int hf);
 void filter_pair_box(int hf, int* bx, int* by, int* tx, int* ty);
-cudaError_t launch_filter_pair(const FieldMaps& in, const TmaFilterParams<float>& p, int hf, int tiles, int chunks,
-                               cudaStream_t s);
+// comp: the compensated form, else the plain filter and blend (the adjoint's transposed filter).
+cudaError_t launch_filter_pair(const FieldMaps& in, const TmaFilterParams<float>& p, int hf, int comp, int tiles,
+                               int chunks, cudaStream_t s);
 // The plane-marching adjoint stage (lee_adjoint_tma.cu): tensor maps of w (5 fields) then the
 // nine J*metrics fields, and its parameters.
 struct __align__(64) AdjMaps {

@@ -157,6 +157,24 @@ def test_recompute_replays_and_precisions_agree(product_lib):
     assert api.rel_l2(g32, g64) <= 1e-4
 
 
+def test_two_point_filter_forms_give_the_same_gradient(product_lib):
+    """With the forward filter in its two-point form the transposed filter of the reverse sweep
+    runs the two-point kernel too (plain form, the transposed rows as its classes): its gradient
+    agrees with the one-row form's to FP32 rounding, with the same objective (the forward filter's
+    bits are the same in both forms) and bit-identical recomputed traces."""
+    case = _grad_case(n=32, nsteps=24)
+    out = {}
+    for form in (1, 3):
+        s = api.Solver(product_lib, case, precision=api.FP32_COMPENSATED, filter_form=form)
+        assert s.info().filter_rows == form
+        dt = s.compute_dt()
+        out[form] = s.adjoint_gradient(case.nsteps, dt, checkpoint_every=8, recompute=True)
+    (J1, g1, m1), (J3, g3, m3) = out[1], out[3]
+    assert m1 == 0 and m3 == 0
+    assert J3 == J1
+    assert api.rel_l2(g3, g1) <= 1e-6
+
+
 def test_autograd_function_gradcheck(product_lib):
     import torch
 
