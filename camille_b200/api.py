@@ -87,6 +87,7 @@ SIGNATURES = {
     "advance_blocks": (C.c_int, [C.c_void_p, C.c_int, _DP]),
     "compute_dt_blocks": (C.c_int, [C.c_void_p, C.c_double, _DP]),
     "set_batch_shapes": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "set_batch_persistent": (C.c_int, [C.c_void_p, C.c_int]),
     "set_overset": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP, _IP, _IP, _IP, _DP, C.c_int, _IP, _IP]),
     "read_overset_file": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "get_overset": (C.c_int, [C.c_void_p, _IP, _LP, _IP, _LP, _DP]),

@@ -8,10 +8,12 @@
 // with asynchronous copies issued a few rows ahead. The arithmetic is that of the per-block
 // kernels (the generic operator order of lee_step.cu and the pointwise update of
 // lee_point.cuh), so a block gives the same bits batched or alone.
+#include <algorithm>
 #include <type_traits>
 
 #include "lee_internal.h"
 #include "lee_point.cuh"
+#include "lee_tma_util.cuh"
 
 namespace lee {
 namespace {
@@ -142,8 +144,8 @@ __device__ __forceinline__ void issue_row(T* ring, int slot, const T* const* fie
 // computed; the pointwise inputs of the next row are loaded into registers while this row is
 // computed. A work item is int4 (block, x0, ys, ye); a CTA takes `per` consecutive items.
 template <typename T, bool COMP, int TX, int PF, int CX>
-__global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __restrict__ prm,
-                                                    const int4* __restrict__ items, int nitems, int per) {
+__device__ __forceinline__ void batch_stage_run(const StageParams<T>* __restrict__ prm,
+                                                const int4* __restrict__ items, int t0, int t1) {
   constexpr int V = 4;
   constexpr int H = kFdH;
   constexpr int SW = CX * TX;  // strip width
@@ -158,7 +160,6 @@ __global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __rest
   const int tid = threadIdx.x;
   if (tid == 0) cur = -1;
   load_op(w, prm[0].fd, tid, TX);
-  const int t0 = blockIdx.x * per, t1 = min(t0 + per, nitems);
   for (int t = t0; t < t1; ++t) {
     const int4 it = items[t];
     __syncthreads();  // every thread is done with the previous item's ring and parameters
@@ -216,15 +217,14 @@ __global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __rest
 // increment form with the two-float sum), term for term. Fields are independent: a CTA takes
 // VF of them (fields blockIdx.y * VF ...), which keeps the register queues short.
 template <typename T, bool COMP, int TX, int PF, int VF>
-__global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* __restrict__ inst,
-                                                     const int4* __restrict__ items, int nitems, int per, OpTable op,
-                                                     T blend) {
+__device__ __forceinline__ void batch_filter_run(const BatchFilterInst<T>* __restrict__ inst,
+                                                 const int4* __restrict__ items, int t0, int t1, const OpTable& op,
+                                                 T blend, int vb) {
   constexpr int V = VF;
   constexpr int H = kFlH;
   constexpr int S = 7;
   constexpr int W = TX + 2 * H;
   constexpr int NX = H + PF + 2;  // state rows r - H - 1 .. r + PF around the row r being filtered in xi
-  const int vb = blockIdx.y * VF;  // the CTA's first field
   extern __shared__ __align__(16) unsigned char dsm[];
   T* X = reinterpret_cast<T*>(dsm);  // [NX][VF][W]
   __shared__ __align__(16) BatchFilterInst<T> P;
@@ -233,7 +233,6 @@ __global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* _
   const int tid = threadIdx.x;
   if (tid == 0) cur = -1;
   load_op(w, op, tid, TX);
-  const int t0 = blockIdx.x * per, t1 = min(t0 + per, nitems);
   for (int t = t0; t < t1; ++t) {
     const int4 it = items[t];
     __syncthreads();
@@ -327,6 +326,86 @@ __global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* _
   }
 }
 
+// The launches of one stage and of the filter: each CTA takes a run of `per` consecutive items
+// (the filter's CTAs in blockIdx.y take fields blockIdx.y * VF ...).
+template <typename T, bool COMP, int TX, int PF, int CX>
+__global__ void __launch_bounds__(TX) k_batch_stage(const StageParams<T>* __restrict__ prm,
+                                                    const int4* __restrict__ items, int nitems, int per) {
+  const int t0 = blockIdx.x * per;
+  batch_stage_run<T, COMP, TX, PF, CX>(prm, items, t0, min(t0 + per, nitems));
+}
+
+template <typename T, bool COMP, int TX, int PF, int VF>
+__global__ void __launch_bounds__(TX) k_batch_filter(const BatchFilterInst<T>* __restrict__ inst,
+                                                     const int4* __restrict__ items, int nitems, int per, OpTable op,
+                                                     T blend) {
+  const int t0 = blockIdx.x * per;
+  batch_filter_run<T, COMP, TX, PF, VF>(inst, items, t0, min(t0 + per, nitems), op, blend, (int)blockIdx.y * VF);
+}
+
+// Fields per filter CTA (of the four of a 2-D block).
+constexpr int kFilterVF = 1;
+
+// Barrier of all CTAs of a persistent launch (co-resident: the launch is cooperative). The
+// counter gb[0] and generation gb[1] start at zero (the host clears them before each launch). A
+// CTA's writes before the barrier are visible to every CTA after it (CTA barrier, then a
+// device-scope fence around the arrival and the wait). The wait is bounded: after `limit_ns`
+// nanoseconds (at once for 0) the CTA records the failure in the device flag and the barrier
+// returns false, and the CTA leaves the kernel, so the others give up at this barrier or the
+// next: nothing waits for ever.
+__device__ __forceinline__ bool grid_barrier(unsigned* gb, unsigned nblk, unsigned long long limit_ns, int* err) {
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = gb + 1;
+    const unsigned g = *gen;  // the current generation: it moves only once this CTA has arrived
+    __threadfence();
+    if (atomicAdd(gb, 1u) == nblk - 1) {
+      atomicExch(gb, 0u);  // reset before the release: no CTA arrives again before it sees it
+      __threadfence();
+      atomicAdd(gb + 1, 1u);
+    } else if (limit_ns == 0) {
+      ok = 0;
+    } else {
+      const unsigned long long t0 = gtimer();
+      for (unsigned it = 1; *gen == g; ++it)
+        if ((it & 63u) == 0u && gtimer() - t0 > limit_ns) {
+          ok = 0;
+          break;
+        }
+    }
+    __threadfence();
+    if (!ok) atomicExch(err, 1);
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
+// One whole batched step in one launch: the ns RK stages over the work list, each followed by a
+// grid barrier, then the filter over the same work list (each field of each item one unit). A
+// CTA takes the same run of items in every stage. The per-point arithmetic is that of the
+// per-phase launches (the same bodies), so the results are the same bits.
+template <typename T, bool COMP, int TX>
+__global__ void __launch_bounds__(TX) k_batch_step(const StageParams<T>* __restrict__ prm, int nbk, int ns,
+                                                   const BatchFilterInst<T>* __restrict__ inst,
+                                                   const int4* __restrict__ items, int nitems, OpTable op, T blend,
+                                                   unsigned* gbar, int* err, unsigned long long wait_ns) {
+  const int G = (int)gridDim.x, b = (int)blockIdx.x;
+  const int per = (nitems + G - 1) / G;
+  const int t0 = min(b * per, nitems), t1 = min(t0 + per, nitems);
+  for (int s = 0; s < ns; ++s) {
+    batch_stage_run<T, COMP, TX, 2, 1>(prm + (size_t)s * nbk, items, t0, t1);
+    if (!grid_barrier(gbar, (unsigned)G, wait_ns, err)) return;
+  }
+  constexpr int FG = 4 / kFilterVF;
+  const int nu = FG * nitems, pu = (nu + G - 1) / G;
+  const int u1 = min(nu, (b + 1) * pu);
+  for (int u = min(nu, b * pu); u < u1;) {
+    const int fg = u / nitems, i0 = u - fg * nitems, i1 = min(nitems, i0 + (u1 - u));
+    batch_filter_run<T, COMP, TX, 2, kFilterVF>(inst, items, i0, i1, op, blend, fg * kFilterVF);
+    u += i1 - i0;
+  }
+}
+
 template <typename T, int SW>
 size_t stage_smem() {
   return sizeof(T) * 4 * (2 * kFdH + 2 + 2) * (SW + 2 * kFdH);
@@ -343,9 +422,6 @@ cudaError_t go_stage(const StageParams<T>* prm, const int4* items, int n, int gr
   k_batch_stage<T, COMP, TX, 2, CX><<<(n + per - 1) / per, TX, smem, s>>>(prm, items, n, per);
   return cudaGetLastError();
 }
-
-// Fields per filter CTA (of the four of a 2-D block).
-constexpr int kFilterVF = 1;
 
 template <typename T, int TX>
 size_t filter_smem() {
@@ -475,6 +551,66 @@ int batch_filter_occupancy(int shape, int comp) {
   return occupancy_filter<T, false>(tx);
 }
 
+// The whole step in one persistent launch (work items of a shape with one column per stage
+// thread): as many CTAs as fit on the device at once, launched cooperatively so that they are
+// all resident (the launch fails rather than waits otherwise).
+template <typename T, bool COMP, int TX>
+cudaError_t go_step(const StageParams<T>* prm, int nbk, int ns, const BatchFilterInst<T>* inst, const int4* items,
+                    int n, const OpTable& op, T blend, unsigned* gbar, int* err, unsigned long long wait_ns,
+                    cudaStream_t s) {
+  const size_t smem = std::max(stage_smem<T, TX>(), filter_smem<T, TX>());
+  auto kern = k_batch_step<T, COMP, TX>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, nsm = 0, per_sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TX, smem)) != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int grid = std::max(1, std::min(per_sm * nsm, n));
+  if ((e = cudaMemsetAsync(gbar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(TX);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, prm, nbk, ns, inst, items, n, op, blend, gbar, err, wait_ns);
+}
+
+bool batch_step_shape(int shape) { return shape >= 0 && shape < kBatchShapes && kShapes[shape][2] == 1; }
+
+template <typename T>
+cudaError_t launch_batch_step(const StageParams<T>* prm, int nbk, int ns, const BatchFilterInst<T>* inst,
+                              const int4* items, int n, int shape, int comp, const OpTable& op, double blend,
+                              unsigned* gbar, int* err, unsigned long long wait_ns, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (!batch_step_shape(shape)) return cudaErrorInvalidValue;
+  const int tx = kShapes[shape][0];
+  const T b = (T)blend;
+#define LEE_STEP_CASE(C, X)                                                                     \
+  if (comp == (C ? 1 : 0) && tx == X)                                                           \
+    return go_step<T, C, X>(prm, nbk, ns, inst, items, n, op, b, gbar, err, wait_ns, s);
+  LEE_STEP_CASE(true, 64)
+  LEE_STEP_CASE(true, 128)
+  LEE_STEP_CASE(true, 256)
+  LEE_STEP_CASE(false, 64)
+  LEE_STEP_CASE(false, 128)
+  LEE_STEP_CASE(false, 256)
+#undef LEE_STEP_CASE
+  return cudaErrorInvalidValue;
+}
+
+template cudaError_t launch_batch_step<double>(const StageParams<double>*, int, int, const BatchFilterInst<double>*,
+                                               const int4*, int, int, int, const OpTable&, double, unsigned*, int*,
+                                               unsigned long long, cudaStream_t);
+template cudaError_t launch_batch_step<float>(const StageParams<float>*, int, int, const BatchFilterInst<float>*,
+                                              const int4*, int, int, int, const OpTable&, double, unsigned*, int*,
+                                              unsigned long long, cudaStream_t);
 template cudaError_t launch_batch_stage<double>(const StageParams<double>*, const int4*, int, int, int, int,
                                                 cudaStream_t);
 template cudaError_t launch_batch_stage<float>(const StageParams<float>*, const int4*, int, int, int, int,

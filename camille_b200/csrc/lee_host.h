@@ -219,6 +219,12 @@ struct lee_ctx {
     void* d_prm_direct = nullptr;  // the same with the amplitudes of the step being launched
     void* d_finst = nullptr;       // BatchFilterInst [block]
     std::vector<double> graph_dts;  // time steps d_prm_graph was built for
+    // lee_set_batch_persistent: -1 the per-phase launches, else the shape of the one persistent
+    // launch per step, its work list and its grid barrier (two words)
+    int pshape = -1;
+    int4* d_ptiles = nullptr;
+    int npt = 0;
+    unsigned* d_gbar = nullptr;
   } batch;
   // discrete adjoint (single block, uniform mean, no BC lines, holes or overset)
   struct {

@@ -225,6 +225,19 @@ int batch_step(lee_ctx* c, const std::vector<double>& dts, bool graph) {
     CK(cudaMemcpyAsync(bt.d_prm_direct, pr.data(), pr.size() * sizeof(pr[0]), cudaMemcpyHostToDevice, c->stream));
     prm = bt.d_prm_direct;
   }
+  if (bt.pshape >= 0) {
+    // the whole step in one persistent launch (stages and filter separated by grid barriers)
+    int e0 = mark(c);
+    CK(launch_batch_step<T>((const StageParams<T>*)prm, nbk, tb.ns, (const BatchFilterInst<T>*)bt.d_finst, bt.d_ptiles,
+                            bt.npt, bt.pshape, c->comp ? 1 : 0, c->comp ? c->fltd : c->flt, c->cfg.filter_blend,
+                            bt.d_gbar, c->d_err,
+                            c->wait_ns, c->stream));
+    int e1 = mark(c);
+    span(c, 0, e0, e1);
+    c->stats.stage_launches += 1;
+    c->stats.kernel_launches += 1;
+    return LEE_OK;
+  }
   for (int s = 0; s < tb.ns; ++s) {
     int e0 = mark(c);
     int rc = batch_launch_stage<T>(c, (const StageParams<T>*)prm + (size_t)s * nbk, bt.d_stiles, bt.nst, bt.sshape,
@@ -283,6 +296,29 @@ int lee_set_batch_shapes(lee_ctx* c, int stage_shape, int filter_shape) {
   bt.sgrid = std::min(bt.nst, nsm * occs);
   bt.fgrid = std::min(4 * bt.nft, nsm * occf);
   if (c->graph.exec) {  // captured launches name the old work lists
+    cudaGraphExecDestroy(c->graph.exec);
+    c->graph.exec = nullptr;
+  }
+  return LEE_OK;
+}
+
+int lee_set_batch_persistent(lee_ctx* c, int shape) {
+  if (!c) return LEE_ERR_ARG;
+  if (!c->prepared || !c->batch.active) return fail(c, LEE_ERR_STATE, "the context does not run batched kernels");
+  if (shape != -1 && !batch_step_shape(shape))
+    return fail(c, LEE_ERR_ARG, "persistent batch shape %d (one column per stage thread: 0 .. 4)", shape);
+  CK(cudaSetDevice(c->cfg.device));
+  auto& bt = c->batch;
+  int rc;
+  if (shape >= 0) {
+    const std::vector<int4> t = batch_tiles(c, shape);
+    if ((rc = dalloc(c, &bt.d_ptiles, t.size()))) return rc;
+    CK(cudaMemcpy(bt.d_ptiles, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    bt.npt = (int)t.size();
+    if (!bt.d_gbar && (rc = dalloc(c, &bt.d_gbar, 2))) return rc;
+  }
+  bt.pshape = shape;
+  if (c->graph.exec) {  // captured launches name the old schedule
     cudaGraphExecDestroy(c->graph.exec);
     c->graph.exec = nullptr;
   }

@@ -413,6 +413,15 @@ struct BatchFilterInst {
 
 constexpr int kBatchShapes = 7;
 void batch_shape(int shape, int* tx, int* ty);
+// A shape the persistent step launch takes (one column per stage thread: shapes 0..4).
+bool batch_step_shape(int shape);
+// The whole batched step (ns stages, then the filter) in one persistent cooperative launch over
+// the work items of `shape` (lee_batch.cu): gbar is a two-word barrier, err the device flag that
+// a barrier wait giving up after wait_ns sets.
+template <typename T>
+cudaError_t launch_batch_step(const StageParams<T>* prm, int nbk, int ns, const BatchFilterInst<T>* inst,
+                              const int4* items, int n, int shape, int comp, const OpTable& op, double blend,
+                              unsigned* gbar, int* err, unsigned long long wait_ns, cudaStream_t s);
 // one launch over the tile list (int4: block, x0, y0, 0) with the blocks' stage parameters
 template <typename T>
 cudaError_t launch_batch_stage(const StageParams<T>* prm, const int4* tiles, int ntiles, int shape, int comp,

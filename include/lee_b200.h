@@ -264,6 +264,15 @@ int lee_compute_dt_blocks(lee_ctx *ctx, double cfl, double *dt);
 /* Override the batched launches' work-item shapes that lee_prepare picked by timing (index
  * 0..6; lee_info reports the strip of each): every shape gives the same results. */
 int lee_set_batch_shapes(lee_ctx *ctx, int stage_shape, int filter_shape);
+/* One launch per batched step (no reference counterpart; the same bits as the per-phase
+ * launches): shape 0..4 (a work-item shape with one column per stage thread; lee_info's tiles
+ * give the strips) runs every RK stage and the filter of lee_advance_blocks in one persistent
+ * cooperative launch over that shape's work items, all of its CTAs resident, the phases separated
+ * by device-wide barriers. A barrier wait gives up after the lee_set_wait_limit limit and the
+ * call ends with LEE_ERR_TIMEOUT (the context stays usable); -1 (the default) goes back to one
+ * launch per stage and per filter. Call after lee_prepare, on a context that runs batched
+ * kernels. */
+int lee_set_batch_persistent(lee_ctx *ctx, int shape);
 /* Sizes and coefficient layout chosen by lee_prepare (no reference counterpart: the
  * reference has no timers or counters, finding F13). */
 typedef struct {

@@ -1487,6 +1487,11 @@ int orc_set_batch_shapes(orc_ctx *c, int stage_shape, int filter_shape) {
   return fail(c, LEE_ERR_STATE, "the oracle has no batched kernels");
 }
 
+int orc_set_batch_persistent(orc_ctx *c, int shape) {
+  (void)shape;
+  return fail(c, LEE_ERR_STATE, "the oracle has no batched kernels");
+}
+
 int orc_set_stage_kernel(orc_ctx *c, int kind) {
   (void)c;
   (void)kind;

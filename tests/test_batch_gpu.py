@@ -143,3 +143,63 @@ def test_batch_without_batched_kernels_matches_instances(product_lib, precision)
         alone = api.Solver(product_lib, cases.instance(case, b), precision=precision)
         alone.advance(case.nsteps, float(dts[b]))
         np.testing.assert_array_equal(s.download(b)[0], alone.download(0)[0])
+
+
+LEE_ERR_TIMEOUT = 8
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+def test_persistent_step_gives_the_same_bits(product_lib, precision):
+    """lee_set_batch_persistent: every RK stage and the filter of a batched step in one persistent
+    launch (grid barriers between the phases) give the bits of the per-phase launches, for every
+    shape it takes, with step graphs and with direct launches, in one launch per step."""
+    case = _batch(nsteps=6)
+    ref = api.Solver(product_lib, case, precision=precision)
+    dts = ref.compute_dt_blocks()
+    ref.advance_blocks(case.nsteps, dts)
+    want = [ref.download(b)[0] for b in range(len(case.blocks))]
+    for shape in range(5):
+        for graphs in (True, False):
+            s = api.Solver(product_lib, case, precision=precision)
+            assert product_lib.set_batch_persistent(s.ctx, shape) == api.LEE_OK
+            assert product_lib.set_finite_check(s.ctx, -1) == api.LEE_OK  # (its sentinel is a launch too)
+            s.set_graphs(graphs)
+            s.advance_blocks(case.nsteps, dts)
+            if not graphs:
+                assert s.stats().kernel_launches == case.nsteps
+            for b in range(len(case.blocks)):
+                np.testing.assert_array_equal(s.download(b)[0], want[b])
+            s.close()
+
+
+def test_persistent_step_refusals(product_lib):
+    case = _batch(nsteps=1)
+    s = api.Solver(product_lib, case)
+    assert product_lib.set_batch_persistent(s.ctx, 5) == api.LEE_ERR_ARG  # two columns per stage thread
+    assert product_lib.set_batch_persistent(s.ctx, -1) == api.LEE_OK
+    one = api.Solver(product_lib, cases.curvi3d(n=16, nsteps=1, halfwidth=2.0))
+    assert product_lib.set_batch_persistent(one.ctx, 0) == api.LEE_ERR_STATE  # not batched
+
+
+@pytest.mark.parametrize("precision", [api.FP64, api.FP32_COMPENSATED])
+def test_persistent_barrier_gives_up_and_the_context_recovers(product_lib, precision):
+    """With a wait limit of 0 every grid barrier of the persistent step gives up at once: the call
+    reports LEE_ERR_TIMEOUT (every CTA leaves the kernel, none waits), and with the default limit
+    restored the same context steps on and matches a fresh context."""
+    case = _batch(nsteps=3)
+    s = api.Solver(product_lib, case, precision=precision)
+    assert product_lib.set_batch_persistent(s.ctx, 0) == api.LEE_OK
+    dts = s.compute_dt_blocks()
+    s.advance_blocks(1, dts)
+    assert product_lib.set_wait_limit(s.ctx, 0.0) == api.LEE_OK
+    with pytest.raises(api.LeeError) as e:
+        s.advance_blocks(2, dts)
+    assert e.value.code == LEE_ERR_TIMEOUT
+    assert product_lib.set_wait_limit(s.ctx, -1.0) == api.LEE_OK
+    for b in range(len(case.blocks)):
+        s.upload(b, case.blocks[b].state)
+    s.advance_blocks(case.nsteps, dts)
+    ref = api.Solver(product_lib, case, precision=precision)
+    ref.advance_blocks(case.nsteps, dts)
+    for b in range(len(case.blocks)):
+        np.testing.assert_array_equal(s.download(b)[0], ref.download(b)[0])
