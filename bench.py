@@ -184,6 +184,25 @@ def batch_result(args, K: int, W: int, sample_clocks: bool) -> dict:
                      "state": [s.download(b)[0] for b in range(len(case.blocks))], "dts": dts,
                      "steps_done": W + K + min(K, args.kernel_steps)}
         s.close()
+    # the FP32-compensated step in one persistent launch (lee_set_batch_persistent), for each
+    # work-item shape it takes: the same steps, timed the same way, and its bits against the
+    # per-phase launches
+    pers = {}
+    for shape in range(5):
+        s = api.Solver(lib, case, precision=api.FP32_COMPENSATED)
+        s._chk(lib.set_batch_persistent(s.ctx, shape))
+        dts = res["fp32c"]["dts"]
+        s.advance_blocks(W, dts)
+        torch.cuda.synchronize()
+        s.advance_blocks(K, dts)
+        ms = s.stats().advance_ms
+        launches = s.stats().kernel_launches
+        s.advance_blocks(min(K, args.kernel_steps), dts)
+        same = all(np.array_equal(s.download(b)[0], res["fp32c"]["state"][b]) for b in range(len(case.blocks)))
+        pers[shape] = {"ms_per_step": ms / K, "value": npts * K / (ms / 1e3), "launches": int(launches),
+                       "same_bits_as_per_phase": bool(same)}
+        s.close()
+    best_shape = min(pers, key=lambda q: pers[q]["ms_per_step"])
     # one at a time, plain FP64, the same steps
     alone_s, errs = 0.0, []
     n_done = res["fp32c"]["steps_done"]
@@ -227,6 +246,12 @@ def batch_result(args, K: int, W: int, sample_clocks: bool) -> dict:
                      "step_frac": step_b * K / (res["fp32c"]["ms"] / 1e3) / 1e9 / peak,
                      "stage_strip": list(info.batch_stage_tile), "filter_strip": list(info.batch_filter_tile)},
         "gpu_launches": int(res["fp32c"]["launches"]), "clocks": clocks,
+        "persistent": {"note": "every stage and the filter of a step in one cooperative launch with grid barriers "
+                               "(lee_set_batch_persistent), FP32-compensated",
+                       "best_shape": best_shape, "value": pers[best_shape]["value"],
+                       "ms_per_step": pers[best_shape]["ms_per_step"],
+                       "over_per_phase": pers[best_shape]["value"] / value,
+                       "by_shape": {str(q): v for q, v in pers.items()}},
     }
 
 
@@ -249,7 +274,7 @@ def run_batch(args) -> None:
             "fp64": r["fp64"], "mixed_over_fp64": r["mixed_over_fp64"],
             "one_at_a_time_fp64": r["one_at_a_time_fp64"], "p_rel_l2_vs_fp64_alone": r["p_rel_l2_vs_fp64_alone"],
             "roofline": r["roofline"], "e2e": None, "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
-            "cpu_baseline": None,
+            "cpu_baseline": None, "persistent": r["persistent"],
         }
         print(json.dumps(line))
 
