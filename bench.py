@@ -255,6 +255,34 @@ def batch_result(args, K: int, W: int, sample_clocks: bool) -> dict:
     }
 
 
+def small_workload(name: str, K: int, W: int, err_steps: int) -> dict:
+    """A configuration that fits in the L2 (the 2-D pulse at 256^2 with 20-cell sponges, the
+    two-block cylinder overset layout): the step time of both precisions through lee_advance's
+    replayed step graphs (CUDA events, K steps after W), and the p' error of the compensated
+    form against FP64 after err_steps steps from the initial state."""
+    case = make_case(name, 256, err_steps)
+    lib = api.product_library()
+    npts = case.npoints
+    nblk = len(case.blocks)
+    ms, p = {}, {}
+    for form, prec in (("fp32c", api.FP32_COMPENSATED), ("fp64", api.FP64)):
+        s = api.Solver(lib, case, precision=prec)
+        dt = s.compute_dt(case.cfl) if form == "fp32c" else dt
+        s.advance(W, dt)
+        s.advance(K, dt)
+        ms[form] = s.stats().advance_ms / K
+        s.close()
+        e = api.Solver(lib, case, precision=prec)
+        e.advance(err_steps, dt)
+        p[form] = np.concatenate([e.download(b)[0][4].ravel() for b in range(nblk)])
+        e.close()
+    return {"workload": WORKLOADS[name].format(n=256), "points": npts, "steps": K,
+            "value": npts / (ms["fp32c"] / 1e3), "ms_per_step": ms["fp32c"],
+            "fp64": {"value": npts / (ms["fp64"] / 1e3), "ms_per_step": ms["fp64"]},
+            "mixed_over_fp64": ms["fp64"] / ms["fp32c"],
+            "p_rel_l2_vs_fp64": {"value": api.rel_l2(p["fp32c"], p["fp64"]), "steps": err_steps}}
+
+
 def run_batch(args) -> None:
     """`--workload batch`: the batch figures as the bench line."""
     import torch
@@ -431,6 +459,11 @@ def run_ours(args) -> None:
     if args.workload == "curvi3d" and not args.no_batch:
         batch = batch_result(args, args.batch_steps, W, sample_clocks=False)
 
+    # the two L2-resident configurations (2-D pulse at 256^2, cylinder overset), both precisions
+    small = None
+    if args.workload == "curvi3d" and not args.no_small:
+        small = {name: small_workload(name, args.small_steps, W, 500) for name in ("pulse2d", "cylinder")}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, lib, local)
@@ -472,6 +505,7 @@ def run_ours(args) -> None:
             "cpu_baseline": cpu,
             "adjoint": adjoint,
             "batch": batch,
+            "l2_resident": small,
         }
         print(json.dumps(line))
     solvers["fp32c"].close()
@@ -625,6 +659,8 @@ def main() -> int:
     ap.add_argument("--stage-kernel", type=int, default=-1,
                     help="lee_set_stage_kernel for the FP32-compensated run (-1: the library's default)")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--no-small", action="store_true", help="skip the pulse2d 256^2 and cylinder figures")
+    ap.add_argument("--small-steps", type=int, default=200)
     ap.add_argument("--ref-n", type=int, default=64)
     ap.add_argument("--ref-ranks", type=int, default=0, help="reference MPI ranks (0: the host's cores, at most 8)")
     args = ap.parse_args()
