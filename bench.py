@@ -327,6 +327,36 @@ def bench_case(n: int, nsteps: int) -> cases.Case:
     return case
 
 
+def replica_barrier(world: int, device: str = "cuda") -> None:
+    """Barrier of the replicas (each rank runs the whole workload on its own GPU; there is no
+    data-path exchange), then the device drained."""
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        dist.barrier()
+    if device == "cuda":
+        torch.cuda.synchronize()
+
+
+def replica_max(x: float, world: int, device: str = "cuda") -> float:
+    """The maximum over the ranks of a device-timed figure: the slowest replica sets the job's time."""
+    import torch
+    import torch.distributed as dist
+
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(points: int, steps: int, ms_max: float, world: int) -> float:
+    """Whole-job throughput of `world` replicas, each advancing `points` points by `steps` steps,
+    timed by the slowest (ms_max)."""
+    return world * points * steps / (ms_max / 1e3)
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -340,16 +370,10 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replica_barrier(world)
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(x, world)
 
     n = args.n
     case = make_case(args.workload, n, args.error_steps)
@@ -425,8 +449,8 @@ def run_ours(args) -> None:
     state_bytes = 5 * npts * 8
 
     r32, r64 = results["fp32c"], results["fp64"]
-    value = world * npts * K / (r32["ms"] / 1e3)
-    value64 = world * npts * K / (r64["ms"] / 1e3)
+    value = replica_value(npts, K, r32["ms"], world)
+    value64 = replica_value(npts, K, r64["ms"], world)
     st = r32["kstats"]
     info = r32["info"]
     peak, peak_kind = measured_hbm_gbs()
